@@ -1,0 +1,266 @@
+/*
+ * mbt.h -- C-ABI of libmbt, the B200 implementation of mbtrack's per-turn
+ * weak-weak tracking loop.
+ *
+ * The reference (fracul/mtrack, C99 + MPI) distributes bunches over MPI
+ * ranks: one manager and one worker per filled bucket, dispatched from
+ * mbtrack-mpi.c:131-155 into manager_weakweak/worker_weakweak
+ * (mbtrack-mpi.h:14-37).  libmbt replaces that seam: every filled bunch of
+ * the ring lives in one GPU's HBM and one context runs the loop of
+ * worker_weakweak.c:259-394 for all of them.
+ *
+ * Conventions
+ *   - every entry point returns 0 on success or a negative MBT_ERR_* code;
+ *     nothing calls exit(); mbt_last_error() gives a message;
+ *   - host pointers unless a name says "dev"; sizes are element counts;
+ *   - a context owns all of its device memory; one context per host thread
+ *     (distinct contexts are independent);
+ *   - particle coordinates are FP64 in the reference's particle_t order
+ *     (types.h:215-220): pos.xtau [s], pos.x [m], pos.z [m],
+ *     slope.xtau [rel. energy], slope.x [rad], slope.z [rad].  A "soa6"
+ *     buffer holds the six coordinate arrays of one bunch back to back,
+ *     each np doubles, in that order.
+ *   - statistics are written per turn per bunch as 12 doubles, in the order
+ *     the reference worker sends them to the manager
+ *     (worker_weakweak.c:321-324): pos[3], pos_sigma[3], slope[3],
+ *     slope_sigma[3], each indexed LON, HOR, VER (def.h:346-353).
+ */
+#ifndef MBT_H
+#define MBT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MBT_OK               0
+#define MBT_ERR_INVALID     -1   /* bad argument or unsupported configuration */
+#define MBT_ERR_CUDA        -2   /* a CUDA runtime call failed */
+#define MBT_ERR_NOMEM       -3   /* device or host allocation failed */
+#define MBT_ERR_CONFIG      -4   /* configuration file missing, unreadable or incomplete */
+#define MBT_ERR_STATE       -5   /* call made in the wrong order */
+#define MBT_ERR_TIMEOUT     -6   /* a bounded device wait gave up */
+#define MBT_ERR_NODEVICE    -7   /* no CUDA device: libmbt has no CPU path */
+
+#define MBT_LON 0
+#define MBT_HOR 1
+#define MBT_VER 2
+
+#define MBT_MAX_RES   32   /* short-range resonators (ring_t.resonators) */
+#define MBT_MAX_LR     8   /* long-range resonators per plane */
+#define MBT_MAX_AHC    8   /* active harmonic cavities */
+#define MBT_MAX_NCELL 1024 /* self-field bins */
+
+/* Noise source of the quantum-excitation term (transform_weak.c:71-75,
+ * 134-138, 182-186). */
+#define MBT_NOISE_PHILOX   0  /* counter-based Philox4x32-10 normals */
+#define MBT_NOISE_INJECTED 1  /* deviates supplied by mbt_set_deviates() */
+
+/*
+ * Everything the per-turn loop reads, after the reference's set-up
+ * (setup_ring_parameters input.c:1553-1695, setup_tracking_parameters
+ * input.c:1698-1772, macrop_model_setup_parameters input.c:1775-1831,
+ * selffield_model_init transform_weak.c:201-239).  Field names follow
+ * ring_t / tracking_t / bunch_macroparticle_model_t / selffield_model_t.
+ * Units are the reference's.
+ */
+typedef struct mbt_params {
+  /* ring_t (types.h:60-129) */
+  int    nharm;          /* harmonic number h */
+  double E0;             /* [GeV] */
+  double T0;             /* revolution time [s] */
+  double wrf;            /* angular RF frequency [rad/s] */
+  double Vrf0;           /* total RF voltage [MV] */
+  double phai0;          /* synchronous phase [rad] */
+  double Urad;           /* U0 / E0 */
+  double De;             /* 2 T0 / taue */
+  double ac;             /* momentum compaction */
+  double QH0, QV0;       /* betatron tunes */
+  double Gzix, Gziz;     /* normalised chromaticities */
+  double CHH, CHV, CVH, CVV;   /* amplitude-dependent tune coefficients */
+  int    amp_dep_qv;     /* AmpDependdQV: gates amplitude detuning in both planes */
+  double beta1[3], alpha1[3], gamma1[3];   /* Twiss at the kick point, [LON,HOR,VER] */
+  double dispH1, disppH1; /* horizontal dispersion and its derivative */
+  double taue, taux, tauz; /* damping times [s] */
+  double Lc;             /* circumference [m] */
+  double rhorw;          /* wall resistivity [Ohm m] */
+  double beffH[2], beffV[2], beffL[2];  /* effective radii (beffH[0] = beffH3 ...) */
+  double Iring;          /* ring current [mA] */
+  int    ideal_hc;       /* EnableIdealHC */
+  int    m_aHC;          /* ideal HC harmonic */
+  double phi_n, HC_k;    /* ideal HC phase and amplitude ratio */
+  int    n_active_hc;
+  double ahc_vpeak[MBT_MAX_AHC], ahc_nhc[MBT_MAX_AHC], ahc_phi[MBT_MAX_AHC];
+
+  /* tracking_t (types.h:145-187) */
+  int    track_plane[3];
+  int    quantum;        /* EnableQuantum */
+  int    rw_long;        /* EnableRW_long */
+  int    Nmlt;           /* turns of RW memory */
+  int    triggerRW;
+  long   nrev_tot, nrev_mon;
+
+  /* bunch_macroparticle_model_t (bunch.h:22-50), SI units */
+  int    np_model;       /* Np of the model (bunchModel.Np) */
+  int    iseed[3];
+  double pos_offset[3], slope_offset[3];
+  double pos_sgm[3], slope_sgm[3];
+  double correlate[3];
+
+  /* selffield_model_t (types.h:190-209) */
+  int    ncell;          /* 0 = no self-field binning */
+  double nsigma;
+  double dT;             /* bin width in units of sigma_tau */
+  double sigma_tau;      /* [s] */
+  double RsisL, aindL;   /* purely resistive / inductive longitudinal terms */
+  int    planeL, planeV, planeH;   /* number of short-range wakes per plane */
+
+  /* long-range resonators (LR_resonator_t, types.h:33-47), per plane */
+  int    n_lr[3];
+  double lr_Rs[3][MBT_MAX_LR];
+  double lr_wr[3][MBT_MAX_LR];
+  double lr_Q[3][MBT_MAX_LR];
+  int    lr_init_turns;  /* Nbumax / h: turns of wake_phasor_init */
+
+  /* rf_feedback_t (feedback_rf.h:5-12) */
+  int    rffb;           /* has_rf_feedback after set-up */
+  int    rffb_resonator; /* 1-based index into the LON long-range resonators */
+  int    rffb_len;       /* averaging length (absolute value) */
+  int    rffb_off_after_init; /* negative averaging_length: correct once, then off */
+  double rffb_vrf_design, rffb_phi0_design;
+} mbt_params;
+
+typedef struct mbt_ctx mbt_ctx;
+
+/* ---- configuration (C host; reference semantics of input.c) ---------- */
+
+/* Read an mbtrack .conf file and run the reference set-up chain
+ * (read_conf_file input.c:278-850, setup_ring_parameters :1553-1695,
+ * macrop_model_setup_parameters :1775-1831, e_beam_setup :1289-1512,
+ * setup_tracking_parameters :1698-1772).  Fills *p and the fill pattern:
+ * bucket[i], ib_frac[i] for the nbunch filled buckets (arrays of at least
+ * p->nharm entries, may be NULL to query nbunch only).  fix_rw_beff != 0
+ * reads beffH3/beffV3 for long-range resistive wall even without
+ * EnableRW_short (the reference leaves them 0, input.c:465-478).
+ * scratch_dir receives nothing; it is accepted for interface symmetry
+ * with the reference's work directory and may be NULL. */
+int mbt_config_load(const char *conf_path, int fix_rw_beff, mbt_params *p,
+                    int *nbunch, int *bucket, double *ib_frac);
+
+/* Short-range Green's functions for ncell bins (construct_greensfunc_resonator
+ * transform_weak.c:288-403, construct_greensfunc_RW :473-547), plus the
+ * resulting planeL/planeV/planeH counts written back into *p.
+ * Gl, Gv, Gh: arrays of p->ncell doubles (zeroed by the call). */
+int mbt_config_greens(const char *conf_path, mbt_params *p,
+                      double *Gl, double *Gv, double *Gh);
+
+/* Bunch current [A] of filled bunch i (manager_weakweak.c:74-75). */
+double mbt_bunch_current(const mbt_params *p, int nbunch, double ib_frac);
+
+/* ---- context --------------------------------------------------------- */
+
+/* Create a tracking context on the current CUDA device.
+ * nbunch filled bunches; bucket[i] is the bucket number of bunch i
+ * (ascending), np[i] its macroparticle count, ib[i] its current [A].
+ * Gl/Gv/Gh: short-range Green's functions (p->ncell each, or NULL when the
+ * corresponding plane count is 0).  noise_mode: MBT_NOISE_*; seed keys the
+ * Philox stream.  Replaces the worker set-up of worker_weakweak.c:19-255
+ * for every bunch at once. */
+int mbt_create(const mbt_params *p, int nbunch, const int *bucket,
+               const int *np, const double *ib,
+               const double *Gl, const double *Gv, const double *Gh,
+               int noise_mode, uint64_t seed, mbt_ctx **out);
+
+int mbt_destroy(mbt_ctx *ctx);
+
+/* Message of the last failing call on this context (or of a failed
+ * mbt_create when ctx is NULL). */
+int mbt_last_error(const mbt_ctx *ctx, char *buf, size_t len);
+
+/* Copy one bunch's coordinates in (host soa6, np doubles per coordinate).
+ * Allowed before mbt_prepare and between runs. */
+int mbt_load_particles(mbt_ctx *ctx, int ibunch, const double *soa6, int np);
+
+/* Copy all bunches' coordinates in at once from one host buffer laid out
+ * bunch after bunch, each bunch a soa6 block of np[i] particles. */
+int mbt_load_all(mbt_ctx *ctx, const double *soa6_all);
+
+/* Draw a matched Gaussian beam on the device (replaces
+ * weak_bunch_normal_distribution bunch_weak.c:86-105 with a counter-based
+ * generator keyed by seed, bunch and particle). */
+int mbt_generate_beam(mbt_ctx *ctx, uint64_t seed);
+
+/* Copy one bunch's coordinates out.  Any long-range resistive-wall kick
+ * still pending from the last turn (it is applied at the start of the
+ * next turn on the device) is included in the copy. */
+int mbt_get_particles(mbt_ctx *ctx, int ibunch, double *soa6, int np);
+int mbt_get_all(mbt_ctx *ctx, double *soa6_all);
+
+/* Initial binning, statistics, long-range wake and RF-feedback
+ * initialisation and resistive-wall history fill
+ * (worker_weakweak.c:109-219).  init_stats (may be NULL) receives the
+ * initial statistics, nbunch x 12 doubles. */
+int mbt_prepare(mbt_ctx *ctx, double *init_stats);
+
+/* Deviates for MBT_NOISE_INJECTED: nturns turns, each turn the bunches in
+ * order, each bunch in the reference draw order (transform_weak.c:73,
+ * 136-137, 184-185): np LON deviates, then 2 np VER (pos, slope per
+ * particle) if VER is tracked, then 2 np HOR.  Values are the reference's
+ * float Marsaglia-polar deviates.  They are consumed by the next nturns
+ * turns. */
+int mbt_set_deviates(mbt_ctx *ctx, const float *dev, long nturns);
+
+/* Run nturns turns of the weak-weak loop (worker_weakweak.c:259-394) for
+ * all bunches.  stats (may be NULL): nturns x nbunch x 12 doubles. */
+int mbt_run_turns(mbt_ctx *ctx, long nturns, double *stats);
+
+/* Same loop, but particles come from and return to host buffers in the
+ * same call (one soa6 block per bunch, bunch after bunch): the call a
+ * host-resident caller makes.  particles may be pinned memory. */
+int mbt_track(mbt_ctx *ctx, double *particles, long nturns, double *stats);
+
+/* Turn counter, RF parameters and long-range phasors after the last turn. */
+typedef struct mbt_state {
+  long   turn;
+  double Vrf0, phai0;
+  double phasor[3][MBT_MAX_LR][2];
+  int    n_trash_low, n_trash_high;   /* summed over bunches */
+} mbt_state;
+int mbt_get_state(mbt_ctx *ctx, mbt_state *st);
+
+/* Histograms of the last binning pass for bunch ibunch (ncell each):
+ * clamped count/Σz/Σx (transform_weak.c:608-631) and dropped
+ * count/Σx/Σz (fnp_ring_update, transform_weak.c:839-865). */
+int mbt_get_histograms(mbt_ctx *ctx, int ibunch, double *fnp, double *dipV,
+                       double *dipH, double *ring_lon, double *ring_hor,
+                       double *ring_ver);
+
+/* Device time of the last mbt_run_turns split by kernel [ms] (CUDA events):
+ * out[0] particle pass, out[1] bunch reduction and wakes, out[2] ring-wide
+ * phasor scan, out[3] total.  Also returns the number of kernel launches
+ * per turn in *launches_per_turn. */
+int mbt_last_timing(mbt_ctx *ctx, double out[4], int *launches_per_turn);
+
+/* ---- per-step device entry points (device pointers) ------------------- */
+
+/* Faddeeva w(z) for n points (complex_errorfunc_wofz_algo680,
+ * physic.c:75-301).  flag (may be NULL) receives the reference's iflag:
+ * 1 ok, -1 overflow region.  stream: a cudaStream_t or NULL. */
+int mbt_wofz_dev(long n, const double *x_dev, const double *y_dev,
+                 double *re_dev, double *im_dev, int *flag_dev, void *stream);
+
+/* Bassetti-Erskine field of a Gaussian slice at n points
+ * (fbi_weakstrong.c:154-197): dx,dy offsets [m] from the slice centre,
+ * sx, sy rms sizes [m] (sx > sy), factdq = dQ / (2 eps0 sqrt(pi) c dt)
+ * as in fbi_weakstrong.c:156 but without the 1/factBE, which is derived
+ * from sx, sy.  Writes Ex, Ey. */
+int mbt_be_field_dev(long n, const double *dx_dev, const double *dy_dev,
+                     double sx, double sy, double factdq,
+                     double *ex_dev, double *ey_dev, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MBT_H */

@@ -1,0 +1,79 @@
+"""ctypes mirror of the C-ABI structures declared in include/mbt.h.
+
+The layouts must match the C declarations field for field; libmbt exports
+``mbt_params_size()`` so the loader can check the size at import time.
+"""
+import ctypes
+
+MBT_MAX_RES = 32
+MBT_MAX_LR = 8
+MBT_MAX_AHC = 8
+MBT_MAX_NCELL = 1024
+
+MBT_OK = 0
+MBT_ERR_INVALID = -1
+MBT_ERR_CUDA = -2
+MBT_ERR_NOMEM = -3
+MBT_ERR_CONFIG = -4
+MBT_ERR_STATE = -5
+MBT_ERR_TIMEOUT = -6
+MBT_ERR_NODEVICE = -7
+
+MBT_NOISE_PHILOX = 0
+MBT_NOISE_INJECTED = 1
+
+LON, HOR, VER = 0, 1, 2
+
+_d = ctypes.c_double
+_i = ctypes.c_int
+_l = ctypes.c_long
+
+
+class MbtParams(ctypes.Structure):
+    """mbt_params (include/mbt.h)."""
+    _fields_ = [
+        ("nharm", _i), ("E0", _d), ("T0", _d), ("wrf", _d), ("Vrf0", _d),
+        ("phai0", _d), ("Urad", _d), ("De", _d), ("ac", _d),
+        ("QH0", _d), ("QV0", _d), ("Gzix", _d), ("Gziz", _d),
+        ("CHH", _d), ("CHV", _d), ("CVH", _d), ("CVV", _d),
+        ("amp_dep_qv", _i),
+        ("beta1", _d * 3), ("alpha1", _d * 3), ("gamma1", _d * 3),
+        ("dispH1", _d), ("disppH1", _d),
+        ("taue", _d), ("taux", _d), ("tauz", _d),
+        ("Lc", _d), ("rhorw", _d),
+        ("beffH", _d * 2), ("beffV", _d * 2), ("beffL", _d * 2),
+        ("Iring", _d),
+        ("ideal_hc", _i), ("m_aHC", _i), ("phi_n", _d), ("HC_k", _d),
+        ("n_active_hc", _i),
+        ("ahc_vpeak", _d * MBT_MAX_AHC), ("ahc_nhc", _d * MBT_MAX_AHC),
+        ("ahc_phi", _d * MBT_MAX_AHC),
+        ("track_plane", _i * 3), ("quantum", _i), ("rw_long", _i),
+        ("Nmlt", _i), ("triggerRW", _i), ("nrev_tot", _l), ("nrev_mon", _l),
+        ("np_model", _i), ("iseed", _i * 3),
+        ("pos_offset", _d * 3), ("slope_offset", _d * 3),
+        ("pos_sgm", _d * 3), ("slope_sgm", _d * 3), ("correlate", _d * 3),
+        ("ncell", _i), ("nsigma", _d), ("dT", _d), ("sigma_tau", _d),
+        ("RsisL", _d), ("aindL", _d),
+        ("planeL", _i), ("planeV", _i), ("planeH", _i),
+        ("n_lr", _i * 3),
+        ("lr_Rs", (_d * MBT_MAX_LR) * 3), ("lr_wr", (_d * MBT_MAX_LR) * 3),
+        ("lr_Q", (_d * MBT_MAX_LR) * 3),
+        ("lr_init_turns", _i),
+        ("rffb", _i), ("rffb_resonator", _i), ("rffb_len", _i),
+        ("rffb_off_after_init", _i),
+        ("rffb_vrf_design", _d), ("rffb_phi0_design", _d),
+    ]
+
+    def copy(self):
+        c = MbtParams()
+        ctypes.memmove(ctypes.byref(c), ctypes.byref(self), ctypes.sizeof(self))
+        return c
+
+
+class MbtState(ctypes.Structure):
+    """mbt_state (include/mbt.h)."""
+    _fields_ = [
+        ("turn", _l), ("Vrf0", _d), ("phai0", _d),
+        ("phasor", ((_d * 2) * MBT_MAX_LR) * 3),
+        ("n_trash_low", _i), ("n_trash_high", _i),
+    ]

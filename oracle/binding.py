@@ -1,0 +1,265 @@
+"""ctypes bindings of the oracle (liboracle.so, the C restatement) and of the
+reference harness (_ref/libmbtref.so, the reference's own sources).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, smoke() and bench.py's CPU
+baseline as the checker, never by the product.
+"""
+import ctypes
+import os
+import re
+import shutil
+import subprocess
+import tempfile
+
+import numpy as np
+
+from mbtrack_b200.abi import MbtParams
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libmbtref.so")
+REFERENCE_DIR = "/root/reference"
+
+_vp = ctypes.c_void_p
+_P = ctypes.POINTER
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def build_oracle(force=False):
+    """Compile liboracle.so (plain C, gcc) if missing."""
+    if force or not os.path.exists(ORACLE_SO):
+        subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
+    return ORACLE_SO
+
+
+def reference_available():
+    return os.path.isdir(os.path.join(REFERENCE_DIR, "src"))
+
+
+def build_reference(force=False):
+    """Compile the reference's own sources into _ref/libmbtref.so.
+
+    Needs the reference tree (present in the build container only); on a
+    machine without it an already built library is used as is."""
+    if os.path.exists(REF_SO) and not force:
+        return REF_SO
+    if not reference_available():
+        return None
+    subprocess.check_call(["make", "-s", "-C", HERE, "ref", "REF=" + REFERENCE_DIR])
+    return REF_SO
+
+
+def conf_with(src, dst, **overrides):
+    """Copy a .conf file replacing `key = value` lines (each key once)."""
+    text = open(src).read()
+    for k, v in overrides.items():
+        text, n = re.subn(r"(?m)^(\s*%s\s*=).*$" % re.escape(k), r"\g<1> %s" % v, text)
+        if n != 1:
+            raise KeyError("%s appears %d times in %s" % (k, n, src))
+    with open(dst, "w") as f:
+        f.write(text)
+    return dst
+
+
+class Oracle:
+    """The C restatement (mbt_oracle.c)."""
+
+    def __init__(self, params, bucket, np_, ib, Gl=None, Gv=None, Gh=None):
+        self.lib = ctypes.CDLL(build_oracle())
+        L = self.lib
+        L.orc_create.restype = _vp
+        L.orc_create.argtypes = [_P(MbtParams), ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp]
+        L.orc_run.restype = ctypes.c_long
+        L.orc_run.argtypes = [_vp, ctypes.c_long, _vp, _vp, _vp, ctypes.c_long]
+        L.orc_deviates_per_turn.restype = ctypes.c_long
+        L.orc_deviates_per_turn.argtypes = [_vp]
+        for f in ("orc_generate_beam", "orc_prepare", "orc_set_particles", "orc_get_particles"):
+            getattr(L, f).restype = ctypes.c_int
+        L.orc_generate_beam.argtypes = [_vp]
+        L.orc_prepare.argtypes = [_vp, _vp]
+        L.orc_set_particles.argtypes = [_vp, ctypes.c_int, _vp]
+        L.orc_get_particles.argtypes = [_vp, ctypes.c_int, _vp]
+        L.orc_state.argtypes = [_vp, ctypes.c_int, _vp, _vp]
+        L.orc_trash.argtypes = [_vp, ctypes.c_int, _vp, _vp]
+        L.orc_histograms.argtypes = [_vp, ctypes.c_int] + [_vp] * 6
+        L.orc_destroy.argtypes = [_vp]
+        self.p = params.copy()
+        self.bucket = np.ascontiguousarray(bucket, dtype=np.int32)
+        self.np = np.ascontiguousarray(np_, dtype=np.int32)
+        self.ib = np.ascontiguousarray(ib, dtype=np.float64)
+        self.nb = len(self.bucket)
+        g = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (Gl, Gv, Gh)]
+        self._g = g
+        self.h = L.orc_create(ctypes.byref(self.p), self.nb, _ptr(self.bucket), _ptr(self.np),
+                              _ptr(self.ib), _ptr(g[0]), _ptr(g[1]), _ptr(g[2]))
+        if not self.h:
+            raise RuntimeError("orc_create failed")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def generate_beam(self):
+        self.lib.orc_generate_beam(self.h)
+
+    def set_particles(self, ib, soa6):
+        a = np.ascontiguousarray(soa6, dtype=np.float64)
+        assert a.size == 6 * self.np[ib]
+        self.lib.orc_set_particles(self.h, ib, _ptr(a))
+
+    def get_particles(self, ib):
+        a = np.empty(6 * self.np[ib])
+        self.lib.orc_get_particles(self.h, ib, _ptr(a))
+        return a.reshape(6, self.np[ib])
+
+    def prepare(self):
+        s = np.zeros(12 * self.nb)
+        self.lib.orc_prepare(self.h, _ptr(s))
+        return s.reshape(self.nb, 12)
+
+    def deviates_per_turn(self):
+        return self.lib.orc_deviates_per_turn(self.h)
+
+    def run(self, nturns, dev_in=None, record=False):
+        st = np.zeros(nturns * self.nb * 12)
+        dev_out = None
+        if record:
+            dev_out = np.zeros(max(1, nturns * self.deviates_per_turn()), dtype=np.float32)
+        if dev_in is not None:
+            dev_in = np.ascontiguousarray(dev_in, dtype=np.float32)
+        self.lib.orc_run(self.h, nturns, _ptr(st), _ptr(dev_in), _ptr(dev_out),
+                         0 if dev_out is None else dev_out.size)
+        st = st.reshape(nturns, self.nb, 12)
+        return (st, dev_out) if record else st
+
+    def state(self, ib=0):
+        v = np.zeros(2)
+        ph = np.zeros(2 * 8)
+        self.lib.orc_state(self.h, ib, _ptr(v), _ptr(ph))
+        return v, ph
+
+    def trash(self, ib):
+        lo, hi = ctypes.c_int(), ctypes.c_int()
+        self.lib.orc_trash(self.h, ib, ctypes.byref(lo), ctypes.byref(hi))
+        return lo.value, hi.value
+
+    def histograms(self, ib):
+        n = self.p.ncell
+        arr = [np.zeros(n) for _ in range(6)]
+        self.lib.orc_histograms(self.h, ib, *[_ptr(a) for a in arr])
+        return arr
+
+
+def wofz(x, y):
+    """Vectorised oracle w(z): returns (re, im, flag)."""
+    lib = ctypes.CDLL(build_oracle())
+    x = np.ascontiguousarray(x, dtype=np.float64).ravel()
+    y = np.ascontiguousarray(y, dtype=np.float64).ravel()
+    re, im = np.empty_like(x), np.empty_like(x)
+    fl = np.empty(x.size, dtype=np.int32)
+    lib.orc_wofz_n.argtypes = [ctypes.c_long, _vp, _vp, _vp, _vp, _vp]
+    lib.orc_wofz_n(x.size, _ptr(x), _ptr(y), _ptr(re), _ptr(im), _ptr(fl))
+    return re, im, fl
+
+
+def be_field(dx, dy, sgm_xx_mm, sgm_zz_mm, factdq):
+    lib = ctypes.CDLL(build_oracle())
+    dx = np.ascontiguousarray(dx, dtype=np.float64).ravel()
+    dy = np.ascontiguousarray(dy, dtype=np.float64).ravel()
+    ex, ey = np.empty_like(dx), np.empty_like(dx)
+    lib.orc_be_field_n.argtypes = [ctypes.c_long, _vp, _vp, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, _vp, _vp]
+    lib.orc_be_field_n(dx.size, _ptr(dx), _ptr(dy), sgm_xx_mm, sgm_zz_mm, factdq, _ptr(ex), _ptr(ey))
+    return ex, ey
+
+
+class Reference:
+    """The reference's own sources run by ref_harness.c."""
+
+    _count = 0
+
+    def __init__(self, conf, fix_rw_beff=True, workdir="/tmp"):
+        so = build_reference()
+        if so is None:
+            raise RuntimeError("reference harness unavailable")
+        # The reference keeps its state in globals and statics (bunch.c's
+        # RNG cache among them): load a private copy of the library per
+        # instance so instances never share them.
+        Reference._count += 1
+        priv = os.path.join(tempfile.gettempdir(), "libmbtref_%d_%d.so" % (os.getpid(), Reference._count))
+        shutil.copyfile(so, priv)
+        self.lib = L = ctypes.CDLL(priv, mode=getattr(os, "RTLD_LOCAL", 0))
+        os.unlink(priv)
+        L.refh_init.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
+        L.refh_run.restype = ctypes.c_int
+        L.refh_run.argtypes = [ctypes.c_long, _vp, _vp, ctypes.c_long]
+        L.refh_prepare.argtypes = [_vp]
+        L.refh_get_particles.argtypes = [ctypes.c_int, _vp]
+        L.refh_set_particles.argtypes = [ctypes.c_int, _vp]
+        L.refh_bunch_info.argtypes = [_vp, _vp, _vp]
+        L.refh_state.argtypes = [ctypes.c_int, _vp, _vp]
+        L.refh_trash.argtypes = [ctypes.c_int, _vp, _vp]
+        L.refh_greens.argtypes = [ctypes.c_int, _vp, _vp, _vp, _vp]
+        L.refh_fill_params.argtypes = [_P(MbtParams)]
+        L.refh_param_table.argtypes = [_vp, _vp, ctypes.c_int]
+        self.nb = L.refh_init(conf.encode(), workdir.encode(), int(fix_rw_beff))
+        if self.nb <= 0:
+            raise RuntimeError("refh_init failed: %d" % self.nb)
+        self.bucket = np.zeros(self.nb, dtype=np.int32)
+        self.np = np.zeros(self.nb, dtype=np.int32)
+        self.ib = np.zeros(self.nb)
+        L.refh_bunch_info(_ptr(self.bucket), _ptr(self.np), _ptr(self.ib))
+        self.prepared = False
+
+    def deviates_exact(self):
+        return bool(self.lib.refh_deviates_exact())
+
+    def get_particles(self, ib):
+        a = np.empty(6 * self.np[ib])
+        self.lib.refh_get_particles(ib, _ptr(a))
+        return a.reshape(6, self.np[ib])
+
+    def set_particles(self, ib, soa6):
+        a = np.ascontiguousarray(soa6, dtype=np.float64)
+        self.lib.refh_set_particles(ib, _ptr(a))
+
+    def prepare(self):
+        s = np.zeros(12 * self.nb)
+        self.lib.refh_prepare(_ptr(s))
+        self.prepared = True
+        return s.reshape(self.nb, 12)
+
+    def params(self):
+        p = MbtParams()
+        self.lib.refh_fill_params(ctypes.byref(p))
+        return p
+
+    def greens(self, ib=0):
+        p = self.params()
+        n = p.ncell
+        g = [np.zeros(max(n, 1)) for _ in range(3)]
+        planes = np.zeros(3, dtype=np.int32)
+        self.lib.refh_greens(ib, _ptr(g[0]), _ptr(g[1]), _ptr(g[2]), _ptr(planes))
+        return g[0][:n], g[1][:n], g[2][:n], planes
+
+    def run(self, nturns, record=False, dev_cap=0):
+        st = np.zeros(nturns * self.nb * 12)
+        dev = np.zeros(max(1, dev_cap), dtype=np.float32) if record else None
+        n = self.lib.refh_run(nturns, _ptr(st), _ptr(dev), dev_cap if record else 0)
+        st = st.reshape(nturns, self.nb, 12)
+        return (st, dev[:n]) if record else st
+
+    def state(self, ib=0):
+        v = np.zeros(2)
+        ph = np.zeros(16)
+        self.lib.refh_state(ib, _ptr(v), _ptr(ph))
+        return v, ph
+
+    def trash(self, ib):
+        lo, hi = ctypes.c_int(), ctypes.c_int()
+        self.lib.refh_trash(ib, ctypes.byref(lo), ctypes.byref(hi))
+        return lo.value, hi.value

@@ -1,0 +1,584 @@
+/*
+ * ref_harness.c -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A single-process driver for the UNMODIFIED reference sources
+ * (fracul/mtrack src/*.c, compiled from where they lie by oracle/Makefile
+ * into oracle/_ref/libmbtref.so).  It replays the weak-weak worker of
+ * worker_weakweak.c:19-394 for every filled bunch inside one process:
+ *
+ *   - each bunch gets the private state an MPI worker process would have
+ *     (its own copy of ring_t with its own Ibunch and rf_feedback, its own
+ *     selffield_model_t, phasor_end arrays, RW trigger counter);
+ *   - the per-turn MPI_Bcast rounds (worker_weakweak.c:143,177,195,215,
+ *     316,365,375,385) only copy data between ranks, so they are replaced
+ *     by one shared fnp_ring/fnp_HOR/fnp_VER array and one shared dipole
+ *     cyclic array that every bunch writes its own slot of; the turn is run
+ *     phase by phase over all bunches so every read sees the data an MPI
+ *     worker would have received;
+ *   - box_muller is wrapped (-Wl,--wrap=box_muller) to record the deviates
+ *     each bunch draws, so the device path can replay them.
+ *
+ * Exactness of the deviates: the reference keeps one glibc rand() state
+ * and one cached Marsaglia deviate per PROCESS (bunch.c:407-436).  Here all
+ * bunches share them, which reproduces the MPI run exactly when every
+ * bunch draws an even number of deviates per turn (np even) and the
+ * per-turn seeds iseed_LON+kb+rev never repeat between consecutive calls;
+ * refh_init() reports otherwise through refh_deviates_exact().
+ *
+ * Nothing in the product links this file; tests and fixture generators
+ * load it through ctypes in the build container.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "types.h"
+#include "bunch.h"
+#include "fbi.h"
+#include "input.h"
+#include "statistics.h"
+#include "transform_weak.h"
+#include "cyclic_array.h"
+#include "feedback_rf.h"
+#include "physic.h"
+#include "tracking.h"
+
+/* The globals main() owns in mbtrack-mpi.c:19-21. */
+ring_t ring;
+tracking_t track;
+grid_t fbii_grid;
+
+/* ------------------------------------------------------------------ */
+/* deviate recorder                                                    */
+
+double __real_box_muller(const int iseed);
+static float *rec_buf = NULL;
+static long rec_pos = 0, rec_cap = 0;
+
+double __wrap_box_muller(const int iseed)
+{
+  double g = __real_box_muller(iseed);
+  if (rec_buf != NULL && rec_pos < rec_cap)
+    rec_buf[rec_pos] = (float) g;
+  rec_pos++;
+  return g;
+}
+
+/* ------------------------------------------------------------------ */
+
+typedef struct worker {
+  int kb;                       /* bucket */
+  ring_t ring;                  /* private copy, as passed by value */
+  double *ibunch;               /* private Ibunch array */
+  rf_feedback_t rffb;           /* private feedback state */
+  bunch_macroparticle_model_t model;
+  selffield_model_t sf;
+  weak_bunch_t bunch;
+  double *phasor_end[3];
+  int fb_off;
+  int iseed;
+  int m;                        /* RW trigger counter (worker_weakweak.c:254) */
+  double scan_val;
+} worker_t;
+
+static int nbunch = 0;
+static worker_t *W = NULL;
+static e_beam_t ebeam;
+static bunch_macroparticle_model_t macrop_model;
+static selffield_model_t sf_model;
+static double *fnp_ring = NULL, *fnp_hor = NULL, *fnp_ver = NULL;
+static cyclic_array_t dipole_rw;
+static FILE *devnull = NULL;
+static long rev_done = 0;
+static int lr_res_sizetot = 0;
+static int exact_deviates = 1;
+static char conf_copy[FILENAME_MAX];
+
+static void rw_beff_fix(const char *conf)
+{
+  /* The reference reads beffH3/beffV3 only with EnableRW_short
+     (input.c:465-478); long-range RW divides by beff^3
+     (transform_weak.c:801,811).  Read them whenever RW long is on. */
+  FILE *fp = fopen(conf, "r");
+  if (fp == NULL) return;
+  int saved = config_get_fprint;
+  config_get_fprint = false;
+  if (track.TrackPlane[HOR]) {
+    config_get_double(fp, "ring", "beffH3", &(ring.beffH[0]));
+    config_get_double(fp, "ring", "beffH4", &(ring.beffH[1]));
+  }
+  if (track.TrackPlane[VER]) {
+    config_get_double(fp, "ring", "beffV3", &(ring.beffV[0]));
+    config_get_double(fp, "ring", "beffV4", &(ring.beffV[1]));
+  }
+  config_get_fprint = saved;
+  fclose(fp);
+}
+
+int refh_init(const char *conf, const char *workdir, int fix_rw_beff)
+{
+  char inp[FILENAME_MAX];
+  snprintf(inp, FILENAME_MAX, "%s", conf);
+  snprintf(conf_copy, FILENAME_MAX, "%s", conf);
+  memset(&ring, 0, sizeof(ring));
+  memset(&track, 0, sizeof(track));
+  memset(&ebeam, 0, sizeof(ebeam));
+  memset(&macrop_model, 0, sizeof(macrop_model));
+  memset(&sf_model, 0, sizeof(sf_model));
+  snprintf(track.work_path, FILENAME_MAX, "%s", workdir ? workdir : "/tmp");
+
+  /* mbtrack-mpi.c:61-81 */
+  if (!read_input(inp, &ring, &track, &ebeam, &macrop_model, &sf_model))
+    return -1;
+  if (fix_rw_beff && track.EnableRW_long) rw_beff_fix(conf);
+  setup_ring_parameters(&ring);
+  macrop_model_setup_parameters(ring, track, &macrop_model);
+  fbii_grid_setup_parameters(&fbii_grid, &ebeam, macrop_model);
+  if (!e_beam_setup(&track, &ring, &ebeam)) return -2;
+  /* mbtrack-mpi.c:148 (the result is ignored by the reference; not here) */
+  if (!setup_tracking_parameters(&ring, &track, &sf_model, &macrop_model))
+    return -3;
+
+  nbunch = ebeam.Nbunch;
+  W = (worker_t *) calloc(nbunch, sizeof(worker_t));
+  devnull = fopen("/dev/null", "w");
+
+  /* manager_weakweak.c:47-78: bucket numbers and currents */
+  int kb, ib = 0;
+  for (kb = 0; kb < (int) ring.Nharm; kb++) {
+    if (!ebeam.nfFill[kb]) continue;
+    double bunch_Ib = ebeam.Ib_frac[ib] * ring.Iring / (((double) ebeam.Nbunch) * FKILO);
+    ring.Ibunch[kb] = bunch_Ib * FKILO;
+    W[ib].kb = kb;
+    W[ib].bunch.Ib = bunch_Ib;
+    ib++;
+  }
+
+  lr_res_sizetot = ring.longrange_resonators_size[LON]
+                 + ring.longrange_resonators_size[HOR]
+                 + ring.longrange_resonators_size[VER];
+
+  for (ib = 0; ib < nbunch; ib++) {
+    worker_t *w = &W[ib];
+    double Ib = w->bunch.Ib;
+    w->ring = ring;
+    w->ibunch = (double *) malloc(ring.Nharm * sizeof(double));
+    memcpy(w->ibunch, ring.Ibunch, ring.Nharm * sizeof(double));
+    w->ring.Ibunch = w->ibunch;
+    if (ring.has_rf_feedback || ring.rf_feedback != NULL) {
+      w->rffb = *ring.rf_feedback;
+      w->ring.rf_feedback = &w->rffb;
+    }
+    w->model = macrop_model;
+    w->model.Np = macrop_model.Np;
+    w->model.fNp = (double) macrop_model.Np;
+    w->sf = sf_model;
+    w->scan_val = track.scan_start;
+    /* worker_weakweak.c:75-79 */
+    if (!weak_bunch_create(&w->bunch, &track, macrop_model.Np, Ib, w->kb, true))
+      return -4;
+    if (!weak_generate_bunch_distribution(&w->bunch, w->model, track.TrackPlane))
+      return -5;
+    w->iseed = macrop_model.iseed[LON] + w->kb;
+    int pl;
+    for (pl = 0; pl < 3; pl++) {
+      int n = ring.longrange_resonators_size[pl];
+      w->phasor_end[pl] = (double *) calloc(2 * (n > 0 ? n : 1), sizeof(double));
+    }
+  }
+  /* Zero the coordinates of untracked planes: the reference leaves them as
+     malloc garbage that is never read by the dynamics. */
+  for (ib = 0; ib < nbunch; ib++) {
+    unsigned jp;
+    for (jp = 0; jp < W[ib].bunch.Np; jp++) {
+      if (!track.TrackPlane[HOR]) { W[ib].bunch.particles[jp].pos.x = 0; W[ib].bunch.particles[jp].slope.x = 0; }
+      if (!track.TrackPlane[VER]) { W[ib].bunch.particles[jp].pos.z = 0; W[ib].bunch.particles[jp].slope.z = 0; }
+    }
+  }
+
+  /* deviate exactness (see header comment) */
+  {
+    int per = 1 + 2 * (track.TrackPlane[VER] != 0) + 2 * (track.TrackPlane[HOR] != 0);
+    exact_deviates = (nbunch == 1) || ((macrop_model.Np * per) % 2 == 0);
+    if (nbunch > 1 && !track.TrackPlane[HOR] && !track.TrackPlane[VER]) exact_deviates = 0;
+  }
+  rev_done = 0;
+  return nbunch;
+}
+
+int refh_deviates_exact(void) { return exact_deviates; }
+int refh_nbunch(void) { return nbunch; }
+
+void refh_bunch_info(int *bucket, int *np, double *ib)
+{
+  int i;
+  for (i = 0; i < nbunch; i++) {
+    bucket[i] = W[i].kb;
+    np[i] = (int) W[i].bunch.Np;
+    ib[i] = W[i].bunch.Ib;
+  }
+}
+
+static int soa_get(const weak_bunch_t *b, double *soa)
+{
+  unsigned n = b->Np, j;
+  for (j = 0; j < n; j++) {
+    const particle_t *p = &b->particles[j];
+    soa[0 * n + j] = p->pos.xtau;
+    soa[1 * n + j] = p->pos.x;
+    soa[2 * n + j] = p->pos.z;
+    soa[3 * n + j] = p->slope.xtau;
+    soa[4 * n + j] = p->slope.x;
+    soa[5 * n + j] = p->slope.z;
+  }
+  return (int) n;
+}
+
+int refh_get_particles(int ib, double *soa)
+{
+  if (ib < 0 || ib >= nbunch) return -1;
+  return soa_get(&W[ib].bunch, soa);
+}
+
+int refh_set_particles(int ib, const double *soa)
+{
+  if (ib < 0 || ib >= nbunch) return -1;
+  weak_bunch_t *b = &W[ib].bunch;
+  unsigned n = b->Np, j;
+  for (j = 0; j < n; j++) {
+    particle_t *p = &b->particles[j];
+    p->pos.xtau = soa[0 * n + j];
+    p->pos.x = soa[1 * n + j];
+    p->pos.z = soa[2 * n + j];
+    p->slope.xtau = soa[3 * n + j];
+    p->slope.x = soa[4 * n + j];
+    p->slope.z = soa[5 * n + j];
+  }
+  return (int) n;
+}
+
+static void put_stats(const weak_bunch_t *b, double *out)
+{
+  const bunch_stats_t *s = &b->stats;
+  int k;
+  for (k = 0; k < 3; k++) {
+    out[0 + k] = s->pos.v[k];
+    out[3 + k] = s->pos_sigma.v[k];
+    out[6 + k] = s->slope.v[k];
+    out[9 + k] = s->slope_sigma.v[k];
+  }
+}
+
+/* Worker set-up after the distribution exists: worker_weakweak.c:80-219. */
+int refh_prepare(double *init_stats)
+{
+  int ib, i, j;
+  int Nbin = sf_model.Ncell;
+  for (ib = 0; ib < nbunch; ib++) {
+    worker_t *w = &W[ib];
+    if (!selffield_model_init(&w->sf, w->model.pos_sgm.xtau, &w->bunch)) return -1;
+    if (w->ring.resonators_size > 0) construct_greensfunc_resonator(&w->sf, &w->ring);
+    if (w->ring.wakefiles_size > 0) construct_greensfunc_file(&w->sf, &w->ring);
+    if (track.EnableRW_short || track.EnableRW_short_LON) construct_greensfunc_RW(&w->sf, &w->ring);
+    weak_bunch_calc_statistics(&w->bunch, &track);
+    if (init_stats) put_stats(&w->bunch, init_stats + 12 * ib);
+  }
+
+  if (ring.longrange_resonators_size[LON] > 0) {
+    fnp_ring = (double *) calloc((size_t) Nbin * ring.Nharm, sizeof(double));
+    for (ib = 0; ib < nbunch; ib++) {
+      worker_t *w = &W[ib];
+      if (w->ring.has_rf_feedback) {
+        if (w->ring.rf_feedback->len_average < 0) {
+          w->ring.rf_feedback->len_average = -1 * w->ring.rf_feedback->len_average;
+          w->fb_off = 1;
+        }
+        rffb_init(w->ring.rf_feedback);
+      }
+      fnp_ring_update(&w->ring, fnp_ring, &w->sf, &w->bunch, w->kb, LON);
+    }
+    for (ib = 0; ib < nbunch; ib++) {
+      worker_t *w = &W[ib];
+      wake_phasor_init(&w->ring, fnp_ring, &w->sf, &w->bunch, w->kb, w->phasor_end[LON], &ebeam, LON);
+      if (w->ring.has_rf_feedback) {
+        double vmbar, phibar;
+        rffb_calc_mean_voltage_phase(w->ring.rf_feedback, &vmbar, &phibar);
+        vmbar = vmbar * w->ring.E0 * FKILO;
+        double tmp_numrtor = w->ring.rf_feedback->vrf_design * sin(w->ring.rf_feedback->phi0_design) - vmbar * sin(phibar);
+        w->ring.phai0 = atan2(tmp_numrtor, w->ring.rf_feedback->vrf_design * cos(w->ring.rf_feedback->phi0_design) - vmbar * cos(phibar));
+        w->ring.Vrf0 = tmp_numrtor / sin(w->ring.phai0);
+        if (w->fb_off) w->ring.has_rf_feedback = 0;
+      }
+    }
+  }
+  if (track.TrackPlane[HOR] && ring.longrange_resonators_size[HOR] > 0) {
+    fnp_hor = (double *) calloc((size_t) Nbin * ring.Nharm, sizeof(double));
+    for (ib = 0; ib < nbunch; ib++)
+      fnp_ring_update(&W[ib].ring, fnp_hor, &W[ib].sf, &W[ib].bunch, W[ib].kb, HOR);
+    for (ib = 0; ib < nbunch; ib++)
+      wake_phasor_init(&W[ib].ring, fnp_hor, &W[ib].sf, &W[ib].bunch, W[ib].kb, W[ib].phasor_end[HOR], &ebeam, HOR);
+  }
+  if (track.TrackPlane[VER] && ring.longrange_resonators_size[VER] > 0) {
+    fnp_ver = (double *) calloc((size_t) Nbin * ring.Nharm, sizeof(double));
+    for (ib = 0; ib < nbunch; ib++)
+      fnp_ring_update(&W[ib].ring, fnp_ver, &W[ib].sf, &W[ib].bunch, W[ib].kb, VER);
+    for (ib = 0; ib < nbunch; ib++)
+      wake_phasor_init(&W[ib].ring, fnp_ver, &W[ib].sf, &W[ib].bunch, W[ib].kb, W[ib].phasor_end[VER], &ebeam, VER);
+  }
+
+  if (track.EnableRW_long > 0) {
+    if (!cyclic_array_create(&dipole_rw, (track.Nmlt + 2) * ring.Nharm, 2)) return -2;
+    for (ib = 0; ib < nbunch; ib++) {
+      double d[2] = {W[ib].bunch.stats.pos.x, W[ib].bunch.stats.pos.z};
+      cyclic_array_set(W[ib].kb, d, &dipole_rw);
+    }
+    for (i = 0; i < (int) ring.Nharm; i++) {
+      if (!ebeam.nfFill[i]) continue;
+      double *mom = cyclic_array_access(i, &dipole_rw);
+      for (j = 1; j < track.Nmlt; j++) cyclic_array_set((j * ring.Nharm + i), mom, &dipole_rw);
+    }
+  }
+  /* The reference resets the running sums after the first output
+     (worker_weakweak.c:234); stats below are per turn, so reset here. */
+  for (ib = 0; ib < nbunch; ib++) weak_bunch_reset_statistics(&W[ib].bunch.stats);
+  return 0;
+}
+
+/* Per-turn loop, worker_weakweak.c:259-394, phase by phase over bunches.
+ * stats: nturns x nbunch x 12 (may be NULL); dev: deviates recorded in
+ * draw order, per turn, per bunch (may be NULL); dev_cap its length. */
+int refh_run(long nturns, double *stats, float *dev, long dev_cap)
+{
+  long t;
+  int ib, i;
+  int Nbin = sf_model.Ncell;
+  rec_buf = dev; rec_cap = dev ? dev_cap : 0; rec_pos = 0;
+  for (t = 0; t < nturns; t++) {
+    long rev = rev_done + t;
+    /* 1. self-field (+ long-range phasors) */
+    for (ib = 0; ib < nbunch; ib++) {
+      worker_t *w = &W[ib];
+      if (w->sf.PlaneL + w->sf.PlaneV + w->sf.PlaneH + lr_res_sizetot > 0)
+        transform_weak_bunch_selffield(&w->bunch, w->sf, NULL, &w->ring, rev, devnull,
+                                       w->scan_val, w->kb, &ebeam, w->phasor_end[LON],
+                                       w->phasor_end[HOR], w->phasor_end[VER],
+                                       fnp_ring, fnp_hor, fnp_ver);
+    }
+    /* 2. RF feedback */
+    for (ib = 0; ib < nbunch; ib++) {
+      worker_t *w = &W[ib];
+      if (w->ring.has_rf_feedback) {
+        double vmbar, phibar;
+        rffb_calc_mean_voltage_phase(w->ring.rf_feedback, &vmbar, &phibar);
+        vmbar = vmbar * w->ring.E0 * FKILO;
+        double tmp_numrtor = w->ring.rf_feedback->vrf_design * sin(w->ring.rf_feedback->phi0_design) - vmbar * sin(phibar);
+        w->ring.phai0 = atan2(tmp_numrtor, w->ring.rf_feedback->vrf_design * cos(w->ring.rf_feedback->phi0_design) - vmbar * cos(phibar));
+        w->ring.Vrf0 = tmp_numrtor / sin(w->ring.phai0);
+      }
+    }
+    /* 3. optics, 4. statistics */
+    for (ib = 0; ib < nbunch; ib++) {
+      worker_t *w = &W[ib];
+      transform_weak_bunch_optic(&w->bunch, &w->model, w->iseed + (int) rev, w->kb, &w->ring);
+      weak_bunch_calc_statistics(&w->bunch, &track);
+      if (stats) put_stats(&w->bunch, stats + (t * nbunch + ib) * 12);
+    }
+    /* 5. dipole history */
+    if (track.EnableRW_long > 0) {
+      for (ib = 0; ib < nbunch; ib++) {
+        double *mom = cyclic_array_access(-rev * ring.Nharm + W[ib].kb, &dipole_rw);
+        mom[0] = W[ib].bunch.stats.pos.x;
+        mom[1] = W[ib].bunch.stats.pos.z;
+      }
+      /* 7. long-range RW kicks */
+      for (ib = 0; ib < nbunch; ib++) {
+        worker_t *w = &W[ib];
+        const int bpos = -rev * ring.Nharm + w->kb;
+        if (track.TrackPlane[HOR])
+          transform_weak_bunch_RW_longrange_cyclic(w->m, bpos, &dipole_rw, HOR, &w->model, &ebeam, &w->bunch, &w->ring, &track);
+        if (track.TrackPlane[VER])
+          transform_weak_bunch_RW_longrange_cyclic(w->m, bpos, &dipole_rw, VER, &w->model, &ebeam, &w->bunch, &w->ring, &track);
+        w->m++;
+      }
+    }
+    /* 8. histograms for the long-range resonators */
+    for (ib = 0; ib < nbunch; ib++) {
+      worker_t *w = &W[ib];
+      if (ring.longrange_resonators_size[LON] > 0)
+        fnp_ring_update(&w->ring, fnp_ring, &w->sf, &w->bunch, w->kb, LON);
+      if (ring.longrange_resonators_size[HOR] > 0 && track.TrackPlane[HOR])
+        fnp_ring_update(&w->ring, fnp_hor, &w->sf, &w->bunch, w->kb, HOR);
+      if (ring.longrange_resonators_size[VER] > 0 && track.TrackPlane[VER])
+        fnp_ring_update(&w->ring, fnp_ver, &w->sf, &w->bunch, w->kb, VER);
+    }
+    /* 9. scan */
+    if ((rev + 1) % track.NrevScan == 0) {
+      for (ib = 0; ib < nbunch; ib++) {
+        tracking_scan_step_worker(rev, &W[ib].scan_val, &track, &W[ib].ring, &ebeam, &W[ib].bunch);
+        W[ib].m = 0;
+      }
+    }
+  }
+  (void) Nbin; (void) i;
+  rev_done += nturns;
+  rec_buf = NULL;
+  return (int) rec_pos;
+}
+
+/* RF parameters / phasors of bunch ib after the last turn. */
+void refh_state(int ib, double *vrf_phi, double *phasor_lon)
+{
+  worker_t *w = &W[ib];
+  vrf_phi[0] = w->ring.Vrf0;
+  vrf_phi[1] = w->ring.phai0;
+  int l;
+  for (l = 0; l < (int) ring.longrange_resonators_size[LON]; l++) {
+    phasor_lon[2 * l] = w->phasor_end[LON][2 * l];
+    phasor_lon[2 * l + 1] = w->phasor_end[LON][2 * l + 1];
+  }
+}
+
+void refh_trash(int ib, int *low, int *high)
+{
+  *low = W[ib].bunch.N_trash_low;
+  *high = W[ib].bunch.N_trash_high;
+}
+
+void refh_greens(int ib, double *Gl, double *Gv, double *Gh, int *planes)
+{
+  worker_t *w = &W[ib];
+  int n = w->sf.Ncell, i;
+  for (i = 0; i < n; i++) {
+    Gl[i] = w->sf.Gl ? w->sf.Gl[i] : 0.0;
+    Gv[i] = w->sf.Gv ? w->sf.Gv[i] : 0.0;
+    Gh[i] = w->sf.Gh ? w->sf.Gh[i] : 0.0;
+  }
+  planes[0] = w->sf.PlaneL; planes[1] = w->sf.PlaneV; planes[2] = w->sf.PlaneH;
+}
+
+/* Derived scalar parameters, as name/value pairs for parser cross-checks.
+ * Returns the number of pairs written (at most cap). */
+int refh_param_table(const char **names, double *values, int cap)
+{
+  int n = 0;
+#define PUT(nm, v) do { if (n < cap) { names[n] = nm; values[n] = (double)(v); } n++; } while (0)
+  PUT("nharm", ring.Nharm); PUT("E0", ring.E0); PUT("T0", ring.T0); PUT("wrf", ring.wrf);
+  PUT("Vrf0", ring.Vrf0); PUT("phai0", ring.phai0); PUT("Urad", ring.Urad); PUT("De", ring.De);
+  PUT("ac", ring.ac); PUT("QH0", ring.QH0); PUT("QV0", ring.QV0); PUT("Gzix", ring.Gzix);
+  PUT("Gziz", ring.Gziz); PUT("CHH", ring.CHH); PUT("CHV", ring.CHV); PUT("CVH", ring.CVH);
+  PUT("CVV", ring.CVV); PUT("amp_dep_qv", ring.AmpDependdQV);
+  PUT("beta1_h", ring.beta1[HOR]); PUT("beta1_v", ring.beta1[VER]);
+  PUT("alpha1_h", ring.alpha1[HOR]); PUT("alpha1_v", ring.alpha1[VER]);
+  PUT("gamma1_h", ring.gamma1[HOR]); PUT("gamma1_v", ring.gamma1[VER]);
+  PUT("dispH1", ring.dispH1); PUT("disppH1", ring.disppH1);
+  PUT("taue", ring.taue); PUT("taux", ring.taux); PUT("tauz", ring.tauz);
+  PUT("Lc", ring.Lc); PUT("rhorw", ring.rhorw); PUT("beffH3", ring.beffH[0]); PUT("beffV3", ring.beffV[0]);
+  PUT("Iring", ring.Iring); PUT("ideal_hc", track.EnableIdealHC); PUT("m_aHC", ring.m_aHC);
+  PUT("phi_n", ring.phi_n); PUT("HC_k", ring.HC_k); PUT("n_active_hc", ring.active_HC_size);
+  PUT("track_h", track.TrackPlane[HOR]); PUT("track_v", track.TrackPlane[VER]);
+  PUT("quantum", track.EnableQuantum); PUT("rw_long", track.EnableRW_long); PUT("Nmlt", track.Nmlt);
+  PUT("triggerRW", track.triggerRW); PUT("nrev_tot", track.NrevTot); PUT("nrev_mon", track.NrevMon);
+  PUT("np_model", macrop_model.Np); PUT("iseed_lon", macrop_model.iseed[LON]);
+  PUT("iseed_hor", macrop_model.iseed[HOR]); PUT("iseed_ver", macrop_model.iseed[VER]);
+  PUT("pos_sgm_lon", macrop_model.pos_sgm.xtau); PUT("pos_sgm_hor", macrop_model.pos_sgm.x);
+  PUT("pos_sgm_ver", macrop_model.pos_sgm.z); PUT("slope_sgm_lon", macrop_model.slope_sgm.xtau);
+  PUT("slope_sgm_hor", macrop_model.slope_sgm.x); PUT("slope_sgm_ver", macrop_model.slope_sgm.z);
+  PUT("pos_off_lon", macrop_model.pos_offset.xtau); PUT("pos_off_hor", macrop_model.pos_offset.x);
+  PUT("pos_off_ver", macrop_model.pos_offset.z); PUT("slope_off_lon", macrop_model.slope_offset.xtau);
+  PUT("corr_hor", macrop_model.correlate.x); PUT("corr_ver", macrop_model.correlate.z);
+  PUT("ncell", sf_model.Ncell); PUT("nsigma", sf_model.Nsigma);
+  PUT("RsisL", sf_model.RsisL); PUT("aindL", sf_model.aindL);
+  PUT("n_lr_lon", ring.longrange_resonators_size[LON]); PUT("n_lr_hor", ring.longrange_resonators_size[HOR]);
+  PUT("n_lr_ver", ring.longrange_resonators_size[VER]);
+  PUT("lr_init_turns", ring.h > 0 ? (double)(int)(ring.Nbumax / ring.h) : 0.0);
+  PUT("rffb", ring.has_rf_feedback);
+  if (ring.rf_feedback != NULL && ring.has_rf_feedback) {
+    PUT("rffb_resonator", ring.rf_feedback->lr_resonator);
+    PUT("rffb_len", ring.rf_feedback->len_average);
+    PUT("rffb_vrf_design", ring.rf_feedback->vrf_design);
+    PUT("rffb_phi0_design", ring.rf_feedback->phi0_design);
+  }
+  PUT("nbunch", ebeam.Nbunch);
+  {
+    int l;
+    static const char *wrn[4] = {"lr_wr_lon_0", "lr_wr_lon_1", "lr_wr_lon_2", "lr_wr_lon_3"};
+    for (l = 0; l < (int) ring.longrange_resonators_size[LON] && l < 4; l++)
+      PUT(wrn[l], ring.longrange_resonators[LON][l].wr);
+  }
+#undef PUT
+  return n;
+}
+
+/* ------------------------------------------------------------------ */
+/* The reference's parsed and derived state as the product's parameter
+ * block (include/mbt.h), so oracle and device path can be driven from
+ * exactly what the reference computed. */
+#include "mbt.h"
+
+int refh_fill_params(mbt_params *p)
+{
+  int pl, l;
+  memset(p, 0, sizeof(*p));
+  p->nharm = (int) ring.Nharm;
+  p->E0 = ring.E0; p->T0 = ring.T0; p->wrf = ring.wrf; p->Vrf0 = ring.Vrf0;
+  p->phai0 = ring.phai0; p->Urad = ring.Urad; p->De = ring.De; p->ac = ring.ac;
+  p->QH0 = ring.QH0; p->QV0 = ring.QV0; p->Gzix = ring.Gzix; p->Gziz = ring.Gziz;
+  p->CHH = ring.CHH; p->CHV = ring.CHV; p->CVH = ring.CVH; p->CVV = ring.CVV;
+  p->amp_dep_qv = ring.AmpDependdQV ? 1 : 0;
+  for (pl = 0; pl < 3; pl++) {
+    p->beta1[pl] = ring.beta1[pl]; p->alpha1[pl] = ring.alpha1[pl]; p->gamma1[pl] = ring.gamma1[pl];
+  }
+  p->dispH1 = ring.dispH1; p->disppH1 = ring.disppH1;
+  p->taue = ring.taue; p->taux = ring.taux; p->tauz = ring.tauz;
+  p->Lc = ring.Lc; p->rhorw = ring.rhorw;
+  p->beffH[0] = ring.beffH[0]; p->beffH[1] = ring.beffH[1];
+  p->beffV[0] = ring.beffV[0]; p->beffV[1] = ring.beffV[1];
+  p->beffL[0] = ring.beffL[0]; p->beffL[1] = ring.beffL[1];
+  p->Iring = ring.Iring;
+  p->ideal_hc = track.EnableIdealHC; p->m_aHC = ring.m_aHC; p->phi_n = ring.phi_n; p->HC_k = ring.HC_k;
+  p->n_active_hc = (int) ring.active_HC_size;
+  for (l = 0; l < p->n_active_hc && l < MBT_MAX_AHC; l++) {
+    p->ahc_vpeak[l] = ring.active_HC[l].Vpeak; p->ahc_nhc[l] = ring.active_HC[l].nHC;
+    p->ahc_phi[l] = ring.active_HC[l].phi_aHC;
+  }
+  for (pl = 0; pl < 3; pl++) p->track_plane[pl] = track.TrackPlane[pl];
+  p->quantum = track.EnableQuantum; p->rw_long = track.EnableRW_long; p->Nmlt = track.Nmlt;
+  p->triggerRW = track.triggerRW; p->nrev_tot = track.NrevTot; p->nrev_mon = track.NrevMon;
+  p->np_model = macrop_model.Np;
+  for (pl = 0; pl < 3; pl++) {
+    p->iseed[pl] = macrop_model.iseed[pl];
+    p->pos_offset[pl] = macrop_model.pos_offset.v[pl];
+    p->slope_offset[pl] = macrop_model.slope_offset.v[pl];
+    p->pos_sgm[pl] = macrop_model.pos_sgm.v[pl];
+    p->slope_sgm[pl] = macrop_model.slope_sgm.v[pl];
+    p->correlate[pl] = macrop_model.correlate.v[pl];
+  }
+  p->ncell = sf_model.Ncell; p->nsigma = sf_model.Nsigma;
+  p->dT = sf_model.Ncell > 0 ? 2.0 * sf_model.Nsigma / ((double) sf_model.Ncell - 1) : 0.0;
+  p->sigma_tau = macrop_model.pos_sgm.xtau;
+  p->RsisL = sf_model.RsisL; p->aindL = sf_model.aindL;
+  if (nbunch > 0) {
+    p->planeL = W[0].sf.PlaneL; p->planeV = W[0].sf.PlaneV; p->planeH = W[0].sf.PlaneH;
+    p->dT = W[0].sf.dT;
+    p->sigma_tau = W[0].sf.sigma_tau;
+  }
+  for (pl = 0; pl < 3; pl++) {
+    p->n_lr[pl] = (int) ring.longrange_resonators_size[pl];
+    for (l = 0; l < p->n_lr[pl] && l < MBT_MAX_LR; l++) {
+      p->lr_Rs[pl][l] = ring.longrange_resonators[pl][l].Rs;
+      p->lr_wr[pl][l] = ring.longrange_resonators[pl][l].wr;
+      p->lr_Q[pl][l] = ring.longrange_resonators[pl][l].Qfactor;
+    }
+  }
+  p->lr_init_turns = ring.h > 0 ? (int) (ring.Nbumax / ring.h) : 0;
+  p->rffb = ring.has_rf_feedback;
+  if (ring.has_rf_feedback && ring.rf_feedback) {
+    p->rffb_resonator = ring.rf_feedback->lr_resonator;
+    p->rffb_len = ring.rf_feedback->len_average < 0 ? -ring.rf_feedback->len_average : ring.rf_feedback->len_average;
+    p->rffb_off_after_init = ring.rf_feedback->len_average < 0;
+    p->rffb_vrf_design = ring.rf_feedback->vrf_design;
+    p->rffb_phi0_design = ring.rf_feedback->phi0_design;
+  }
+  return 0;
+}

@@ -144,13 +144,16 @@ typedef struct mbt_ctx mbt_ctx;
  * p->nharm entries, may be NULL to query nbunch only).  fix_rw_beff != 0
  * reads beffH3/beffV3 for long-range resistive wall even without
  * EnableRW_short (the reference leaves them 0, input.c:465-478).
- * scratch_dir receives nothing; it is accepted for interface symmetry
- * with the reference's work directory and may be NULL. */
+ * Returns MBT_ERR_CONFIG (message in mbt_config_error()) for a missing or
+ * malformed key, and for what this library does not run: short-range
+ * resistive wall, parameter scans, BunchModel = STRONG, modeHT excitation
+ * and distribution files. */
 int mbt_config_load(const char *conf_path, int fix_rw_beff, mbt_params *p,
                     int *nbunch, int *bucket, double *ib_frac);
 
-/* Short-range Green's functions for ncell bins (construct_greensfunc_resonator
- * transform_weak.c:288-403, construct_greensfunc_RW :473-547), plus the
+/* Short-range Green's functions for ncell bins from the [resonator_N] and
+ * [wake_file_N] sections (construct_greensfunc_resonator
+ * transform_weak.c:288-403, construct_greensfunc_file :405-471), plus the
  * resulting planeL/planeV/planeH counts written back into *p.
  * Gl, Gv, Gh: arrays of p->ncell doubles (zeroed by the call). */
 int mbt_config_greens(const char *conf_path, mbt_params *p,
@@ -158,6 +161,12 @@ int mbt_config_greens(const char *conf_path, mbt_params *p,
 
 /* Bunch current [A] of filled bunch i (manager_weakweak.c:74-75). */
 double mbt_bunch_current(const mbt_params *p, int nbunch, double ib_frac);
+
+/* Message of the last failing mbt_config_* call of this process. */
+const char *mbt_config_error(void);
+
+/* sizeof(mbt_params) as compiled into the library (binding check). */
+size_t mbt_params_size(void);
 
 /* ---- context --------------------------------------------------------- */
 
@@ -237,11 +246,18 @@ int mbt_get_histograms(mbt_ctx *ctx, int ibunch, double *fnp, double *dipV,
                        double *dipH, double *ring_lon, double *ring_hor,
                        double *ring_ver);
 
-/* Device time of the last mbt_run_turns split by kernel [ms] (CUDA events):
- * out[0] particle pass, out[1] bunch reduction and wakes, out[2] ring-wide
- * phasor scan, out[3] total.  Also returns the number of kernel launches
- * per turn in *launches_per_turn. */
+/* Device time of the last mbt_run_turns [ms] (CUDA events) in out[3]
+ * (out[0..2] are 0), and the number of kernel launches per turn. */
 int mbt_last_timing(mbt_ctx *ctx, double out[4], int *launches_per_turn);
+
+/* Run nturns turns with the four kernels of a turn launched one by one and
+ * CUDA events between them; out[0..3] receive the average device time per
+ * turn [ms] of the particle pass, the bunch reduction, the ring-wide
+ * phasor scan and the bunch wakes. */
+int mbt_profile_turns(mbt_ctx *ctx, long nturns, double out[4]);
+
+/* Device layout: padded particle count, tile size, number of tiles. */
+int mbt_geometry(mbt_ctx *ctx, int *npad, int *tile, int *ntile);
 
 /* ---- per-step device entry points (device pointers) ------------------- */
 
@@ -251,13 +267,14 @@ int mbt_last_timing(mbt_ctx *ctx, double out[4], int *launches_per_turn);
 int mbt_wofz_dev(long n, const double *x_dev, const double *y_dev,
                  double *re_dev, double *im_dev, int *flag_dev, void *stream);
 
-/* Bassetti-Erskine field of a Gaussian slice at n points
- * (fbi_weakstrong.c:154-197): dx,dy offsets [m] from the slice centre,
- * sx, sy rms sizes [m] (sx > sy), factdq = dQ / (2 eps0 sqrt(pi) c dt)
- * as in fbi_weakstrong.c:156 but without the 1/factBE, which is derived
- * from sx, sy.  Writes Ex, Ey. */
+/* Bassetti-Erskine field of a flat Gaussian slice at n points
+ * (fbi_weakstrong.c:154-197, replaces the inner loop of
+ * fbi_weakstrong_bunch): dx, dy offsets [m] from the slice centre,
+ * sgm_xx_mm > sgm_zz_mm its rms sizes [mm] (the reference's units),
+ * factdq the reference's factdQ = dQ / (2 eps0 sqrt(pi) factBE c deltT)
+ * (fbi_weakstrong.c:156).  Writes Ex, Ey. */
 int mbt_be_field_dev(long n, const double *dx_dev, const double *dy_dev,
-                     double sx, double sy, double factdq,
+                     double sgm_xx_mm, double sgm_zz_mm, double factdq,
                      double *ex_dev, double *ey_dev, void *stream);
 
 #ifdef __cplusplus

@@ -77,3 +77,33 @@ class MbtState(ctypes.Structure):
         ("phasor", ((_d * 2) * MBT_MAX_LR) * 3),
         ("n_trash_low", _i), ("n_trash_high", _i),
     ]
+
+
+def params_to_dict(p):
+    """Flatten an MbtParams into {field: scalar or nested list}."""
+    out = {}
+    for name, _ in MbtParams._fields_:
+        v = getattr(p, name)
+        if isinstance(v, ctypes.Array):
+            v = [list(x) if isinstance(x, ctypes.Array) else x for x in v]
+        out[name] = v
+    return out
+
+
+def params_from_dict(d):
+    p = MbtParams()
+    for name, _ in MbtParams._fields_:
+        if name not in d:
+            continue
+        v = d[name]
+        cur = getattr(p, name)
+        if isinstance(cur, ctypes.Array):
+            for i, x in enumerate(v):
+                if isinstance(cur[i], ctypes.Array):
+                    for j, y in enumerate(x):
+                        cur[i][j] = y
+                else:
+                    cur[i] = x
+        else:
+            setattr(p, name, v)
+    return p

@@ -1,0 +1,231 @@
+"""Python mirror of libmbt's C-ABI (include/mbt.h), used by tests and bench.
+
+Names follow the reference's worker interface: a ``Tracker`` holds every
+filled bunch of the ring on one GPU and runs the weak-weak loop of
+worker_weakweak.c:259-394 for all of them per call.  There is no CPU path:
+loading fails loudly when libmbt.so is missing, and every call that needs
+a device fails with MBT_ERR_NODEVICE when there is none.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .abi import (MBT_NOISE_INJECTED, MBT_NOISE_PHILOX, MbtParams, MbtState)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmbt.so")
+
+_vp = ctypes.c_void_p
+_P = ctypes.POINTER
+_lib = None
+
+# every symbol include/mbt.h declares, with its ctypes signature
+SIGNATURES = {
+    "mbt_params_size": (ctypes.c_size_t, []),
+    "mbt_config_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _P(MbtParams), _vp, _vp, _vp]),
+    "mbt_config_greens": (ctypes.c_int, [ctypes.c_char_p, _P(MbtParams), _vp, _vp, _vp]),
+    "mbt_config_error": (ctypes.c_char_p, []),
+    "mbt_bunch_current": (ctypes.c_double, [_P(MbtParams), ctypes.c_int, ctypes.c_double]),
+    "mbt_create": (ctypes.c_int, [_P(MbtParams), ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp,
+                                  ctypes.c_int, ctypes.c_uint64, _P(_vp)]),
+    "mbt_destroy": (ctypes.c_int, [_vp]),
+    "mbt_last_error": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_size_t]),
+    "mbt_load_particles": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
+    "mbt_load_all": (ctypes.c_int, [_vp, _vp]),
+    "mbt_generate_beam": (ctypes.c_int, [_vp, ctypes.c_uint64]),
+    "mbt_get_particles": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
+    "mbt_get_all": (ctypes.c_int, [_vp, _vp]),
+    "mbt_prepare": (ctypes.c_int, [_vp, _vp]),
+    "mbt_set_deviates": (ctypes.c_int, [_vp, _vp, ctypes.c_long]),
+    "mbt_run_turns": (ctypes.c_int, [_vp, ctypes.c_long, _vp]),
+    "mbt_track": (ctypes.c_int, [_vp, _vp, ctypes.c_long, _vp]),
+    "mbt_profile_turns": (ctypes.c_int, [_vp, ctypes.c_long, _vp]),
+    "mbt_get_state": (ctypes.c_int, [_vp, _P(MbtState)]),
+    "mbt_get_histograms": (ctypes.c_int, [_vp, ctypes.c_int] + [_vp] * 6),
+    "mbt_last_timing": (ctypes.c_int, [_vp, _vp, _vp]),
+    "mbt_geometry": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "mbt_wofz_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "mbt_be_field_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, _vp, _vp, _vp]),
+}
+
+
+class MbtError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("libmbt error %d: %s" % (code, msg))
+        self.code = code
+
+
+def lib():
+    """Load libmbt.so (built by mbtrack_b200.build); raises when missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libmbt.so not built: run `python -m mbtrack_b200.build` "
+                              "(the tracking path has no CPU implementation)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        if L.mbt_params_size() != ctypes.sizeof(MbtParams):
+            raise ImportError("mbt_params layout mismatch: C %d bytes, ctypes %d bytes"
+                              % (L.mbt_params_size(), ctypes.sizeof(MbtParams)))
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def _check(rc, ctx=None):
+    if rc != 0:
+        buf = ctypes.create_string_buffer(512)
+        lib().mbt_last_error(ctx, buf, 512)
+        raise MbtError(rc, buf.value.decode(errors="replace"))
+
+
+class Config:
+    """A .conf file read with the reference's semantics (mbt_config_load)."""
+
+    def __init__(self, path, fix_rw_beff=True):
+        L = lib()
+        self.path = path
+        self.params = MbtParams()
+        h = 100000
+        bucket = np.zeros(h, dtype=np.int32)
+        frac = np.zeros(h)
+        nb = ctypes.c_int()
+        rc = L.mbt_config_load(path.encode(), int(fix_rw_beff), ctypes.byref(self.params),
+                               ctypes.byref(nb), _ptr(bucket), _ptr(frac))
+        if rc != 0:
+            raise MbtError(rc, L.mbt_config_error().decode())
+        self.nbunch = nb.value
+        self.bucket = bucket[:self.nbunch].copy()
+        self.ib_frac = frac[:self.nbunch].copy()
+        n = max(self.params.ncell, 1)
+        self.Gl, self.Gv, self.Gh = np.zeros(n), np.zeros(n), np.zeros(n)
+        rc = L.mbt_config_greens(path.encode(), ctypes.byref(self.params), _ptr(self.Gl),
+                                 _ptr(self.Gv), _ptr(self.Gh))
+        if rc != 0:
+            raise MbtError(rc, L.mbt_config_error().decode())
+
+    def bunch_currents(self):
+        L = lib()
+        return np.array([L.mbt_bunch_current(ctypes.byref(self.params), self.nbunch, f)
+                         for f in self.ib_frac])
+
+
+class Tracker:
+    """One tracking context (mbt_ctx) holding every filled bunch."""
+
+    def __init__(self, params, bucket, np_, ib, Gl=None, Gv=None, Gh=None,
+                 noise=MBT_NOISE_PHILOX, seed=0):
+        L = lib()
+        self.params = params.copy()
+        self.bucket = np.ascontiguousarray(bucket, dtype=np.int32)
+        self.np = np.ascontiguousarray(np_, dtype=np.int32)
+        self.ib = np.ascontiguousarray(ib, dtype=np.float64)
+        self.nb = len(self.bucket)
+        g = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (Gl, Gv, Gh)]
+        self._g = g
+        h = _vp()
+        rc = L.mbt_create(ctypes.byref(self.params), self.nb, _ptr(self.bucket), _ptr(self.np),
+                          _ptr(self.ib), _ptr(g[0]), _ptr(g[1]), _ptr(g[2]), noise, seed,
+                          ctypes.byref(h))
+        _check(rc, None)
+        self.h = h
+
+    @classmethod
+    def from_config(cls, cfg, np_per_bunch=None, noise=MBT_NOISE_PHILOX, seed=0):
+        n = np.full(cfg.nbunch, cfg.params.np_model if np_per_bunch is None else np_per_bunch)
+        return cls(cfg.params, cfg.bucket, n, cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh,
+                   noise=noise, seed=seed)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mbt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_particles(self, ib, soa6):
+        a = np.ascontiguousarray(soa6, dtype=np.float64)
+        _check(lib().mbt_load_particles(self.h, ib, _ptr(a), int(self.np[ib])), self.h)
+
+    def load_all(self, soa6_all):
+        a = np.ascontiguousarray(soa6_all, dtype=np.float64)
+        assert a.size == 6 * int(self.np.sum())
+        _check(lib().mbt_load_all(self.h, _ptr(a)), self.h)
+
+    def generate_beam(self, seed):
+        _check(lib().mbt_generate_beam(self.h, seed), self.h)
+
+    def get_particles(self, ib):
+        a = np.empty(6 * int(self.np[ib]))
+        _check(lib().mbt_get_particles(self.h, ib, _ptr(a), int(self.np[ib])), self.h)
+        return a.reshape(6, int(self.np[ib]))
+
+    def get_all(self):
+        a = np.empty(6 * int(self.np.sum()))
+        _check(lib().mbt_get_all(self.h, _ptr(a)), self.h)
+        return a
+
+    def prepare(self):
+        s = np.zeros(12 * self.nb)
+        _check(lib().mbt_prepare(self.h, _ptr(s)), self.h)
+        return s.reshape(self.nb, 12)
+
+    def set_deviates(self, dev, nturns):
+        d = np.ascontiguousarray(dev, dtype=np.float32)
+        _check(lib().mbt_set_deviates(self.h, _ptr(d), nturns), self.h)
+
+    def run(self, nturns, stats=True):
+        s = np.zeros(nturns * self.nb * 12) if stats else None
+        _check(lib().mbt_run_turns(self.h, nturns, _ptr(s)), self.h)
+        return None if s is None else s.reshape(nturns, self.nb, 12)
+
+    def track(self, particles, nturns, stats=None):
+        _check(lib().mbt_track(self.h, _ptr(particles), nturns, _ptr(stats)), self.h)
+
+    def profile(self, nturns):
+        out = np.zeros(4)
+        _check(lib().mbt_profile_turns(self.h, nturns, _ptr(out)), self.h)
+        return out
+
+    def state(self):
+        st = MbtState()
+        _check(lib().mbt_get_state(self.h, ctypes.byref(st)), self.h)
+        return st
+
+    def histograms(self, ib):
+        n = self.params.ncell
+        arr = [np.zeros(n) for _ in range(6)]
+        _check(lib().mbt_get_histograms(self.h, ib, *[_ptr(a) for a in arr]), self.h)
+        return arr
+
+    def timing(self):
+        out = np.zeros(4)
+        nl = ctypes.c_int()
+        _check(lib().mbt_last_timing(self.h, _ptr(out), ctypes.byref(nl)), self.h)
+        return out, nl.value
+
+    def geometry(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().mbt_geometry(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), self.h)
+        return a.value, b.value, c.value
+
+
+def wofz_dev(x_ptr, y_ptr, re_ptr, im_ptr, n, flag_ptr=None, stream=None):
+    """w(z) on device buffers (raw pointers, e.g. torch .data_ptr())."""
+    _check(lib().mbt_wofz_dev(n, x_ptr, y_ptr, re_ptr, im_ptr, flag_ptr, stream))
+
+
+def be_field_dev(dx_ptr, dy_ptr, n, sgm_xx_mm, sgm_zz_mm, factdq, ex_ptr, ey_ptr, stream=None):
+    _check(lib().mbt_be_field_dev(n, dx_ptr, dy_ptr, sgm_xx_mm, sgm_zz_mm, factdq, ex_ptr, ey_ptr, stream))

@@ -1,0 +1,153 @@
+// mbt_device.cuh -- device-side data of one tracking context.
+//
+// HBM layout (one context):
+//   coord   6 x npad doubles, structure of arrays in the reference's
+//           particle_t order (types.h:215-220): xtau, x, z, eps, xp, zp.
+//           Bunch b occupies [off[b], off[b]+np[b]); off[b] is a multiple
+//           of 32 particles so every tile starts 256-byte aligned.
+//   tiles   the particle pass works on tiles of at most `tile` particles,
+//           each inside one bunch; tile t writes one partial record.
+//   part    ntile x prec doubles: in-range histograms (count, sum x,
+//           sum z), out-of-range counters, shifted moment sums.
+//   per bunch: histograms of the last binning, kick tables for the next
+//           pass, pending resistive-wall kick, moment shifts, stats.
+//   ring    long-range phasors, resistive-wall dipole history, RF feedback.
+#pragma once
+#include <cstdint>
+
+#define MBT_NOISE_NONE 2   // EnableQuantum = 0: no deviates drawn
+
+namespace mbt {
+
+constexpr int kMaxLr = 8;          // MBT_MAX_LR
+constexpr int kMaxAhc = 8;         // MBT_MAX_AHC
+constexpr int kPartialExtra = 18;  // 6 out-of-range values + 12 moment sums
+constexpr int kBlock = 256;        // threads per block of every kernel
+
+// Offsets inside a partial record (after the 3 x ncell histograms).
+constexpr int kTrLowN = 0, kTrLowX = 1, kTrLowZ = 2;
+constexpr int kTrHighN = 3, kTrHighX = 4, kTrHighZ = 5;
+constexpr int kMomSum = 6;     // 6 shifted sums
+constexpr int kMomSq = 12;     // 6 shifted sums of squares
+
+struct Tile {
+  int bunch;   // bunch index
+  int start;   // first particle (global index into coord)
+  int count;   // particles in this tile
+  int pad;
+};
+
+// Scalars the particle map reads (transform_weak.c:35-46 and the ring
+// values it uses).  Written once at set-up.
+struct OpticConst {
+  double damp, excite;
+  double qv_pos, qv_slope, qh_pos, qh_slope;
+  double E0;
+  double wrf, Urad, T0, ac;
+  double psiV0, psiH0, Gziz, Gzix;
+  double CHH, CHV, CVH, CVV;
+  double alphaV, betaV, gammaV, alphaH, betaH, gammaH;
+  double dispH, disppH;
+  double HC_k, m_aHC_d, m_phi_n;   // ideal HC: HC_k, (double) m_aHC, m_aHC * phi_n
+  double ahc_amp[kMaxAhc];          // Vpeak / (E0 * 1e9)
+  double ahc_w[kMaxAhc];            // wrf * nHC
+  double ahc_phi[kMaxAhc];
+  double ahc_nhc[kMaxAhc];
+  int n_ahc;
+  int ideal_hc;
+  int amp_dep;
+  int quantum;
+  int track_h, track_v;
+  // binning (transform_weak.c:611-613)
+  double sigma_tau, nsigma, dT;
+  int ncell;
+};
+
+// Mutable ring-wide state, device resident, read by every kernel.
+struct RingState {
+  long turn;           // turns completed
+  double Vrf0, phai0;  // RF parameters after the feedback correction
+  int rffb_on;
+  int rffb_count;
+  int rw_m;            // resistive-wall trigger counter (worker_weakweak.c:254)
+  int error;           // sticky device error word (0 = ok)
+  int trash_low, trash_high;
+  double phasor[3][kMaxLr][2];
+};
+
+// Per long-range resonator constants (construct_wake_phasor
+// transform_weak.c:976-1004).
+struct LrConst {
+  int plane, l;
+  double Amp;          // 2 alpha Rs T0 / E0 / 1e9
+  double prog[2];      // one bin
+  double pn[2];        // ncell bins (product of prog, computed on the host)
+  double gap[3];       // exp, cos, sin over the inter-bunch gap
+  double emp[3];       // exp, cos, sin over an empty bucket
+  double p2b[2], pb2b[2];
+  int fb;              // this resonator drives the RF feedback
+};
+
+struct Args {
+  // geometry
+  int nbunch, ntile, npad, tile, prec, ncell, nharm;
+  // particles
+  double *coord;
+  const Tile *tiles;
+  // per bunch
+  const int *bunch_tile0;     // first tile of each bunch
+  const int *bunch_ntile;
+  const int *bunch_np;
+  const int *bunch_kb;
+  const int *bunch_off;
+  const double *bunch_ib;     // [A]
+  const double *bunch_fac;    // per long-range resonator: Amp / Np * 1e-3  [nlr][nbunch]
+  const double *bunch_factg;  // factG (transform_weak.c:567)
+  double *part;               // ntile x prec
+  double *shift;              // nbunch x 6
+  double *hist;               // nbunch x 6 x ncell: fnp, dipV, dipH (clamped), ring L, H, V (dropped)
+  int *cellrange;             // nbunch x 2: icellmin, icellmax
+  double *kick;               // nbunch x 3 x ncell: L, V, H kick tables
+  double *rwkick;             // nbunch x 2: pending RW kick (HOR, VER)
+  double *stats;              // stats_cap x nbunch x 12
+  int stats_cap;
+  // long-range resonators
+  int nlr;
+  const LrConst *lr;          // nlr
+  double *lr_u;               // nlr x nbunch x ncell x 2: in-bucket phasor from 0
+  double *lr_b;               // nlr x nbunch x ncell: source terms Ib fnp fac
+  double *lr_vs;              // nlr x nharm x 2: phasor at bucket start
+  const double *lr_pw;        // nlr x ncell x 2: prog^(j+1)
+  const int *bucket_bunch;    // nharm: bunch index or -1
+  const double *ibunch;       // nharm: [mA]
+  int lr_kick[3];             // apply long-range wake in plane (kick gate)
+  // self-field
+  const double *Gl, *Gv, *Gh;
+  int planeL, planeV, planeH;
+  double RsisL, aindL, sgmatau2, dTau2;
+  int hist_xz;                // dipole histograms needed
+  int selffield;              // binning + kicks active
+  // resistive wall
+  int rw_long, Nmlt;
+  double *dipole;             // (Nmlt+2) nharm x 2
+  const double *rw_rsq;       // (Nmlt+1) nharm + 1: 1 / sqrt(m T0 / h)
+  double rw_const[2][2];      // [trigger halved?][plane-1]
+  int triggerRW;
+  // RF feedback
+  int rffb_len;
+  int rffb_off_after_init;
+  double *rffb_hist;          // len x 2
+  double rffb_vrf_design, rffb_phi0_design;
+  double E0;
+  // noise
+  int noise;                  // MBT_NOISE_PHILOX / _INJECTED / NONE
+  uint64_t seed;
+  const float *dev;           // injected deviates: turns x 5 x npad
+  long dev_turn0;             // first turn held in dev
+  long dev_nturn;
+  // state
+  RingState *rs;
+  OpticConst oc;
+};
+
+}  // namespace mbt

@@ -1,0 +1,627 @@
+// mbt_kernels.cuh -- the per-turn kernels of the weak-weak loop.
+//
+// One turn of worker_weakweak.c:259-394 for every bunch is four launches:
+//
+//   turn_map      particle pass over all bunches (K1): pending resistive-
+//                 wall kick (transform_weak.c:829-830 of the previous
+//                 turn), self-field and long-range wake kick
+//                 (transform_weak.c:697-731), RF/radiation/noise/drift
+//                 (:49-97), vertical and horizontal betatron maps
+//                 (:101-190); then, on the new coordinates, shifted moment
+//                 sums (statistics.c:91-128) and the binning of the next
+//                 turn (transform_weak.c:608-631, :839-865).  HBM-bound.
+//   bunch_reduce  one block per bunch: partial records -> histograms,
+//                 statistics, resistive-wall dipole history
+//                 (worker_weakweak.c:306-318), in-bucket phasor recurrence
+//                 of each long-range resonator (transform_weak.c:1014-1027).
+//   ring_scan     one block: the phasor of each long-range resonator around
+//                 the ring, bucket h-1 .. 0 (transform_weak.c:1006-1044),
+//                 RF-feedback samples and correction (feedback_rf.c,
+//                 worker_weakweak.c:268-278).
+//   bunch_wakes   one block per bunch: causal convolutions with the Green's
+//                 functions (transform_weak.c:653-731), long-range wake per
+//                 bin, kick tables, resistive-wall sum over the dipole
+//                 history (transform_weak.c:813-825).
+//
+// Arithmetic that the parity tests compare against the oracle keeps the
+// reference's operation order; the library is compiled with -fmad=false.
+#pragma once
+#include <cstdint>
+#include "mbt_device.cuh"
+#include "mbt_philox.cuh"
+
+namespace mbt {
+
+#define MBT_PI 3.14159265358979323846
+
+__device__ __forceinline__ int bin_of(double xtau, double sgm, double nsig, double dT) {
+  // icell = (int)((Tau + Nsigma)/dT + 1), Tau = -xtau/sigma
+  // (transform_weak.c:611-613): IEEE division, truncation toward zero.
+  const double Tau = __ddiv_rn(-xtau, sgm);
+  const double q = __ddiv_rn(__dadd_rn(Tau, nsig), dT);
+  return __double2int_rz(__dadd_rn(q, 1.0));
+}
+
+__device__ __forceinline__ long cyc_slot(long k, long n) {
+  // cyclic_array_get/access (cyclic_array.c:21-34) with an int index
+  const int in = (int)k;
+  const long r = (long)in % n;
+  return in < 0 ? (r + n) % n : r;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------- K1
+
+template <bool MOVE, int NOISE, bool HISTXZ>
+__global__ void __launch_bounds__(kBlock) turn_map(Args a) {
+  extern __shared__ double smem[];
+  const int nc = a.ncell;
+  const Tile tile = a.tiles[blockIdx.x];
+  const int b = tile.bunch;
+  double *kL = smem;
+  double *kV = smem + nc;
+  double *kH = smem + 2 * nc;
+  double *hx = smem + 3 * nc;
+  double *hz = smem + 4 * nc;
+  int *hc = reinterpret_cast<int *>(smem + 5 * nc);
+  __shared__ double red[kBlock / 32][kPartialExtra];
+
+  const bool sf = MOVE && a.selffield;
+  for (int i = threadIdx.x; i < nc; i += kBlock) {
+    if (sf) {
+      kL[i] = a.kick[(size_t)(b * 3 + 0) * nc + i];
+      kV[i] = a.kick[(size_t)(b * 3 + 1) * nc + i];
+      kH[i] = a.kick[(size_t)(b * 3 + 2) * nc + i];
+    }
+    hc[i] = 0;
+    if (HISTXZ) { hx[i] = 0.0; hz[i] = 0.0; }
+  }
+  __syncthreads();
+
+  const OpticConst &oc = a.oc;
+  const long turn = a.rs->turn;
+  const double eps_const = a.rs->Vrf0 / (oc.E0 * 1.0e3);
+  const double phai0 = a.rs->phai0;
+  const int kb = a.bunch_kb[b];
+  double sh[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) sh[k] = a.shift[b * 6 + k];
+  double rwH = 0.0, rwV = 0.0;
+  const bool rw = MOVE && a.rw_long && turn > 0;
+  if (rw) { rwH = a.rwkick[b * 2 + 0]; rwV = a.rwkick[b * 2 + 1]; }
+  const bool kick_l = sf && a.lr_kick[0];
+  const bool kick_h = sf && a.lr_kick[1];
+  const bool kick_v = sf && a.lr_kick[2];
+  // aHC->nHC * kb * 2 * M_PI, per active harmonic cavity
+  double ahc_ph[kMaxAhc];
+#pragma unroll
+  for (int j = 0; j < kMaxAhc; ++j)
+    ahc_ph[j] = (j < oc.n_ahc) ? oc.ahc_phi[j] : 0.0;
+
+  double ms[6] = {0, 0, 0, 0, 0, 0}, mq[6] = {0, 0, 0, 0, 0, 0};
+  double lowN = 0, lowX = 0, lowZ = 0, highN = 0, highX = 0, highZ = 0;
+  const int jb0 = tile.start - a.bunch_off[b];   // index of the tile's first particle in its bunch
+  const size_t np6 = (size_t)a.npad;
+  double *__restrict__ C = a.coord;
+
+  for (int i = threadIdx.x; i < tile.count; i += kBlock) {
+    const size_t p = (size_t)tile.start + i;
+    double xtau = C[p], x = C[np6 + p], z = C[2 * np6 + p];
+    double eps = C[3 * np6 + p], xp = C[4 * np6 + p], zp = C[5 * np6 + p];
+    if (MOVE) {
+      if (rw) {
+        if (oc.track_h) xp = xp + rwH;
+        if (oc.track_v) zp = zp + rwV;
+      }
+      if (sf) {
+        int ic = bin_of(xtau, oc.sigma_tau, oc.nsigma, oc.dT);
+        ic = ic < 0 ? 0 : (ic >= nc ? nc - 1 : ic);
+        if (kick_l) eps = eps + kL[ic];
+        if (kick_v) zp = zp + kV[ic];
+        if (kick_h) xp = xp + kH[ic];
+      }
+      // ---- longitudinal (transform_weak.c:49-97)
+      const double xtau0 = xtau, eps0 = eps, x0 = x, xp0 = xp, z0 = z, zp0 = zp;
+      double g;
+      if (!oc.ideal_hc) {
+        g = eps_const * sin(oc.wrf * xtau0 + phai0);
+        for (int j = 0; j < oc.n_ahc; ++j) {
+          const double ph = oc.ahc_nhc[j] * (double)kb * 2 * MBT_PI;
+          g += oc.ahc_amp[j] * sin(oc.ahc_w[j] * xtau0 + ahc_ph[j] + ph);
+        }
+      } else {
+        g = eps_const * (sin(oc.wrf * xtau0 + phai0) + oc.HC_k * sin(oc.m_aHC_d * oc.wrf * xtau0 + oc.m_phi_n));
+      }
+      float dv[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+      if (NOISE == MBT_NOISE_PHILOX) {
+        turn_normals(a.seed, (uint32_t)(jb0 + i), (uint32_t)kb, (uint64_t)turn, dv);
+      } else if (NOISE == MBT_NOISE_INJECTED) {
+        const long dt = turn - a.dev_turn0;
+        if (dt >= 0 && dt < a.dev_nturn) {
+          const float *d = a.dev + (size_t)dt * 5 * np6 + p;
+#pragma unroll
+          for (int k = 0; k < 5; ++k) dv[k] = d[(size_t)k * np6];
+        } else if (threadIdx.x == 0) {
+          atomicOr(&a.rs->error, 1);
+        }
+      }
+      eps = eps0 + g - oc.Urad;
+      double rff = 1.0;
+      if (NOISE != MBT_NOISE_NONE) {
+        eps = eps * oc.damp + oc.excite * (double)dv[0];
+        rff = (1.0 + eps0) / (1.0 + eps0 + g);
+      }
+      xtau = xtau0 - eps * oc.T0 * oc.ac;
+      // ---- amplitude terms (transform_weak.c:115-123, 159-167)
+      double EV = 0.0, EH = 0.0;
+      if (oc.amp_dep) {
+        EV = oc.gammaV * z0 * z0 + 2 * oc.alphaV * z0 * zp0 + oc.betaV * zp0 * zp0;
+        EH = oc.gammaV * x0 * x0 + 2 * oc.alphaV * x0 * xp0 + oc.betaV * xp0 * xp0;
+      }
+      // ---- vertical (transform_weak.c:101-141)
+      if (oc.track_v) {
+        const double dQ = oc.amp_dep ? (oc.CVH * EH + oc.CVV * EV) : 0.0;
+        const double psi = oc.psiV0 * (1.0 + oc.Gziz * eps0 + dQ);
+        double sn, cs;
+        sincos(psi, &sn, &cs);
+        const double a11 = cs + oc.alphaV * sn, a12 = oc.betaV * sn;
+        const double a21 = -oc.gammaV * sn, a22 = cs - oc.alphaV * sn;
+        z = a11 * z0 + a12 * zp0;
+        zp = a21 * z0 + a22 * zp0;
+        if (NOISE != MBT_NOISE_NONE) {
+          z = z + oc.qv_pos * (double)dv[1];
+          zp = rff * zp + oc.qv_slope * (double)dv[2];
+        }
+      }
+      // ---- horizontal (transform_weak.c:144-190)
+      if (oc.track_h) {
+        const double dQ = oc.amp_dep ? (oc.CHH * EH + oc.CHV * EV) : 0.0;
+        const double psi = oc.psiH0 * (1.0 + oc.Gzix * eps0 + dQ);
+        double sn, cs;
+        sincos(psi, &sn, &cs);
+        const double a11 = cs + oc.alphaH * sn;
+        const double a12 = oc.betaH * sn;
+        const double a13 = (1.0 - a11) * oc.dispH - a12 * oc.disppH;
+        const double a21 = -oc.gammaH * sn;
+        const double a22 = cs - oc.alphaH * sn;
+        const double a23 = -a21 * oc.dispH + (1.0 - a22) * oc.disppH;
+        x = a11 * x0 + a12 * xp0 + a13 * eps;
+        xp = a21 * x0 + a22 * xp0 + a23 * eps;
+        if (NOISE != MBT_NOISE_NONE) {
+          x = x + oc.qh_pos * (double)dv[3];
+          xp = rff * xp + oc.qh_slope * (double)dv[4];
+        }
+      }
+      C[p] = xtau; C[np6 + p] = x; C[2 * np6 + p] = z;
+      C[3 * np6 + p] = eps; C[4 * np6 + p] = xp; C[5 * np6 + p] = zp;
+    }
+    // ---- moments (statistics.c:91-128), shifted sums
+    {
+      const double c6[6] = {xtau, x, z, eps, xp, zp};
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double d = c6[k] - sh[k];
+        ms[k] += d;
+        mq[k] += d * d;
+      }
+    }
+    // ---- binning of the next turn
+    if (a.selffield) {
+      const int ic = bin_of(xtau, oc.sigma_tau, oc.nsigma, oc.dT);
+      if (ic >= 0 && ic < nc) {
+        atomicAdd(&hc[ic], 1);
+        if (HISTXZ) {
+          atomicAdd(&hx[ic], x);
+          atomicAdd(&hz[ic], z);
+        }
+      } else if (ic < 0) {
+        lowN += 1.0; lowX += x; lowZ += z;
+      } else {
+        highN += 1.0; highX += x; highZ += z;
+      }
+    }
+  }
+
+  // ---- block reduction in a fixed order
+  double v[kPartialExtra] = {lowN, lowX, lowZ, highN, highX, highZ,
+                             ms[0], ms[1], ms[2], ms[3], ms[4], ms[5],
+                             mq[0], mq[1], mq[2], mq[3], mq[4], mq[5]};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kPartialExtra; ++k) {
+    const double s = warp_sum(v[k]);
+    if (lane == 0) red[warp][k] = s;
+  }
+  __syncthreads();
+  double *rec = a.part + (size_t)blockIdx.x * a.prec;
+  if (threadIdx.x < kPartialExtra) {
+    double s = 0.0;
+    for (int w = 0; w < kBlock / 32; ++w) s += red[w][threadIdx.x];
+    rec[3 * nc + threadIdx.x] = s;
+  }
+  for (int i = threadIdx.x; i < nc; i += kBlock) {
+    rec[i] = (double)hc[i];
+    rec[nc + i] = HISTXZ ? hx[i] : 0.0;
+    rec[2 * nc + i] = HISTXZ ? hz[i] : 0.0;
+  }
+}
+
+// ---------------------------------------------------------------- K2a
+
+enum { kReduceTurn = 0, kReducePrologue = 1 };
+
+__global__ void __launch_bounds__(kBlock) bunch_reduce(Args a, int mode, double *stats_init) {
+  extern __shared__ double tot[];   // prec doubles
+  const int b = blockIdx.x, nc = a.ncell;
+  const int t0 = a.bunch_tile0[b], nt = a.bunch_ntile[b];
+  for (int e = threadIdx.x; e < a.prec; e += kBlock) {
+    double s = 0.0;
+    for (int k = 0; k < nt; ++k) s += a.part[(size_t)(t0 + k) * a.prec + e];
+    tot[e] = s;
+  }
+  __syncthreads();
+  const double *ex = tot + 3 * nc;
+  const double N = (double)a.bunch_np[b];
+  const int kb = a.bunch_kb[b];
+  const long turn = a.rs->turn;
+
+  // histograms: clamped (bins 0 and ncell-1 collect the out-of-range
+  // particles, transform_weak.c:615-624) and dropped (:857-862)
+  double *H = a.hist + (size_t)b * 6 * nc;
+  if (a.selffield) {
+    for (int j = threadIdx.x; j < nc; j += kBlock) {
+      const double cn = tot[j], sx = tot[nc + j], sz = tot[2 * nc + j];
+      double f = cn, dv = sz, dh = sx;
+      if (j == 0) { f += ex[kTrLowN]; dv += ex[kTrLowZ]; dh += ex[kTrLowX]; }
+      if (j == nc - 1) { f += ex[kTrHighN]; dv += ex[kTrHighZ]; dh += ex[kTrHighX]; }
+      H[j] = f;
+      H[nc + j] = dv;
+      H[2 * nc + j] = dh;
+      H[3 * nc + j] = cn;
+      H[4 * nc + j] = sx;
+      H[5 * nc + j] = sz;
+    }
+  }
+  __shared__ double mean6[6];
+  if (threadIdx.x < 6) {
+    const int k = threadIdx.x;
+    const int plane = k % 3;
+    const bool tracked = plane == 0 || (plane == 1 ? a.oc.track_h : a.oc.track_v);
+    double mean = 0.0, rms = 0.0;
+    if (tracked && N > 0) {
+      const double s = ex[kMomSum + k] / N;
+      const double q = ex[kMomSq + k] / N;
+      mean = a.shift[b * 6 + k] + s;
+      const double var = q - s * s;
+      rms = sqrt(var > 0.0 ? var : 0.0);
+      a.shift[b * 6 + k] = mean;
+    }
+    mean6[k] = mean;
+    // row order pos[3], pos_sigma[3], slope[3], slope_sigma[3]
+    const int col = (k < 3) ? k : 6 + (k - 3);
+    double *row = (mode == kReduceTurn)
+                      ? a.stats + ((size_t)(turn % a.stats_cap) * a.nbunch + b) * 12
+                      : stats_init + (size_t)b * 12;
+    row[col] = mean;
+    row[col + 3] = rms;
+  }
+  if (threadIdx.x == 0 && a.selffield) {
+    atomicAdd(&a.rs->trash_low, (int)ex[kTrLowN]);
+    atomicAdd(&a.rs->trash_high, (int)ex[kTrHighN]);
+  }
+  __syncthreads();
+  // resistive-wall dipole history (worker_weakweak.c:306-318; set-up
+  // fill :203-219)
+  if (a.rw_long && threadIdx.x == 0) {
+    const long n = (long)(a.Nmlt + 2) * a.nharm;
+    if (mode == kReduceTurn) {
+      double *mom = a.dipole + 2 * cyc_slot(-turn * a.nharm + kb, n);
+      mom[0] = mean6[1];
+      mom[1] = mean6[2];
+    } else {
+      const int jmax = a.Nmlt > 1 ? a.Nmlt : 1;
+      for (int j = 0; j < jmax; ++j) {
+        double *mom = a.dipole + 2 * cyc_slot((long)j * a.nharm + kb, n);
+        mom[0] = mean6[1];
+        mom[1] = mean6[2];
+      }
+    }
+  }
+  // in-bucket phasor of each long-range resonator, starting from zero:
+  // V_j = V_{j-1} prog - Ib fnp_j fac  (transform_weak.c:1017-1018)
+  if (a.selffield && threadIdx.x < a.nlr) {
+    const int r = threadIdx.x;
+    const LrConst L = a.lr[r];
+    const double *src = H + (size_t)(3 + L.plane) * nc;   // dropped histogram of the plane
+    const double fac = a.bunch_fac[(size_t)r * a.nbunch + b];
+    const double ib = a.ibunch[kb];
+    double *u = a.lr_u + ((size_t)r * a.nbunch + b) * nc * 2;
+    double *bb = a.lr_b + ((size_t)r * a.nbunch + b) * nc;
+    double v0 = 0.0, v1 = 0.0;
+    for (int j = 0; j < nc; ++j) {
+      const double s = ib * src[j] * fac;
+      const double n0 = (v0 * L.prog[0] - v1 * L.prog[1]) - s;
+      const double n1 = (v0 * L.prog[1] + v1 * L.prog[0]);
+      v0 = n0; v1 = n1;
+      u[2 * j] = v0;
+      u[2 * j + 1] = v1;
+      bb[j] = s;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- K2b
+
+// Feedback sample (rffb_get_vrf_phi, feedback_rf.c:5-12): note atan2(real, imag).
+__device__ __forceinline__ void rffb_store(Args &a, int slot, double vr, double vi) {
+  a.rffb_hist[2 * slot] = sqrt(vr * vr + vi * vi);
+  a.rffb_hist[2 * slot + 1] = atan2(vr, vi);
+}
+
+// passes: number of turns of phasor propagation; init: wake_phasor_init
+// semantics (V starts at 0); advance: bump the turn counter afterwards.
+// vbuf: scratch of 2 x nharm complex values (before/after each bucket).
+__global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init, int advance,
+                                                    double *vbuf) {
+  RingState *rs = a.rs;
+  const int h = a.nharm;
+  __shared__ int fb_live;
+  if (threadIdx.x == 0) fb_live = rs->rffb_on;
+  __syncthreads();
+  for (int r = 0; r < a.nlr; ++r) {
+    const LrConst L = a.lr[r];
+    const bool fb = L.fb && fb_live;
+    double v0, v1;
+    if (init) { v0 = 0.0; v1 = 0.0; } else { v0 = rs->phasor[L.plane][L.l][0]; v1 = rs->phasor[L.plane][L.l][1]; }
+    for (int pass = 0; pass < passes; ++pass) {
+      if (threadIdx.x == 0) {
+        double *vs = a.lr_vs + (size_t)r * h * 2;
+        for (int m = 0; m < h; ++m) {
+          const int i = h - m - 1;
+          if (fb) { vbuf[4 * m] = v0; vbuf[4 * m + 1] = v1; }
+          vs[2 * i] = v0;
+          vs[2 * i + 1] = v1;
+          const int bi = a.bucket_bunch[i];
+          if (bi >= 0) {
+            const double *u = a.lr_u + ((size_t)r * a.nbunch + bi) * a.ncell * 2 + 2 * (a.ncell - 1);
+            const double n0 = (v0 * L.pn[0] - v1 * L.pn[1]) + u[0];
+            const double n1 = (v0 * L.pn[1] + v1 * L.pn[0]) + u[1];
+            v0 = (n0 * L.gap[0] * L.gap[1] - n1 * L.gap[0] * L.gap[2]);
+            v1 = (n0 * L.gap[0] * L.gap[2] + n1 * L.gap[0] * L.gap[1]);
+          } else {
+            const double n0 = v0, n1 = v1;
+            v0 = (n0 * L.emp[0] * L.emp[1] - n1 * L.emp[0] * L.emp[2]);
+            v1 = (n0 * L.emp[0] * L.emp[2] + n1 * L.emp[0] * L.emp[1]);
+          }
+          if (fb) { vbuf[4 * m + 2] = v0; vbuf[4 * m + 3] = v1; }
+        }
+        rs->phasor[L.plane][L.l][0] = v0;
+        rs->phasor[L.plane][L.l][1] = v1;
+      }
+      __syncthreads();
+      if (fb) {
+        // samples s = 2m (before bucket h-1-m, rotated to the beam) and
+        // s = 2m+1 (after it); only the last len samples survive.
+        const int ns = 2 * h, len = a.rffb_len;
+        const int count0 = rs->rffb_count;
+        const int first = ns > len ? ns - len : 0;
+        for (int s = first + threadIdx.x; s < ns; s += kBlock) {
+          const int m = s >> 1;
+          const double w0 = vbuf[4 * m + 2 * (s & 1)], w1 = vbuf[4 * m + 2 * (s & 1) + 1];
+          const double *q = (s & 1) ? L.pb2b : L.p2b;
+          const double vr = w0 * q[0] - w1 * q[1];
+          const double vi = w0 * q[1] + w1 * q[0];
+          rffb_store(a, (int)(((unsigned)count0 + (unsigned)s) % (unsigned)len), vr, vi);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) rs->rffb_count = count0 + ns;
+        __syncthreads();
+      }
+      __syncthreads();
+    }
+  }
+  // RF-feedback correction (worker_weakweak.c:149-162, 268-278)
+  if (fb_live && a.rffb_len > 0) {
+    __shared__ double sv[kBlock / 32][2];
+    double s0 = 0.0, s1 = 0.0;
+    for (int m = threadIdx.x; m < a.rffb_len; m += kBlock) { s0 += a.rffb_hist[2 * m]; s1 += a.rffb_hist[2 * m + 1]; }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    if ((threadIdx.x & 31) == 0) { sv[threadIdx.x >> 5][0] = s0; sv[threadIdx.x >> 5][1] = s1; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double vs = 0.0, ps = 0.0;
+      for (int w = 0; w < kBlock / 32; ++w) { vs += sv[w][0]; ps += sv[w][1]; }
+      double vmbar = vs / a.rffb_len;
+      const double phibar = ps / a.rffb_len;
+      vmbar = vmbar * a.E0 * 1.0e3;
+      const double tmp = a.rffb_vrf_design * sin(a.rffb_phi0_design) - vmbar * sin(phibar);
+      const double ph = atan2(tmp, a.rffb_vrf_design * cos(a.rffb_phi0_design) - vmbar * cos(phibar));
+      rs->phai0 = ph;
+      rs->Vrf0 = tmp / sin(ph);
+      if (init && a.rffb_off_after_init) rs->rffb_on = 0;
+    }
+  }
+  if (threadIdx.x == 0 && advance) {
+    rs->turn += 1;
+    if (a.rw_long) rs->rw_m += 1;
+  }
+}
+
+// ---------------------------------------------------------------- K2c
+
+__global__ void __launch_bounds__(kBlock) bunch_wakes(Args a, int with_rw) {
+  extern __shared__ double sm[];
+  const int nc = a.ncell, b = blockIdx.x;
+  const int PADC = 4;
+  double *fnp = sm + PADC;                    // nc + 2 PADC
+  double *dipV = sm + (nc + 2 * PADC) + PADC;
+  double *dipH = sm + 2 * (nc + 2 * PADC) + PADC;
+  double *lr = sm + 3 * (nc + 2 * PADC);      // 3 x nc
+  const double *H = a.hist + (size_t)b * 6 * nc;
+  const int kb = a.bunch_kb[b];
+  __shared__ int cmin, cmax;
+  __shared__ double red[kBlock / 32][2];
+
+  if (a.selffield) {
+    for (int j = threadIdx.x - PADC; j < nc + PADC; j += kBlock) {
+      const bool in = j >= 0 && j < nc;
+      fnp[j] = in ? H[j] : 0.0;
+      dipV[j] = in ? H[nc + j] : 0.0;
+      dipH[j] = in ? H[2 * nc + j] : 0.0;
+    }
+    for (int j = threadIdx.x; j < 3 * nc; j += kBlock) lr[j] = 0.0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      // transform_weak.c:633-651
+      int mn = nc - 1, mx = 0;
+      for (int i = 0; i < mn; ++i) if (fnp[i] > 0) { mn = i; break; }
+      for (int i = nc - 1; i > mx; --i) if (fnp[i] > 0) { mx = i; break; }
+      cmin = mn; cmax = mx;
+    }
+    __syncthreads();
+    // long-range wake per bin: V_j = Vs prog^(j+1) + U_j; the reference
+    // adds V_j + Ib fnp_j fac / 2 for every resonator of the plane
+    // (transform_weak.c:1020-1023)
+    for (int r = 0; r < a.nlr; ++r) {
+      const LrConst L = a.lr[r];
+      const double *vs = a.lr_vs + (size_t)r * a.nharm * 2 + 2 * kb;
+      const double *u = a.lr_u + ((size_t)r * a.nbunch + b) * nc * 2;
+      const double *bb = a.lr_b + ((size_t)r * a.nbunch + b) * nc;
+      const double *pw = a.lr_pw + (size_t)r * nc * 2;
+      const double s0 = vs[0], s1 = vs[1];
+      for (int j = threadIdx.x; j < nc; j += kBlock) {
+        const double v0 = (s0 * pw[2 * j] - s1 * pw[2 * j + 1]) + u[2 * j];
+        lr[L.plane * nc + j] += v0 + 0.5 * bb[j];
+      }
+      __syncthreads();
+    }
+    const double factG = a.bunch_factg[b];
+    const int icellmin = cmin, icellmax = cmax;
+    for (int j = threadIdx.x; j < nc; j += kBlock) {
+      double GL1 = 0.0, GV = 0.0, GH = 0.0;
+      if (a.planeL > 0 && j >= icellmin) {
+        double Gn = 0.0;
+        for (int k = j; k >= icellmin; --k) Gn += fnp[k] * a.Gl[j - k];
+        GL1 = 1 * Gn;
+        if (a.RsisL > 0 && j >= icellmin + 1 && j <= icellmax) {
+          const double ntmoy = (0.5 * fnp[j - 1] + fnp[j] + 0.5 * fnp[j + 1]) / 2.0;
+          GL1 += a.RsisL * ntmoy / (a.oc.sigma_tau * a.oc.dT);
+        }
+        if (a.aindL > 0 && j >= icellmin + 1 && j <= icellmax) {
+          const double ntmoy0 = (0.25 * fnp[j - 3] + 0.5 * fnp[j - 2] + fnp[j - 1] + 0.5 * fnp[j] + 0.25 * fnp[j + 1]) / 2.5;
+          const double ntmoy1 = (0.25 * fnp[j - 1] + 0.5 * fnp[j] + fnp[j + 1] + 0.5 * fnp[j + 2] + 0.25 * fnp[j + 3]) / 2.5;
+          GL1 += (ntmoy1 - ntmoy0) / (2.0 * a.sgmatau2 * a.dTau2) * a.aindL;
+        }
+      }
+      if (a.planeV > 0) {
+        double Gn = 0.0;
+        for (int k = j; k >= 0; --k) Gn += dipV[k] * a.Gv[j - k];
+        GV = 1 * Gn;
+      }
+      if (a.planeH > 0 && j >= 1) {
+        double Gn = 0.0;
+        for (int k = j; k >= 0; --k) Gn += dipH[k] * a.Gh[j - k];
+        GH = 1 * Gn;
+      }
+      double *K = a.kick + (size_t)b * 3 * nc;
+      K[j] = factG * GL1 + lr[0 * nc + j];
+      K[nc + j] = -factG * GV + lr[2 * nc + j];
+      K[2 * nc + j] = -factG * GH + lr[1 * nc + j];
+    }
+  }
+  // long-range resistive wall (transform_weak.c:779-833) of the turn just
+  // completed; applied at the start of the next particle pass
+  if (a.rw_long) {
+    const long turn = a.rs->turn - 1;
+    const int mtrig = a.rs->rw_m - 1;
+    const int h = a.nharm;
+    const long n = (long)(a.Nmlt + 2) * h;
+    const long bpos = -turn * h + kb;
+    const int M = (a.Nmlt + 1) * h;
+    for (int pl = 1; pl <= 2; ++pl) {
+      const bool tracked = (pl == 1) ? a.oc.track_h : a.oc.track_v;
+      double s = 0.0;
+      if (with_rw && tracked) {
+        for (int m = 1 + threadIdx.x; m <= M; m += kBlock) {
+          const int k = (int)(bpos + m);
+          const int in_mod = k < 0 ? (k % h + h) % h : k % h;
+          if (a.bucket_bunch[in_mod] >= 0) {
+            const double *mom = a.dipole + 2 * cyc_slot(k, n);
+            s += mom[pl - 1] * a.ibunch[in_mod] * a.rw_rsq[m];
+          }
+        }
+      }
+      s = warp_sum(s);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][pl - 1] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      const int pl = threadIdx.x + 1;
+      double s = 0.0;
+      for (int w = 0; w < kBlock / 32; ++w) s += red[w][pl - 1];
+      const int trig = (a.triggerRW && mtrig < 50) ? 1 : 0;
+      a.rwkick[b * 2 + (pl - 1)] = with_rw ? s * a.rw_const[trig][pl - 1] : 0.0;
+    }
+  }
+}
+
+// ------------------------------------------------------------ helpers
+
+// Adds the pending resistive-wall kick to a copy of the coordinates (what
+// the next particle pass would start from).
+__global__ void add_pending_rw(Args a, double *out) {
+  if (!(a.rw_long && a.rs->turn > 0)) return;
+  const size_t n6 = (size_t)a.npad;
+  const int b = blockIdx.y;
+  const int off = a.bunch_off[b], np = a.bunch_np[b];
+  const double rh = a.rwkick[2 * b], rv = a.rwkick[2 * b + 1];
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += gridDim.x * blockDim.x) {
+    if (a.oc.track_h) out[4 * n6 + off + j] = a.coord[4 * n6 + off + j] + rh;
+    if (a.oc.track_v) out[5 * n6 + off + j] = a.coord[5 * n6 + off + j] + rv;
+  }
+}
+
+// First-particle shifts for the moment sums of the first binning pass.
+__global__ void init_shift(Args a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.nbunch) return;
+  const size_t n6 = (size_t)a.npad;
+  const int off = a.bunch_off[b];
+  for (int k = 0; k < 6; ++k) a.shift[b * 6 + k] = a.bunch_np[b] > 0 ? a.coord[k * n6 + off] : 0.0;
+}
+
+// Matched Gaussian beam from Philox normals (replaces
+// weak_bunch_normal_distribution, bunch_weak.c:86-105).
+__global__ void generate_beam(Args a, uint64_t seed, const double *pos_off, const double *slope_off,
+                              const double *pos_sgm, const double *slope_sgm, const double *corr) {
+  const int b = blockIdx.y;
+  const int np = a.bunch_np[b], off = a.bunch_off[b], kb = a.bunch_kb[b];
+  const size_t n6 = (size_t)a.npad;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += gridDim.x * blockDim.x) {
+    float g[5];
+    turn_normals(seed, (uint32_t)j, (uint32_t)kb, 0xFFFFFFFF00000000ull, g);
+    float g2[5];
+    turn_normals(seed, (uint32_t)j, (uint32_t)kb, 0xFFFFFFFE00000000ull, g2);
+    const float n[6] = {g[0], g[1], g[2], g[3], g[4], g2[0]};
+    for (int pl = 0; pl < 3; ++pl) {
+      const bool tracked = pl == 0 || (pl == 1 ? a.oc.track_h : a.oc.track_v);
+      double pos = 0.0, slope = 0.0;
+      if (tracked) {
+        const double tmp = pos_sgm[pl] * (double)n[2 * pl];
+        pos = pos_off[pl] + tmp;
+        slope = slope_off[pl] + slope_sgm[pl] * (double)n[2 * pl + 1] + corr[pl] * tmp;
+      }
+      a.coord[(size_t)pl * n6 + off + j] = pos;
+      a.coord[(size_t)(3 + pl) * n6 + off + j] = slope;
+    }
+  }
+}
+
+}  // namespace mbt

@@ -1,0 +1,68 @@
+// mbt_philox.cuh -- counter-based normal deviates for quantum excitation.
+//
+// Philox4x32-10 (J. K. Salmon, M. A. Moraes, R. O. Dror, D. E. Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC'11), keyed by the
+// run seed, with the counter (particle index in its bunch, bucket, turn,
+// block).  Normals come from the Box-Muller transform in single precision,
+// matching the single-precision deviates of the reference's generator
+// (bunch.c:407-436).  Every (seed, bucket, particle, turn) gets the same
+// deviates whatever the tiling or launch shape.
+#pragma once
+#include <cstdint>
+
+namespace mbt {
+
+struct U4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U4 philox_round(U4 c, uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+  uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+  U4 r;
+  r.x = hi1 ^ c.y ^ k0;
+  r.y = lo1;
+  r.z = hi0 ^ c.w ^ k1;
+  r.w = lo0;
+  return r;
+}
+
+__device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    c = philox_round(c, k0, k1);
+    k0 += W0;
+    k1 += W1;
+  }
+  return c;
+}
+
+// Two standard normals from two 32-bit words (Box-Muller, float).
+__device__ __forceinline__ void box_muller2(uint32_t a, uint32_t b, float &n0, float &n1) {
+  const float u1 = (float)((a >> 8) + 1u) * 5.9604644775390625e-08f;  // (0, 1]
+  const float u2 = (float)(b >> 8) * 5.9604644775390625e-08f;         // [0, 1)
+  const float r = sqrtf(-2.0f * logf(u1));
+  float s, c;
+  sincospif(2.0f * u2, &s, &c);
+  n0 = r * c;
+  n1 = r * s;
+}
+
+// The five deviates one particle draws per turn, in the reference's roles:
+// g[0] energy, g[1] z, g[2] z', g[3] x, g[4] x'.
+__device__ __forceinline__ void turn_normals(uint64_t seed, uint32_t particle, uint32_t bucket,
+                                             uint64_t turn, float g[5]) {
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  U4 c0 = {particle, bucket, (uint32_t)turn, ((uint32_t)(turn >> 32) << 1) | 0u};
+  U4 r0 = philox4x32_10(c0, k0, k1);
+  float a, b, c, d, e, f;
+  box_muller2(r0.x, r0.y, a, b);
+  box_muller2(r0.z, r0.w, c, d);
+  U4 c1 = c0;
+  c1.w |= 1u;
+  U4 r1 = philox4x32_10(c1, k0, k1);
+  box_muller2(r1.x, r1.y, e, f);
+  g[0] = a; g[1] = b; g[2] = c; g[3] = d; g[4] = e;
+}
+
+}  // namespace mbt

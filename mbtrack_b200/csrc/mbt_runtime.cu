@@ -1,0 +1,792 @@
+// mbt_runtime.cu -- libmbt C-ABI (include/mbt.h): tracking contexts on one
+// B200, replacing the MPI manager/worker distribution of
+// manager_weakweak.c / worker_weakweak.c with bunch-indexed blocks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "mbt.h"
+#include "mbt_device.cuh"
+#include "mbt_kernels.cuh"
+#include "mbt_wofz.cuh"
+
+using mbt::Args;
+using mbt::LrConst;
+using mbt::RingState;
+using mbt::Tile;
+
+namespace {
+
+constexpr double FKILO = 1.0e3, FGIGA = 1.0e9, FMILLI = 1.0e-3, FTERA = 1.0e12;
+constexpr double C_LIGHT = 2.997925e+08, Z_0 = 376.73;
+constexpr double PI = 3.14159265358979323846;
+
+thread_local char g_create_error[512] = "";
+
+}  // namespace
+
+struct mbt_ctx {
+  mbt_params p{};
+  int nbunch = 0, npad = 0, tile = 0, ntile = 0, prec = 0, nc = 0, nlr = 0;
+  std::vector<int> bucket, np, off, tile0, ntiles, bucket_bunch;
+  std::vector<double> ib;
+  std::vector<Tile> tiles;
+  std::vector<LrConst> lr;
+  int noise = MBT_NOISE_PHILOX;
+  uint64_t seed = 0;
+  int prepared = 0;
+  int histxz = 0;
+  Args a{};
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graph_turns = 0;
+  std::vector<void *> allocs;
+  float *dev = nullptr;
+  size_t dev_cap = 0;
+  double *vbuf = nullptr;
+  double *stats_init = nullptr;
+  double *xfer = nullptr;        // device staging for exports
+  double *pinned = nullptr;      // host staging
+  size_t pinned_bytes = 0;
+  cudaEvent_t ev[6] = {};
+  double timing[4] = {0, 0, 0, 0};
+  int device = 0;
+  char err[512] = "";
+};
+
+namespace {
+
+int fail(mbt_ctx *c, int code, const char *fmt, ...) {
+  char *dst = c ? c->err : g_create_error;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(dst, 512, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CK(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess)                                                         \
+      return fail(c, MBT_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                  __FILE__, __LINE__);                                             \
+  } while (0)
+
+template <typename T>
+int dalloc(mbt_ctx *c, T **ptr, size_t n) {
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess) return fail(c, MBT_ERR_NOMEM, "cudaMalloc(%zu): %s", n * sizeof(T), cudaGetErrorString(e));
+  cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(T));
+  c->allocs.push_back(p);
+  *ptr = static_cast<T *>(p);
+  return 0;
+}
+
+template <typename T>
+int dupload(mbt_ctx *c, T **ptr, const T *src, size_t n) {
+  int r = dalloc(c, ptr, n);
+  if (r) return r;
+  if (n) CK(cudaMemcpy(*ptr, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int check_device(mbt_ctx *c) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(c, MBT_ERR_NODEVICE, "no CUDA device (%s): libmbt has no CPU path",
+                e == cudaSuccess ? "count 0" : cudaGetErrorString(e));
+  return 0;
+}
+
+// Smallest tile that still fills the GPU: at least 4 tiles per SM when the
+// beam allows it, tiles between 512 and 8192 particles.
+int choose_tile(const std::vector<int> &np, int sms) {
+  long total = 0;
+  for (int n : np) total += n;
+  long want = std::max<long>(1, total / (4L * sms));
+  int t = 512;
+  while (t < 8192 && t < want) t <<= 1;
+  return t;
+}
+
+void cmul(double a0, double a1, double b0, double b1, double &r0, double &r1) {
+  r0 = a0 * b0 - a1 * b1;
+  r1 = a0 * b1 + a1 * b0;
+}
+
+int validate(mbt_ctx *c, const mbt_params *p, int nbunch, const int *bucket, const int *np) {
+  if (!p || nbunch <= 0 || !bucket || !np) return fail(c, MBT_ERR_INVALID, "null argument or nbunch <= 0");
+  if (p->nharm <= 0) return fail(c, MBT_ERR_INVALID, "nharm must be positive");
+  if (p->ncell < 0 || p->ncell > MBT_MAX_NCELL) return fail(c, MBT_ERR_INVALID, "ncell %d outside 0..%d", p->ncell, MBT_MAX_NCELL);
+  for (int i = 0; i < nbunch; ++i) {
+    if (bucket[i] < 0 || bucket[i] >= p->nharm) return fail(c, MBT_ERR_INVALID, "bucket[%d]=%d outside 0..h-1", i, bucket[i]);
+    if (i > 0 && bucket[i] <= bucket[i - 1]) return fail(c, MBT_ERR_INVALID, "buckets must be strictly ascending");
+    if (np[i] <= 0) return fail(c, MBT_ERR_INVALID, "np[%d]=%d must be positive", i, np[i]);
+  }
+  int nlr = p->n_lr[0] + p->n_lr[1] + p->n_lr[2];
+  for (int pl = 0; pl < 3; ++pl)
+    if (p->n_lr[pl] < 0 || p->n_lr[pl] > MBT_MAX_LR) return fail(c, MBT_ERR_INVALID, "n_lr[%d] outside 0..%d", pl, MBT_MAX_LR);
+  for (int pl = 1; pl < 3; ++pl)
+    if (p->n_lr[pl] > 0 && !p->track_plane[pl])
+      return fail(c, MBT_ERR_INVALID, "long-range resonator in an untracked plane %d", pl);
+  if ((nlr > 0 || p->planeL + p->planeV + p->planeH > 0) && p->ncell <= 0)
+    return fail(c, MBT_ERR_INVALID, "wakes need ncell > 0");
+  if (p->rffb && (p->n_lr[0] <= 0 || p->rffb_resonator < 1 || p->rffb_resonator > p->n_lr[0] || p->rffb_len <= 0))
+    return fail(c, MBT_ERR_INVALID, "RF feedback needs a longitudinal long-range resonator and a positive averaging length");
+  if (p->n_active_hc < 0 || p->n_active_hc > MBT_MAX_AHC) return fail(c, MBT_ERR_INVALID, "n_active_hc outside 0..%d", MBT_MAX_AHC);
+  if (p->rw_long && (p->Nmlt < 0 || p->beffH[0] <= 0 && p->track_plane[1] || p->beffV[0] <= 0 && p->track_plane[2]))
+    return fail(c, MBT_ERR_INVALID, "long-range resistive wall needs Nmlt >= 0 and beffH3/beffV3 > 0");
+  if (!p->track_plane[0]) return fail(c, MBT_ERR_INVALID, "the longitudinal plane is always tracked");
+  return 0;
+}
+
+template <bool MOVE, int NOISE, bool HISTXZ>
+void launch_map(mbt_ctx *c) {
+  const size_t sm = (size_t)c->nc * 5 * sizeof(double) + (size_t)c->nc * sizeof(int);
+  mbt::turn_map<MOVE, NOISE, HISTXZ><<<c->ntile, mbt::kBlock, sm, c->stream>>>(c->a);
+}
+
+template <bool MOVE>
+void launch_map_noise(mbt_ctx *c, int noise) {
+  if (c->histxz) {
+    if (!MOVE || noise == MBT_NOISE_NONE) launch_map<MOVE, MBT_NOISE_NONE, true>(c);
+    else if (noise == MBT_NOISE_PHILOX) launch_map<MOVE, MBT_NOISE_PHILOX, true>(c);
+    else launch_map<MOVE, MBT_NOISE_INJECTED, true>(c);
+  } else {
+    if (!MOVE || noise == MBT_NOISE_NONE) launch_map<MOVE, MBT_NOISE_NONE, false>(c);
+    else if (noise == MBT_NOISE_PHILOX) launch_map<MOVE, MBT_NOISE_PHILOX, false>(c);
+    else launch_map<MOVE, MBT_NOISE_INJECTED, false>(c);
+  }
+}
+
+int effective_noise(const mbt_ctx *c) { return c->p.quantum ? c->noise : MBT_NOISE_NONE; }
+
+size_t smem_reduce(const mbt_ctx *c) { return (size_t)c->prec * sizeof(double); }
+size_t smem_wakes(const mbt_ctx *c) { return ((size_t)3 * (c->nc + 8) + 3 * (size_t)c->nc) * sizeof(double); }
+
+// One turn: particle pass, bunch reduction, ring scan, bunch wakes.
+void enqueue_turn(mbt_ctx *c, cudaEvent_t *ev) {
+  if (ev) cudaEventRecord(ev[0], c->stream);
+  launch_map_noise<true>(c, effective_noise(c));
+  if (ev) cudaEventRecord(ev[1], c->stream);
+  mbt::bunch_reduce<<<c->nbunch, mbt::kBlock, smem_reduce(c), c->stream>>>(c->a, mbt::kReduceTurn, nullptr);
+  if (ev) cudaEventRecord(ev[2], c->stream);
+  mbt::ring_scan<<<1, mbt::kBlock, 0, c->stream>>>(c->a, 1, 0, 1, c->vbuf);
+  if (ev) cudaEventRecord(ev[3], c->stream);
+  mbt::bunch_wakes<<<c->nbunch, mbt::kBlock, smem_wakes(c), c->stream>>>(c->a, 1);
+  if (ev) cudaEventRecord(ev[4], c->stream);
+}
+
+int sync_and_check(mbt_ctx *c) {
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  RingState rs;
+  CK(cudaMemcpy(&rs, c->a.rs, sizeof(rs), cudaMemcpyDeviceToHost));
+  if (rs.error) return fail(c, MBT_ERR_STATE, "device error word %d (deviates exhausted?)", rs.error);
+  return 0;
+}
+
+int ensure_pinned(mbt_ctx *c, size_t bytes) {
+  if (c->pinned_bytes >= bytes) return 0;
+  if (c->pinned) cudaFreeHost(c->pinned);
+  c->pinned = nullptr;
+  c->pinned_bytes = 0;
+  CK(cudaMallocHost((void **)&c->pinned, bytes));
+  c->pinned_bytes = bytes;
+  return 0;
+}
+
+int build_graph(mbt_ctx *c, int turns) {
+  if (c->graph && c->graph_turns == turns) return 0;
+  if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  for (int t = 0; t < turns; ++t) enqueue_turn(c, nullptr);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (e != cudaSuccess) return fail(c, MBT_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&c->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(c, MBT_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  c->graph_turns = turns;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t mbt_params_size(void) { return sizeof(mbt_params); }
+
+int mbt_last_error(const mbt_ctx *ctx, char *buf, size_t len) {
+  if (!buf || len == 0) return MBT_ERR_INVALID;
+  snprintf(buf, len, "%s", ctx ? ctx->err : g_create_error);
+  return 0;
+}
+
+int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np, const double *ib,
+               const double *Gl, const double *Gv, const double *Gh, int noise_mode, uint64_t seed,
+               mbt_ctx **out) {
+  mbt_ctx *c = nullptr;
+  if (!out) return fail(nullptr, MBT_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  int r = check_device(nullptr);
+  if (r) return r;
+  r = validate(nullptr, p, nbunch, bucket, np);
+  if (r) return r;
+  if (!ib) return fail(nullptr, MBT_ERR_INVALID, "ib is NULL");
+  if (noise_mode != MBT_NOISE_PHILOX && noise_mode != MBT_NOISE_INJECTED)
+    return fail(nullptr, MBT_ERR_INVALID, "unknown noise mode %d", noise_mode);
+  c = new (std::nothrow) mbt_ctx;
+  if (!c) return fail(nullptr, MBT_ERR_NOMEM, "host allocation");
+  c->p = *p;
+  c->nbunch = nbunch;
+  c->noise = noise_mode;
+  c->seed = seed;
+  c->bucket.assign(bucket, bucket + nbunch);
+  c->np.assign(np, np + nbunch);
+  c->ib.assign(ib, ib + nbunch);
+  cudaGetDevice(&c->device);
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, c->device);
+  auto bail = [&](int code) { int rc = code; mbt_destroy(c); return rc; };
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(nullptr, MBT_ERR_CUDA, "stream create"));
+  for (auto &e : c->ev) cudaEventCreate(&e);
+
+  // geometry: bunches padded to 32 particles, tiles inside bunches
+  c->tile = choose_tile(c->np, prop.multiProcessorCount);
+  c->off.resize(nbunch);
+  c->tile0.resize(nbunch);
+  c->ntiles.resize(nbunch);
+  long pos = 0;
+  for (int b = 0; b < nbunch; ++b) {
+    c->off[b] = (int)pos;
+    c->tile0[b] = (int)c->tiles.size();
+    int nt = 0;
+    for (int s = 0; s < c->np[b]; s += c->tile) {
+      Tile t{b, (int)(pos + s), std::min(c->tile, c->np[b] - s), 0};
+      c->tiles.push_back(t);
+      ++nt;
+    }
+    c->ntiles[b] = nt;
+    pos += (c->np[b] + 31) / 32 * 32;
+  }
+  if (pos > 0x7fffffffL / 6) return bail(fail(nullptr, MBT_ERR_INVALID, "beam too large for one context"));
+  c->npad = (int)pos;
+  c->ntile = (int)c->tiles.size();
+  c->nc = std::max(p->ncell, 1);
+  c->prec = 3 * c->nc + mbt::kPartialExtra;
+  c->bucket_bunch.assign(p->nharm, -1);
+  for (int b = 0; b < nbunch; ++b) c->bucket_bunch[c->bucket[b]] = b;
+
+  Args &a = c->a;
+  a.nbunch = nbunch;
+  a.ntile = c->ntile;
+  a.npad = c->npad;
+  a.tile = c->tile;
+  a.prec = c->prec;
+  a.ncell = c->nc;
+  a.nharm = p->nharm;
+  const int lr_tot = p->n_lr[0] + p->n_lr[1] + p->n_lr[2];
+  a.selffield = (p->ncell > 0 && p->planeL + p->planeV + p->planeH + lr_tot > 0) ? 1 : 0;
+  c->histxz = a.selffield && (p->planeV > 0 || p->planeH > 0 || p->n_lr[1] > 0 || p->n_lr[2] > 0);
+  a.hist_xz = c->histxz;
+  a.lr_kick[0] = (p->n_lr[0] + p->planeL) > 0;
+  a.lr_kick[1] = p->planeH > 0;
+  a.lr_kick[2] = p->planeV > 0;
+  a.planeL = p->planeL; a.planeV = p->planeV; a.planeH = p->planeH;
+  a.RsisL = p->RsisL; a.aindL = p->aindL;
+  a.sgmatau2 = p->sigma_tau * p->sigma_tau;
+  a.dTau2 = p->dT * p->dT;
+  a.rw_long = p->rw_long; a.Nmlt = p->Nmlt; a.triggerRW = p->triggerRW;
+  a.E0 = p->E0;
+  a.noise = noise_mode;
+  a.seed = seed;
+
+  std::vector<int> np_v(c->np), kb_v(c->bucket);
+  std::vector<double> ibunch(p->nharm, 0.0), factg(nbunch);
+  for (int b = 0; b < nbunch; ++b) {
+    ibunch[c->bucket[b]] = c->ib[b] * FKILO;   // manager_weakweak.c:78
+    factg[b] = -p->T0 * c->ib[b] / (c->np[b] * p->E0 * FGIGA);   // transform_weak.c:567
+  }
+
+  // long-range resonator constants (transform_weak.c:976-1004)
+  const double hd = (double)p->nharm;
+  const double dTau = p->dT * p->sigma_tau;
+  const double tbucket = (p->T0 / hd - p->ncell * dTau);
+  std::vector<double> fac, pw;
+  for (int pl = 0; pl < 3; ++pl) {
+    for (int l = 0; l < p->n_lr[pl]; ++l) {
+      LrConst L{};
+      L.plane = pl;
+      L.l = l;
+      const double wr = p->lr_wr[pl][l], Q = p->lr_Q[pl][l], Rs = p->lr_Rs[pl][l];
+      const double alpha = wr * 0.5 / Q;
+      L.Amp = 2 * alpha * Rs * p->T0 / p->E0 / FGIGA;
+      const double C0 = -alpha, C1 = wr;
+      L.prog[0] = exp(C0 * dTau) * cos(C1 * dTau);
+      L.prog[1] = exp(C0 * dTau) * sin(C1 * dTau);
+      L.fb = (p->rffb && pl == 0 && p->rffb_resonator == l + 1) ? 1 : 0;
+      double taubeam = 0, taub2beam = 0;
+      if (L.fb) {
+        taubeam = p->nsigma * p->sigma_tau + dTau * 1.5;
+        taub2beam = -p->nsigma * p->sigma_tau + dTau * 0.5 - tbucket;
+      }
+      L.p2b[0] = exp(C0 * taubeam) * cos(C1 * taubeam);
+      L.p2b[1] = exp(C0 * taubeam) * sin(C1 * taubeam);
+      L.pb2b[0] = exp(C0 * taub2beam) * cos(C1 * taub2beam);
+      L.pb2b[1] = exp(C0 * taub2beam) * sin(C1 * taub2beam);
+      L.gap[0] = exp(C0 * tbucket); L.gap[1] = cos(C1 * tbucket); L.gap[2] = sin(C1 * tbucket);
+      L.emp[0] = exp(C0 * p->T0 / hd); L.emp[1] = cos(C1 * p->T0 / hd); L.emp[2] = sin(C1 * p->T0 / hd);
+      double q0 = 1.0, q1 = 0.0;
+      for (int j = 0; j < c->nc; ++j) {
+        double r0, r1;
+        cmul(q0, q1, L.prog[0], L.prog[1], r0, r1);
+        q0 = r0; q1 = r1;
+        pw.push_back(q0);
+        pw.push_back(q1);
+      }
+      L.pn[0] = q0; L.pn[1] = q1;
+      for (int b = 0; b < nbunch; ++b) fac.push_back(L.Amp / c->np[b] * FMILLI);   // per source bunch
+      c->lr.push_back(L);
+    }
+  }
+  c->nlr = (int)c->lr.size();
+  a.nlr = c->nlr;
+
+  // resistive wall: RWconst (transform_weak.c:811) and 1/sqrt(m T0/h)
+  std::vector<double> rsq;
+  if (p->rw_long) {
+    const int M = (p->Nmlt + 1) * p->nharm;
+    rsq.resize(M + 1);
+    const double deltab = p->T0 / hd;
+    rsq[0] = 0.0;
+    for (int m = 1; m <= M; ++m) rsq[m] = 1.0 / sqrt(m * deltab);
+    for (int trig = 0; trig < 2; ++trig) {
+      for (int pl = 1; pl <= 2; ++pl) {
+        double beff3 = pl == 1 ? p->beffH[0] : p->beffV[0];
+        if (trig) beff3 /= 2;
+        // The reference divides RWconst by fNp and multiplies every term of
+        // the sum by fNp (transform_weak.c:811,822); both are left out.
+        a.rw_const[trig][pl - 1] = p->T0 / p->E0 / FTERA * p->Lc / (PI * pow(beff3, 3)) * sqrt(Z_0 * C_LIGHT * p->rhorw / PI);
+      }
+    }
+  }
+
+  // optics constants (transform_weak.c:35-46)
+  mbt::OpticConst &oc = a.oc;
+  oc.damp = 1.0 - p->De;
+  oc.excite = 2.0 * p->slope_sgm[0] * sqrt(p->T0 / p->taue);
+  oc.qv_pos = p->pos_sgm[2] * sqrt(2.0 * p->T0 / p->tauz);
+  oc.qv_slope = p->slope_sgm[2] * sqrt(2.0 * p->T0 / p->tauz);
+  oc.qh_pos = p->pos_sgm[1] * sqrt(2.0 * p->T0 / p->taux);
+  oc.qh_slope = p->slope_sgm[1] * sqrt(2.0 * p->T0 / p->taux);
+  oc.E0 = p->E0;
+  oc.wrf = p->wrf; oc.Urad = p->Urad; oc.T0 = p->T0; oc.ac = p->ac;
+  oc.psiV0 = 2.0 * PI * p->QV0;
+  oc.psiH0 = 2.0 * PI * p->QH0;
+  oc.Gziz = p->Gziz; oc.Gzix = p->Gzix;
+  oc.CHH = p->CHH; oc.CHV = p->CHV; oc.CVH = p->CVH; oc.CVV = p->CVV;
+  oc.alphaV = p->alpha1[2]; oc.betaV = p->beta1[2]; oc.gammaV = p->gamma1[2];
+  oc.alphaH = p->alpha1[1]; oc.betaH = p->beta1[1]; oc.gammaH = p->gamma1[1];
+  oc.dispH = p->dispH1; oc.disppH = p->disppH1;
+  oc.HC_k = p->HC_k; oc.m_aHC_d = (double)p->m_aHC; oc.m_phi_n = p->m_aHC * p->phi_n;
+  oc.n_ahc = p->n_active_hc;
+  for (int j = 0; j < p->n_active_hc; ++j) {
+    oc.ahc_amp[j] = p->ahc_vpeak[j] / (p->E0 * FGIGA);
+    oc.ahc_w[j] = p->wrf * p->ahc_nhc[j];
+    oc.ahc_phi[j] = p->ahc_phi[j];
+    oc.ahc_nhc[j] = p->ahc_nhc[j];
+  }
+  oc.ideal_hc = p->ideal_hc;
+  oc.amp_dep = p->amp_dep_qv;
+  oc.quantum = p->quantum;
+  oc.track_h = p->track_plane[1];
+  oc.track_v = p->track_plane[2];
+  oc.sigma_tau = p->sigma_tau;
+  oc.nsigma = p->nsigma;
+  oc.dT = p->dT;
+  oc.ncell = c->nc;
+
+  // device allocations
+  int rc = 0;
+  std::vector<double> g0(c->nc, 0.0);
+  auto gl = [&](const double *g) { return g ? g : g0.data(); };
+  rc = rc ? rc : dalloc(c, &a.coord, (size_t)6 * c->npad);
+  Tile *tiles_d = nullptr;
+  rc = rc ? rc : dupload(c, &tiles_d, c->tiles.data(), c->tiles.size());
+  a.tiles = tiles_d;
+  int *ip;
+  rc = rc ? rc : dupload(c, &ip, c->tile0.data(), nbunch); a.bunch_tile0 = ip;
+  rc = rc ? rc : dupload(c, &ip, c->ntiles.data(), nbunch); a.bunch_ntile = ip;
+  rc = rc ? rc : dupload(c, &ip, np_v.data(), nbunch); a.bunch_np = ip;
+  rc = rc ? rc : dupload(c, &ip, kb_v.data(), nbunch); a.bunch_kb = ip;
+  rc = rc ? rc : dupload(c, &ip, c->off.data(), nbunch); a.bunch_off = ip;
+  rc = rc ? rc : dupload(c, &ip, c->bucket_bunch.data(), p->nharm); a.bucket_bunch = ip;
+  double *dp;
+  rc = rc ? rc : dupload(c, &dp, c->ib.data(), nbunch); a.bunch_ib = dp;
+  rc = rc ? rc : dupload(c, &dp, fac.empty() ? g0.data() : fac.data(), std::max<size_t>(fac.size(), 1)); a.bunch_fac = dp;
+  rc = rc ? rc : dupload(c, &dp, factg.data(), nbunch); a.bunch_factg = dp;
+  rc = rc ? rc : dupload(c, &dp, ibunch.data(), p->nharm); a.ibunch = dp;
+  rc = rc ? rc : dupload(c, &dp, gl(Gl), c->nc); a.Gl = dp;
+  rc = rc ? rc : dupload(c, &dp, gl(Gv), c->nc); a.Gv = dp;
+  rc = rc ? rc : dupload(c, &dp, gl(Gh), c->nc); a.Gh = dp;
+  rc = rc ? rc : dalloc(c, &a.part, (size_t)c->ntile * c->prec);
+  rc = rc ? rc : dalloc(c, &a.shift, (size_t)nbunch * 6);
+  rc = rc ? rc : dalloc(c, &a.hist, (size_t)nbunch * 6 * c->nc);
+  rc = rc ? rc : dalloc(c, &a.cellrange, (size_t)nbunch * 2);
+  rc = rc ? rc : dalloc(c, &a.kick, (size_t)nbunch * 3 * c->nc);
+  rc = rc ? rc : dalloc(c, &a.rwkick, (size_t)nbunch * 2);
+  a.stats_cap = 256;
+  rc = rc ? rc : dalloc(c, &a.stats, (size_t)a.stats_cap * nbunch * 12);
+  rc = rc ? rc : dalloc(c, &c->stats_init, (size_t)nbunch * 12);
+  LrConst *lr_d = nullptr;
+  rc = rc ? rc : dupload(c, &lr_d, c->lr.empty() ? nullptr : c->lr.data(), c->lr.size());
+  a.lr = lr_d;
+  const size_t nlr1 = std::max(c->nlr, 1);
+  rc = rc ? rc : dalloc(c, &a.lr_u, nlr1 * nbunch * c->nc * 2);
+  rc = rc ? rc : dalloc(c, &a.lr_b, nlr1 * nbunch * c->nc);
+  rc = rc ? rc : dalloc(c, &a.lr_vs, nlr1 * p->nharm * 2);
+  rc = rc ? rc : dupload(c, &dp, pw.empty() ? g0.data() : pw.data(), std::max<size_t>(pw.size(), 1)); a.lr_pw = dp;
+  rc = rc ? rc : dalloc(c, &c->vbuf, (size_t)4 * p->nharm);
+  rc = rc ? rc : dalloc(c, &a.dipole, p->rw_long ? (size_t)(p->Nmlt + 2) * p->nharm * 2 : 1);
+  rc = rc ? rc : dupload(c, &dp, rsq.empty() ? g0.data() : rsq.data(), std::max<size_t>(rsq.size(), 1)); a.rw_rsq = dp;
+  a.rffb_len = p->rffb ? p->rffb_len : 0;
+  a.rffb_off_after_init = p->rffb_off_after_init;
+  a.rffb_vrf_design = p->rffb_vrf_design;
+  a.rffb_phi0_design = p->rffb_phi0_design;
+  rc = rc ? rc : dalloc(c, &a.rffb_hist, (size_t)2 * std::max(a.rffb_len, 1));
+  rc = rc ? rc : dalloc(c, &a.rs, 1);
+  rc = rc ? rc : dalloc(c, &c->xfer, (size_t)6 * c->npad);
+  if (rc) { snprintf(g_create_error, sizeof g_create_error, "%s", c->err); return bail(rc); }
+  RingState rs{};
+  rs.turn = 0;
+  rs.Vrf0 = p->Vrf0;
+  rs.phai0 = p->phai0;
+  rs.rffb_on = p->rffb;
+  if (cudaMemcpy(a.rs, &rs, sizeof rs, cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(fail(nullptr, MBT_ERR_CUDA, "state upload"));
+  const size_t smw = smem_wakes(c);
+  if (smw > 48 * 1024)
+    cudaFuncSetAttribute(mbt::bunch_wakes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw);
+  *out = c;
+  return 0;
+}
+
+int mbt_destroy(mbt_ctx *c) {
+  if (!c) return 0;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  for (void *p : c->allocs) cudaFree(p);
+  if (c->dev) cudaFree(c->dev);
+  if (c->pinned) cudaFreeHost(c->pinned);
+  for (auto &e : c->ev) if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return 0;
+}
+
+int mbt_load_particles(mbt_ctx *c, int ibunch, const double *soa6, int np) {
+  if (!c || !soa6) return MBT_ERR_INVALID;
+  if (ibunch < 0 || ibunch >= c->nbunch) return fail(c, MBT_ERR_INVALID, "bunch %d out of range", ibunch);
+  if (np != c->np[ibunch]) return fail(c, MBT_ERR_INVALID, "bunch %d holds %d particles, got %d", ibunch, c->np[ibunch], np);
+  for (int k = 0; k < 6; ++k)
+    CK(cudaMemcpyAsync(c->a.coord + (size_t)k * c->npad + c->off[ibunch], soa6 + (size_t)k * np,
+                       np * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int mbt_load_all(mbt_ctx *c, const double *soa6_all) {
+  if (!c || !soa6_all) return MBT_ERR_INVALID;
+  size_t pos = 0;
+  for (int b = 0; b < c->nbunch; ++b) {
+    for (int k = 0; k < 6; ++k)
+      CK(cudaMemcpyAsync(c->a.coord + (size_t)k * c->npad + c->off[b], soa6_all + pos + (size_t)k * c->np[b],
+                         c->np[b] * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    pos += (size_t)6 * c->np[b];
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int mbt_generate_beam(mbt_ctx *c, uint64_t seed) {
+  if (!c) return MBT_ERR_INVALID;
+  double h[15];
+  for (int k = 0; k < 3; ++k) {
+    h[k] = c->p.pos_offset[k];
+    h[3 + k] = c->p.slope_offset[k];
+    h[6 + k] = c->p.pos_sgm[k];
+    h[9 + k] = c->p.slope_sgm[k];
+    h[12 + k] = c->p.correlate[k];
+  }
+  double *d = c->xfer;
+  CK(cudaMemcpyAsync(d, h, sizeof h, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->a.coord, 0, (size_t)6 * c->npad * sizeof(double), c->stream));
+  dim3 grid(64, c->nbunch);
+  mbt::generate_beam<<<grid, 256, 0, c->stream>>>(c->a, seed, d, d + 3, d + 6, d + 9, d + 12);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+static int export_all(mbt_ctx *c) {
+  CK(cudaMemcpyAsync(c->xfer, c->a.coord, (size_t)6 * c->npad * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  dim3 grid(16, c->nbunch);
+  mbt::add_pending_rw<<<grid, 256, 0, c->stream>>>(c->a, c->xfer);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int mbt_get_particles(mbt_ctx *c, int ibunch, double *soa6, int np) {
+  if (!c || !soa6) return MBT_ERR_INVALID;
+  if (ibunch < 0 || ibunch >= c->nbunch) return fail(c, MBT_ERR_INVALID, "bunch %d out of range", ibunch);
+  if (np != c->np[ibunch]) return fail(c, MBT_ERR_INVALID, "bunch %d holds %d particles, got %d", ibunch, c->np[ibunch], np);
+  int r = export_all(c);
+  if (r) return r;
+  for (int k = 0; k < 6; ++k)
+    CK(cudaMemcpyAsync(soa6 + (size_t)k * np, c->xfer + (size_t)k * c->npad + c->off[ibunch],
+                       np * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int mbt_get_all(mbt_ctx *c, double *soa6_all) {
+  if (!c || !soa6_all) return MBT_ERR_INVALID;
+  int r = export_all(c);
+  if (r) return r;
+  size_t pos = 0;
+  for (int b = 0; b < c->nbunch; ++b) {
+    for (int k = 0; k < 6; ++k)
+      CK(cudaMemcpyAsync(soa6_all + pos + (size_t)k * c->np[b], c->xfer + (size_t)k * c->npad + c->off[b],
+                         c->np[b] * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    pos += (size_t)6 * c->np[b];
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int mbt_prepare(mbt_ctx *c, double *init_stats) {
+  if (!c) return MBT_ERR_INVALID;
+  Args &a = c->a;
+  mbt::init_shift<<<(c->nbunch + 255) / 256, 256, 0, c->stream>>>(a);
+  launch_map_noise<false>(c, MBT_NOISE_NONE);
+  mbt::bunch_reduce<<<c->nbunch, mbt::kBlock, smem_reduce(c), c->stream>>>(a, mbt::kReducePrologue, c->stats_init);
+  if (c->nlr > 0 && c->p.lr_init_turns > 0)
+    mbt::ring_scan<<<1, mbt::kBlock, 0, c->stream>>>(a, c->p.lr_init_turns, 1, 0, c->vbuf);
+  mbt::ring_scan<<<1, mbt::kBlock, 0, c->stream>>>(a, 1, 0, 0, c->vbuf);
+  mbt::bunch_wakes<<<c->nbunch, mbt::kBlock, smem_wakes(c), c->stream>>>(a, 0);
+  CK(cudaGetLastError());
+  int r = sync_and_check(c);
+  if (r) return r;
+  if (init_stats)
+    CK(cudaMemcpy(init_stats, c->stats_init, (size_t)c->nbunch * 12 * sizeof(double), cudaMemcpyDeviceToHost));
+  c->prepared = 1;
+  return 0;
+}
+
+int mbt_set_deviates(mbt_ctx *c, const float *dev, long nturns) {
+  if (!c || !dev || nturns <= 0) return MBT_ERR_INVALID;
+  if (c->noise != MBT_NOISE_INJECTED) return fail(c, MBT_ERR_STATE, "context was not created with MBT_NOISE_INJECTED");
+  const int per = 1 + 2 * (c->p.track_plane[2] != 0) + 2 * (c->p.track_plane[1] != 0);
+  const size_t need = (size_t)nturns * 5 * c->npad;
+  if (need > c->dev_cap) {
+    if (c->dev) cudaFree(c->dev);
+    c->dev = nullptr;
+    c->dev_cap = 0;
+    CK(cudaMalloc(&c->dev, need * sizeof(float)));
+    c->dev_cap = need;
+  }
+  std::vector<float> h(need, 0.0f);
+  size_t src = 0;
+  for (long t = 0; t < nturns; ++t) {
+    float *T = h.data() + (size_t)t * 5 * c->npad;
+    for (int b = 0; b < c->nbunch; ++b) {
+      const int n = c->np[b], o = c->off[b];
+      for (int j = 0; j < n; ++j) T[o + j] = dev[src + j];
+      size_t q = src + n;
+      if (c->p.track_plane[2]) {
+        for (int j = 0; j < n; ++j) {
+          T[(size_t)1 * c->npad + o + j] = dev[q + 2 * j];
+          T[(size_t)2 * c->npad + o + j] = dev[q + 2 * j + 1];
+        }
+        q += 2 * (size_t)n;
+      }
+      if (c->p.track_plane[1]) {
+        for (int j = 0; j < n; ++j) {
+          T[(size_t)3 * c->npad + o + j] = dev[q + 2 * j];
+          T[(size_t)4 * c->npad + o + j] = dev[q + 2 * j + 1];
+        }
+      }
+      src += (size_t)per * n;
+    }
+  }
+  CK(cudaMemcpy(c->dev, h.data(), need * sizeof(float), cudaMemcpyHostToDevice));
+  RingState rs;
+  CK(cudaMemcpy(&rs, c->a.rs, sizeof rs, cudaMemcpyDeviceToHost));
+  c->a.dev = c->dev;
+  c->a.dev_turn0 = rs.turn;
+  c->a.dev_nturn = nturns;
+  if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; c->graph_turns = 0; }
+  return 0;
+}
+
+static int run_core(mbt_ctx *c, long nturns, double *stats, bool use_graph) {
+  if (!c->prepared) return fail(c, MBT_ERR_STATE, "mbt_prepare must come first");
+  RingState rs;
+  CK(cudaMemcpy(&rs, c->a.rs, sizeof rs, cudaMemcpyDeviceToHost));
+  long turn = rs.turn;
+  const long cap = c->a.stats_cap;
+  long done = 0;
+  CK(cudaEventRecord(c->ev[5], c->stream));
+  while (done < nturns) {
+    // a chunk never crosses a wrap of the statistics buffer
+    const long slot = turn % cap;
+    const long chunk = std::min(nturns - done, cap - slot);
+    long t = 0;
+    if (use_graph && chunk >= 8) {
+      const int G = 8;
+      int r = build_graph(c, G);
+      if (r) return r;
+      for (; t + G <= chunk; t += G) CK(cudaGraphLaunch(c->graph, c->stream));
+    }
+    for (; t < chunk; ++t) enqueue_turn(c, nullptr);
+    CK(cudaGetLastError());
+    if (stats)
+      CK(cudaMemcpyAsync(stats + (size_t)done * c->nbunch * 12, c->a.stats + (size_t)slot * c->nbunch * 12,
+                         (size_t)chunk * c->nbunch * 12 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    done += chunk;
+    turn += chunk;
+  }
+  CK(cudaEventRecord(c->ev[4], c->stream));
+  int r = sync_and_check(c);
+  if (r) return r;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[5], c->ev[4]);
+  c->timing[3] = ms;
+  return 0;
+}
+
+int mbt_run_turns(mbt_ctx *c, long nturns, double *stats) {
+  if (!c || nturns < 0) return MBT_ERR_INVALID;
+  return run_core(c, nturns, stats, true);
+}
+
+int mbt_track(mbt_ctx *c, double *particles, long nturns, double *stats) {
+  if (!c || !particles || nturns < 0) return MBT_ERR_INVALID;
+  int r = mbt_load_all(c, particles);
+  if (r) return r;
+  if (!c->prepared) { r = mbt_prepare(c, nullptr); if (r) return r; }
+  r = run_core(c, nturns, stats, true);
+  if (r) return r;
+  return mbt_get_all(c, particles);
+}
+
+// Per-kernel device times of nturns turns launched one by one with CUDA
+// events between the kernels: out[0..3] = average ms per turn of the
+// particle pass, bunch reduction, ring scan, bunch wakes.
+int mbt_profile_turns(mbt_ctx *c, long nturns, double out[4]) {
+  if (!c || nturns <= 0 || !out) return MBT_ERR_INVALID;
+  if (!c->prepared) return fail(c, MBT_ERR_STATE, "mbt_prepare must come first");
+  double acc[4] = {0, 0, 0, 0};
+  for (long t = 0; t < nturns; ++t) {
+    enqueue_turn(c, c->ev);
+    CK(cudaEventSynchronize(c->ev[4]));
+    for (int k = 0; k < 4; ++k) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]);
+      acc[k] += ms;
+    }
+  }
+  int r = sync_and_check(c);
+  if (r) return r;
+  for (int k = 0; k < 4; ++k) out[k] = acc[k] / nturns;
+  return 0;
+}
+
+int mbt_get_state(mbt_ctx *c, mbt_state *st) {
+  if (!c || !st) return MBT_ERR_INVALID;
+  RingState rs;
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(&rs, c->a.rs, sizeof rs, cudaMemcpyDeviceToHost));
+  memset(st, 0, sizeof *st);
+  st->turn = rs.turn;
+  st->Vrf0 = rs.Vrf0;
+  st->phai0 = rs.phai0;
+  for (int pl = 0; pl < 3; ++pl)
+    for (int l = 0; l < MBT_MAX_LR; ++l)
+      for (int k = 0; k < 2; ++k) st->phasor[pl][l][k] = rs.phasor[pl][l][k];
+  st->n_trash_low = rs.trash_low;
+  st->n_trash_high = rs.trash_high;
+  return 0;
+}
+
+int mbt_get_histograms(mbt_ctx *c, int ibunch, double *fnp, double *dipV, double *dipH, double *ring_lon,
+                       double *ring_hor, double *ring_ver) {
+  if (!c) return MBT_ERR_INVALID;
+  if (ibunch < 0 || ibunch >= c->nbunch) return fail(c, MBT_ERR_INVALID, "bunch %d out of range", ibunch);
+  std::vector<double> h((size_t)6 * c->nc);
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(h.data(), c->a.hist + (size_t)ibunch * 6 * c->nc, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  double *dst[6] = {fnp, dipV, dipH, ring_lon, ring_hor, ring_ver};
+  for (int k = 0; k < 6; ++k)
+    if (dst[k]) memcpy(dst[k], h.data() + (size_t)k * c->nc, c->p.ncell * sizeof(double));
+  return 0;
+}
+
+int mbt_last_timing(mbt_ctx *c, double out[4], int *launches_per_turn) {
+  if (!c || !out) return MBT_ERR_INVALID;
+  for (int k = 0; k < 4; ++k) out[k] = c->timing[k];
+  if (launches_per_turn) *launches_per_turn = 4;
+  return 0;
+}
+
+int mbt_geometry(mbt_ctx *c, int *npad, int *tile, int *ntile) {
+  if (!c) return MBT_ERR_INVALID;
+  if (npad) *npad = c->npad;
+  if (tile) *tile = c->tile;
+  if (ntile) *ntile = c->ntile;
+  return 0;
+}
+
+// ---- per-step device entry points
+
+int mbt_wofz_dev(long n, const double *x, const double *y, double *re, double *im, int *flag, void *stream) {
+  mbt_ctx *c = nullptr;
+  if (n < 0 || (n > 0 && (!x || !y || !re || !im))) return fail(c, MBT_ERR_INVALID, "bad wofz arguments");
+  if (n == 0) return 0;
+  int r = check_device(c);
+  if (r) return r;
+  const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 16);
+  mbt::wofz_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(n, x, y, re, im, flag);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int mbt_be_field_dev(long n, const double *dx, const double *dy, double sgm_xx_mm, double sgm_zz_mm, double factdq,
+                     double *ex, double *ey, void *stream) {
+  mbt_ctx *c = nullptr;
+  if (n < 0 || (n > 0 && (!dx || !dy || !ex || !ey))) return fail(c, MBT_ERR_INVALID, "bad be_field arguments");
+  if (!(sgm_xx_mm > sgm_zz_mm) || !(sgm_zz_mm > 0))
+    return fail(c, MBT_ERR_INVALID, "Bassetti-Erskine needs sgm_xx > sgm_zz > 0");
+  if (n == 0) return 0;
+  int r = check_device(c);
+  if (r) return r;
+  const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 16);
+  mbt::be_field_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(n, dx, dy, sgm_xx_mm, sgm_zz_mm, factdq, ex, ey);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+}  // extern "C"

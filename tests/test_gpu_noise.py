@@ -1,0 +1,41 @@
+"""The counter-based noise of the device path (Philox4x32-10 + Box-Muller)
+against the reference's generator, statistically: the equilibrium beam
+sizes it produces, and reproducibility for a fixed seed."""
+import numpy as np
+import pytest
+
+from mbtrack_b200 import api
+from oracle.binding import Oracle
+from tests.util import small_conf
+
+pytestmark = pytest.mark.gpu
+
+
+def test_equilibrium_sizes_match_reference_generator(tmp_path, cuda_device, libmbt):
+    cfg = api.Config(small_conf(tmp_path, "single_bunch.conf", Np=20000, EnableQuantum=1))
+    o = Oracle(cfg.params, cfg.bucket, [cfg.params.np_model], cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh)
+    o.generate_beam()
+    t = api.Tracker.from_config(cfg, seed=1234)
+    t.load_particles(0, o.get_particles(0))
+    o.prepare()
+    t.prepare()
+    turns = 1500
+    so = o.run(turns)
+    st = t.run(turns)
+    # rms energy spread, bunch length, horizontal and vertical sizes over the
+    # last 500 turns: same equilibrium within the statistical error
+    for col in (3, 4, 5, 9, 10, 11):
+        a = st[-500:, 0, col].mean()
+        b = so[-500:, 0, col].mean()
+        assert abs(a - b) / b < 0.02, (col, a, b)
+
+
+def test_philox_is_reproducible(tmp_path, cuda_device, libmbt):
+    cfg = api.Config(small_conf(tmp_path, "single_bunch.conf", Np=5000, EnableQuantum=1))
+    runs = []
+    for _ in range(2):
+        t = api.Tracker.from_config(cfg, seed=99)
+        t.generate_beam(7)
+        t.prepare()
+        runs.append(t.run(20))
+    assert np.array_equal(runs[0], runs[1])

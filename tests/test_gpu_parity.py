@@ -1,0 +1,164 @@
+"""Parity of the CUDA path (libmbt through its C-ABI) with the oracle.
+
+Bars (north star of this port): coordinates within 1e-12 relative after N
+turns (relative to each coordinate's rms spread), centroid and rms histories
+within 1e-10, histogram counts bit-exact on identical coordinates."""
+import numpy as np
+import pytest
+
+from mbtrack_b200 import api
+from mbtrack_b200.abi import MBT_NOISE_INJECTED
+from oracle.binding import Oracle
+from tests.golden_cases import CASES, Case
+from tests.util import coord_err, small_conf, stats_err
+
+pytestmark = pytest.mark.gpu
+
+COORD_TOL = 1e-12
+STATS_TOL = 1e-10
+
+
+def tracker_for(c, noise=None):
+    mode = MBT_NOISE_INJECTED if c.params.quantum else 0
+    return api.Tracker(c.params, c.bucket, c.np, c.ib, c.Gl, c.Gv, c.Gh, noise=mode)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fixture_cases(name, cuda_device, libmbt):
+    c = Case(name)
+    t = tracker_for(c)
+    init = c.bunch_slices(c.init)
+    for i in range(c.nb):
+        t.load_particles(i, init[i])
+    st0 = t.prepare()
+    assert np.max(stats_err(st0, c.init_stats)) < STATS_TOL
+    if c.params.quantum:
+        t.set_deviates(c.deviates, c.turns)
+    st = t.run(c.turns)
+    assert np.max(stats_err(st, c.stats)) < STATS_TOL
+    final = c.bunch_slices(c.final)
+    worst = 0.0
+    for i in range(c.nb):
+        worst = max(worst, np.max(coord_err(t.get_particles(i), final[i])))
+    assert worst < COORD_TOL, worst
+    s = t.state()
+    assert abs(s.Vrf0 - c.vrf_phi[0]) <= 1e-12 * abs(c.vrf_phi[0])
+    assert abs(s.phai0 - c.vrf_phi[1]) <= 1e-12 * abs(c.vrf_phi[1])
+    t.close()
+
+
+def _oracle_and_tracker(cfg, noise_injected=False):
+    o = Oracle(cfg.params, cfg.bucket, np.full(cfg.nbunch, cfg.params.np_model),
+               cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh)
+    o.generate_beam()
+    t = api.Tracker.from_config(cfg, noise=MBT_NOISE_INJECTED if noise_injected else 0)
+    for i in range(cfg.nbunch):
+        t.load_particles(i, o.get_particles(i))
+    return o, t
+
+
+def test_single_bunch_full_size_2000_turns(tmp_path, cuda_device, libmbt):
+    """Single bunch, 1e5 macroparticles, broadband resonator in three planes,
+    noise off, 2000 turns: checked after 1, 10 and 2000 turns."""
+    cfg = api.Config(small_conf(tmp_path, "single_bunch.conf", xxCM_offset=0.05, zzCM_offset=0.02))
+    o, t = _oracle_and_tracker(cfg)
+    so0, st0 = o.prepare(), t.prepare()
+    assert np.max(stats_err(st0, so0)) < STATS_TOL
+    done = 0
+    for upto in (1, 10, 2000):
+        n = upto - done
+        so = o.run(n)
+        st = t.run(n)
+        done = upto
+        assert np.max(stats_err(st, so)) < STATS_TOL, upto
+        err = coord_err(t.get_particles(0), o.get_particles(0))
+        assert np.max(err) < COORD_TOL, (upto, err)
+
+
+def test_uniform_fill_all_buckets_with_noise(tmp_path, cuda_device, libmbt):
+    """All 416 buckets, RW over a 50-turn history plus the HOM, injected
+    deviates (reduced macroparticle count so the oracle stays fast)."""
+    cfg = api.Config(small_conf(tmp_path, "uniform_fill.conf", Np=64, xxCM_offset=0.05))
+    o, t = _oracle_and_tracker(cfg, noise_injected=True)
+    o.prepare()
+    t.prepare()
+    turns = 6
+    so, dev = o.run(turns, record=True)
+    t.set_deviates(dev, turns)
+    st = t.run(turns)
+    assert np.max(stats_err(st, so)) < STATS_TOL
+    worst = max(np.max(coord_err(t.get_particles(i), o.get_particles(i))) for i in range(cfg.nbunch))
+    assert worst < COORD_TOL
+
+
+def test_uneven_fill_feedback(tmp_path, cuda_device, libmbt):
+    """Uneven fill with the camshaft, RF feedback on the detuned fundamental
+    cavity, RW and HOM; shortened averaging so all paths are exercised."""
+    cfg = api.Config(small_conf(tmp_path, "uneven_fill.conf", Np=32, EnableQuantum=0))
+    o, t = _oracle_and_tracker(cfg)
+    so0, st0 = o.prepare(), t.prepare()
+    assert np.max(stats_err(st0, so0)) < STATS_TOL
+    so = o.run(4)
+    st = t.run(4)
+    assert np.max(stats_err(st, so)) < STATS_TOL
+    v, _ = o.state(0)
+    s = t.state()
+    assert abs(s.Vrf0 - v[0]) < 1e-11 * abs(v[0]) and abs(s.phai0 - v[1]) < 1e-11 * abs(v[1])
+
+
+def test_histogram_counts_bit_exact(tmp_path, cuda_device, libmbt):
+    """On identical coordinates the device binning (clamped and dropped
+    histograms, transform_weak.c:608-631 and :839-865) equals the oracle's:
+    counts bit for bit, position sums to rounding."""
+    c = Case("feedback_hc")
+    o = Oracle(c.params, c.bucket, c.np, c.ib, c.Gl, c.Gv, c.Gh)
+    o.generate_beam()
+    o.prepare()
+    o.run(7)
+    X = [o.get_particles(i) for i in range(c.nb)]
+    t = tracker_for(c)
+    for i in range(c.nb):
+        t.load_particles(i, X[i])
+    t.prepare()
+    o2 = Oracle(c.params, c.bucket, c.np, c.ib, c.Gl, c.Gv, c.Gh)
+    for i in range(c.nb):
+        o2.set_particles(i, X[i])
+    o2.prepare()                                   # dropped histograms of X
+    dropped = [o2.histograms(i)[3:5] for i in range(c.nb)]
+    o2.run(1)                                      # clamped histograms of X
+    for i in range(c.nb):
+        g = t.histograms(i)
+        r = o2.histograms(i)
+        assert np.array_equal(g[0], r[0]), "clamped counts, bunch %d" % i
+        assert np.array_equal(g[3], dropped[i][0]), "dropped counts, bunch %d" % i
+        scale = np.max(np.abs(X[i][1])) * c.np[i]
+        assert np.max(np.abs(g[2] - r[2])) <= 1e-13 * scale
+        assert np.max(np.abs(g[4] - dropped[i][1])) <= 1e-13 * scale
+
+
+def test_track_call_matches_resident_run(tmp_path, cuda_device, libmbt):
+    """mbt_track (host buffers in and out) gives the device-resident result."""
+    c = Case("train_rw_hom")
+    a = tracker_for(c)
+    b = tracker_for(c)
+    init = c.bunch_slices(c.init)
+    for i in range(c.nb):
+        a.load_particles(i, init[i])
+    a.prepare()
+    sa = a.run(5)
+    buf = np.concatenate([x.ravel() for x in init])
+    sb = np.zeros_like(sa)
+    b.track(buf, 5, sb)
+    assert np.array_equal(sa, sb)
+    assert np.array_equal(a.get_all(), buf)
+
+
+def test_errors_are_reported(cuda_device, libmbt):
+    c = Case("single_noiseoff")
+    t = tracker_for(c)
+    with pytest.raises(api.MbtError) as e:
+        t.run(1)
+    assert e.value.code == -5
+    with pytest.raises(api.MbtError) as e:
+        t.load_particles(0, np.zeros(6 * 3))
+    assert e.value.code == -1

@@ -1,0 +1,53 @@
+"""Shared helpers of the test-suite: configuration fixtures and comparisons."""
+import os
+
+import numpy as np
+
+from oracle.binding import conf_with
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CONFS = os.path.join(HERE, "confs")
+GOLDEN = os.path.join(HERE, "golden")
+
+
+def conf(name):
+    return os.path.join(CONFS, name)
+
+
+def small_conf(tmp_path, name, **overrides):
+    """A copy of tests/confs/<name> with `key = value` overrides; the fill
+    file of the uneven configuration is made absolute."""
+    src = conf(name)
+    text = open(src).read()
+    if "uneven_fill.txt" in text and "filling" not in overrides:
+        overrides["filling"] = os.path.join(CONFS, "uneven_fill.txt")
+    dst = os.path.join(str(tmp_path), name)
+    return conf_with(src, dst, **overrides)
+
+
+def coord_err(a, b):
+    """Largest difference per coordinate, relative to that coordinate's rms
+    spread in b (coordinates near zero have no meaningful relative error)."""
+    a = np.asarray(a).reshape(6, -1)
+    b = np.asarray(b).reshape(6, -1)
+    out = np.zeros(6)
+    for k in range(6):
+        scale = np.std(b[k])
+        if scale == 0:
+            scale = max(np.max(np.abs(b[k])), 1e-300)
+        out[k] = np.max(np.abs(a[k] - b[k])) / scale if a[k].size else 0.0
+    return out
+
+
+def stats_err(a, b):
+    """Statistics histories: centroids relative to the rms of the same
+    plane, rms values relative to themselves (12 columns, see mbt.h)."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    err = np.zeros(a.shape[:-1] + (12,))
+    for k in range(3):
+        for mean_col, rms_col in ((k, 3 + k), (6 + k, 9 + k)):
+            scale = np.maximum(np.abs(b[..., rms_col]), 1e-300)
+            err[..., mean_col] = np.abs(a[..., mean_col] - b[..., mean_col]) / scale
+            err[..., rms_col] = np.abs(a[..., rms_col] - b[..., rms_col]) / scale
+    return err

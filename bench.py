@@ -1,0 +1,366 @@
+"""Benchmark of the per-turn weak-weak tracking loop on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload uniform|single|uneven]
+
+Default workload (the uniform multi-bunch configuration): all 416 buckets
+filled at 0.5 nC, 2e4 macroparticles per bunch (8.32e6, 400 MB of FP64
+coordinates, larger than the 126 MB L2 so no flush is needed), long-range
+resistive wall over a 50-turn history plus a longitudinal HOM, quantum
+excitation on.  One step is one turn of the whole ring.
+
+b200 arm: `value` is device-timed (CUDA events on the context's stream)
+throughput with the beam resident in HBM; `e2e` goes through mbt_track, the
+host-buffer C-ABI call, with the beam uploaded from pinned host memory and
+statistics and beam downloaded inside the timed region; `roofline` times the
+particle-pass kernel alone with CUDA events between the kernels of a turn.
+With N GPUs every rank tracks its own independent ring (replicas, weak
+scaling); the time is the max over ranks.
+
+reference arm: the reference's own CPU code (oracle/_ref, the reference's
+sources compiled unmodified; the C restatement in oracle/ when that library
+is absent) on the host cores, bunches split across one process per core.
+"""
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import re
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFS = os.path.join(ROOT, "tests", "confs")
+WORKLOADS = {
+    "uniform": ("uniform_fill.conf", {}, "uniform fill: 416 bunches x 2e4 macroparticles, long-range RW "
+                                         "(50-turn history) + HOM, quantum excitation on"),
+    "single": ("single_bunch.conf", {"EnableQuantum": 1}, "single bunch: 1e5 macroparticles, broadband "
+                                                          "resonator in 3 planes, quantum excitation on"),
+    "uneven": ("uneven_fill.conf", {}, "uneven fill: 321 bunches incl. 5 nC camshaft, RW + HOM + RF "
+                                       "feedback, quantum excitation on"),
+}
+BYTES_PER_MP_TURN = 96   # 6 FP64 coordinates read and written per macroparticle per turn
+METRIC = "macroparticle-turns/s"
+
+
+def conf_path(workload, tmpdir):
+    from oracle.binding import conf_with
+    name, over, _ = WORKLOADS[workload]
+    src = os.path.join(CONFS, name)
+    over = dict(over)
+    if "uneven" in name:
+        over["filling"] = os.path.join(CONFS, "uneven_fill.txt")
+    if not over:
+        return src
+    return conf_with(src, os.path.join(tmpdir, name), **over)
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(workload):
+    """DRAM bytes per particle-pass launch from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "turn_map_%s_fill.md" % workload)
+    if not os.path.exists(p):
+        p = os.path.join(ROOT, "profiles", "turn_map_%s.md" % workload)
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.out = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.out = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ CPU side
+
+def _cpu_worker(args):
+    """One host process: bunches [lo, hi) of the ring for `turns` turns;
+    returns the wall time of each turn."""
+    kind, conf, lo, hi, turns = args
+    sys.path.insert(0, ROOT)
+    if kind == "reference":
+        from oracle.binding import Reference
+        R = Reference(conf, bunch_range=(lo, hi))
+        R.prepare()
+        step = lambda: R.lib.refh_run(1, None, None, 0)   # noqa: E731
+    else:
+        import numpy as np
+        from mbtrack_b200 import api as _api   # configuration parser only (C host)
+        from oracle.binding import Oracle
+        cfg = _api.Config(conf)
+        O = Oracle(cfg.params, cfg.bucket, np.full(cfg.nbunch, cfg.params.np_model),
+                   cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh)
+        O.set_range(lo, hi)
+        O.generate_beam()
+        O.prepare()
+        step = lambda: O.lib.orc_run(O.h, 1, None, None, None, 0)   # noqa: E731
+    times = []
+    for _ in range(turns):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def cpu_kind():
+    from oracle import binding
+    if binding.build_reference() is not None:
+        return "reference"
+    binding.build_oracle()
+    return "port"
+
+
+def cpu_run(workload, turns, tmpdir, cores=None):
+    """Time `turns` turns of the whole ring on the host cores (bunches split
+    over one process per core).  Returns (per-turn seconds list, info)."""
+    from mbtrack_b200 import api
+    conf = conf_path(workload, tmpdir)
+    cfg = api.Config(conf)
+    nb = cfg.nbunch
+    if cores is None:
+        cores = len(os.sched_getaffinity(0))
+    procs = max(1, min(cores, nb))
+    edges = [round(i * nb / procs) for i in range(procs + 1)]
+    kind = cpu_kind()
+    jobs = [(kind, conf, edges[i], edges[i + 1], turns) for i in range(procs)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_cpu_worker, jobs)
+    per_turn = [max(r[t] for r in res) for t in range(turns)]
+    info = {"kind": kind, "cores": procs, "bunches": nb,
+            "particles": int(nb * cfg.params.np_model)}
+    return per_turn, info
+
+
+# ------------------------------------------------------------ GPU side
+
+def rank_info():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from mbtrack_b200 import api
+    import tempfile
+    tmp = tempfile.mkdtemp()
+    conf = conf_path(args.workload, tmp)
+    cfg = api.Config(conf)
+    npart = int(cfg.nbunch * cfg.params.np_model)
+
+    # CPU baseline first (spawned processes; rank 0 at N=1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        per_turn, info = cpu_run(args.workload, args.cpu_turns, tmp)
+        t = float(np.mean(per_turn[1:])) if len(per_turn) > 1 else per_turn[0]
+        cpu = {"value": npart / t, "unit": METRIC, "cores": info["cores"], "kind": info["kind"],
+               "sample": "%d turns of the whole ring (%d bunches x %d macroparticles) split over %d "
+                         "processes, one per core; first turn dropped; time = slowest process"
+                         % (args.cpu_turns, info["bunches"], cfg.params.np_model, info["cores"])}
+
+    trk = api.Tracker.from_config(cfg, seed=1000 + rank)
+    trk.generate_beam(77 + rank)
+    trk.prepare()
+    trk.run(args.warmup, stats=False)
+
+    # timed region: device time of K turns (CUDA events inside mbt_run_turns)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        stats = trk.run(args.steps, stats=True)
+    torch.cuda.synchronize()
+    dev_ms = float(trk.timing()[0][3])
+    t_local = dev_ms / 1e3
+    if dist:
+        tt = torch.tensor([t_local], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+        dist.barrier()
+    else:
+        t_max = t_local
+    value = world * npart * args.steps / t_max
+
+    # per-kernel device times (events between the four kernels of a turn)
+    prof = trk.profile(args.profile_turns)
+    k1_ms = float(prof[0])
+    peak, peak_kind = measured_peak()
+    achieved = BYTES_PER_MP_TURN * npart / (k1_ms * 1e-3) / 1e9
+    traffic = profile_traffic(args.workload)
+
+    # end to end through mbt_track with pinned host buffers
+    e2e_turns = args.e2e_turns
+    pinned = torch.empty(6 * npart, dtype=torch.float64, pin_memory=True)
+    host = pinned.numpy()
+    host[:] = trk.get_all()
+    st_pinned = torch.empty(e2e_turns * cfg.nbunch * 12, dtype=torch.float64, pin_memory=True)
+    st_host = st_pinned.numpy()
+    e2e_t = []
+    for _ in range(args.e2e_steps + 1):
+        t0 = time.perf_counter()
+        trk.track(host, e2e_turns, st_host)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_sec = float(np.mean(e2e_t[1:]))
+    if dist:
+        tt = torch.tensor([e2e_sec], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_sec = float(tt.item())
+    e2e_value = world * npart * e2e_turns / e2e_sec
+    ok = bool(np.all(np.isfinite(stats)))
+    trk.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    _, name_over, desc = WORKLOADS[args.workload]
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "bunches": int(cfg.nbunch), "np_per_bunch": int(cfg.params.np_model),
+                   "macroparticles": npart, "turns_per_step": 1, "noise": "Philox4x32-10 counter RNG",
+                   "l2": "beam of %.0f MB > 126 MB L2, no flush" % (npart * 48 / 1e6),
+                   "parallelism": "replicas x%d" % world},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "turn_map (particle pass)", "peak_source": peak_kind,
+                     "bytes_per_launch": BYTES_PER_MP_TURN * npart, "launch_ms": k1_ms},
+        "kernels_ms_per_turn": {"turn_map": k1_ms, "bunch_reduce": float(prof[1]),
+                                "ring_scan": float(prof[2]), "bunch_wakes": float(prof[3])},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 6 * 8 * npart,
+                "d2h_bytes_per_step": 6 * 8 * npart + e2e_turns * cfg.nbunch * 12 * 8,
+                "turns_per_step": e2e_turns, "steps": args.e2e_steps,
+                "call": "mbt_track (pinned host beam in, %d turns, stats + beam out)" % e2e_turns},
+        "gpu_launches": 4 * args.steps,
+        "clocks": clk.summary(),
+        "finite": ok,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line))
+
+
+def run_reference(args):
+    import numpy as np
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    import tempfile
+    tmp = tempfile.mkdtemp()
+    turns = args.warmup + args.steps
+    per_turn, info = cpu_run(args.workload, turns, tmp)
+    timed = per_turn[args.warmup:]
+    t = float(np.sum(timed))
+    value = info["particles"] * len(timed) / t
+    _, _, desc = WORKLOADS[args.workload]
+    sample = ("%d warm-up + %d timed turns of the whole ring (%d bunches) split over %d processes, "
+              "one per core; time per turn = slowest process" % (args.warmup, args.steps, info["bunches"],
+                                                                 info["cores"]))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3 / len(timed),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": desc, "bunches": info["bunches"], "macroparticles": info["particles"],
+                   "turns_per_step": 1, "parallelism": "%d host processes" % info["cores"]},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": info["cores"], "kind": info["kind"],
+                         "sample": sample},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="uniform")
+    ap.add_argument("--profile-turns", type=int, default=20)
+    ap.add_argument("--e2e-turns", type=int, default=100)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-turns", type=int, default=4)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

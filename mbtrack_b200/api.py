@@ -156,8 +156,10 @@ class Tracker:
             pass
 
     def load_particles(self, ib, soa6):
-        a = np.ascontiguousarray(soa6, dtype=np.float64)
-        _check(lib().mbt_load_particles(self.h, ib, _ptr(a), int(self.np[ib])), self.h)
+        a = np.ascontiguousarray(soa6, dtype=np.float64).ravel()
+        if a.size % 6:
+            raise ValueError("a soa6 buffer holds 6 arrays of equal length")
+        _check(lib().mbt_load_particles(self.h, ib, _ptr(a), a.size // 6), self.h)
 
     def load_all(self, soa6_all):
         a = np.ascontiguousarray(soa6_all, dtype=np.float64)
@@ -183,7 +185,11 @@ class Tracker:
         return s.reshape(self.nb, 12)
 
     def set_deviates(self, dev, nturns):
-        d = np.ascontiguousarray(dev, dtype=np.float32)
+        d = np.ascontiguousarray(dev, dtype=np.float32).ravel()
+        per = 1 + 2 * (self.params.track_plane[2] != 0) + 2 * (self.params.track_plane[1] != 0)
+        if d.size < nturns * per * int(self.np.sum()):
+            raise ValueError("%d deviates given, %d turns need %d"
+                             % (d.size, nturns, nturns * per * int(self.np.sum())))
         _check(lib().mbt_set_deviates(self.h, _ptr(d), nturns), self.h)
 
     def run(self, nturns, stats=True):
@@ -192,6 +198,11 @@ class Tracker:
         return None if s is None else s.reshape(nturns, self.nb, 12)
 
     def track(self, particles, nturns, stats=None):
+        if particles.dtype != np.float64 or not particles.flags.c_contiguous or \
+                particles.size != 6 * int(self.np.sum()):
+            raise ValueError("particles must be a contiguous float64 buffer of 6 * sum(np)")
+        if stats is not None and (stats.dtype != np.float64 or stats.size < nturns * self.nb * 12):
+            raise ValueError("stats must hold nturns * nbunch * 12 doubles")
         _check(lib().mbt_track(self.h, _ptr(particles), nturns, _ptr(stats)), self.h)
 
     def profile(self, nturns):

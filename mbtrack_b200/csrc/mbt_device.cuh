@@ -73,6 +73,9 @@ struct RingState {
   int error;           // sticky device error word (0 = ok)
   int trash_low, trash_high;
   double phasor[3][kMaxLr][2];
+  // values of the last completed turn (what the reference holds after it)
+  double Vrf0_last, phai0_last;
+  double phasor_last[3][kMaxLr][2];
 };
 
 // Per long-range resonator constants (construct_wake_phasor
@@ -91,6 +94,7 @@ struct LrConst {
 struct Args {
   // geometry
   int nbunch, ntile, npad, tile, prec, ncell, nharm;
+  int hoff;                   // offset of the extras in a partial record: (hist_xz ? 3 : 1) * ncell
   // particles
   double *coord;
   const Tile *tiles;
@@ -130,6 +134,7 @@ struct Args {
   // resistive wall
   int rw_long, Nmlt;
   double *dipole;             // (Nmlt+2) nharm x 2
+  double *rw_e;               // 2 x (Nmlt+2) nharm: dipole x bucket current [mA], planar
   const double *rw_rsq;       // (Nmlt+1) nharm + 1: 1 / sqrt(m T0 / h)
   double rw_const[2][2];      // [trigger halved?][plane-1]
   int triggerRW;

@@ -56,6 +56,44 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
+// Complex affine map V -> V M + A; compose(f, g) applies f then g.
+struct Aff {
+  double m0, m1, a0, a1;
+};
+
+__device__ __forceinline__ Aff aff_id() { return Aff{1.0, 0.0, 0.0, 0.0}; }
+
+__device__ __forceinline__ Aff compose(const Aff &f, const Aff &g) {
+  Aff r;
+  r.m0 = f.m0 * g.m0 - f.m1 * g.m1;
+  r.m1 = f.m0 * g.m1 + f.m1 * g.m0;
+  r.a0 = (f.a0 * g.m0 - f.a1 * g.m1) + g.a0;
+  r.a1 = (f.a0 * g.m1 + f.a1 * g.m0) + g.a1;
+  return r;
+}
+
+__device__ __forceinline__ Aff shfl_up(const Aff &x, int o) {
+  Aff y;
+  y.m0 = __shfl_up_sync(0xffffffffu, x.m0, o);
+  y.m1 = __shfl_up_sync(0xffffffffu, x.m1, o);
+  y.a0 = __shfl_up_sync(0xffffffffu, x.a0, o);
+  y.a1 = __shfl_up_sync(0xffffffffu, x.a1, o);
+  return y;
+}
+
+// Exclusive scan of affine maps over the lanes of a warp (lane order =
+// application order).
+__device__ __forceinline__ Aff warp_exclusive_scan(Aff x, int lane) {
+  Aff inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const Aff y = shfl_up(inc, o);
+    if (lane >= o) inc = compose(y, inc);
+  }
+  Aff ex = shfl_up(inc, 1);
+  return lane == 0 ? aff_id() : ex;
+}
+
 // ---------------------------------------------------------------- K1
 
 template <bool MOVE, int NOISE, bool HISTXZ>
@@ -243,12 +281,14 @@ __global__ void __launch_bounds__(kBlock) turn_map(Args a) {
   if (threadIdx.x < kPartialExtra) {
     double s = 0.0;
     for (int w = 0; w < kBlock / 32; ++w) s += red[w][threadIdx.x];
-    rec[3 * nc + threadIdx.x] = s;
+    rec[a.hoff + threadIdx.x] = s;
   }
   for (int i = threadIdx.x; i < nc; i += kBlock) {
     rec[i] = (double)hc[i];
-    rec[nc + i] = HISTXZ ? hx[i] : 0.0;
-    rec[2 * nc + i] = HISTXZ ? hz[i] : 0.0;
+    if (HISTXZ) {
+      rec[nc + i] = hx[i];
+      rec[2 * nc + i] = hz[i];
+    }
   }
 }
 
@@ -266,7 +306,7 @@ __global__ void __launch_bounds__(kBlock) bunch_reduce(Args a, int mode, double 
     tot[e] = s;
   }
   __syncthreads();
-  const double *ex = tot + 3 * nc;
+  const double *ex = tot + a.hoff;
   const double N = (double)a.bunch_np[b];
   const int kb = a.bunch_kb[b];
   const long turn = a.rs->turn;
@@ -276,7 +316,8 @@ __global__ void __launch_bounds__(kBlock) bunch_reduce(Args a, int mode, double 
   double *H = a.hist + (size_t)b * 6 * nc;
   if (a.selffield) {
     for (int j = threadIdx.x; j < nc; j += kBlock) {
-      const double cn = tot[j], sx = tot[nc + j], sz = tot[2 * nc + j];
+      const double cn = tot[j];
+      const double sx = a.hist_xz ? tot[nc + j] : 0.0, sz = a.hist_xz ? tot[2 * nc + j] : 0.0;
       double f = cn, dv = sz, dh = sx;
       if (j == 0) { f += ex[kTrLowN]; dv += ex[kTrLowZ]; dh += ex[kTrLowX]; }
       if (j == nc - 1) { f += ex[kTrHighN]; dv += ex[kTrHighZ]; dh += ex[kTrHighX]; }
@@ -320,38 +361,55 @@ __global__ void __launch_bounds__(kBlock) bunch_reduce(Args a, int mode, double 
   // fill :203-219)
   if (a.rw_long && threadIdx.x == 0) {
     const long n = (long)(a.Nmlt + 2) * a.nharm;
+    const double ibk = a.ibunch[kb];
     if (mode == kReduceTurn) {
-      double *mom = a.dipole + 2 * cyc_slot(-turn * a.nharm + kb, n);
-      mom[0] = mean6[1];
-      mom[1] = mean6[2];
+      const long sl = cyc_slot(-turn * a.nharm + kb, n);
+      a.dipole[2 * sl] = mean6[1];
+      a.dipole[2 * sl + 1] = mean6[2];
+      a.rw_e[sl] = mean6[1] * ibk;
+      a.rw_e[n + sl] = mean6[2] * ibk;
     } else {
       const int jmax = a.Nmlt > 1 ? a.Nmlt : 1;
       for (int j = 0; j < jmax; ++j) {
-        double *mom = a.dipole + 2 * cyc_slot((long)j * a.nharm + kb, n);
-        mom[0] = mean6[1];
-        mom[1] = mean6[2];
+        const long sl = cyc_slot((long)j * a.nharm + kb, n);
+        a.dipole[2 * sl] = mean6[1];
+        a.dipole[2 * sl + 1] = mean6[2];
+        a.rw_e[sl] = mean6[1] * ibk;
+        a.rw_e[n + sl] = mean6[2] * ibk;
       }
     }
   }
   // in-bucket phasor of each long-range resonator, starting from zero:
-  // V_j = V_{j-1} prog - Ib fnp_j fac  (transform_weak.c:1017-1018)
-  if (a.selffield && threadIdx.x < a.nlr) {
-    const int r = threadIdx.x;
-    const LrConst L = a.lr[r];
-    const double *src = H + (size_t)(3 + L.plane) * nc;   // dropped histogram of the plane
-    const double fac = a.bunch_fac[(size_t)r * a.nbunch + b];
+  // V_j = V_{j-1} prog - Ib fnp_j fac  (transform_weak.c:1017-1018), as a
+  // warp scan of affine maps over the bins, one warp per resonator
+  if (a.selffield) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int chunk = (nc + 31) / 32;
+    const int j0 = min(lane * chunk, nc), j1 = min(j0 + chunk, nc);
     const double ib = a.ibunch[kb];
-    double *u = a.lr_u + ((size_t)r * a.nbunch + b) * nc * 2;
-    double *bb = a.lr_b + ((size_t)r * a.nbunch + b) * nc;
-    double v0 = 0.0, v1 = 0.0;
-    for (int j = 0; j < nc; ++j) {
-      const double s = ib * src[j] * fac;
-      const double n0 = (v0 * L.prog[0] - v1 * L.prog[1]) - s;
-      const double n1 = (v0 * L.prog[1] + v1 * L.prog[0]);
-      v0 = n0; v1 = n1;
-      u[2 * j] = v0;
-      u[2 * j + 1] = v1;
-      bb[j] = s;
+    for (int r = warp; r < a.nlr; r += kBlock / 32) {
+      const LrConst &L = a.lr[r];
+      const double *src = H + (size_t)(3 + L.plane) * nc;   // dropped histogram of the plane
+      const double fac = a.bunch_fac[(size_t)r * a.nbunch + b];
+      double *u = a.lr_u + ((size_t)r * a.nbunch + b) * nc * 2;
+      double *bb = a.lr_b + ((size_t)r * a.nbunch + b) * nc;
+      Aff f = aff_id();
+      for (int j = j0; j < j1; ++j) {
+        const Aff g{L.prog[0], L.prog[1], -(ib * src[j] * fac), 0.0};
+        f = compose(f, g);
+      }
+      const Aff ex = warp_exclusive_scan(f, lane);
+      double v0 = ex.a0, v1 = ex.a1;
+      for (int j = j0; j < j1; ++j) {
+        const double s = ib * src[j] * fac;
+        const double n0 = (v0 * L.prog[0] - v1 * L.prog[1]) - s;
+        const double n1 = (v0 * L.prog[1] + v1 * L.prog[0]);
+        v0 = n0;
+        v1 = n1;
+        u[2 * j] = v0;
+        u[2 * j + 1] = v1;
+        bb[j] = s;
+      }
     }
   }
 }
@@ -364,50 +422,95 @@ __device__ __forceinline__ void rffb_store(Args &a, int slot, double vr, double 
   a.rffb_hist[2 * slot + 1] = atan2(vr, vi);
 }
 
-// passes: number of turns of phasor propagation; init: wake_phasor_init
-// semantics (V starts at 0); advance: bump the turn counter afterwards.
-// vbuf: scratch of 2 x nharm complex values (before/after each bucket).
+// The phasor of each long-range resonator around the ring, bucket h-1 .. 0
+// (one pass per turn; `passes` turns for wake_phasor_init), as a warp scan
+// of affine maps: a filled bucket maps V to (V prog^ncell + U_last) G_gap,
+// an empty one to V G_empty (transform_weak.c:1006-1044, :911-947).
+// init: wake_phasor_init semantics (start from 0, no snapshot);
+// advance: bump the turn counter afterwards.
+// vbuf: 4 x nharm doubles, the phasor before/after each bucket.
 __global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init, int advance,
                                                     double *vbuf) {
   RingState *rs = a.rs;
   const int h = a.nharm;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __shared__ int fb_live;
-  if (threadIdx.x == 0) fb_live = rs->rffb_on;
+  if (threadIdx.x == 0) {
+    fb_live = rs->rffb_on;
+    if (!init) {
+      rs->Vrf0_last = rs->Vrf0;
+      rs->phai0_last = rs->phai0;
+      for (int pl = 0; pl < 3; ++pl)
+        for (int l = 0; l < kMaxLr; ++l) {
+          rs->phasor_last[pl][l][0] = rs->phasor[pl][l][0];
+          rs->phasor_last[pl][l][1] = rs->phasor[pl][l][1];
+        }
+    }
+  }
   __syncthreads();
+  const int chunk = (h + 31) / 32;
+  const int m0 = min(lane * chunk, h), m1 = min(m0 + chunk, h);
   for (int r = 0; r < a.nlr; ++r) {
-    const LrConst L = a.lr[r];
+    const LrConst &L = a.lr[r];
     const bool fb = L.fb && fb_live;
-    double v0, v1;
-    if (init) { v0 = 0.0; v1 = 0.0; } else { v0 = rs->phasor[L.plane][L.l][0]; v1 = rs->phasor[L.plane][L.l][1]; }
+    const double G0 = L.gap[0] * L.gap[1], G1 = L.gap[0] * L.gap[2];
+    const double E0 = L.emp[0] * L.emp[1], E1 = L.emp[0] * L.emp[2];
+    const double PG0 = L.pn[0] * G0 - L.pn[1] * G1, PG1 = L.pn[0] * G1 + L.pn[1] * G0;
+    double V0 = init ? 0.0 : rs->phasor[L.plane][L.l][0];
+    double V1 = init ? 0.0 : rs->phasor[L.plane][L.l][1];
     for (int pass = 0; pass < passes; ++pass) {
-      if (threadIdx.x == 0) {
-        double *vs = a.lr_vs + (size_t)r * h * 2;
-        for (int m = 0; m < h; ++m) {
-          const int i = h - m - 1;
-          if (fb) { vbuf[4 * m] = v0; vbuf[4 * m + 1] = v1; }
-          vs[2 * i] = v0;
-          vs[2 * i + 1] = v1;
-          const int bi = a.bucket_bunch[i];
+      if (warp == 0) {
+        Aff f = aff_id();
+        for (int m = m0; m < m1; ++m) {
+          const int bi = a.bucket_bunch[h - m - 1];
+          Aff g;
           if (bi >= 0) {
             const double *u = a.lr_u + ((size_t)r * a.nbunch + bi) * a.ncell * 2 + 2 * (a.ncell - 1);
-            const double n0 = (v0 * L.pn[0] - v1 * L.pn[1]) + u[0];
-            const double n1 = (v0 * L.pn[1] + v1 * L.pn[0]) + u[1];
-            v0 = (n0 * L.gap[0] * L.gap[1] - n1 * L.gap[0] * L.gap[2]);
-            v1 = (n0 * L.gap[0] * L.gap[2] + n1 * L.gap[0] * L.gap[1]);
+            g = Aff{PG0, PG1, u[0] * G0 - u[1] * G1, u[0] * G1 + u[1] * G0};
           } else {
-            const double n0 = v0, n1 = v1;
-            v0 = (n0 * L.emp[0] * L.emp[1] - n1 * L.emp[0] * L.emp[2]);
-            v1 = (n0 * L.emp[0] * L.emp[2] + n1 * L.emp[0] * L.emp[1]);
+            g = Aff{E0, E1, 0.0, 0.0};
           }
+          f = compose(f, g);
+        }
+        const Aff ex = warp_exclusive_scan(f, lane);
+        double v0 = V0 * ex.m0 - V1 * ex.m1 + ex.a0;
+        double v1 = V0 * ex.m1 + V1 * ex.m0 + ex.a1;
+        double *vs = a.lr_vs + (size_t)r * h * 2;
+        for (int m = m0; m < m1; ++m) {
+          const int i = h - m - 1;
+          const int bi = a.bucket_bunch[i];
+          vs[2 * i] = v0;
+          vs[2 * i + 1] = v1;
+          if (fb) { vbuf[4 * m] = v0; vbuf[4 * m + 1] = v1; }
+          double n0, n1;
+          if (bi >= 0) {
+            const double *u = a.lr_u + ((size_t)r * a.nbunch + bi) * a.ncell * 2 + 2 * (a.ncell - 1);
+            const double w0 = (v0 * L.pn[0] - v1 * L.pn[1]) + u[0];
+            const double w1 = (v0 * L.pn[1] + v1 * L.pn[0]) + u[1];
+            n0 = w0 * G0 - w1 * G1;
+            n1 = w0 * G1 + w1 * G0;
+          } else {
+            n0 = v0 * E0 - v1 * E1;
+            n1 = v0 * E1 + v1 * E0;
+          }
+          v0 = n0;
+          v1 = n1;
           if (fb) { vbuf[4 * m + 2] = v0; vbuf[4 * m + 3] = v1; }
         }
-        rs->phasor[L.plane][L.l][0] = v0;
-        rs->phasor[L.plane][L.l][1] = v1;
+        // the phasor after the last bucket sits in the lane holding m = h-1
+        const int last = (h - 1) / chunk;
+        V0 = __shfl_sync(0xffffffffu, v0, last);
+        V1 = __shfl_sync(0xffffffffu, v1, last);
+        if (lane == 0) {
+          rs->phasor[L.plane][L.l][0] = V0;
+          rs->phasor[L.plane][L.l][1] = V1;
+        }
       }
       __syncthreads();
       if (fb) {
         // samples s = 2m (before bucket h-1-m, rotated to the beam) and
-        // s = 2m+1 (after it); only the last len samples survive.
+        // s = 2m+1 (after it, rotated to the next bunch); only the last
+        // len samples survive in the cyclic history (feedback_rf.c:5-12)
         const int ns = 2 * h, len = a.rffb_len;
         const int count0 = rs->rffb_count;
         const int first = ns > len ? ns - len : 0;
@@ -423,7 +526,6 @@ __global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init
         if (threadIdx.x == 0) rs->rffb_count = count0 + ns;
         __syncthreads();
       }
-      __syncthreads();
     }
   }
   // RF-feedback correction (worker_weakweak.c:149-162, 268-278)
@@ -433,7 +535,7 @@ __global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init
     for (int m = threadIdx.x; m < a.rffb_len; m += kBlock) { s0 += a.rffb_hist[2 * m]; s1 += a.rffb_hist[2 * m + 1]; }
     s0 = warp_sum(s0);
     s1 = warp_sum(s1);
-    if ((threadIdx.x & 31) == 0) { sv[threadIdx.x >> 5][0] = s0; sv[threadIdx.x >> 5][1] = s1; }
+    if (lane == 0) { sv[warp][0] = s0; sv[warp][1] = s1; }
     __syncthreads();
     if (threadIdx.x == 0) {
       double vs = 0.0, ps = 0.0;
@@ -537,37 +639,40 @@ __global__ void __launch_bounds__(kBlock) bunch_wakes(Args a, int with_rw) {
     }
   }
   // long-range resistive wall (transform_weak.c:779-833) of the turn just
-  // completed; applied at the start of the next particle pass
+  // completed; applied at the start of the next particle pass.  The sum
+  // over m = 1 .. (Nmlt+1) h runs over consecutive slots of the dipole
+  // history (one wrap at most), each already multiplied by its bucket's
+  // current; empty buckets hold 0.
   if (a.rw_long) {
     const long turn = a.rs->turn - 1;
     const int mtrig = a.rs->rw_m - 1;
     const int h = a.nharm;
-    const long n = (long)(a.Nmlt + 2) * h;
-    const long bpos = -turn * h + kb;
+    const int n = (a.Nmlt + 2) * h;
     const int M = (a.Nmlt + 1) * h;
-    for (int pl = 1; pl <= 2; ++pl) {
-      const bool tracked = (pl == 1) ? a.oc.track_h : a.oc.track_v;
-      double s = 0.0;
-      if (with_rw && tracked) {
-        for (int m = 1 + threadIdx.x; m <= M; m += kBlock) {
-          const int k = (int)(bpos + m);
-          const int in_mod = k < 0 ? (k % h + h) % h : k % h;
-          if (a.bucket_bunch[in_mod] >= 0) {
-            const double *mom = a.dipole + 2 * cyc_slot(k, n);
-            s += mom[pl - 1] * a.ibunch[in_mod] * a.rw_rsq[m];
-          }
-        }
+    const int base = (int)cyc_slot(-turn * h + kb + 1, n);
+    const bool th = with_rw && a.oc.track_h, tv = with_rw && a.oc.track_v;
+    double s0 = 0.0, s1 = 0.0;
+    if (th || tv) {
+      const double *E0 = a.rw_e, *E1 = a.rw_e + n;
+      for (int j = threadIdx.x; j < M; j += kBlock) {
+        int idx = base + j;
+        idx -= (idx >= n) ? n : 0;
+        const double w = a.rw_rsq[j + 1];
+        s0 += E0[idx] * w;
+        s1 += E1[idx] * w;
       }
-      s = warp_sum(s);
-      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][pl - 1] = s;
     }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5][0] = s0; red[threadIdx.x >> 5][1] = s1; }
     __syncthreads();
     if (threadIdx.x < 2) {
       const int pl = threadIdx.x + 1;
       double s = 0.0;
       for (int w = 0; w < kBlock / 32; ++w) s += red[w][pl - 1];
       const int trig = (a.triggerRW && mtrig < 50) ? 1 : 0;
-      a.rwkick[b * 2 + (pl - 1)] = with_rw ? s * a.rw_const[trig][pl - 1] : 0.0;
+      const bool on = (pl == 1) ? th : tv;
+      a.rwkick[b * 2 + (pl - 1)] = on ? s * a.rw_const[trig][pl - 1] : 0.0;
     }
   }
 }

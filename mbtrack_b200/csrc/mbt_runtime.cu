@@ -54,8 +54,6 @@ struct mbt_ctx {
   double *vbuf = nullptr;
   double *stats_init = nullptr;
   double *xfer = nullptr;        // device staging for exports
-  double *pinned = nullptr;      // host staging
-  size_t pinned_bytes = 0;
   cudaEvent_t ev[6] = {};
   double timing[4] = {0, 0, 0, 0};
   int device = 0;
@@ -197,16 +195,6 @@ int sync_and_check(mbt_ctx *c) {
   return 0;
 }
 
-int ensure_pinned(mbt_ctx *c, size_t bytes) {
-  if (c->pinned_bytes >= bytes) return 0;
-  if (c->pinned) cudaFreeHost(c->pinned);
-  c->pinned = nullptr;
-  c->pinned_bytes = 0;
-  CK(cudaMallocHost((void **)&c->pinned, bytes));
-  c->pinned_bytes = bytes;
-  return 0;
-}
-
 int build_graph(mbt_ctx *c, int turns) {
   if (c->graph && c->graph_turns == turns) return 0;
   if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
@@ -273,20 +261,20 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   for (int b = 0; b < nbunch; ++b) {
     c->off[b] = (int)pos;
     c->tile0[b] = (int)c->tiles.size();
-    int nt = 0;
-    for (int s = 0; s < c->np[b]; s += c->tile) {
-      Tile t{b, (int)(pos + s), std::min(c->tile, c->np[b] - s), 0};
+    // ceil(np / tile) tiles of equal size (a multiple of 32 particles)
+    const int nt = (c->np[b] + c->tile - 1) / c->tile;
+    const int per = ((c->np[b] + nt - 1) / nt + 31) / 32 * 32;
+    for (int s = 0; s < c->np[b]; s += per) {
+      Tile t{b, (int)(pos + s), std::min(per, c->np[b] - s), 0};
       c->tiles.push_back(t);
-      ++nt;
     }
-    c->ntiles[b] = nt;
+    c->ntiles[b] = (int)c->tiles.size() - c->tile0[b];
     pos += (c->np[b] + 31) / 32 * 32;
   }
   if (pos > 0x7fffffffL / 6) return bail(fail(nullptr, MBT_ERR_INVALID, "beam too large for one context"));
   c->npad = (int)pos;
   c->ntile = (int)c->tiles.size();
   c->nc = std::max(p->ncell, 1);
-  c->prec = 3 * c->nc + mbt::kPartialExtra;
   c->bucket_bunch.assign(p->nharm, -1);
   for (int b = 0; b < nbunch; ++b) c->bucket_bunch[c->bucket[b]] = b;
 
@@ -295,13 +283,16 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   a.ntile = c->ntile;
   a.npad = c->npad;
   a.tile = c->tile;
-  a.prec = c->prec;
   a.ncell = c->nc;
   a.nharm = p->nharm;
   const int lr_tot = p->n_lr[0] + p->n_lr[1] + p->n_lr[2];
   a.selffield = (p->ncell > 0 && p->planeL + p->planeV + p->planeH + lr_tot > 0) ? 1 : 0;
   c->histxz = a.selffield && (p->planeV > 0 || p->planeH > 0 || p->n_lr[1] > 0 || p->n_lr[2] > 0);
   a.hist_xz = c->histxz;
+  // partial record: counts [, sum x, sum z], then the extras
+  a.hoff = (c->histxz ? 3 : 1) * c->nc;
+  c->prec = a.hoff + mbt::kPartialExtra;
+  a.prec = c->prec;
   a.lr_kick[0] = (p->n_lr[0] + p->planeL) > 0;
   a.lr_kick[1] = p->planeH > 0;
   a.lr_kick[2] = p->planeV > 0;
@@ -461,6 +452,7 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   rc = rc ? rc : dupload(c, &dp, pw.empty() ? g0.data() : pw.data(), std::max<size_t>(pw.size(), 1)); a.lr_pw = dp;
   rc = rc ? rc : dalloc(c, &c->vbuf, (size_t)4 * p->nharm);
   rc = rc ? rc : dalloc(c, &a.dipole, p->rw_long ? (size_t)(p->Nmlt + 2) * p->nharm * 2 : 1);
+  rc = rc ? rc : dalloc(c, &a.rw_e, p->rw_long ? (size_t)(p->Nmlt + 2) * p->nharm * 2 : 1);
   rc = rc ? rc : dupload(c, &dp, rsq.empty() ? g0.data() : rsq.data(), std::max<size_t>(rsq.size(), 1)); a.rw_rsq = dp;
   a.rffb_len = p->rffb ? p->rffb_len : 0;
   a.rffb_off_after_init = p->rffb_off_after_init;
@@ -475,6 +467,8 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   rs.Vrf0 = p->Vrf0;
   rs.phai0 = p->phai0;
   rs.rffb_on = p->rffb;
+  rs.Vrf0_last = p->Vrf0;
+  rs.phai0_last = p->phai0;
   if (cudaMemcpy(a.rs, &rs, sizeof rs, cudaMemcpyHostToDevice) != cudaSuccess)
     return bail(fail(nullptr, MBT_ERR_CUDA, "state upload"));
   const size_t smw = smem_wakes(c);
@@ -490,7 +484,6 @@ int mbt_destroy(mbt_ctx *c) {
   if (c->graph) cudaGraphExecDestroy(c->graph);
   for (void *p : c->allocs) cudaFree(p);
   if (c->dev) cudaFree(c->dev);
-  if (c->pinned) cudaFreeHost(c->pinned);
   for (auto &e : c->ev) if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -721,12 +714,16 @@ int mbt_get_state(mbt_ctx *c, mbt_state *st) {
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaMemcpy(&rs, c->a.rs, sizeof rs, cudaMemcpyDeviceToHost));
   memset(st, 0, sizeof *st);
+  // The device runs one ring scan ahead (it prepares the next turn's
+  // wakes and RF correction); report the values of the last completed
+  // turn, as the reference holds them after that turn.
+  const bool ahead = c->prepared != 0;
   st->turn = rs.turn;
-  st->Vrf0 = rs.Vrf0;
-  st->phai0 = rs.phai0;
+  st->Vrf0 = ahead ? rs.Vrf0_last : rs.Vrf0;
+  st->phai0 = ahead ? rs.phai0_last : rs.phai0;
   for (int pl = 0; pl < 3; ++pl)
     for (int l = 0; l < MBT_MAX_LR; ++l)
-      for (int k = 0; k < 2; ++k) st->phasor[pl][l][k] = rs.phasor[pl][l][k];
+      for (int k = 0; k < 2; ++k) st->phasor[pl][l][k] = ahead ? rs.phasor_last[pl][l][k] : rs.phasor[pl][l][k];
   st->n_trash_low = rs.trash_low;
   st->n_trash_high = rs.trash_high;
   return 0;

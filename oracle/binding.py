@@ -86,6 +86,7 @@ class Oracle:
         L.orc_trash.argtypes = [_vp, ctypes.c_int, _vp, _vp]
         L.orc_histograms.argtypes = [_vp, ctypes.c_int] + [_vp] * 6
         L.orc_destroy.argtypes = [_vp]
+        L.orc_set_range.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
         self.p = params.copy()
         self.bucket = np.ascontiguousarray(bucket, dtype=np.int32)
         self.np = np.ascontiguousarray(np_, dtype=np.int32)
@@ -102,6 +103,10 @@ class Oracle:
         if getattr(self, "h", None):
             self.lib.orc_destroy(self.h)
             self.h = None
+
+    def set_range(self, lo, hi):
+        """Track only bunches [lo, hi) (see orc_set_range)."""
+        self.lib.orc_set_range(self.h, int(lo), int(hi))
 
     def generate_beam(self):
         self.lib.orc_generate_beam(self.h)
@@ -182,7 +187,7 @@ class Reference:
 
     _count = 0
 
-    def __init__(self, conf, fix_rw_beff=True, workdir="/tmp"):
+    def __init__(self, conf, fix_rw_beff=True, workdir="/tmp", bunch_range=None):
         so = build_reference()
         if so is None:
             raise RuntimeError("reference harness unavailable")
@@ -206,6 +211,9 @@ class Reference:
         L.refh_greens.argtypes = [ctypes.c_int, _vp, _vp, _vp, _vp]
         L.refh_fill_params.argtypes = [_P(MbtParams)]
         L.refh_param_table.argtypes = [_vp, _vp, ctypes.c_int]
+        L.refh_set_range.argtypes = [ctypes.c_int, ctypes.c_int]
+        if bunch_range is not None:
+            L.refh_set_range(int(bunch_range[0]), int(bunch_range[1]))
         self.nb = L.refh_init(conf.encode(), workdir.encode(), int(fix_rw_beff))
         if self.nb <= 0:
             raise RuntimeError("refh_init failed: %d" % self.nb)

@@ -73,7 +73,16 @@ struct orc_ctx {
   const float *dev_in;
   float *dev_out;
   long dev_pos, dev_cap;
+  int lo, hi;   /* bunches tracked by this instance (orc_set_range) */
 };
+
+#define IN_RANGE(o, ib) ((ib) >= (o)->lo && (ib) < (o)->hi)
+
+void orc_set_range(orc_ctx *o, int lo, int hi)
+{
+  o->lo = lo;
+  o->hi = hi;
+}
 
 /* ---------------------------------------------------------------- RNG */
 
@@ -158,6 +167,8 @@ orc_ctx *orc_create(const mbt_params *p, int nbunch, const int *bucket,
   if (!o) return NULL;
   o->p = *p;
   o->nb = nbunch;
+  o->lo = 0;
+  o->hi = nbunch;
   o->b = (orc_bunch *) calloc(nbunch, sizeof(orc_bunch));
   o->filled = (int *) calloc(h, sizeof(int));
   o->ibunch = (double *) calloc(h, sizeof(double));
@@ -246,7 +257,7 @@ int orc_generate_beam(orc_ctx *o)
   for (i = 0; i < o->nb; i++) {
     orc_bunch *b = &o->b[i];
     for (k = 0; k < 6; k++) memset(b->c[k], 0, b->np * sizeof(double));
-    if (b->np == 0) continue;
+    if (b->np == 0 || !IN_RANGE(o, i)) continue;
     if (b->np == 1) {
       b->c[0][0] = p->pos_offset[LON]; b->c[3][0] = p->slope_offset[LON];
       if (p->track_plane[HOR]) { b->c[1][0] = p->pos_offset[HOR]; b->c[4][0] = p->slope_offset[HOR]; }
@@ -687,16 +698,18 @@ int orc_prepare(orc_ctx *o, double *init_stats)
   const mbt_params *p = &o->p;
   int ib, i, j, pl;
   for (ib = 0; ib < o->nb; ib++) {
+    if (!IN_RANGE(o, ib)) continue;
     calc_stats(o, &o->b[ib]);
     if (init_stats) memcpy(init_stats + 12 * ib, o->b[ib].stats, 12 * sizeof(double));
   }
   if (p->n_lr[LON] > 0) {
     for (ib = 0; ib < o->nb; ib++) {
       o->b[ib].rffb_count = 0;   /* rffb_init feedback_rf.c:14-19 */
-      ring_hist(o, &o->b[ib], LON);
+      if (IN_RANGE(o, ib)) ring_hist(o, &o->b[ib], LON);
     }
     for (ib = 0; ib < o->nb; ib++) {
       orc_bunch *b = &o->b[ib];
+      if (!IN_RANGE(o, ib)) continue;
       wake_phasor_init(o, b, LON);
       if (b->rffb_on) {
         rffb_correct(p, b);
@@ -706,13 +719,14 @@ int orc_prepare(orc_ctx *o, double *init_stats)
   }
   for (pl = HOR; pl <= VER; pl++) {
     if (p->track_plane[pl] && p->n_lr[pl] > 0) {
-      for (ib = 0; ib < o->nb; ib++) ring_hist(o, &o->b[ib], pl);
-      for (ib = 0; ib < o->nb; ib++) wake_phasor_init(o, &o->b[ib], pl);
+      for (ib = 0; ib < o->nb; ib++) if (IN_RANGE(o, ib)) ring_hist(o, &o->b[ib], pl);
+      for (ib = 0; ib < o->nb; ib++) if (IN_RANGE(o, ib)) wake_phasor_init(o, &o->b[ib], pl);
     }
   }
   if (p->rw_long) {
     for (ib = 0; ib < o->nb; ib++) {
       double *d = cyc(o, o->b[ib].kb);
+      if (!IN_RANGE(o, ib)) continue;
       d[0] = o->b[ib].stats[0 + HOR];
       d[1] = o->b[ib].stats[0 + VER];
     }
@@ -754,22 +768,23 @@ long orc_run(orc_ctx *o, long nturns, double *stats, const float *dev_in,
   for (t = 0; t < nturns; t++) {
     long rev = o->rev + t;
     if (p->ncell > 0 && p->planeL + p->planeV + p->planeH + lr_tot > 0)
-      for (ib = 0; ib < o->nb; ib++) selffield(o, &o->b[ib]);
-    for (ib = 0; ib < o->nb; ib++)
+      for (ib = o->lo; ib < o->hi && ib < o->nb; ib++) selffield(o, &o->b[ib]);
+    for (ib = o->lo; ib < o->hi && ib < o->nb; ib++)
       if (o->b[ib].rffb_on) rffb_correct(p, &o->b[ib]);
     for (ib = 0; ib < o->nb; ib++) {
       orc_bunch *b = &o->b[ib];
+      if (!IN_RANGE(o, ib)) continue;
       optic(o, b, p->iseed[LON] + b->kb + (int) rev);
       calc_stats(o, b);
       if (stats) memcpy(stats + (t * o->nb + ib) * 12, b->stats, 12 * sizeof(double));
     }
     if (p->rw_long) {
-      for (ib = 0; ib < o->nb; ib++) {
+      for (ib = o->lo; ib < o->hi && ib < o->nb; ib++) {
         double *mom = cyc(o, -rev * p->nharm + o->b[ib].kb);
         mom[0] = o->b[ib].stats[0 + HOR];
         mom[1] = o->b[ib].stats[0 + VER];
       }
-      for (ib = 0; ib < o->nb; ib++) {
+      for (ib = o->lo; ib < o->hi && ib < o->nb; ib++) {
         orc_bunch *b = &o->b[ib];
         const long bpos = -rev * p->nharm + b->kb;
         if (p->track_plane[HOR]) rw_kick(o, b, bpos, HOR);
@@ -777,7 +792,7 @@ long orc_run(orc_ctx *o, long nturns, double *stats, const float *dev_in,
         b->m++;
       }
     }
-    for (ib = 0; ib < o->nb; ib++) {
+    for (ib = o->lo; ib < o->hi && ib < o->nb; ib++) {
       if (p->n_lr[LON] > 0) ring_hist(o, &o->b[ib], LON);
       if (p->n_lr[HOR] > 0 && p->track_plane[HOR]) ring_hist(o, &o->b[ib], HOR);
       if (p->n_lr[VER] > 0 && p->track_plane[VER]) ring_hist(o, &o->b[ib], VER);

@@ -31,6 +31,11 @@ orc_ctx *orc_create(const mbt_params *p, int nbunch, const int *bucket,
                     const double *Gv, const double *Gh);
 void orc_destroy(orc_ctx *o);
 
+/* Track only bunches [lo, hi): the others keep zero histograms and
+ * dipoles, so the ring-wide phasor and resistive-wall sums still cost what
+ * a full worker pays (used to split the CPU baseline over host cores). */
+void orc_set_range(orc_ctx *o, int lo, int hi);
+
 /* Matched Gaussian of the reference (weak_generate_bunch_distribution,
  * bunch_weak.c:173-292, c_fnorm bunch.c:379-405) with each bunch's own
  * glibc random() state, as each MPI worker process has. */

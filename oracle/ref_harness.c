@@ -94,6 +94,14 @@ static long rev_done = 0;
 static int lr_res_sizetot = 0;
 static int exact_deviates = 1;
 static char conf_copy[FILENAME_MAX];
+/* Bunches [range_lo, range_hi) are generated, set up and tracked; the
+   others keep zero histograms and dipoles, so a process that tracks a
+   share of the ring still does the ring-wide phasor and RW work of a full
+   MPI worker (used to split the CPU baseline over host cores). */
+static int range_lo = 0, range_hi = 1 << 30;
+
+void refh_set_range(int lo, int hi) { range_lo = lo; range_hi = hi; }
+#define IN_RANGE(ib) ((ib) >= range_lo && (ib) < range_hi)
 
 static void rw_beff_fix(const char *conf)
 {
@@ -176,9 +184,9 @@ int refh_init(const char *conf, const char *workdir, int fix_rw_beff)
     w->sf = sf_model;
     w->scan_val = track.scan_start;
     /* worker_weakweak.c:75-79 */
-    if (!weak_bunch_create(&w->bunch, &track, macrop_model.Np, Ib, w->kb, true))
+    if (!weak_bunch_create(&w->bunch, &track, IN_RANGE(ib) ? macrop_model.Np : 0, Ib, w->kb, true))
       return -4;
-    if (!weak_generate_bunch_distribution(&w->bunch, w->model, track.TrackPlane))
+    if (IN_RANGE(ib) && !weak_generate_bunch_distribution(&w->bunch, w->model, track.TrackPlane))
       return -5;
     w->iseed = macrop_model.iseed[LON] + w->kb;
     int pl;
@@ -278,6 +286,7 @@ int refh_prepare(double *init_stats)
   for (ib = 0; ib < nbunch; ib++) {
     worker_t *w = &W[ib];
     if (!selffield_model_init(&w->sf, w->model.pos_sgm.xtau, &w->bunch)) return -1;
+    if (!IN_RANGE(ib)) continue;
     if (w->ring.resonators_size > 0) construct_greensfunc_resonator(&w->sf, &w->ring);
     if (w->ring.wakefiles_size > 0) construct_greensfunc_file(&w->sf, &w->ring);
     if (track.EnableRW_short || track.EnableRW_short_LON) construct_greensfunc_RW(&w->sf, &w->ring);
@@ -296,10 +305,11 @@ int refh_prepare(double *init_stats)
         }
         rffb_init(w->ring.rf_feedback);
       }
-      fnp_ring_update(&w->ring, fnp_ring, &w->sf, &w->bunch, w->kb, LON);
+      if (IN_RANGE(ib)) fnp_ring_update(&w->ring, fnp_ring, &w->sf, &w->bunch, w->kb, LON);
     }
     for (ib = 0; ib < nbunch; ib++) {
       worker_t *w = &W[ib];
+      if (!IN_RANGE(ib)) continue;
       wake_phasor_init(&w->ring, fnp_ring, &w->sf, &w->bunch, w->kb, w->phasor_end[LON], &ebeam, LON);
       if (w->ring.has_rf_feedback) {
         double vmbar, phibar;
@@ -315,16 +325,16 @@ int refh_prepare(double *init_stats)
   if (track.TrackPlane[HOR] && ring.longrange_resonators_size[HOR] > 0) {
     fnp_hor = (double *) calloc((size_t) Nbin * ring.Nharm, sizeof(double));
     for (ib = 0; ib < nbunch; ib++)
-      fnp_ring_update(&W[ib].ring, fnp_hor, &W[ib].sf, &W[ib].bunch, W[ib].kb, HOR);
+      if (IN_RANGE(ib)) fnp_ring_update(&W[ib].ring, fnp_hor, &W[ib].sf, &W[ib].bunch, W[ib].kb, HOR);
     for (ib = 0; ib < nbunch; ib++)
-      wake_phasor_init(&W[ib].ring, fnp_hor, &W[ib].sf, &W[ib].bunch, W[ib].kb, W[ib].phasor_end[HOR], &ebeam, HOR);
+      if (IN_RANGE(ib)) wake_phasor_init(&W[ib].ring, fnp_hor, &W[ib].sf, &W[ib].bunch, W[ib].kb, W[ib].phasor_end[HOR], &ebeam, HOR);
   }
   if (track.TrackPlane[VER] && ring.longrange_resonators_size[VER] > 0) {
     fnp_ver = (double *) calloc((size_t) Nbin * ring.Nharm, sizeof(double));
     for (ib = 0; ib < nbunch; ib++)
-      fnp_ring_update(&W[ib].ring, fnp_ver, &W[ib].sf, &W[ib].bunch, W[ib].kb, VER);
+      if (IN_RANGE(ib)) fnp_ring_update(&W[ib].ring, fnp_ver, &W[ib].sf, &W[ib].bunch, W[ib].kb, VER);
     for (ib = 0; ib < nbunch; ib++)
-      wake_phasor_init(&W[ib].ring, fnp_ver, &W[ib].sf, &W[ib].bunch, W[ib].kb, W[ib].phasor_end[VER], &ebeam, VER);
+      if (IN_RANGE(ib)) wake_phasor_init(&W[ib].ring, fnp_ver, &W[ib].sf, &W[ib].bunch, W[ib].kb, W[ib].phasor_end[VER], &ebeam, VER);
   }
 
   if (track.EnableRW_long > 0) {
@@ -359,6 +369,7 @@ int refh_run(long nturns, double *stats, float *dev, long dev_cap)
     /* 1. self-field (+ long-range phasors) */
     for (ib = 0; ib < nbunch; ib++) {
       worker_t *w = &W[ib];
+      if (!IN_RANGE(ib)) continue;
       if (w->sf.PlaneL + w->sf.PlaneV + w->sf.PlaneH + lr_res_sizetot > 0)
         transform_weak_bunch_selffield(&w->bunch, w->sf, NULL, &w->ring, rev, devnull,
                                        w->scan_val, w->kb, &ebeam, w->phasor_end[LON],
@@ -368,6 +379,7 @@ int refh_run(long nturns, double *stats, float *dev, long dev_cap)
     /* 2. RF feedback */
     for (ib = 0; ib < nbunch; ib++) {
       worker_t *w = &W[ib];
+      if (!IN_RANGE(ib)) continue;
       if (w->ring.has_rf_feedback) {
         double vmbar, phibar;
         rffb_calc_mean_voltage_phase(w->ring.rf_feedback, &vmbar, &phibar);
@@ -380,6 +392,7 @@ int refh_run(long nturns, double *stats, float *dev, long dev_cap)
     /* 3. optics, 4. statistics */
     for (ib = 0; ib < nbunch; ib++) {
       worker_t *w = &W[ib];
+      if (!IN_RANGE(ib)) continue;
       transform_weak_bunch_optic(&w->bunch, &w->model, w->iseed + (int) rev, w->kb, &w->ring);
       weak_bunch_calc_statistics(&w->bunch, &track);
       if (stats) put_stats(&w->bunch, stats + (t * nbunch + ib) * 12);
@@ -387,6 +400,7 @@ int refh_run(long nturns, double *stats, float *dev, long dev_cap)
     /* 5. dipole history */
     if (track.EnableRW_long > 0) {
       for (ib = 0; ib < nbunch; ib++) {
+        if (!IN_RANGE(ib)) continue;
         double *mom = cyclic_array_access(-rev * ring.Nharm + W[ib].kb, &dipole_rw);
         mom[0] = W[ib].bunch.stats.pos.x;
         mom[1] = W[ib].bunch.stats.pos.z;
@@ -395,6 +409,7 @@ int refh_run(long nturns, double *stats, float *dev, long dev_cap)
       for (ib = 0; ib < nbunch; ib++) {
         worker_t *w = &W[ib];
         const int bpos = -rev * ring.Nharm + w->kb;
+        if (!IN_RANGE(ib)) continue;
         if (track.TrackPlane[HOR])
           transform_weak_bunch_RW_longrange_cyclic(w->m, bpos, &dipole_rw, HOR, &w->model, &ebeam, &w->bunch, &w->ring, &track);
         if (track.TrackPlane[VER])
@@ -405,6 +420,7 @@ int refh_run(long nturns, double *stats, float *dev, long dev_cap)
     /* 8. histograms for the long-range resonators */
     for (ib = 0; ib < nbunch; ib++) {
       worker_t *w = &W[ib];
+      if (!IN_RANGE(ib)) continue;
       if (ring.longrange_resonators_size[LON] > 0)
         fnp_ring_update(&w->ring, fnp_ring, &w->sf, &w->bunch, w->kb, LON);
       if (ring.longrange_resonators_size[HOR] > 0 && track.TrackPlane[HOR])

@@ -277,6 +277,21 @@ int mbt_be_field_dev(long n, const double *dx_dev, const double *dy_dev,
                      double sgm_xx_mm, double sgm_zz_mm, double factdq,
                      double *ex_dev, double *ey_dev, void *stream);
 
+/* Statistics and in-range histograms of one bunch held in device memory:
+ * weak_bunch_mean_rms (statistics.c:91-128) for every tracked plane and
+ * the binning of fnp_ring_update (transform_weak.c:838-865).
+ *   coord_dev  soa6 block of np particles (device)
+ *   sigma_tau, nsigma, dT, ncell  binning (transform_weak.c:611-613);
+ *              ncell = 0 skips the histograms
+ *   stats      12 doubles (host), the order of mbt_run_turns
+ *   hist_dev   3 x ncell doubles (device): count, sum x, sum z per bin
+ * Block partial sums are kept in scratch device memory that this call
+ * allocates and frees. */
+int mbt_bunch_moments_dev(int np, const double *coord_dev, double sigma_tau,
+                          double nsigma, double dT, int ncell,
+                          const int track_plane[3], double *stats,
+                          double *hist_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

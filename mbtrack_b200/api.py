@@ -45,6 +45,8 @@ SIGNATURES = {
     "mbt_get_histograms": (ctypes.c_int, [_vp, ctypes.c_int] + [_vp] * 6),
     "mbt_last_timing": (ctypes.c_int, [_vp, _vp, _vp]),
     "mbt_geometry": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "mbt_bunch_moments_dev": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, _vp]),
     "mbt_wofz_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mbt_be_field_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, _vp, _vp, _vp]),
@@ -240,3 +242,13 @@ def wofz_dev(x_ptr, y_ptr, re_ptr, im_ptr, n, flag_ptr=None, stream=None):
 
 def be_field_dev(dx_ptr, dy_ptr, n, sgm_xx_mm, sgm_zz_mm, factdq, ex_ptr, ey_ptr, stream=None):
     _check(lib().mbt_be_field_dev(n, dx_ptr, dy_ptr, sgm_xx_mm, sgm_zz_mm, factdq, ex_ptr, ey_ptr, stream))
+
+
+def bunch_moments_dev(np_, coord_ptr, sigma_tau, nsigma, dT, ncell, track_plane, hist_ptr=None, stream=None):
+    """Statistics (12 values, mbt.h order) of one bunch on the device; the
+    in-range histograms go to hist_ptr (3 x ncell doubles, device)."""
+    st = np.zeros(12)
+    tp = np.ascontiguousarray(track_plane, dtype=np.int32)
+    _check(lib().mbt_bunch_moments_dev(np_, coord_ptr, sigma_tau, nsigma, dT, ncell, _ptr(tp), _ptr(st),
+                                       hist_ptr, stream))
+    return st

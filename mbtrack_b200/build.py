@@ -21,9 +21,9 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--expt-re
                      "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-I" + os.path.join(ROOT, "include")]
 
-CU_SOURCES = ["mbt_runtime.cu"]
+CU_SOURCES = ["mbt_runtime.cu", "mbt_step.cu"]
 C_SOURCES = ["mbt_host.c"]
-HEADERS = ["mbt_device.cuh", "mbt_kernels.cuh", "mbt_philox.cuh", "mbt_wofz.cuh"]
+HEADERS = ["mbt_common.cuh", "mbt_device.cuh", "mbt_kernels.cuh", "mbt_philox.cuh", "mbt_wofz.cuh"]
 
 
 def _run(cmd):

@@ -1,0 +1,159 @@
+// mbt_step.cu -- per-step device entry points on caller-owned device data.
+//
+// mbt_bunch_moments_dev: statistics and binning of one bunch
+// (weak_bunch_mean_rms statistics.c:91-128 for every tracked plane, and the
+// in-range histograms of fnp_ring_update transform_weak.c:838-865) in two
+// kernels: block partial records, then one block that reduces them in a
+// fixed order.  The partial records are scratch memory.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "mbt.h"
+#include "mbt_common.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kExtra = 12;           // 6 shifted sums, 6 shifted sums of squares
+
+// Record of one block: counts[nc], sum x[nc], sum z[nc], kExtra sums.
+__global__ void __launch_bounds__(kThreads)
+moments_partial(int np, const double *__restrict__ c, double sgm, double nsig, double dT, int nc,
+                double *__restrict__ part, int prec) {
+  extern __shared__ double sh[];
+  double *hx = sh, *hz = sh + nc;
+  int *hc = reinterpret_cast<int *>(sh + 2 * nc);
+  __shared__ double red[kThreads / 32][kExtra];
+  for (int i = threadIdx.x; i < nc; i += kThreads) { hx[i] = 0.0; hz[i] = 0.0; hc[i] = 0; }
+  __syncthreads();
+  const size_t n6 = (size_t)np;
+  double s[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) s[k] = c[k * n6];   // shift: the first particle
+  double ms[6] = {0, 0, 0, 0, 0, 0}, mq[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < np; i += gridDim.x * kThreads) {
+    double v[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      v[k] = c[k * n6 + i];
+      const double d = v[k] - s[k];
+      ms[k] += d;
+      mq[k] += d * d;
+    }
+    if (nc > 0) {
+      const int ic = mbt::bin_of(v[0], sgm, nsig, dT);
+      if (ic >= 0 && ic < nc) {
+        atomicAdd(&hc[ic], 1);
+        atomicAdd(&hx[ic], v[1]);
+        atomicAdd(&hz[ic], v[2]);
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const double a = mbt::warp_sum(ms[k]), b = mbt::warp_sum(mq[k]);
+    if (lane == 0) { red[warp][k] = a; red[warp][6 + k] = b; }
+  }
+  __syncthreads();
+  double *rec = part + (size_t)blockIdx.x * prec;
+  if (threadIdx.x < kExtra) {
+    double t = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) t += red[w][threadIdx.x];
+    rec[3 * nc + threadIdx.x] = t;
+  }
+  for (int i = threadIdx.x; i < nc; i += kThreads) {
+    rec[i] = (double)hc[i];
+    rec[nc + i] = hx[i];
+    rec[2 * nc + i] = hz[i];
+  }
+}
+
+// One block: records summed in block order; stats (12 doubles, mbt.h
+// order) and histograms written to `out` (12 + 3 nc doubles).
+__global__ void __launch_bounds__(kThreads)
+moments_final(int np, const double *__restrict__ c, int nc, int nblk, const double *__restrict__ part,
+              int prec, int th, int tv, double *__restrict__ out) {
+  const size_t n6 = (size_t)np;
+  for (int e = threadIdx.x; e < prec; e += kThreads) {
+    double t = 0.0;
+    for (int b = 0; b < nblk; ++b) t += part[(size_t)b * prec + e];
+    if (e < 3 * nc) out[12 + e] = t;
+    else {
+      const int k = (e - 3 * nc) % 6;
+      const bool sq = (e - 3 * nc) >= 6;
+      const int plane = k % 3;
+      const bool tracked = plane == 0 || (plane == 1 ? th : tv);
+      // stash: sums into out[] temporarily
+      if (!sq) out[12 + 3 * nc + k] = tracked ? t : 0.0;
+      else out[12 + 3 * nc + 6 + k] = tracked ? t : 0.0;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int k = threadIdx.x;
+    const double N = (double)np;
+    const double sum = out[12 + 3 * nc + k], sq = out[12 + 3 * nc + 6 + k];
+    const int plane = k % 3;
+    const bool tracked = plane == 0 || (plane == 1 ? th : tv);
+    double mean = 0.0, rms = 0.0;
+    if (tracked && np > 0) {
+      const double a = sum / N, q = sq / N;
+      mean = c[k * n6] + a;
+      const double var = q - a * a;
+      rms = sqrt(var > 0.0 ? var : 0.0);
+    }
+    const int col = (k < 3) ? k : 6 + (k - 3);
+    out[col] = mean;
+    out[col + 3] = rms;
+  }
+}
+
+int blocks_for(int np) {
+  return std::max(1, std::min((np + kThreads * 8 - 1) / (kThreads * 8), 148 * 4));
+}
+
+int check_args(int np, const double *coord, double sgm, double dT, int ncell, const int *tp,
+               const double *stats, const double *hist) {
+  if (np <= 0 || !coord || !tp || !stats) return MBT_ERR_INVALID;
+  if (ncell < 0 || ncell > MBT_MAX_NCELL) return MBT_ERR_INVALID;
+  if (ncell > 0 && (!hist || !(sgm > 0.0) || !(dT > 0.0))) return MBT_ERR_INVALID;
+  return 0;
+}
+
+int run_moments(int np, const double *coord, double sgm, double nsig, double dT, int ncell, const int *tp,
+                double *stats, double *hist, cudaStream_t st, double *scratch, int nblk) {
+  const int prec = 3 * ncell + kExtra;
+  const size_t smem = (size_t)ncell * (2 * sizeof(double) + sizeof(int));
+  double *part = scratch, *out = scratch + (size_t)nblk * prec;
+  moments_partial<<<nblk, kThreads, smem, st>>>(np, coord, sgm, nsig, dT, ncell, part, prec);
+  moments_final<<<1, kThreads, 0, st>>>(np, coord, ncell, nblk, part, prec, tp[1] != 0, tp[2] != 0, out);
+  if (cudaGetLastError() != cudaSuccess) return MBT_ERR_CUDA;
+  if (ncell > 0 &&
+      cudaMemcpyAsync(hist, out + 12, (size_t)3 * ncell * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return MBT_ERR_CUDA;
+  if (cudaMemcpyAsync(stats, out, 12 * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess) return MBT_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return MBT_ERR_CUDA;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int mbt_bunch_moments_dev(int np, const double *coord_dev, double sigma_tau, double nsigma, double dT,
+                                     int ncell, const int track_plane[3], double *stats, double *hist_dev,
+                                     void *stream) {
+  int r = check_args(np, coord_dev, sigma_tau, dT, ncell, track_plane, stats, hist_dev);
+  if (r) return r;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MBT_ERR_NODEVICE;
+  const int nblk = blocks_for(np);
+  const size_t n = (size_t)nblk * (3 * ncell + kExtra) + 12 + 3 * (size_t)ncell + 12;
+  double *scratch = nullptr;
+  if (cudaMalloc(&scratch, n * sizeof(double)) != cudaSuccess) return MBT_ERR_NOMEM;
+  r = run_moments(np, coord_dev, sigma_tau, nsigma, dT, ncell, track_plane, stats, hist_dev,
+                  (cudaStream_t)stream, scratch, nblk);
+  cudaFree(scratch);
+  return r;
+}

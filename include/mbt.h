@@ -292,6 +292,23 @@ int mbt_bunch_moments_dev(int np, const double *coord_dev, double sigma_tau,
                           const int track_plane[3], double *stats,
                           double *hist_dev, void *stream);
 
+/* Same result as mbt_bunch_moments_dev, for callers that must not allocate
+ * device memory during the call (their memory is owned by a pool or a
+ * framework allocator, or they cannot afford a possibly synchronising
+ * cudaMalloc per call).  It has no counterpart in the reference.
+ * Its scratch is a fixed 2 MiB device array inside libmbt, present on every
+ * GPU that loads the library until the process exits; the first call on a
+ * device looks up that array's address, so make it before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU race.
+ * ncell is limited to MBT_NOALLOC_MAX_NCELL (larger values return
+ * MBT_ERR_INVALID); np is not limited.  It calls no allocator. */
+#define MBT_NOALLOC_MAX_NCELL 1024
+int mbt_bunch_moments_dev_noalloc(int np, const double *coord_dev,
+                                  double sigma_tau, double nsigma, double dT,
+                                  int ncell, const int track_plane[3],
+                                  double *stats, double *hist_dev,
+                                  void *stream);
+
 #ifdef __cplusplus
 }
 #endif

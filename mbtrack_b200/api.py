@@ -47,6 +47,8 @@ SIGNATURES = {
     "mbt_geometry": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "mbt_bunch_moments_dev": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_double, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "mbt_bunch_moments_dev_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_double, ctypes.c_double,
+                                                     ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, _vp]),
     "mbt_wofz_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mbt_be_field_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, _vp, _vp, _vp]),
@@ -251,4 +253,15 @@ def bunch_moments_dev(np_, coord_ptr, sigma_tau, nsigma, dT, ncell, track_plane,
     tp = np.ascontiguousarray(track_plane, dtype=np.int32)
     _check(lib().mbt_bunch_moments_dev(np_, coord_ptr, sigma_tau, nsigma, dT, ncell, _ptr(tp), _ptr(st),
                                        hist_ptr, stream))
+    return st
+
+
+def bunch_moments_dev_noalloc(np_, coord_ptr, sigma_tau, nsigma, dT, ncell, track_plane, hist_ptr=None,
+                              stream=None):
+    """As bunch_moments_dev, through the entry point that allocates nothing
+    (its scratch is a fixed device array inside libmbt)."""
+    st = np.zeros(12)
+    tp = np.ascontiguousarray(track_plane, dtype=np.int32)
+    _check(lib().mbt_bunch_moments_dev_noalloc(np_, coord_ptr, sigma_tau, nsigma, dT, ncell, _ptr(tp),
+                                               _ptr(st), hist_ptr, stream))
     return st

@@ -33,6 +33,17 @@ thread_local char g_create_error[512] = "";
 
 }  // namespace
 
+namespace mbt {
+// Message for mbt_last_error(NULL, ...) from entry points without a context.
+int fail_global(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_create_error, sizeof g_create_error, fmt, ap);
+  va_end(ap);
+  return code;
+}
+}  // namespace mbt
+
 struct mbt_ctx {
   mbt_params p{};
   int nbunch = 0, npad = 0, tile = 0, ntile = 0, prec = 0, nc = 0, nlr = 0;

@@ -13,6 +13,10 @@
 #include "mbt.h"
 #include "mbt_common.cuh"
 
+namespace mbt {
+int fail_global(int code, const char *fmt, ...);
+}
+
 namespace {
 
 constexpr int kThreads = 256;
@@ -117,9 +121,12 @@ int blocks_for(int np) {
 
 int check_args(int np, const double *coord, double sgm, double dT, int ncell, const int *tp,
                const double *stats, const double *hist) {
-  if (np <= 0 || !coord || !tp || !stats) return MBT_ERR_INVALID;
-  if (ncell < 0 || ncell > MBT_MAX_NCELL) return MBT_ERR_INVALID;
-  if (ncell > 0 && (!hist || !(sgm > 0.0) || !(dT > 0.0))) return MBT_ERR_INVALID;
+  if (np <= 0 || !coord || !tp || !stats)
+    return mbt::fail_global(MBT_ERR_INVALID, "bunch moments: np must be positive, pointers non-NULL");
+  if (ncell < 0 || ncell > MBT_MAX_NCELL)
+    return mbt::fail_global(MBT_ERR_INVALID, "bunch moments: ncell %d outside 0..%d", ncell, MBT_MAX_NCELL);
+  if (ncell > 0 && (!hist || !(sgm > 0.0) || !(dT > 0.0)))
+    return mbt::fail_global(MBT_ERR_INVALID, "bunch moments: binning needs hist_dev, sigma_tau > 0, dT > 0");
   return 0;
 }
 
@@ -147,13 +154,82 @@ extern "C" int mbt_bunch_moments_dev(int np, const double *coord_dev, double sig
   int r = check_args(np, coord_dev, sigma_tau, dT, ncell, track_plane, stats, hist_dev);
   if (r) return r;
   int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MBT_ERR_NODEVICE;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return mbt::fail_global(MBT_ERR_NODEVICE, "no CUDA device: libmbt has no CPU path");
   const int nblk = blocks_for(np);
   const size_t n = (size_t)nblk * (3 * ncell + kExtra) + 12 + 3 * (size_t)ncell + 12;
   double *scratch = nullptr;
-  if (cudaMalloc(&scratch, n * sizeof(double)) != cudaSuccess) return MBT_ERR_NOMEM;
+  if (cudaMalloc(&scratch, n * sizeof(double)) != cudaSuccess)
+    return mbt::fail_global(MBT_ERR_NOMEM, "bunch moments: cudaMalloc of %zu bytes failed", n * sizeof(double));
   r = run_moments(np, coord_dev, sigma_tau, nsigma, dT, ncell, track_plane, stats, hist_dev,
                   (cudaStream_t)stream, scratch, nblk);
   cudaFree(scratch);
   return r;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of mbt_bunch_moments_dev.
+//
+// Some callers cannot call cudaMalloc at the moment they need the bunch
+// statistics: a host that owns all device memory through its own pool (or a
+// framework's caching allocator) and must keep every byte accounted for, or a
+// latency-critical loop where an allocation per call, which may synchronise
+// the device, is not acceptable.  For them the block partial sums live in
+// one file-scope device array of fixed size instead of per-call memory.
+//
+// That array exists once on every GPU that loads this library and stays
+// allocated until the process exits.  Its device address is looked up once
+// per device (cudaGetSymbolAddress) by the first call made with that device
+// current; make that first call before any stream capture.  Every call uses
+// the same array and leaves its contents behind; each call writes every
+// element it later reads (partial records, then the result area), so nothing
+// has to be cleared.  Two calls whose work overlaps on the GPU (different
+// streams, or different host threads on one device) race on the array.
+
+namespace {
+
+constexpr size_t kNoAllocDoubles = 262144;      // 2 MiB
+constexpr int kNoAllocMaxDevices = 64;
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+double *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+int noalloc_scratch(double **out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0)
+    return mbt::fail_global(MBT_ERR_NODEVICE, "no CUDA device: libmbt has no CPU path");
+  if (dev >= kNoAllocMaxDevices)
+    return mbt::fail_global(MBT_ERR_INVALID, "device %d: the allocation-free path serves devices 0..%d", dev,
+                            kNoAllocMaxDevices - 1);
+  if (g_noalloc_addr[dev] == nullptr) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      return mbt::fail_global(MBT_ERR_CUDA, "cudaGetSymbolAddress of the scratch array: %s", cudaGetErrorString(e));
+    g_noalloc_addr[dev] = static_cast<double *>(p);
+  }
+  *out = g_noalloc_addr[dev];
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int mbt_bunch_moments_dev_noalloc(int np, const double *coord_dev, double sigma_tau, double nsigma,
+                                             double dT, int ncell, const int track_plane[3], double *stats,
+                                             double *hist_dev, void *stream) {
+  int r = check_args(np, coord_dev, sigma_tau, dT, ncell, track_plane, stats, hist_dev);
+  if (r) return r;
+  if (ncell > MBT_NOALLOC_MAX_NCELL)
+    return mbt::fail_global(MBT_ERR_INVALID, "allocation-free bunch moments: ncell %d exceeds %d", ncell,
+                            MBT_NOALLOC_MAX_NCELL);
+  double *scratch = nullptr;
+  r = noalloc_scratch(&scratch);
+  if (r) return r;
+  const int prec = 3 * ncell + kExtra;
+  const size_t result = 12 + 3 * (size_t)ncell + 12;
+  const int fit = (int)((kNoAllocDoubles - result) / (size_t)prec);
+  const int nblk = std::min(blocks_for(np), fit);
+  if (nblk < 1)
+    return mbt::fail_global(MBT_ERR_INVALID, "allocation-free bunch moments: ncell %d does not fit the scratch", ncell);
+  return run_moments(np, coord_dev, sigma_tau, nsigma, dT, ncell, track_plane, stats, hist_dev,
+                     (cudaStream_t)stream, scratch, nblk);
 }

@@ -15,6 +15,49 @@ __device__ __forceinline__ int bin_of(double xtau, double sgm, double nsig, doub
   return __double2int_rz(__dadd_rn(q, 1.0));
 }
 
+// The same bin index from two multiplications, exact wherever the estimate
+// is farther than 1e-9 from an integer (both it and the IEEE sequence are
+// within ~1e-12 of the true quotient for |index| < 2^10, so they truncate
+// alike); closer than that the IEEE sequence decides.
+__device__ __forceinline__ int bin_fast(double xtau, double sgm, double nsig, double dT,
+                                        double inv_sgm, double inv_dT) {
+  const double q = fma(fma(-xtau, inv_sgm, nsig), inv_dT, 1.0);
+  if (fabs(q - rint(q)) > 1e-9) return __double2int_rz(q);
+  return bin_of(xtau, sgm, nsig, dT);
+}
+
+// sin and cos of (a + d) from S = sin a, C = cos a and a small offset
+// |d| <= 0.25: angle addition, with sin d and cos d - 1 from their Taylor
+// series (terms to d^11 and d^12; truncation below 1e-17 relative).
+__device__ __forceinline__ void sincos_near(double d, double S, double C, double &s, double &c) {
+  const double d2 = d * d;
+  double ps = -1.0 / 39916800.0;
+  ps = fma(ps, d2, 1.0 / 362880.0);
+  ps = fma(ps, d2, -1.0 / 5040.0);
+  ps = fma(ps, d2, 1.0 / 120.0);
+  ps = fma(ps, d2, -1.0 / 6.0);
+  const double sd = fma(d * d2, ps, d);            // sin d
+  double pc = 1.0 / 479001600.0;
+  pc = fma(pc, d2, -1.0 / 3628800.0);
+  pc = fma(pc, d2, 1.0 / 40320.0);
+  pc = fma(pc, d2, -1.0 / 720.0);
+  pc = fma(pc, d2, 1.0 / 24.0);
+  pc = fma(pc, d2, -0.5);
+  const double cm1 = pc * d2;                      // cos d - 1
+  s = S + fma(S, cm1, C * sd);
+  c = C + fma(C, cm1, -(S * sd));
+}
+
+// a / b for b near 1 (|b - 1| < 0.5): single-precision reciprocal refined
+// by two Newton steps (relative error ~1e-28) then one product; within one
+// rounding of the IEEE quotient.
+__device__ __forceinline__ double div_near1(double a, double b) {
+  double r = (double)(1.0f / (float)b);
+  r = r * fma(-b, r, 2.0);
+  r = r * fma(-b, r, 2.0);
+  return a * r;
+}
+
 __device__ __forceinline__ long cyc_slot(long k, long n) {
   // cyclic_array_get/access (cyclic_array.c:21-34) with an int index
   const int in = (int)k;
@@ -65,6 +108,84 @@ __device__ __forceinline__ Aff warp_exclusive_scan(Aff x, int lane) {
   }
   Aff ex = shfl_up(inc, 1);
   return lane == 0 ? aff_id() : ex;
+}
+
+}  // namespace mbt
+
+// ---- bulk asynchronous copies (TMA, non-tensor) and mbarriers -----------
+// One thread issues cp.async.bulk copies between global memory and shared
+// memory; completion of loads is tracked by an mbarrier with a transaction
+// count, stores by bulk groups.  No cluster multicast is used anywhere.
+
+namespace mbt {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// Global -> shared bulk copy completing on `bar`; bytes a multiple of 16,
+// both addresses 16-byte aligned.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Shared -> global bulk copy in the current bulk group.
+__device__ __forceinline__ void bulk_store(void *dst, const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// Wait until at most N committed store groups still read shared memory.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+// Wait until every committed store group has completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// Make this thread's generic-proxy shared-memory writes visible to the
+// async proxy (before a bulk store reads them).
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Bounded wait for phase `parity` of `bar`: returns false (and leaves the
+// wait) after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long limit) {
+  const uint32_t a = smem_u32(bar);
+  for (long k = 0; k < limit; ++k) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
 }
 
 }  // namespace mbt

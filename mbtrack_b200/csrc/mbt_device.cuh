@@ -60,13 +60,17 @@ struct OpticConst {
   int track_h, track_v;
   // binning (transform_weak.c:611-613)
   double sigma_tau, nsigma, dT;
+  double inv_sigma_tau, inv_dT;     // for the fast exact bin index
   int ncell;
+  // sin and cos of the betatron phase advances 2 pi Q (PsiV0, PsiH0)
+  double sin_psiV0, cos_psiV0, sin_psiH0, cos_psiH0;
 };
 
 // Mutable ring-wide state, device resident, read by every kernel.
 struct RingState {
   long turn;           // turns completed
   double Vrf0, phai0;  // RF parameters after the feedback correction
+  double sin_phai0, cos_phai0;
   int rffb_on;
   int rffb_count;
   int rw_m;            // resistive-wall trigger counter (worker_weakweak.c:254)

@@ -35,19 +35,147 @@ namespace mbt {
 
 // ---------------------------------------------------------------- K1
 
+// One macroparticle through the pending RW kick, the wake kick and the
+// one-turn map (transform_weak.c:21-192); coordinates updated in place.
+template <int NOISE>
+__device__ __forceinline__ void advance_particle(const Args &a, const OpticConst &oc, double &xtau, double &x,
+                                                 double &z, double &eps, double &xp, double &zp, bool rw,
+                                                 double rwH, double rwV, bool sf, bool kick_l, bool kick_v,
+                                                 bool kick_h, const double *kL, const double *kV,
+                                                 const double *kH, int nc, double eps_const, double phai0,
+                                                 double sin_ph, double cos_ph, int kb, uint32_t jb,
+                                                 long turn, size_t p) {
+  if (rw) {
+    if (oc.track_h) xp = xp + rwH;
+    if (oc.track_v) zp = zp + rwV;
+  }
+  if (sf) {
+    int ic = bin_fast(xtau, oc.sigma_tau, oc.nsigma, oc.dT, oc.inv_sigma_tau, oc.inv_dT);
+    ic = ic < 0 ? 0 : (ic >= nc ? nc - 1 : ic);
+    if (kick_l) eps = eps + kL[ic];
+    if (kick_v) zp = zp + kV[ic];
+    if (kick_h) xp = xp + kH[ic];
+  }
+  // ---- longitudinal (transform_weak.c:49-97)
+  const double xtau0 = xtau, eps0 = eps, x0 = x, xp0 = xp, z0 = z, zp0 = zp;
+  double g;
+  if (!oc.ideal_hc) {
+    // sin(wrf xtau + phai0) with the reference's rounding of the argument
+    const double arg = oc.wrf * xtau0 + phai0;
+    const double d = arg - phai0;
+    double sr, cr;
+    if (fabs(d) <= 0.25) sincos_near(d, sin_ph, cos_ph, sr, cr);
+    else sr = sin(arg);
+    g = eps_const * sr;
+    for (int j = 0; j < oc.n_ahc; ++j) {
+      const double ph = oc.ahc_nhc[j] * (double)kb * 2 * MBT_PI;
+      g += oc.ahc_amp[j] * sin(oc.ahc_w[j] * xtau0 + oc.ahc_phi[j] + ph);
+    }
+  } else {
+    g = eps_const * (sin(oc.wrf * xtau0 + phai0) + oc.HC_k * sin(oc.m_aHC_d * oc.wrf * xtau0 + oc.m_phi_n));
+  }
+  float dv[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  if (NOISE == MBT_NOISE_PHILOX) {
+    turn_normals1(a.seed, jb, (uint32_t)kb, (uint64_t)turn, dv);
+  } else if (NOISE == MBT_NOISE_INJECTED) {
+    const long dt = turn - a.dev_turn0;
+    if (dt >= 0 && dt < a.dev_nturn) {
+      const float *dd = a.dev + (size_t)dt * 5 * (size_t)a.npad + p;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) dv[k] = dd[(size_t)k * a.npad];
+    } else {
+      atomicOr(&a.rs->error, 1);
+    }
+  }
+  eps = eps0 + g - oc.Urad;
+  double rff = 1.0;
+  if (NOISE != MBT_NOISE_NONE) {
+    eps = eps * oc.damp + oc.excite * (double)dv[0];
+    rff = div_near1(1.0 + eps0, 1.0 + eps0 + g);
+  }
+  xtau = xtau0 - eps * oc.T0 * oc.ac;
+  // ---- amplitude terms (transform_weak.c:115-123, 159-167)
+  double EV = 0.0, EH = 0.0;
+  if (oc.amp_dep) {
+    EV = oc.gammaV * z0 * z0 + 2 * oc.alphaV * z0 * zp0 + oc.betaV * zp0 * zp0;
+    EH = oc.gammaV * x0 * x0 + 2 * oc.alphaV * x0 * xp0 + oc.betaV * xp0 * xp0;
+  }
+  // ---- vertical (transform_weak.c:101-141)
+  if (oc.track_v) {
+    const double dQ = oc.amp_dep ? (oc.CVH * EH + oc.CVV * EV) : 0.0;
+    const double psi = oc.psiV0 * (1.0 + oc.Gziz * eps0 + dQ);
+    double sn, cs;
+    const double d = psi - oc.psiV0;
+    if (fabs(d) <= 0.25) sincos_near(d, oc.sin_psiV0, oc.cos_psiV0, sn, cs);
+    else sincos(psi, &sn, &cs);
+    const double a11 = cs + oc.alphaV * sn, a12 = oc.betaV * sn;
+    const double a21 = -oc.gammaV * sn, a22 = cs - oc.alphaV * sn;
+    z = a11 * z0 + a12 * zp0;
+    zp = a21 * z0 + a22 * zp0;
+    if (NOISE != MBT_NOISE_NONE) {
+      z = z + oc.qv_pos * (double)dv[1];
+      zp = rff * zp + oc.qv_slope * (double)dv[2];
+    }
+  }
+  // ---- horizontal (transform_weak.c:144-190)
+  if (oc.track_h) {
+    const double dQ = oc.amp_dep ? (oc.CHH * EH + oc.CHV * EV) : 0.0;
+    const double psi = oc.psiH0 * (1.0 + oc.Gzix * eps0 + dQ);
+    double sn, cs;
+    const double d = psi - oc.psiH0;
+    if (fabs(d) <= 0.25) sincos_near(d, oc.sin_psiH0, oc.cos_psiH0, sn, cs);
+    else sincos(psi, &sn, &cs);
+    const double a11 = cs + oc.alphaH * sn;
+    const double a12 = oc.betaH * sn;
+    const double a13 = (1.0 - a11) * oc.dispH - a12 * oc.disppH;
+    const double a21 = -oc.gammaH * sn;
+    const double a22 = cs - oc.alphaH * sn;
+    const double a23 = -a21 * oc.dispH + (1.0 - a22) * oc.disppH;
+    x = a11 * x0 + a12 * xp0 + a13 * eps;
+    xp = a21 * x0 + a22 * xp0 + a23 * eps;
+    if (NOISE != MBT_NOISE_NONE) {
+      x = x + oc.qh_pos * (double)dv[3];
+      xp = rff * xp + oc.qh_slope * (double)dv[4];
+    }
+  }
+}
+
+// Particle pass (K1).  Each block streams its tile through a ring of
+// kStages shared-memory stages of kChunk particles: thread 0 issues six
+// bulk loads per stage (one per coordinate array, completion on the
+// stage's mbarrier), every thread advances one particle of the chunk in
+// place, and thread 0 writes the stage back with six bulk stores before
+// refilling it.  Moments and next-turn histograms come from the updated
+// coordinates in shared memory.
+constexpr int kChunk = 256;
+constexpr int kStages = 3;
+constexpr long kWaitLimit = 1L << 24;   // polls before a wait is declared failed
+
+// stages, per-thread moment sums (12 x kBlock), kick tables and histograms
+__host__ __device__ constexpr size_t turn_map_smem(int nc) {
+  return (size_t)kStages * 6 * kChunk * sizeof(double) + (size_t)12 * kBlock * sizeof(double) +
+         (size_t)nc * 5 * sizeof(double) + (size_t)nc * sizeof(int);
+}
+
 template <bool MOVE, int NOISE, bool HISTXZ>
-__global__ void __launch_bounds__(kBlock) turn_map(Args a) {
-  extern __shared__ double smem[];
+__global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
+  extern __shared__ __align__(128) double smem[];
   const int nc = a.ncell;
   const Tile tile = a.tiles[blockIdx.x];
   const int b = tile.bunch;
-  double *kL = smem;
-  double *kV = smem + nc;
-  double *kH = smem + 2 * nc;
-  double *hx = smem + 3 * nc;
-  double *hz = smem + 4 * nc;
-  int *hc = reinterpret_cast<int *>(smem + 5 * nc);
-  __shared__ double red[kBlock / 32][kPartialExtra];
+  double *stage = smem;
+  double *acct = smem + kStages * 6 * kChunk;    // [12][kBlock]: this thread's shifted sums
+  double *kL = acct + 12 * kBlock;
+  double *kV = kL + nc;
+  double *kH = kL + 2 * nc;
+  double *hx = kL + 3 * nc;
+  double *hz = kL + 4 * nc;
+  int *hc = reinterpret_cast<int *>(kL + 5 * nc);
+  __shared__ __align__(8) uint64_t bars[kStages];
+  __shared__ double red[kBlock / 32][12];
+  __shared__ double trash[6];
+  __shared__ double shift[6];
+  __shared__ int abort_flag;
 
   const bool sf = MOVE && a.selffield;
   for (int i = threadIdx.x; i < nc; i += kBlock) {
@@ -59,168 +187,145 @@ __global__ void __launch_bounds__(kBlock) turn_map(Args a) {
     hc[i] = 0;
     if (HISTXZ) { hx[i] = 0.0; hz[i] = 0.0; }
   }
+  if (threadIdx.x < 6) {
+    trash[threadIdx.x] = 0.0;
+    shift[threadIdx.x] = a.shift[b * 6 + threadIdx.x];
+  }
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acct[k * kBlock + threadIdx.x] = 0.0;
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
   __syncthreads();
+
+  const size_t np6 = (size_t)a.npad;
+  double *__restrict__ C = a.coord;
+  const int nchunk = (tile.count + kChunk - 1) / kChunk;
+  auto chunk_bytes = [&](int c) -> uint32_t {
+    const int n = min(kChunk, tile.count - c * kChunk);
+    return (uint32_t)(((n * 8) + 15) & ~15);
+  };
+  auto issue_load = [&](int c) {
+    const int s = c % kStages;
+    const uint32_t bytes = chunk_bytes(c);
+    mbar_expect_tx(&bars[s], 6 * bytes);
+    const size_t g0 = (size_t)tile.start + (size_t)c * kChunk;
+    for (int k = 0; k < 6; ++k)
+      bulk_load(stage + (size_t)(s * 6 + k) * kChunk, C + k * np6 + g0, bytes, &bars[s]);
+  };
+  // prologue: kStages-1 chunks in flight; chunk c+kStages-1 is loaded at
+  // the end of iteration c into the stage chunk c-1 used
+  if (threadIdx.x == 0)
+    for (int c = 0; c < min(kStages - 1, nchunk); ++c) issue_load(c);
 
   const OpticConst &oc = a.oc;
   const long turn = a.rs->turn;
   const double eps_const = a.rs->Vrf0 / (oc.E0 * 1.0e3);
   const double phai0 = a.rs->phai0;
+  const double sin_ph = a.rs->sin_phai0, cos_ph = a.rs->cos_phai0;
   const int kb = a.bunch_kb[b];
-  double sh[6];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) sh[k] = a.shift[b * 6 + k];
   double rwH = 0.0, rwV = 0.0;
   const bool rw = MOVE && a.rw_long && turn > 0;
   if (rw) { rwH = a.rwkick[b * 2 + 0]; rwV = a.rwkick[b * 2 + 1]; }
   const bool kick_l = sf && a.lr_kick[0];
   const bool kick_h = sf && a.lr_kick[1];
   const bool kick_v = sf && a.lr_kick[2];
-  // aHC->nHC * kb * 2 * M_PI, per active harmonic cavity
-  double ahc_ph[kMaxAhc];
-#pragma unroll
-  for (int j = 0; j < kMaxAhc; ++j)
-    ahc_ph[j] = (j < oc.n_ahc) ? oc.ahc_phi[j] : 0.0;
-
-  double ms[6] = {0, 0, 0, 0, 0, 0}, mq[6] = {0, 0, 0, 0, 0, 0};
-  double lowN = 0, lowX = 0, lowZ = 0, highN = 0, highX = 0, highZ = 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int jb0 = tile.start - a.bunch_off[b];   // index of the tile's first particle in its bunch
-  const size_t np6 = (size_t)a.npad;
-  double *__restrict__ C = a.coord;
+  int consumed = 0;
 
-  for (int i = threadIdx.x; i < tile.count; i += kBlock) {
-    const size_t p = (size_t)tile.start + i;
-    double xtau = C[p], x = C[np6 + p], z = C[2 * np6 + p];
-    double eps = C[3 * np6 + p], xp = C[4 * np6 + p], zp = C[5 * np6 + p];
-    if (MOVE) {
-      if (rw) {
-        if (oc.track_h) xp = xp + rwH;
-        if (oc.track_v) zp = zp + rwV;
-      }
-      if (sf) {
-        int ic = bin_of(xtau, oc.sigma_tau, oc.nsigma, oc.dT);
-        ic = ic < 0 ? 0 : (ic >= nc ? nc - 1 : ic);
-        if (kick_l) eps = eps + kL[ic];
-        if (kick_v) zp = zp + kV[ic];
-        if (kick_h) xp = xp + kH[ic];
-      }
-      // ---- longitudinal (transform_weak.c:49-97)
-      const double xtau0 = xtau, eps0 = eps, x0 = x, xp0 = xp, z0 = z, zp0 = zp;
-      double g;
-      if (!oc.ideal_hc) {
-        g = eps_const * sin(oc.wrf * xtau0 + phai0);
-        for (int j = 0; j < oc.n_ahc; ++j) {
-          const double ph = oc.ahc_nhc[j] * (double)kb * 2 * MBT_PI;
-          g += oc.ahc_amp[j] * sin(oc.ahc_w[j] * xtau0 + ahc_ph[j] + ph);
-        }
-      } else {
-        g = eps_const * (sin(oc.wrf * xtau0 + phai0) + oc.HC_k * sin(oc.m_aHC_d * oc.wrf * xtau0 + oc.m_phi_n));
-      }
-      float dv[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-      if (NOISE == MBT_NOISE_PHILOX) {
-        turn_normals(a.seed, (uint32_t)(jb0 + i), (uint32_t)kb, (uint64_t)turn, dv);
-      } else if (NOISE == MBT_NOISE_INJECTED) {
-        const long dt = turn - a.dev_turn0;
-        if (dt >= 0 && dt < a.dev_nturn) {
-          const float *d = a.dev + (size_t)dt * 5 * np6 + p;
-#pragma unroll
-          for (int k = 0; k < 5; ++k) dv[k] = d[(size_t)k * np6];
-        } else if (threadIdx.x == 0) {
-          atomicOr(&a.rs->error, 1);
-        }
-      }
-      eps = eps0 + g - oc.Urad;
-      double rff = 1.0;
-      if (NOISE != MBT_NOISE_NONE) {
-        eps = eps * oc.damp + oc.excite * (double)dv[0];
-        rff = (1.0 + eps0) / (1.0 + eps0 + g);
-      }
-      xtau = xtau0 - eps * oc.T0 * oc.ac;
-      // ---- amplitude terms (transform_weak.c:115-123, 159-167)
-      double EV = 0.0, EH = 0.0;
-      if (oc.amp_dep) {
-        EV = oc.gammaV * z0 * z0 + 2 * oc.alphaV * z0 * zp0 + oc.betaV * zp0 * zp0;
-        EH = oc.gammaV * x0 * x0 + 2 * oc.alphaV * x0 * xp0 + oc.betaV * xp0 * xp0;
-      }
-      // ---- vertical (transform_weak.c:101-141)
-      if (oc.track_v) {
-        const double dQ = oc.amp_dep ? (oc.CVH * EH + oc.CVV * EV) : 0.0;
-        const double psi = oc.psiV0 * (1.0 + oc.Gziz * eps0 + dQ);
-        double sn, cs;
-        sincos(psi, &sn, &cs);
-        const double a11 = cs + oc.alphaV * sn, a12 = oc.betaV * sn;
-        const double a21 = -oc.gammaV * sn, a22 = cs - oc.alphaV * sn;
-        z = a11 * z0 + a12 * zp0;
-        zp = a21 * z0 + a22 * zp0;
-        if (NOISE != MBT_NOISE_NONE) {
-          z = z + oc.qv_pos * (double)dv[1];
-          zp = rff * zp + oc.qv_slope * (double)dv[2];
-        }
-      }
-      // ---- horizontal (transform_weak.c:144-190)
-      if (oc.track_h) {
-        const double dQ = oc.amp_dep ? (oc.CHH * EH + oc.CHV * EV) : 0.0;
-        const double psi = oc.psiH0 * (1.0 + oc.Gzix * eps0 + dQ);
-        double sn, cs;
-        sincos(psi, &sn, &cs);
-        const double a11 = cs + oc.alphaH * sn;
-        const double a12 = oc.betaH * sn;
-        const double a13 = (1.0 - a11) * oc.dispH - a12 * oc.disppH;
-        const double a21 = -oc.gammaH * sn;
-        const double a22 = cs - oc.alphaH * sn;
-        const double a23 = -a21 * oc.dispH + (1.0 - a22) * oc.disppH;
-        x = a11 * x0 + a12 * xp0 + a13 * eps;
-        xp = a21 * x0 + a22 * xp0 + a23 * eps;
-        if (NOISE != MBT_NOISE_NONE) {
-          x = x + oc.qh_pos * (double)dv[3];
-          xp = rff * xp + oc.qh_slope * (double)dv[4];
-        }
-      }
-      C[p] = xtau; C[np6 + p] = x; C[2 * np6 + p] = z;
-      C[3 * np6 + p] = eps; C[4 * np6 + p] = xp; C[5 * np6 + p] = zp;
-    }
-    // ---- moments (statistics.c:91-128), shifted sums
-    {
-      const double c6[6] = {xtau, x, z, eps, xp, zp};
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        const double d = c6[k] - sh[k];
-        ms[k] += d;
-        mq[k] += d * d;
+  for (int c = 0; c < nchunk; ++c) {
+    const int s = c % kStages;
+    if (!mbar_wait(&bars[s], (uint32_t)((c / kStages) & 1), kWaitLimit)) abort_flag = 1;
+    double *st = stage + (size_t)s * 6 * kChunk;
+    const int i = c * kChunk + threadIdx.x;
+    const bool live = i < tile.count;
+    double xtau = 0.0, x = 0.0, z = 0.0, eps = 0.0, xp = 0.0, zp = 0.0;
+    if (live) {
+      xtau = st[threadIdx.x]; x = st[kChunk + threadIdx.x]; z = st[2 * kChunk + threadIdx.x];
+      eps = st[3 * kChunk + threadIdx.x]; xp = st[4 * kChunk + threadIdx.x]; zp = st[5 * kChunk + threadIdx.x];
+      if (MOVE) {
+        advance_particle<NOISE>(a, oc, xtau, x, z, eps, xp, zp, rw, rwH, rwV, sf, kick_l, kick_v, kick_h, kL,
+                                kV, kH, nc, eps_const, phai0, sin_ph, cos_ph, kb, (uint32_t)(jb0 + i), turn,
+                                (size_t)tile.start + i);
+        st[threadIdx.x] = xtau; st[kChunk + threadIdx.x] = x; st[2 * kChunk + threadIdx.x] = z;
+        st[3 * kChunk + threadIdx.x] = eps; st[4 * kChunk + threadIdx.x] = xp; st[5 * kChunk + threadIdx.x] = zp;
       }
     }
-    // ---- binning of the next turn
-    if (a.selffield) {
-      const int ic = bin_of(xtau, oc.sigma_tau, oc.nsigma, oc.dT);
+    // ---- binning of the next turn (out-of-range particles are rare: shared atomics)
+    if (a.selffield && live) {
+      const int ic = bin_fast(xtau, oc.sigma_tau, oc.nsigma, oc.dT, oc.inv_sigma_tau, oc.inv_dT);
       if (ic >= 0 && ic < nc) {
         atomicAdd(&hc[ic], 1);
         if (HISTXZ) {
           atomicAdd(&hx[ic], x);
           atomicAdd(&hz[ic], z);
         }
-      } else if (ic < 0) {
-        lowN += 1.0; lowX += x; lowZ += z;
       } else {
-        highN += 1.0; highX += x; highZ += z;
+        double *t = trash + (ic < 0 ? 0 : 3);
+        atomicAdd(&t[0], 1.0);
+        atomicAdd(&t[1], x);
+        atomicAdd(&t[2], z);
+      }
+    }
+    // ---- moments (statistics.c:91-128): this thread's shifted sums
+    if (live) {
+      const double c6[6] = {xtau, x, z, eps, xp, zp};
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double d = c6[k] - shift[k];
+        acct[k * kBlock + threadIdx.x] += d;
+        acct[(6 + k) * kBlock + threadIdx.x] += d * d;
+      }
+    }
+    if (MOVE) fence_proxy_async();
+    __syncthreads();
+    consumed = c + 1;
+    if (abort_flag) break;
+    if (threadIdx.x == 0) {
+      if (MOVE) {
+        const uint32_t bytes = chunk_bytes(c);
+        const size_t g0 = (size_t)tile.start + (size_t)c * kChunk;
+        for (int k = 0; k < 6; ++k) bulk_store(C + k * np6 + g0, st + (size_t)k * kChunk, bytes);
+        bulk_commit();
+      }
+      if (c + kStages - 1 < nchunk) {
+        // the stage of chunk c-1: its store (the older of the two pending
+        // groups) must have finished reading shared memory
+        if (MOVE) bulk_wait_read<1>();
+        issue_load(c + kStages - 1);
       }
     }
   }
-
-  // ---- block reduction in a fixed order
-  double v[kPartialExtra] = {lowN, lowX, lowZ, highN, highX, highZ,
-                             ms[0], ms[1], ms[2], ms[3], ms[4], ms[5],
-                             mq[0], mq[1], mq[2], mq[3], mq[4], mq[5]};
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    if (abort_flag) {
+      // drain the loads still in flight (bounded), then report
+      // chunks consumed-1 .. consumed+kStages-3 have loads issued
+      for (int c = consumed - 1; c < min(consumed - 2 + kStages, nchunk); ++c)
+        mbar_wait(&bars[c % kStages], (uint32_t)((c / kStages) & 1), kWaitLimit);
+      atomicOr(&a.rs->error, 2);
+    }
+    bulk_wait_all();
+  }
+  __syncthreads();
+  // per-thread sums -> block sums, in a fixed order
 #pragma unroll
-  for (int k = 0; k < kPartialExtra; ++k) {
-    const double s = warp_sum(v[k]);
-    if (lane == 0) red[warp][k] = s;
+  for (int k = 0; k < 12; ++k) {
+    const double v = warp_sum(acct[k * kBlock + threadIdx.x]);
+    if (lane == 0) red[warp][k] = v;
   }
   __syncthreads();
   double *rec = a.part + (size_t)blockIdx.x * a.prec;
   if (threadIdx.x < kPartialExtra) {
-    double s = 0.0;
-    for (int w = 0; w < kBlock / 32; ++w) s += red[w][threadIdx.x];
-    rec[a.hoff + threadIdx.x] = s;
+    double sum = 0.0;
+    if (threadIdx.x < 6) {
+      sum = trash[threadIdx.x];
+    } else {
+      for (int w = 0; w < kBlock / 32; ++w) sum += red[w][threadIdx.x - 6];
+    }
+    rec[a.hoff + threadIdx.x] = sum;
   }
   for (int i = threadIdx.x; i < nc; i += kBlock) {
     rec[i] = (double)hc[i];
@@ -486,6 +591,8 @@ __global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init
       const double ph = atan2(tmp, a.rffb_vrf_design * cos(a.rffb_phi0_design) - vmbar * cos(phibar));
       rs->phai0 = ph;
       rs->Vrf0 = tmp / sin(ph);
+      rs->sin_phai0 = sin(ph);
+      rs->cos_phai0 = cos(ph);
       if (init && a.rffb_off_after_init) rs->rffb_on = 0;
     }
   }

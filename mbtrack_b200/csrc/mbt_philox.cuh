@@ -48,8 +48,39 @@ __device__ __forceinline__ void box_muller2(uint32_t a, uint32_t b, float &n0, f
   n1 = r * s;
 }
 
-// The five deviates one particle draws per turn, in the reference's roles:
-// g[0] energy, g[1] z, g[2] z', g[3] x, g[4] x'.
+// Two normals from a 24-bit radius word and an 18-bit angle word, with the
+// hardware approximations of log, sqrt and sin/cos (absolute errors near
+// 2^-21: below the single-precision resolution of the reference's deviates).
+// The angle runs over [-pi, pi), which flips both signs: the pair stays an
+// independent standard normal pair.
+__device__ __forceinline__ void box_muller_bits(uint32_t r24, uint32_t a18, float &n0, float &n1) {
+  const float u1 = (float)(r24 + 1u) * 5.9604644775390625e-08f;          // (0, 1], 2^-24 steps
+  const float th = (float)((int)a18 - 131072) * 2.396844980841821872e-05f; // [-pi, pi), 2 pi / 2^18 steps
+  const float r = __fsqrt_rn(-2.0f * __logf(u1));
+  float s, c;
+  __sincosf(th, &s, &c);
+  n0 = r * c;
+  n1 = r * s;
+}
+
+// The five deviates one particle draws per turn, in the reference's roles
+// g[0] energy, g[1] z, g[2] z', g[3] x, g[4] x', from ONE Philox call: its
+// 128 bits give three (24-bit radius, 18-bit angle) pairs.
+__device__ __forceinline__ void turn_normals1(uint64_t seed, uint32_t particle, uint32_t bucket,
+                                              uint64_t turn, float g[5]) {
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  const U4 c0 = {particle, bucket, (uint32_t)turn, ((uint32_t)(turn >> 32) << 1) | 0u};
+  const U4 r = philox4x32_10(c0, k0, k1);
+  float n5;
+  box_muller_bits(r.x >> 8, r.y >> 14, g[0], g[1]);
+  box_muller_bits(r.z >> 8, r.w >> 14, g[2], g[3]);
+  const uint32_t rr = ((r.x & 0xFFu) << 16) | ((r.y & 0x3FFFu) << 2) | (r.z & 0x3u);
+  const uint32_t aa = (((r.z >> 2) & 0x3Fu) << 12) | (r.w & 0xFFFu);
+  box_muller_bits(rr, aa, g[4], n5);
+}
+
+// Five deviates from two Philox calls (full 24-bit uniforms for both
+// members of every pair); kept for the beam generator.
 __device__ __forceinline__ void turn_normals(uint64_t seed, uint32_t particle, uint32_t bucket,
                                              uint64_t turn, float g[5]) {
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);

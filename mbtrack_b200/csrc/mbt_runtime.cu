@@ -162,7 +162,13 @@ int validate(mbt_ctx *c, const mbt_params *p, int nbunch, const int *bucket, con
 
 template <bool MOVE, int NOISE, bool HISTXZ>
 void launch_map(mbt_ctx *c) {
-  const size_t sm = (size_t)c->nc * 5 * sizeof(double) + (size_t)c->nc * sizeof(int);
+  const size_t sm = mbt::turn_map_smem(c->nc);
+  static bool attr_set = false;   // per instantiation, per process
+  if (!attr_set) {
+    cudaFuncSetAttribute(mbt::turn_map<MOVE, NOISE, HISTXZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)mbt::turn_map_smem(MBT_MAX_NCELL));
+    attr_set = true;
+  }
   mbt::turn_map<MOVE, NOISE, HISTXZ><<<c->ntile, mbt::kBlock, sm, c->stream>>>(c->a);
 }
 
@@ -419,6 +425,12 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   oc.sigma_tau = p->sigma_tau;
   oc.nsigma = p->nsigma;
   oc.dT = p->dT;
+  oc.inv_sigma_tau = p->sigma_tau > 0 ? 1.0 / p->sigma_tau : 0.0;
+  oc.inv_dT = p->dT > 0 ? 1.0 / p->dT : 0.0;
+  oc.sin_psiV0 = sin(oc.psiV0);
+  oc.cos_psiV0 = cos(oc.psiV0);
+  oc.sin_psiH0 = sin(oc.psiH0);
+  oc.cos_psiH0 = cos(oc.psiH0);
   oc.ncell = c->nc;
 
   // device allocations
@@ -480,6 +492,8 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   rs.rffb_on = p->rffb;
   rs.Vrf0_last = p->Vrf0;
   rs.phai0_last = p->phai0;
+  rs.sin_phai0 = sin(p->phai0);
+  rs.cos_phai0 = cos(p->phai0);
   if (cudaMemcpy(a.rs, &rs, sizeof rs, cudaMemcpyHostToDevice) != cudaSuccess)
     return bail(fail(nullptr, MBT_ERR_CUDA, "state upload"));
   const size_t smw = smem_wakes(c);

@@ -23,6 +23,8 @@ constexpr int kMaxLr = 8;          // MBT_MAX_LR
 constexpr int kMaxAhc = 8;         // MBT_MAX_AHC
 constexpr int kPartialExtra = 18;  // 6 out-of-range values + 12 moment sums
 constexpr int kBlock = 256;        // threads per block of every kernel
+constexpr int kRwGroup = 4;        // bunches per resistive-wall sum block
+constexpr int kRwSplit = 4;        // parts of the resistive-wall history per bunch
 
 // Offsets inside a partial record (after the 3 x ncell histograms).
 constexpr int kTrLowN = 0, kTrLowX = 1, kTrLowZ = 2;
@@ -116,7 +118,7 @@ struct Args {
   double *hist;               // nbunch x 6 x ncell: fnp, dipV, dipH (clamped), ring L, H, V (dropped)
   int *cellrange;             // nbunch x 2: icellmin, icellmax
   double *kick;               // nbunch x 3 x ncell: L, V, H kick tables
-  double *rwkick;             // nbunch x 2: pending RW kick (HOR, VER)
+  double *rw_part;            // nbunch x kRwSplit x 2: partial RW kicks (HOR, VER)
   double *stats;              // stats_cap x nbunch x 12
   int stats_cap;
   // long-range resonators

@@ -61,7 +61,7 @@ __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst
   double g;
   if (!oc.ideal_hc) {
     // sin(wrf xtau + phai0) with the reference's rounding of the argument
-    const double arg = oc.wrf * xtau0 + phai0;
+    const double arg = __dadd_rn(__dmul_rn(oc.wrf, xtau0), phai0);
     const double d = arg - phai0;
     double sr, cr;
     if (fabs(d) <= 0.25) sincos_near(d, sin_ph, cos_ph, sr, cr);
@@ -103,7 +103,7 @@ __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst
   // ---- vertical (transform_weak.c:101-141)
   if (oc.track_v) {
     const double dQ = oc.amp_dep ? (oc.CVH * EH + oc.CVV * EV) : 0.0;
-    const double psi = oc.psiV0 * (1.0 + oc.Gziz * eps0 + dQ);
+    const double psi = __dmul_rn(oc.psiV0, __dadd_rn(__dadd_rn(1.0, __dmul_rn(oc.Gziz, eps0)), dQ));
     double sn, cs;
     const double d = psi - oc.psiV0;
     if (fabs(d) <= 0.25) sincos_near(d, oc.sin_psiV0, oc.cos_psiV0, sn, cs);
@@ -120,7 +120,7 @@ __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst
   // ---- horizontal (transform_weak.c:144-190)
   if (oc.track_h) {
     const double dQ = oc.amp_dep ? (oc.CHH * EH + oc.CHV * EV) : 0.0;
-    const double psi = oc.psiH0 * (1.0 + oc.Gzix * eps0 + dQ);
+    const double psi = __dmul_rn(oc.psiH0, __dadd_rn(__dadd_rn(1.0, __dmul_rn(oc.Gzix, eps0)), dQ));
     double sn, cs;
     const double d = psi - oc.psiH0;
     if (fabs(d) <= 0.25) sincos_near(d, oc.sin_psiH0, oc.cos_psiH0, sn, cs);
@@ -228,7 +228,12 @@ __global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
   const int kb = a.bunch_kb[b];
   double rwH = 0.0, rwV = 0.0;
   const bool rw = MOVE && a.rw_long && turn > 0;
-  if (rw) { rwH = a.rwkick[b * 2 + 0]; rwV = a.rwkick[b * 2 + 1]; }
+  if (rw) {
+    for (int q = 0; q < kRwSplit; ++q) {
+      rwH += a.rw_part[((size_t)b * kRwSplit + q) * 2 + 0];
+      rwV += a.rw_part[((size_t)b * kRwSplit + q) * 2 + 1];
+    }
+  }
   const bool kick_l = sf && a.lr_kick[0];
   const bool kick_h = sf && a.lr_kick[1];
   const bool kick_v = sf && a.lr_kick[2];
@@ -466,15 +471,93 @@ __device__ __forceinline__ void rffb_store(Args &a, int slot, double vr, double 
   a.rffb_hist[2 * slot + 1] = atan2(vr, vi);
 }
 
+// Long-range resistive wall (transform_weak.c:779-833) of the turn just
+// completed, applied at the start of the next particle pass.  Bunch b sums
+// w_m E[base_b + m - 1], m = 1 .. (Nmlt+1) h, over consecutive slots of the
+// dipole history (E = dipole x bucket current, empty buckets 0), with
+// base_b = base_b0 + (kb_b - kb_b0).  A block serves kRwGroup consecutive
+// bunches and one of kRwSplit parts of the m range: it stages that part of
+// the history once in shared memory.  The kRwSplit partial kicks of a bunch
+// are summed, in order, by the particle pass.
+
+__host__ __device__ constexpr size_t rw_window_doubles(int Nmlt, int nharm) {
+  return (size_t)2 * (((size_t)(Nmlt + 1) * nharm + kRwSplit - 1) / kRwSplit + nharm);
+}
+
+__device__ void rw_partial_sums(const Args &a, int blk, double *win) {
+  const int ngroup = (a.nbunch + kRwGroup - 1) / kRwGroup;
+  const int grp = blk % ngroup, part = blk / ngroup;
+  const int b0 = grp * kRwGroup, b1 = min(b0 + kRwGroup, a.nbunch);
+  const long turn = a.rs->turn;              // the turn just completed (advanced by bunch_wakes)
+  const int h = a.nharm;
+  const int n = (a.Nmlt + 2) * h;
+  const int M = (a.Nmlt + 1) * h;
+  const int per = (M + kRwSplit - 1) / kRwSplit;
+  const int q0 = part * per, q1 = min(M, q0 + per);
+  const int kb0 = a.bunch_kb[b0];
+  const int span = a.bunch_kb[b1 - 1] - kb0;
+  const int base0 = (int)cyc_slot(-turn * h + kb0 + 1, n);
+  const bool th = a.oc.track_h, tv = a.oc.track_v;
+  const int len = max(0, q1 - q0) + span;
+  double *w0 = win, *w1 = win + per + h;
+  const double *E0 = a.rw_e, *E1 = a.rw_e + n;
+  for (int t = threadIdx.x; t < len; t += kBlock) {
+    int idx = base0 + q0 + t;
+    idx -= (idx >= n) ? n : 0;
+    idx -= (idx >= n) ? n : 0;
+    w0[t] = E0[idx];
+    w1[t] = E1[idx];
+  }
+  __syncthreads();
+  int dk[kRwGroup];
+#pragma unroll
+  for (int g = 0; g < kRwGroup; ++g) dk[g] = (b0 + g < b1) ? a.bunch_kb[b0 + g] - kb0 : -1;
+  double s[2 * kRwGroup];
+#pragma unroll
+  for (int g = 0; g < 2 * kRwGroup; ++g) s[g] = 0.0;
+  for (int j = threadIdx.x; j < q1 - q0; j += kBlock) {
+    const double w = a.rw_rsq[q0 + j + 1];
+#pragma unroll
+    for (int g = 0; g < kRwGroup; ++g) {
+      if (dk[g] >= 0) {
+        s[2 * g] += w0[j + dk[g]] * w;
+        s[2 * g + 1] += w1[j + dk[g]] * w;
+      }
+    }
+  }
+  __shared__ double red[kBlock / 32][2 * kRwGroup];
+#pragma unroll
+  for (int g = 0; g < 2 * kRwGroup; ++g) {
+    const double v = warp_sum(s[g]);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][g] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * kRwGroup) {
+    const int g = threadIdx.x >> 1, pl = threadIdx.x & 1;
+    if (b0 + g < b1) {
+      double v = 0.0;
+      for (int w = 0; w < kBlock / 32; ++w) v += red[w][threadIdx.x];
+      const int mtrig = a.rs->rw_m;          // RW kicks done before this one
+      const int trig = (a.triggerRW && mtrig < 50) ? 1 : 0;
+      const bool on = pl == 0 ? th : tv;
+      a.rw_part[((size_t)(b0 + g) * kRwSplit + part) * 2 + pl] = on ? v * a.rw_const[trig][pl] : 0.0;
+    }
+  }
+}
+
 // The phasor of each long-range resonator around the ring, bucket h-1 .. 0
 // (one pass per turn; `passes` turns for wake_phasor_init), as a warp scan
 // of affine maps: a filled bucket maps V to (V prog^ncell + U_last) G_gap,
 // an empty one to V G_empty (transform_weak.c:1006-1044, :911-947).
-// init: wake_phasor_init semantics (start from 0, no snapshot);
-// advance: bump the turn counter afterwards.
+// init: wake_phasor_init semantics (start from 0, no snapshot).  Blocks
+// after the first compute the resistive-wall partial sums.
 // vbuf: 4 x nharm doubles, the phasor before/after each bucket.
-__global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init, int advance,
-                                                    double *vbuf) {
+__global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init, double *vbuf) {
+  extern __shared__ double dyn[];
+  if (blockIdx.x > 0) {                      // resistive-wall partial sums
+    rw_partial_sums(a, blockIdx.x - 1, dyn);
+    return;
+  }
   RingState *rs = a.rs;
   const int h = a.nharm;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -596,17 +679,25 @@ __global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init
       if (init && a.rffb_off_after_init) rs->rffb_on = 0;
     }
   }
-  if (threadIdx.x == 0 && advance) {
-    rs->turn += 1;
-    if (a.rw_long) rs->rw_m += 1;
-  }
 }
 
 // ---------------------------------------------------------------- K2c
 
-__global__ void __launch_bounds__(kBlock) bunch_wakes(Args a, int with_rw) {
+__host__ __device__ constexpr size_t bunch_wakes_smem(int nc) {
+  return ((size_t)3 * (nc + 8) + 3 * (size_t)nc) * sizeof(double);
+}
+
+// One block per bunch: causal convolutions with the Green's functions,
+// long-range wake per bin and the kick tables of the next particle pass.
+// advance: bump the turn counter (no block of this launch reads it; the
+// next particle pass does).
+__global__ void __launch_bounds__(kBlock) bunch_wakes(Args a, int advance) {
   extern __shared__ double sm[];
   const int nc = a.ncell, b = blockIdx.x;
+  if (advance && b == 0 && threadIdx.x == 0) {
+    a.rs->turn += 1;
+    if (a.rw_long) a.rs->rw_m += 1;
+  }
   const int PADC = 4;
   double *fnp = sm + PADC;                    // nc + 2 PADC
   double *dipV = sm + (nc + 2 * PADC) + PADC;
@@ -615,111 +706,71 @@ __global__ void __launch_bounds__(kBlock) bunch_wakes(Args a, int with_rw) {
   const double *H = a.hist + (size_t)b * 6 * nc;
   const int kb = a.bunch_kb[b];
   __shared__ int cmin, cmax;
-  __shared__ double red[kBlock / 32][2];
-
-  if (a.selffield) {
-    for (int j = threadIdx.x - PADC; j < nc + PADC; j += kBlock) {
-      const bool in = j >= 0 && j < nc;
-      fnp[j] = in ? H[j] : 0.0;
-      dipV[j] = in ? H[nc + j] : 0.0;
-      dipH[j] = in ? H[2 * nc + j] : 0.0;
-    }
-    for (int j = threadIdx.x; j < 3 * nc; j += kBlock) lr[j] = 0.0;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      // transform_weak.c:633-651
-      int mn = nc - 1, mx = 0;
-      for (int i = 0; i < mn; ++i) if (fnp[i] > 0) { mn = i; break; }
-      for (int i = nc - 1; i > mx; --i) if (fnp[i] > 0) { mx = i; break; }
-      cmin = mn; cmax = mx;
-    }
-    __syncthreads();
-    // long-range wake per bin: V_j = Vs prog^(j+1) + U_j; the reference
-    // adds V_j + Ib fnp_j fac / 2 for every resonator of the plane
-    // (transform_weak.c:1020-1023)
-    for (int r = 0; r < a.nlr; ++r) {
-      const LrConst L = a.lr[r];
-      const double *vs = a.lr_vs + (size_t)r * a.nharm * 2 + 2 * kb;
-      const double *u = a.lr_u + ((size_t)r * a.nbunch + b) * nc * 2;
-      const double *bb = a.lr_b + ((size_t)r * a.nbunch + b) * nc;
-      const double *pw = a.lr_pw + (size_t)r * nc * 2;
-      const double s0 = vs[0], s1 = vs[1];
-      for (int j = threadIdx.x; j < nc; j += kBlock) {
-        const double v0 = (s0 * pw[2 * j] - s1 * pw[2 * j + 1]) + u[2 * j];
-        lr[L.plane * nc + j] += v0 + 0.5 * bb[j];
-      }
-      __syncthreads();
-    }
-    const double factG = a.bunch_factg[b];
-    const int icellmin = cmin, icellmax = cmax;
-    for (int j = threadIdx.x; j < nc; j += kBlock) {
-      double GL1 = 0.0, GV = 0.0, GH = 0.0;
-      if (a.planeL > 0 && j >= icellmin) {
-        double Gn = 0.0;
-        for (int k = j; k >= icellmin; --k) Gn += fnp[k] * a.Gl[j - k];
-        GL1 = 1 * Gn;
-        if (a.RsisL > 0 && j >= icellmin + 1 && j <= icellmax) {
-          const double ntmoy = (0.5 * fnp[j - 1] + fnp[j] + 0.5 * fnp[j + 1]) / 2.0;
-          GL1 += a.RsisL * ntmoy / (a.oc.sigma_tau * a.oc.dT);
-        }
-        if (a.aindL > 0 && j >= icellmin + 1 && j <= icellmax) {
-          const double ntmoy0 = (0.25 * fnp[j - 3] + 0.5 * fnp[j - 2] + fnp[j - 1] + 0.5 * fnp[j] + 0.25 * fnp[j + 1]) / 2.5;
-          const double ntmoy1 = (0.25 * fnp[j - 1] + 0.5 * fnp[j] + fnp[j + 1] + 0.5 * fnp[j + 2] + 0.25 * fnp[j + 3]) / 2.5;
-          GL1 += (ntmoy1 - ntmoy0) / (2.0 * a.sgmatau2 * a.dTau2) * a.aindL;
-        }
-      }
-      if (a.planeV > 0) {
-        double Gn = 0.0;
-        for (int k = j; k >= 0; --k) Gn += dipV[k] * a.Gv[j - k];
-        GV = 1 * Gn;
-      }
-      if (a.planeH > 0 && j >= 1) {
-        double Gn = 0.0;
-        for (int k = j; k >= 0; --k) Gn += dipH[k] * a.Gh[j - k];
-        GH = 1 * Gn;
-      }
-      double *K = a.kick + (size_t)b * 3 * nc;
-      K[j] = factG * GL1 + lr[0 * nc + j];
-      K[nc + j] = -factG * GV + lr[2 * nc + j];
-      K[2 * nc + j] = -factG * GH + lr[1 * nc + j];
-    }
+  if (!a.selffield) return;
+  for (int j = threadIdx.x - PADC; j < nc + PADC; j += kBlock) {
+    const bool in = j >= 0 && j < nc;
+    fnp[j] = in ? H[j] : 0.0;
+    dipV[j] = in ? H[nc + j] : 0.0;
+    dipH[j] = in ? H[2 * nc + j] : 0.0;
   }
-  // long-range resistive wall (transform_weak.c:779-833) of the turn just
-  // completed; applied at the start of the next particle pass.  The sum
-  // over m = 1 .. (Nmlt+1) h runs over consecutive slots of the dipole
-  // history (one wrap at most), each already multiplied by its bucket's
-  // current; empty buckets hold 0.
-  if (a.rw_long) {
-    const long turn = a.rs->turn - 1;
-    const int mtrig = a.rs->rw_m - 1;
-    const int h = a.nharm;
-    const int n = (a.Nmlt + 2) * h;
-    const int M = (a.Nmlt + 1) * h;
-    const int base = (int)cyc_slot(-turn * h + kb + 1, n);
-    const bool th = with_rw && a.oc.track_h, tv = with_rw && a.oc.track_v;
-    double s0 = 0.0, s1 = 0.0;
-    if (th || tv) {
-      const double *E0 = a.rw_e, *E1 = a.rw_e + n;
-      for (int j = threadIdx.x; j < M; j += kBlock) {
-        int idx = base + j;
-        idx -= (idx >= n) ? n : 0;
-        const double w = a.rw_rsq[j + 1];
-        s0 += E0[idx] * w;
-        s1 += E1[idx] * w;
+  for (int j = threadIdx.x; j < 3 * nc; j += kBlock) lr[j] = 0.0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // transform_weak.c:633-651
+    int mn = nc - 1, mx = 0;
+    for (int i = 0; i < mn; ++i) if (fnp[i] > 0) { mn = i; break; }
+    for (int i = nc - 1; i > mx; --i) if (fnp[i] > 0) { mx = i; break; }
+    cmin = mn; cmax = mx;
+  }
+  __syncthreads();
+  // long-range wake per bin: V_j = Vs prog^(j+1) + U_j; the reference adds
+  // V_j + Ib fnp_j fac / 2 for every resonator of the plane
+  // (transform_weak.c:1020-1023)
+  for (int r = 0; r < a.nlr; ++r) {
+    const LrConst &L = a.lr[r];
+    const double *vs = a.lr_vs + (size_t)r * a.nharm * 2 + 2 * kb;
+    const double *u = a.lr_u + ((size_t)r * a.nbunch + b) * nc * 2;
+    const double *bb = a.lr_b + ((size_t)r * a.nbunch + b) * nc;
+    const double *pw = a.lr_pw + (size_t)r * nc * 2;
+    const double s0 = vs[0], s1 = vs[1];
+    for (int j = threadIdx.x; j < nc; j += kBlock) {
+      const double v0 = (s0 * pw[2 * j] - s1 * pw[2 * j + 1]) + u[2 * j];
+      lr[L.plane * nc + j] += v0 + 0.5 * bb[j];
+    }
+    __syncthreads();
+  }
+  const double factG = a.bunch_factg[b];
+  const int icellmin = cmin, icellmax = cmax;
+  for (int j = threadIdx.x; j < nc; j += kBlock) {
+    double GL1 = 0.0, GV = 0.0, GH = 0.0;
+    if (a.planeL > 0 && j >= icellmin) {
+      double Gn = 0.0;
+      for (int k = j; k >= icellmin; --k) Gn += fnp[k] * a.Gl[j - k];
+      GL1 = 1 * Gn;
+      if (a.RsisL > 0 && j >= icellmin + 1 && j <= icellmax) {
+        const double ntmoy = (0.5 * fnp[j - 1] + fnp[j] + 0.5 * fnp[j + 1]) / 2.0;
+        GL1 += a.RsisL * ntmoy / (a.oc.sigma_tau * a.oc.dT);
+      }
+      if (a.aindL > 0 && j >= icellmin + 1 && j <= icellmax) {
+        const double ntmoy0 = (0.25 * fnp[j - 3] + 0.5 * fnp[j - 2] + fnp[j - 1] + 0.5 * fnp[j] + 0.25 * fnp[j + 1]) / 2.5;
+        const double ntmoy1 = (0.25 * fnp[j - 1] + 0.5 * fnp[j] + fnp[j + 1] + 0.5 * fnp[j + 2] + 0.25 * fnp[j + 3]) / 2.5;
+        GL1 += (ntmoy1 - ntmoy0) / (2.0 * a.sgmatau2 * a.dTau2) * a.aindL;
       }
     }
-    s0 = warp_sum(s0);
-    s1 = warp_sum(s1);
-    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5][0] = s0; red[threadIdx.x >> 5][1] = s1; }
-    __syncthreads();
-    if (threadIdx.x < 2) {
-      const int pl = threadIdx.x + 1;
-      double s = 0.0;
-      for (int w = 0; w < kBlock / 32; ++w) s += red[w][pl - 1];
-      const int trig = (a.triggerRW && mtrig < 50) ? 1 : 0;
-      const bool on = (pl == 1) ? th : tv;
-      a.rwkick[b * 2 + (pl - 1)] = on ? s * a.rw_const[trig][pl - 1] : 0.0;
+    if (a.planeV > 0) {
+      double Gn = 0.0;
+      for (int k = j; k >= 0; --k) Gn += dipV[k] * a.Gv[j - k];
+      GV = 1 * Gn;
     }
+    if (a.planeH > 0 && j >= 1) {
+      double Gn = 0.0;
+      for (int k = j; k >= 0; --k) Gn += dipH[k] * a.Gh[j - k];
+      GH = 1 * Gn;
+    }
+    double *K = a.kick + (size_t)b * 3 * nc;
+    K[j] = factG * GL1 + lr[0 * nc + j];
+    K[nc + j] = -factG * GV + lr[2 * nc + j];
+    K[2 * nc + j] = -factG * GH + lr[1 * nc + j];
   }
 }
 
@@ -732,7 +783,11 @@ __global__ void add_pending_rw(Args a, double *out) {
   const size_t n6 = (size_t)a.npad;
   const int b = blockIdx.y;
   const int off = a.bunch_off[b], np = a.bunch_np[b];
-  const double rh = a.rwkick[2 * b], rv = a.rwkick[2 * b + 1];
+  double rh = 0.0, rv = 0.0;
+  for (int q = 0; q < kRwSplit; ++q) {
+    rh += a.rw_part[((size_t)b * kRwSplit + q) * 2 + 0];
+    rv += a.rw_part[((size_t)b * kRwSplit + q) * 2 + 1];
+  }
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += gridDim.x * blockDim.x) {
     if (a.oc.track_h) out[4 * n6 + off + j] = a.coord[4 * n6 + off + j] + rh;
     if (a.oc.track_v) out[5 * n6 + off + j] = a.coord[5 * n6 + off + j] + rv;

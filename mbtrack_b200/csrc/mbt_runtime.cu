@@ -16,7 +16,6 @@
 #include "mbt.h"
 #include "mbt_device.cuh"
 #include "mbt_kernels.cuh"
-#include "mbt_wofz.cuh"
 
 using mbt::Args;
 using mbt::LrConst;
@@ -188,7 +187,13 @@ void launch_map_noise(mbt_ctx *c, int noise) {
 int effective_noise(const mbt_ctx *c) { return c->p.quantum ? c->noise : MBT_NOISE_NONE; }
 
 size_t smem_reduce(const mbt_ctx *c) { return (size_t)c->prec * sizeof(double); }
-size_t smem_wakes(const mbt_ctx *c) { return ((size_t)3 * (c->nc + 8) + 3 * (size_t)c->nc) * sizeof(double); }
+size_t smem_wakes(const mbt_ctx *c) { return mbt::bunch_wakes_smem(c->nc); }
+int rw_blocks(const mbt_ctx *c) {
+  return c->p.rw_long ? (c->nbunch + mbt::kRwGroup - 1) / mbt::kRwGroup * mbt::kRwSplit : 0;
+}
+size_t smem_scan(const mbt_ctx *c) {
+  return c->p.rw_long ? mbt::rw_window_doubles(c->p.Nmlt, c->p.nharm) * sizeof(double) : 0;
+}
 
 // One turn: particle pass, bunch reduction, ring scan, bunch wakes.
 void enqueue_turn(mbt_ctx *c, cudaEvent_t *ev) {
@@ -197,7 +202,7 @@ void enqueue_turn(mbt_ctx *c, cudaEvent_t *ev) {
   if (ev) cudaEventRecord(ev[1], c->stream);
   mbt::bunch_reduce<<<c->nbunch, mbt::kBlock, smem_reduce(c), c->stream>>>(c->a, mbt::kReduceTurn, nullptr);
   if (ev) cudaEventRecord(ev[2], c->stream);
-  mbt::ring_scan<<<1, mbt::kBlock, 0, c->stream>>>(c->a, 1, 0, 1, c->vbuf);
+  mbt::ring_scan<<<1 + rw_blocks(c), mbt::kBlock, smem_scan(c), c->stream>>>(c->a, 1, 0, c->vbuf);
   if (ev) cudaEventRecord(ev[3], c->stream);
   mbt::bunch_wakes<<<c->nbunch, mbt::kBlock, smem_wakes(c), c->stream>>>(c->a, 1);
   if (ev) cudaEventRecord(ev[4], c->stream);
@@ -461,7 +466,7 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   rc = rc ? rc : dalloc(c, &a.hist, (size_t)nbunch * 6 * c->nc);
   rc = rc ? rc : dalloc(c, &a.cellrange, (size_t)nbunch * 2);
   rc = rc ? rc : dalloc(c, &a.kick, (size_t)nbunch * 3 * c->nc);
-  rc = rc ? rc : dalloc(c, &a.rwkick, (size_t)nbunch * 2);
+  rc = rc ? rc : dalloc(c, &a.rw_part, (size_t)nbunch * mbt::kRwSplit * 2);
   a.stats_cap = 256;
   rc = rc ? rc : dalloc(c, &a.stats, (size_t)a.stats_cap * nbunch * 12);
   rc = rc ? rc : dalloc(c, &c->stats_init, (size_t)nbunch * 12);
@@ -499,6 +504,9 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   const size_t smw = smem_wakes(c);
   if (smw > 48 * 1024)
     cudaFuncSetAttribute(mbt::bunch_wakes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw);
+  const size_t sms = smem_scan(c);
+  if (sms > 48 * 1024)
+    cudaFuncSetAttribute(mbt::ring_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms);
   *out = c;
   return 0;
 }
@@ -602,8 +610,8 @@ int mbt_prepare(mbt_ctx *c, double *init_stats) {
   launch_map_noise<false>(c, MBT_NOISE_NONE);
   mbt::bunch_reduce<<<c->nbunch, mbt::kBlock, smem_reduce(c), c->stream>>>(a, mbt::kReducePrologue, c->stats_init);
   if (c->nlr > 0 && c->p.lr_init_turns > 0)
-    mbt::ring_scan<<<1, mbt::kBlock, 0, c->stream>>>(a, c->p.lr_init_turns, 1, 0, c->vbuf);
-  mbt::ring_scan<<<1, mbt::kBlock, 0, c->stream>>>(a, 1, 0, 0, c->vbuf);
+    mbt::ring_scan<<<1, mbt::kBlock, 0, c->stream>>>(a, c->p.lr_init_turns, 1, c->vbuf);
+  mbt::ring_scan<<<1, mbt::kBlock, 0, c->stream>>>(a, 1, 0, c->vbuf);
   mbt::bunch_wakes<<<c->nbunch, mbt::kBlock, smem_wakes(c), c->stream>>>(a, 0);
   CK(cudaGetLastError());
   int r = sync_and_check(c);
@@ -783,32 +791,5 @@ int mbt_geometry(mbt_ctx *c, int *npad, int *tile, int *ntile) {
 }
 
 // ---- per-step device entry points
-
-int mbt_wofz_dev(long n, const double *x, const double *y, double *re, double *im, int *flag, void *stream) {
-  mbt_ctx *c = nullptr;
-  if (n < 0 || (n > 0 && (!x || !y || !re || !im))) return fail(c, MBT_ERR_INVALID, "bad wofz arguments");
-  if (n == 0) return 0;
-  int r = check_device(c);
-  if (r) return r;
-  const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 16);
-  mbt::wofz_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(n, x, y, re, im, flag);
-  CK(cudaGetLastError());
-  return 0;
-}
-
-int mbt_be_field_dev(long n, const double *dx, const double *dy, double sgm_xx_mm, double sgm_zz_mm, double factdq,
-                     double *ex, double *ey, void *stream) {
-  mbt_ctx *c = nullptr;
-  if (n < 0 || (n > 0 && (!dx || !dy || !ex || !ey))) return fail(c, MBT_ERR_INVALID, "bad be_field arguments");
-  if (!(sgm_xx_mm > sgm_zz_mm) || !(sgm_zz_mm > 0))
-    return fail(c, MBT_ERR_INVALID, "Bassetti-Erskine needs sgm_xx > sgm_zz > 0");
-  if (n == 0) return 0;
-  int r = check_device(c);
-  if (r) return r;
-  const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 16);
-  mbt::be_field_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(n, dx, dy, sgm_xx_mm, sgm_zz_mm, factdq, ex, ey);
-  CK(cudaGetLastError());
-  return 0;
-}
 
 }  // extern "C"

@@ -151,10 +151,10 @@ constexpr int kChunk = 256;
 constexpr int kStages = 3;
 constexpr long kWaitLimit = 1L << 24;   // polls before a wait is declared failed
 
-// stages, per-thread moment sums (12 x kBlock), kick tables and histograms
+// stages, kick tables and histograms
 __host__ __device__ constexpr size_t turn_map_smem(int nc) {
-  return (size_t)kStages * 6 * kChunk * sizeof(double) + (size_t)12 * kBlock * sizeof(double) +
-         (size_t)nc * 5 * sizeof(double) + (size_t)nc * sizeof(int);
+  return (size_t)kStages * 6 * kChunk * sizeof(double) + (size_t)nc * 5 * sizeof(double) +
+         (size_t)nc * sizeof(int);
 }
 
 template <bool MOVE, int NOISE, bool HISTXZ>
@@ -164,8 +164,7 @@ __global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
   const Tile tile = a.tiles[blockIdx.x];
   const int b = tile.bunch;
   double *stage = smem;
-  double *acct = smem + kStages * 6 * kChunk;    // [12][kBlock]: this thread's shifted sums
-  double *kL = acct + 12 * kBlock;
+  double *kL = smem + kStages * 6 * kChunk;
   double *kV = kL + nc;
   double *kH = kL + 2 * nc;
   double *hx = kL + 3 * nc;
@@ -191,8 +190,6 @@ __global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
     trash[threadIdx.x] = 0.0;
     shift[threadIdx.x] = a.shift[b * 6 + threadIdx.x];
   }
-#pragma unroll
-  for (int k = 0; k < 12; ++k) acct[k * kBlock + threadIdx.x] = 0.0;
   if (threadIdx.x == 0) {
     abort_flag = 0;
     for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
@@ -240,6 +237,9 @@ __global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int jb0 = tile.start - a.bunch_off[b];   // index of the tile's first particle in its bunch
   int consumed = 0;
+  // moments: warp w < 6 owns coordinate column w of every staged chunk
+  const double col_shift = warp < 6 ? shift[warp] : 0.0;
+  double col_s = 0.0, col_q = 0.0;
 
   for (int c = 0; c < nchunk; ++c) {
     const int s = c % kStages;
@@ -275,20 +275,23 @@ __global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
         atomicAdd(&t[2], z);
       }
     }
-    // ---- moments (statistics.c:91-128): this thread's shifted sums
-    if (live) {
-      const double c6[6] = {xtau, x, z, eps, xp, zp};
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        const double d = c6[k] - shift[k];
-        acct[k * kBlock + threadIdx.x] += d;
-        acct[(6 + k) * kBlock + threadIdx.x] += d * d;
-      }
-    }
     if (MOVE) fence_proxy_async();
     __syncthreads();
     consumed = c + 1;
     if (abort_flag) break;
+    // ---- moments (statistics.c:91-128): shifted sums of the updated chunk,
+    //      one coordinate column per warp (the bulk store only reads it too)
+    if (warp < 6) {
+      const double *col = st + (size_t)warp * kChunk;
+      const int nlive = min(kChunk, tile.count - c * kChunk);
+#pragma unroll
+      for (int q = 0; q < kChunk / 32; ++q) {
+        const int e = q * 32 + lane;
+        const double d = e < nlive ? col[e] - col_shift : 0.0;
+        col_s += d;
+        col_q += d * d;
+      }
+    }
     if (threadIdx.x == 0) {
       if (MOVE) {
         const uint32_t bytes = chunk_bytes(c);
@@ -314,22 +317,18 @@ __global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
     }
     bulk_wait_all();
   }
-  __syncthreads();
-  // per-thread sums -> block sums, in a fixed order
-#pragma unroll
-  for (int k = 0; k < 12; ++k) {
-    const double v = warp_sum(acct[k * kBlock + threadIdx.x]);
-    if (lane == 0) red[warp][k] = v;
+  // column sums -> block sums, in a fixed order
+  {
+    const double vs = warp_sum(col_s), vq = warp_sum(col_q);
+    if (lane == 0 && warp < 6) {
+      red[0][warp] = vs;
+      red[0][6 + warp] = vq;
+    }
   }
   __syncthreads();
   double *rec = a.part + (size_t)blockIdx.x * a.prec;
   if (threadIdx.x < kPartialExtra) {
-    double sum = 0.0;
-    if (threadIdx.x < 6) {
-      sum = trash[threadIdx.x];
-    } else {
-      for (int w = 0; w < kBlock / 32; ++w) sum += red[w][threadIdx.x - 6];
-    }
+    const double sum = threadIdx.x < 6 ? trash[threadIdx.x] : red[0][threadIdx.x - 6];
     rec[a.hoff + threadIdx.x] = sum;
   }
   for (int i = threadIdx.x; i < nc; i += kBlock) {

@@ -170,6 +170,16 @@ __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// One arrival on `bar` (release at CTA scope).
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Barrier among `count` threads (a multiple of 32) on hardware barrier `id`.
+__device__ __forceinline__ void named_barrier(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
 // Bounded wait for phase `parity` of `bar`: returns false (and leaves the
 // wait) after `limit` polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long limit) {

@@ -153,6 +153,7 @@ struct Args {
   // noise
   int noise;                  // MBT_NOISE_PHILOX / _INJECTED / NONE
   uint64_t seed;
+  uint32_t philox_k0[10], philox_k1[10];   // round keys of the seed
   const float *dev;           // injected deviates: turns x 5 x npad
   long dev_turn0;             // first turn held in dev
   long dev_nturn;

@@ -76,7 +76,10 @@ __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst
   }
   float dv[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
   if (NOISE == MBT_NOISE_PHILOX) {
-    turn_normals1(a.seed, jb, (uint32_t)kb, (uint64_t)turn, dv);
+    PhiloxKeys K;
+#pragma unroll
+    for (int q = 0; q < 10; ++q) { K.k0[q] = a.philox_k0[q]; K.k1[q] = a.philox_k1[q]; }
+    turn_normals1(K, jb, (uint32_t)kb, (uint64_t)turn, dv);
   } else if (NOISE == MBT_NOISE_INJECTED) {
     const long dt = turn - a.dev_turn0;
     if (dt >= 0 && dt < a.dev_nturn) {
@@ -141,15 +144,18 @@ __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst
 }
 
 // Particle pass (K1).  Each block streams its tile through a ring of
-// kStages shared-memory stages of kChunk particles: thread 0 issues six
-// bulk loads per stage (one per coordinate array, completion on the
-// stage's mbarrier), every thread advances one particle of the chunk in
-// place, and thread 0 writes the stage back with six bulk stores before
-// refilling it.  Moments and next-turn histograms come from the updated
-// coordinates in shared memory.
-constexpr int kChunk = 256;
+// kStages shared-memory stages of kChunk particles.  Warp 8 is the
+// producer: it issues six bulk loads per stage (completion on the stage's
+// `full` mbarrier) and, once the eight compute warps have released a stage
+// (`empty` mbarrier), six bulk stores of the updated coordinates.  Compute
+// warps advance one particle per thread per chunk in place, then sum the
+// moments column-wise from the staged chunk; they synchronise only among
+// themselves (hardware barrier 1).
+constexpr int kPPT = 1;                    // particles per compute thread per chunk
+constexpr int kChunk = kPPT * kBlock;
 constexpr int kStages = 3;
-constexpr long kWaitLimit = 1L << 24;   // polls before a wait is declared failed
+constexpr int kMapThreads = kBlock + 32;   // 8 compute warps + 1 producer warp
+constexpr long kWaitLimit = 1L << 24;      // polls before a wait is declared failed
 
 // stages, kick tables and histograms
 __host__ __device__ constexpr size_t turn_map_smem(int nc) {
@@ -158,7 +164,7 @@ __host__ __device__ constexpr size_t turn_map_smem(int nc) {
 }
 
 template <bool MOVE, int NOISE, bool HISTXZ>
-__global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
+__global__ void __launch_bounds__(kMapThreads, 3) turn_map(Args a) {
   extern __shared__ __align__(128) double smem[];
   const int nc = a.ncell;
   const Tile tile = a.tiles[blockIdx.x];
@@ -170,14 +176,14 @@ __global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
   double *hx = kL + 3 * nc;
   double *hz = kL + 4 * nc;
   int *hc = reinterpret_cast<int *>(kL + 5 * nc);
-  __shared__ __align__(8) uint64_t bars[kStages];
-  __shared__ double red[kBlock / 32][12];
+  __shared__ __align__(8) uint64_t full[kStages];
+  __shared__ __align__(8) uint64_t empty[kStages];
+  __shared__ double red[12];
   __shared__ double trash[6];
   __shared__ double shift[6];
-  __shared__ int abort_flag;
 
   const bool sf = MOVE && a.selffield;
-  for (int i = threadIdx.x; i < nc; i += kBlock) {
+  for (int i = threadIdx.x; i < nc; i += kMapThreads) {
     if (sf) {
       kL[i] = a.kick[(size_t)(b * 3 + 0) * nc + i];
       kV[i] = a.kick[(size_t)(b * 3 + 1) * nc + i];
@@ -191,8 +197,10 @@ __global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
     shift[threadIdx.x] = a.shift[b * 6 + threadIdx.x];
   }
   if (threadIdx.x == 0) {
-    abort_flag = 0;
-    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kBlock / 32);
+    }
     fence_mbar_init();
   }
   __syncthreads();
@@ -200,23 +208,44 @@ __global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
   const size_t np6 = (size_t)a.npad;
   double *__restrict__ C = a.coord;
   const int nchunk = (tile.count + kChunk - 1) / kChunk;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto chunk_bytes = [&](int c) -> uint32_t {
     const int n = min(kChunk, tile.count - c * kChunk);
     return (uint32_t)(((n * 8) + 15) & ~15);
   };
-  auto issue_load = [&](int c) {
-    const int s = c % kStages;
-    const uint32_t bytes = chunk_bytes(c);
-    mbar_expect_tx(&bars[s], 6 * bytes);
-    const size_t g0 = (size_t)tile.start + (size_t)c * kChunk;
-    for (int k = 0; k < 6; ++k)
-      bulk_load(stage + (size_t)(s * 6 + k) * kChunk, C + k * np6 + g0, bytes, &bars[s]);
-  };
-  // prologue: kStages-1 chunks in flight; chunk c+kStages-1 is loaded at
-  // the end of iteration c into the stage chunk c-1 used
-  if (threadIdx.x == 0)
-    for (int c = 0; c < min(kStages - 1, nchunk); ++c) issue_load(c);
 
+  if (warp == kBlock / 32) {
+    // ---------------- producer warp
+    if (lane == 0) {
+      auto store = [&](int cc) {
+        const int s = cc % kStages;
+        if (!mbar_wait(&empty[s], (uint32_t)((cc / kStages) & 1), kWaitLimit)) atomicOr(&a.rs->error, 2);
+        if (MOVE) {
+          const uint32_t bytes = chunk_bytes(cc);
+          const size_t g0 = (size_t)tile.start + (size_t)cc * kChunk;
+          for (int k = 0; k < 6; ++k) bulk_store(C + k * np6 + g0, stage + (size_t)(s * 6 + k) * kChunk, bytes);
+          bulk_commit();
+        }
+      };
+      for (int c = 0; c < nchunk; ++c) {
+        const int s = c % kStages;
+        if (c >= kStages) {
+          store(c - kStages);              // frees stage s once the store has read it
+          if (MOVE) bulk_wait_read<0>();
+        }
+        const uint32_t bytes = chunk_bytes(c);
+        mbar_expect_tx(&full[s], 6 * bytes);
+        const size_t g0 = (size_t)tile.start + (size_t)c * kChunk;
+        for (int k = 0; k < 6; ++k)
+          bulk_load(stage + (size_t)(s * 6 + k) * kChunk, C + k * np6 + g0, bytes, &full[s]);
+      }
+      for (int cc = max(0, nchunk - kStages); cc < nchunk; ++cc) store(cc);
+      bulk_wait_all();
+    }
+    return;
+  }
+
+  // ---------------- compute warps
   const OpticConst &oc = a.oc;
   const long turn = a.rs->turn;
   const double eps_const = a.rs->Vrf0 / (oc.E0 * 1.0e3);
@@ -234,51 +263,67 @@ __global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
   const bool kick_l = sf && a.lr_kick[0];
   const bool kick_h = sf && a.lr_kick[1];
   const bool kick_v = sf && a.lr_kick[2];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int jb0 = tile.start - a.bunch_off[b];   // index of the tile's first particle in its bunch
-  int consumed = 0;
   // moments: warp w < 6 owns coordinate column w of every staged chunk
   const double col_shift = warp < 6 ? shift[warp] : 0.0;
   double col_s = 0.0, col_q = 0.0;
 
   for (int c = 0; c < nchunk; ++c) {
     const int s = c % kStages;
-    if (!mbar_wait(&bars[s], (uint32_t)((c / kStages) & 1), kWaitLimit)) abort_flag = 1;
+    if (!mbar_wait(&full[s], (uint32_t)((c / kStages) & 1), kWaitLimit)) atomicOr(&a.rs->error, 2);
     double *st = stage + (size_t)s * 6 * kChunk;
-    const int i = c * kChunk + threadIdx.x;
-    const bool live = i < tile.count;
-    double xtau = 0.0, x = 0.0, z = 0.0, eps = 0.0, xp = 0.0, zp = 0.0;
-    if (live) {
-      xtau = st[threadIdx.x]; x = st[kChunk + threadIdx.x]; z = st[2 * kChunk + threadIdx.x];
-      eps = st[3 * kChunk + threadIdx.x]; xp = st[4 * kChunk + threadIdx.x]; zp = st[5 * kChunk + threadIdx.x];
-      if (MOVE) {
-        advance_particle<NOISE>(a, oc, xtau, x, z, eps, xp, zp, rw, rwH, rwV, sf, kick_l, kick_v, kick_h, kL,
-                                kV, kH, nc, eps_const, phai0, sin_ph, cos_ph, kb, (uint32_t)(jb0 + i), turn,
-                                (size_t)tile.start + i);
-        st[threadIdx.x] = xtau; st[kChunk + threadIdx.x] = x; st[2 * kChunk + threadIdx.x] = z;
-        st[3 * kChunk + threadIdx.x] = eps; st[4 * kChunk + threadIdx.x] = xp; st[5 * kChunk + threadIdx.x] = zp;
+    // kPPT independent particles per thread: t, t + kBlock, ...
+    double v[kPPT][6];
+    bool live[kPPT];
+#pragma unroll
+    for (int u = 0; u < kPPT; ++u) {
+      const int e = u * kBlock + threadIdx.x;
+      live[u] = c * kChunk + e < tile.count;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) v[u][k] = live[u] ? st[k * kChunk + e] : 0.0;
+    }
+    if (MOVE) {
+#pragma unroll
+      for (int u = 0; u < kPPT; ++u) {
+        const int e = u * kBlock + threadIdx.x;
+        const int i = c * kChunk + e;
+        if (live[u])
+          advance_particle<NOISE>(a, oc, v[u][0], v[u][1], v[u][2], v[u][3], v[u][4], v[u][5], rw, rwH, rwV, sf,
+                                  kick_l, kick_v, kick_h, kL, kV, kH, nc, eps_const, phai0, sin_ph, cos_ph, kb,
+                                  (uint32_t)(jb0 + i), turn, (size_t)tile.start + i);
+      }
+#pragma unroll
+      for (int u = 0; u < kPPT; ++u) {
+        const int e = u * kBlock + threadIdx.x;
+        if (live[u]) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) st[k * kChunk + e] = v[u][k];
+        }
       }
     }
     // ---- binning of the next turn (out-of-range particles are rare: shared atomics)
-    if (a.selffield && live) {
-      const int ic = bin_fast(xtau, oc.sigma_tau, oc.nsigma, oc.dT, oc.inv_sigma_tau, oc.inv_dT);
-      if (ic >= 0 && ic < nc) {
-        atomicAdd(&hc[ic], 1);
-        if (HISTXZ) {
-          atomicAdd(&hx[ic], x);
-          atomicAdd(&hz[ic], z);
+    if (a.selffield) {
+#pragma unroll
+      for (int u = 0; u < kPPT; ++u) {
+        if (!live[u]) continue;
+        const double xtau = v[u][0], x = v[u][1], z = v[u][2];
+        const int ic = bin_fast(xtau, oc.sigma_tau, oc.nsigma, oc.dT, oc.inv_sigma_tau, oc.inv_dT);
+        if (ic >= 0 && ic < nc) {
+          atomicAdd(&hc[ic], 1);
+          if (HISTXZ) {
+            atomicAdd(&hx[ic], x);
+            atomicAdd(&hz[ic], z);
+          }
+        } else {
+          double *t = trash + (ic < 0 ? 0 : 3);
+          atomicAdd(&t[0], 1.0);
+          atomicAdd(&t[1], x);
+          atomicAdd(&t[2], z);
         }
-      } else {
-        double *t = trash + (ic < 0 ? 0 : 3);
-        atomicAdd(&t[0], 1.0);
-        atomicAdd(&t[1], x);
-        atomicAdd(&t[2], z);
       }
     }
     if (MOVE) fence_proxy_async();
-    __syncthreads();
-    consumed = c + 1;
-    if (abort_flag) break;
+    named_barrier(1, kBlock);
     // ---- moments (statistics.c:91-128): shifted sums of the updated chunk,
     //      one coordinate column per warp (the bulk store only reads it too)
     if (warp < 6) {
@@ -292,43 +337,21 @@ __global__ void __launch_bounds__(kBlock, 3) turn_map(Args a) {
         col_q += d * d;
       }
     }
-    if (threadIdx.x == 0) {
-      if (MOVE) {
-        const uint32_t bytes = chunk_bytes(c);
-        const size_t g0 = (size_t)tile.start + (size_t)c * kChunk;
-        for (int k = 0; k < 6; ++k) bulk_store(C + k * np6 + g0, st + (size_t)k * kChunk, bytes);
-        bulk_commit();
-      }
-      if (c + kStages - 1 < nchunk) {
-        // the stage of chunk c-1: its store (the older of the two pending
-        // groups) must have finished reading shared memory
-        if (MOVE) bulk_wait_read<1>();
-        issue_load(c + kStages - 1);
-      }
-    }
-  }
-  if (threadIdx.x == 0) {
-    if (abort_flag) {
-      // drain the loads still in flight (bounded), then report
-      // chunks consumed-1 .. consumed+kStages-3 have loads issued
-      for (int c = consumed - 1; c < min(consumed - 2 + kStages, nchunk); ++c)
-        mbar_wait(&bars[c % kStages], (uint32_t)((c / kStages) & 1), kWaitLimit);
-      atomicOr(&a.rs->error, 2);
-    }
-    bulk_wait_all();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
   }
   // column sums -> block sums, in a fixed order
   {
     const double vs = warp_sum(col_s), vq = warp_sum(col_q);
     if (lane == 0 && warp < 6) {
-      red[0][warp] = vs;
-      red[0][6 + warp] = vq;
+      red[warp] = vs;
+      red[6 + warp] = vq;
     }
   }
-  __syncthreads();
+  named_barrier(1, kBlock);
   double *rec = a.part + (size_t)blockIdx.x * a.prec;
   if (threadIdx.x < kPartialExtra) {
-    const double sum = threadIdx.x < 6 ? trash[threadIdx.x] : red[0][threadIdx.x - 6];
+    const double sum = threadIdx.x < 6 ? trash[threadIdx.x] : red[threadIdx.x - 6];
     rec[a.hoff + threadIdx.x] = sum;
   }
   for (int i = threadIdx.x; i < nc; i += kBlock) {

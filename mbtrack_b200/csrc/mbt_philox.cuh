@@ -48,6 +48,36 @@ __device__ __forceinline__ void box_muller2(uint32_t a, uint32_t b, float &n0, f
   n1 = r * s;
 }
 
+// Philox4x32-10 with the ten round keys given (they depend on the seed
+// only, so a launch computes them once).
+struct PhiloxKeys {
+  uint32_t k0[10], k1[10];
+};
+
+__host__ __device__ inline PhiloxKeys philox_keys(uint64_t seed) {
+  PhiloxKeys K;
+  uint32_t a = (uint32_t)seed, b = (uint32_t)(seed >> 32);
+  for (int i = 0; i < 10; ++i) {
+    K.k0[i] = a;
+    K.k1[i] = b;
+    a += 0x9E3779B9u;
+    b += 0xBB67AE85u;
+  }
+  return K;
+}
+
+__device__ __forceinline__ U4 philox4x32_10k(U4 c, const PhiloxKeys &K) {
+#pragma unroll
+  for (int i = 0; i < 10; ++i) c = philox_round(c, K.k0[i], K.k1[i]);
+  return c;
+}
+
+// Uniform (0, 1] from the top 23 bits of a word, built in the mantissa of
+// a float in [1, 2) (exact, no integer conversion).
+__device__ __forceinline__ float u01_open0(uint32_t w) {
+  return 2.0f - __uint_as_float(0x3F800000u | (w >> 9));
+}
+
 // Two normals from a 24-bit radius word and an 18-bit angle word, with the
 // hardware approximations of log, sqrt and sin/cos (absolute errors near
 // 2^-21: below the single-precision resolution of the reference's deviates).
@@ -63,20 +93,32 @@ __device__ __forceinline__ void box_muller_bits(uint32_t r24, uint32_t a18, floa
   n1 = r * s;
 }
 
+// Two normals from a radius uniform in (0, 1] and an angle word whose top
+// 18 bits give the angle over [-pi, pi) (both signs flip: the pair is still
+// an independent standard normal pair).
+__device__ __forceinline__ void box_muller_u(float u1, uint32_t angle_word, float &n0, float &n1) {
+  const float th = (float)((int)(angle_word >> 14) - 131072) * 2.396844980841821872e-05f;
+  const float r = __fsqrt_rn(-2.0f * __logf(u1));
+  float s, c;
+  __sincosf(th, &s, &c);
+  n0 = r * c;
+  n1 = r * s;
+}
+
 // The five deviates one particle draws per turn, in the reference's roles
 // g[0] energy, g[1] z, g[2] z', g[3] x, g[4] x', from ONE Philox call: its
-// 128 bits give three (24-bit radius, 18-bit angle) pairs.
-__device__ __forceinline__ void turn_normals1(uint64_t seed, uint32_t particle, uint32_t bucket,
+// 128 bits give three (23-bit radius, 18-bit angle) pairs.
+__device__ __forceinline__ void turn_normals1(const PhiloxKeys &K, uint32_t particle, uint32_t bucket,
                                               uint64_t turn, float g[5]) {
-  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
   const U4 c0 = {particle, bucket, (uint32_t)turn, ((uint32_t)(turn >> 32) << 1) | 0u};
-  const U4 r = philox4x32_10(c0, k0, k1);
+  const U4 r = philox4x32_10k(c0, K);
   float n5;
-  box_muller_bits(r.x >> 8, r.y >> 14, g[0], g[1]);
-  box_muller_bits(r.z >> 8, r.w >> 14, g[2], g[3]);
-  const uint32_t rr = ((r.x & 0xFFu) << 16) | ((r.y & 0x3FFFu) << 2) | (r.z & 0x3u);
-  const uint32_t aa = (((r.z >> 2) & 0x3Fu) << 12) | (r.w & 0xFFFu);
-  box_muller_bits(rr, aa, g[4], n5);
+  box_muller_u(u01_open0(r.x), r.y, g[0], g[1]);
+  box_muller_u(u01_open0(r.z), r.w, g[2], g[3]);
+  // third pair from the low bits: radius 9 + 14 = 23 bits, angle 18 bits
+  const uint32_t rr = ((r.x & 0x1FFu) << 23) | ((r.y & 0x3FFFu) << 9);
+  const uint32_t aa = (((r.z & 0x1FFu) << 9) | (r.w & 0x1FFu)) << 14;
+  box_muller_u(u01_open0(rr), aa, g[4], n5);
 }
 
 // Five deviates from two Philox calls (full 24-bit uniforms for both

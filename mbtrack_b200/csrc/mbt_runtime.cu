@@ -168,7 +168,7 @@ void launch_map(mbt_ctx *c) {
                          (int)mbt::turn_map_smem(MBT_MAX_NCELL));
     attr_set = true;
   }
-  mbt::turn_map<MOVE, NOISE, HISTXZ><<<c->ntile, mbt::kBlock, sm, c->stream>>>(c->a);
+  mbt::turn_map<MOVE, NOISE, HISTXZ><<<c->ntile, mbt::kMapThreads, sm, c->stream>>>(c->a);
 }
 
 template <bool MOVE>
@@ -326,6 +326,10 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   a.E0 = p->E0;
   a.noise = noise_mode;
   a.seed = seed;
+  {
+    const mbt::PhiloxKeys K = mbt::philox_keys(seed);
+    for (int q = 0; q < 10; ++q) { a.philox_k0[q] = K.k0[q]; a.philox_k1[q] = K.k1[q]; }
+  }
 
   std::vector<int> np_v(c->np), kb_v(c->bucket);
   std::vector<double> ibunch(p->nharm, 0.0), factg(nbunch);

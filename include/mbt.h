@@ -225,6 +225,13 @@ int mbt_set_deviates(mbt_ctx *ctx, const float *dev, long nturns);
  * all bunches.  stats (may be NULL): nturns x nbunch x 12 doubles. */
 int mbt_run_turns(mbt_ctx *ctx, long nturns, double *stats);
 
+/* As mbt_run_turns, also returning the amplitude invariants of every turn
+ * (weak_bunch_calc_ampinv statistics.c:163-195, which the reference
+ * evaluates every NrevMon turns): ampinv is nturns x nbunch x 6 doubles,
+ * <gamma u^2 + 2 alpha u u' + beta u'^2> over the particles for
+ * u = LON, HOR, VER, then the same of the centroid (ampinv_cm). */
+int mbt_run_turns_ampinv(mbt_ctx *ctx, long nturns, double *stats, double *ampinv);
+
 /* Same loop, but particles come from and return to host buffers in the
  * same call (one soa6 block per bunch, bunch after bunch): the call a
  * host-resident caller makes.  particles may be pinned memory. */

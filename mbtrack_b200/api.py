@@ -39,6 +39,7 @@ SIGNATURES = {
     "mbt_prepare": (ctypes.c_int, [_vp, _vp]),
     "mbt_set_deviates": (ctypes.c_int, [_vp, _vp, ctypes.c_long]),
     "mbt_run_turns": (ctypes.c_int, [_vp, ctypes.c_long, _vp]),
+    "mbt_run_turns_ampinv": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp]),
     "mbt_track": (ctypes.c_int, [_vp, _vp, ctypes.c_long, _vp]),
     "mbt_profile_turns": (ctypes.c_int, [_vp, ctypes.c_long, _vp]),
     "mbt_get_state": (ctypes.c_int, [_vp, _P(MbtState)]),
@@ -200,6 +201,13 @@ class Tracker:
         s = np.zeros(nturns * self.nb * 12) if stats else None
         _check(lib().mbt_run_turns(self.h, nturns, _ptr(s)), self.h)
         return None if s is None else s.reshape(nturns, self.nb, 12)
+
+    def run_ampinv(self, nturns):
+        """Statistics and amplitude invariants of every turn."""
+        s = np.zeros(nturns * self.nb * 12)
+        ai = np.zeros(nturns * self.nb * 6)
+        _check(lib().mbt_run_turns_ampinv(self.h, nturns, _ptr(s), _ptr(ai)), self.h)
+        return s.reshape(nturns, self.nb, 12), ai.reshape(nturns, self.nb, 6)
 
     def track(self, particles, nturns, stats=None):
         if particles.dtype != np.float64 or not particles.flags.c_contiguous or \

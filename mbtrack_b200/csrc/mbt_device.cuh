@@ -21,7 +21,7 @@ namespace mbt {
 
 constexpr int kMaxLr = 8;          // MBT_MAX_LR
 constexpr int kMaxAhc = 8;         // MBT_MAX_AHC
-constexpr int kPartialExtra = 18;  // 6 out-of-range values + 12 moment sums
+constexpr int kPartialExtra = 20;  // 6 out-of-range values + 12 moment sums + 2 cross sums
 constexpr int kBlock = 256;        // threads per block of every kernel
 constexpr int kRwGroup = 4;        // bunches per resistive-wall sum block
 constexpr int kRwSplit = 4;        // parts of the resistive-wall history per bunch
@@ -31,6 +31,7 @@ constexpr int kTrLowN = 0, kTrLowX = 1, kTrLowZ = 2;
 constexpr int kTrHighN = 3, kTrHighX = 4, kTrHighZ = 5;
 constexpr int kMomSum = 6;     // 6 shifted sums
 constexpr int kMomSq = 12;     // 6 shifted sums of squares
+constexpr int kMomCross = 18;  // shifted sums of x x' and z z'
 
 struct Tile {
   int bunch;   // bunch index
@@ -63,6 +64,7 @@ struct OpticConst {
   // binning (transform_weak.c:611-613)
   double sigma_tau, nsigma, dT;
   double inv_sigma_tau, inv_dT;     // for the fast exact bin index
+  double gammaL, alphaL, betaL;     // Twiss of the LON row of ring_t (0 unless set)
   int ncell;
   // sin and cos of the betatron phase advances 2 pi Q (PsiV0, PsiH0)
   double sin_psiV0, cos_psiV0, sin_psiH0, cos_psiH0;
@@ -120,6 +122,7 @@ struct Args {
   double *kick;               // nbunch x 3 x ncell: L, V, H kick tables
   double *rw_part;            // nbunch x kRwSplit x 2: partial RW kicks (HOR, VER)
   double *stats;              // stats_cap x nbunch x 12
+  double *ampinv;             // stats_cap x nbunch x 6: ampinv[3], ampinv_cm[3]
   int stats_cap;
   // long-range resonators
   int nlr;

@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kMapThreads, 3) turn_map(Args a) {
   int *hc = reinterpret_cast<int *>(kL + 5 * nc);
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ __align__(8) uint64_t empty[kStages];
-  __shared__ double red[12];
+  __shared__ double red[14];
   __shared__ double trash[6];
   __shared__ double shift[6];
 
@@ -264,8 +264,11 @@ __global__ void __launch_bounds__(kMapThreads, 3) turn_map(Args a) {
   const bool kick_h = sf && a.lr_kick[1];
   const bool kick_v = sf && a.lr_kick[2];
   const int jb0 = tile.start - a.bunch_off[b];   // index of the tile's first particle in its bunch
-  // moments: warp w < 6 owns coordinate column w of every staged chunk
+  // moments: warp w < 6 owns coordinate column w of every staged chunk;
+  // warps 6 and 7 sum the cross products x x' and z z' (columns 1*4, 2*5)
   const double col_shift = warp < 6 ? shift[warp] : 0.0;
+  const int cx = warp == 6 ? 1 : 2;
+  const double sh_a = warp >= 6 ? shift[cx] : 0.0, sh_b = warp >= 6 ? shift[cx + 3] : 0.0;
   double col_s = 0.0, col_q = 0.0;
 
   for (int c = 0; c < nchunk; ++c) {
@@ -326,15 +329,22 @@ __global__ void __launch_bounds__(kMapThreads, 3) turn_map(Args a) {
     named_barrier(1, kBlock);
     // ---- moments (statistics.c:91-128): shifted sums of the updated chunk,
     //      one coordinate column per warp (the bulk store only reads it too)
+    const int nlive = min(kChunk, tile.count - c * kChunk);
     if (warp < 6) {
       const double *col = st + (size_t)warp * kChunk;
-      const int nlive = min(kChunk, tile.count - c * kChunk);
 #pragma unroll
       for (int q = 0; q < kChunk / 32; ++q) {
         const int e = q * 32 + lane;
         const double d = e < nlive ? col[e] - col_shift : 0.0;
         col_s += d;
         col_q += d * d;
+      }
+    } else {
+      const double *ca = st + (size_t)cx * kChunk, *cb = st + (size_t)(cx + 3) * kChunk;
+#pragma unroll
+      for (int q = 0; q < kChunk / 32; ++q) {
+        const int e = q * 32 + lane;
+        col_s += e < nlive ? (ca[e] - sh_a) * (cb[e] - sh_b) : 0.0;
       }
     }
     __syncwarp();
@@ -343,9 +353,13 @@ __global__ void __launch_bounds__(kMapThreads, 3) turn_map(Args a) {
   // column sums -> block sums, in a fixed order
   {
     const double vs = warp_sum(col_s), vq = warp_sum(col_q);
-    if (lane == 0 && warp < 6) {
-      red[warp] = vs;
-      red[6 + warp] = vq;
+    if (lane == 0) {
+      if (warp < 6) {
+        red[warp] = vs;
+        red[6 + warp] = vq;
+      } else {
+        red[12 + (warp - 6)] = vs;
+      }
     }
   }
   named_barrier(1, kBlock);
@@ -422,6 +436,34 @@ __global__ void __launch_bounds__(kBlock) bunch_reduce(Args a, int mode, double 
                       : stats_init + (size_t)b * 12;
     row[col] = mean;
     row[col + 3] = rms;
+  }
+  __syncthreads();
+  // amplitude invariants (weak_bunch_calc_ampinv statistics.c:163-195):
+  // <gamma u^2 + 2 alpha u u' + beta u'^2> over particles, and the same of
+  // the centroid, from the shifted first and second moments
+  if (threadIdx.x < 3) {
+    const int pl = threadIdx.x;
+    const bool tracked = pl == 0 || (pl == 1 ? a.oc.track_h : a.oc.track_v);
+    double ai = 0.0, aic = 0.0;
+    if (tracked && N > 0) {
+      const double g = pl == 0 ? a.oc.gammaL : (pl == 1 ? a.oc.gammaH : a.oc.gammaV);
+      const double al = pl == 0 ? a.oc.alphaL : (pl == 1 ? a.oc.alphaH : a.oc.alphaV);
+      const double be = pl == 0 ? a.oc.betaL : (pl == 1 ? a.oc.betaH : a.oc.betaV);
+      const double m = mean6[pl], mp = mean6[3 + pl];
+      const double su = ex[kMomSum + pl] / N, sp = ex[kMomSum + 3 + pl] / N;
+      const double vu = ex[kMomSq + pl] / N - su * su;         // variance of u
+      const double vp = ex[kMomSq + 3 + pl] / N - sp * sp;     // variance of u'
+      const double cuv = pl == 0 ? 0.0 : ex[kMomCross + pl - 1] / N - su * sp;
+      // (the reference never sets the LON Twiss values, so its LON
+      // invariants are 0; no LON cross moment is kept)
+      aic = g * m * m + 2.0 * al * m * mp + be * mp * mp;
+      ai = g * (vu + m * m) + 2.0 * al * (cuv + m * mp) + be * (vp + mp * mp);
+    }
+    double *row = (mode == kReduceTurn) ? a.ampinv + ((size_t)(turn % a.stats_cap) * a.nbunch + b) * 6 : nullptr;
+    if (row) {
+      row[pl] = ai;
+      row[3 + pl] = aic;
+    }
   }
   if (threadIdx.x == 0 && a.selffield) {
     atomicAdd(&a.rs->trash_low, (int)ex[kTrLowN]);

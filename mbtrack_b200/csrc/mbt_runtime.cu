@@ -434,6 +434,7 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   oc.sigma_tau = p->sigma_tau;
   oc.nsigma = p->nsigma;
   oc.dT = p->dT;
+  oc.gammaL = p->gamma1[0]; oc.alphaL = p->alpha1[0]; oc.betaL = p->beta1[0];
   oc.inv_sigma_tau = p->sigma_tau > 0 ? 1.0 / p->sigma_tau : 0.0;
   oc.inv_dT = p->dT > 0 ? 1.0 / p->dT : 0.0;
   oc.sin_psiV0 = sin(oc.psiV0);
@@ -474,6 +475,7 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   a.stats_cap = 256;
   rc = rc ? rc : dalloc(c, &a.stats, (size_t)a.stats_cap * nbunch * 12);
   rc = rc ? rc : dalloc(c, &c->stats_init, (size_t)nbunch * 12);
+  rc = rc ? rc : dalloc(c, &a.ampinv, (size_t)a.stats_cap * nbunch * 6);
   LrConst *lr_d = nullptr;
   rc = rc ? rc : dupload(c, &lr_d, c->lr.empty() ? nullptr : c->lr.data(), c->lr.size());
   a.lr = lr_d;
@@ -672,7 +674,7 @@ int mbt_set_deviates(mbt_ctx *c, const float *dev, long nturns) {
   return 0;
 }
 
-static int run_core(mbt_ctx *c, long nturns, double *stats, bool use_graph) {
+static int run_core(mbt_ctx *c, long nturns, double *stats, double *ampinv, bool use_graph) {
   if (!c->prepared) return fail(c, MBT_ERR_STATE, "mbt_prepare must come first");
   RingState rs;
   CK(cudaMemcpy(&rs, c->a.rs, sizeof rs, cudaMemcpyDeviceToHost));
@@ -696,6 +698,9 @@ static int run_core(mbt_ctx *c, long nturns, double *stats, bool use_graph) {
     if (stats)
       CK(cudaMemcpyAsync(stats + (size_t)done * c->nbunch * 12, c->a.stats + (size_t)slot * c->nbunch * 12,
                          (size_t)chunk * c->nbunch * 12 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (ampinv)
+      CK(cudaMemcpyAsync(ampinv + (size_t)done * c->nbunch * 6, c->a.ampinv + (size_t)slot * c->nbunch * 6,
+                         (size_t)chunk * c->nbunch * 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     done += chunk;
     turn += chunk;
   }
@@ -710,7 +715,12 @@ static int run_core(mbt_ctx *c, long nturns, double *stats, bool use_graph) {
 
 int mbt_run_turns(mbt_ctx *c, long nturns, double *stats) {
   if (!c || nturns < 0) return MBT_ERR_INVALID;
-  return run_core(c, nturns, stats, true);
+  return run_core(c, nturns, stats, nullptr, true);
+}
+
+int mbt_run_turns_ampinv(mbt_ctx *c, long nturns, double *stats, double *ampinv) {
+  if (!c || nturns < 0) return MBT_ERR_INVALID;
+  return run_core(c, nturns, stats, ampinv, true);
 }
 
 int mbt_track(mbt_ctx *c, double *particles, long nturns, double *stats) {
@@ -718,7 +728,7 @@ int mbt_track(mbt_ctx *c, double *particles, long nturns, double *stats) {
   int r = mbt_load_all(c, particles);
   if (r) return r;
   if (!c->prepared) { r = mbt_prepare(c, nullptr); if (r) return r; }
-  r = run_core(c, nturns, stats, true);
+  r = run_core(c, nturns, stats, nullptr, true);
   if (r) return r;
   return mbt_get_all(c, particles);
 }

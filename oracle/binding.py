@@ -152,6 +152,12 @@ class Oracle:
         self.lib.orc_trash(self.h, ib, ctypes.byref(lo), ctypes.byref(hi))
         return lo.value, hi.value
 
+    def ampinv(self, ib):
+        out = np.zeros(6)
+        self.lib.orc_ampinv.argtypes = [_vp, ctypes.c_int, _vp]
+        self.lib.orc_ampinv(self.h, ib, _ptr(out))
+        return out
+
     def histograms(self, ib):
         n = self.p.ncell
         arr = [np.zeros(n) for _ in range(6)]
@@ -271,3 +277,9 @@ class Reference:
         lo, hi = ctypes.c_int(), ctypes.c_int()
         self.lib.refh_trash(ib, ctypes.byref(lo), ctypes.byref(hi))
         return lo.value, hi.value
+
+    def ampinv(self, ib):
+        out = np.zeros(6)
+        self.lib.refh_ampinv.argtypes = [ctypes.c_int, _vp]
+        self.lib.refh_ampinv(ib, _ptr(out))
+        return out

@@ -972,3 +972,29 @@ void orc_be_field_n(long n, const double *dx, const double *dy,
     ey[i] = -factdQ * (u1[0] - e * u2[0]);
   }
 }
+
+/* weak_bunch_calc_ampinv, statistics.c:163-195: per tracked plane the mean
+ * of gamma u^2 + 2 alpha u u' + beta u'^2 over the particles (ampinv) and
+ * the same of the centroid of the last statistics (ampinv_cm). */
+void orc_ampinv(const orc_ctx *o, int ib, double *out6)
+{
+  const orc_bunch *b = &o->b[ib];
+  const mbt_params *p = &o->p;
+  int plane, jp;
+  for (plane = 0; plane < 3; plane++) {
+    out6[plane] = 0.0;
+    out6[3 + plane] = 0.0;
+    if (!p->track_plane[plane]) continue;
+    {
+      const double *u = b->c[plane], *up = b->c[3 + plane];
+      double s = 0.0;
+      const double pos = b->stats[0 + plane], slope = b->stats[6 + plane];
+      for (jp = 0; jp < b->np; jp++)
+        s += p->gamma1[plane] * (u[jp] * u[jp]) + 2.0 * p->alpha1[plane] * u[jp] * up[jp]
+             + p->beta1[plane] * (up[jp] * up[jp]);
+      out6[plane] = s / ((double) b->np);
+      out6[3 + plane] = p->gamma1[plane] * (pos * pos) + 2.0 * p->alpha1[plane] * pos * slope
+                        + p->beta1[plane] * (slope * slope);
+    }
+  }
+}

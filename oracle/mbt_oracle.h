@@ -59,6 +59,10 @@ long orc_run(orc_ctx *o, long nturns, double *stats, const float *dev_in,
 long orc_deviates_per_turn(const orc_ctx *o);
 
 void orc_state(const orc_ctx *o, int ib, double *vrf_phi, double *phasor_lon);
+
+/* Amplitude invariants of bunch ib (statistics.c:163-195): ampinv[3],
+ * ampinv_cm[3]. */
+void orc_ampinv(const orc_ctx *o, int ib, double *out6);
 void orc_trash(const orc_ctx *o, int ib, int *low, int *high);
 
 /* Histograms of bunch ib from the last binning (clamped and dropped). */

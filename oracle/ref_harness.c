@@ -598,3 +598,14 @@ int refh_fill_params(mbt_params *p)
   }
   return 0;
 }
+
+/* weak_bunch_calc_ampinv of the reference on bunch ib. */
+void refh_ampinv(int ib, double *out6)
+{
+  int k;
+  weak_bunch_calc_ampinv(&W[ib].bunch, &track);
+  for (k = 0; k < 3; k++) {
+    out6[k] = W[ib].bunch.stats.ampinv.v[k];
+    out6[3 + k] = W[ib].bunch.stats.ampinv_cm.v[k];
+  }
+}

@@ -162,3 +162,25 @@ def test_errors_are_reported(cuda_device, libmbt):
     with pytest.raises(api.MbtError) as e:
         t.load_particles(0, np.zeros(6 * 3))
     assert e.value.code == -1
+
+
+def test_amplitude_invariants(cuda_device, libmbt):
+    """ampinv / ampinv_cm (statistics.c:163-195) of every turn, from the
+    device moments, against the oracle after the same turns."""
+    c = Case("single_noiseoff")
+    t = tracker_for(c)
+    init = c.bunch_slices(c.init)
+    t.load_particles(0, init[0])
+    t.prepare()
+    o = Oracle(c.params, c.bucket, c.np, c.ib, c.Gl, c.Gv, c.Gh)
+    o.set_particles(0, init[0])
+    o.prepare()
+    for turns in (1, 9):
+        st, ai = t.run_ampinv(turns)
+        o.run(turns)
+        ref = o.ampinv(0)
+        got = ai[-1, 0]
+        for k in (1, 2):                       # HOR, VER (LON Twiss are 0 in the reference)
+            assert abs(got[k] - ref[k]) <= 1e-10 * abs(ref[k])
+            assert abs(got[3 + k] - ref[3 + k]) <= 1e-10 * abs(ref[k])
+        assert got[0] == 0.0 and got[3] == 0.0

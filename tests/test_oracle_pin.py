@@ -1,0 +1,43 @@
+"""Live pin of the oracle against the reference's own sources (compiled
+unmodified into oracle/_ref/libmbtref.so).  Needs the reference tree, so it
+runs in the build container; the committed fixtures carry the same pin to
+machines without it (tests/test_oracle_golden.py)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import binding
+from oracle.binding import Oracle, Reference
+from tests.util import small_conf
+
+pytestmark = pytest.mark.skipif(not (binding.reference_available() or os.path.exists(binding.REF_SO)),
+                                reason="reference sources not present")
+
+
+def _pair(path):
+    R = Reference(path)
+    p = R.params()
+    st0 = R.prepare()
+    p = R.params()
+    Gl, Gv, Gh, _ = R.greens()
+    O = Oracle(p, R.bucket, R.np, R.ib, Gl, Gv, Gh)
+    O.generate_beam()
+    assert np.array_equal(O.prepare(), st0)
+    return R, O
+
+
+@pytest.mark.parametrize("conf,over,turns", [
+    ("single_bunch.conf", {"Np": 600, "xxCM_offset": 0.05, "EnableQuantum": 1}, 15),
+    ("uniform_fill.conf", {"Np": 40, "Nmlt": 2, "xxCM_offset": 0.05}, 3),
+    ("feedback_hc.conf", {}, 12),
+])
+def test_oracle_is_the_reference(tmp_path, conf, over, turns):
+    R, O = _pair(small_conf(tmp_path, conf, **over))
+    sr = R.run(turns)
+    so = O.run(turns)
+    assert np.array_equal(sr, so)
+    for i in range(R.nb):
+        assert np.array_equal(R.get_particles(i), O.get_particles(i))
+        assert np.array_equal(R.ampinv(i), O.ampinv(i))
+    assert np.array_equal(R.state(0)[0], O.state(0)[0])

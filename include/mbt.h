@@ -43,6 +43,7 @@ extern "C" {
 #define MBT_ERR_STATE       -5   /* call made in the wrong order */
 #define MBT_ERR_TIMEOUT     -6   /* a bounded device wait gave up */
 #define MBT_ERR_NODEVICE    -7   /* no CUDA device: libmbt has no CPU path */
+#define MBT_ERR_IO          -8   /* an output file could not be opened or written */
 
 #define MBT_LON 0
 #define MBT_HOR 1
@@ -168,7 +169,40 @@ const char *mbt_config_error(void);
 /* sizeof(mbt_params) as compiled into the library (binding check). */
 size_t mbt_params_size(void);
 
+/* What the reference's output writers read from tracking_t and
+ * bunch_macroparticle_model_t (read_conf_file input.c:298-355, 547-549,
+ * 811-844; e_beam_setup input.c:1316-1427; e_beam_fileread :1445-1512). */
+typedef struct mbt_output_cfg {
+  char   jobtitle[80];          /* [tracking] jobtitle (first word, "%s") */
+  char   gendst_file[3][1024];  /* [distribution] gendst_datafile_LON/HOR/VER */
+  long   nrev_scan;             /* NrevScan; NrevTot + 1 without a scan */
+  long   nrev_potentials_out;   /* NrevPotentialsOut (0 when absent) */
+  int    ampinv_out;            /* EnableAmpinv_out (0 when absent) */
+  double scan_start;            /* scan value printed in the statistics files */
+  int    n_out;                 /* tracking_t.Nbunch_out */
+} mbt_output_cfg;
+
+/* Output settings of an mbtrack .conf file.  bunch_out (nharm ints, or
+ * NULL) receives the bucket numbers of the output bunches
+ * (tracking_t.bunch_out): the fixed lists of e_beam_setup for the named
+ * fillings, the third column of a filling file. */
+int mbt_config_output(const char *conf_path, mbt_output_cfg *o, int *bunch_out);
+
+/* Initial coordinates of the bunch in `bucket`, identical to the
+ * reference's generated distribution (weak_generate_bunch_distribution
+ * bunch_weak.c:173-292, weak_bunch_normal_distribution :86-105): per
+ * tracked plane, pos = offset + sgm g1, slope = offset + sgm g2 +
+ * correlate (pos - offset), g = sum of 12 glibc rand() uniforms - 6
+ * (c_fnorm bunch.c:379-405), the generator seeded with iseed[plane] +
+ * bucket as one MPI worker process seeds it.  soa6: 6 np doubles (host).
+ * Reentrant: bunches may be generated on several host threads. */
+int mbt_reference_beam(const mbt_params *p, int bucket, int np, double *soa6);
+
 /* ---- context --------------------------------------------------------- */
+
+/* Make CUDA device `device` current for the calling thread: the device of
+ * the contexts it creates next. */
+int mbt_use_device(int device);
 
 /* Create a tracking context on the current CUDA device.
  * nbunch filled bunches; bucket[i] is the bucket number of bunch i
@@ -206,6 +240,25 @@ int mbt_generate_beam(mbt_ctx *ctx, uint64_t seed);
  * next turn on the device) is included in the copy. */
 int mbt_get_particles(mbt_ctx *ctx, int ibunch, double *soa6, int np);
 int mbt_get_all(mbt_ctx *ctx, double *soa6_all);
+
+/* Statistics of the current coordinates, pending resistive-wall kick
+ * included: what weak_bunch_calc_statistics gives after the last turn
+ * (worker_weakweak.c:396-404).  stats: nbunch x 12 doubles (host). */
+int mbt_get_stats(mbt_ctx *ctx, double *stats);
+
+/* Record, on every turn, the potential terms the following turn applies to
+ * up to MBT_MAX_WATCH bunches (the reference prints them for its output
+ * bunches, transform_weak.c:735-768).  Call before mbt_prepare. */
+#define MBT_MAX_WATCH 16
+int mbt_watch_potentials(mbt_ctx *ctx, int n, const int *ibunch);
+
+/* Potential terms of watched bunch ibunch for the next turn: 7 x ncell
+ * doubles, factG GL1 (short-range longitudinal wake potential), the
+ * longitudinal long-range wake, fnp (macroparticles per bin), -factG
+ * GlambdaV, dipoleV, -factG GlambdaH, dipoleH (transform_weak.c:757-763).
+ * After mbt_prepare they belong to turn 0; after turn t, to turn t + 1.
+ * The RF voltage and phase of that turn's potentials are mbt_get_state's. */
+int mbt_get_potentials(mbt_ctx *ctx, int ibunch, double *pot);
 
 /* Initial binning, statistics, long-range wake and RF-feedback
  * initialisation and resistive-wall history fill
@@ -315,6 +368,89 @@ int mbt_bunch_moments_dev_noalloc(int np, const double *coord_dev,
                                   int ncell, const int track_plane[3],
                                   double *stats, double *hist_dev,
                                   void *stream);
+
+/* ---- output files (C host; the reference's text formats) ------------- */
+
+/* A writer produces, in work_path, the files the reference's manager and
+ * output workers write for a weak-weak run, byte for byte in the
+ * reference's formats, from the statistics libmbt returns:
+ *   mean_bunch_all.dat      all-bunch turn averages (manager_weakweak.c:104-127,
+ *                           :291-302; bunch_stats_fprintf bunch.c:792-804)
+ *   mean_bunch_<kb>.dat     per output bunch (worker_weakweak.c:225-234,
+ *                           :293-302; worker_weak_stat_output bunch.c:773-789)
+ *   ampinv_<P>_<rev>.dat    every NrevMon turns when EnableAmpinv_out
+ *                           (bunch_weak_writeout_ampinv bunch.c:588-640)
+ *   mean_bunch_end.dat      end statistics (manager_weakweak.c:307-331)
+ *   bunchbybunch_<P>.dat    centroid history (weak_bunch_writeout_tbtbbb
+ *                           bunch_weak.c:343-387)
+ *   ampinv_<P>_mean.dat     (weak_bunch_writeout_mean_ampinv bunch_weak.c:390-447)
+ *   wakes.dat               short-range Green's functions (worker_weakweak.c:96-106)
+ *   dipoles_history.dat     resistive-wall dipole ring buffer
+ *                           (worker_weakweak.c:418-438)
+ *   gendst_datafile_*       end distribution of the first output bunch
+ *                           (weak_writeout_bunch_distribution bunch_weak.c:296-332).
+ * Numbers go through the reference's printf formats, so a run whose
+ * statistics agree with the reference's to printing precision gives
+ * identical files.
+ *
+ * The reference prints the per-monitor ampinv files and ampinv_<P>_mean.dat
+ * from its history array indexed by monitor number plus bucket number
+ * (bunch.c:599-601, bunch_weak.c:415-428): bunch jb of monitor m shows the
+ * entry m + jb (m Nbunch + jb for the mean), not its own.  By default the
+ * writer reproduces that indexing, printing 0 where the reference reads
+ * past its array; MBT_WRITER_OWN_AMPINV writes each bunch's own values. */
+#define MBT_WRITER_OWN_AMPINV 1
+
+typedef struct mbt_writer mbt_writer;
+
+/* Open a writer for a run of nbunch bunches in buckets bucket[] with
+ * currents ib[] [A]; bunch_out[o->n_out] lists the output buckets.
+ * work_path is used as the reference uses track.work_path (joined with
+ * "/"; the reference's default is "work/").  Creates mean_bunch_all.dat
+ * and the mean_bunch_<kb>.dat files. */
+int mbt_writer_open(const char *work_path, const mbt_params *p,
+                    const mbt_output_cfg *o, const int *bunch_out,
+                    int nbunch, const int *bucket, const double *ib,
+                    int flags, mbt_writer **out);
+
+/* wakes.dat from the short-range Green's functions (p->ncell each). */
+int mbt_writer_wakes(mbt_writer *w, const double *Gl, const double *Gv,
+                     const double *Gh);
+
+/* Initial statistics (nbunch x 12, as mbt_prepare returns them): the
+ * header and first line of every statistics file. */
+int mbt_writer_begin(mbt_writer *w, const double *init_stats);
+
+/* The next nturns turns: stats nturns x nbunch x 12 and ampinv
+ * nturns x nbunch x 6 (mbt_run_turns_ampinv; ampinv may be NULL when no
+ * turn of the block is a monitor turn). */
+int mbt_writer_turns(mbt_writer *w, long nturns, const double *stats,
+                     const double *ampinv);
+
+/* After the last turn: end statistics (mbt_get_stats) into
+ * mean_bunch_end.dat, and the history files. */
+int mbt_writer_end(mbt_writer *w, const double *end_stats);
+
+/* 1 when the reference prints the potentials of turn rev (0-based) to
+ * potentials_bunch_<kb>.dat (transform_weak.c:735), else 0. */
+int mbt_writer_potentials_due(const mbt_writer *w, long rev);
+
+/* Potentials of output bunch ibunch at the start of turn rev: pot as
+ * mbt_get_potentials returns it after rev turns, vrf0 [MV] and phai0 the
+ * RF voltage and phase mbt_get_state reports then. */
+int mbt_writer_potentials(mbt_writer *w, int ibunch, long rev,
+                          const double *pot, double vrf0, double phai0);
+
+/* The end distribution of bunch ibunch (soa6, np particles) into the
+ * gendst_datafile_* files, one per tracked plane. */
+int mbt_writer_distribution(mbt_writer *w, int ibunch, const double *soa6,
+                            int np);
+
+/* Close every file and free the writer. */
+int mbt_writer_close(mbt_writer *w);
+
+/* Message of the last failing mbt_writer_* call of this process. */
+const char *mbt_writer_error(void);
 
 #ifdef __cplusplus
 }

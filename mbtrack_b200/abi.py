@@ -79,6 +79,19 @@ class MbtState(ctypes.Structure):
     ]
 
 
+class MbtOutputCfg(ctypes.Structure):
+    """mbt_output_cfg (include/mbt.h)."""
+    _fields_ = [
+        ("jobtitle", ctypes.c_char * 80),
+        ("gendst_file", (ctypes.c_char * 1024) * 3),
+        ("nrev_scan", _l), ("nrev_potentials_out", _l),
+        ("ampinv_out", _i), ("scan_start", _d), ("n_out", _i),
+    ]
+
+
+MBT_WRITER_OWN_AMPINV = 1
+
+
 def params_to_dict(p):
     """Flatten an MbtParams into {field: scalar or nested list}."""
     out = {}

@@ -11,7 +11,8 @@ import os
 
 import numpy as np
 
-from .abi import (MBT_NOISE_INJECTED, MBT_NOISE_PHILOX, MbtParams, MbtState)
+from .abi import (MBT_NOISE_INJECTED, MBT_NOISE_PHILOX, MBT_WRITER_OWN_AMPINV, MbtOutputCfg, MbtParams,
+                  MbtState)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmbt.so")
@@ -50,6 +51,24 @@ SIGNATURES = {
                                              ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, _vp]),
     "mbt_bunch_moments_dev_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_double, ctypes.c_double,
                                                      ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "mbt_config_output": (ctypes.c_int, [ctypes.c_char_p, _P(MbtOutputCfg), _vp]),
+    "mbt_reference_beam": (ctypes.c_int, [_P(MbtParams), ctypes.c_int, ctypes.c_int, _vp]),
+    "mbt_use_device": (ctypes.c_int, [ctypes.c_int]),
+    "mbt_get_stats": (ctypes.c_int, [_vp, _vp]),
+    "mbt_watch_potentials": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "mbt_get_potentials": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "mbt_writer_open": (ctypes.c_int, [ctypes.c_char_p, _P(MbtParams), _P(MbtOutputCfg), _vp, ctypes.c_int,
+                                       _vp, _vp, ctypes.c_int, _P(_vp)]),
+    "mbt_writer_wakes": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "mbt_writer_begin": (ctypes.c_int, [_vp, _vp]),
+    "mbt_writer_turns": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp]),
+    "mbt_writer_potentials_due": (ctypes.c_int, [_vp, ctypes.c_long]),
+    "mbt_writer_potentials": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_long, _vp, ctypes.c_double,
+                                             ctypes.c_double]),
+    "mbt_writer_end": (ctypes.c_int, [_vp, _vp]),
+    "mbt_writer_distribution": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
+    "mbt_writer_close": (ctypes.c_int, [_vp]),
+    "mbt_writer_error": (ctypes.c_char_p, []),
     "mbt_wofz_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mbt_be_field_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, _vp, _vp, _vp]),
@@ -122,6 +141,92 @@ class Config:
         return np.array([L.mbt_bunch_current(ctypes.byref(self.params), self.nbunch, f)
                          for f in self.ib_frac])
 
+    def output(self):
+        """(mbt_output_cfg, output bucket numbers) of the file."""
+        L = lib()
+        o = MbtOutputCfg()
+        out = np.zeros(max(self.params.nharm, 1), dtype=np.int32)
+        rc = L.mbt_config_output(self.path.encode(), ctypes.byref(o), _ptr(out))
+        if rc != 0:
+            raise MbtError(rc, L.mbt_config_error().decode())
+        return o, out[:o.n_out].copy()
+
+    def reference_beam(self, np_=None):
+        """The reference's initial distribution of every bunch (host),
+        a list of [6, np] arrays (mbt_reference_beam)."""
+        L = lib()
+        n = self.params.np_model if np_ is None else np_
+        beams = []
+        for kb in self.bucket:
+            a = np.zeros((6, n))
+            rc = L.mbt_reference_beam(ctypes.byref(self.params), int(kb), n, _ptr(a))
+            if rc != 0:
+                raise MbtError(rc, "mbt_reference_beam")
+            beams.append(a)
+        return beams
+
+
+class Writer:
+    """The reference's output files (mbt_writer_*)."""
+
+    def __init__(self, work_path, params, ocfg, bunch_out, bucket, ib, own_ampinv=False):
+        L = lib()
+        self.params = params.copy()
+        self.ocfg = ocfg
+        self.bunch_out = np.ascontiguousarray(bunch_out, dtype=np.int32)
+        self.bucket = np.ascontiguousarray(bucket, dtype=np.int32)
+        self.ib = np.ascontiguousarray(ib, dtype=np.float64)
+        self.nb = len(self.bucket)
+        h = _vp()
+        rc = L.mbt_writer_open(work_path.encode(), ctypes.byref(self.params), ctypes.byref(self.ocfg),
+                               _ptr(self.bunch_out), self.nb, _ptr(self.bucket), _ptr(self.ib),
+                               MBT_WRITER_OWN_AMPINV if own_ampinv else 0, ctypes.byref(h))
+        self._check(rc)
+        self.h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise MbtError(rc, lib().mbt_writer_error().decode(errors="replace"))
+
+    def wakes(self, Gl, Gv, Gh):
+        g = [np.ascontiguousarray(a, dtype=np.float64) for a in (Gl, Gv, Gh)]
+        self._check(lib().mbt_writer_wakes(self.h, *[_ptr(a) for a in g]))
+
+    def begin(self, init_stats):
+        a = np.ascontiguousarray(init_stats, dtype=np.float64)
+        self._check(lib().mbt_writer_begin(self.h, _ptr(a)))
+
+    def turns(self, stats, ampinv=None):
+        st = np.ascontiguousarray(stats, dtype=np.float64)
+        ai = None if ampinv is None else np.ascontiguousarray(ampinv, dtype=np.float64)
+        self._check(lib().mbt_writer_turns(self.h, st.shape[0], _ptr(st), _ptr(ai)))
+
+    def potentials_due(self, rev):
+        return bool(lib().mbt_writer_potentials_due(self.h, rev))
+
+    def potentials(self, ibunch, rev, pot, vrf0, phai0):
+        a = np.ascontiguousarray(pot, dtype=np.float64)
+        self._check(lib().mbt_writer_potentials(self.h, ibunch, rev, _ptr(a), vrf0, phai0))
+
+    def end(self, end_stats):
+        a = np.ascontiguousarray(end_stats, dtype=np.float64)
+        self._check(lib().mbt_writer_end(self.h, _ptr(a)))
+
+    def distribution(self, ibunch, soa6):
+        a = np.ascontiguousarray(soa6, dtype=np.float64)
+        self._check(lib().mbt_writer_distribution(self.h, ibunch, _ptr(a), a.size // 6))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mbt_writer_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
 
 class Tracker:
     """One tracking context (mbt_ctx) holding every filled bunch."""
@@ -183,6 +288,22 @@ class Tracker:
         a = np.empty(6 * int(self.np.sum()))
         _check(lib().mbt_get_all(self.h, _ptr(a)), self.h)
         return a
+
+    def get_stats(self):
+        """Statistics of the current coordinates (pending RW kick included)."""
+        s = np.zeros(12 * self.nb)
+        _check(lib().mbt_get_stats(self.h, _ptr(s)), self.h)
+        return s.reshape(self.nb, 12)
+
+    def watch_potentials(self, bunches):
+        b = np.ascontiguousarray(bunches, dtype=np.int32)
+        _check(lib().mbt_watch_potentials(self.h, len(b), _ptr(b)), self.h)
+
+    def potentials(self, ib):
+        """7 x ncell potential terms of the next turn (mbt_get_potentials)."""
+        a = np.zeros(7 * self.params.ncell)
+        _check(lib().mbt_get_potentials(self.h, ib, _ptr(a)), self.h)
+        return a.reshape(7, self.params.ncell)
 
     def prepare(self):
         s = np.zeros(12 * self.nb)

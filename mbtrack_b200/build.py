@@ -20,13 +20,17 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # explicit round-to-nearest intrinsics in the kernels.
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
                      "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
-CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-I" + os.path.join(ROOT, "include")]
+# host C: no contraction of multiply-adds, as in the reference's x86-64 build
+CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include")]
 
 CU_SOURCES = ["mbt_runtime.cu", "mbt_step.cu", "mbt_fields.cu"]
 # per-file extra flags: w(z) and the BE field keep every multiply and add
 # separately rounded, as the reference's x86-64 build does
 CU_EXTRA = {"mbt_fields.cu": ["-fmad=false"]}
-C_SOURCES = ["mbt_host.c"]
+C_SOURCES = ["mbt_host.c", "mbt_beam.c", "mbt_output.c"]
+# the drop-in executable for mbtrack-mpi's weak-weak runs
+CLI_SOURCE = "mbtrack_gpu.c"
+CLI = os.path.join(HERE, "mbtrack-gpu")
 HEADERS = ["mbt_common.cuh", "mbt_device.cuh", "mbt_kernels.cuh", "mbt_philox.cuh", "mbt_wofz.cuh"]
 
 
@@ -61,6 +65,10 @@ def build(verbose_ptxas=False, force=False):
         objs.append(o)
     if force or _stale(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lm"])
+    cli_src = os.path.join(CSRC, CLI_SOURCE)
+    if force or _stale(CLI, [cli_src, LIB] + hdrs):
+        _run(["gcc"] + CC_FLAGS + [cli_src, "-o", CLI, "-L" + HERE, "-lmbt", "-lpthread", "-lm",
+                                   "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 

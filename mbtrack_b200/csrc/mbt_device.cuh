@@ -120,6 +120,8 @@ struct Args {
   double *hist;               // nbunch x 6 x ncell: fnp, dipV, dipH (clamped), ring L, H, V (dropped)
   int *cellrange;             // nbunch x 2: icellmin, icellmax
   double *kick;               // nbunch x 3 x ncell: L, V, H kick tables
+  double *pot;                // watched bunches x 7 x ncell: potential terms of the next turn, or null
+  const int *pot_slot;        // nbunch: watch slot or -1
   double *rw_part;            // nbunch x kRwSplit x 2: partial RW kicks (HOR, VER)
   double *stats;              // stats_cap x nbunch x 12
   double *ampinv;             // stats_cap x nbunch x 6: ampinv[3], ampinv_cm[3]

@@ -12,7 +12,7 @@
  *   setup_tracking_parameters input.c:1698-1772
  *   construct_greensfunc_*    transform_weak.c:288-471
  *
- * Differences from the reference, deliberate and listed in DESIGN.md:
+ * Deliberate differences from the reference:
  *   - the set-up result is checked (mbtrack-mpi.c:97,148 ignore it);
  *   - with fix_rw_beff, beffH3/beffV3 are read whenever long-range RW is
  *     on (the reference reads them only with EnableRW_short,
@@ -181,11 +181,19 @@ static int get_double(const conf_t *c, const char *sec, const char *key, double 
   return 0;
 }
 
+/* config_get_str (input.c:1093-1100) scans "%s": the first word */
 static int get_str(const conf_t *c, const char *sec, const char *key, char *r, size_t cap)
 {
   const char *v = get_raw(c, sec, key);
+  size_t n = 0;
   if (!v) return 0;
-  snprintf(r, cap, "%s", v);
+  while (*v == ' ' || *v == '\t' || *v == '\n' || *v == '\r') v++;
+  if (*v == '\0') return 0;
+  while (v[n] != '\0' && v[n] != ' ' && v[n] != '\t' && v[n] != '\n' && v[n] != '\r' && n + 1 < cap) {
+    r[n] = v[n];
+    n++;
+  }
+  r[n] = '\0';
   return 1;
 }
 
@@ -242,6 +250,8 @@ typedef struct cfg {
   double scan_start, scan_step;
   int Nslc;
   double q;                      /* ring->q = U0 / Vrf0 / 1e6 (input.c:1606) */
+  mbt_output_cfg out;            /* output settings */
+  int *bunch_out;                /* nharm: output buckets (setup_beam) */
 } cfg_t;
 
 static int read_conf(const char *path, int fix_rw_beff, cfg_t *g)
@@ -265,6 +275,7 @@ static int read_conf(const char *path, int fix_rw_beff, cfg_t *g)
 
   /* [tracking] */
   REQ_S("tracking", "jobtitle", s);
+  snprintf(g->out.jobtitle, sizeof g->out.jobtitle, "%.79s", s);
   if (get_str(&C, "tracking", "filling", s, sizeof s)) {
     g->filling = -1;
     for (i = 0; i < 13; i++) if (strcmp(fillings[i], s) == 0) g->filling = i;
@@ -285,6 +296,8 @@ static int read_conf(const char *path, int fix_rw_beff, cfg_t *g)
   REQ_I("tracking", "EnableIdealHC", &p->ideal_hc);
   if (!get_int(&C, "tracking", "EnableRW_short_LON", &g->enable_rw_short_lon))
     g->enable_rw_short_lon = g->enable_rw_short;
+  if (!get_long(&C, "tracking", "NrevPotentialsOut", &g->out.nrev_potentials_out)) g->out.nrev_potentials_out = 0;
+  if (!get_int(&C, "tracking", "EnableAmpinv_out", &g->out.ampinv_out)) g->out.ampinv_out = 0;
   if (!get_int(&C, "tracking", "triggerRW", &p->triggerRW)) p->triggerRW = 0;
   if (!get_int(&C, "tracking", "Nmlt", &p->Nmlt) && p->rw_long) p->Nmlt = 0;
   if (!get_int(&C, "tracking", "EnableResonators", &enable_res)) enable_res = 1;
@@ -372,9 +385,9 @@ static int read_conf(const char *path, int fix_rw_beff, cfg_t *g)
     if (!get_int(&C, "distribution", "iseed_HOR", &p->iseed[1])) p->iseed[1] = seed;
     if (!get_int(&C, "distribution", "iseed_VER", &p->iseed[2])) p->iseed[2] = seed;
   }
-  REQ_S("distribution", "gendst_datafile_LON", s);
-  REQ_S("distribution", "gendst_datafile_HOR", s);
-  REQ_S("distribution", "gendst_datafile_VER", s);
+  REQ_S("distribution", "gendst_datafile_LON", g->out.gendst_file[0]);
+  REQ_S("distribution", "gendst_datafile_HOR", g->out.gendst_file[1]);
+  REQ_S("distribution", "gendst_datafile_VER", g->out.gendst_file[2]);
   REQ_D("distribution", "xtauCM_offset", &g->cm[0]);
   REQ_D("distribution", "xepsCM_offset", &g->cm[1]);
   REQ_D("distribution", "sgm_xtau", &g->sgm[0]);
@@ -661,7 +674,10 @@ static int setup_beam(cfg_t *g, int *nbunch, int *bucket, double *ib_frac)
       if (fscanf(f, "%d %lf %d\n", &nb_tmp, &crat_tmp, &bout_tmp) != 3) break;
       if (nb_tmp >= H) break;
       while (nb_tmp > kb) { ratio[kb] = 0; kb++; }
-      if (crat_tmp > 0) { fill[kb] = 1; ratio[kb] = crat_tmp; crat_tot += crat_tmp; nb++; }
+      if (crat_tmp > 0) {
+        fill[kb] = 1; ratio[kb] = crat_tmp; crat_tot += crat_tmp; nb++;
+        if (bout_tmp && g->bunch_out) g->bunch_out[g->out.n_out++] = kb;
+      }
       else ratio[kb] = 0.0;
     }
     fclose(f);
@@ -676,6 +692,24 @@ static int setup_beam(cfg_t *g, int *nbunch, int *bucket, double *ib_frac)
         }
     }
   } else {
+    /* output buckets of each named filling (input.c:1316-1426) */
+    int bo[3] = {0, 0, 0}, nbo = 1;
+    switch (g->filling) {
+      case 7: nbo = 3; bo[1] = H / 8; bo[2] = H / 4 - 1; break;
+      case 1: nbo = 3; bo[1] = H / 6; bo[2] = H / 3 - 1; break;
+      case 2: nbo = 3; bo[1] = H / 3; bo[2] = 2 * H / 3 - 1; break;
+      case 6: nbo = 3; bo[1] = 3 * H / 8; bo[2] = 3 * H / 4 - 1; break;
+      case 4: nbo = 2; bo[1] = 1; break;
+      case 5: nbo = 3; bo[1] = 1; bo[2] = 2; break;
+      case 8: nbo = 3; bo[1] = 4; bo[2] = 9; break;
+      case 9: nbo = 3; bo[1] = 9; bo[2] = 19; break;
+      case 10: nbo = 3; bo[1] = 14; bo[2] = 29; break;
+      default: break;
+    }
+    if (g->bunch_out) {
+      for (kb = 0; kb < nbo; kb++) g->bunch_out[kb] = bo[kb];
+      g->out.n_out = nbo;
+    }
     switch (g->filling) {
       case 0: for (kb = 0; kb < H; kb++) fill[kb] = 1; break;
       case 7: for (kb = 0; kb < H / 4; kb++) fill[kb] = 1; break;
@@ -724,6 +758,32 @@ int mbt_config_load(const char *conf_path, int fix_rw_beff, mbt_params *p, int *
     *p = g->p;
     if (nbunch) *nbunch = nb;
   }
+  free(g);
+  return r;
+}
+
+int mbt_config_output(const char *conf_path, mbt_output_cfg *o, int *bunch_out)
+{
+  cfg_t *g;
+  int r, nb = 0;
+  if (!conf_path || !o) return MBT_ERR_INVALID;
+  g = (cfg_t *) calloc(1, sizeof(cfg_t));
+  if (!g) return MBT_ERR_NOMEM;
+  r = read_conf(conf_path, 1, g);
+  if (!r) r = setup_ring(g);
+  if (!r) r = setup_tracking(g);
+  if (!r) {
+    g->bunch_out = (int *) calloc(g->p.nharm > 0 ? g->p.nharm : 1, sizeof(int));
+    if (!g->bunch_out) r = MBT_ERR_NOMEM;
+  }
+  if (!r) r = setup_beam(g, &nb, NULL, NULL);
+  if (!r) {
+    g->out.nrev_scan = g->nrev_scan;
+    g->out.scan_start = g->scan_start;
+    *o = g->out;
+    if (bunch_out) memcpy(bunch_out, g->bunch_out, (size_t) g->out.n_out * sizeof(int));
+  }
+  free(g->bunch_out);
   free(g);
   return r;
 }

@@ -24,7 +24,9 @@
 //                 history (transform_weak.c:813-825).
 //
 // Arithmetic that the parity tests compare against the oracle keeps the
-// reference's operation order; the library is compiled with -fmad=false.
+// reference's operation order; where the compiler would contract a multiply
+// and an add of such an expression into one FMA, the multiply and the add
+// are written with the round-to-nearest intrinsics (__dmul_rn, __dadd_rn).
 #pragma once
 #include <cstdint>
 #include "mbt_device.cuh"
@@ -835,6 +837,17 @@ __global__ void __launch_bounds__(kBlock) bunch_wakes(Args a, int advance) {
     K[j] = factG * GL1 + lr[0 * nc + j];
     K[nc + j] = -factG * GV + lr[2 * nc + j];
     K[2 * nc + j] = -factG * GH + lr[1 * nc + j];
+    if (a.pot != nullptr && a.pot_slot[b] >= 0) {
+      // the columns of the potentials output (transform_weak.c:735-768)
+      double *P = a.pot + (size_t)a.pot_slot[b] * 7 * nc;
+      P[j] = __dmul_rn(factG, GL1);
+      P[nc + j] = lr[0 * nc + j];
+      P[2 * nc + j] = fnp[j];
+      P[3 * nc + j] = __dmul_rn(-factG, GV);
+      P[4 * nc + j] = dipV[j];
+      P[5 * nc + j] = __dmul_rn(-factG, GH);
+      P[6 * nc + j] = dipH[j];
+    }
   }
 }
 

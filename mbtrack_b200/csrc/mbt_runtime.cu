@@ -33,6 +33,9 @@ thread_local char g_create_error[512] = "";
 }  // namespace
 
 namespace mbt {
+size_t stats_scratch_doubles(int np);
+int bunch_stats_strided(int np, const double *coord, size_t ld, const int tp[3], double *stats, void *stream,
+                        double *scratch);
 // Message for mbt_last_error(NULL, ...) from entry points without a context.
 int fail_global(int code, const char *fmt, ...) {
   va_list ap;
@@ -64,6 +67,8 @@ struct mbt_ctx {
   double *vbuf = nullptr;
   double *stats_init = nullptr;
   double *xfer = nullptr;        // device staging for exports
+  double *stat_scratch = nullptr; // block partials of mbt_get_stats
+  std::vector<int> watch;        // bunches whose potentials are recorded
   cudaEvent_t ev[6] = {};
   double timing[4] = {0, 0, 0, 0};
   int device = 0;
@@ -237,6 +242,16 @@ int build_graph(mbt_ctx *c, int turns) {
 extern "C" {
 
 size_t mbt_params_size(void) { return sizeof(mbt_params); }
+
+int mbt_use_device(int device) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return fail(nullptr, MBT_ERR_NODEVICE, "no CUDA device: libmbt has no CPU path");
+  if (device < 0 || device >= n) return fail(nullptr, MBT_ERR_INVALID, "device %d outside 0..%d", device, n - 1);
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(nullptr, MBT_ERR_CUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+  return 0;
+}
 
 int mbt_last_error(const mbt_ctx *ctx, char *buf, size_t len) {
   if (!buf || len == 0) return MBT_ERR_INVALID;
@@ -606,6 +621,63 @@ int mbt_get_all(mbt_ctx *c, double *soa6_all) {
     pos += (size_t)6 * c->np[b];
   }
   CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int mbt_get_stats(mbt_ctx *c, double *stats) {
+  if (!c || !stats) return MBT_ERR_INVALID;
+  int r = export_all(c);
+  if (r) return r;
+  if (!c->stat_scratch) {
+    int npmax = 1;
+    for (int n : c->np) npmax = std::max(npmax, n);
+    r = dalloc(c, &c->stat_scratch, mbt::stats_scratch_doubles(npmax));
+    if (r) return r;
+  }
+  for (int b = 0; b < c->nbunch; ++b) {
+    r = mbt::bunch_stats_strided(c->np[b], c->xfer + c->off[b], (size_t)c->npad, c->p.track_plane, stats + 12 * b,
+                                 c->stream, c->stat_scratch);
+    if (r) return fail(c, r, "statistics of bunch %d: %s", b, cudaGetErrorString(cudaGetLastError()));
+  }
+  return 0;
+}
+
+int mbt_watch_potentials(mbt_ctx *c, int n, const int *ibunch) {
+  if (!c || n < 0 || n > MBT_MAX_WATCH || (n > 0 && !ibunch))
+    return c ? fail(c, MBT_ERR_INVALID, "watch list: 0..%d bunches", MBT_MAX_WATCH) : MBT_ERR_INVALID;
+  if (c->prepared) return fail(c, MBT_ERR_STATE, "mbt_watch_potentials must precede mbt_prepare");
+  if (!c->watch.empty() || c->a.pot) return fail(c, MBT_ERR_STATE, "potentials are already watched");
+  if (n == 0) return 0;
+  std::vector<int> slot(c->nbunch, -1);
+  for (int i = 0; i < n; ++i) {
+    if (ibunch[i] < 0 || ibunch[i] >= c->nbunch) return fail(c, MBT_ERR_INVALID, "bunch %d out of range", ibunch[i]);
+    if (slot[ibunch[i]] >= 0) return fail(c, MBT_ERR_INVALID, "bunch %d listed twice", ibunch[i]);
+    slot[ibunch[i]] = i;
+  }
+  double *pot = nullptr;
+  int *ps = nullptr;
+  int r = dalloc(c, &pot, (size_t)n * 7 * c->nc);
+  if (!r) r = dupload(c, &ps, slot.data(), slot.size());
+  if (r) return r;
+  c->a.pot = pot;
+  c->a.pot_slot = ps;
+  c->watch.assign(ibunch, ibunch + n);
+  if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; c->graph_turns = 0; }
+  return 0;
+}
+
+int mbt_get_potentials(mbt_ctx *c, int ibunch, double *pot) {
+  if (!c || !pot) return MBT_ERR_INVALID;
+  int slot = -1;
+  for (size_t i = 0; i < c->watch.size(); ++i)
+    if (c->watch[i] == ibunch) slot = (int)i;
+  if (slot < 0) return fail(c, MBT_ERR_INVALID, "bunch %d is not watched", ibunch);
+  if (!c->prepared) return fail(c, MBT_ERR_STATE, "mbt_prepare has not run");
+  CK(cudaStreamSynchronize(c->stream));
+  const int nc = c->p.ncell;
+  for (int k = 0; k < 7; ++k)
+    CK(cudaMemcpy(pot + (size_t)k * nc, c->a.pot + ((size_t)slot * 7 + k) * c->nc, nc * sizeof(double),
+                  cudaMemcpyDeviceToHost));
   return 0;
 }
 

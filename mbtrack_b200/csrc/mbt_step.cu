@@ -24,7 +24,7 @@ constexpr int kExtra = 12;           // 6 shifted sums, 6 shifted sums of square
 
 // Record of one block: counts[nc], sum x[nc], sum z[nc], kExtra sums.
 __global__ void __launch_bounds__(kThreads)
-moments_partial(int np, const double *__restrict__ c, double sgm, double nsig, double dT, int nc,
+moments_partial(int np, const double *__restrict__ c, size_t ld, double sgm, double nsig, double dT, int nc,
                 double *__restrict__ part, int prec) {
   extern __shared__ double sh[];
   double *hx = sh, *hz = sh + nc;
@@ -32,7 +32,7 @@ moments_partial(int np, const double *__restrict__ c, double sgm, double nsig, d
   __shared__ double red[kThreads / 32][kExtra];
   for (int i = threadIdx.x; i < nc; i += kThreads) { hx[i] = 0.0; hz[i] = 0.0; hc[i] = 0; }
   __syncthreads();
-  const size_t n6 = (size_t)np;
+  const size_t n6 = ld;
   double s[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k) s[k] = c[k * n6];   // shift: the first particle
@@ -78,9 +78,9 @@ moments_partial(int np, const double *__restrict__ c, double sgm, double nsig, d
 // One block: records summed in block order; stats (12 doubles, mbt.h
 // order) and histograms written to `out` (12 + 3 nc doubles).
 __global__ void __launch_bounds__(kThreads)
-moments_final(int np, const double *__restrict__ c, int nc, int nblk, const double *__restrict__ part,
+moments_final(int np, const double *__restrict__ c, size_t ld, int nc, int nblk, const double *__restrict__ part,
               int prec, int th, int tv, double *__restrict__ out) {
-  const size_t n6 = (size_t)np;
+  const size_t n6 = ld;
   for (int e = threadIdx.x; e < prec; e += kThreads) {
     double t = 0.0;
     for (int b = 0; b < nblk; ++b) t += part[(size_t)b * prec + e];
@@ -130,13 +130,13 @@ int check_args(int np, const double *coord, double sgm, double dT, int ncell, co
   return 0;
 }
 
-int run_moments(int np, const double *coord, double sgm, double nsig, double dT, int ncell, const int *tp,
-                double *stats, double *hist, cudaStream_t st, double *scratch, int nblk) {
+int run_moments(int np, const double *coord, size_t ld, double sgm, double nsig, double dT, int ncell,
+                const int *tp, double *stats, double *hist, cudaStream_t st, double *scratch, int nblk) {
   const int prec = 3 * ncell + kExtra;
   const size_t smem = (size_t)ncell * (2 * sizeof(double) + sizeof(int));
   double *part = scratch, *out = scratch + (size_t)nblk * prec;
-  moments_partial<<<nblk, kThreads, smem, st>>>(np, coord, sgm, nsig, dT, ncell, part, prec);
-  moments_final<<<1, kThreads, 0, st>>>(np, coord, ncell, nblk, part, prec, tp[1] != 0, tp[2] != 0, out);
+  moments_partial<<<nblk, kThreads, smem, st>>>(np, coord, ld, sgm, nsig, dT, ncell, part, prec);
+  moments_final<<<1, kThreads, 0, st>>>(np, coord, ld, ncell, nblk, part, prec, tp[1] != 0, tp[2] != 0, out);
   if (cudaGetLastError() != cudaSuccess) return MBT_ERR_CUDA;
   if (ncell > 0 &&
       cudaMemcpyAsync(hist, out + 12, (size_t)3 * ncell * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
@@ -147,6 +147,18 @@ int run_moments(int np, const double *coord, double sgm, double nsig, double dT,
 }
 
 }  // namespace
+
+namespace mbt {
+// Statistics of one bunch whose six coordinate arrays start `ld` doubles
+// apart (a context's padded layout), without histograms.  scratch holds at
+// least stats_scratch_doubles(np) doubles.
+size_t stats_scratch_doubles(int np) { return (size_t)blocks_for(np) * kExtra + 12 + kExtra; }
+int bunch_stats_strided(int np, const double *coord, size_t ld, const int tp[3], double *stats, void *stream,
+                        double *scratch) {
+  return run_moments(np, coord, ld, 1.0, 0.0, 1.0, 0, tp, stats, nullptr, (cudaStream_t)stream, scratch,
+                     blocks_for(np));
+}
+}  // namespace mbt
 
 extern "C" int mbt_bunch_moments_dev(int np, const double *coord_dev, double sigma_tau, double nsigma, double dT,
                                      int ncell, const int track_plane[3], double *stats, double *hist_dev,
@@ -161,7 +173,7 @@ extern "C" int mbt_bunch_moments_dev(int np, const double *coord_dev, double sig
   double *scratch = nullptr;
   if (cudaMalloc(&scratch, n * sizeof(double)) != cudaSuccess)
     return mbt::fail_global(MBT_ERR_NOMEM, "bunch moments: cudaMalloc of %zu bytes failed", n * sizeof(double));
-  r = run_moments(np, coord_dev, sigma_tau, nsigma, dT, ncell, track_plane, stats, hist_dev,
+  r = run_moments(np, coord_dev, (size_t)np, sigma_tau, nsigma, dT, ncell, track_plane, stats, hist_dev,
                   (cudaStream_t)stream, scratch, nblk);
   cudaFree(scratch);
   return r;
@@ -230,6 +242,6 @@ extern "C" int mbt_bunch_moments_dev_noalloc(int np, const double *coord_dev, do
   const int nblk = std::min(blocks_for(np), fit);
   if (nblk < 1)
     return mbt::fail_global(MBT_ERR_INVALID, "allocation-free bunch moments: ncell %d does not fit the scratch", ncell);
-  return run_moments(np, coord_dev, sigma_tau, nsigma, dT, ncell, track_plane, stats, hist_dev,
+  return run_moments(np, coord_dev, (size_t)np, sigma_tau, nsigma, dT, ncell, track_plane, stats, hist_dev,
                      (cudaStream_t)stream, scratch, nblk);
 }

@@ -1,0 +1,246 @@
+/*
+ * mbtrack_gpu.c -- `mbtrack-gpu input.conf [/path/to/work]`: the weak-weak
+ * run of mbtrack-mpi (mbtrack-mpi.c:22-160 with manager_weakweak and
+ * worker_weakweak) on one GPU, without MPI and without the rank-count check
+ * of mbtrack-mpi.c:85-90.
+ *
+ * The arguments, the terminal messages and the files in the work directory
+ * are the reference's.  Options (anywhere on the command line):
+ *   --own-ampinv    ampinv files show each bunch's own invariants (the
+ *                   reference's history indexing otherwise)
+ *   --seed N        key of the counter-based quantum-excitation noise
+ *                   (default: iseed_LON)
+ *   --device N      CUDA device (default 0)
+ * The initial distribution is the reference's (same generator, same seeds).
+ * The quantum-excitation noise is a Philox stream instead of glibc rand():
+ * with EnableQuantum = 0 the run reproduces the reference's numbers, with
+ * noise it reproduces their statistics.
+ */
+#define _DEFAULT_SOURCE
+#include <pthread.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include <unistd.h>
+
+#include "mbt.h"
+
+typedef struct beam_job {
+  const mbt_params *p;
+  const int *bucket;
+  const int *np;
+  const size_t *start;
+  double *all;
+  int nb, next, err;
+  pthread_mutex_t lock;
+} beam_job;
+
+static void *beam_worker(void *arg)
+{
+  beam_job *j = (beam_job *) arg;
+  for (;;) {
+    int b, r;
+    pthread_mutex_lock(&j->lock);
+    b = j->next++;
+    pthread_mutex_unlock(&j->lock);
+    if (b >= j->nb) return NULL;
+    r = mbt_reference_beam(j->p, j->bucket[b], j->np[b], j->all + j->start[b]);
+    if (r) j->err = r;
+  }
+}
+
+/* every bunch's reference distribution, bunch after bunch (soa6 blocks),
+ * generated on the host cores */
+static int reference_beam_all(const mbt_params *p, int nb, const int *bucket, const int *np, double *all)
+{
+  beam_job j;
+  pthread_t th[256];
+  size_t *start = (size_t *) malloc((nb + 1) * sizeof(size_t));
+  long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+  int i, nt;
+  if (!start) return MBT_ERR_NOMEM;
+  start[0] = 0;
+  for (i = 0; i < nb; i++) start[i + 1] = start[i] + (size_t) 6 * np[i];
+  memset(&j, 0, sizeof j);
+  j.p = p; j.bucket = bucket; j.np = np; j.start = start; j.all = all; j.nb = nb;
+  pthread_mutex_init(&j.lock, NULL);
+  nt = (int) (ncpu < 1 ? 1 : ncpu > 256 ? 256 : ncpu);
+  if (nt > nb) nt = nb;
+  for (i = 0; i < nt; i++) pthread_create(&th[i], NULL, beam_worker, &j);
+  for (i = 0; i < nt; i++) pthread_join(th[i], NULL);
+  pthread_mutex_destroy(&j.lock);
+  free(start);
+  return j.err;
+}
+
+static void ctx_error(mbt_ctx *ctx, const char *what)
+{
+  char msg[512];
+  mbt_last_error(ctx, msg, sizeof msg);
+  fprintf(stderr, "ERROR: %s: %s\n", what, msg);
+}
+
+int main(int argc, char **argv)
+{
+  const char *conf = NULL, *work = "work/";
+  int own_ampinv = 0, device = 0, have_seed = 0, npos = 0, i, r, nb = 0;
+  unsigned long long seed = 0;
+  mbt_params p;
+  mbt_output_cfg o;
+  int *bucket = NULL, *np = NULL, *bunch_out = NULL, *watch = NULL, nwatch = 0;
+  double *frac = NULL, *ib = NULL, *Gl = NULL, *Gv = NULL, *Gh = NULL, *beam = NULL;
+  double *init_stats = NULL, *stats = NULL, *ampinv = NULL, *pot = NULL;
+  size_t nbeam = 0;
+  long rev, chunk;
+  mbt_ctx *ctx = NULL;
+  mbt_writer *w = NULL;
+  mbt_state st;
+  time_t now;
+  struct tm *tnow;
+
+  for (i = 1; i < argc; i++) {
+    if (strcmp(argv[i], "--own-ampinv") == 0) own_ampinv = 1;
+    else if (strcmp(argv[i], "--seed") == 0 && i + 1 < argc) { seed = strtoull(argv[++i], NULL, 0); have_seed = 1; }
+    else if (strcmp(argv[i], "--device") == 0 && i + 1 < argc) device = atoi(argv[++i]);
+    else if (npos == 0) { conf = argv[i]; npos++; }
+    else if (npos == 1) { work = argv[i]; npos++; }
+    else npos = 3;
+  }
+  if (npos < 1 || npos > 2) {
+    fprintf(stderr, "ERROR ! \n\nUsage:\nmbtrack-gpu inputfile.conf [/path/to/work] [--own-ampinv] [--seed N] [--device N]\n");
+    return -1;
+  }
+  if (mbt_use_device(device) != 0) {
+    ctx_error(NULL, "device");
+    return -1;
+  }
+
+  /* read_input + setup_* (mbtrack-mpi.c:61-97), checked */
+  if (mbt_config_load(conf, 1, &p, &nb, NULL, NULL) != 0) {
+    fprintf(stderr, "ERROR: read_input failed: %s\n", mbt_config_error());
+    return -1;
+  }
+  bucket = (int *) calloc(p.nharm, sizeof(int));
+  frac = (double *) calloc(p.nharm, sizeof(double));
+  bunch_out = (int *) calloc(p.nharm, sizeof(int));
+  np = (int *) calloc(nb > 0 ? nb : 1, sizeof(int));
+  ib = (double *) calloc(nb > 0 ? nb : 1, sizeof(double));
+  if (!bucket || !frac || !bunch_out || !np || !ib) { fprintf(stderr, "ERROR: out of host memory\n"); return -1; }
+  if (mbt_config_load(conf, 1, &p, &nb, bucket, frac) != 0 || mbt_config_output(conf, &o, bunch_out) != 0) {
+    fprintf(stderr, "ERROR: read_input failed: %s\n", mbt_config_error());
+    return -1;
+  }
+  if (nb <= 0) { fprintf(stderr, "ERROR: e_beam_setup: no filled bucket\n"); return -1; }
+  if (p.ncell > 0) {
+    Gl = (double *) calloc(p.ncell, sizeof(double));
+    Gv = (double *) calloc(p.ncell, sizeof(double));
+    Gh = (double *) calloc(p.ncell, sizeof(double));
+    if (!Gl || !Gv || !Gh || mbt_config_greens(conf, &p, Gl, Gv, Gh) != 0) {
+      fprintf(stderr, "ERROR: Green's functions: %s\n", mbt_config_error());
+      return -1;
+    }
+  }
+
+  printf("Starting job \"%s\"\n\n", o.jobtitle);
+  printf("Generating initial distribution...\n");
+  for (i = 0; i < nb; i++) {
+    np[i] = p.np_model;                              /* manager_weakweak.c:61 */
+    ib[i] = mbt_bunch_current(&p, nb, frac[i]);     /* manager_weakweak.c:74-75 */
+    nbeam += (size_t) 6 * np[i];
+  }
+  beam = (double *) malloc(nbeam * sizeof(double));
+  if (!beam) { fprintf(stderr, "ERROR: out of host memory for %zu coordinates\n", nbeam); return -1; }
+  if ((r = reference_beam_all(&p, nb, bucket, np, beam)) != 0) {
+    fprintf(stderr, "ERROR: weak_generate_bunch_distribution (%d)\n", r);
+    return -1;
+  }
+
+  if (!have_seed) seed = (unsigned long long) (unsigned) p.iseed[0];
+  if (mbt_create(&p, nb, bucket, np, ib, Gl, Gv, Gh, MBT_NOISE_PHILOX, seed, &ctx) != 0) {
+    ctx_error(NULL, "mbt_create");
+    return -1;
+  }
+  if (mbt_load_all(ctx, beam) != 0) { ctx_error(ctx, "loading the beam"); return -1; }
+
+  /* the output bunches */
+  watch = (int *) calloc(nb, sizeof(int));
+  for (i = 0; i < nb && watch; i++) {
+    int j;
+    for (j = 0; j < o.n_out; j++)
+      if (bunch_out[j] == bucket[i] && nwatch < MBT_MAX_WATCH) { watch[nwatch++] = i; break; }
+  }
+  if (o.nrev_potentials_out <= p.nrev_tot && nwatch > 0 && mbt_watch_potentials(ctx, nwatch, watch) != 0) {
+    ctx_error(ctx, "mbt_watch_potentials");
+    return -1;
+  }
+  init_stats = (double *) malloc((size_t) nb * 12 * sizeof(double));
+  if (!init_stats || mbt_prepare(ctx, init_stats) != 0) { ctx_error(ctx, "mbt_prepare"); return -1; }
+  if (mbt_writer_open(work, &p, &o, bunch_out, nb, bucket, ib, own_ampinv ? MBT_WRITER_OWN_AMPINV : 0, &w) != 0 ||
+      mbt_writer_wakes(w, Gl, Gv, Gh) != 0 || mbt_writer_begin(w, init_stats) != 0) {
+    fprintf(stderr, "ERROR: %s\n", mbt_writer_error());
+    return -1;
+  }
+
+  printf("Starting multi bunch tracking...\n");
+  /* blocks of turns bounded by the host buffers and by the turns whose
+   * potentials are printed (they are read before such a turn runs) */
+  chunk = (long) (64L * 1024 * 1024 / ((size_t) nb * 18 * sizeof(double)));
+  if (chunk < 1) chunk = 1;
+  if (chunk > p.nrev_tot) chunk = p.nrev_tot > 0 ? p.nrev_tot : 1;
+  stats = (double *) malloc((size_t) chunk * nb * 12 * sizeof(double));
+  ampinv = (double *) malloc((size_t) chunk * nb * 6 * sizeof(double));
+  pot = (double *) malloc((size_t) 7 * (p.ncell > 0 ? p.ncell : 1) * sizeof(double));
+  if (!stats || !ampinv || !pot) { fprintf(stderr, "ERROR: out of host memory\n"); return -1; }
+  for (rev = 0; rev < p.nrev_tot;) {
+    long n = 1, k;
+    if (mbt_writer_potentials_due(w, rev)) {
+      if (mbt_get_state(ctx, &st) != 0) { ctx_error(ctx, "mbt_get_state"); return -1; }
+      for (i = 0; i < nwatch; i++)
+        if (mbt_get_potentials(ctx, watch[i], pot) != 0 ||
+            mbt_writer_potentials(w, watch[i], rev, pot, st.Vrf0, st.phai0) != 0) {
+          fprintf(stderr, "ERROR: potentials of turn %ld\n", rev);
+          return -1;
+        }
+    }
+    while (n < chunk && rev + n < p.nrev_tot && !mbt_writer_potentials_due(w, rev + n)) n++;
+    if (mbt_run_turns_ampinv(ctx, n, stats, ampinv) != 0) { ctx_error(ctx, "mbt_run_turns"); return -1; }
+    if (mbt_writer_turns(w, n, stats, ampinv) != 0) { fprintf(stderr, "ERROR: %s\n", mbt_writer_error()); return -1; }
+    /* terminal output of manager_weakweak.c:181-188, 309-318 */
+    for (k = rev; k < rev + n; k++) {
+      if (k % 5000 == 0) {
+        if (k + 4999 >= p.nrev_tot) printf("Transformation for turn %3ld to %3ld", k, p.nrev_tot - 1);
+        else printf("Transformation for turn %3ld to %3ld", k, k + 4999);
+        fflush(stdout);
+      }
+      if (k % 500 == 499) printf(".");
+      fflush(stdout);
+      if (k % 5000 == 4999 || k == p.nrev_tot - 1) {
+        time(&now);
+        tnow = localtime(&now);
+        printf(" done (at time: %d:%d:%d)\n", tnow->tm_hour, tnow->tm_min, tnow->tm_sec);
+      }
+    }
+    rev += n;
+  }
+
+  if (mbt_get_stats(ctx, init_stats) != 0) { ctx_error(ctx, "mbt_get_stats"); return -1; }
+  if (mbt_writer_end(w, init_stats) != 0) { fprintf(stderr, "ERROR: %s\n", mbt_writer_error()); return -1; }
+  if (nwatch > 0) {
+    const int b = watch[0];
+    if (mbt_get_particles(ctx, b, beam, np[b]) != 0) { ctx_error(ctx, "mbt_get_particles"); return -1; }
+    if (mbt_writer_distribution(w, b, beam, np[b]) != 0) fprintf(stderr, "ERROR: %s\n", mbt_writer_error());
+  }
+  if (mbt_get_state(ctx, &st) == 0) {
+    if (st.n_trash_low != 0 || st.n_trash_high != 0)
+      printf("\n WARNING - Binning for selffields (all bunches):\n %d particles below first bin,    %d particles above last bin\n",
+             st.n_trash_low, st.n_trash_high);
+    if (p.rffb && nwatch > 0) printf("\nFinal RF voltage and phase: %.7f MV, %.5f\n", st.Vrf0, st.phai0);
+  }
+  mbt_writer_close(w);
+  mbt_destroy(ctx);
+  free(bucket); free(frac); free(bunch_out); free(np); free(ib); free(Gl); free(Gv); free(Gh);
+  free(beam); free(init_stats); free(stats); free(ampinv); free(pot); free(watch);
+  return 0;
+}

@@ -152,6 +152,34 @@ class Oracle:
         self.lib.orc_trash(self.h, ib, ctypes.byref(lo), ctypes.byref(hi))
         return lo.value, hi.value
 
+    def run_files(self):
+        """The rest of the run (NrevTot turns after prepare) with the
+        reference's output files written into the work directory
+        (refh_run_files); returns the per-turn statistics, invariants, RF
+        voltage/phase at each turn's start and the end statistics."""
+        L = self.lib
+        L.refh_run_files.argtypes = [_vp, _vp, _vp, _vp]
+        p = self.params()
+        n = int(p.nrev_tot)
+        st = np.zeros((n, self.nb, 12))
+        ai = np.zeros((n, self.nb, 6))
+        vp = np.zeros((n, self.nb, 2))
+        end = np.zeros((self.nb, 12))
+        rc = L.refh_run_files(_ptr(st), _ptr(ai), _ptr(vp), _ptr(end))
+        if rc != 0:
+            raise RuntimeError("refh_run_files failed: %d" % rc)
+        return st, ai, vp, end
+
+    def output_info(self):
+        L = self.lib
+        L.refh_output_info.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_int]
+        a, b = ctypes.c_long(), ctypes.c_long()
+        c = ctypes.c_int()
+        out = np.zeros(4096, dtype=np.int32)
+        n = L.refh_output_info(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), _ptr(out), 4096)
+        return {"nrev_scan": a.value, "nrev_potentials_out": b.value, "ampinv_out": c.value,
+                "bunch_out": out[:n].copy()}
+
     def ampinv(self, ib):
         out = np.zeros(6)
         self.lib.orc_ampinv.argtypes = [_vp, ctypes.c_int, _vp]
@@ -277,6 +305,34 @@ class Reference:
         lo, hi = ctypes.c_int(), ctypes.c_int()
         self.lib.refh_trash(ib, ctypes.byref(lo), ctypes.byref(hi))
         return lo.value, hi.value
+
+    def run_files(self):
+        """The rest of the run (NrevTot turns after prepare) with the
+        reference's output files written into the work directory
+        (refh_run_files); returns the per-turn statistics, invariants, RF
+        voltage/phase at each turn's start and the end statistics."""
+        L = self.lib
+        L.refh_run_files.argtypes = [_vp, _vp, _vp, _vp]
+        p = self.params()
+        n = int(p.nrev_tot)
+        st = np.zeros((n, self.nb, 12))
+        ai = np.zeros((n, self.nb, 6))
+        vp = np.zeros((n, self.nb, 2))
+        end = np.zeros((self.nb, 12))
+        rc = L.refh_run_files(_ptr(st), _ptr(ai), _ptr(vp), _ptr(end))
+        if rc != 0:
+            raise RuntimeError("refh_run_files failed: %d" % rc)
+        return st, ai, vp, end
+
+    def output_info(self):
+        L = self.lib
+        L.refh_output_info.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_int]
+        a, b = ctypes.c_long(), ctypes.c_long()
+        c = ctypes.c_int()
+        out = np.zeros(4096, dtype=np.int32)
+        n = L.refh_output_info(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), _ptr(out), 4096)
+        return {"nrev_scan": a.value, "nrev_potentials_out": b.value, "ampinv_out": c.value,
+                "bunch_out": out[:n].copy()}
 
     def ampinv(self, ib):
         out = np.zeros(6)

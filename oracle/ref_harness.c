@@ -2,7 +2,7 @@
  * ref_harness.c -- TEST INFRASTRUCTURE ONLY.
  *
  * A single-process driver for the UNMODIFIED reference sources
- * (fracul/mtrack src/*.c, compiled from where they lie by oracle/Makefile
+ * (fracul/mtrack src/<file>.c, compiled from where they lie by oracle/Makefile
  * into oracle/_ref/libmbtref.so).  It replays the weak-weak worker of
  * worker_weakweak.c:19-394 for every filled bunch inside one process:
  *
@@ -94,6 +94,10 @@ static long rev_done = 0;
 static int lr_res_sizetot = 0;
 static int exact_deviates = 1;
 static char conf_copy[FILENAME_MAX];
+/* refh_run_files: potentials file per bunch (NULL: none) and the
+   amplitude invariants of the current turn, nbunch x 6 (NULL: none) */
+static FILE **pot_fps = NULL;
+static double *ampinv_turn = NULL;
 /* Bunches [range_lo, range_hi) are generated, set up and tracked; the
    others keep zero histograms and dipoles, so a process that tracks a
    share of the ring still does the ring-wide phasor and RW work of a full
@@ -371,7 +375,8 @@ int refh_run(long nturns, double *stats, float *dev, long dev_cap)
       worker_t *w = &W[ib];
       if (!IN_RANGE(ib)) continue;
       if (w->sf.PlaneL + w->sf.PlaneV + w->sf.PlaneH + lr_res_sizetot > 0)
-        transform_weak_bunch_selffield(&w->bunch, w->sf, NULL, &w->ring, rev, devnull,
+        transform_weak_bunch_selffield(&w->bunch, w->sf, NULL, &w->ring, rev,
+                                       (pot_fps && pot_fps[ib]) ? pot_fps[ib] : devnull,
                                        w->scan_val, w->kb, &ebeam, w->phasor_end[LON],
                                        w->phasor_end[HOR], w->phasor_end[VER],
                                        fnp_ring, fnp_hor, fnp_ver);
@@ -396,6 +401,15 @@ int refh_run(long nturns, double *stats, float *dev, long dev_cap)
       transform_weak_bunch_optic(&w->bunch, &w->model, w->iseed + (int) rev, w->kb, &w->ring);
       weak_bunch_calc_statistics(&w->bunch, &track);
       if (stats) put_stats(&w->bunch, stats + (t * nbunch + ib) * 12);
+      /* worker_weakweak.c:327-332: invariants before the RW kick */
+      if (ampinv_turn && (rev + 1) % track.NrevMon == 0) {
+        int k;
+        weak_bunch_calc_ampinv(&w->bunch, &track);
+        for (k = 0; k < 3; k++) {
+          ampinv_turn[6 * ib + k] = w->bunch.stats.ampinv.v[k];
+          ampinv_turn[6 * ib + 3 + k] = w->bunch.stats.ampinv_cm.v[k];
+        }
+      }
     }
     /* 5. dipole history */
     if (track.EnableRW_long > 0) {
@@ -608,4 +622,207 @@ void refh_ampinv(int ib, double *out6)
     out6[k] = W[ib].bunch.stats.ampinv.v[k];
     out6[3 + k] = W[ib].bunch.stats.ampinv_cm.v[k];
   }
+}
+
+/* ------------------------------------------------------------------ */
+/* A whole run with the reference's output files                       */
+
+/* The rest of the run (after refh_prepare) writing, into track.work_path,
+ * the files of manager_weakweak (mean_bunch_all.dat, ampinv_<P>_<rev>.dat,
+ * mean_bunch_end.dat, bunchbybunch_<P>.dat, ampinv_<P>_mean.dat) and of the
+ * output workers (wakes.dat, mean_bunch_<kb>.dat, potentials_bunch_<kb>.dat,
+ * dipoles_history.dat, the distribution files).  Every number is printed by
+ * the reference's own functions (bunch_stats_fprintf, worker_weak_stat_
+ * output, bunch_weak_writeout_ampinv, weak_bunch_writeout_tbtbbb,
+ * weak_bunch_writeout_mean_ampinv, weak_writeout_bunch_distribution, and
+ * transform_weak_bunch_selffield for the potentials) from the reference's
+ * accumulators; the manager/worker control flow around them follows
+ * manager_weakweak.c:104-349 and worker_weakweak.c:96-106, 225-302,
+ * 394-438, with the MPI messages replaced by reads of the bunch state.
+ * Where several output workers write one file the reference keeps the
+ * last one to finish; here the first output bunch's content is kept.
+ *
+ * stats: NrevTot x nbunch x 12, ampinv: NrevTot x nbunch x 6 (monitor
+ * turns filled), vrfphi: NrevTot x nbunch x 2 (RF voltage and phase at the
+ * start of each turn), end_stats: nbunch x 12.  Returns 0 or < 0. */
+int refh_run_files(double *stats, double *ampinv, double *vrfphi, double *end_stats)
+{
+  const long tot = track.NrevTot, mon = track.NrevMon;
+  const int H = (int) ring.Nharm;
+  int ib, pl;
+  long rev, nstat = 0;
+  long *nstat_w = (long *) calloc(nbunch, sizeof(long));
+  FILE **out_fp = (FILE **) calloc(nbunch, sizeof(FILE *));
+  char fn[FILENAME_MAX];
+  bunch_CM_history_weak_t cmhist;
+  bunch_stats_t allstats;
+  double *scan_val_hist = (double *) calloc(tot / mon + track.Nscan + 1, sizeof(double));
+  double scan_val = track.scan_start;
+  int m = 0;
+  FILE *all_fp;
+
+  pot_fps = (FILE **) calloc(nbunch, sizeof(FILE *));
+  bunch_CM_history_weak_init(&cmhist, (int) (tot / mon * nbunch));
+
+  /* manager_weakweak.c:104-127 */
+  snprintf(fn, FILENAME_MAX, "%s/mean_bunch_all.dat", track.work_path);
+  all_fp = fopen(fn, "w+");
+  if (!all_fp) return -1;
+  weak_bunch_reset_statistics(&allstats);
+  for (ib = 0; ib < nbunch; ib++) weak_bunch_add_statistics(&allstats, &W[ib].bunch.stats);
+  weak_bunch_update_statistics(&allstats, nbunch);
+  fprintf(all_fp, " # bunch statistics, AVEraged over all bunches & turns, Ib = %g A ;\n", W[0].bunch.Ib);
+  fprintf(all_fp, " # turn - scan_var - AVE_CM_LON - SIG_CM_LON - AVE_delE_LON - SIG_delE_LON -  AVE_sigmaL_LON - SIG_sigmaL_LON - AVE_sigmaE_LON - SIG_sigmaE_LON... (_HOR) ... (_VER)\n # ");
+  bunch_stats_fprintf(all_fp, -100, &allstats, 0.0);
+  fprintf(all_fp, "\n");
+  weak_bunch_reset_statistics(&allstats);
+
+  /* output workers: worker_weakweak.c:96-106, 225-249 */
+  for (ib = 0; ib < nbunch; ib++) {
+    worker_t *w = &W[ib];
+    int nc;
+    if (w->bunch.kb_out != 1) continue;
+    snprintf(fn, FILENAME_MAX, "%s/wakes.dat", track.work_path);
+    FILE *wf = fopen(fn, "w+");
+    if (wf) {
+      fprintf(wf, "# bin (%.2e s)   total wake L     - V -      - H -\n", w->sf.dT * w->sf.sigma_tau);
+      for (nc = 0; nc < w->sf.Ncell; nc++)
+        fprintf(wf, "%d  %e   %e   %e\n", nc, w->sf.Gl[nc], w->sf.Gv[nc], w->sf.Gh[nc]);
+      fclose(wf);
+    }
+    snprintf(fn, FILENAME_MAX, "%s/mean_bunch_%d.dat", track.work_path, w->kb);
+    out_fp[ib] = fopen(fn, "w+");
+    if (!out_fp[ib]) return -1;
+    worker_weak_stat_output(out_fp[ib], &w->bunch.stats, w->bunch.Ib);
+    weak_bunch_reset_statistics(&w->bunch.stats);
+    if (track.NrevPotentialsOut <= track.NrevTot) {
+      snprintf(fn, FILENAME_MAX, "%s/potentials_bunch_%d.dat", track.work_path, w->kb);
+      pot_fps[ib] = fopen(fn, "w+");
+      if (!pot_fps[ib]) return -1;
+      fprintf(pot_fps[ib], " # potentials and distributions, Ib = %g A ;\n", w->bunch.Ib);
+      fprintf(pot_fps[ib], " # rev  scan_val         tau         LON_wake_pot       HC_pot        rf_pot      active_cav      ideal_HC        bunch_shape");
+      if (w->sf.PlaneV > 0) fprintf(pot_fps[ib], "     VER_wake_pot     VER_dipole_mom");
+      if (w->sf.PlaneH > 0) fprintf(pot_fps[ib], "     HOR_wake_pot     HOR_dipole_mom");
+      fprintf(pot_fps[ib], "\n");
+    }
+  }
+
+  ampinv_turn = (double *) calloc((size_t) nbunch * 6, sizeof(double));
+  for (rev = 0; rev < tot; rev++) {
+    double *st = stats + (size_t) rev * nbunch * 12;
+    for (ib = 0; ib < nbunch; ib++) {
+      vrfphi[((size_t) rev * nbunch + ib) * 2] = W[ib].ring.Vrf0;
+      vrfphi[((size_t) rev * nbunch + ib) * 2 + 1] = W[ib].ring.phai0;
+    }
+    refh_run(1, st, NULL, 0);
+    /* workers: worker_weakweak.c:290-302 */
+    for (ib = 0; ib < nbunch; ib++) {
+      if (W[ib].bunch.kb_out != 1) continue;
+      nstat_w[ib]++;
+      if (nstat_w[ib] % mon == 0 || (rev + 1) % track.NrevScan == 0) {
+        weak_bunch_update_statistics(&W[ib].bunch.stats, nstat_w[ib]);
+        bunch_stats_fprintf(out_fp[ib], rev, &W[ib].bunch.stats, W[ib].scan_val);
+        weak_bunch_reset_statistics(&W[ib].bunch.stats);
+        nstat_w[ib] = 0;
+      }
+    }
+    /* manager: manager_weakweak.c:235-302 */
+    for (ib = 0; ib < nbunch; ib++) {
+      bunch_stats_t *bs = &W[ib].bunch.stats;
+      if ((rev + 1) % mon == 0) {
+        const long irevmon = rev / mon;
+        int k;
+        for (k = 0; k < 3; k++) {
+          cmhist.ampinv[irevmon * nbunch + ib].v[k] = ampinv_turn[6 * ib + k];
+          cmhist.ampinv_cm[irevmon * nbunch + ib].v[k] = ampinv_turn[6 * ib + 3 + k];
+          ampinv[((size_t) rev * nbunch + ib) * 6 + k] = ampinv_turn[6 * ib + k];
+          ampinv[((size_t) rev * nbunch + ib) * 6 + 3 + k] = ampinv_turn[6 * ib + 3 + k];
+        }
+        cmhist.cm[irevmon * nbunch + ib] = bs->pos;
+      }
+      weak_bunch_add_statistics(&allstats, bs);
+    }
+    nstat++;
+    if (nstat % mon == 0 || (rev + 1) % track.NrevScan == 0) {
+      nstat *= nbunch;
+      weak_bunch_update_statistics(&allstats, nstat);
+      scan_val_hist[m] = scan_val;
+      m++;
+      if (track.EnableAmpinv_out) bunch_weak_writeout_ampinv(rev, rev / mon, &cmhist, ebeam);
+      bunch_stats_fprintf(all_fp, rev, &allstats, scan_val);
+      weak_bunch_reset_statistics(&allstats);
+      nstat = 0;
+    }
+  }
+  free(ampinv_turn);
+  ampinv_turn = NULL;
+
+  /* end statistics: worker_weakweak.c:396-404, manager_weakweak.c:307-331 */
+  snprintf(fn, FILENAME_MAX, "%s/mean_bunch_end.dat", track.work_path);
+  FILE *end_fp = fopen(fn, "w+");
+  if (!end_fp) return -1;
+  fprintf(end_fp, " # bunch statistics end of run, turns = %i; Ib = %g A ;\n", (int) tot, W[0].bunch.Ib);
+  fprintf(end_fp, " # bunch_num    CM    bunch_length    energy_dev    energy_spread;\n");
+  for (ib = 0; ib < nbunch; ib++) {
+    bunch_stats_t *bs = &W[ib].bunch.stats;
+    weak_bunch_calc_statistics(&W[ib].bunch, &track);
+    put_stats(&W[ib].bunch, end_stats + 12 * ib);
+    fprintf(end_fp, " %d     %e    %e    %e    %e\n", W[ib].kb, bs->pos.xtau, bs->pos_sigma.xtau, bs->slope.xtau, bs->slope_sigma.xtau);
+  }
+  fclose(end_fp);
+
+  /* output workers, last bunch first so the first one's files remain:
+     worker_weakweak.c:407-438 */
+  for (ib = nbunch - 1; ib >= 0; ib--) {
+    worker_t *w = &W[ib];
+    if (w->bunch.kb_out != 1) continue;
+    weak_writeout_bunch_distribution(&w->bunch, w->model, LON, w->model.nGen[LON]);
+    if (track.TrackPlane[HOR]) weak_writeout_bunch_distribution(&w->bunch, w->model, HOR, w->model.nGen[HOR]);
+    if (track.TrackPlane[VER]) weak_writeout_bunch_distribution(&w->bunch, w->model, VER, w->model.nGen[VER]);
+    if (track.EnableRW_long) {
+      int i, j;
+      snprintf(fn, FILENAME_MAX, "%s/dipoles_history.dat", track.work_path);
+      FILE *df = fopen(fn, "w+");
+      if (!df) return -1;
+      fprintf(df, " # history of dipole moments at rev = %i; Ib = %g A ;\n", (int) tot, w->bunch.Ib);
+      fprintf(df, " # Nhist  kb   rev   dipole_HOR    dipole_VER\n");
+      for (j = 0; j < track.Nmlt; j++)
+        for (i = 0; i < H; i++) {
+          const double *mom = cyclic_array_get((j * H + i), &dipole_rw);
+          fprintf(df, " %d    %d    %d           %e    %e \n", j * H + i, i, j, mom[0], mom[1]);
+        }
+      fclose(df);
+    }
+  }
+  for (ib = 0; ib < nbunch; ib++) {
+    if (out_fp[ib]) fclose(out_fp[ib]);
+    if (pot_fps[ib]) fclose(pot_fps[ib]);
+  }
+  free(pot_fps);
+  pot_fps = NULL;
+
+  /* manager_weakweak.c:333-345 */
+  weak_bunch_writeout_tbtbbb(tot, mon, &cmhist, ebeam, LON, scan_val_hist);
+  for (pl = HOR; pl <= VER; pl++)
+    if (track.TrackPlane[pl]) {
+      weak_bunch_writeout_mean_ampinv(tot, mon, &cmhist, ebeam, (plane_t) pl, scan_val_hist);
+      weak_bunch_writeout_tbtbbb(tot, mon, &cmhist, ebeam, (plane_t) pl, scan_val_hist);
+    }
+  fclose(all_fp);
+  bunch_CM_history_weak_destroy(&cmhist);
+  free(scan_val_hist);
+  free(nstat_w);
+  free(out_fp);
+  return 0;
+}
+
+/* Output settings and output buckets as the reference's set-up made them. */
+int refh_output_info(long *nrev_scan, long *nrev_pot, int *ampinv_out, int *bunch_out, int cap)
+{
+  int i;
+  *nrev_scan = track.NrevScan;
+  *nrev_pot = track.NrevPotentialsOut;
+  *ampinv_out = track.EnableAmpinv_out;
+  for (i = 0; i < track.Nbunch_out && i < cap; i++) bunch_out[i] = track.bunch_out[i];
+  return track.Nbunch_out;
 }

@@ -25,6 +25,40 @@ def small_conf(tmp_path, name, **overrides):
     return conf_with(src, dst, **overrides)
 
 
+def add_tracking_keys(path, **keys):
+    """Insert `key = value` lines at the top of the [tracking] section (for
+    optional keys the fixture files do not carry)."""
+    text = open(path).read()
+    lines = "".join("\n  %s = %s" % (k, v) for k, v in keys.items())
+    text = text.replace("[tracking]", "[tracking]" + lines, 1)
+    with open(path, "w") as f:
+        f.write(text)
+    return path
+
+
+# Output-file cases: (conf, overrides, [tracking] additions).  The
+# distribution files are named relative to the working directory.
+WRITER_CASES = {
+    "single": ("single_bunch.conf",
+               {"Np": 200, "NrevTot": 40, "NrevMon": 20, "xxCM_offset": 0.05, "zzCM_offset": 0.02,
+                "gendst_datafile_LON": "dist_LON.dat", "gendst_datafile_HOR": "dist_HOR.dat",
+                "gendst_datafile_VER": "dist_VER.dat"},
+               {"EnableAmpinv_out": 1}),
+    "train_rw": ("uniform_fill.conf",
+                 {"Np": 100, "Nmlt": 2, "filling": "SINGLE10", "NrevTot": 30, "NrevMon": 10,
+                  "EnableQuantum": 0, "xxCM_offset": 0.05,
+                  "gendst_datafile_LON": "dist_LON.dat", "gendst_datafile_HOR": "dist_HOR.dat",
+                  "gendst_datafile_VER": "dist_VER.dat"},
+                 {"EnableAmpinv_out": 1, "NrevPotentialsOut": 15}),
+}
+
+
+def writer_conf(tmp_path, case):
+    name, over, add = WRITER_CASES[case]
+    path = small_conf(tmp_path, name, **over)
+    return add_tracking_keys(path, **add)
+
+
 def coord_err(a, b):
     """Largest difference per coordinate, relative to that coordinate's rms
     spread in b (coordinates near zero have no meaningful relative error)."""

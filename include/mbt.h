@@ -369,6 +369,65 @@ int mbt_bunch_moments_dev_noalloc(int np, const double *coord_dev,
                                   double *stats, double *hist_dev,
                                   void *stream);
 
+/* ---- beam-ion interaction (weak-strong, per macroparticle) ------------- */
+
+/* Fast beam-ion interaction of a bunch train with the residual gas.  The
+ * reference models it with rigid electron slices and one lumped
+ * interaction point (fbi_weakstrong.c:45-451, factF :40, gas density
+ * :20-35); this stage follows its physics with every electron
+ * macroparticle kicked:
+ *   - n_ip interaction points at betatron phase advances 2 pi Q k / n_ip
+ *     from the kick point (same Twiss functions), each with its own ion
+ *     cloud, cleared every turn by the gap after the train;
+ *   - at every bunch passage each point creates ions_per_passage
+ *     macro-ions from the bunch's transverse Gaussian (Philox stream keyed
+ *     by seed), worth Ne sigma_ion n_gas (Lc / n_ip) / ions_per_passage ions
+ *     each (n_gas = 3.22e22 P[Torr] m^-3 as fbi_weakstrong.c:24);
+ *   - between passages the ions drift (fbi_weakstrong.c:370-375); each
+ *     passage kicks them with the Bassetti-Erskine field of the bunch
+ *     (fbi_weakstrong.c:154-197, :393-405) and kicks every electron with the
+ *     field of the cloud's Gaussian (total ions, centroid, rms), the
+ *     thin-lens deflection -2 pi r_e N G / gamma, mapped back to the kick
+ *     point through the linear optics;
+ *   - it runs after the turn's statistics, like the resistive-wall kick.
+ * Both transverse planes must be tracked. */
+typedef struct mbt_beam_ion {
+  int      n_ip;              /* interaction points */
+  int      ions_per_passage;  /* macro-ions per bunch passage per point */
+  double   gas_A;             /* ion mass number */
+  double   pressure;          /* [Torr] */
+  double   sigma_ion;         /* ionisation cross-section [m^2] */
+  uint64_t seed;              /* key of the ion-generation stream */
+  int      surrogate;         /* 0: Faddeeva field, 1: MLP surrogate */
+  double   audit_fraction;    /* share of surrogate fields re-evaluated exactly */
+} mbt_beam_ion;
+
+/* The [beam_ion] section of a .conf file (n_ip, ions_per_passage, gas_A,
+ * pressure_nTorr, sigma_ion_Mb, seed, surrogate, audit_fraction).
+ * Returns 1 when the section is absent (bi untouched), 0 when read. */
+int mbt_config_beam_ion(const char *conf_path, mbt_beam_ion *bi);
+
+/* Switch the stage on for a context; call before mbt_prepare. */
+int mbt_enable_beam_ion(mbt_ctx *ctx, const mbt_beam_ion *bi);
+
+/* The ion clouds every bunch met in the last turn: n_ip x nbunch x 5
+ * doubles (ions, centroid x, centroid y [m], rms x, rms y [m] in the
+ * frame of the interaction point). */
+int mbt_beam_ion_clouds(mbt_ctx *ctx, double *clouds);
+
+/* Average device time [ms] of the beam-ion stage per turn in the last
+ * mbt_profile_turns call (0 when the stage is off). */
+int mbt_beam_ion_timing(mbt_ctx *ctx, double *ms_per_turn);
+
+/* Unit-charge field of an elliptic Gaussian at n points (device arrays):
+ * E = lambda / (2 eps0) (gx, gy) for line density lambda.  Bassetti-
+ * Erskine with w(z) for aspect ratios up to 0.995, a Gauss-Legendre
+ * quadrature of the field integral closer to round; axes swapped when
+ * sy > sx.  The function every beam-ion kick uses. */
+int mbt_gauss_field_dev(long n, const double *dx_dev, const double *dy_dev,
+                        const double *sx_dev, const double *sy_dev,
+                        double *gx_dev, double *gy_dev, void *stream);
+
 /* ---- output files (C host; the reference's text formats) ------------- */
 
 /* A writer produces, in work_path, the files the reference's manager and

@@ -92,6 +92,14 @@ class MbtOutputCfg(ctypes.Structure):
 MBT_WRITER_OWN_AMPINV = 1
 
 
+class MbtBeamIon(ctypes.Structure):
+    """mbt_beam_ion (include/mbt.h)."""
+    _fields_ = [
+        ("n_ip", _i), ("ions_per_passage", _i), ("gas_A", _d), ("pressure", _d),
+        ("sigma_ion", _d), ("seed", ctypes.c_uint64), ("surrogate", _i), ("audit_fraction", _d),
+    ]
+
+
 def params_to_dict(p):
     """Flatten an MbtParams into {field: scalar or nested list}."""
     out = {}

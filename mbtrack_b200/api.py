@@ -11,8 +11,8 @@ import os
 
 import numpy as np
 
-from .abi import (MBT_NOISE_INJECTED, MBT_NOISE_PHILOX, MBT_WRITER_OWN_AMPINV, MbtOutputCfg, MbtParams,
-                  MbtState)
+from .abi import (MBT_NOISE_INJECTED, MBT_NOISE_PHILOX, MBT_WRITER_OWN_AMPINV, MbtBeamIon, MbtOutputCfg,
+                  MbtParams, MbtState)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmbt.so")
@@ -69,6 +69,11 @@ SIGNATURES = {
     "mbt_writer_distribution": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
     "mbt_writer_close": (ctypes.c_int, [_vp]),
     "mbt_writer_error": (ctypes.c_char_p, []),
+    "mbt_config_beam_ion": (ctypes.c_int, [ctypes.c_char_p, _P(MbtBeamIon)]),
+    "mbt_enable_beam_ion": (ctypes.c_int, [_vp, _P(MbtBeamIon)]),
+    "mbt_beam_ion_clouds": (ctypes.c_int, [_vp, _vp]),
+    "mbt_beam_ion_timing": (ctypes.c_int, [_vp, _vp]),
+    "mbt_gauss_field_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mbt_wofz_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mbt_be_field_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, _vp, _vp, _vp]),
@@ -150,6 +155,17 @@ class Config:
         if rc != 0:
             raise MbtError(rc, L.mbt_config_error().decode())
         return o, out[:o.n_out].copy()
+
+    def beam_ion(self):
+        """The [beam_ion] section (MbtBeamIon), or None when absent."""
+        L = lib()
+        bi = MbtBeamIon()
+        rc = L.mbt_config_beam_ion(self.path.encode(), ctypes.byref(bi))
+        if rc == 1:
+            return None
+        if rc != 0:
+            raise MbtError(rc, L.mbt_config_error().decode())
+        return bi
 
     def reference_beam(self, np_=None):
         """The reference's initial distribution of every bunch (host),
@@ -294,6 +310,20 @@ class Tracker:
         s = np.zeros(12 * self.nb)
         _check(lib().mbt_get_stats(self.h, _ptr(s)), self.h)
         return s.reshape(self.nb, 12)
+
+    def enable_beam_ion(self, bi):
+        _check(lib().mbt_enable_beam_ion(self.h, ctypes.byref(bi)), self.h)
+        self.bi = bi
+
+    def beam_ion_clouds(self):
+        a = np.zeros(self.bi.n_ip * self.nb * 5)
+        _check(lib().mbt_beam_ion_clouds(self.h, _ptr(a)), self.h)
+        return a.reshape(self.bi.n_ip, self.nb, 5)
+
+    def beam_ion_timing(self):
+        v = ctypes.c_double()
+        _check(lib().mbt_beam_ion_timing(self.h, ctypes.byref(v)), self.h)
+        return v.value
 
     def watch_potentials(self, bunches):
         b = np.ascontiguousarray(bunches, dtype=np.int32)

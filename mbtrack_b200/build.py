@@ -31,7 +31,8 @@ C_SOURCES = ["mbt_host.c", "mbt_beam.c", "mbt_output.c"]
 # the drop-in executable for mbtrack-mpi's weak-weak runs
 CLI_SOURCE = "mbtrack_gpu.c"
 CLI = os.path.join(HERE, "mbtrack-gpu")
-HEADERS = ["mbt_common.cuh", "mbt_device.cuh", "mbt_kernels.cuh", "mbt_philox.cuh", "mbt_wofz.cuh"]
+HEADERS = ["mbt_beamion.cuh", "mbt_common.cuh", "mbt_device.cuh", "mbt_kernels.cuh", "mbt_philox.cuh",
+           "mbt_wofz.cuh"]
 
 
 def _run(cmd):

@@ -120,6 +120,7 @@ struct Args {
   double *hist;               // nbunch x 6 x ncell: fnp, dipV, dipH (clamped), ring L, H, V (dropped)
   int *cellrange;             // nbunch x 2: icellmin, icellmax
   double *kick;               // nbunch x 3 x ncell: L, V, H kick tables
+  double *bi_mom;             // nbunch x 10: transverse moments for the beam-ion stage, or null
   double *pot;                // watched bunches x 7 x ncell: potential terms of the next turn, or null
   const int *pot_slot;        // nbunch: watch slot or -1
   double *rw_part;            // nbunch x kRwSplit x 2: partial RW kicks (HOR, VER)

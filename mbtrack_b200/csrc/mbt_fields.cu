@@ -19,6 +19,41 @@ int fail_global(int code, const char *fmt, ...);
     if (e_ != cudaSuccess) return mbt::fail_global(MBT_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
   } while (0)
 
+namespace mbt {
+
+__global__ void wofz_kernel(long n, const double *__restrict__ x, const double *__restrict__ y,
+                            double *__restrict__ re, double *__restrict__ im, int *__restrict__ flag) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double u, v;
+    const int f = wofz_dev(x[i], y[i], u, v);
+    re[i] = u;
+    im[i] = v;
+    if (flag) flag[i] = f;
+  }
+}
+
+// fbi_weakstrong.c:155-191 for one slice: sizes in mm, offsets in m.
+__global__ void be_field_kernel(long n, const double *__restrict__ dx, const double *__restrict__ dy,
+                                double sgm_xx, double sgm_zz, double factdQ,
+                                double *__restrict__ ex, double *__restrict__ ey) {
+  const double factBE = sqrt(2 * (sgm_xx * sgm_xx - sgm_zz * sgm_zz)) / 1.0e3;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double Dx = dx[i], Dy = dy[i];
+    const double xi1 = Dx / factBE;
+    const double xi2 = xi1 * sgm_zz / sgm_xx;
+    const double yi1 = Dy / factBE;
+    const double yi2 = yi1 * sgm_xx / sgm_zz;
+    double u1r, u1i, u2r, u2i;
+    wofz_dev(xi1, yi1, u1r, u1i);
+    wofz_dev(xi2, yi2, u2r, u2i);
+    const double e = exp(-(Dx * Dx * 1.0e6 / (2 * sgm_xx * sgm_xx) + Dy * Dy * 1.0e6 / (2 * sgm_zz * sgm_zz)));
+    ex[i] = -factdQ * (u1i - e * u2i);
+    ey[i] = -factdQ * (u1r - e * u2r);
+  }
+}
+
+}  // namespace mbt
+
 namespace {
 int check_device() {
   int n = 0;

@@ -788,6 +788,39 @@ int mbt_config_output(const char *conf_path, mbt_output_cfg *o, int *bunch_out)
   return r;
 }
 
+/* [beam_ion]: the stage of mbt_enable_beam_ion (no reference section; the
+ * defaults are the reference's CO model, fbi_weakstrong.c:18-43, with the
+ * gas spread over the whole ring) */
+int mbt_config_beam_ion(const char *conf_path, mbt_beam_ion *bi)
+{
+  conf_t C;
+  double tmp;
+  int r = 0, itmp;
+  if (!conf_path || !bi) return MBT_ERR_INVALID;
+  if (conf_read(conf_path, &C) != 0) return cfg_fail("cannot open %s", conf_path);
+  if (!have_section(&C, "beam_ion")) { conf_free(&C); return 1; }
+  memset(bi, 0, sizeof(*bi));
+  bi->n_ip = 1;
+  bi->ions_per_passage = 1000;
+  bi->gas_A = 28.0;
+  bi->pressure = 1.0e-9;
+  bi->sigma_ion = 1.78e-22;
+  bi->seed = 1;
+  bi->audit_fraction = 0.01;
+  if (get_int(&C, "beam_ion", "n_ip", &itmp)) bi->n_ip = itmp;
+  if (get_int(&C, "beam_ion", "ions_per_passage", &itmp)) bi->ions_per_passage = itmp;
+  if (get_double(&C, "beam_ion", "gas_A", &tmp)) bi->gas_A = tmp;
+  if (get_double(&C, "beam_ion", "pressure_nTorr", &tmp)) bi->pressure = tmp * FNANO;
+  if (get_double(&C, "beam_ion", "sigma_ion_Mb", &tmp)) bi->sigma_ion = tmp * 1.0e-22;
+  if (get_int(&C, "beam_ion", "seed", &itmp)) bi->seed = (uint64_t) (uint32_t) itmp;
+  if (get_int(&C, "beam_ion", "surrogate", &itmp)) bi->surrogate = itmp;
+  if (get_double(&C, "beam_ion", "audit_fraction", &tmp)) bi->audit_fraction = tmp;
+  if (bi->n_ip < 1 || bi->ions_per_passage < 1 || !(bi->gas_A > 0) || bi->pressure < 0 || bi->sigma_ion < 0)
+    r = cfg_fail("[beam_ion]: n_ip, ions_per_passage, gas_A must be positive");
+  conf_free(&C);
+  return r;
+}
+
 double mbt_bunch_current(const mbt_params *p, int nbunch, double ib_frac)
 {
   /* manager_weakweak.c:74-75 */

@@ -467,6 +467,24 @@ __global__ void __launch_bounds__(kBlock) bunch_reduce(Args a, int mode, double 
       row[3 + pl] = aic;
     }
   }
+  // transverse moments for the beam-ion stage: means, variances and the
+  // position-slope covariance per plane
+  if (a.bi_mom != nullptr && threadIdx.x < 2 && mode == kReduceTurn) {
+    const int pl = 1 + threadIdx.x;
+    double *m = a.bi_mom + (size_t)b * 10 + 5 * threadIdx.x;
+    double vu = 0.0, vp = 0.0, cuv = 0.0;
+    if (N > 0) {
+      const double su = ex[kMomSum + pl] / N, sp = ex[kMomSum + 3 + pl] / N;
+      vu = ex[kMomSq + pl] / N - su * su;
+      vp = ex[kMomSq + 3 + pl] / N - sp * sp;
+      cuv = ex[kMomCross + pl - 1] / N - su * sp;
+    }
+    m[0] = mean6[pl];
+    m[1] = mean6[3 + pl];
+    m[2] = vu;
+    m[3] = cuv;
+    m[4] = vp;
+  }
   if (threadIdx.x == 0 && a.selffield) {
     atomicAdd(&a.rs->trash_low, (int)ex[kTrLowN]);
     atomicAdd(&a.rs->trash_high, (int)ex[kTrHighN]);

@@ -16,6 +16,7 @@
 #include "mbt.h"
 #include "mbt_device.cuh"
 #include "mbt_kernels.cuh"
+#include "mbt_beamion.cuh"
 
 using mbt::Args;
 using mbt::LrConst;
@@ -68,6 +69,11 @@ struct mbt_ctx {
   double *stats_init = nullptr;
   double *xfer = nullptr;        // device staging for exports
   double *stat_scratch = nullptr; // block partials of mbt_get_stats
+  int bi_on = 0;                 // beam-ion stage
+  mbt_beam_ion bicfg{};
+  mbt::BiArgs bi{};
+  cudaEvent_t bi_ev = nullptr;   // end of the beam-ion stage (profiling)
+  double bi_ms = 0.0;            // its average device time in the last mbt_profile_turns
   std::vector<int> watch;        // bunches whose potentials are recorded
   cudaEvent_t ev[6] = {};
   double timing[4] = {0, 0, 0, 0};
@@ -200,7 +206,20 @@ size_t smem_scan(const mbt_ctx *c) {
   return c->p.rw_long ? mbt::rw_window_doubles(c->p.Nmlt, c->p.nharm) * sizeof(double) : 0;
 }
 
-// One turn: particle pass, bunch reduction, ring scan, bunch wakes.
+// The beam-ion stage of a turn: frames, ion clouds, electron kicks.
+void enqueue_beam_ion(mbt_ctx *c) {
+  const mbt::BiArgs &bi = c->bi;
+  const int n = bi.n_ip * bi.nb;
+  mbt::bi_frames<<<(n + 127) / 128, 128, 0, c->stream>>>(bi);
+  if (bi.nb > 1) {
+    mbt::bi_ions<<<dim3(bi.bpp, bi.nb - 1, bi.n_ip), mbt::kBiThreads, 0, c->stream>>>(bi);
+  }
+  mbt::bi_clouds<<<dim3(bi.nb, bi.n_ip), mbt::kBiThreads, 0, c->stream>>>(bi);
+  mbt::bi_kick<<<c->ntile, mbt::kBiThreads, 0, c->stream>>>(c->a, bi);
+}
+
+// One turn: particle pass, bunch reduction, ring scan, bunch wakes, and
+// the beam-ion stage when it is on.
 void enqueue_turn(mbt_ctx *c, cudaEvent_t *ev) {
   if (ev) cudaEventRecord(ev[0], c->stream);
   launch_map_noise<true>(c, effective_noise(c));
@@ -211,6 +230,10 @@ void enqueue_turn(mbt_ctx *c, cudaEvent_t *ev) {
   if (ev) cudaEventRecord(ev[3], c->stream);
   mbt::bunch_wakes<<<c->nbunch, mbt::kBlock, smem_wakes(c), c->stream>>>(c->a, 1);
   if (ev) cudaEventRecord(ev[4], c->stream);
+  if (c->bi_on) {
+    enqueue_beam_ion(c);
+    if (ev) cudaEventRecord(c->bi_ev, c->stream);
+  }
 }
 
 int sync_and_check(mbt_ctx *c) {
@@ -536,6 +559,7 @@ int mbt_destroy(mbt_ctx *c) {
   if (!c) return 0;
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->graph) cudaGraphExecDestroy(c->graph);
+  if (c->bi_ev) cudaEventDestroy(c->bi_ev);
   for (void *p : c->allocs) cudaFree(p);
   if (c->dev) cudaFree(c->dev);
   for (auto &e : c->ev) if (e) cudaEventDestroy(e);
@@ -681,6 +705,97 @@ int mbt_get_potentials(mbt_ctx *c, int ibunch, double *pot) {
   return 0;
 }
 
+int mbt_enable_beam_ion(mbt_ctx *c, const mbt_beam_ion *cfg) {
+  if (!c || !cfg) return MBT_ERR_INVALID;
+  if (c->prepared) return fail(c, MBT_ERR_STATE, "mbt_enable_beam_ion must precede mbt_prepare");
+  if (c->bi_on) return fail(c, MBT_ERR_STATE, "the beam-ion stage is already on");
+  const mbt_params *p = &c->p;
+  if (!p->track_plane[1] || !p->track_plane[2])
+    return fail(c, MBT_ERR_INVALID, "the beam-ion stage needs both transverse planes tracked");
+  if (cfg->n_ip < 1 || cfg->n_ip > mbt::kBiMaxIp)
+    return fail(c, MBT_ERR_INVALID, "n_ip %d outside 1..%d", cfg->n_ip, mbt::kBiMaxIp);
+  if (cfg->ions_per_passage < 1 || cfg->ions_per_passage > (1 << 20))
+    return fail(c, MBT_ERR_INVALID, "ions_per_passage %d outside 1..2^20", cfg->ions_per_passage);
+  if (!(cfg->gas_A > 0) || !(cfg->pressure >= 0) || !(cfg->sigma_ion >= 0))
+    return fail(c, MBT_ERR_INVALID, "gas_A must be positive, pressure and sigma_ion non-negative");
+  if (c->nbunch > 65535) return fail(c, MBT_ERR_INVALID, "the beam-ion stage serves up to 65535 bunches");
+  if (cfg->surrogate) return fail(c, MBT_ERR_INVALID, "the surrogate field is not available in this build");
+  // constants of the reference (def.h:21-26, input.c:1562)
+  const double c_light = 2.997925e+08, eps0 = 8.854187817620e-12, e_charge = 1.602e-19, e_mass = 9.1e-31;
+  const double r_e = 2.819e-15, mp_o_em = 1.836e3;
+  const double gamma = 1957.0 * p->E0;
+  const double factF = e_charge / (cfg->gas_A * mp_o_em * e_mass);     // fbi_weakstrong.c:40
+  const double n_gas = 3.22e22 * cfg->pressure;                       // fbi_weakstrong.c:24
+  const double L_ip = p->Lc / cfg->n_ip;
+  mbt::BiArgs &bi = c->bi;
+  bi.n_ip = cfg->n_ip;
+  bi.n_new = cfg->ions_per_passage;
+  bi.bpp = (cfg->ions_per_passage + mbt::kBiThreads - 1) / mbt::kBiThreads;
+  bi.nb = c->nbunch;
+  bi.T = (long)c->nbunch * (c->nbunch - 1) / 2;
+  bi.dt_bucket = p->T0 / p->nharm;
+  bi.kion_per_amp = -factF * p->T0 / (2.0 * eps0 * c_light);
+  bi.ke = -2.0 * PI * r_e / gamma;
+  bi.w_per_amp = p->T0 / e_charge * cfg->sigma_ion * n_gas * L_ip / cfg->ions_per_passage;
+  bi.betaH = p->beta1[1]; bi.alphaH = p->alpha1[1];
+  bi.betaV = p->beta1[2]; bi.alphaV = p->alpha1[2];
+  bi.keys = mbt::philox_keys(cfg->seed);
+  std::vector<double> trig((size_t)4 * cfg->n_ip);
+  for (int k = 0; k < cfg->n_ip; ++k) {
+    const double mux = 2.0 * PI * p->QH0 * k / cfg->n_ip, muy = 2.0 * PI * p->QV0 * k / cfg->n_ip;
+    trig[4 * k] = cos(mux); trig[4 * k + 1] = sin(mux);
+    trig[4 * k + 2] = cos(muy); trig[4 * k + 3] = sin(muy);
+  }
+  std::vector<double> ibv(c->ib.begin(), c->ib.end());
+  double *tr = nullptr, *mom = nullptr, *frame = nullptr, *part = nullptr, *cloud = nullptr, *ibd = nullptr;
+  const size_t nslot = (size_t)cfg->n_ip * std::max<long>(bi.T, 1) * bi.bpp * 5;
+  int r = dupload(c, &tr, trig.data(), trig.size());
+  if (!r) r = dalloc(c, &mom, (size_t)c->nbunch * 10);
+  if (!r) r = dalloc(c, &frame, (size_t)cfg->n_ip * c->nbunch * 4);
+  if (!r) r = dalloc(c, &part, nslot);
+  if (!r) r = dalloc(c, &cloud, (size_t)cfg->n_ip * c->nbunch * 5);
+  if (!r) r = dupload(c, &ibd, ibv.data(), ibv.size());
+  if (r) return r;
+  bi.trig = tr; bi.mom = mom; bi.frame = frame; bi.part = part; bi.cloud = cloud; bi.ib = ibd;
+  bi.bunch_kb = c->a.bunch_kb;
+  bi.turn = &c->a.rs->turn;
+  c->a.bi_mom = mom;
+  if (!c->bi_ev) CK(cudaEventCreate(&c->bi_ev));
+  c->bicfg = *cfg;
+  c->bi_on = 1;
+  if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; c->graph_turns = 0; }
+  return 0;
+}
+
+int mbt_beam_ion_clouds(mbt_ctx *c, double *clouds) {
+  if (!c || !clouds) return MBT_ERR_INVALID;
+  if (!c->bi_on) return fail(c, MBT_ERR_STATE, "the beam-ion stage is off");
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(clouds, c->bi.cloud, (size_t)c->bi.n_ip * c->nbunch * 5 * sizeof(double), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int mbt_beam_ion_timing(mbt_ctx *c, double *ms_per_turn) {
+  if (!c || !ms_per_turn) return MBT_ERR_INVALID;
+  *ms_per_turn = c->bi_on ? c->bi_ms : 0.0;
+  return 0;
+}
+
+int mbt_gauss_field_dev(long n, const double *dx, const double *dy, const double *sx, const double *sy, double *gx,
+                        double *gy, void *stream) {
+  if (n < 0 || (n > 0 && (!dx || !dy || !sx || !sy || !gx || !gy)))
+    return mbt::fail_global(MBT_ERR_INVALID, "bad gauss_field arguments");
+  if (n == 0) return 0;
+  int nd = 0;
+  if (cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0)
+    return mbt::fail_global(MBT_ERR_NODEVICE, "no CUDA device: libmbt has no CPU path");
+  const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 16);
+  mbt::gauss_field_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(n, dx, dy, sx, sy, gx, gy);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return mbt::fail_global(MBT_ERR_CUDA, "gauss_field: %s", cudaGetErrorString(e));
+  return 0;
+}
+
 int mbt_prepare(mbt_ctx *c, double *init_stats) {
   if (!c) return MBT_ERR_INVALID;
   Args &a = c->a;
@@ -811,19 +926,25 @@ int mbt_track(mbt_ctx *c, double *particles, long nturns, double *stats) {
 int mbt_profile_turns(mbt_ctx *c, long nturns, double out[4]) {
   if (!c || nturns <= 0 || !out) return MBT_ERR_INVALID;
   if (!c->prepared) return fail(c, MBT_ERR_STATE, "mbt_prepare must come first");
-  double acc[4] = {0, 0, 0, 0};
+  double acc[4] = {0, 0, 0, 0}, acc_bi = 0.0;
   for (long t = 0; t < nturns; ++t) {
     enqueue_turn(c, c->ev);
-    CK(cudaEventSynchronize(c->ev[4]));
+    CK(cudaEventSynchronize(c->bi_on ? c->bi_ev : c->ev[4]));
     for (int k = 0; k < 4; ++k) {
       float ms = 0;
       cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]);
       acc[k] += ms;
     }
+    if (c->bi_on) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, c->ev[4], c->bi_ev);
+      acc_bi += ms;
+    }
   }
   int r = sync_and_check(c);
   if (r) return r;
   for (int k = 0; k < 4; ++k) out[k] = acc[k] / nturns;
+  c->bi_ms = acc_bi / nturns;
   return 0;
 }
 

@@ -1,5 +1,6 @@
-// mbt_wofz.cuh -- Faddeeva function w(z) = exp(-z^2) erfc(-iz) in FP64 and
-// the Bassetti-Erskine field of a flat Gaussian slice.
+// mbt_wofz.cuh -- Faddeeva function w(z) = exp(-z^2) erfc(-iz) in FP64, the
+// building block of every Bassetti-Erskine field (mbt_fields.cu,
+// mbt_beamion.cuh).
 //
 // Algorithm: ACM TOMS 680 (G. P. M. Poppe and C. M. J. Wijers, "More
 // efficient computation of the complex error function", ACM Trans. Math.
@@ -8,8 +9,7 @@
 // (physic.c:143-301): power series (Abramowitz & Stegun 7.1.5) for
 // qrho < 0.085264, Laplace continued fraction for qrho > 1, Taylor series
 // with continued-fraction derivatives in between, reflection w(conj z)
-// relations for the lower half plane.  Branches are per point; the BE kernel
-// evaluates two points per field value (fbi_weakstrong.c:171-180).
+// relations for the lower half plane.  Branches are per point.
 #pragma once
 
 namespace mbt {
@@ -105,37 +105,6 @@ __device__ __forceinline__ int wofz_dev(double xi, double yi, double &re, double
   re = u;
   im = v;
   return 1;
-}
-
-__global__ void wofz_kernel(long n, const double *__restrict__ x, const double *__restrict__ y,
-                            double *__restrict__ re, double *__restrict__ im, int *__restrict__ flag) {
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    double u, v;
-    const int f = wofz_dev(x[i], y[i], u, v);
-    re[i] = u;
-    im[i] = v;
-    if (flag) flag[i] = f;
-  }
-}
-
-// fbi_weakstrong.c:155-191 for one slice: sizes in mm, offsets in m.
-__global__ void be_field_kernel(long n, const double *__restrict__ dx, const double *__restrict__ dy,
-                                double sgm_xx, double sgm_zz, double factdQ,
-                                double *__restrict__ ex, double *__restrict__ ey) {
-  const double factBE = sqrt(2 * (sgm_xx * sgm_xx - sgm_zz * sgm_zz)) / 1.0e3;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    const double Dx = dx[i], Dy = dy[i];
-    const double xi1 = Dx / factBE;
-    const double xi2 = xi1 * sgm_zz / sgm_xx;
-    const double yi1 = Dy / factBE;
-    const double yi2 = yi1 * sgm_xx / sgm_zz;
-    double u1r, u1i, u2r, u2i;
-    wofz_dev(xi1, yi1, u1r, u1i);
-    wofz_dev(xi2, yi2, u2r, u2i);
-    const double e = exp(-(Dx * Dx * 1.0e6 / (2 * sgm_xx * sgm_xx) + Dy * Dy * 1.0e6 / (2 * sgm_zz * sgm_zz)));
-    ex[i] = -factdQ * (u1i - e * u2i);
-    ey[i] = -factdQ * (u1r - e * u2r);
-  }
 }
 
 }  // namespace mbt

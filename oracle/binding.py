@@ -186,6 +186,18 @@ class Oracle:
         self.lib.orc_ampinv(self.h, ib, _ptr(out))
         return out
 
+    def enable_beam_ion(self, bi):
+        from mbtrack_b200.abi import MbtBeamIon
+        self.lib.orc_enable_beam_ion.argtypes = [_vp, _P(MbtBeamIon)]
+        self.lib.orc_enable_beam_ion(self.h, ctypes.byref(bi))
+        self.bi = bi
+
+    def beam_ion_clouds(self):
+        a = np.zeros(self.bi.n_ip * self.nb * 5)
+        self.lib.orc_beam_ion_clouds.argtypes = [_vp, _vp]
+        self.lib.orc_beam_ion_clouds(self.h, _ptr(a))
+        return a.reshape(self.bi.n_ip, self.nb, 5)
+
     def histograms(self, ib):
         n = self.p.ncell
         arr = [np.zeros(n) for _ in range(6)]
@@ -203,6 +215,21 @@ def wofz(x, y):
     lib.orc_wofz_n.argtypes = [ctypes.c_long, _vp, _vp, _vp, _vp, _vp]
     lib.orc_wofz_n(x.size, _ptr(x), _ptr(y), _ptr(re), _ptr(im), _ptr(fl))
     return re, im, fl
+
+
+def gauss_field(dx, dy, sx, sy):
+    """orc_gauss_field at every point (arrays of equal length)."""
+    L = ctypes.CDLL(build_oracle())
+    f = L.orc_gauss_field
+    f.argtypes = [ctypes.c_double] * 4 + [_P(ctypes.c_double)] * 2
+    dx, dy, sx, sy = [np.broadcast_to(np.asarray(a, dtype=np.float64), np.shape(dx)).ravel()
+                      for a in (dx, dy, sx, sy)]
+    gx, gy = np.zeros(dx.size), np.zeros(dx.size)
+    a, b = ctypes.c_double(), ctypes.c_double()
+    for i in range(dx.size):
+        f(dx[i], dy[i], sx[i], sy[i], ctypes.byref(a), ctypes.byref(b))
+        gx[i], gy[i] = a.value, b.value
+    return gx, gy
 
 
 def be_field(dx, dy, sgm_xx_mm, sgm_zz_mm, factdq):

@@ -7,6 +7,7 @@
  */
 #define _GNU_SOURCE
 #include <math.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -74,6 +75,12 @@ struct orc_ctx {
   float *dev_out;
   long dev_pos, dev_cap;
   int lo, hi;   /* bunches tracked by this instance (orc_set_range) */
+  /* beam-ion stage (orc_enable_beam_ion) */
+  int bi_on;
+  mbt_beam_ion bi;
+  double *bi_frame;   /* [n_ip][nb][4] */
+  double *bi_cloud;   /* [n_ip][nb][5] */
+  double *bi_sum;     /* [n_ip][nb][5] */
 };
 
 #define IN_RANGE(o, ib) ((ib) >= (o)->lo && (ib) < (o)->hi)
@@ -211,6 +218,7 @@ void orc_destroy(orc_ctx *o)
   }
   for (k = 0; k < 3; k++) free(o->fnp_ring[k]);
   free(o->dipole); free(o->b); free(o->filled); free(o->ibunch);
+  free(o->bi_frame); free(o->bi_cloud); free(o->bi_sum);
   free(o->Gl); free(o->Gv); free(o->Gh);
   free(o);
 }
@@ -754,6 +762,233 @@ long orc_deviates_per_turn(const orc_ctx *o)
 }
 
 /* worker_weakweak.c:259-394, phase by phase over the bunches */
+/* ------------------------------------------------------------ beam-ion */
+
+/* The beam-ion stage of mbt.h (mbt_beam_ion), restated loop by loop in
+ * plain C.  Physics after fbi_weakstrong.c (constants def.h:21-26, factF
+ * :40, gas density :24, ion drift :370-375, ion kick :393-405, the
+ * Bassetti-Erskine field :154-197 through orc_wofz); the per-particle
+ * electron kick, the interaction points at betatron phase advances and
+ * the cloud moments are the stage's own model. */
+
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) */
+typedef struct { uint32_t x, y, z, w; } u4_t;
+static u4_t philox10(u4_t c, uint64_t seed)
+{
+  uint32_t k0 = (uint32_t) seed, k1 = (uint32_t) (seed >> 32);
+  int i;
+  for (i = 0; i < 10; i++) {
+    const uint64_t p0 = (uint64_t) 0xD2511F53u * c.x, p1 = (uint64_t) 0xCD9E8D57u * c.z;
+    u4_t r;
+    r.x = (uint32_t) (p1 >> 32) ^ c.y ^ k0;
+    r.y = (uint32_t) p1;
+    r.z = (uint32_t) (p0 >> 32) ^ c.w ^ k1;
+    r.w = (uint32_t) p0;
+    c = r;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+static const double GL16_X[16] = {
+  0.005299532504175031, 0.0277124884633837, 0.06718439880608412, 0.1222977958224985,
+  0.19106187779867811, 0.2709916111713863, 0.35919822461037054, 0.4524937450811813,
+  0.5475062549188188, 0.6408017753896295, 0.7290083888286136, 0.8089381222013219,
+  0.8777022041775016, 0.9328156011939159, 0.9722875115366163, 0.994700467495825};
+static const double GL16_W[16] = {
+  0.013576229705877088, 0.031126761969323728, 0.0475792558412463, 0.062314485627767036,
+  0.07479799440828835, 0.08457825969750132, 0.09130170752246182, 0.09472530522753432,
+  0.09472530522753432, 0.09130170752246182, 0.08457825969750132, 0.07479799440828835,
+  0.062314485627767036, 0.0475792558412463, 0.031126761969323728, 0.013576229705877088};
+
+/* unit-charge field of an elliptic Gaussian (mbt_gauss_field_dev) */
+void orc_gauss_field(double dx, double dy, double sx, double sy, double *gx, double *gy)
+{
+  const double sgx = dx < 0.0 ? -1.0 : 1.0, sgy = dy < 0.0 ? -1.0 : 1.0;
+  double ax = fabs(dx), ay = fabs(dy), r, fx, fy;
+  const int swap = sy > sx;
+  if (swap) {
+    double t = ax; ax = ay; ay = t;
+    t = sx; sx = sy; sy = t;
+  }
+  if (sy < 1e-6 * sx) sy = 1e-6 * sx;
+  r = sy / sx;
+  if (r <= 0.995) {
+    const double fbe = sqrt(2.0 * (sx * sx - sy * sy));
+    const double x1 = ax / fbe, y1 = ay / fbe;
+    double w1r, w1i, w2r, w2i, e, c;
+    orc_wofz(x1, y1, &w1r, &w1i);
+    orc_wofz(x1 * r, y1 / r, &w2r, &w2i);
+    e = exp(-(ax * ax / (2.0 * sx * sx) + ay * ay / (2.0 * sy * sy)));
+    c = 1.0 / (1.7724538509055160273 * fbe);
+    fx = c * (w1i - e * w2i);
+    fy = c * (w1r - e * w2r);
+  } else {
+    const double q = 1.0 - r * r, inv2 = 1.0 / (2.0 * sx * sx);
+    const double a0 = (ax * ax + ay * ay) * inv2;
+    const double T = a0 > 40.0 ? sqrt(40.0 / a0) : 1.0, h = 0.25 * T;
+    double ix = 0.0, iy = 0.0, c;
+    int pnl, i;
+    for (pnl = 0; pnl < 4; pnl++)
+      for (i = 0; i < 16; i++) {
+        const double t = h * (pnl + GL16_X[i]);
+        const double D = 1.0 - q * t * t;
+        const double f = t * exp(-(t * t) * (ax * ax + ay * ay / D) * inv2) / sqrt(D);
+        const double wgt = h * GL16_W[i];
+        ix += wgt * f;
+        iy += wgt * (f / D);
+      }
+    c = 1.0 / (M_PI * sx * sx);
+    fx = c * ax * ix;
+    fy = c * ay * iy;
+  }
+  if (swap) { double t = fx; fx = fy; fy = t; }
+  *gx = sgx * fx;
+  *gy = sgy * fy;
+}
+
+int orc_enable_beam_ion(orc_ctx *o, const mbt_beam_ion *bi)
+{
+  const size_t n = (size_t) bi->n_ip * o->nb;
+  o->bi = *bi;
+  o->bi_frame = (double *) calloc(n * 4, sizeof(double));
+  o->bi_cloud = (double *) calloc(n * 5, sizeof(double));
+  o->bi_sum = (double *) calloc(n * 5, sizeof(double));
+  o->bi_on = 1;
+  return 0;
+}
+
+void orc_beam_ion_clouds(const orc_ctx *o, double *clouds)
+{
+  memcpy(clouds, o->bi_cloud, (size_t) o->bi.n_ip * o->nb * 5 * sizeof(double));
+}
+
+/* one turn of the stage; `turn` keys the ion generation (turns completed) */
+static void beam_ion(orc_ctx *o, long turn)
+{
+  const mbt_params *p = &o->p;
+  const mbt_beam_ion *cfg = &o->bi;
+  const int nip = cfg->n_ip, nb = o->nb, nnew = cfg->ions_per_passage;
+  const double c_light = 2.997925e+08, eps0 = 8.854187817620e-12, e_charge = 1.602e-19, e_mass = 9.1e-31;
+  const double r_e = 2.819e-15, mp_o_em = 1.836e3, gamma = 1957.0 * p->E0;
+  const double factF = e_charge / (cfg->gas_A * mp_o_em * e_mass);
+  const double n_gas = 3.22e22 * cfg->pressure, L_ip = p->Lc / nip;
+  const double kion_per_amp = -factF * p->T0 / (2.0 * eps0 * c_light);
+  const double ke = -2.0 * M_PI * r_e / gamma;
+  const double w_per_amp = p->T0 / e_charge * cfg->sigma_ion * n_gas * L_ip / nnew;
+  const double dt_bucket = p->T0 / p->nharm;
+  const double bH = p->beta1[HOR], aH = p->alpha1[HOR], bV = p->beta1[VER], aV = p->alpha1[VER];
+  int k, b, b0, j, jp;
+  /* 1. moments of every bunch and its frame at every point */
+  for (b = 0; b < nb; b++) {
+    const orc_bunch *e = &o->b[b];
+    double m[10];
+    int pl;
+    for (pl = 0; pl < 2; pl++) {
+      const double *u = e->c[1 + pl], *up = e->c[4 + pl];
+      double su = 0.0, sp = 0.0, vu = 0.0, vp = 0.0, cv = 0.0;
+      for (jp = 0; jp < e->np; jp++) { su += u[jp]; sp += up[jp]; }
+      su /= e->np; sp /= e->np;
+      for (jp = 0; jp < e->np; jp++) {
+        const double du = u[jp] - su, dp = up[jp] - sp;
+        vu += du * du; vp += dp * dp; cv += du * dp;
+      }
+      m[5 * pl] = su; m[5 * pl + 1] = sp;
+      m[5 * pl + 2] = vu / e->np; m[5 * pl + 3] = cv / e->np; m[5 * pl + 4] = vp / e->np;
+    }
+    for (k = 0; k < nip; k++) {
+      const double mux = 2.0 * M_PI * p->QH0 * k / nip, muy = 2.0 * M_PI * p->QV0 * k / nip;
+      const double mx = cos(mux) + aH * sin(mux), sxb = bH * sin(mux);
+      const double my = cos(muy) + aV * sin(muy), syb = bV * sin(muy);
+      double *F = o->bi_frame + ((size_t) k * nb + b) * 4;
+      const double vx = mx * mx * m[2] + 2.0 * mx * sxb * m[3] + sxb * sxb * m[4];
+      const double vy = my * my * m[7] + 2.0 * my * syb * m[8] + syb * syb * m[9];
+      F[0] = mx * m[0] + sxb * m[1];
+      F[1] = my * m[5] + syb * m[6];
+      F[2] = sqrt(vx > 0.0 ? vx : 0.0);
+      F[3] = sqrt(vy > 0.0 ? vy : 0.0);
+    }
+  }
+  /* 2. ions: created at passage b0, drift and kick at every later one */
+  memset(o->bi_sum, 0, (size_t) nip * nb * 5 * sizeof(double));
+  for (k = 0; k < nip; k++)
+    for (b0 = 0; b0 + 1 < nb; b0++)
+      for (j = 0; j < nnew; j++) {
+        const double *F0 = o->bi_frame + ((size_t) k * nb + b0) * 4;
+        u4_t c, r;
+        double u1, u2, u3, u4, x, y, vx = 0.0, vy = 0.0, w;
+        c.x = (uint32_t) j; c.y = (uint32_t) b0 | ((uint32_t) k << 20);
+        c.z = (uint32_t) turn; c.w = (uint32_t) ((uint64_t) turn >> 32);
+        r = philox10(c, cfg->seed);
+        u1 = ((double) r.x + 1.0) * 2.3283064365386962890625e-10;
+        u2 = (double) r.y * 2.3283064365386962890625e-10;
+        u3 = ((double) r.z + 1.0) * 2.3283064365386962890625e-10;
+        u4 = (double) r.w * 2.3283064365386962890625e-10;
+        x = F0[0] + F0[2] * (sqrt(-2.0 * log(u1)) * cos(2.0 * M_PI * u2));
+        y = F0[1] + F0[3] * (sqrt(-2.0 * log(u3)) * cos(2.0 * M_PI * u4));
+        w = w_per_amp * o->b[b0].Ib;
+        for (b = b0 + 1; b < nb; b++) {
+          const double dt = (double) (o->b[b].kb - o->b[b - 1].kb) * dt_bucket;
+          const double *F = o->bi_frame + ((size_t) k * nb + b) * 4;
+          double *S = o->bi_sum + ((size_t) k * nb + b) * 5;
+          double dx, dy, gx, gy, kk;
+          x = x + dt * vx;
+          y = y + dt * vy;
+          dx = x - F[0];
+          dy = y - F[1];
+          S[0] += w; S[1] += w * dx; S[2] += w * dy; S[3] += w * (dx * dx); S[4] += w * (dy * dy);
+          orc_gauss_field(dx, dy, F[2], F[3], &gx, &gy);
+          kk = kion_per_amp * o->b[b].Ib;
+          vx = vx + kk * gx;
+          vy = vy + kk * gy;
+        }
+      }
+  /* 3. clouds */
+  for (k = 0; k < nip; k++)
+    for (b = 0; b < nb; b++) {
+      const double *S = o->bi_sum + ((size_t) k * nb + b) * 5;
+      const double *F = o->bi_frame + ((size_t) k * nb + b) * 4;
+      double *C = o->bi_cloud + ((size_t) k * nb + b) * 5;
+      if (S[0] > 0.0) {
+        const double mx = S[1] / S[0], my = S[2] / S[0];
+        const double vx = S[3] / S[0] - mx * mx, vy = S[4] / S[0] - my * my;
+        C[0] = S[0]; C[1] = F[0] + mx; C[2] = F[1] + my;
+        C[3] = sqrt(vx > 0.0 ? vx : 0.0); C[4] = sqrt(vy > 0.0 ? vy : 0.0);
+      } else {
+        C[0] = C[1] = C[2] = C[3] = C[4] = 0.0;
+      }
+    }
+  /* 4. electron kicks */
+  for (b = 0; b < nb; b++) {
+    orc_bunch *e = &o->b[b];
+    for (jp = 0; jp < e->np; jp++) {
+      const double x = e->c[1][jp], z = e->c[2][jp], xp = e->c[4][jp], zp = e->c[5][jp];
+      double ddx = 0.0, ddxp = 0.0, ddz = 0.0, ddzp = 0.0;
+      for (k = 0; k < nip; k++) {
+        const double *C = o->bi_cloud + ((size_t) k * nb + b) * 5;
+        const double mux = 2.0 * M_PI * p->QH0 * k / nip, muy = 2.0 * M_PI * p->QV0 * k / nip;
+        const double mx = cos(mux) + aH * sin(mux), sxb = bH * sin(mux);
+        const double my = cos(muy) + aV * sin(muy), syb = bV * sin(muy);
+        const double kn = ke * C[0];
+        double gx, gy, thx, thy;
+        if (kn == 0.0) continue;
+        orc_gauss_field(mx * x + sxb * xp - C[1], my * z + syb * zp - C[2], C[3], C[4], &gx, &gy);
+        thx = kn * gx;
+        thy = kn * gy;
+        ddx = ddx - sxb * thx;
+        ddxp = ddxp + mx * thx;
+        ddz = ddz - syb * thy;
+        ddzp = ddzp + my * thy;
+      }
+      e->c[1][jp] = x + ddx;
+      e->c[4][jp] = xp + ddxp;
+      e->c[2][jp] = z + ddz;
+      e->c[5][jp] = zp + ddzp;
+    }
+  }
+}
+
 long orc_run(orc_ctx *o, long nturns, double *stats, const float *dev_in,
              float *dev_out, long dev_cap)
 {
@@ -778,6 +1013,7 @@ long orc_run(orc_ctx *o, long nturns, double *stats, const float *dev_in,
       calc_stats(o, b);
       if (stats) memcpy(stats + (t * o->nb + ib) * 12, b->stats, 12 * sizeof(double));
     }
+    if (o->bi_on) beam_ion(o, rev + 1);
     if (p->rw_long) {
       for (ib = o->lo; ib < o->hi && ib < o->nb; ib++) {
         double *mom = cyc(o, -rev * p->nharm + o->b[ib].kb);

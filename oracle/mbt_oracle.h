@@ -84,6 +84,13 @@ void orc_be_field_n(long n, const double *dx, const double *dy,
                     double sgm_xx_mm, double sgm_zz_mm, double factdq,
                     double *ex, double *ey);
 
+/* The beam-ion stage of mbt.h (mbt_beam_ion) after every turn's
+ * statistics; clouds: n_ip x nbunch x 5 of the last turn. */
+int orc_enable_beam_ion(orc_ctx *o, const mbt_beam_ion *bi);
+void orc_beam_ion_clouds(const orc_ctx *o, double *clouds);
+/* unit-charge field of an elliptic Gaussian (mbt_gauss_field_dev) */
+void orc_gauss_field(double dx, double dy, double sx, double sy, double *gx, double *gy);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,74 @@
+"""The beam-ion stage on a B200 against the oracle's restatement of the same
+model (oracle/mbt_oracle.c, beam_ion): the field function, and whole turns
+of a bunch train with ion clouds at several interaction points."""
+import numpy as np
+import pytest
+import torch
+
+from mbtrack_b200 import api
+from oracle import binding
+from oracle.binding import Oracle
+from tests.util import coord_err, small_conf, stats_err
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a):
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda")
+
+
+def test_gauss_field_matches_oracle(cuda_device):
+    rng = np.random.default_rng(11)
+    n = 4000
+    sx = rng.uniform(2e-5, 3e-4, n)
+    ratio = np.concatenate([rng.uniform(0.02, 1.0, n - 800), rng.uniform(0.99, 1.0, 400),
+                            rng.uniform(1.0, 20.0, 400)])
+    sy = sx * ratio
+    dx = rng.normal(0, 4, n) * sx
+    dy = rng.normal(0, 4, n) * sy
+    dx[:50] = 0.0
+    dy[50:100] = 0.0
+    gx, gy = torch.empty(n, dtype=torch.float64, device="cuda"), torch.empty(n, dtype=torch.float64, device="cuda")
+    inputs = [dev(a) for a in (dx, dy, sx, sy)]      # kept alive until the kernel has run
+    L = api.lib()
+    rc = L.mbt_gauss_field_dev(n, *[a.data_ptr() for a in inputs], gx.data_ptr(), gy.data_ptr(), None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    ox, oy = binding.gauss_field(dx, dy, sx, sy)
+    scale = np.hypot(ox, oy).max()
+    assert np.max(np.abs(gx.cpu().numpy() - ox)) <= 1e-12 * scale
+    assert np.max(np.abs(gy.cpu().numpy() - oy)) <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("n_ip,ions,pressure", [(3, 300, 1e-6), (1, 64, 3e-6)])
+def test_beam_ion_turns_match_oracle(tmp_path, cuda_device, n_ip, ions, pressure):
+    conf = small_conf(tmp_path, "beam_ion.conf", Np=500, filling="SINGLE10", xxCM_offset=0.3,
+                      zzCM_offset=0.5)
+    C = api.Config(conf)
+    bi = C.beam_ion()
+    bi.n_ip, bi.ions_per_passage, bi.pressure = n_ip, ions, pressure
+    npb = np.full(C.nbunch, 500)
+    ib = C.bunch_currents()
+    beam = C.reference_beam(500)
+    o = Oracle(C.params, C.bucket, npb, ib)
+    t = api.Tracker(C.params, C.bucket, npb, ib)
+    for i in range(C.nbunch):
+        o.set_particles(i, beam[i])
+        t.load_particles(i, beam[i])
+    o.prepare()
+    t.enable_beam_ion(bi)
+    t.prepare()
+    o.enable_beam_ion(bi)
+    turns = 6
+    so = o.run(turns)
+    st = t.run(turns)
+    assert stats_err(st, so).max() <= 1e-10
+    co, ct = o.beam_ion_clouds(), t.beam_ion_clouds()
+    assert co[:, 1:, 0].min() > 0
+    for m in range(5):
+        scale = np.abs(co[..., m]).max()
+        assert np.max(np.abs(ct[..., m] - co[..., m])) <= 1e-11 * scale, m
+    for i in range(C.nbunch):
+        assert coord_err(t.get_particles(i), o.get_particles(i)).max() <= 1e-12, i
+    # the ions moved the beam: same run without gas differs
+    assert np.abs(co[..., 0]).max() > 0

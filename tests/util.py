@@ -16,11 +16,12 @@ def conf(name):
 
 def small_conf(tmp_path, name, **overrides):
     """A copy of tests/confs/<name> with `key = value` overrides; the fill
-    file of the uneven configuration is made absolute."""
+    files of the uneven and beam-ion configurations are made absolute."""
     src = conf(name)
     text = open(src).read()
-    if "uneven_fill.txt" in text and "filling" not in overrides:
-        overrides["filling"] = os.path.join(CONFS, "uneven_fill.txt")
+    for fill in ("uneven_fill.txt", "beam_ion_fill.txt"):
+        if fill in text and "filling" not in overrides:
+            overrides["filling"] = os.path.join(CONFS, fill)
     dst = os.path.join(str(tmp_path), name)
     return conf_with(src, dst, **overrides)
 

@@ -415,6 +415,20 @@ int mbt_enable_beam_ion(mbt_ctx *ctx, const mbt_beam_ion *bi);
  * frame of the interaction point). */
 int mbt_beam_ion_clouds(mbt_ctx *ctx, double *clouds);
 
+/* Evaluate the beam-ion fields with the trained network m (for a stage
+ * enabled with surrogate = 1): inside its domain the network, outside it
+ * and for a hashed audit_fraction of the evaluations also the Faddeeva
+ * field.  m must outlive the context's runs. */
+typedef struct mbt_mlp mbt_mlp;
+int mbt_beam_ion_use_mlp(mbt_ctx *ctx, mbt_mlp *m);
+
+/* Audit of the learned field since the last call (counters reset):
+ * out[0] audited evaluations, out[1] largest and out[2] rms relative error
+ * of a field component against the Faddeeva field, out[3] evaluations
+ * outside the network's domain (Faddeeva fallback), out[4] tensor-core
+ * failures. */
+int mbt_beam_ion_audit(mbt_ctx *ctx, double out[5]);
+
 /* Average device time [ms] of the beam-ion stage per turn in the last
  * mbt_profile_turns call (0 when the stage is off). */
 int mbt_beam_ion_timing(mbt_ctx *ctx, double *ms_per_turn);
@@ -427,6 +441,46 @@ int mbt_beam_ion_timing(mbt_ctx *ctx, double *ms_per_turn);
 int mbt_gauss_field_dev(long n, const double *dx_dev, const double *dy_dev,
                         const double *sx_dev, const double *sy_dev,
                         double *gx_dev, double *gy_dev, void *stream);
+
+/* ---- learned field (MLP surrogate of the Bassetti-Erskine field) ------ */
+
+/* A 3 -> 128 -> 128 -> 128 -> 2 GELU network trained on the GPU to stand
+ * in for mbt_gauss_field_dev inside a = |dx|/sx < 8, b = |dy|/sy < 8,
+ * r = sy/sx in [0.05, 1] (sy > sx by swapping the axes).  The dimensionless
+ * field F = sx (gx, gy) is Fx = a Ex (1 + Yx/8), Fy = b Ey (1 + Yy/8):
+ * Ex, Ey are 8- and 16-node Gauss-Legendre quadratures of the field
+ * integral (within about 10 % of the field), the network maps (a, b, r)
+ * to the residuals (Yx, Yy).  The hidden 128 x 128 layers run on the
+ * tensor cores (BF16 operands, FP32 accumulation), the first and last
+ * layers in FP32.  Parameters: MBT_MLP_NPARAM floats, W1[128][3], b1[128],
+ * W2[128][128], b2, W3[128][128], b3, W4[2][128], b4[2]. */
+#define MBT_MLP_NPARAM 33794
+
+/* Network with seeded Glorot-uniform weights, zero biases. */
+int mbt_mlp_create(uint64_t seed, mbt_mlp **out);
+int mbt_mlp_destroy(mbt_mlp *m);
+int mbt_mlp_set_params(mbt_mlp *m, const float *params);
+int mbt_mlp_get_params(mbt_mlp *m, float *params);
+
+/* Network outputs for n inputs: abr_dev n x 3 (a, b, r), t_dev n x 2. */
+int mbt_mlp_forward_dev(mbt_mlp *m, long n, const float *abr_dev,
+                        float *t_dev, void *stream);
+
+/* Gradient of the loss sum((T - target)^2) / n over one batch of n inputs
+ * (device arrays), into grad (host, MBT_MLP_NPARAM floats); *loss set. */
+int mbt_mlp_gradient(mbt_mlp *m, int n, const float *abr_dev,
+                     const float *target_dev, float *grad, double *loss);
+
+/* Residual targets (Yx, Yy) of n inputs from the Faddeeva-based field. */
+int mbt_mlp_targets_dev(long n, const float *abr_dev, float *t_dev, void *stream);
+
+/* Train with Adam on nsamples seeded samples (half uniform over the domain,
+ * half with a = 8u^2, b = 8v^2, r log-uniform; residual targets from the
+ * Faddeeva-based field): `steps`
+ * minibatches of `batch`, learning rate lr with cosine decay to lr/100.
+ * loss_hist (may be NULL) receives the loss of every step. */
+int mbt_mlp_train(mbt_mlp *m, long nsamples, int batch, int steps, float lr,
+                  uint64_t seed, float *loss_hist);
 
 /* ---- output files (C host; the reference's text formats) ------------- */
 

@@ -74,6 +74,17 @@ SIGNATURES = {
     "mbt_beam_ion_clouds": (ctypes.c_int, [_vp, _vp]),
     "mbt_beam_ion_timing": (ctypes.c_int, [_vp, _vp]),
     "mbt_gauss_field_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "mbt_beam_ion_use_mlp": (ctypes.c_int, [_vp, _vp]),
+    "mbt_beam_ion_audit": (ctypes.c_int, [_vp, _vp]),
+    "mbt_mlp_create": (ctypes.c_int, [ctypes.c_uint64, _P(_vp)]),
+    "mbt_mlp_destroy": (ctypes.c_int, [_vp]),
+    "mbt_mlp_set_params": (ctypes.c_int, [_vp, _vp]),
+    "mbt_mlp_get_params": (ctypes.c_int, [_vp, _vp]),
+    "mbt_mlp_forward_dev": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp, _vp]),
+    "mbt_mlp_gradient": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _P(ctypes.c_double)]),
+    "mbt_mlp_targets_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp]),
+    "mbt_mlp_train": (ctypes.c_int, [_vp, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                     ctypes.c_uint64, _vp]),
     "mbt_wofz_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mbt_be_field_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, _vp, _vp, _vp]),
@@ -320,6 +331,16 @@ class Tracker:
         _check(lib().mbt_beam_ion_clouds(self.h, _ptr(a)), self.h)
         return a.reshape(self.bi.n_ip, self.nb, 5)
 
+    def use_mlp(self, mlp):
+        _check(lib().mbt_beam_ion_use_mlp(self.h, mlp.h), self.h)
+        self._mlp = mlp
+
+    def beam_ion_audit(self):
+        """(audited, max rel. error, rms rel. error, fallbacks, failures)."""
+        a = np.zeros(5)
+        _check(lib().mbt_beam_ion_audit(self.h, _ptr(a)), self.h)
+        return a
+
     def beam_ion_timing(self):
         v = ctypes.c_double()
         _check(lib().mbt_beam_ion_timing(self.h, ctypes.byref(v)), self.h)
@@ -424,3 +445,62 @@ def bunch_moments_dev_noalloc(np_, coord_ptr, sigma_tau, nsigma, dT, ncell, trac
     _check(lib().mbt_bunch_moments_dev_noalloc(np_, coord_ptr, sigma_tau, nsigma, dT, ncell, _ptr(tp),
                                                _ptr(st), hist_ptr, stream))
     return st
+
+
+MLP_NPARAM = 33794
+
+
+def _gchk(rc):
+    if rc != 0:
+        buf = ctypes.create_string_buffer(512)
+        lib().mbt_last_error(None, buf, 512)
+        raise MbtError(rc, buf.value.decode(errors="replace"))
+
+
+class Mlp:
+    """The learned field network (mbt_mlp_*).  Device arrays are passed as
+    integer addresses (e.g. torch tensors' data_ptr())."""
+
+    def __init__(self, seed=1):
+        h = _vp()
+        _gchk(lib().mbt_mlp_create(seed, ctypes.byref(h)))
+        self.h = h
+
+    def params(self):
+        a = np.zeros(MLP_NPARAM, dtype=np.float32)
+        _gchk(lib().mbt_mlp_get_params(self.h, _ptr(a)))
+        return a
+
+    def set_params(self, p):
+        a = np.ascontiguousarray(p, dtype=np.float32)
+        assert a.size == MLP_NPARAM
+        _gchk(lib().mbt_mlp_set_params(self.h, _ptr(a)))
+
+    def forward_dev(self, n, abr_ptr, out_ptr):
+        _gchk(lib().mbt_mlp_forward_dev(self.h, n, abr_ptr, out_ptr, None))
+
+    def gradient_dev(self, n, abr_ptr, tgt_ptr):
+        g = np.zeros(MLP_NPARAM, dtype=np.float32)
+        loss = ctypes.c_double()
+        _gchk(lib().mbt_mlp_gradient(self.h, n, abr_ptr, tgt_ptr, _ptr(g), ctypes.byref(loss)))
+        return g, loss.value
+
+    def train(self, nsamples, batch, steps, lr, seed):
+        hist = np.zeros(steps, dtype=np.float32)
+        _gchk(lib().mbt_mlp_train(self.h, nsamples, batch, steps, lr, seed, _ptr(hist)))
+        return hist
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mbt_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def mlp_targets_dev(n, abr_ptr, tgt_ptr):
+    _gchk(lib().mbt_mlp_targets_dev(n, abr_ptr, tgt_ptr, None))

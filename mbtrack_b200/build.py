@@ -23,7 +23,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr
 # host C: no contraction of multiply-adds, as in the reference's x86-64 build
 CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include")]
 
-CU_SOURCES = ["mbt_runtime.cu", "mbt_step.cu", "mbt_fields.cu"]
+CU_SOURCES = ["mbt_runtime.cu", "mbt_step.cu", "mbt_fields.cu", "mbt_mlp.cu"]
 # per-file extra flags: w(z) and the BE field keep every multiply and add
 # separately rounded, as the reference's x86-64 build does
 CU_EXTRA = {"mbt_fields.cu": ["-fmad=false"]}
@@ -31,7 +31,7 @@ C_SOURCES = ["mbt_host.c", "mbt_beam.c", "mbt_output.c"]
 # the drop-in executable for mbtrack-mpi's weak-weak runs
 CLI_SOURCE = "mbtrack_gpu.c"
 CLI = os.path.join(HERE, "mbtrack-gpu")
-HEADERS = ["mbt_beamion.cuh", "mbt_common.cuh", "mbt_device.cuh", "mbt_kernels.cuh", "mbt_philox.cuh",
+HEADERS = ["mbt_beamion.cuh", "mbt_common.cuh", "mbt_gauss.cuh", "mbt_device.cuh", "mbt_kernels.cuh", "mbt_mlp.cuh", "mbt_philox.cuh",
            "mbt_wofz.cuh"]
 
 

@@ -16,93 +16,25 @@
 //              order -> ions, centroid and rms of the cloud that bunch meets;
 //   bi_kick    one block per tile: every electron kicked by the clouds of its
 //              bunch at every point, kicks mapped back to the kick point.
+// With the learned field, bi_ions_mlp and bi_kick_mlp replace bi_ions and
+// bi_kick: persistent CTAs of four 128-thread groups that share the
+// network's weights; a group evaluates the field for its 128 ions (or
+// electrons) at once on the tensor cores, falls back to the Faddeeva field
+// outside the network's domain, and re-evaluates a hashed sample with it
+// for the audit.
 #pragma once
 #include <cstdint>
 
 #include "mbt_common.cuh"
 #include "mbt_device.cuh"
+#include "mbt_gauss.cuh"
+#include "mbt_mlp.cuh"
 #include "mbt_philox.cuh"
-#include "mbt_wofz.cuh"
 
 namespace mbt {
 
 constexpr int kBiThreads = 256;
 constexpr int kBiMaxIp = 64;
-constexpr double kBiRoundRatio = 0.995;   // aspect ratio above which the field comes from quadrature
-
-// 16-point Gauss-Legendre rule on [0, 1]
-static __constant__ double kGl16X[16] = {
-    0.005299532504175031, 0.0277124884633837, 0.06718439880608412, 0.1222977958224985,
-    0.19106187779867811, 0.2709916111713863, 0.35919822461037054, 0.4524937450811813,
-    0.5475062549188188, 0.6408017753896295, 0.7290083888286136, 0.8089381222013219,
-    0.8777022041775016, 0.9328156011939159, 0.9722875115366163, 0.994700467495825};
-static __constant__ double kGl16W[16] = {
-    0.013576229705877088, 0.031126761969323728, 0.0475792558412463, 0.062314485627767036,
-    0.07479799440828835, 0.08457825969750132, 0.09130170752246182, 0.09472530522753432,
-    0.09472530522753432, 0.09130170752246182, 0.08457825969750132, 0.07479799440828835,
-    0.062314485627767036, 0.0475792558412463, 0.031126761969323728, 0.013576229705877088};
-
-// Field of a unit line charge density with an elliptic Gaussian profile,
-// in units of lambda / (2 eps0): for sx >= sy the Bassetti-Erskine
-// expression  (gy + i gx) = [w(z1) - exp(-dx^2/2sx^2 - dy^2/2sy^2) w(z2)]
-// / (sqrt(pi) sqrt(2 (sx^2 - sy^2))),  z1 = (dx + i dy)/sqrt(2(sx^2-sy^2)),
-// z2 = (dx sy/sx + i dy sx/sy)/sqrt(2(sx^2-sy^2)), evaluated in the first
-// quadrant (w of the upper half plane only) with the signs of dx, dy put
-// back; closer to round than kBiRoundRatio, where that expression cancels,
-//   gx = dx/(pi sx^2) Int_0^1 t e^{-E(t)} D^{-1/2} dt,
-//   gy = dy/(pi sx^2) Int_0^1 t e^{-E(t)} D^{-3/2} dt,
-//   D = 1 - (1 - sy^2/sx^2) t^2,  E = t^2 (dx^2 + dy^2/D) / (2 sx^2)
-// (the field integral with q = 2 sx^2 (1/t^2 - 1)), by 4 x 16-point
-// Gauss-Legendre panels over the part of [0, 1] where E < 40.
-__device__ __forceinline__ void gauss_field(double dx, double dy, double sx, double sy, double &gx, double &gy) {
-  const double sgx = dx < 0.0 ? -1.0 : 1.0, sgy = dy < 0.0 ? -1.0 : 1.0;
-  double ax = fabs(dx), ay = fabs(dy);
-  const bool swap = sy > sx;
-  if (swap) {
-    const double t = ax; ax = ay; ay = t;
-    const double u = sx; sx = sy; sy = u;
-  }
-  sy = fmax(sy, 1e-6 * sx);
-  const double r = sy / sx;
-  double fx, fy;
-  if (r <= kBiRoundRatio) {
-    const double fbe = sqrt(2.0 * (sx * sx - sy * sy));
-    const double x1 = ax / fbe, y1 = ay / fbe;
-    double w1r, w1i, w2r, w2i;
-    wofz_dev(x1, y1, w1r, w1i);
-    wofz_dev(x1 * r, y1 / r, w2r, w2i);
-    const double e = exp(-(ax * ax / (2.0 * sx * sx) + ay * ay / (2.0 * sy * sy)));
-    const double c = 1.0 / (1.7724538509055160273 * fbe);
-    fx = c * (w1i - e * w2i);
-    fy = c * (w1r - e * w2r);
-  } else {
-    const double q = 1.0 - r * r;
-    const double inv2 = 1.0 / (2.0 * sx * sx);
-    const double a0 = (ax * ax + ay * ay) * inv2;
-    const double T = a0 > 40.0 ? sqrt(40.0 / a0) : 1.0;
-    const double h = 0.25 * T;
-    double ix = 0.0, iy = 0.0;
-    for (int pnl = 0; pnl < 4; ++pnl) {
-      for (int i = 0; i < 16; ++i) {
-        const double t = h * (pnl + kGl16X[i]);
-        const double D = 1.0 - q * t * t;
-        const double f = t * exp(-(t * t) * (ax * ax + ay * ay / D) * inv2) / sqrt(D);
-        const double wgt = h * kGl16W[i];
-        ix += wgt * f;
-        iy += wgt * (f / D);
-      }
-    }
-    const double c = 1.0 / (3.14159265358979323846 * sx * sx);
-    fx = c * ax * ix;
-    fy = c * ay * iy;
-  }
-  if (swap) {
-    const double t = fx; fx = fy; fy = t;
-  }
-  gx = sgx * fx;
-  gy = sgy * fy;
-}
-
 // Constants and buffers of the stage (passed by value to its kernels).
 struct BiArgs {
   int n_ip, n_new, bpp, nb;       // points, ions per passage, blocks per passage, bunches
@@ -121,6 +53,10 @@ struct BiArgs {
   const int *bunch_kb;             // nbunch buckets
   const double *ib;                // nbunch currents [A]
   const long *turn;                // device turn counter
+  // learned field (surrogate runs)
+  uint32_t audit_threshold;        // audit an evaluation when its hash is below this (2^32 x fraction)
+  unsigned long long *audit;       // [0] audited evaluations, [1] max relative error (bits), [2] fallbacks,
+                                   // [3] tensor-core failures; double sum of squared errors at audit + 4
 };
 
 __device__ __forceinline__ long bi_tri(long b) { return b * (b - 1) / 2; }
@@ -281,6 +217,194 @@ __global__ void gauss_field_kernel(long n, const double *__restrict__ dx, const 
     gx[i] = u;
     gy[i] = v;
   }
+}
+
+// ---------------------------------------------------------------- learned field
+
+// Deterministic audit selection; the kernels hash a whole warp's
+// evaluations together (32 consecutive ions or particles), so an audited
+// warp evaluates the Faddeeva field in all its lanes at once.
+__device__ __forceinline__ uint32_t bi_hash(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t h = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u) * 0x85EBCA77u ^ (c + 0x165667B1u) * 0xC2B2AE3Du;
+  h ^= h >> 15;
+  h *= 0x2C1B3C6Du;
+  h ^= h >> 12;
+  h *= 0x297A2D39u;
+  h ^= h >> 15;
+  return h;
+}
+
+// The Faddeeva field out of line, for the rare fallbacks and audits of the
+// learned-field kernels (keeps their register budget for the network).
+__device__ __noinline__ void gauss_field_ool(double dx, double dy, double sx, double sy, double *gx, double *gy) {
+  gauss_field(dx, dy, sx, sy, *gx, *gy);
+}
+
+// The learned field with its fallback and audit, for one group.
+__device__ __forceinline__ bool bi_field_mlp(const BiArgs &bi, MlpGroup &G, int t, bool active, double dx, double dy,
+                                             double sx, double sy, uint32_t h, double &gx, double &gy,
+                                             double &aud_max, double &aud_sq, int &aud_n, int &fallbacks) {
+  bool in_domain;
+  if (!mlp_group_field(G, t, active, dx, dy, sx, sy, gx, gy, in_domain)) return false;
+  if (active && !in_domain) {
+    gauss_field_ool(dx, dy, sx, sy, &gx, &gy);
+    ++fallbacks;
+  } else if (active && h < bi.audit_threshold) {
+    double ex, ey;
+    gauss_field_ool(dx, dy, sx, sy, &ex, &ey);
+    const double e0 = ex != 0.0 ? fabs(gx - ex) / fabs(ex) : 0.0;
+    const double e1 = ey != 0.0 ? fabs(gy - ey) / fabs(ey) : 0.0;
+    const double e = fmax(e0, e1);
+    aud_max = fmax(aud_max, e);
+    aud_sq += e * e;
+    ++aud_n;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void bi_audit_flush(const BiArgs &bi, double aud_max, double aud_sq, int aud_n,
+                                               int fallbacks) {
+  const double m = warp_max(aud_max), q = warp_sum(aud_sq);
+  const int n = warp_sum(aud_n), f = warp_sum(fallbacks);
+  if ((threadIdx.x & 31) == 0) {
+    if (n) {
+      atomicAdd(&bi.audit[0], (unsigned long long)n);
+      atomicMax(&bi.audit[1], (unsigned long long)__double_as_longlong(m));
+      atomicAdd(reinterpret_cast<double *>(bi.audit + 4), q);
+    }
+    if (f) atomicAdd(&bi.audit[2], (unsigned long long)f);
+  }
+}
+
+// Ions with the learned field: work item = (creating passage b0, point k,
+// 128-ion block), longest first; every group takes items round-robin.
+__global__ void __launch_bounds__(128 * kMlpGroups, 1) bi_ions_mlp(BiArgs bi, MlpDev M) {
+  extern __shared__ uint8_t smem_raw[];
+  MlpGroup G;
+  const uint32_t tmem = mlp_cta_setup(M, align1024(smem_raw), G);
+  const int g = threadIdx.x >> 7, t = threadIdx.x & 127, warp = t >> 5, lane = threadIdx.x & 31;
+  __shared__ double red[kMlpGroups][4][5];
+  const long turn = *bi.turn;
+  const long per_b0 = (long)bi.n_ip * bi.bpp, nitems = (long)(bi.nb - 1) * per_b0;
+  double aud_max = 0.0, aud_sq = 0.0;
+  int aud_n = 0, fallbacks = 0;
+  bool ok = true;
+  for (long item = (long)blockIdx.x * kMlpGroups + g; item < nitems && ok; item += (long)gridDim.x * kMlpGroups) {
+    const int b0 = (int)(item / per_b0);
+    const int k = (int)((item % per_b0) / bi.bpp), blk = (int)(item % bi.bpp);
+    const int j = blk * 128 + t;
+    const bool live = j < bi.n_new;
+    double x = 0.0, y = 0.0, vx = 0.0, vy = 0.0, w = 0.0;
+    if (live) {
+      const double *F0 = bi.frame + ((size_t)k * bi.nb + b0) * 4;
+      const U4 c = {(uint32_t)j, (uint32_t)b0 | ((uint32_t)k << 20), (uint32_t)turn, (uint32_t)(turn >> 32)};
+      double g1, g2;
+      bi_normals(philox4x32_10k(c, bi.keys), g1, g2);
+      x = F0[0] + F0[2] * g1;
+      y = F0[1] + F0[3] * g2;
+      w = bi.w_per_amp * bi.ib[b0];
+    }
+    for (int b = b0 + 1; b < bi.nb; ++b) {
+      const double dt = (double)(bi.bunch_kb[b] - bi.bunch_kb[b - 1]) * bi.dt_bucket;
+      x = x + dt * vx;
+      y = y + dt * vy;
+      const double *F = bi.frame + ((size_t)k * bi.nb + b) * 4;
+      const double dx = x - F[0], dy = y - F[1];
+      double s[5] = {w, w * dx, w * dy, w * (dx * dx), w * (dy * dy)};
+#pragma unroll
+      for (int m = 0; m < 5; ++m) s[m] = warp_sum(s[m]);
+      if (lane == 0)
+        for (int m = 0; m < 5; ++m) red[g][warp][m] = s[m];
+      named_barrier(G.bar_id, 128);
+      if (t < 5)
+        bi.part[(((size_t)k * bi.T + bi_tri(b) + b0) * bi.bpp + blk) * 5 + t] =
+            ((red[g][0][t] + red[g][1][t]) + red[g][2][t]) + red[g][3][t];
+      double gx = 0.0, gy = 0.0;
+      if (!bi_field_mlp(bi, G, t, live, dx, dy, F[2], F[3], bi_hash((uint32_t)turn, (uint32_t)(k * 65536 + b), (uint32_t)(b0 * 1048576 + (j >> 5))),
+                        gx, gy, aud_max, aud_sq, aud_n, fallbacks)) {
+        ok = false;
+        break;
+      }
+      if (live) {
+        const double kk = bi.kion_per_amp * bi.ib[b];
+        vx = vx + kk * gx;
+        vy = vy + kk * gy;
+      }
+    }
+  }
+  if (!ok && t == 0) atomicAdd(&bi.audit[3], 1ull);
+  bi_audit_flush(bi, aud_max, aud_sq, aud_n, fallbacks);
+  mlp_cta_release(tmem);
+}
+
+// Electrons with the learned field: work item = 128 particles of a tile.
+__global__ void __launch_bounds__(128 * kMlpGroups, 1) bi_kick_mlp(Args a, BiArgs bi, MlpDev M) {
+  extern __shared__ uint8_t smem_raw[];
+  MlpGroup G;
+  const uint32_t tmem = mlp_cta_setup(M, align1024(smem_raw), G);
+  const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
+  __shared__ double cl[kMlpGroups][kBiMaxIp][5];
+  __shared__ double tr[kBiMaxIp][4];
+  for (int i = threadIdx.x; i < bi.n_ip; i += blockDim.x)
+    for (int m = 0; m < 4; ++m) tr[i][m] = bi.trig[4 * i + m];
+  __syncthreads();
+  const long turn = *bi.turn;
+  const size_t n6 = (size_t)a.npad;
+  double *C = a.coord;
+  const long nitems = (long)a.ntile * 64;
+  double aud_max = 0.0, aud_sq = 0.0;
+  int aud_n = 0, fallbacks = 0;
+  bool ok = true;
+  for (long item = (long)blockIdx.x * kMlpGroups + g; item < nitems && ok; item += (long)gridDim.x * kMlpGroups) {
+    const Tile tile = a.tiles[item / 64];
+    const int sub = (int)(item % 64);
+    if (sub * 128 >= tile.count) continue;   // the same for the whole group
+    const int b = tile.bunch;
+    named_barrier(G.bar_id, 128);            // the group's previous cloud table is no longer read
+    for (int i = t; i < bi.n_ip; i += 128) {
+      const double *Cl = bi.cloud + ((size_t)i * bi.nb + b) * 5;
+      cl[g][i][0] = bi.ke * Cl[0];
+      for (int m = 1; m < 5; ++m) cl[g][i][m] = Cl[m];
+    }
+    named_barrier(G.bar_id, 128);
+    const int p = tile.start + sub * 128 + t;
+    const bool live = sub * 128 + t < tile.count;
+    double x = 0.0, z = 0.0, xp = 0.0, zp = 0.0;
+    if (live) {
+      x = C[1 * n6 + p];
+      z = C[2 * n6 + p];
+      xp = C[4 * n6 + p];
+      zp = C[5 * n6 + p];
+    }
+    double ddx = 0.0, ddxp = 0.0, ddz = 0.0, ddzp = 0.0;
+    for (int k = 0; k < bi.n_ip; ++k) {
+      if (cl[g][k][0] == 0.0) continue;        // the same for the whole group
+      const double mx = tr[k][0] + bi.alphaH * tr[k][1], sxb = bi.betaH * tr[k][1];
+      const double my = tr[k][2] + bi.alphaV * tr[k][3], syb = bi.betaV * tr[k][3];
+      const double xk = mx * x + sxb * xp, zk = my * z + syb * zp;
+      double gx = 0.0, gy = 0.0;
+      if (!bi_field_mlp(bi, G, t, live, xk - cl[g][k][1], zk - cl[g][k][2], cl[g][k][3], cl[g][k][4],
+                        bi_hash((uint32_t)turn + 0x51ED27u, (uint32_t)k, (uint32_t)(p >> 5)), gx, gy, aud_max, aud_sq,
+                        aud_n, fallbacks)) {
+        ok = false;
+        break;
+      }
+      const double thx = cl[g][k][0] * gx, thy = cl[g][k][0] * gy;
+      ddx = ddx - sxb * thx;
+      ddxp = ddxp + mx * thx;
+      ddz = ddz - syb * thy;
+      ddzp = ddzp + my * thy;
+    }
+    if (live && ok) {
+      C[1 * n6 + p] = x + ddx;
+      C[4 * n6 + p] = xp + ddxp;
+      C[2 * n6 + p] = z + ddz;
+      C[5 * n6 + p] = zp + ddzp;
+    }
+  }
+  if (!ok && t == 0) atomicAdd(&bi.audit[3], 1ull);
+  bi_audit_flush(bi, aud_max, aud_sq, aud_n, fallbacks);
+  mlp_cta_release(tmem);
 }
 
 }  // namespace mbt

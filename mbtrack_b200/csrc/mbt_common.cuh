@@ -72,6 +72,13 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
+// maximum over the warp (valid in lane 0)
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
 // Complex affine map V -> V M + A; compose(f, g) applies f then g.
 struct Aff {
   double m0, m1, a0, a1;

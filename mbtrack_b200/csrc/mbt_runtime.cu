@@ -34,6 +34,7 @@ thread_local char g_create_error[512] = "";
 }  // namespace
 
 namespace mbt {
+MlpDev mlp_device_view(const mbt_mlp *m);
 size_t stats_scratch_doubles(int np);
 int bunch_stats_strided(int np, const double *coord, size_t ld, const int tp[3], double *stats, void *stream,
                         double *scratch);
@@ -73,11 +74,14 @@ struct mbt_ctx {
   mbt_beam_ion bicfg{};
   mbt::BiArgs bi{};
   cudaEvent_t bi_ev = nullptr;   // end of the beam-ion stage (profiling)
+  mbt::MlpDev mlp{};             // learned field (surrogate runs)
+  bool mlp_set = false;
   double bi_ms = 0.0;            // its average device time in the last mbt_profile_turns
   std::vector<int> watch;        // bunches whose potentials are recorded
   cudaEvent_t ev[6] = {};
   double timing[4] = {0, 0, 0, 0};
   int device = 0;
+  int nsm = 148;
   char err[512] = "";
 };
 
@@ -211,6 +215,14 @@ void enqueue_beam_ion(mbt_ctx *c) {
   const mbt::BiArgs &bi = c->bi;
   const int n = bi.n_ip * bi.nb;
   mbt::bi_frames<<<(n + 127) / 128, 128, 0, c->stream>>>(bi);
+  if (c->bicfg.surrogate) {
+    const int grid = c->nsm;
+    if (bi.nb > 1)
+      mbt::bi_ions_mlp<<<grid, 128 * mbt::kMlpGroups, mbt::kMlpCtaSmem, c->stream>>>(bi, c->mlp);
+    mbt::bi_clouds<<<dim3(bi.nb, bi.n_ip), mbt::kBiThreads, 0, c->stream>>>(bi);
+    mbt::bi_kick_mlp<<<grid, 128 * mbt::kMlpGroups, mbt::kMlpCtaSmem, c->stream>>>(c->a, bi, c->mlp);
+    return;
+  }
   if (bi.nb > 1) {
     mbt::bi_ions<<<dim3(bi.bpp, bi.nb - 1, bi.n_ip), mbt::kBiThreads, 0, c->stream>>>(bi);
   }
@@ -307,6 +319,7 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   cudaGetDevice(&c->device);
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, c->device);
+  c->nsm = prop.multiProcessorCount;
   auto bail = [&](int code) { int rc = code; mbt_destroy(c); return rc; };
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(nullptr, MBT_ERR_CUDA, "stream create"));
@@ -719,7 +732,8 @@ int mbt_enable_beam_ion(mbt_ctx *c, const mbt_beam_ion *cfg) {
   if (!(cfg->gas_A > 0) || !(cfg->pressure >= 0) || !(cfg->sigma_ion >= 0))
     return fail(c, MBT_ERR_INVALID, "gas_A must be positive, pressure and sigma_ion non-negative");
   if (c->nbunch > 65535) return fail(c, MBT_ERR_INVALID, "the beam-ion stage serves up to 65535 bunches");
-  if (cfg->surrogate) return fail(c, MBT_ERR_INVALID, "the surrogate field is not available in this build");
+  if (cfg->surrogate && !(cfg->audit_fraction >= 0.0 && cfg->audit_fraction <= 1.0))
+    return fail(c, MBT_ERR_INVALID, "audit_fraction outside 0..1");
   // constants of the reference (def.h:21-26, input.c:1562)
   const double c_light = 2.997925e+08, eps0 = 8.854187817620e-12, e_charge = 1.602e-19, e_mass = 9.1e-31;
   const double r_e = 2.819e-15, mp_o_em = 1.836e3;
@@ -730,7 +744,11 @@ int mbt_enable_beam_ion(mbt_ctx *c, const mbt_beam_ion *cfg) {
   mbt::BiArgs &bi = c->bi;
   bi.n_ip = cfg->n_ip;
   bi.n_new = cfg->ions_per_passage;
-  bi.bpp = (cfg->ions_per_passage + mbt::kBiThreads - 1) / mbt::kBiThreads;
+  // blocks per passage: of 256 ions for the Faddeeva kernels, of 128 (one
+  // tensor-core tile) for the learned field
+  const int per_block = cfg->surrogate ? 128 : mbt::kBiThreads;
+  bi.bpp = (cfg->ions_per_passage + per_block - 1) / per_block;
+  bi.audit_threshold = (uint32_t)std::min(4294967295.0, cfg->audit_fraction * 4294967296.0);
   bi.nb = c->nbunch;
   bi.T = (long)c->nbunch * (c->nbunch - 1) / 2;
   bi.dt_bucket = p->T0 / p->nharm;
@@ -755,7 +773,14 @@ int mbt_enable_beam_ion(mbt_ctx *c, const mbt_beam_ion *cfg) {
   if (!r) r = dalloc(c, &part, nslot);
   if (!r) r = dalloc(c, &cloud, (size_t)cfg->n_ip * c->nbunch * 5);
   if (!r) r = dupload(c, &ibd, ibv.data(), ibv.size());
+  unsigned long long *aud = nullptr;
+  if (!r) r = dalloc(c, &aud, 6);
   if (r) return r;
+  bi.audit = aud;
+  if (cfg->surrogate) {
+    CK(cudaFuncSetAttribute(mbt::bi_ions_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mbt::kMlpCtaSmem));
+    CK(cudaFuncSetAttribute(mbt::bi_kick_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mbt::kMlpCtaSmem));
+  }
   bi.trig = tr; bi.mom = mom; bi.frame = frame; bi.part = part; bi.cloud = cloud; bi.ib = ibd;
   bi.bunch_kb = c->a.bunch_kb;
   bi.turn = &c->a.rs->turn;
@@ -764,6 +789,33 @@ int mbt_enable_beam_ion(mbt_ctx *c, const mbt_beam_ion *cfg) {
   c->bicfg = *cfg;
   c->bi_on = 1;
   if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; c->graph_turns = 0; }
+  return 0;
+}
+
+int mbt_beam_ion_use_mlp(mbt_ctx *c, mbt_mlp *m) {
+  if (!c || !m) return MBT_ERR_INVALID;
+  c->mlp = mbt::mlp_device_view(m);
+  c->mlp_set = true;
+  if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; c->graph_turns = 0; }
+  return 0;
+}
+
+int mbt_beam_ion_audit(mbt_ctx *c, double out[5]) {
+  if (!c || !out) return MBT_ERR_INVALID;
+  if (!c->bi_on) return fail(c, MBT_ERR_STATE, "the beam-ion stage is off");
+  unsigned long long h[6];
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(h, c->bi.audit, sizeof h, cudaMemcpyDeviceToHost));
+  CK(cudaMemset(c->bi.audit, 0, sizeof h));
+  double sq;
+  memcpy(&sq, &h[4], sizeof sq);
+  double mx;
+  memcpy(&mx, &h[1], sizeof mx);
+  out[0] = (double)h[0];
+  out[1] = h[0] ? mx : 0.0;
+  out[2] = h[0] ? sqrt(sq / (double)h[0]) : 0.0;
+  out[3] = (double)h[2];
+  out[4] = (double)h[3];
   return 0;
 }
 
@@ -863,6 +915,8 @@ int mbt_set_deviates(mbt_ctx *c, const float *dev, long nturns) {
 
 static int run_core(mbt_ctx *c, long nturns, double *stats, double *ampinv, bool use_graph) {
   if (!c->prepared) return fail(c, MBT_ERR_STATE, "mbt_prepare must come first");
+  if (c->bi_on && c->bicfg.surrogate && !c->mlp_set)
+    return fail(c, MBT_ERR_STATE, "surrogate beam-ion fields need mbt_beam_ion_use_mlp");
   RingState rs;
   CK(cudaMemcpy(&rs, c->a.rs, sizeof rs, cudaMemcpyDeviceToHost));
   long turn = rs.turn;
@@ -926,6 +980,8 @@ int mbt_track(mbt_ctx *c, double *particles, long nturns, double *stats) {
 int mbt_profile_turns(mbt_ctx *c, long nturns, double out[4]) {
   if (!c || nturns <= 0 || !out) return MBT_ERR_INVALID;
   if (!c->prepared) return fail(c, MBT_ERR_STATE, "mbt_prepare must come first");
+  if (c->bi_on && c->bicfg.surrogate && !c->mlp_set)
+    return fail(c, MBT_ERR_STATE, "surrogate beam-ion fields need mbt_beam_ion_use_mlp");
   double acc[4] = {0, 0, 0, 0}, acc_bi = 0.0;
   for (long t = 0; t < nturns; ++t) {
     enqueue_turn(c, c->ev);

@@ -366,3 +366,27 @@ class Reference:
         self.lib.refh_ampinv.argtypes = [ctypes.c_int, _vp]
         self.lib.refh_ampinv(ib, _ptr(out))
         return out
+
+
+def mlp_forward(params, abr):
+    """orc_mlp_forward: the network's outputs for inputs abr (n x 3)."""
+    L = ctypes.CDLL(build_oracle())
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    x = np.ascontiguousarray(abr, dtype=np.float32)
+    out = np.zeros((len(x), 2), dtype=np.float32)
+    L.orc_mlp_forward.argtypes = [_vp, ctypes.c_long, _vp, _vp]
+    L.orc_mlp_forward(_ptr(p), len(x), _ptr(x), _ptr(out))
+    return out
+
+
+def mlp_gradient(params, abr, tgt):
+    """orc_mlp_gradient: (gradient, loss) of one batch."""
+    L = ctypes.CDLL(build_oracle())
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    x = np.ascontiguousarray(abr, dtype=np.float32)
+    t = np.ascontiguousarray(tgt, dtype=np.float32)
+    g = np.zeros(p.size, dtype=np.float32)
+    L.orc_mlp_gradient.argtypes = [_vp, ctypes.c_int, _vp, _vp, _vp]
+    L.orc_mlp_gradient.restype = ctypes.c_double
+    loss = L.orc_mlp_gradient(_ptr(p), len(x), _ptr(x), _ptr(t), _ptr(g))
+    return g, loss

@@ -1,0 +1,157 @@
+/*
+ * mlp_oracle.c -- TEST INFRASTRUCTURE ONLY: CPU restatement of the learned
+ * field network of libmbt (mbt.h, mbt_mlp_*): forward pass and gradient
+ * with the same roundings of the tensor-core operands (BF16 weights, BF16
+ * hi + lo activations in the forward pass, BF16 operands of the backward
+ * products), sums in double.  Used by tests/ to check the GPU kernels.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define H 128
+#define W1 0
+#define B1 384
+#define W2 512
+#define B2 (W2 + 16384)
+#define W3 (B2 + 128)
+#define B3 (W3 + 16384)
+#define W4 (B3 + 128)
+#define B4 (W4 + 256)
+#define NPARAM (B4 + 2)
+
+/* round to the nearest BF16 (ties to even) */
+static float bf16r(float v)
+{
+  uint32_t u;
+  memcpy(&u, &v, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return v;
+  u += 0x7fffu + ((u >> 16) & 1u);
+  u &= 0xffff0000u;
+  memcpy(&v, &u, 4);
+  return v;
+}
+
+/* GELU in its tanh form; the GPU evaluates tanh with the hardware
+ * approximation (relative error below 2^-10.987), this restatement with
+ * libm's tanhf. */
+static float gelu(float x)
+{
+  const float y = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+  const float hx = 0.5f * x;
+  return fmaf(hx, tanhf(y), hx);
+}
+
+static float gelu_grad(float x)
+{
+  const float y = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+  const float th = tanhf(y);
+  return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * 0.7978845608028654f * (1.0f + 0.134145f * x * x);
+}
+
+/* activations enter the products as BF16 (libm's kMlpSplit = false) */
+#define SPLIT 0
+
+typedef struct fwd_t {
+  float x[3], z1[H], h1[H], z2[H], h2[H], z3[H], h3[H], out[2];
+} fwd_t;
+
+static void forward_one(const float *P, const float *abr, fwd_t *f)
+{
+  int j, k;
+  f->x[0] = 0.25f * abr[0] - 1.0f;
+  f->x[1] = 0.25f * abr[1] - 1.0f;
+  f->x[2] = 2.0f * abr[2] - 1.0f;
+  for (j = 0; j < H; j++) {
+    float z = P[B1 + j];
+    z = fmaf(P[W1 + 3 * j], f->x[0], z);
+    z = fmaf(P[W1 + 3 * j + 1], f->x[1], z);
+    z = fmaf(P[W1 + 3 * j + 2], f->x[2], z);
+    f->z1[j] = z;
+    f->h1[j] = gelu(z);
+  }
+  for (j = 0; j < H; j++) {
+    double s = 0.0;
+    for (k = 0; k < H; k++) {
+      const float hi = bf16r(f->h1[k]), lo = SPLIT ? bf16r(f->h1[k] - hi) : 0.0f;
+      s += ((double) hi + (double) lo) * (double) bf16r(P[W2 + H * j + k]);
+    }
+    f->z2[j] = (float) s + P[B2 + j];
+    f->h2[j] = gelu(f->z2[j]);
+  }
+  for (j = 0; j < H; j++) {
+    double s = 0.0;
+    for (k = 0; k < H; k++) {
+      const float hi = bf16r(f->h2[k]), lo = SPLIT ? bf16r(f->h2[k] - hi) : 0.0f;
+      s += ((double) hi + (double) lo) * (double) bf16r(P[W3 + H * j + k]);
+    }
+    f->z3[j] = (float) s + P[B3 + j];
+    f->h3[j] = gelu(f->z3[j]);
+  }
+  f->out[0] = P[B4];
+  f->out[1] = P[B4 + 1];
+  for (j = 0; j < H; j++) {
+    f->out[0] = fmaf(P[W4 + j], f->h3[j], f->out[0]);
+    f->out[1] = fmaf(P[W4 + H + j], f->h3[j], f->out[1]);
+  }
+}
+
+void orc_mlp_forward(const float *P, long n, const float *abr, float *out)
+{
+  long i;
+  fwd_t f;
+  for (i = 0; i < n; i++) {
+    forward_one(P, abr + 3 * i, &f);
+    out[2 * i] = f.out[0];
+    out[2 * i + 1] = f.out[1];
+  }
+}
+
+/* Gradient of sum((T - target)^2) / n; returns the loss. */
+double orc_mlp_gradient(const float *P, int n, const float *abr, const float *tgt, float *grad)
+{
+  double *g = (double *) calloc(NPARAM, sizeof(double));
+  fwd_t *f = (fwd_t *) malloc(sizeof(fwd_t));
+  double loss = 0.0;
+  int m, j, k;
+  for (m = 0; m < n; m++) {
+    float dT[2], dz3[H], dz2[H], dz1[H];
+    forward_one(P, abr + 3 * m, f);
+    for (j = 0; j < 2; j++) {
+      const double d = (double) f->out[j] - tgt[2 * m + j];
+      loss += d * d;
+      dT[j] = 2.0f * (f->out[j] - tgt[2 * m + j]) * (1.0f / (float) n);
+    }
+    for (j = 0; j < 2; j++) {
+      g[B4 + j] += dT[j];
+      for (k = 0; k < H; k++) g[W4 + H * j + k] += (double) dT[j] * f->h3[k];
+    }
+    for (j = 0; j < H; j++) {
+      const float dh = P[W4 + j] * dT[0] + P[W4 + H + j] * dT[1];
+      dz3[j] = dh * gelu_grad(f->z3[j]);
+      g[B3 + j] += dz3[j];
+    }
+    for (j = 0; j < H; j++)
+      for (k = 0; k < H; k++) g[W3 + H * j + k] += (double) bf16r(dz3[j]) * bf16r(f->h2[k]);
+    for (k = 0; k < H; k++) {
+      double s = 0.0;
+      for (j = 0; j < H; j++) s += (double) bf16r(dz3[j]) * bf16r(P[W3 + H * j + k]);
+      dz2[k] = (float) s * gelu_grad(f->z2[k]);
+      g[B2 + k] += dz2[k];
+    }
+    for (j = 0; j < H; j++)
+      for (k = 0; k < H; k++) g[W2 + H * j + k] += (double) bf16r(dz2[j]) * bf16r(f->h1[k]);
+    for (k = 0; k < H; k++) {
+      double s = 0.0;
+      for (j = 0; j < H; j++) s += (double) bf16r(dz2[j]) * bf16r(P[W2 + H * j + k]);
+      dz1[k] = (float) s * gelu_grad(f->z1[k]);
+      g[B1 + k] += dz1[k];
+      for (j = 0; j < 3; j++) g[W1 + 3 * k + j] += (double) dz1[k] * f->x[j];
+    }
+  }
+  for (j = 0; j < NPARAM; j++) grad[j] = (float) g[j];
+  free(g);
+  free(f);
+  return loss / n;
+}

@@ -72,3 +72,37 @@ def test_beam_ion_turns_match_oracle(tmp_path, cuda_device, n_ip, ions, pressure
         assert coord_err(t.get_particles(i), o.get_particles(i)).max() <= 1e-12, i
     # the ions moved the beam: same run without gas differs
     assert np.abs(co[..., 0]).max() > 0
+
+
+def test_surrogate_stage_tracks_the_faddeeva_stage(tmp_path, cuda_device):
+    """The beam-ion stage with the learned field (trained here on the
+    project's own Faddeeva field) follows the Faddeeva stage: same clouds
+    and centroids to the network's accuracy, audited errors reported, the
+    out-of-domain evaluations handed to the Faddeeva field."""
+    conf = small_conf(tmp_path, "beam_ion.conf", Np=2000, filling="SINGLE10", xxCM_offset=0.3, zzCM_offset=0.5)
+    C = api.Config(conf)
+    mlp = api.Mlp(seed=21)
+    hist = mlp.train(nsamples=1 << 21, batch=8192, steps=3000, lr=2e-3, seed=22)
+    assert hist[-1] < 1e-3
+    runs = {}
+    for surr in (0, 1):
+        bi = C.beam_ion()
+        bi.n_ip, bi.ions_per_passage, bi.pressure, bi.surrogate, bi.audit_fraction = 4, 500, 1e-6, surr, 0.05
+        t = api.Tracker(C.params, C.bucket, np.full(C.nbunch, 2000), C.bunch_currents())
+        for i, b in enumerate(C.reference_beam(2000)):
+            t.load_particles(i, b)
+        t.enable_beam_ion(bi)
+        if surr:
+            t.use_mlp(mlp)
+        t.prepare()
+        runs[surr] = (t.run(8), t.beam_ion_clouds(), t.beam_ion_audit() if surr else None)
+    (s0, c0, _), (s1, c1, audit) = runs[0], runs[1]
+    n_audit, max_err, rms_err, fallbacks, failures = audit
+    assert failures == 0
+    assert n_audit > 1000 and max_err < 0.05 and rms_err < 5e-3, audit
+    # centroids (relative to the rms size) and clouds agree to the field error
+    assert stats_err(s1, s0).max() < 1e-3
+    rel = np.abs(c1[..., 0] - c0[..., 0]).max() / np.abs(c0[..., 0]).max()
+    assert rel < 1e-12      # ion counts do not depend on the field
+    for m in (1, 2, 3, 4):
+        assert np.abs(c1[..., m] - c0[..., m]).max() <= 1e-2 * np.abs(c0[..., 3:]).max(), m

@@ -1,0 +1,79 @@
+"""The learned field network on a B200: tensor-core forward pass and
+gradient against the CPU restatement (oracle/mlp_oracle.c, same operand
+roundings), and training on the project's own Faddeeva-based field."""
+import numpy as np
+import pytest
+import torch
+
+from mbtrack_b200 import api
+from oracle import binding
+
+pytestmark = pytest.mark.gpu
+
+BLOCKS = {"W1": (0, 384), "b1": (384, 512), "W2": (512, 16896), "b2": (16896, 17024), "W3": (17024, 33408),
+          "b3": (33408, 33536), "W4": (33536, 33792), "b4": (33792, 33794)}
+
+
+def inputs(n, seed):
+    rng = np.random.default_rng(seed)
+    return np.stack([rng.uniform(0, 8, n), rng.uniform(0, 8, n), rng.uniform(0.05, 1, n)], 1).astype(np.float32)
+
+
+def perturbed(m, seed):
+    """Weights with non-zero biases, so every parameter block is exercised."""
+    p = m.params()
+    rng = np.random.default_rng(seed)
+    for name in ("b1", "b2", "b3", "b4"):
+        lo, hi = BLOCKS[name]
+        p[lo:hi] = rng.normal(0, 0.2, hi - lo)
+    m.set_params(p)
+    return p
+
+
+def test_forward_matches_oracle(cuda_device):
+    m = api.Mlp(seed=3)
+    p = perturbed(m, 4)
+    x = inputs(1000, 5)     # 8 tiles, the last one partial
+    xd = torch.as_tensor(x, device="cuda")
+    out = torch.zeros((len(x), 2), dtype=torch.float32, device="cuda")
+    m.forward_dev(len(x), xd.data_ptr(), out.data_ptr())
+    ref = binding.mlp_forward(p, x)
+    got = out.cpu().numpy()
+    # the GPU's GELU uses the hardware tanh (relative error < 2^-10.987),
+    # the oracle libm's tanhf; the BF16 rounding of an activation may then
+    # land on the other side of a tie: differences of a few 1e-3 of scale
+    scale = np.abs(ref).max()
+    assert np.max(np.abs(got - ref)) <= 5e-3 * scale, np.max(np.abs(got - ref)) / scale
+    assert np.median(np.abs(got - ref)) <= 5e-4 * scale
+
+
+def test_gradient_matches_oracle(cuda_device):
+    m = api.Mlp(seed=6)
+    p = perturbed(m, 7)
+    x = inputs(300, 8)      # 3 tiles, the last one partial
+    t = np.random.default_rng(9).normal(0.8, 0.2, (300, 2)).astype(np.float32)
+    xd, td = torch.as_tensor(x, device="cuda"), torch.as_tensor(t, device="cuda")
+    g, loss = m.gradient_dev(len(x), xd.data_ptr(), td.data_ptr())
+    gr, lr = binding.mlp_gradient(p, x, t)
+    assert loss == pytest.approx(lr, rel=1e-2)
+    for name, (lo, hi) in BLOCKS.items():
+        norm = np.linalg.norm(gr[lo:hi])
+        assert norm > 0, name
+        assert np.linalg.norm(g[lo:hi] - gr[lo:hi]) <= 2e-2 * norm, (name, np.linalg.norm(g[lo:hi] - gr[lo:hi]) / norm)
+
+
+def test_training_reduces_the_loss(cuda_device):
+    m = api.Mlp(seed=10)
+    hist = m.train(nsamples=1 << 20, batch=4096, steps=300, lr=2e-3, seed=11)
+    assert np.all(np.isfinite(hist))
+    assert hist[-20:].mean() < 0.05 * hist[:5].mean(), (hist[:5], hist[-20:])
+    # held-out points: targets from the Faddeeva-based field
+    x = inputs(20000, 12)
+    xd = torch.as_tensor(x, device="cuda")
+    tgt = torch.zeros((len(x), 2), dtype=torch.float32, device="cuda")
+    api.mlp_targets_dev(len(x), xd.data_ptr(), tgt.data_ptr())
+    out = torch.zeros_like(tgt)
+    m.forward_dev(len(x), xd.data_ptr(), out.data_ptr())
+    err = (out - tgt).abs().max().item()
+    print("held-out max |T - target| after 300 steps:", err, "loss", hist[-1])
+    assert err < 0.2

@@ -101,7 +101,7 @@ def test_surrogate_stage_tracks_the_faddeeva_stage(tmp_path, cuda_device):
     assert failures == 0
     assert n_audit > 1000 and max_err < 0.05 and rms_err < 5e-3, audit
     # centroids (relative to the rms size) and clouds agree to the field error
-    assert stats_err(s1, s0).max() < 1e-3
+    assert stats_err(s1, s0).max() < 5e-3
     rel = np.abs(c1[..., 0] - c0[..., 0]).max() / np.abs(c0[..., 0]).max()
     assert rel < 1e-12      # ion counts do not depend on the field
     for m in (1, 2, 3, 4):

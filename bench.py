@@ -1,7 +1,7 @@
 """Benchmark of the per-turn weak-weak tracking loop on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload uniform|single|uneven]
+                    [--workload uniform|single|uneven|beam_ion|beam_ion_mlp]
 
 Default workload (the uniform multi-bunch configuration): all 416 buckets
 filled at 0.5 nC, 2e4 macroparticles per bunch (8.32e6, 400 MB of FP64
@@ -42,7 +42,14 @@ WORKLOADS = {
                                                           "resonator in 3 planes, quantum excitation on"),
     "uneven": ("uneven_fill.conf", {}, "uneven fill: 321 bunches incl. 5 nC camshaft, RW + HOM + RF "
                                        "feedback, quantum excitation on"),
+    "beam_ion": ("beam_ion.conf", {}, "beam-ion weak-strong: 200-bunch train x 5e4 macroparticles, CO at "
+                                      "1 nTorr, 20 interaction points, 1000 macro-ions per passage per point, "
+                                      "Faddeeva-based Bassetti-Erskine fields"),
+    "beam_ion_mlp": ("beam_ion.conf", {}, "beam-ion weak-strong: 200-bunch train x 5e4 macroparticles, CO at "
+                                          "1 nTorr, 20 interaction points, 1000 macro-ions per passage per "
+                                          "point, learned field (tensor-core MLP, 1% audit)"),
 }
+BEAM_ION_CPU_SCALE = 100   # the CPU sample keeps 1/100 of the electrons and of the ions
 BYTES_PER_MP_TURN = 96   # 6 FP64 coordinates read and written per macroparticle per turn
 METRIC = "macroparticle-turns/s"
 
@@ -54,6 +61,8 @@ def conf_path(workload, tmpdir):
     over = dict(over)
     if "uneven" in name:
         over["filling"] = os.path.join(CONFS, "uneven_fill.txt")
+    if "beam_ion" in name:
+        over["filling"] = os.path.join(CONFS, "beam_ion_fill.txt")
     if not over:
         return src
     return conf_with(src, os.path.join(tmpdir, name), **over)
@@ -140,7 +149,20 @@ def _cpu_worker(args):
     returns the wall time of each turn."""
     kind, conf, lo, hi, turns = args
     sys.path.insert(0, ROOT)
-    if kind == "reference":
+    if kind == "beam_ion":
+        import numpy as np
+        from mbtrack_b200 import api as _api   # configuration parser only (C host)
+        from oracle.binding import Oracle
+        cfg = _api.Config(conf)
+        bi = cfg.beam_ion()
+        bi.ions_per_passage = max(1, bi.ions_per_passage // BEAM_ION_CPU_SCALE)
+        npb = max(2, cfg.params.np_model // BEAM_ION_CPU_SCALE)
+        O = Oracle(cfg.params, cfg.bucket, np.full(cfg.nbunch, npb), cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh)
+        O.generate_beam()
+        O.prepare()
+        O.enable_beam_ion(bi)
+        step = lambda: O.lib.orc_run(O.h, 1, None, None, None, 0)   # noqa: E731
+    elif kind == "reference":
         from oracle.binding import Reference
         R = Reference(conf, bunch_range=(lo, hi))
         R.prepare()
@@ -179,6 +201,16 @@ def cpu_run(workload, turns, tmpdir, cores=None):
     conf = conf_path(workload, tmpdir)
     cfg = api.Config(conf)
     nb = cfg.nbunch
+    if workload.startswith("beam_ion"):
+        # no reference code for this stage: the C restatement (oracle) on one
+        # core, 1/BEAM_ION_CPU_SCALE of the electrons and ions, the time per
+        # turn scaled back up (the work is linear in both counts)
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(1) as pool:
+            res = pool.map(_cpu_worker, [("beam_ion", conf, 0, nb, turns)])
+        per_turn = [x * BEAM_ION_CPU_SCALE for x in res[0]]
+        return per_turn, {"kind": "port", "cores": 1, "bunches": nb, "particles": int(nb * cfg.params.np_model),
+                          "scaled": BEAM_ION_CPU_SCALE}
     if cores is None:
         cores = len(os.sched_getaffinity(0))
     procs = max(1, min(cores, nb))
@@ -227,11 +259,34 @@ def run_b200(args):
                "sample": "%d turns of the whole ring (%d bunches x %d macroparticles) split over %d "
                          "processes, one per core; first turn dropped; time = slowest process"
                          % (args.cpu_turns, info["bunches"], cfg.params.np_model, info["cores"])}
+        if info.get("scaled"):
+            cpu["sample"] = ("%d turns of the C restatement (no reference code exists for this stage) on one "
+                             "core with 1/%d of the electrons and of the macro-ions, time scaled by %d; first "
+                             "turn dropped" % (args.cpu_turns, info["scaled"], info["scaled"]))
 
     trk = api.Tracker.from_config(cfg, seed=1000 + rank)
     trk.generate_beam(77 + rank)
+    bi_info = None
+    if args.workload.startswith("beam_ion"):
+        bi = cfg.beam_ion()
+        bi.surrogate = 1 if args.workload == "beam_ion_mlp" else 0
+        trk.enable_beam_ion(bi)
+        bi_info = {"n_ip": bi.n_ip, "ions_per_passage": bi.ions_per_passage,
+                   "field_evaluations_per_turn": bi.n_ip * (bi.ions_per_passage * cfg.nbunch * (cfg.nbunch - 1) // 2
+                                                            + cfg.params.np_model * (cfg.nbunch - 1))}
+        if bi.surrogate:
+            mlp = api.Mlp(seed=31 + rank)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            hist = mlp.train(nsamples=1 << 23, batch=8192, steps=args.mlp_steps, lr=2e-3, seed=32 + rank)
+            torch.cuda.synchronize()
+            bi_info["training"] = {"seconds": time.perf_counter() - t0, "steps": args.mlp_steps, "batch": 8192,
+                                   "samples": 1 << 23, "final_loss": float(hist[-1])}
+            trk.use_mlp(mlp)
     trk.prepare()
     trk.run(args.warmup, stats=False)
+    if bi_info is not None and bi_info.get("training"):
+        trk.beam_ion_audit()   # reset the audit counters before the timed region
 
     # timed region: device time of K turns (CUDA events inside mbt_run_turns)
     if dist:
@@ -251,15 +306,27 @@ def run_b200(args):
         t_max = t_local
     value = world * npart * args.steps / t_max
 
+    audit = trk.beam_ion_audit() if (bi_info is not None and bi_info.get("training")) else None
     # per-kernel device times (events between the four kernels of a turn)
     prof = trk.profile(args.profile_turns)
     k1_ms = float(prof[0])
+    if bi_info is not None:
+        bi_ms = trk.beam_ion_timing()
+        bi_info["stage_ms_per_turn"] = bi_ms
+        bi_info["field_evaluations_per_s"] = bi_info["field_evaluations_per_turn"] / (bi_ms * 1e-3)
+        if audit is not None:
+            bi_info["audit"] = {"audited": int(audit[0]), "max_rel_error": float(audit[1]),
+                                "rms_rel_error": float(audit[2]), "faddeeva_fallbacks": int(audit[3]),
+                                "tensor_failures": int(audit[4])}
+            # network FLOPs: 2 x (3x128 + 2x128x128 + 128x2) per evaluation
+            tfl = 66816.0 * bi_info["field_evaluations_per_turn"] / (bi_ms * 1e-3) / 1e12
+            bi_info["network_tflops"] = tfl
     peak, peak_kind = measured_peak()
     achieved = BYTES_PER_MP_TURN * npart / (k1_ms * 1e-3) / 1e9
     traffic = profile_traffic(args.workload)
 
     # end to end through mbt_track with pinned host buffers
-    e2e_turns = args.e2e_turns
+    e2e_turns = args.e2e_turns if bi_info is None else min(args.e2e_turns, 5)
     pinned = torch.empty(6 * npart, dtype=torch.float64, pin_memory=True)
     host = pinned.numpy()
     host[:] = trk.get_all()
@@ -302,10 +369,13 @@ def run_b200(args):
                 "d2h_bytes_per_step": 6 * 8 * npart + e2e_turns * cfg.nbunch * 12 * 8,
                 "turns_per_step": e2e_turns, "steps": args.e2e_steps,
                 "call": "mbt_track (pinned host beam in, %d turns, stats + beam out)" % e2e_turns},
-        "gpu_launches": 4 * args.steps,
+        "gpu_launches": (4 if bi_info is None else 8) * args.steps,
         "clocks": clk.summary(),
         "finite": ok,
     }
+    if bi_info is not None:
+        line["beam_ion"] = bi_info
+        line["config"]["noise"] = "off"
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line))
@@ -319,14 +389,24 @@ def run_reference(args):
     import tempfile
     tmp = tempfile.mkdtemp()
     turns = args.warmup + args.steps
+    if args.workload.startswith("beam_ion"):
+        turns = 3 + min(args.steps, 2)   # about 10 s a turn even on the sample
     per_turn, info = cpu_run(args.workload, turns, tmp)
+    if args.workload.startswith("beam_ion"):
+        args.warmup, args.steps = 3, turns - 3
     timed = per_turn[args.warmup:]
     t = float(np.sum(timed))
+    if info.get("scaled"):
+        info["cores"] = 1
     value = info["particles"] * len(timed) / t
     _, _, desc = WORKLOADS[args.workload]
     sample = ("%d warm-up + %d timed turns of the whole ring (%d bunches) split over %d processes, "
               "one per core; time per turn = slowest process" % (args.warmup, args.steps, info["bunches"],
                                                                  info["cores"]))
+    if info.get("scaled"):
+        sample = ("%d warm-up + %d timed turns of the C restatement (no reference code exists for this stage) "
+                  "on one core with 1/%d of the electrons and of the macro-ions, time per turn scaled by %d"
+                  % (args.warmup, args.steps, info["scaled"], info["scaled"]))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3 / len(timed),
@@ -344,7 +424,8 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed turns (200; 20 for the beam-ion workloads)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="uniform")
@@ -353,7 +434,12 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-turns", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--mlp-steps", type=int, default=12000, help="training steps of the learned field")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 20 if args.workload.startswith("beam_ion") else 200
+    if args.workload.startswith("beam_ion"):
+        args.cpu_turns = min(args.cpu_turns, 2)
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
     if args.impl == "reference":

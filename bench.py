@@ -264,7 +264,22 @@ def run_b200(args):
                              "core with 1/%d of the electrons and of the macro-ions, time scaled by %d; first "
                              "turn dropped" % (args.cpu_turns, info["scaled"], info["scaled"]))
 
-    trk = api.Tracker.from_config(cfg, seed=1000 + rank)
+    tiles = None
+    if args.workload == "uneven":
+        # macroparticles proportional to the bunch charge, clamped to
+        # 2e3 .. 1e5, about 8e6 in total
+        frac = np.asarray(cfg.ib_frac, dtype=np.float64)
+        lo, hi = 1.0, 1e7
+        for _ in range(100):
+            k = math.sqrt(lo * hi)
+            tot = np.clip(np.rint(k * frac), 2000, 100000).sum()
+            lo, hi = (k, hi) if tot < 8e6 else (lo, k)
+        npb = np.clip(np.rint(k * frac), 2000, 100000).astype(np.int32)
+        trk = api.Tracker(cfg.params, cfg.bucket, npb, cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh,
+                          seed=1000 + rank)
+        npart = int(npb.sum())
+    else:
+        trk = api.Tracker.from_config(cfg, seed=1000 + rank)
     trk.generate_beam(77 + rank)
     bi_info = None
     if args.workload.startswith("beam_ion"):
@@ -284,6 +299,8 @@ def run_b200(args):
                                    "samples": 1 << 23, "final_loss": float(hist[-1])}
             trk.use_mlp(mlp)
     trk.prepare()
+    if args.workload == "uneven":
+        tiles = [int(x) for x in trk.autotune(trial_turns=10)]   # its trial turns are warm-up turns
     trk.run(args.warmup, stats=False)
     if bi_info is not None and bi_info.get("training"):
         trk.beam_ion_audit()   # reset the audit counters before the timed region
@@ -376,6 +393,10 @@ def run_b200(args):
     if bi_info is not None:
         line["beam_ion"] = bi_info
         line["config"]["noise"] = "off"
+    if tiles is not None:
+        line["config"]["np_per_bunch"] = "proportional to charge, clamped to 2e3..1e5"
+        line["config"]["tiles_per_size_class"] = {"np<=4096": tiles[0], "np<=32768": tiles[1], "larger": tiles[2]}
+        line["config"]["tiles_chosen_by"] = "mbt_autotune (coordinate descent, 10 device-timed turns per candidate)"
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line))

@@ -316,8 +316,20 @@ int mbt_last_timing(mbt_ctx *ctx, double out[4], int *launches_per_turn);
  * phasor scan and the bunch wakes. */
 int mbt_profile_turns(mbt_ctx *ctx, long nturns, double out[4]);
 
-/* Device layout: padded particle count, tile size, number of tiles. */
+/* Device layout: padded particle count, largest tile size, number of tiles. */
 int mbt_geometry(mbt_ctx *ctx, int *npad, int *tile, int *ntile);
+
+/* Tile sizes (particles per CTA of the particle pass, powers of two in
+ * 512..8192) per bunch-size class: bunches of up to 4096, up to 32768, and
+ * more macroparticles.  Each bunch is cut into ceil(np / T) equal tiles. */
+int mbt_set_tiles(mbt_ctx *ctx, const int tile[3]);
+
+/* Autotuner of the tile sizes: starting from the current sizes, tries every
+ * size for each class present (one pass of coordinate descent), timing
+ * trial_turns turns per candidate on the device, and keeps the fastest;
+ * tile_out (may be NULL) receives them.  After mbt_prepare; the trial turns
+ * are real turns of the run (their statistics are not returned). */
+int mbt_autotune(mbt_ctx *ctx, int trial_turns, int tile_out[3]);
 
 /* ---- per-step device entry points (device pointers) ------------------- */
 

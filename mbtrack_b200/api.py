@@ -47,6 +47,8 @@ SIGNATURES = {
     "mbt_get_histograms": (ctypes.c_int, [_vp, ctypes.c_int] + [_vp] * 6),
     "mbt_last_timing": (ctypes.c_int, [_vp, _vp, _vp]),
     "mbt_geometry": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "mbt_set_tiles": (ctypes.c_int, [_vp, _vp]),
+    "mbt_autotune": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     "mbt_bunch_moments_dev": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_double, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, _vp]),
     "mbt_bunch_moments_dev_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_double, ctypes.c_double,
@@ -404,6 +406,15 @@ class Tracker:
         arr = [np.zeros(n) for _ in range(6)]
         _check(lib().mbt_get_histograms(self.h, ib, *[_ptr(a) for a in arr]), self.h)
         return arr
+
+    def set_tiles(self, tiles):
+        t = np.ascontiguousarray(tiles, dtype=np.int32)
+        _check(lib().mbt_set_tiles(self.h, _ptr(t)), self.h)
+
+    def autotune(self, trial_turns=10):
+        t = np.zeros(3, dtype=np.int32)
+        _check(lib().mbt_autotune(self.h, trial_turns, _ptr(t)), self.h)
+        return t
 
     def timing(self):
         out = np.zeros(4)

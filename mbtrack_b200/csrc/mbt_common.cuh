@@ -28,21 +28,31 @@ __device__ __forceinline__ int bin_fast(double xtau, double sgm, double nsig, do
 
 // sin and cos of (a + d) from S = sin a, C = cos a and a small offset
 // |d| <= 0.25: angle addition, with sin d and cos d - 1 from their Taylor
-// series (terms to d^11 and d^12; truncation below 1e-17 relative).
+// series, to d^11 and d^12 in general and to d^7 and d^8 for |d| <= 0.04
+// (truncation below 1e-17 relative either way).
 __device__ __forceinline__ void sincos_near(double d, double S, double C, double &s, double &c) {
   const double d2 = d * d;
-  double ps = -1.0 / 39916800.0;
-  ps = fma(ps, d2, 1.0 / 362880.0);
-  ps = fma(ps, d2, -1.0 / 5040.0);
-  ps = fma(ps, d2, 1.0 / 120.0);
-  ps = fma(ps, d2, -1.0 / 6.0);
+  double ps, pc;
+  if (fabs(d) <= 0.04) {
+    ps = fma(-1.0 / 5040.0, d2, 1.0 / 120.0);
+    ps = fma(ps, d2, -1.0 / 6.0);
+    pc = fma(1.0 / 40320.0, d2, -1.0 / 720.0);
+    pc = fma(pc, d2, 1.0 / 24.0);
+    pc = fma(pc, d2, -0.5);
+  } else {
+    ps = -1.0 / 39916800.0;
+    ps = fma(ps, d2, 1.0 / 362880.0);
+    ps = fma(ps, d2, -1.0 / 5040.0);
+    ps = fma(ps, d2, 1.0 / 120.0);
+    ps = fma(ps, d2, -1.0 / 6.0);
+    pc = 1.0 / 479001600.0;
+    pc = fma(pc, d2, -1.0 / 3628800.0);
+    pc = fma(pc, d2, 1.0 / 40320.0);
+    pc = fma(pc, d2, -1.0 / 720.0);
+    pc = fma(pc, d2, 1.0 / 24.0);
+    pc = fma(pc, d2, -0.5);
+  }
   const double sd = fma(d * d2, ps, d);            // sin d
-  double pc = 1.0 / 479001600.0;
-  pc = fma(pc, d2, -1.0 / 3628800.0);
-  pc = fma(pc, d2, 1.0 / 40320.0);
-  pc = fma(pc, d2, -1.0 / 720.0);
-  pc = fma(pc, d2, 1.0 / 24.0);
-  pc = fma(pc, d2, -0.5);
   const double cm1 = pc * d2;                      // cos d - 1
   s = S + fma(S, cm1, C * sd);
   c = C + fma(C, cm1, -(S * sd));

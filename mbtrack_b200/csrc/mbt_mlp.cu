@@ -42,7 +42,6 @@ constexpr int kFwdThreads = 256;   // training forward: two groups of 128
 constexpr int kBwdThreads = 128;
 constexpr size_t kFwdSmem = 6 * kTileBytes + 1024 + 8192;
 constexpr int kInfThreads = 128 * kMlpGroups;
-constexpr int kActTiles = kMlpSplit ? 2 : 1;      // activation tiles per group
 constexpr size_t kInfSmem = kMlpCtaSmem;
 constexpr size_t kBwdSmem = 5 * kTileBytes + 1024 + 2048;
 

@@ -167,10 +167,9 @@ __device__ __forceinline__ void store_row_bf16(uint8_t *t, int row, const float 
 }
 // Row `row` of an activation tile: 128 values -> hi and lo BF16 tiles.
 __device__ __forceinline__ void store_row_split(uint8_t *hi, uint8_t *lo, int row, const float *h) {
-  if (!kMlpSplit) {
+  if constexpr (!kMlpSplit) {
     store_row_bf16(hi, row, h);
-    return;
-  }
+  } else {
 #pragma unroll
   for (int c = 0; c < 16; ++c) {
     float v[8], l[8];
@@ -185,6 +184,7 @@ __device__ __forceinline__ void store_row_split(uint8_t *hi, uint8_t *lo, int ro
                                 pack_bf16(l[6], l[7]));
     *reinterpret_cast<uint4 *>(hi + sw128_chunk(row, c)) = ph;
     if (kMlpSplit) *reinterpret_cast<uint4 *>(lo + sw128_chunk(row, c)) = pl;
+  }
   }
 }
 // Column `col` of a tile (the transpose of a row), BF16.
@@ -219,11 +219,10 @@ struct MlpGroup {
 
 // 8 hidden values -> one 16-byte chunk of the hi and lo tiles of row t.
 __device__ __forceinline__ void store_chunk_split(const MlpGroup &G, int t, int c, const float *h) {
-  if (!kMlpSplit) {
+  if constexpr (!kMlpSplit) {
     *reinterpret_cast<uint4 *>(G.Ahi + sw128_chunk(t, c)) =
         make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]), pack_bf16(h[6], h[7]));
-    return;
-  }
+  } else {
   float v[8], l[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
@@ -234,6 +233,7 @@ __device__ __forceinline__ void store_chunk_split(const MlpGroup &G, int t, int 
       make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
   *reinterpret_cast<uint4 *>(G.Alo + sw128_chunk(t, c)) =
       make_uint4(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]), pack_bf16(l[4], l[5]), pack_bf16(l[6], l[7]));
+  }
 }
 
 // The network on this thread's features x -> y (Yx, Yy).  Every thread of

@@ -112,13 +112,14 @@ __device__ __forceinline__ void turn_normals1(const PhiloxKeys &K, uint32_t part
                                               uint64_t turn, float g[5]) {
   const U4 c0 = {particle, bucket, (uint32_t)turn, ((uint32_t)(turn >> 32) << 1) | 0u};
   const U4 r = philox4x32_10k(c0, K);
-  float n5;
   box_muller_u(u01_open0(r.x), r.y, g[0], g[1]);
   box_muller_u(u01_open0(r.z), r.w, g[2], g[3]);
-  // third pair from the low bits: radius 9 + 14 = 23 bits, angle 18 bits
+  // fifth deviate from the low bits: radius 9 + 14 = 23 bits, angle 18 bits
+  // (the cosine member of the pair; its sine partner is not needed)
   const uint32_t rr = ((r.x & 0x1FFu) << 23) | ((r.y & 0x3FFFu) << 9);
   const uint32_t aa = (((r.z & 0x1FFu) << 9) | (r.w & 0x1FFu)) << 14;
-  box_muller_u(u01_open0(rr), aa, g[4], n5);
+  const float th = (float)((int)(aa >> 14) - 131072) * 2.396844980841821872e-05f;
+  g[4] = __fsqrt_rn(-2.0f * __logf(u01_open0(rr))) * __cosf(th);
 }
 
 // Five deviates from two Philox calls (full 24-bit uniforms for both

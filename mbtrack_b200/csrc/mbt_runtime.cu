@@ -51,6 +51,8 @@ int fail_global(int code, const char *fmt, ...) {
 struct mbt_ctx {
   mbt_params p{};
   int nbunch = 0, npad = 0, tile = 0, ntile = 0, prec = 0, nc = 0, nlr = 0;
+  int class_tile[3] = {0, 0, 0};   // tile size per bunch-size class (mbt_set_tiles)
+  int tile_cap = 0;                // tiles the device arrays hold
   std::vector<int> bucket, np, off, tile0, ntiles, bucket_bunch;
   std::vector<double> ib;
   std::vector<Tile> tiles;
@@ -141,6 +143,29 @@ int choose_tile(const std::vector<int> &np, int sms) {
   int t = 512;
   while (t < 8192 && t < want) t <<= 1;
   return t;
+}
+
+// Bunch-size class of a bunch for the tile table: up to 4096, up to 32768,
+// more macroparticles.
+int size_class(int np) { return np <= 4096 ? 0 : (np <= 32768 ? 1 : 2); }
+
+// Tiles of every bunch from the class tile sizes: ceil(np / T) tiles of
+// equal size (a multiple of 32 particles) inside each bunch.
+void layout_tiles(mbt_ctx *c) {
+  c->tiles.clear();
+  for (int b = 0; b < c->nbunch; ++b) {
+    const int T = c->class_tile[size_class(c->np[b])];
+    c->tile0[b] = (int)c->tiles.size();
+    const int nt = (c->np[b] + T - 1) / T;
+    const int per = ((c->np[b] + nt - 1) / nt + 31) / 32 * 32;
+    for (int s = 0; s < c->np[b]; s += per) {
+      Tile t{b, c->off[b] + s, std::min(per, c->np[b] - s), 0};
+      c->tiles.push_back(t);
+    }
+    c->ntiles[b] = (int)c->tiles.size() - c->tile0[b];
+  }
+  c->ntile = (int)c->tiles.size();
+  c->tile = std::max(c->class_tile[0], std::max(c->class_tile[1], c->class_tile[2]));
 }
 
 void cmul(double a0, double a1, double b0, double b1, double &r0, double &r1) {
@@ -326,27 +351,21 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   for (auto &e : c->ev) cudaEventCreate(&e);
 
   // geometry: bunches padded to 32 particles, tiles inside bunches
-  c->tile = choose_tile(c->np, prop.multiProcessorCount);
+  const int t0 = choose_tile(c->np, prop.multiProcessorCount);
+  for (int k = 0; k < 3; ++k) c->class_tile[k] = t0;
   c->off.resize(nbunch);
   c->tile0.resize(nbunch);
   c->ntiles.resize(nbunch);
   long pos = 0;
   for (int b = 0; b < nbunch; ++b) {
     c->off[b] = (int)pos;
-    c->tile0[b] = (int)c->tiles.size();
-    // ceil(np / tile) tiles of equal size (a multiple of 32 particles)
-    const int nt = (c->np[b] + c->tile - 1) / c->tile;
-    const int per = ((c->np[b] + nt - 1) / nt + 31) / 32 * 32;
-    for (int s = 0; s < c->np[b]; s += per) {
-      Tile t{b, (int)(pos + s), std::min(per, c->np[b] - s), 0};
-      c->tiles.push_back(t);
-    }
-    c->ntiles[b] = (int)c->tiles.size() - c->tile0[b];
     pos += (c->np[b] + 31) / 32 * 32;
+    c->tile_cap += (c->np[b] + 511) / 512;   // the most tiles the smallest tile size makes
   }
   if (pos > 0x7fffffffL / 6) return bail(fail(nullptr, MBT_ERR_INVALID, "beam too large for one context"));
   c->npad = (int)pos;
-  c->ntile = (int)c->tiles.size();
+  layout_tiles(c);
+  c->tile_cap = std::max(c->tile_cap, c->ntile);
   c->nc = std::max(p->ncell, 1);
   c->bucket_bunch.assign(p->nharm, -1);
   for (int b = 0; b < nbunch; ++b) c->bucket_bunch[c->bucket[b]] = b;
@@ -500,7 +519,9 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   auto gl = [&](const double *g) { return g ? g : g0.data(); };
   rc = rc ? rc : dalloc(c, &a.coord, (size_t)6 * c->npad);
   Tile *tiles_d = nullptr;
-  rc = rc ? rc : dupload(c, &tiles_d, c->tiles.data(), c->tiles.size());
+  rc = rc ? rc : dalloc(c, &tiles_d, (size_t)c->tile_cap);
+  if (!rc && cudaMemcpy(tiles_d, c->tiles.data(), c->tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = fail(nullptr, MBT_ERR_CUDA, "tile upload");
   a.tiles = tiles_d;
   int *ip;
   rc = rc ? rc : dupload(c, &ip, c->tile0.data(), nbunch); a.bunch_tile0 = ip;
@@ -517,7 +538,7 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   rc = rc ? rc : dupload(c, &dp, gl(Gl), c->nc); a.Gl = dp;
   rc = rc ? rc : dupload(c, &dp, gl(Gv), c->nc); a.Gv = dp;
   rc = rc ? rc : dupload(c, &dp, gl(Gh), c->nc); a.Gh = dp;
-  rc = rc ? rc : dalloc(c, &a.part, (size_t)c->ntile * c->prec);
+  rc = rc ? rc : dalloc(c, &a.part, (size_t)c->tile_cap * c->prec);
   rc = rc ? rc : dalloc(c, &a.shift, (size_t)nbunch * 6);
   rc = rc ? rc : dalloc(c, &a.hist, (size_t)nbunch * 6 * c->nc);
   rc = rc ? rc : dalloc(c, &a.cellrange, (size_t)nbunch * 2);
@@ -1042,6 +1063,68 @@ int mbt_last_timing(mbt_ctx *c, double out[4], int *launches_per_turn) {
   if (!c || !out) return MBT_ERR_INVALID;
   for (int k = 0; k < 4; ++k) out[k] = c->timing[k];
   if (launches_per_turn) *launches_per_turn = 4;
+  return 0;
+}
+
+int mbt_set_tiles(mbt_ctx *c, const int tile[3]) {
+  if (!c || !tile) return MBT_ERR_INVALID;
+  for (int k = 0; k < 3; ++k)
+    if (tile[k] < 512 || tile[k] > 8192 || (tile[k] & (tile[k] - 1)))
+      return fail(c, MBT_ERR_INVALID, "tile sizes are powers of two in 512..8192 (class %d: %d)", k, tile[k]);
+  for (int k = 0; k < 3; ++k) c->class_tile[k] = tile[k];
+  layout_tiles(c);
+  if (c->ntile > c->tile_cap) return fail(c, MBT_ERR_INVALID, "tile table overflow");
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(const_cast<Tile *>(c->a.tiles), c->tiles.data(), c->tiles.size() * sizeof(Tile),
+                cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(const_cast<int *>(c->a.bunch_tile0), c->tile0.data(), c->nbunch * sizeof(int),
+                cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(const_cast<int *>(c->a.bunch_ntile), c->ntiles.data(), c->nbunch * sizeof(int),
+                cudaMemcpyHostToDevice));
+  c->a.ntile = c->ntile;
+  c->a.tile = c->tile;
+  if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; c->graph_turns = 0; }
+  return 0;
+}
+
+int mbt_autotune(mbt_ctx *c, int trial_turns, int tile_out[3]) {
+  if (!c || trial_turns < 1) return MBT_ERR_INVALID;
+  if (!c->prepared) return fail(c, MBT_ERR_STATE, "mbt_prepare must come first");
+  bool present[3] = {false, false, false};
+  for (int b = 0; b < c->nbunch; ++b) present[size_class(c->np[b])] = true;
+  int best[3] = {c->class_tile[0], c->class_tile[1], c->class_tile[2]};
+  auto trial = [&](const int *t, double *ms) {
+    int r = mbt_set_tiles(c, t);
+    if (r) return r;
+    r = run_core(c, 1, nullptr, nullptr, true);   // graph build and warm-up
+    if (r) return r;
+    r = run_core(c, trial_turns, nullptr, nullptr, true);
+    *ms = c->timing[3];
+    return r;
+  };
+  double best_ms = 0.0;
+  int r = trial(best, &best_ms);
+  if (r) return r;
+  // one pass of coordinate descent over the classes present
+  for (int k = 0; k < 3; ++k) {
+    if (!present[k]) continue;
+    for (int T = 512; T <= 8192; T <<= 1) {
+      if (T == best[k]) continue;
+      int cand[3] = {best[0], best[1], best[2]};
+      cand[k] = T;
+      double ms = 0.0;
+      r = trial(cand, &ms);
+      if (r) return r;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best[k] = T;
+      }
+    }
+  }
+  r = mbt_set_tiles(c, best);
+  if (r) return r;
+  if (tile_out)
+    for (int k = 0; k < 3; ++k) tile_out[k] = best[k];
   return 0;
 }
 

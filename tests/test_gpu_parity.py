@@ -184,3 +184,32 @@ def test_amplitude_invariants(cuda_device, libmbt):
             assert abs(got[k] - ref[k]) <= 1e-10 * abs(ref[k])
             assert abs(got[3 + k] - ref[3 + k]) <= 1e-10 * abs(ref[k])
         assert got[0] == 0.0 and got[3] == 0.0
+
+
+def test_tile_sizes_do_not_change_the_physics(tmp_path, cuda_device):
+    """Re-tiling (mbt_set_tiles, as the autotuner does) changes only the
+    grouping of the moment sums: statistics agree to rounding, counts are
+    exact; the autotuner returns valid sizes."""
+    conf = small_conf(tmp_path, "uneven_fill.conf", Np=4000)
+    C = api.Config(conf)
+    rng = np.random.default_rng(3)
+    npb = rng.integers(1000, 40000, C.nbunch).astype(np.int32)
+    beams = None
+    out = []
+    for tiles in ([4096, 4096, 4096], [512, 2048, 8192]):
+        t = api.Tracker(C.params, C.bucket, npb, C.bunch_currents(), C.Gl, C.Gv, C.Gh, seed=5)
+        if beams is None:
+            t.generate_beam(9)
+            beams = [t.get_particles(i) for i in range(C.nbunch)]
+        else:
+            for i, b in enumerate(beams):
+                t.load_particles(i, b)
+        t.prepare()
+        t.set_tiles(tiles)
+        out.append((t.run(10), t.histograms(7)[0]))
+        if tiles[0] == 512:
+            chosen = t.autotune(trial_turns=2)
+            assert all(512 <= x <= 8192 and (x & (x - 1)) == 0 for x in chosen)
+    from tests.util import stats_err
+    assert stats_err(out[1][0], out[0][0]).max() < 1e-11
+    assert np.array_equal(out[1][1], out[0][1])

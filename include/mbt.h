@@ -102,6 +102,18 @@ typedef struct mbt_params {
   int    Nmlt;           /* turns of RW memory */
   int    triggerRW;
   long   nrev_tot, nrev_mon;
+  /* [scan] (input.c:807-846, setup_tracking_parameters :1710-1736):
+   * scan 0 none; 1 ring current, stepped by scan_step [mA] every
+   * nrev_scan turns (tracking_scan_step_worker tracking.c:43-57);
+   * 2 chromaticity and 3, 4 Q factor, which the reference steps nothing
+   * for (3 and 4 scale the LON resonators' Q at set-up).  Every scan
+   * boundary restarts the resistive-wall trigger count
+   * (worker_weakweak.c:389-393).  nrev_scan = NrevTot + 1 without a scan;
+   * with one NrevTot = nscan x nrev_scan.  scan_start is the value the
+   * statistics files print before the first step. */
+  int    scan;
+  long   nscan, nrev_scan;
+  double scan_start, scan_step;
 
   /* bunch_macroparticle_model_t (bunch.h:22-50), SI units */
   int    np_model;       /* Np of the model (bunchModel.Np) */
@@ -147,8 +159,8 @@ typedef struct mbt_ctx mbt_ctx;
  * EnableRW_short (the reference leaves them 0, input.c:465-478).
  * Returns MBT_ERR_CONFIG (message in mbt_config_error()) for a missing or
  * malformed key, and for what this library does not run: short-range
- * resistive wall, parameter scans, BunchModel = STRONG, modeHT excitation
- * and distribution files. */
+ * resistive wall, BunchModel = STRONG, modeHT excitation and distribution
+ * files. */
 int mbt_config_load(const char *conf_path, int fix_rw_beff, mbt_params *p,
                     int *nbunch, int *bucket, double *ib_frac);
 
@@ -175,10 +187,8 @@ size_t mbt_params_size(void);
 typedef struct mbt_output_cfg {
   char   jobtitle[80];          /* [tracking] jobtitle (first word, "%s") */
   char   gendst_file[3][1024];  /* [distribution] gendst_datafile_LON/HOR/VER */
-  long   nrev_scan;             /* NrevScan; NrevTot + 1 without a scan */
   long   nrev_potentials_out;   /* NrevPotentialsOut (0 when absent) */
   int    ampinv_out;            /* EnableAmpinv_out (0 when absent) */
-  double scan_start;            /* scan value printed in the statistics files */
   int    n_out;                 /* tracking_t.Nbunch_out */
 } mbt_output_cfg;
 

@@ -49,6 +49,8 @@ class MbtParams(ctypes.Structure):
         ("ahc_phi", _d * MBT_MAX_AHC),
         ("track_plane", _i * 3), ("quantum", _i), ("rw_long", _i),
         ("Nmlt", _i), ("triggerRW", _i), ("nrev_tot", _l), ("nrev_mon", _l),
+        ("scan", _i), ("nscan", _l), ("nrev_scan", _l),
+        ("scan_start", _d), ("scan_step", _d),
         ("np_model", _i), ("iseed", _i * 3),
         ("pos_offset", _d * 3), ("slope_offset", _d * 3),
         ("pos_sgm", _d * 3), ("slope_sgm", _d * 3), ("correlate", _d * 3),
@@ -84,8 +86,7 @@ class MbtOutputCfg(ctypes.Structure):
     _fields_ = [
         ("jobtitle", ctypes.c_char * 80),
         ("gendst_file", (ctypes.c_char * 1024) * 3),
-        ("nrev_scan", _l), ("nrev_potentials_out", _l),
-        ("ampinv_out", _i), ("scan_start", _d), ("n_out", _i),
+        ("nrev_potentials_out", _l), ("ampinv_out", _i), ("n_out", _i),
     ]
 
 

@@ -112,9 +112,9 @@ struct Args {
   const int *bunch_np;
   const int *bunch_kb;
   const int *bunch_off;
-  const double *bunch_ib;     // [A]
+  double *bunch_ib;           // [A]; stepped by a current scan
   const double *bunch_fac;    // per long-range resonator: Amp / Np * 1e-3  [nlr][nbunch]
-  const double *bunch_factg;  // factG (transform_weak.c:567)
+  double *bunch_factg;        // factG (transform_weak.c:567), follows bunch_ib
   double *part;               // ntile x prec
   double *shift;              // nbunch x 6
   double *hist;               // nbunch x 6 x ncell: fnp, dipV, dipH (clamped), ring L, H, V (dropped)
@@ -135,7 +135,7 @@ struct Args {
   double *lr_vs;              // nlr x nharm x 2: phasor at bucket start
   const double *lr_pw;        // nlr x ncell x 2: prog^(j+1)
   const int *bucket_bunch;    // nharm: bunch index or -1
-  const double *ibunch;       // nharm: [mA]
+  double *ibunch;             // nharm: [mA], the current the next turn's wakes use
   int lr_kick[3];             // apply long-range wake in plane (kick gate)
   // self-field
   const double *Gl, *Gv, *Gh;
@@ -147,6 +147,8 @@ struct Args {
   int rw_long, Nmlt;
   double *dipole;             // (Nmlt+2) nharm x 2
   double *rw_e;               // 2 x (Nmlt+2) nharm: dipole x bucket current [mA], planar
+  double *rw_ib;              // nharm: [mA], the current of this turn's resistive-wall kick
+                              // (ibunch itself unless a current scan runs)
   const double *rw_rsq;       // (Nmlt+1) nharm + 1: 1 / sqrt(m T0 / h)
   double rw_const[2][2];      // [trigger halved?][plane-1]
   int triggerRW;

@@ -245,9 +245,6 @@ typedef struct cfg {
   int lr_m[MBT_MAX_LR];
   double lr_detune[MBT_MAX_LR];
   int rffb_len_raw;
-  int scan;
-  long nscan, nrev_scan;
-  double scan_start, scan_step;
   int Nslc;
   double q;                      /* ring->q = U0 / Vrf0 / 1e6 (input.c:1606) */
   mbt_output_cfg out;            /* output settings */
@@ -491,21 +488,26 @@ static int read_conf(const char *path, int fix_rw_beff, cfg_t *g)
     }
   }
   /* [scan] */
-  g->scan = 0;
-  g->nscan = 1;
-  g->nrev_scan = p->nrev_tot + 1;
+  p->scan = 0;
+  p->nscan = 1;
+  p->nrev_scan = p->nrev_tot + 1;
+  p->scan_start = 0.0;
+  p->scan_step = 0.0;
   if (have_section(&C, "scan")) {
-    REQ_I("scan", "scan_type", &g->scan);
-    if (g->scan != 0) {
-      REQ_L("scan", "Nscan", &g->nscan);
-      REQ_L("scan", "NrevScan", &g->nrev_scan);
-      if (g->scan == 1) { REQ_D("scan", "scan_start", &g->scan_start); REQ_D("scan", "scan_step", &g->scan_step); }
-      if (g->scan == 4) REQ_D("scan", "scan_start", &g->scan_start);
-      p->nrev_tot = g->nscan * g->nrev_scan;
+    REQ_I("scan", "scan_type", &p->scan);
+    if (p->scan != 0) {
+      REQ_L("scan", "Nscan", &p->nscan);
+      REQ_L("scan", "NrevScan", &p->nrev_scan);
+      if (p->scan == 1) { REQ_D("scan", "scan_start", &p->scan_start); REQ_D("scan", "scan_step", &p->scan_step); }
+      if (p->scan == 4) REQ_D("scan", "scan_start", &p->scan_start);
+      p->nrev_tot = p->nscan * p->nrev_scan;
     }
   }
   if (g->enable_rw_short || g->enable_rw_short_lon) { r = cfg_fail("short-range resistive wall is not supported yet"); goto out; }
-  if (g->scan != 0) { r = cfg_fail("parameter scans are not supported yet"); goto out; }
+  /* the reference takes any integer type (and steps only type 1) and
+     divides by NrevScan every turn */
+  if (p->scan < 0 || p->scan > 4) { r = cfg_fail("[scan] scan_type %d is not 0..4", p->scan); goto out; }
+  if (p->scan != 0 && (p->nscan < 1 || p->nrev_scan < 1)) { r = cfg_fail("[scan] Nscan and NrevScan must be positive"); goto out; }
   (void) ltmp;
 out:
   conf_free(&C);
@@ -647,6 +649,19 @@ static int setup_tracking(cfg_t *g)
     }
     p->HC_k = -cos(p->phai0) / (p->m_aHC * cos(p->m_aHC * p->phi_n));
   }
+  if (p->scan == 1) p->Iring = p->scan_start;
+  if (p->scan == 3 || p->scan == 4) {
+    int i;
+    if (p->n_lr[0] < 1) return cfg_fail("Qfactor scan but no longrange resonator given");
+    if (p->scan == 3) {
+      p->scan_start = 1. / p->nscan;
+      p->scan_step = 1. / p->nscan;
+      for (i = 0; i < p->n_lr[0]; i++) p->lr_Q[0][i] = p->lr_Q[0][i] / p->nscan;
+    } else {
+      p->scan_step = (1. - p->scan_start) / (p->nscan - 1);
+      for (i = 0; i < p->n_lr[0]; i++) p->lr_Q[0][i] = p->lr_Q[0][i] * p->scan_start;
+    }
+  }
   b = p->beffL[1];
   if (p->beffH[1] > b && p->track_plane[1] == 1) b = p->beffH[1];
   else if (p->beffV[1] > b && p->track_plane[2] == 1) b = p->beffV[1];
@@ -778,8 +793,6 @@ int mbt_config_output(const char *conf_path, mbt_output_cfg *o, int *bunch_out)
   }
   if (!r) r = setup_beam(g, &nb, NULL, NULL);
   if (!r) {
-    g->out.nrev_scan = g->nrev_scan;
-    g->out.scan_start = g->scan_start;
     *o = g->out;
     if (bunch_out) memcpy(bunch_out, g->bunch_out, (size_t) g->out.n_out * sizeof(int));
   }

@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(kBlock) bunch_reduce(Args a, int mode, double 
   // fill :203-219)
   if (a.rw_long && threadIdx.x == 0) {
     const long n = (long)(a.Nmlt + 2) * a.nharm;
-    const double ibk = a.ibunch[kb];
+    const double ibk = a.rw_ib[kb];
     if (mode == kReduceTurn) {
       const long sl = cyc_slot(-turn * a.nharm + kb, n);
       a.dipole[2 * sl] = mean6[1];
@@ -887,6 +887,45 @@ __global__ void add_pending_rw(Args a, double *out) {
     if (a.oc.track_h) out[4 * n6 + off + j] = a.coord[4 * n6 + off + j] + rh;
     if (a.oc.track_v) out[5 * n6 + off + j] = a.coord[5 * n6 + off + j] + rv;
   }
+}
+
+// Current-scan step, first half (tracking_scan_step_worker tracking.c:43-57,
+// called at the end of turn rev when (rev+1) % NrevScan == 0): the bucket
+// currents of the long-range source terms and the bunch currents behind
+// factG (transform_weak.c:567).  It runs before the bunch reduction of that
+// turn, whose long-range terms, ring scan and bunch wakes all belong to
+// the next turn's self-field step.  d_ma = scan_step / Nbunch [mA],
+// d_a = scan_step / (Nbunch 1e3) [A].
+__global__ void scan_currents(Args a, double d_ma, double d_a, double T0, double E0) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < a.nharm && a.bucket_bunch[i] >= 0) a.ibunch[i] = __dadd_rn(a.ibunch[i], d_ma);
+  if (i < a.nbunch) {
+    const double ib = __dadd_rn(a.bunch_ib[i], d_a);
+    a.bunch_ib[i] = ib;
+    a.bunch_factg[i] = __ddiv_rn(__dmul_rn(-T0, ib), __dmul_rn(__dmul_rn((double)a.bunch_np[i], E0), 1.0e9));
+  }
+}
+
+// Current-scan step, second half, at the end of the same turn (after its
+// resistive-wall sums): every dipole of the history is weighted with its
+// bucket's new current, as the reference's kick reads Ibunch when it runs
+// (transform_weak.c:822); the trigger count restarts
+// (worker_weakweak.c:392).  rescale = 0 restarts the count only (the scan
+// types that step nothing).  bi_ib: the beam-ion stage's bunch currents
+// [A], or null.
+__global__ void scan_rw(Args a, int rescale, double d_a, double *bi_ib) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0 && a.rw_long) a.rs->rw_m = 0;
+  if (rescale && a.rw_long) {
+    const long n = (long)(a.Nmlt + 2) * a.nharm;
+    if (i < n) {
+      const double ib = a.ibunch[i % a.nharm];
+      a.rw_e[i] = a.dipole[2 * i] * ib;
+      a.rw_e[n + i] = a.dipole[2 * i + 1] * ib;
+    }
+    if (i < a.nharm) a.rw_ib[i] = a.ibunch[i];
+  }
+  if (rescale && bi_ib != nullptr && i < a.nbunch) bi_ib[i] = __dadd_rn(bi_ib[i], d_a);
 }
 
 // First-particle shifts for the moment sums of the first binning pass.

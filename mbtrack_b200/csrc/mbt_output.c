@@ -84,7 +84,10 @@ struct mbt_writer {
   double (*cm)[3], (*ai)[3], (*aic)[3];
   double *scan_hist;
   long nscan_hist, m;
-  double scan_val;
+  long nrev_scan;                   /* NrevScan (NrevTot + 1 without a scan) */
+  double scan_val, iring;           /* manager's scan value and ring current */
+  double scan_val_w, iring_w;       /* the workers' (they step one turn earlier
+                                       when NrevScan = 1) */
   double (*dip)[2];                 /* resistive-wall dipole ring buffer */
   long ndip;
   int began;
@@ -168,6 +171,7 @@ int mbt_writer_open(const char *work_path, const mbt_params *p, const mbt_output
     return werr(MBT_ERR_INVALID, "writer: null argument or nbunch <= 0");
   if (p->nrev_mon <= 0 || p->nrev_tot < 0 || p->nharm <= 0)
     return werr(MBT_ERR_INVALID, "writer: NrevMon must be positive");
+  if (p->scan != 0 && p->nrev_scan < 1) return werr(MBT_ERR_INVALID, "writer: NrevScan must be positive");
   for (i = 0; i < nbunch; i++)
     if (bucket[i] < 0 || bucket[i] >= p->nharm || (i > 0 && bucket[i] <= bucket[i - 1]))
       return werr(MBT_ERR_INVALID, "writer: buckets must be ascending in 0..h-1");
@@ -191,9 +195,12 @@ int mbt_writer_open(const char *work_path, const mbt_params *p, const mbt_output
   w->cm = calloc(w->nhist, sizeof(*w->cm));
   w->ai = calloc(w->nhist, sizeof(*w->ai));
   w->aic = calloc(w->nhist, sizeof(*w->aic));
-  w->nscan_hist = w->nmon_rows + 1;
+  /* manager_weakweak.c:29-32: one entry per statistics line */
+  w->nscan_hist = w->nmon_rows + (p->scan != 0 ? p->nscan : 1) + 1;
   w->scan_hist = (double *) calloc(w->nscan_hist, sizeof(double));
-  w->scan_val = o->scan_start;
+  w->nrev_scan = p->scan != 0 ? p->nrev_scan : p->nrev_tot + 1;
+  w->scan_val = w->scan_val_w = p->scan_start;
+  w->iring = w->iring_w = p->Iring;
   if (p->rw_long) {
     w->ndip = (long) (p->Nmlt + 2) * p->nharm;
     w->dip = calloc(w->ndip, sizeof(*w->dip));
@@ -374,15 +381,15 @@ int mbt_writer_turns(mbt_writer *w, long nturns, const double *stats, const doub
     for (i = 0; i < w->n_out; i++) {
       acc_add_tracked(&w->out_acc[i], st + 12 * w->out[i], tp);
       w->nstat_out[i]++;
-      if (w->nstat_out[i] % mon == 0 || (rev + 1) % w->o.nrev_scan == 0) {
+      if (w->nstat_out[i] % mon == 0 || (rev + 1) % w->nrev_scan == 0) {
         acc_update(&w->out_acc[i], w->nstat_out[i]);
-        acc_print(w->out_fp[i], rev, &w->out_acc[i], w->scan_val, tp);
+        acc_print(w->out_fp[i], rev, &w->out_acc[i], w->scan_val_w, tp);
         acc_reset(&w->out_acc[i]);
         w->nstat_out[i] = 0;
       }
     }
     /* manager output (manager_weakweak.c:291-302) */
-    if (w->nstat_all % mon == 0 || (rev + 1) % w->o.nrev_scan == 0) {
+    if (w->nstat_all % mon == 0 || (rev + 1) % w->nrev_scan == 0) {
       w->nstat_all *= w->nb;
       acc_update(&w->all, w->nstat_all);
       if (w->m < w->nscan_hist) w->scan_hist[w->m] = w->scan_val;
@@ -394,6 +401,18 @@ int mbt_writer_turns(mbt_writer *w, long nturns, const double *stats, const doub
       acc_print(w->all_fp, rev, &w->all, w->scan_val, tp);
       acc_reset(&w->all);
       w->nstat_all = 0;
+    }
+    /* scan step: manager after turn 0 only (manager_weakweak.c:287-288,
+       tracking.c:10-16), workers on every boundary (worker_weakweak.c:389-391,
+       tracking.c:43-48); only a current scan moves the value */
+    if ((rev + 1) % w->nrev_scan == 0 && w->p.scan == 1) {
+      if (rev > 0) {
+        w->iring += w->p.scan_step;
+        w->scan_val = w->iring;
+      }
+      w->iring_w += w->p.scan_step;
+      w->scan_val_w = w->iring_w;
+      for (b = 0; b < w->nb; b++) w->ib[b] += w->p.scan_step / (((double) w->nb) * FKILO);
     }
     /* resistive-wall ring buffer (worker_weakweak.c:306-318) */
     if (w->p.rw_long) {
@@ -415,7 +434,7 @@ int mbt_writer_potentials_due(const mbt_writer *w, long rev)
   /* the self-field step runs (worker_weakweak.c:264-265) */
   if (p->ncell <= 0 || p->planeL + p->planeV + p->planeH + p->n_lr[0] + p->n_lr[1] + p->n_lr[2] <= 0) return 0;
   return (rev + 1) % w->p.nrev_mon == 0 &&
-         rev + 1 >= w->o.nrev_potentials_out + (rev / w->o.nrev_scan) * w->o.nrev_scan;
+         rev + 1 >= w->o.nrev_potentials_out + (rev / w->nrev_scan) * w->nrev_scan;
 }
 
 int mbt_writer_potentials(mbt_writer *w, int ibunch, long rev, const double *pot, double vrf0, double phai0)
@@ -441,7 +460,7 @@ int mbt_writer_potentials(mbt_writer *w, int ibunch, long rev, const double *pot
       active += p->ahc_vpeak[j] / (p->E0 * FGIGA) *
                 sin(p->wrf * p->ahc_nhc[j] * taucell + p->ahc_phi[j] + p->ahc_nhc[j] * kb * 2 * M_PI);
     ideal = facI * sin(p->m_aHC * p->wrf * taucell + p->m_aHC * p->phi_n);
-    fprintf(fp, "\n %ld   %e   %e   %e    %e   %e   %e   %e   %e", rev + 1, w->scan_val, taucell, pot[icell],
+    fprintf(fp, "\n %ld   %e   %e   %e    %e   %e   %e   %e   %e", rev + 1, w->scan_val_w, taucell, pot[icell],
             pot[nc + icell], rftest, active, ideal, pot[2 * nc + icell]);
     if (p->planeV > 0) fprintf(fp, "   %e   %e", pot[3 * nc + icell], pot[4 * nc + icell]);
     if (p->planeH > 0) fprintf(fp, "   %e   %e", pot[5 * nc + icell], pot[6 * nc + icell]);
@@ -460,16 +479,18 @@ int mbt_writer_end(mbt_writer *w, const double *end_stats)
   if (!w || !end_stats) return werr(MBT_ERR_INVALID, "writer end: null argument");
   if (w->rev != w->p.nrev_tot)
     return werr(MBT_ERR_STATE, "writer end: %ld of %ld turns received", w->rev, w->p.nrev_tot);
-  /* mean_bunch_end.dat (the reference writes it when no scan runs) */
-  fp = open_in(w, "mean_bunch_end.dat", "w+");
-  if (!fp) return werr(MBT_ERR_IO, "cannot create %s/mean_bunch_end.dat", w->dir);
-  fprintf(fp, " # bunch statistics end of run, turns = %i; Ib = %g A ;\n", (int) w->rev, w->ib[0]);
-  fprintf(fp, " # bunch_num    CM    bunch_length    energy_dev    energy_spread;\n");
-  for (b = 0; b < w->nb; b++) {
-    const double *s = end_stats + 12 * b;
-    fprintf(fp, " %d     %e    %e    %e    %e\n", w->bucket[b], s[0], s[3], s[6], s[9]);
+  /* mean_bunch_end.dat, written when no scan runs (manager_weakweak.c:302) */
+  if (w->p.scan == 0) {
+    fp = open_in(w, "mean_bunch_end.dat", "w+");
+    if (!fp) return werr(MBT_ERR_IO, "cannot create %s/mean_bunch_end.dat", w->dir);
+    fprintf(fp, " # bunch statistics end of run, turns = %i; Ib = %g A ;\n", (int) w->rev, w->ib[0]);
+    fprintf(fp, " # bunch_num    CM    bunch_length    energy_dev    energy_spread;\n");
+    for (b = 0; b < w->nb; b++) {
+      const double *s = end_stats + 12 * b;
+      fprintf(fp, " %d     %e    %e    %e    %e\n", w->bucket[b], s[0], s[3], s[6], s[9]);
+    }
+    fclose(fp);
   }
-  fclose(fp);
   /* resistive-wall dipole history of the first output bunch */
   if (w->p.rw_long && w->n_out > 0) {
     int i, j;

@@ -80,6 +80,8 @@ struct mbt_ctx {
   bool mlp_set = false;
   double bi_ms = 0.0;            // its average device time in the last mbt_profile_turns
   std::vector<int> watch;        // bunches whose potentials are recorded
+  int scan_steps = 0;            // a scan boundary launches scan_currents / scan_rw
+  double scan_d_ma = 0.0, scan_d_a = 0.0;   // current steps [mA] per bucket, [A] per bunch
   cudaEvent_t ev[6] = {};
   double timing[4] = {0, 0, 0, 0};
   int device = 0;
@@ -196,6 +198,8 @@ int validate(mbt_ctx *c, const mbt_params *p, int nbunch, const int *bucket, con
   if (p->rw_long && (p->Nmlt < 0 || p->beffH[0] <= 0 && p->track_plane[1] || p->beffV[0] <= 0 && p->track_plane[2]))
     return fail(c, MBT_ERR_INVALID, "long-range resistive wall needs Nmlt >= 0 and beffH3/beffV3 > 0");
   if (!p->track_plane[0]) return fail(c, MBT_ERR_INVALID, "the longitudinal plane is always tracked");
+  if (p->scan < 0 || p->scan > 4 || (p->scan != 0 && p->nrev_scan < 1))
+    return fail(c, MBT_ERR_INVALID, "scan type %d outside 0..4 or NrevScan %ld < 1", p->scan, p->nrev_scan);
   return 0;
 }
 
@@ -255,12 +259,24 @@ void enqueue_beam_ion(mbt_ctx *c) {
   mbt::bi_kick<<<c->ntile, mbt::kBiThreads, 0, c->stream>>>(c->a, bi);
 }
 
+// Whether turn `turn` (0-based) ends a scan interval: (rev+1) % NrevScan
+// == 0 (worker_weakweak.c:389).
+bool scan_boundary(const mbt_ctx *c, long turn) {
+  return c->scan_steps && (turn + 1) % c->p.nrev_scan == 0;
+}
+
 // One turn: particle pass, bunch reduction, ring scan, bunch wakes, and
-// the beam-ion stage when it is on.
-void enqueue_turn(mbt_ctx *c, cudaEvent_t *ev) {
+// the beam-ion stage when it is on.  boundary: the turn ends a scan
+// interval (two small launches more).
+void enqueue_turn(mbt_ctx *c, cudaEvent_t *ev, bool boundary = false) {
+  const bool current_scan = boundary && c->p.scan == 1;
   if (ev) cudaEventRecord(ev[0], c->stream);
   launch_map_noise<true>(c, effective_noise(c));
   if (ev) cudaEventRecord(ev[1], c->stream);
+  if (current_scan) {
+    const int n = std::max(c->p.nharm, c->nbunch);
+    mbt::scan_currents<<<(n + 255) / 256, 256, 0, c->stream>>>(c->a, c->scan_d_ma, c->scan_d_a, c->p.T0, c->p.E0);
+  }
   mbt::bunch_reduce<<<c->nbunch, mbt::kBlock, smem_reduce(c), c->stream>>>(c->a, mbt::kReduceTurn, nullptr);
   if (ev) cudaEventRecord(ev[2], c->stream);
   mbt::ring_scan<<<1 + rw_blocks(c), mbt::kBlock, smem_scan(c), c->stream>>>(c->a, 1, 0, c->vbuf);
@@ -270,6 +286,11 @@ void enqueue_turn(mbt_ctx *c, cudaEvent_t *ev) {
   if (c->bi_on) {
     enqueue_beam_ion(c);
     if (ev) cudaEventRecord(c->bi_ev, c->stream);
+  }
+  if (boundary) {
+    const long n = std::max<long>(std::max<long>((long)(c->p.Nmlt + 2) * c->p.nharm, c->p.nharm), c->nbunch);
+    mbt::scan_rw<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->a, current_scan ? 1 : 0, c->scan_d_a,
+                                                                      c->bi_on ? const_cast<double *>(c->bi.ib) : nullptr);
   }
 }
 
@@ -535,6 +556,13 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   rc = rc ? rc : dupload(c, &dp, fac.empty() ? g0.data() : fac.data(), std::max<size_t>(fac.size(), 1)); a.bunch_fac = dp;
   rc = rc ? rc : dupload(c, &dp, factg.data(), nbunch); a.bunch_factg = dp;
   rc = rc ? rc : dupload(c, &dp, ibunch.data(), p->nharm); a.ibunch = dp;
+  // a current scan changes the wake currents one step before the
+  // resistive-wall current (scan_currents / scan_rw); otherwise they are one
+  a.rw_ib = a.ibunch;
+  if (p->scan == 1 && p->rw_long) { rc = rc ? rc : dupload(c, &dp, ibunch.data(), p->nharm); a.rw_ib = dp; }
+  c->scan_steps = p->scan == 1 || (p->scan != 0 && p->rw_long);
+  c->scan_d_ma = p->scan_step / (double)nbunch;             // tracking.c:53
+  c->scan_d_a = p->scan_step / ((double)nbunch * FKILO);    // tracking.c:49
   rc = rc ? rc : dupload(c, &dp, gl(Gl), c->nc); a.Gl = dp;
   rc = rc ? rc : dupload(c, &dp, gl(Gv), c->nc); a.Gv = dp;
   rc = rc ? rc : dupload(c, &dp, gl(Gh), c->nc); a.Gh = dp;
@@ -794,6 +822,8 @@ int mbt_enable_beam_ion(mbt_ctx *c, const mbt_beam_ion *cfg) {
   if (!r) r = dalloc(c, &part, nslot);
   if (!r) r = dalloc(c, &cloud, (size_t)cfg->n_ip * c->nbunch * 5);
   if (!r) r = dupload(c, &ibd, ibv.data(), ibv.size());
+  // the bunch currents as they stand (a current scan may have stepped them)
+  if (!r) CK(cudaMemcpy(ibd, c->a.bunch_ib, (size_t)c->nbunch * sizeof(double), cudaMemcpyDeviceToDevice));
   unsigned long long *aud = nullptr;
   if (!r) r = dalloc(c, &aud, 6);
   if (r) return r;
@@ -945,17 +975,25 @@ static int run_core(mbt_ctx *c, long nturns, double *stats, double *ampinv, bool
   long done = 0;
   CK(cudaEventRecord(c->ev[5], c->stream));
   while (done < nturns) {
-    // a chunk never crosses a wrap of the statistics buffer
+    // a chunk never crosses a wrap of the statistics buffer, and ends at
+    // the next scan boundary
     const long slot = turn % cap;
-    const long chunk = std::min(nturns - done, cap - slot);
+    long chunk = std::min(nturns - done, cap - slot);
+    bool boundary = false;
+    if (c->scan_steps) {
+      const long left = c->p.nrev_scan - turn % c->p.nrev_scan;   // turns up to the boundary, inclusive
+      if (left <= chunk) { chunk = left; boundary = true; }
+    }
+    const long plain = boundary ? chunk - 1 : chunk;
     long t = 0;
-    if (use_graph && chunk >= 8) {
+    if (use_graph && plain >= 8) {
       const int G = 8;
       int r = build_graph(c, G);
       if (r) return r;
-      for (; t + G <= chunk; t += G) CK(cudaGraphLaunch(c->graph, c->stream));
+      for (; t + G <= plain; t += G) CK(cudaGraphLaunch(c->graph, c->stream));
     }
-    for (; t < chunk; ++t) enqueue_turn(c, nullptr);
+    for (; t < plain; ++t) enqueue_turn(c, nullptr);
+    if (boundary) enqueue_turn(c, nullptr, true);
     CK(cudaGetLastError());
     if (stats)
       CK(cudaMemcpyAsync(stats + (size_t)done * c->nbunch * 12, c->a.stats + (size_t)slot * c->nbunch * 12,
@@ -1004,8 +1042,10 @@ int mbt_profile_turns(mbt_ctx *c, long nturns, double out[4]) {
   if (c->bi_on && c->bicfg.surrogate && !c->mlp_set)
     return fail(c, MBT_ERR_STATE, "surrogate beam-ion fields need mbt_beam_ion_use_mlp");
   double acc[4] = {0, 0, 0, 0}, acc_bi = 0.0;
+  RingState rs;
+  CK(cudaMemcpy(&rs, c->a.rs, sizeof rs, cudaMemcpyDeviceToHost));
   for (long t = 0; t < nturns; ++t) {
-    enqueue_turn(c, c->ev);
+    enqueue_turn(c, c->ev, scan_boundary(c, rs.turn + t));
     CK(cudaEventSynchronize(c->bi_on ? c->bi_ev : c->ev[4]));
     for (int k = 0; k < 4; ++k) {
       float ms = 0;

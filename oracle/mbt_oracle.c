@@ -1033,6 +1033,19 @@ long orc_run(orc_ctx *o, long nturns, double *stats, const float *dev_in,
       if (p->n_lr[HOR] > 0 && p->track_plane[HOR]) ring_hist(o, &o->b[ib], HOR);
       if (p->n_lr[VER] > 0 && p->track_plane[VER]) ring_hist(o, &o->b[ib], VER);
     }
+    /* scan step, worker_weakweak.c:388-393 with tracking_scan_step_worker
+       tracking.c:43-57: a current scan adds scan_step / Nbunch to every
+       filled bucket's current and to every bunch's; any scan restarts the
+       resistive-wall trigger count */
+    if (p->scan != 0 && (rev + 1) % p->nrev_scan == 0) {
+      if (p->scan == 1) {
+        int i;
+        for (ib = 0; ib < o->nb; ib++) o->b[ib].Ib += p->scan_step / (((double) o->nb) * FKILO);
+        for (i = 0; i < p->nharm; i++)
+          if (o->filled[i]) o->ibunch[i] += p->scan_step / ((double) o->nb);
+      }
+      for (ib = 0; ib < o->nb; ib++) o->b[ib].m = 0;
+    }
   }
   o->rev += nturns;
   o->dev_in = NULL;

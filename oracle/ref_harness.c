@@ -575,6 +575,8 @@ int refh_fill_params(mbt_params *p)
   for (pl = 0; pl < 3; pl++) p->track_plane[pl] = track.TrackPlane[pl];
   p->quantum = track.EnableQuantum; p->rw_long = track.EnableRW_long; p->Nmlt = track.Nmlt;
   p->triggerRW = track.triggerRW; p->nrev_tot = track.NrevTot; p->nrev_mon = track.NrevMon;
+  p->scan = track.scan; p->nscan = track.Nscan; p->nrev_scan = track.NrevScan;
+  p->scan_start = track.scan_start; p->scan_step = track.scan_step;
   p->np_model = macrop_model.Np;
   for (pl = 0; pl < 3; pl++) {
     p->iseed[pl] = macrop_model.iseed[pl];
@@ -652,6 +654,7 @@ int refh_run_files(double *stats, double *ampinv, double *vrfphi, double *end_st
   int ib, pl;
   long rev, nstat = 0;
   long *nstat_w = (long *) calloc(nbunch, sizeof(long));
+  double *sv_w = (double *) calloc(nbunch, sizeof(double));
   FILE **out_fp = (FILE **) calloc(nbunch, sizeof(FILE *));
   char fn[FILENAME_MAX];
   bunch_CM_history_weak_t cmhist;
@@ -714,6 +717,9 @@ int refh_run_files(double *stats, double *ampinv, double *vrfphi, double *end_st
       vrfphi[((size_t) rev * nbunch + ib) * 2] = W[ib].ring.Vrf0;
       vrfphi[((size_t) rev * nbunch + ib) * 2 + 1] = W[ib].ring.phai0;
     }
+    /* the workers print before their scan step (worker_weakweak.c:296-302
+       then :388-393); refh_run makes the step within the turn */
+    for (ib = 0; ib < nbunch; ib++) sv_w[ib] = W[ib].scan_val;
     refh_run(1, st, NULL, 0);
     /* workers: worker_weakweak.c:290-302 */
     for (ib = 0; ib < nbunch; ib++) {
@@ -721,7 +727,7 @@ int refh_run_files(double *stats, double *ampinv, double *vrfphi, double *end_st
       nstat_w[ib]++;
       if (nstat_w[ib] % mon == 0 || (rev + 1) % track.NrevScan == 0) {
         weak_bunch_update_statistics(&W[ib].bunch.stats, nstat_w[ib]);
-        bunch_stats_fprintf(out_fp[ib], rev, &W[ib].bunch.stats, W[ib].scan_val);
+        bunch_stats_fprintf(out_fp[ib], rev, &W[ib].bunch.stats, sv_w[ib]);
         weak_bunch_reset_statistics(&W[ib].bunch.stats);
         nstat_w[ib] = 0;
       }
@@ -753,23 +759,37 @@ int refh_run_files(double *stats, double *ampinv, double *vrfphi, double *end_st
       weak_bunch_reset_statistics(&allstats);
       nstat = 0;
     }
+    /* manager_weakweak.c:287-288.  tracking_scan_step_manager also adds
+       to bunches[i].Ib for every filled bucket i < Nharm of an array of
+       Nbunch bunches (out of bounds for a partial fill) and the manager
+       prints those currents only without a scan, so only its scan value
+       is kept here. */
+    if ((rev + 1) % track.NrevScan == 0 && rev > 0 && track.scan == 1) {
+      ring.Iring += track.scan_step;
+      scan_val = ring.Iring;
+    }
   }
   free(ampinv_turn);
   ampinv_turn = NULL;
 
-  /* end statistics: worker_weakweak.c:396-404, manager_weakweak.c:307-331 */
-  snprintf(fn, FILENAME_MAX, "%s/mean_bunch_end.dat", track.work_path);
-  FILE *end_fp = fopen(fn, "w+");
-  if (!end_fp) return -1;
-  fprintf(end_fp, " # bunch statistics end of run, turns = %i; Ib = %g A ;\n", (int) tot, W[0].bunch.Ib);
-  fprintf(end_fp, " # bunch_num    CM    bunch_length    energy_dev    energy_spread;\n");
+  /* end statistics: worker_weakweak.c:396-404, manager_weakweak.c:301-331
+     (the file only without a scan; end_stats are filled either way) */
+  FILE *end_fp = NULL;
+  if (track.scan == 0) {
+    snprintf(fn, FILENAME_MAX, "%s/mean_bunch_end.dat", track.work_path);
+    end_fp = fopen(fn, "w+");
+    if (!end_fp) return -1;
+    fprintf(end_fp, " # bunch statistics end of run, turns = %i; Ib = %g A ;\n", (int) tot, W[0].bunch.Ib);
+    fprintf(end_fp, " # bunch_num    CM    bunch_length    energy_dev    energy_spread;\n");
+  }
   for (ib = 0; ib < nbunch; ib++) {
     bunch_stats_t *bs = &W[ib].bunch.stats;
     weak_bunch_calc_statistics(&W[ib].bunch, &track);
     put_stats(&W[ib].bunch, end_stats + 12 * ib);
-    fprintf(end_fp, " %d     %e    %e    %e    %e\n", W[ib].kb, bs->pos.xtau, bs->pos_sigma.xtau, bs->slope.xtau, bs->slope_sigma.xtau);
+    if (end_fp)
+      fprintf(end_fp, " %d     %e    %e    %e    %e\n", W[ib].kb, bs->pos.xtau, bs->pos_sigma.xtau, bs->slope.xtau, bs->slope_sigma.xtau);
   }
-  fclose(end_fp);
+  if (end_fp) fclose(end_fp);
 
   /* output workers, last bunch first so the first one's files remain:
      worker_weakweak.c:407-438 */
@@ -812,6 +832,7 @@ int refh_run_files(double *stats, double *ampinv, double *vrfphi, double *end_st
   bunch_CM_history_weak_destroy(&cmhist);
   free(scan_val_hist);
   free(nstat_w);
+  free(sv_w);
   free(out_fp);
   return 0;
 }

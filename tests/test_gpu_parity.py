@@ -57,6 +57,33 @@ def _oracle_and_tracker(cfg, noise_injected=False):
     return o, t
 
 
+@pytest.mark.parametrize("scan", [
+    {"scan_type": 1, "Nscan": 3, "NrevScan": 25, "scan_start": 120.0, "scan_step": 40.0},
+    {"scan_type": 4, "Nscan": 3, "NrevScan": 25, "scan_start": 0.5},
+])
+def test_scan_steps(tmp_path, scan, cuda_device, libmbt):
+    """Current scan (bucket and bunch currents, factG and the weighting of
+    the resistive-wall history change at each boundary) and Q scan (only the
+    resistive-wall trigger count restarts, here after 25 of its 50 kicks),
+    run in calls whose ends fall inside and on the scan intervals."""
+    from tests.util import add_section, add_tracking_keys
+    path = small_conf(tmp_path, "uniform_fill.conf", Np=300, Nmlt=3, filling="SINGLE20", xxCM_offset=0.05,
+                      EnableQuantum=0, NrevTot=1)
+    add_tracking_keys(path, triggerRW=1)
+    cfg = api.Config(add_section(path, "scan", **scan))
+    assert cfg.params.nrev_tot == 75
+    o, t = _oracle_and_tracker(cfg)
+    so0, st0 = o.prepare(), t.prepare()
+    assert np.max(stats_err(st0, so0)) < STATS_TOL
+    for n in (7, 18, 30, 20):
+        so = o.run(n)
+        st = t.run(n)
+        assert np.max(stats_err(st, so)) < STATS_TOL, n
+        worst = max(np.max(coord_err(t.get_particles(i), o.get_particles(i))) for i in range(cfg.nbunch))
+        assert worst < COORD_TOL, (n, worst)
+    t.close()
+
+
 def test_single_bunch_full_size_2000_turns(tmp_path, cuda_device, libmbt):
     """Single bunch, 1e5 macroparticles, broadband resonator in three planes,
     noise off, 2000 turns: checked after 1, 10 and 2000 turns."""

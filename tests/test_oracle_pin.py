@@ -41,3 +41,24 @@ def test_oracle_is_the_reference(tmp_path, conf, over, turns):
         assert np.array_equal(R.get_particles(i), O.get_particles(i))
         assert np.array_equal(R.ampinv(i), O.ampinv(i))
     assert np.array_equal(R.state(0)[0], O.state(0)[0])
+
+
+@pytest.mark.parametrize("scan", [
+    {"scan_type": 1, "Nscan": 3, "NrevScan": 4, "scan_start": 120.0, "scan_step": 40.0},
+    {"scan_type": 3, "Nscan": 2, "NrevScan": 30},
+])
+def test_oracle_is_the_reference_through_scan_steps(tmp_path, scan):
+    """Current and Q-factor scans (tracking_scan_step_worker tracking.c:43-57,
+    worker_weakweak.c:388-393) with long-range resistive wall, its 50-kick
+    trigger (restarted at every boundary) and a longitudinal resonator:
+    bit-identical across the scan boundaries."""
+    from tests.util import add_section, add_tracking_keys
+    path = small_conf(tmp_path, "uniform_fill.conf", Np=40, Nmlt=2, filling="SINGLE10", xxCM_offset=0.05,
+                      NrevTot=1)
+    add_tracking_keys(path, triggerRW=1)
+    R, O = _pair(add_section(path, "scan", **scan))
+    turns = scan["Nscan"] * scan["NrevScan"]
+    assert np.array_equal(R.run(turns), O.run(turns))
+    for i in range(R.nb):
+        assert np.array_equal(R.get_particles(i), O.get_particles(i))
+    assert np.array_equal(R.state(0)[0], O.state(0)[0])

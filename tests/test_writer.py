@@ -143,9 +143,10 @@ def test_config_output_lists(tmp_path):
               "TWOTHIRD": [0, 138, 276], "THREEFOURTH": [0, 156, 311], "EVENHALF": [0]}
     for fill, buckets in expect.items():
         conf = small_conf(tmp_path, "single_bunch.conf", filling=fill)
-        o, bout = api.Config(conf).output()
+        C = api.Config(conf)
+        o, bout = C.output()
         assert list(bout) == buckets, fill
-        assert o.nrev_scan == 2001
+        assert C.params.scan == 0 and C.params.nrev_scan == C.params.nrev_tot + 1
         assert o.ampinv_out == 0 and o.nrev_potentials_out == 0
         assert o.jobtitle == b"single"
     conf = small_conf(tmp_path, "uneven_fill.conf")

@@ -37,8 +37,22 @@ def add_tracking_keys(path, **keys):
     return path
 
 
-# Output-file cases: (conf, overrides, [tracking] additions).  The
-# distribution files are named relative to the working directory.
+def add_section(path, name, **keys):
+    """Append a `[name]` section with `key = value` lines."""
+    with open(path, "a") as f:
+        f.write("\n[%s]\n" % name + "".join("  %s = %s\n" % (k, v) for k, v in keys.items()))
+    return path
+
+
+_TRAIN = {"Np": 100, "Nmlt": 2, "filling": "SINGLE10", "EnableQuantum": 0, "xxCM_offset": 0.05,
+          "gendst_datafile_LON": "dist_LON.dat", "gendst_datafile_HOR": "dist_HOR.dat",
+          "gendst_datafile_VER": "dist_VER.dat"}
+
+# Output-file cases: (conf, overrides, [tracking] additions[, added
+# sections]).  The distribution files are named relative to the working
+# directory.  The scan cases put the statistics lines of NrevMon and of the
+# scan boundaries out of step, as the reference's scan value history then
+# is.
 WRITER_CASES = {
     "single": ("single_bunch.conf",
                {"Np": 200, "NrevTot": 40, "NrevMon": 20, "xxCM_offset": 0.05, "zzCM_offset": 0.02,
@@ -51,13 +65,23 @@ WRITER_CASES = {
                   "gendst_datafile_LON": "dist_LON.dat", "gendst_datafile_HOR": "dist_HOR.dat",
                   "gendst_datafile_VER": "dist_VER.dat"},
                  {"EnableAmpinv_out": 1, "NrevPotentialsOut": 15}),
+    "scan_current": ("uniform_fill.conf", dict(_TRAIN, NrevTot=1, NrevMon=6),
+                     {"EnableAmpinv_out": 1, "NrevPotentialsOut": 3},
+                     {"scan": {"scan_type": 1, "Nscan": 3, "NrevScan": 8, "scan_start": 150.0,
+                               "scan_step": 30.0}}),
+    "scan_q": ("uniform_fill.conf", dict(_TRAIN, NrevTot=1, NrevMon=4),
+               {"EnableAmpinv_out": 1, "NrevPotentialsOut": 2},
+               {"scan": {"scan_type": 3, "Nscan": 2, "NrevScan": 6}}),
 }
 
 
 def writer_conf(tmp_path, case):
-    name, over, add = WRITER_CASES[case]
-    path = small_conf(tmp_path, name, **over)
-    return add_tracking_keys(path, **add)
+    name, over, add = WRITER_CASES[case][:3]
+    path = small_conf(tmp_path, name, **dict(over))
+    add_tracking_keys(path, **add)
+    for sec, keys in (WRITER_CASES[case][3] if len(WRITER_CASES[case]) > 3 else {}).items():
+        add_section(path, sec, **keys)
+    return path
 
 
 def coord_err(a, b):

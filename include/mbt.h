@@ -158,19 +158,29 @@ typedef struct mbt_ctx mbt_ctx;
  * reads beffH3/beffV3 for long-range resistive wall even without
  * EnableRW_short (the reference leaves them 0, input.c:465-478).
  * Returns MBT_ERR_CONFIG (message in mbt_config_error()) for a missing or
- * malformed key, and for what this library does not run: short-range
- * resistive wall, BunchModel = STRONG, modeHT excitation and distribution
- * files. */
+ * malformed key, for a set-up the reference reports as failing (a
+ * short-range resistive wall on bins narrower than 20 s0, a Q scan without
+ * a longitudinal resonator) and for what this library does not run:
+ * BunchModel = STRONG, modeHT excitation and distribution files. */
 int mbt_config_load(const char *conf_path, int fix_rw_beff, mbt_params *p,
                     int *nbunch, int *bucket, double *ib_frac);
 
 /* Short-range Green's functions for ncell bins from the [resonator_N] and
- * [wake_file_N] sections (construct_greensfunc_resonator
- * transform_weak.c:288-403, construct_greensfunc_file :405-471), plus the
- * resulting planeL/planeV/planeH counts written back into *p.
+ * [wake_file_N] sections and the short-range resistive wall
+ * (construct_greensfunc_resonator transform_weak.c:288-403,
+ * construct_greensfunc_file :405-471, construct_greensfunc_RW :473-547),
+ * plus the resulting planeL/planeV/planeH counts written back into *p.
  * Gl, Gv, Gh: arrays of p->ncell doubles (zeroed by the call). */
 int mbt_config_greens(const char *conf_path, mbt_params *p,
                       double *Gl, double *Gv, double *Gh);
+
+/* First-bin values of the short-range resistive wall for a bin of u s0
+ * (replaces RW_table_LON / RW_table_TRANS, rw_table.c:310-391): the bin
+ * averages of the Bane-Sands longitudinal wake and of its integral (the
+ * transverse wake), dimensionless; computed by quadrature, not
+ * interpolated.  u above 2000 takes the values at 2000 as the reference's
+ * table does.  Either output may be NULL.  Returns 0, or -1 for u < 19.8. */
+int mbt_rw_first_bin(double u, double *lon, double *trans);
 
 /* Bunch current [A] of filled bunch i (manager_weakweak.c:74-75). */
 double mbt_bunch_current(const mbt_params *p, int nbunch, double ib_frac);

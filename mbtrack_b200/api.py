@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-from .abi import (MBT_NOISE_INJECTED, MBT_NOISE_PHILOX, MBT_WRITER_OWN_AMPINV, MbtBeamIon, MbtOutputCfg,
+from .abi import (MBT_ERR_INVALID, MBT_NOISE_INJECTED, MBT_NOISE_PHILOX, MBT_WRITER_OWN_AMPINV, MbtBeamIon, MbtOutputCfg,
                   MbtParams, MbtState)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -28,6 +28,7 @@ SIGNATURES = {
     "mbt_config_greens": (ctypes.c_int, [ctypes.c_char_p, _P(MbtParams), _vp, _vp, _vp]),
     "mbt_config_error": (ctypes.c_char_p, []),
     "mbt_bunch_current": (ctypes.c_double, [_P(MbtParams), ctypes.c_int, ctypes.c_double]),
+    "mbt_rw_first_bin": (ctypes.c_int, [ctypes.c_double, _P(ctypes.c_double), _P(ctypes.c_double)]),
     "mbt_create": (ctypes.c_int, [_P(MbtParams), ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp,
                                   ctypes.c_int, ctypes.c_uint64, _P(_vp)]),
     "mbt_destroy": (ctypes.c_int, [_vp]),
@@ -426,6 +427,15 @@ class Tracker:
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _check(lib().mbt_geometry(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), self.h)
         return a.value, b.value, c.value
+
+
+def rw_first_bin(u):
+    """(longitudinal, transverse) first-bin values of the short-range
+    resistive wall for a bin of u s0 (mbt_rw_first_bin)."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    if lib().mbt_rw_first_bin(float(u), ctypes.byref(a), ctypes.byref(b)) != 0:
+        raise MbtError(MBT_ERR_INVALID, "bin of %g s0 is narrower than 19.8 s0" % u)
+    return a.value, b.value
 
 
 def wofz_dev(x_ptr, y_ptr, re_ptr, im_ptr, n, flag_ptr=None, stream=None):

@@ -19,8 +19,12 @@
  *     input.c:465-478, and then divides by zero in transform_weak.c:811);
  *   - long keys are parsed as longs (the reference scans "%d" into a long,
  *     input.c:1077, which only works for non-negative values);
- *   - short-range resistive wall, the legacy .inp format and the
- *     excitation mode (modeHT) are rejected with MBT_ERR_CONFIG.
+ *   - the legacy .inp format and the excitation mode (modeHT) are
+ *     rejected with MBT_ERR_CONFIG;
+ *   - the first-bin values of the short-range resistive wall are the
+ *     bin averages of the Bane-Sands wakes computed by quadrature
+ *     (mbt_rw_first_bin), where the reference interpolates a printed
+ *     table (rw_table.c); a bin narrower than 20 s0 is an error.
  */
 #include <math.h>
 #include <stdarg.h>
@@ -41,6 +45,7 @@
 #define FMEGA  1.0e+06
 #define FGIGA  1.0e+09
 #define C_LIGHT 2.997925e+08
+#define Z_0     376.73
 #define LINE_MAX_MBT 256
 
 /* ------------------------------------------------------------ scanner */
@@ -503,7 +508,6 @@ static int read_conf(const char *path, int fix_rw_beff, cfg_t *g)
       p->nrev_tot = p->nscan * p->nrev_scan;
     }
   }
-  if (g->enable_rw_short || g->enable_rw_short_lon) { r = cfg_fail("short-range resistive wall is not supported yet"); goto out; }
   /* the reference takes any integer type (and steps only type 1) and
      divides by NrevScan every turn */
   if (p->scan < 0 || p->scan > 4) { r = cfg_fail("[scan] scan_type %d is not 0..4", p->scan); goto out; }
@@ -665,6 +669,14 @@ static int setup_tracking(cfg_t *g)
   b = p->beffL[1];
   if (p->beffH[1] > b && p->track_plane[1] == 1) b = p->beffH[1];
   else if (p->beffV[1] > b && p->track_plane[2] == 1) b = p->beffV[1];
+  if (g->enable_rw_short || g->enable_rw_short_lon) {
+    /* input.c:1744-1756: the short-range wake needs bins of >= 20 s0 */
+    const double s0 = pow((2 * b * b * p->rhorw / Z_0), 1.0 / 3.0);
+    const double dT = 2.0 * p->nsigma / ((double) p->ncell - 1);
+    const double mult = dT * p->pos_sgm[0] * C_LIGHT / s0;
+    if (mult < 20.)
+      return cfg_fail("Selffield Model has too small binwidth for RW treatment (bin = %.3g s0, needs 20)", mult);
+  }
   if (p->rw_long && p->Nmlt == 0) {
     double tmp = p->Lc * sqrt(p->rhorw) / pow(b, 3);
     p->Nmlt = 1 + ((int) 500e3 / tmp);
@@ -883,6 +895,185 @@ static int greens_file(const char *fname, int plane, mbt_params *p, double *Gl, 
   return 0;
 }
 
+/* ---------------------------------------- short-range resistive wall */
+
+/* Gauss-Legendre nodes and weights on [-1, 1] (Newton iteration on the
+ * Legendre recurrence (j+1) P_{j+1} = (2j+1) x P_j - j P_{j-1}). */
+static void gl_rule(int n, double *x, double *w)
+{
+  int i, j;
+  for (i = 0; i < (n + 1) / 2; i++) {
+    double z = cos(M_PI * (i + 0.75) / (n + 0.5)), dz = 1.0, p1 = 1.0, p2 = 0.0, dp = 1.0;
+    int it;
+    for (it = 0; it < 100 && fabs(dz) > 1e-16; it++) {
+      p1 = 1.0;
+      p2 = 0.0;
+      for (j = 1; j <= n; j++) {
+        const double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      dp = n * (z * p1 - p2) / (z * z - 1.0);
+      dz = p1 / dp;
+      z -= dz;
+    }
+    x[i] = -z;
+    x[n - 1 - i] = z;
+    w[i] = w[n - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+
+typedef double (*integrand_t)(double t, double u);
+
+static double gl_panel(integrand_t f, double u, double a, double b, int n, const double *x, const double *w)
+{
+  const double c = 0.5 * (a + b), h = 0.5 * (b - a);
+  double s = 0.0;
+  int i;
+  for (i = 0; i < n; i++) s += w[i] * f(c + h * x[i], u);
+  return s * h;
+}
+
+/* Adaptive Gauss-Legendre: a panel is accepted when the 12- and 24-point
+ * rules agree to tol (absolute, the same for every panel), else halved;
+ * at most 2^20 panels per call. */
+static double integrate(integrand_t f, double u, double a, double b, double tol, int depth)
+{
+  static double x12[12], w12[12], x24[24], w24[24];
+  static int ready = 0;
+  double i12, i24;
+  if (!ready) {
+    gl_rule(12, x12, w12);
+    gl_rule(24, x24, w24);
+    ready = 1;
+  }
+  i12 = gl_panel(f, u, a, b, 12, x12, w12);
+  i24 = gl_panel(f, u, a, b, 24, x24, w24);
+  if (fabs(i24 - i12) <= tol || depth >= 20) return i24;
+  return integrate(f, u, a, 0.5 * (a + b), tol, depth + 1) + integrate(f, u, 0.5 * (a + b), b, tol, depth + 1);
+}
+
+/* exp(-t^2 u) / (t^6 + 8) */
+static double rw_k(double t, double u) { return exp(-t * t * u) / (pow(t, 6) + 8.0); }
+
+/* (1 - exp(-t^2 u)) / (t^2 (t^6 + 8)); u / 8 at t = 0 */
+static double rw_j(double t, double u)
+{
+  const double y = t * t * u;
+  const double q = y < 1e-8 ? u * (1.0 - 0.5 * y) : -expm1(-y) / (t * t);
+  return q / (pow(t, 6) + 8.0);
+}
+
+/* the same after t = 1/s, for t in [1, inf): s^6 (1 - exp(-u/s^2)) / (1 + 8 s^6) */
+static double rw_j_tail(double s, double u)
+{
+  if (s <= 0.0) return 0.0;
+  return pow(s, 6) * -expm1(-u / (s * s)) / (1.0 + 8.0 * pow(s, 6));
+}
+
+/* Bin averages over [0, u s0] of the Bane-Sands short-range resistive-wall
+ * wakes of a round pipe (K. Bane and M. Sands, "The short-range resistive
+ * wall wakefields", SLAC-PUB-95-7074), in units of s0 = (2 b^2 rho /
+ * Z0)^(1/3):
+ *   w(x)  = e^-x cos(sqrt3 x) / 3 - sqrt2/pi int_0^inf t^2 e^(-t^2 x) / (t^6+8) dt
+ *           (longitudinal, times 4 Z0 c / (pi b^2)),
+ *   W(x)  = int_0^x w      (transverse, times 8 Z0 c s0 / (pi b^4)),
+ *   lon   = (1/u) int_0^u w = [e^-u (sqrt3 sin - cos)(sqrt3 u) / 12
+ *                              + sqrt2/pi int e^(-t^2 u) / (t^6+8) dt] / u,
+ *   trans = (1/u) int_0^u W = [(sqrt3 Fs - Fc) / 12
+ *                              + sqrt2/pi int (1 - e^(-t^2 u)) / (t^2 (t^6+8)) dt] / u,
+ * with Fc, Fs = int_0^u e^-x cos, sin(sqrt3 x) dx; the terms growing like u
+ * cancel analytically (int_0^inf dt / (t^6+8) = pi / (12 sqrt2)).  These
+ * are the quantities the reference tabulates for u in [19.8, 2000]
+ * (RW_table_LON / RW_table_TRANS, rw_table.c:310-391); like it, u above
+ * 2000 takes the values at 2000.  Returns 0, or -1 for u < 19.8 (where the
+ * reference's table has no entry). */
+int mbt_rw_first_bin(double u, double *lon, double *trans)
+{
+  const double k = sqrt(3.0), c2 = sqrt(2.0) / M_PI;
+  double e, cs, sn, Fc, Fs, K = 0.0, J = 0.0, a, tk;
+  if (!(u >= 19.8)) return -1;
+  if (u > 2000.) u = 2000.;
+  e = exp(-u);
+  cs = cos(k * u);
+  sn = sin(k * u);
+  Fc = 0.25 + e * (-cs + k * sn) / 4.0;
+  Fs = k / 4.0 + e * (-k * cs - sn) / 4.0;
+  /* panels at the Gaussian's scale 1/sqrt(u), then to where it vanishes;
+     tolerances 1e-16 of each integral's size (K ~ sqrt(pi/u)/16, J ~
+     sqrt(pi u)/8 + 0.1) */
+  a = 0.0;
+  for (tk = 0.25 / sqrt(u); a < sqrt(800.0 / u); tk *= 2.0) {
+    K += integrate(rw_k, u, a, tk, 1e-16 * sqrt(M_PI / u) / 16.0, 0);
+    a = tk;
+  }
+  a = 0.0;
+  for (tk = 0.25 / sqrt(u); a < 1.0; tk *= 2.0) {
+    const double b = tk < 1.0 ? tk : 1.0;
+    J += integrate(rw_j, u, a, b, 1e-16 * sqrt(M_PI * u) / 8.0, 0);
+    a = b;
+  }
+  J += integrate(rw_j_tail, u, 0.0, 1.0, 1e-16 * sqrt(M_PI * u) / 8.0, 0);
+  if (lon) *lon = (e * (k * sn - cs) / 12.0 + c2 * K) / u;
+  if (trans) *trans = ((k * Fs - Fc) / 12.0 + c2 * J) / u;
+  return 0;
+}
+
+/* construct_greensfunc_RW, transform_weak.c:473-547: the long-time
+ * asymptotes 1/t^(3/2) (LON) and 1/t^(1/2) (transverse) from bin 1 on, the
+ * bin average of the full wake in bin 0.  The reference adds the
+ * longitudinal part when EnableRW_short_LON is set and the transverse ones
+ * only with EnableRW_short. */
+static int greens_rw(const cfg_t *g, mbt_params *p, double *Gl, double *Gv, double *Gh)
+{
+  const int ncellmax = p->ncell;
+  const double sgmatau = p->sigma_tau, dTau = p->dT;
+  const double beffL1 = p->beffL[0], beffL2 = pow(p->beffL[1], 2);
+  const double beffV3 = pow(p->beffV[0], 3), beffH3 = pow(p->beffH[0], 3);
+  const double beffV4 = pow(p->beffV[1], 4), beffH4 = pow(p->beffH[1], 4);
+  const double sigmarw = 1.0 / p->rhorw, t_const = sgmatau * dTau;
+  double s0, rw0, rwt;
+  int nc;
+  if (p->track_plane[0] && g->enable_rw_short_lon) {
+    const double ARW = sqrt(Z_0 / (sigmarw * C_LIGHT * M_PI)) / (4 * beffL1 * M_PI) * p->Lc;
+    for (nc = 1; nc < ncellmax; nc++) {
+      const double tRW = (nc + 0.5) * t_const;
+      Gl[nc] -= ARW / (tRW * sqrt(tRW));
+    }
+    s0 = pow((2 * beffL2 * p->rhorw / Z_0), 1.0 / 3.0);
+    if (mbt_rw_first_bin(sgmatau * dTau * C_LIGHT / s0, &rw0, NULL) < 0)
+      return cfg_fail("short-range RW: longitudinal bin narrower than 19.8 s0");
+    Gl[0] += rw0 * 4 * Z_0 * C_LIGHT / (M_PI * beffL2) * p->Lc;
+    p->planeL++;
+    if (!g->enable_rw_short) return 0;
+  }
+  if (p->track_plane[2]) {
+    const double ARW = sqrt(Z_0 * C_LIGHT / sigmarw / M_PI) / (M_PI * beffV3) * p->Lc;
+    s0 = pow((2 * p->beffV[1] * p->beffV[1] * p->rhorw / Z_0), 1.0 / 3.0);
+    if (mbt_rw_first_bin(sgmatau * dTau * C_LIGHT / s0, NULL, &rwt) < 0)
+      return cfg_fail("short-range RW: vertical bin narrower than 19.8 s0");
+    Gv[0] += rwt * 8 * Z_0 * C_LIGHT / (M_PI * beffV4) * s0 * p->Lc;
+    for (nc = 1; nc < ncellmax; nc++) {
+      const double tRW = (nc + 0.5) * t_const;
+      Gv[nc] += ARW / sqrt(tRW);
+    }
+    p->planeV++;
+  }
+  if (p->track_plane[1]) {
+    const double ARW = sqrt(Z_0 * C_LIGHT / sigmarw / M_PI) / (M_PI * beffH3) * p->Lc;
+    s0 = pow((2 * p->beffH[1] * p->beffH[1] * p->rhorw / Z_0), 1.0 / 3.0);
+    if (mbt_rw_first_bin(sgmatau * dTau * C_LIGHT / s0, NULL, &rwt) < 0)
+      return cfg_fail("short-range RW: horizontal bin narrower than 19.8 s0");
+    Gh[0] += rwt * 8 * Z_0 * C_LIGHT / (M_PI * beffH4) * s0 * p->Lc;
+    for (nc = 1; nc < ncellmax; nc++) {
+      const double tRW = (nc + 0.5) * t_const;
+      Gh[nc] += ARW / sqrt(tRW);
+    }
+    p->planeH++;
+  }
+  return 0;
+}
+
 int mbt_config_greens(const char *conf_path, mbt_params *p, double *Gl, double *Gv, double *Gh)
 {
   cfg_t *g;
@@ -934,6 +1125,8 @@ int mbt_config_greens(const char *conf_path, mbt_params *p, double *Gl, double *
     }
   }
   for (j = 0; j < g->nwake && nc > 0 && !r; j++) r = greens_file(g->wake_file[j], g->wake_plane[j], p, Gl, Gv, Gh);
+  /* worker_weakweak.c:93-94 */
+  if (!r && nc > 0 && (g->enable_rw_short || g->enable_rw_short_lon)) r = greens_rw(g, p, Gl, Gv, Gh);
   free(g);
   return r;
 }

@@ -128,3 +128,95 @@ def test_scan_rejects_bad_sections(tmp_path, libmbt):
     p = add_section(small_conf(d, "single_bunch.conf", NrevTot=1), "scan", scan_type=3, Nscan=2, NrevScan=3)
     with pytest.raises(api.MbtError):
         api.Config(p)
+
+
+def _rw_first_bin(u):
+    try:
+        return (0,) + api.rw_first_bin(u)
+    except api.MbtError:
+        return (-1, 0.0, 0.0)
+
+
+def test_rw_first_bin_against_reference_table(libmbt):
+    """The reference interpolates a printed table (rw_table.c); its
+    longitudinal entries carry a constant error of 4.6e-4 in the integral of
+    the wake over the bin (the exact integral of the resistive-wall wake
+    over all s is zero), so |ours - table| u stays below 4.7e-4; the
+    transverse entries agree to 1.5e-4 relative.  Values from the
+    reference's own functions (tests/golden/make_rw_golden.py)."""
+    import os
+    from tests.util import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "rw_first_bin.npz"))
+    for u, lon_ref, trans_ref in zip(z["u"], z["lon"], z["trans"]):
+        r, lon, trans = _rw_first_bin(u)
+        assert r == 0
+        assert abs(lon - lon_ref) * min(u, 2000.0) < 4.7e-4, u
+        assert abs(trans / trans_ref - 1) < 1.5e-4, u
+    assert _rw_first_bin(19.7)[0] == -1
+    assert _rw_first_bin(2500.0)[1:] == _rw_first_bin(2000.0)[1:]
+
+
+def test_rw_first_bin_is_the_bane_sands_bin_average(libmbt):
+    """Independent check of the quadrature: the bin average of the
+    Bane-Sands wake w(x) = e^-x cos(sqrt3 x)/3 - sqrt2/pi int t^2 e^(-t^2 x)
+    / (t^6+8) dt, and of its running integral, by nested scipy quadrature
+    of that definition."""
+    from scipy.integrate import quad
+
+    def w(x):
+        inner = quad(lambda t: t * t * np.exp(-t * t * x) / (t ** 6 + 8), 0, np.inf, epsabs=1e-15, limit=200)[0]
+        return np.exp(-x) * np.cos(np.sqrt(3) * x) / 3 - np.sqrt(2) / np.pi * inner
+
+    for u in (25.0, 140.0):
+        pts = [0, 0.5, 2, 6, 15, u]
+        lon = sum(quad(w, a, b, epsabs=1e-14, limit=200)[0] for a, b in zip(pts[:-1], pts[1:])) / u
+        # int_0^u W = int_0^u (u - x) w(x) dx
+        trans = sum(quad(lambda x: (u - x) * w(x), a, b, epsabs=1e-13, limit=200)[0]
+                    for a, b in zip(pts[:-1], pts[1:])) / u
+        r, l2, t2 = _rw_first_bin(u)
+        assert abs(l2 - lon) < 1e-9 * abs(lon) + 1e-13, (u, l2, lon)
+        assert abs(t2 / trans - 1) < 1e-9, (u, t2, trans)
+
+
+def test_rw_short_greens_match_reference(tmp_path, libmbt):
+    """construct_greensfunc_RW (transform_weak.c:473-547) on top of the
+    resonators: every bin from 1 on bit-identical to the reference's, bin 0
+    apart by exactly the first-bin value difference times its factor."""
+    from oracle.binding import Reference, build_reference, reference_available
+    from tests.util import rw_short_conf
+    if not reference_available() or build_reference() is None:
+        pytest.skip("reference tree not present")
+    conf = rw_short_conf(tmp_path)
+    cfg = api.Config(conf)
+    R = Reference(conf, workdir=str(tmp_path))
+    R.prepare()
+    Gl, Gv, Gh, _ = R.greens()
+    p = cfg.params
+    n = p.ncell
+    assert (p.planeL, p.planeV, p.planeH) == (2, 2, 2)
+    for ours, ref in ((cfg.Gl, Gl), (cfg.Gv, Gv), (cfg.Gh, Gh)):
+        assert np.array_equal(ours[1:n], ref[1:n])
+    import ctypes
+    from oracle import binding
+    tab = ctypes.CDLL(binding.REF_SO)
+    Z0, c = 376.73, 2.997925e8
+    binw = p.sigma_tau * p.dT * c
+    for G, Gr, b, kind in ((cfg.Gl, Gl, p.beffL[1], 0), (cfg.Gv, Gv, p.beffV[1], 1), (cfg.Gh, Gh, p.beffH[1], 1)):
+        s0 = (2 * b * b * p.rhorw / Z0) ** (1 / 3)
+        u = binw / s0
+        v = ctypes.c_double()
+        f = tab.RW_table_LON if kind == 0 else tab.RW_table_TRANS
+        f.argtypes = [ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+        f(u, v)
+        ours = _rw_first_bin(u)[1 + kind]
+        fac = 4 * Z0 * c / (np.pi * b * b) * p.Lc if kind == 0 else 8 * Z0 * c / (np.pi * b ** 4) * s0 * p.Lc
+        assert abs((G[0] - Gr[0]) - (ours - v.value) * fac) <= 1e-9 * abs(Gr[0]), kind
+
+
+def test_rw_short_needs_wide_bins(tmp_path, libmbt):
+    """input.c:1744-1756: bins narrower than 20 s0 are refused (the
+    reference prints the error and runs on with a half-built set-up)."""
+    from tests.util import rw_short_conf
+    with pytest.raises(api.MbtError) as e:
+        api.Config(rw_short_conf(tmp_path, Nsigma=0.5))
+    assert "binwidth" in str(e.value)

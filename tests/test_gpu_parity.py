@@ -84,6 +84,21 @@ def test_scan_steps(tmp_path, scan, cuda_device, libmbt):
     t.close()
 
 
+def test_short_range_rw(tmp_path, cuda_device, libmbt):
+    """Short-range resistive wall in three planes (its Green's functions
+    from mbt_config_greens) with the broadband resonators, 300 turns."""
+    from tests.util import rw_short_conf
+    cfg = api.Config(rw_short_conf(tmp_path, Np=20000, xxCM_offset=0.05, zzCM_offset=0.02))
+    assert (cfg.params.planeL, cfg.params.planeV, cfg.params.planeH) == (2, 2, 2)
+    o, t = _oracle_and_tracker(cfg)
+    so0, st0 = o.prepare(), t.prepare()
+    assert np.max(stats_err(st0, so0)) < STATS_TOL
+    so, st = o.run(300), t.run(300)
+    assert np.max(stats_err(st, so)) < STATS_TOL
+    assert np.max(coord_err(t.get_particles(0), o.get_particles(0))) < COORD_TOL
+    t.close()
+
+
 def test_single_bunch_full_size_2000_turns(tmp_path, cuda_device, libmbt):
     """Single bunch, 1e5 macroparticles, broadband resonator in three planes,
     noise off, 2000 turns: checked after 1, 10 and 2000 turns."""

@@ -62,3 +62,12 @@ def test_oracle_is_the_reference_through_scan_steps(tmp_path, scan):
     for i in range(R.nb):
         assert np.array_equal(R.get_particles(i), O.get_particles(i))
     assert np.array_equal(R.state(0)[0], O.state(0)[0])
+
+
+def test_oracle_is_the_reference_with_short_range_rw(tmp_path):
+    """Short-range resistive wall in three planes on top of the broadband
+    resonators (the reference's Green's functions given to the oracle)."""
+    from tests.util import rw_short_conf
+    R, O = _pair(rw_short_conf(tmp_path, Np=500, xxCM_offset=0.05, zzCM_offset=0.02))
+    assert np.array_equal(R.run(20), O.run(20))
+    assert np.array_equal(R.get_particles(0), O.get_particles(0))

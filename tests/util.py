@@ -26,15 +26,28 @@ def small_conf(tmp_path, name, **overrides):
     return conf_with(src, dst, **overrides)
 
 
-def add_tracking_keys(path, **keys):
-    """Insert `key = value` lines at the top of the [tracking] section (for
-    optional keys the fixture files do not carry)."""
+def add_keys(path, section, **keys):
+    """Insert `key = value` lines at the top of a section (for optional keys
+    the fixture files do not carry)."""
     text = open(path).read()
     lines = "".join("\n  %s = %s" % (k, v) for k, v in keys.items())
-    text = text.replace("[tracking]", "[tracking]" + lines, 1)
+    text = text.replace("[%s]" % section, "[%s]" % section + lines, 1)
     with open(path, "w") as f:
         f.write(text)
     return path
+
+
+def add_tracking_keys(path, **keys):
+    return add_keys(path, "tracking", **keys)
+
+
+def rw_short_conf(tmp_path, **over):
+    """The single-bunch configuration with the short-range resistive wall
+    in three planes on 64 bins of 0.16 sigma (sigma_tau = 50 ps): bins of
+    about 100 s0 for an 11 mm copper chamber."""
+    path = small_conf(tmp_path, "single_bunch.conf", EnableRW_short=1, Ncell=64, sgm_xtau=0.05, **over)
+    return add_keys(path, "ring", rhorw=1.678e-8, beffL1=0.011, beffL2=0.011, beffH3=0.012, beffH4=0.012,
+                    beffV3=0.009, beffV4=0.009)
 
 
 def add_section(path, name, **keys):

@@ -455,7 +455,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-turns", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--mlp-steps", type=int, default=12000, help="training steps of the learned field")
+    ap.add_argument("--mlp-steps", type=int, default=48000, help="training steps of the learned field")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 20 if args.workload.startswith("beam_ion") else 200

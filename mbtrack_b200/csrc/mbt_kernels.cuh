@@ -153,9 +153,15 @@ __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst
 // warps advance one particle per thread per chunk in place, then sum the
 // moments column-wise from the staged chunk; they synchronise only among
 // themselves (hardware barrier 1).
-constexpr int kPPT = 1;                    // particles per compute thread per chunk
+#ifndef MBT_MAP_PPT
+#define MBT_MAP_PPT 1
+#endif
+#ifndef MBT_MAP_STAGES
+#define MBT_MAP_STAGES 3
+#endif
+constexpr int kPPT = MBT_MAP_PPT;          // particles per compute thread per chunk
 constexpr int kChunk = kPPT * kBlock;
-constexpr int kStages = 3;
+constexpr int kStages = MBT_MAP_STAGES;
 constexpr int kMapThreads = kBlock + 32;   // 8 compute warps + 1 producer warp
 constexpr long kWaitLimit = 1L << 24;      // polls before a wait is declared failed
 
@@ -165,8 +171,14 @@ __host__ __device__ constexpr size_t turn_map_smem(int nc) {
          (size_t)nc * sizeof(int);
 }
 
+// Resident CTAs per SM the register allocation is sized for (shared memory
+// allows 4 at 256 bins).
+#ifndef MBT_MAP_MIN_BLOCKS
+#define MBT_MAP_MIN_BLOCKS 3
+#endif
+
 template <bool MOVE, int NOISE, bool HISTXZ>
-__global__ void __launch_bounds__(kMapThreads, 3) turn_map(Args a) {
+__global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args a) {
   extern __shared__ __align__(128) double smem[];
   const int nc = a.ncell;
   const Tile tile = a.tiles[blockIdx.x];

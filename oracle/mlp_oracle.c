@@ -38,14 +38,14 @@ static float bf16r(float v)
  * libm's tanhf. */
 static float gelu(float x)
 {
-  const float y = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+  const float y = x * fmaf(0.035677408136300125f, x * x, 0.7978845608028654f);
   const float hx = 0.5f * x;
   return fmaf(hx, tanhf(y), hx);
 }
 
 static float gelu_grad(float x)
 {
-  const float y = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+  const float y = x * fmaf(0.035677408136300125f, x * x, 0.7978845608028654f);
   const float th = tanhf(y);
   return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * 0.7978845608028654f * (1.0f + 0.134145f * x * x);
 }
@@ -62,7 +62,7 @@ static void forward_one(const float *P, const float *abr, fwd_t *f)
   int j, k;
   f->x[0] = 0.25f * abr[0] - 1.0f;
   f->x[1] = 0.25f * abr[1] - 1.0f;
-  f->x[2] = 2.0f * abr[2] - 1.0f;
+  f->x[2] = fmaf(0.66761703f, logf(abr[2]), 1.0f);   /* 1 + 2 ln r / ln 20 */
   for (j = 0; j < H; j++) {
     float z = P[B1 + j];
     z = fmaf(P[W1 + 3 * j], f->x[0], z);

@@ -1,13 +1,15 @@
 // mbt_mlp.cu -- training and inference of the learned Bassetti-Erskine
 // field (mbt_mlp.cuh) with the project's own kernels.
 //
-//   mlp_prepare   FP32 master weights -> BF16 operand tiles (W2, W3 and
-//                 their transposes) in the swizzled K-major layout
-//   mlp_forward   128-point tiles, two tile groups per CTA (256 threads):
-//                 layer 1 and layer 4 on the FP32 pipes, layers 2 and 3 as
-//                 16 tcgen05.mma each (BF16 hi + lo activations, FP32
-//                 accumulation in tensor memory); optionally keeps z and h
-//                 of every point for the backward pass
+//   mlp_prepare   FP32 master weights -> operand tiles in the swizzled
+//                 K-major layout: FP16 W2, W3, W4 (forward), BF16 W2^T,
+//                 W3^T (backward)
+//   mlp_forward   128-point tiles, two tile groups per CTA (256 threads),
+//                 the inference path of mbt_mlp.cuh (layer 1 on the FP32
+//                 pipes, layers 2, 3 and 4 as tcgen05.mma with FP16
+//                 operands and FP32 accumulation in tensor memory, GELU in
+//                 FP16 pairs), keeping z and h of every point for the
+//                 backward pass
 //   mlp_backward  per 128-point tile: dz3 -> dh2 = dz3 W3 and
 //                 dW3 += dz3^T h2 on the tensor cores, dz2 -> dh1 = dz2 W2
 //                 and dW2 += dz2^T h1; dW2, dW3 accumulate in tensor memory
@@ -38,9 +40,10 @@ namespace {
 
 using namespace mbt;
 
-constexpr int kFwdThreads = 256;   // training forward: two groups of 128
+constexpr int kFwdGroups = 2;      // training forward: two groups of 128
+constexpr int kFwdThreads = 128 * kFwdGroups;
 constexpr int kBwdThreads = 128;
-constexpr size_t kFwdSmem = 6 * kTileBytes + 1024 + 8192;
+constexpr size_t kFwdSmem = mlp_cta_smem(kFwdGroups);
 constexpr int kInfThreads = 128 * kMlpGroups;
 constexpr size_t kInfSmem = kMlpCtaSmem;
 constexpr size_t kBwdSmem = 5 * kTileBytes + 1024 + 2048;
@@ -50,14 +53,17 @@ struct MlpSave {
   float *z1, *z2, *z3, *h1, *h2, *h3;
 };
 
-__global__ void mlp_prepare(const float *P, uint8_t *W2t, uint8_t *W3t, uint8_t *W2tT, uint8_t *W3tT) {
+__global__ void mlp_prepare(const float *P, uint8_t *W2t, uint8_t *W3t, uint8_t *W2tT, uint8_t *W3tT, uint8_t *W4t) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 128 * 128; i += gridDim.x * blockDim.x) {
     const int n = i / 128, k = i % 128;
-    const __nv_bfloat16 w2 = __float2bfloat16_rn(P[kMlpW2 + i]), w3 = __float2bfloat16_rn(P[kMlpW3 + i]);
-    *reinterpret_cast<__nv_bfloat16 *>(W2t + sw128_elem(n, k)) = w2;
-    *reinterpret_cast<__nv_bfloat16 *>(W3t + sw128_elem(n, k)) = w3;
-    *reinterpret_cast<__nv_bfloat16 *>(W2tT + sw128_elem(k, n)) = w2;
-    *reinterpret_cast<__nv_bfloat16 *>(W3tT + sw128_elem(k, n)) = w3;
+    *reinterpret_cast<__half *>(W2t + sw128_elem(n, k)) = __float2half_rn(P[kMlpW2 + i]);
+    *reinterpret_cast<__half *>(W3t + sw128_elem(n, k)) = __float2half_rn(P[kMlpW3 + i]);
+    *reinterpret_cast<__nv_bfloat16 *>(W2tT + sw128_elem(k, n)) = __float2bfloat16_rn(P[kMlpW2 + i]);
+    *reinterpret_cast<__nv_bfloat16 *>(W3tT + sw128_elem(k, n)) = __float2bfloat16_rn(P[kMlpW3 + i]);
+    if (i < 16 * 128) {
+      const float w4 = n < 2 ? P[kMlpW4 + i] : 0.0f;
+      *reinterpret_cast<__half *>(W4t + sw128_chunk_rows(n, k >> 3, 16) + (k & 7) * 2) = __float2half_rn(w4);
+    }
   }
 }
 
@@ -67,145 +73,57 @@ __device__ __forceinline__ void copy_tile(uint8_t *dst, const uint8_t *src, int 
   for (int i = tid; i < kTileBytes / 16; i += nthr) d[i] = s[i];
 }
 
-// Forward pass over n points (a, b, r) -> (Tx, Ty).  With `sv`, the
-// pre-activations and activations of every point are kept; with `tgt`,
-// the squared error against the targets is summed into loss_part[cta].
+// Forward pass over n points (a, b, r) -> (Tx, Ty), the inference path
+// with the forward values kept: with `sv`, the pre-activations and
+// activations of every point; with `tgt`, the squared error against the
+// targets is summed into loss_part[cta].
 __global__ void __launch_bounds__(kFwdThreads, 1)
 mlp_forward(MlpDev M, long n, const float *__restrict__ abr, float *__restrict__ out, MlpSave sv,
             const float *__restrict__ tgt, double *loss_part, int *err) {
   extern __shared__ uint8_t smem_raw[];
-  uint8_t *base = align1024(smem_raw);
-  uint8_t *sW2 = base, *sW3 = base + kTileBytes;
+  MlpGroup G;
+  const uint32_t tmem = mlp_cta_setup(M, align1024(smem_raw), G, kFwdGroups);
   const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
-  uint8_t *sAhi = base + (2 + 2 * g) * kTileBytes, *sAlo = sAhi + kTileBytes;
-  float *fp = reinterpret_cast<float *>(base + 6 * kTileBytes);
-  float *sW1 = fp, *sB1 = fp + 384, *sB2 = fp + 512, *sB3 = fp + 640, *sW4 = fp + 768, *sB4 = fp + 1024;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(fp + 1032);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(fp + 1040);
   __shared__ double lred[kFwdThreads / 32];
-
-  copy_tile(sW2, M.W2t, threadIdx.x, kFwdThreads);
-  copy_tile(sW3, M.W3t, threadIdx.x, kFwdThreads);
-  for (int i = threadIdx.x; i < 384; i += kFwdThreads) sW1[i] = M.P[kMlpW1 + i];
-  for (int i = threadIdx.x; i < 128; i += kFwdThreads) {
-    sB1[i] = M.P[kMlpB1 + i];
-    sB2[i] = M.P[kMlpB2 + i];
-    sB3[i] = M.P[kMlpB3 + i];
-  }
-  for (int i = threadIdx.x; i < 256; i += kFwdThreads) sW4[i] = M.P[kMlpW4 + i];
-  if (threadIdx.x < 2) sB4[threadIdx.x] = M.P[kMlpB4 + threadIdx.x];
-  if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    fence_mbar_init();
-  }
-  if (threadIdx.x < 32) {
-    tmem_alloc(tslot, 256);
-    tmem_relinquish();
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tslot;
-  const uint32_t dcol = tmem + 128u * g;                            // this group's accumulator
-  const uint32_t lane_addr = dcol + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16);
-  const uint32_t aW2 = smem_u32(sW2), aW3 = smem_u32(sW3), aHi = smem_u32(sAhi),
-                 aLo = kMlpSplit ? smem_u32(sAlo) : 0u;
-  uint32_t phase = 0;
-  bool ok = true;
   double lsum = 0.0;
   const long ntiles = (n + 127) / 128;
-  for (long tile = (long)blockIdx.x * 2 + g; tile < ntiles && ok; tile += (long)gridDim.x * 2) {
+  for (long tile = (long)blockIdx.x * kFwdGroups + g; tile < ntiles; tile += (long)gridDim.x * kFwdGroups) {
     const long m = tile * 128 + t;
     const bool live = m < n;
-    float x[3] = {-1.0f, -1.0f, -1.0f};
+    float x[3] = {-1.0f, -1.0f, -1.0f}, y[2];
     if (live) mlp_features(abr[3 * m], abr[3 * m + 1], abr[3 * m + 2], x);
-    float h[128];
-    // layer 1 (FP32)
-#pragma unroll 4
-    for (int j = 0; j < 128; ++j) {
-      float z = sB1[j];
-      z = fmaf(sW1[3 * j], x[0], z);
-      z = fmaf(sW1[3 * j + 1], x[1], z);
-      z = fmaf(sW1[3 * j + 2], x[2], z);
-      if (sv.z1 && live) sv.z1[m * 128 + j] = z;
-      h[j] = gelu_f(z);
-      if (sv.h1 && live) sv.h1[m * 128 + j] = h[j];
+    MlpRowSave rs = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    const bool save = sv.z1 != nullptr && live;
+    if (save) {
+      const size_t o = (size_t)m * 128;
+      rs = {sv.z1 + o, sv.z2 + o, sv.z3 + o, sv.h1 + o, sv.h2 + o, sv.h3 + o};
     }
-    store_row_split(sAhi, sAlo, t, h);
-    // layers 2 and 3 (tensor cores)
-    for (int layer = 0; layer < 2 && ok; ++layer) {
-      fence_proxy_async();
-      tc_fence_before();
-      named_barrier(1 + g, 128);
-      if (t == 0) {
-        tc_fence_after();
-        issue_layer(dcol, aHi, aLo, layer == 0 ? aW2 : aW3, false);
-        umma_commit(&bar[g]);
-      }
-      ok = group_all(mbar_wait(&bar[g], phase, kMlpWaitLimit), 1 + g, 128);
-      if (!ok) {
-        // give the MMAs in flight a second bounded wait, then leave
-        if (t == 0) atomicOr(err, 1);
-        mbar_wait(&bar[g], phase, kMlpWaitLimit);
-        break;
-      }
-      phase ^= 1u;
-      tc_fence_after();
-      const float *bias = layer == 0 ? sB2 : sB3;
-      float *zs = layer == 0 ? sv.z2 : sv.z3;
-      float *hs = layer == 0 ? sv.h2 : sv.h3;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        tmem_ld32(lane_addr + 32 * q, h + 32 * q);
-      }
-      tmem_ld_wait();
-#pragma unroll 4
-      for (int j = 0; j < 128; ++j) {
-        const float z = h[j] + bias[j];
-        if (zs && live) zs[m * 128 + j] = z;
-        h[j] = gelu_f(z);
-        if (hs && live) hs[m * 128 + j] = h[j];
-      }
-      if (layer == 0) {
-        tc_fence_before();
-        named_barrier(1 + g, 128);   // every thread has read the accumulator; the tile may be overwritten
-        store_row_split(sAhi, sAlo, t, h);
-      }
-    }
-    // layer 4 (FP32)
-    float o0 = sB4[0], o1 = sB4[1];
-#pragma unroll 4
-    for (int j = 0; j < 128; ++j) {
-      o0 = fmaf(sW4[j], h[j], o0);
-      o1 = fmaf(sW4[128 + j], h[j], o1);
+    if (!mlp_group_eval(G, t, x, y, save ? &rs : nullptr)) {
+      if (t == 0) atomicOr(err, 1);
+      break;
     }
     if (live) {
       if (out) {
-        out[2 * m] = o0;
-        out[2 * m + 1] = o1;
+        out[2 * m] = y[0];
+        out[2 * m + 1] = y[1];
       }
       if (tgt) {
-        const double d0 = (double)o0 - tgt[2 * m], d1 = (double)o1 - tgt[2 * m + 1];
+        const double d0 = (double)y[0] - tgt[2 * m], d1 = (double)y[1] - tgt[2 * m + 1];
         lsum += d0 * d0 + d1 * d1;
       }
     }
-    tc_fence_before();
-    named_barrier(1 + g, 128);
   }
   if (loss_part) {
     const double s = warp_sum(lsum);
     if ((threadIdx.x & 31) == 0) lred[threadIdx.x >> 5] = s;
   }
-  tc_fence_before();
   __syncthreads();
-  tc_fence_after();
   if (loss_part && threadIdx.x == 0) {
     double s = 0.0;
     for (int w = 0; w < kFwdThreads / 32; ++w) s += lred[w];
     loss_part[blockIdx.x] = s;
   }
-  if (threadIdx.x < 32) tmem_dealloc(tmem, 256);
+  mlp_cta_release(tmem, kFwdGroups);
 }
 
 // Inference over n points (a, b, r) -> (Yx, Yy): two groups of 128 threads
@@ -300,8 +218,8 @@ mlp_backward(MlpDev M, int n, const float *__restrict__ out, const float *__rest
       __syncthreads();
       if (t == 0) {
         tc_fence_after();
-        issue_layer(step == 0 ? cW3 : cW2, aX, 0, aY, !first);   // dW += dz^T h
-        issue_layer(cS, aA, 0, step == 0 ? aW3T : aW2T, false);  // dh = dz W
+        issue_layer(step == 0 ? cW3 : cW2, aX, aY, !first);   // dW += dz^T h
+        issue_layer(cS, aA, step == 0 ? aW3T : aW2T, false);  // dh = dz W
         umma_commit(bar);
       }
       ok = __syncthreads_and(mbar_wait(bar, phase, kMlpWaitLimit)) != 0;
@@ -462,7 +380,7 @@ __global__ void mlp_targets_kernel(long n, const float *abr, float *tgt) {
 
 struct mbt_mlp {
   float *P = nullptr, *G = nullptr, *Mo = nullptr, *Ve = nullptr;
-  uint8_t *W = nullptr;   // 4 BF16 tiles
+  uint8_t *W = nullptr;   // operand tiles: FP16 W2, W3; BF16 W2^T, W3^T; FP16 W4 (16 rows)
   int *err = nullptr;
   long adam_t = 0;
   int nsm = 148;
@@ -482,6 +400,7 @@ MlpDev dev_view(const mbt_mlp *m) {
   d.W3t = m->W + kTileBytes;
   d.W2tT = m->W + 2 * kTileBytes;
   d.W3tT = m->W + 3 * kTileBytes;
+  d.W4t = m->W + 4 * kTileBytes;
   return d;
 }
 
@@ -491,7 +410,8 @@ int ck(cudaError_t e, const char *what) {
 }
 
 int prepare(mbt_mlp *m, cudaStream_t st) {
-  mlp_prepare<<<64, 256, 0, st>>>(m->P, m->W, m->W + kTileBytes, m->W + 2 * kTileBytes, m->W + 3 * kTileBytes);
+  mlp_prepare<<<64, 256, 0, st>>>(m->P, m->W, m->W + kTileBytes, m->W + 2 * kTileBytes, m->W + 3 * kTileBytes,
+                                  m->W + 4 * kTileBytes);
   return ck(cudaGetLastError(), "mlp_prepare");
 }
 
@@ -586,7 +506,7 @@ int mbt_mlp_create(uint64_t seed, mbt_mlp **out) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, dev);
   if (cudaMalloc(&m->P, kMlpNParam * 4) || cudaMalloc(&m->G, kMlpNParam * 4) || cudaMalloc(&m->Mo, kMlpNParam * 4) ||
-      cudaMalloc(&m->Ve, kMlpNParam * 4) || cudaMalloc(&m->W, 4 * kTileBytes) || cudaMalloc(&m->err, sizeof(int))) {
+      cudaMalloc(&m->Ve, kMlpNParam * 4) || cudaMalloc(&m->W, 4 * kTileBytes + kW4TileBytes) || cudaMalloc(&m->err, sizeof(int))) {
     mbt_mlp_destroy(m);
     return mbt::fail_global(MBT_ERR_NOMEM, "MLP parameters");
   }

@@ -20,23 +20,24 @@
 // field divided by 8 and by the envelope's share.
 
 // Numerics of a forward pass (the oracle restates them):
-//   x = (a/4 - 1, b/4 - 1, 1 + 2 ln r / ln 20);  z1 = W1 x + b1;  h1 = gelu(z1)  (FP32)
-//   z2 = W2b bf16(h1) + b2: W2b = W2 rounded to BF16, FP32 sums
-//   h2 = gelu(z2);  z3 = W3b bf16(h2) + b3;  h3 = gelu(z3)
-//   Y = W4 h3 + b4  (FP32)
+//   x = (a/4 - 1, b/4 - 1, 1 + 2 ln r / ln 20);  z1 = W1 x + b1  (FP32)
+//   h1 = gelu(z1) in FP16 pair arithmetic (gelu_h2), an FP16 value
+//   z2 = W2h h1 + b2: W2h = W2 rounded to FP16, FP32 sums on the tensor
+//   cores, FP32 bias;  h2 = gelu(z2);  z3 = W3h h2 + b3;  h3 = gelu(z3)
+//   Y = W4h h3 + b4  (tensor cores, N = 16 with W4 padded; FP32 bias)
 // gelu(x) = x (1 + tanh(x (c1 + c1 c2 x^2))) / 2, c1 = sqrt(2/pi),
-// c2 = 0.044715, with the hardware tanh; activations rounded to BF16 as MMA
-// operands (kMlpSplit).  ln r spreads the flat aspect ratios, where the
-// field changes fastest and the beam-ion stage evaluates most, over the
-// feature range.
+// c2 = 0.044715 (FP16 constants), with the hardware tanh.  ln r spreads the
+// flat aspect ratios, where the field changes fastest and the beam-ion
+// stage evaluates most, over the feature range.
 //
-// Tile shape: 128 points per MMA tile (M = 128, N = 128, K = 16 per
+// Tile shape: 128 points per MMA tile (M = 128, N = 128 or 16, K = 16 per
 // instruction, 8 k-steps); operands in the canonical K-major 128-byte-
 // swizzled layout: a [128][128] BF16 tile is two 16 KB column blocks of 64
 // elements, each 16 groups of 8 rows x 128 B, the 16-byte chunk index of a
 // row XORed with the row index inside its group.
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cstdint>
 
 #include "mbt_common.cuh"
@@ -143,22 +144,33 @@ __device__ __forceinline__ float tanh_hw(float x) {
   return y;
 }
 constexpr float kGeluC1 = 0.7978845608028654f, kGeluC1C2 = 0.035677408136300125f;
-__device__ __forceinline__ float gelu_f(float x) {
-  const float y = x * fmaf(kGeluC1C2, x * x, kGeluC1);
-  const float hx = 0.5f * x;
-  return fmaf(hx, tanh_hw(y), hx);
-}
 __device__ __forceinline__ float gelu_grad(float x) {
   const float y = x * fmaf(kGeluC1C2, x * x, kGeluC1);
   const float th = tanh_hw(y);
   return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * 0.7978845608028654f * (1.0f + 0.134145f * x * x);
 }
 
-// Activations enter the tensor cores as BF16 (kMlpSplit false) or as a BF16
-// pair hi + lo that carries 16 bits of the FP32 value (true, twice the MMAs
-// and the activation tiles).
-constexpr bool kMlpSplit = false;
-constexpr int kMlpGroups = kMlpSplit ? 2 : 4;      // 128-thread groups per inference CTA
+// Forward operands are FP16 (the weights W2, W3, W4 and the activations;
+// FP16 keeps 11 significant bits where BF16 keeps 8), backward operands
+// BF16 (gradients need BF16's exponent range).  In one MMA both operands
+// have the same type.
+constexpr int kMlpGroups = 4;                       // 128-thread groups per inference CTA
+constexpr int kW4TileBytes = 16 * 128 * 2;          // W4 as a [16][128] FP16 tile (rows 2..15 zero)
+
+// FP32 accumulator, FP16 A and B, both K-major, M = 128, N = n
+__host__ __device__ constexpr uint32_t idesc_f16(uint32_t n) {
+  return (1u << 4) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+constexpr uint32_t kIdescF16 = idesc_f16(128), kIdescF16N16 = idesc_f16(16);
+
+// byte offset of the 16-byte chunk c of row `row` in a tile of `rows` rows
+__device__ __forceinline__ uint32_t sw128_chunk_rows(int row, int c, int rows) {
+  return (uint32_t)((c >> 3) * rows * 128 + (row >> 3) * 1024 + (row & 7) * 128 + (((c & 7) ^ (row & 7)) << 4));
+}
+// descriptor of k-step s of a tile of `rows` rows at `base`
+__device__ __forceinline__ uint64_t tile_desc_rows(uint32_t base, int s, int rows) {
+  return sw128_desc(base + (uint32_t)(s >> 2) * (uint32_t)(rows * 128) + (uint32_t)(s & 3) * 32u);
+}
 
 // Row `row` of a tile, BF16 only (backward operands).
 __device__ __forceinline__ void store_row_bf16(uint8_t *t, int row, const float *h) {
@@ -169,28 +181,6 @@ __device__ __forceinline__ void store_row_bf16(uint8_t *t, int row, const float 
     *reinterpret_cast<uint4 *>(t + sw128_chunk(row, c)) = p;
   }
 }
-// Row `row` of an activation tile: 128 values -> hi and lo BF16 tiles.
-__device__ __forceinline__ void store_row_split(uint8_t *hi, uint8_t *lo, int row, const float *h) {
-  if constexpr (!kMlpSplit) {
-    store_row_bf16(hi, row, h);
-  } else {
-#pragma unroll
-  for (int c = 0; c < 16; ++c) {
-    float v[8], l[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      v[i] = bf16_round(h[8 * c + i]);
-      l[i] = h[8 * c + i] - v[i];
-    }
-    const uint4 ph = make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
-                                pack_bf16(v[6], v[7]));
-    const uint4 pl = make_uint4(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]), pack_bf16(l[4], l[5]),
-                                pack_bf16(l[6], l[7]));
-    *reinterpret_cast<uint4 *>(hi + sw128_chunk(row, c)) = ph;
-    if (kMlpSplit) *reinterpret_cast<uint4 *>(lo + sw128_chunk(row, c)) = pl;
-  }
-  }
-}
 // Column `col` of a tile (the transpose of a row), BF16.
 __device__ __forceinline__ void store_col_bf16(uint8_t *t, int col, const float *h) {
 #pragma unroll 8
@@ -198,135 +188,224 @@ __device__ __forceinline__ void store_col_bf16(uint8_t *t, int col, const float 
     *reinterpret_cast<__nv_bfloat16 *>(t + sw128_elem(k, col)) = __float2bfloat16_rn(h[k]);
 }
 
-// Issue one 128 x 128 x 128 layer: D = Ahi.B^T + Alo.B^T (Alo may be 0).
-__device__ __forceinline__ void issue_layer(uint32_t d_tmem, uint32_t a_hi, uint32_t a_lo, uint32_t b, bool acc0) {
+// Issue one 128 x 128 x 128 BF16 product D (+)= A.B^T (backward).
+__device__ __forceinline__ void issue_layer(uint32_t d_tmem, uint32_t a, uint32_t b, bool acc0) {
 #pragma unroll
-  for (int s = 0; s < 8; ++s) {
-    umma_bf16(d_tmem, tile_desc(a_hi, s), tile_desc(b, s), kIdescBf16, (s > 0 || acc0) ? 1u : 0u);
-    if (a_lo) umma_bf16(d_tmem, tile_desc(a_lo, s), tile_desc(b, s), kIdescBf16, 1u);
-  }
+  for (int s = 0; s < 8; ++s)
+    umma_bf16(d_tmem, tile_desc(a, s), tile_desc(b, s), kIdescBf16, (s > 0 || acc0) ? 1u : 0u);
+}
+// The forward products: a hidden layer (N = 128) and the output layer
+// (N = 16, W4 padded), FP16 operands.
+__device__ __forceinline__ void issue_hidden_f16(uint32_t d_tmem, uint32_t a, uint32_t b) {
+#pragma unroll
+  for (int s = 0; s < 8; ++s) umma_bf16(d_tmem, tile_desc(a, s), tile_desc(b, s), kIdescF16, s > 0 ? 1u : 0u);
+}
+__device__ __forceinline__ void issue_out_f16(uint32_t d_tmem, uint32_t a, uint32_t b16) {
+#pragma unroll
+  for (int s = 0; s < 8; ++s)
+    umma_bf16(d_tmem, tile_desc(a, s), tile_desc_rows(b16, s, 16), kIdescF16N16, s > 0 ? 1u : 0u);
+}
+
+// Two FP32 columns of this thread's tensor-memory lane.
+__device__ __forceinline__ void tmem_ld2(uint32_t taddr, float &a, float &b) {
+  uint32_t r0, r1;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(r0), "=r"(r1) : "r"(taddr));
+  a = __uint_as_float(r0);
+  b = __uint_as_float(r1);
+}
+
+// GELU of a pair of pre-activations in FP16 pair arithmetic, one
+// instruction per step for both values and one hardware tanh per pair:
+//   z = fp16(z),  y = z (c1 + c1c2 z^2),  h = z/2 + (z/2) tanh(y),
+// with the FP16 constants c1c2 = 0x2891, c1 = 0x3A62, 1/2 = 0x3800 and every
+// step rounded to FP16.  Returns the FP16 pair (low half from z0).
+constexpr uint32_t kH2C1C2 = 0x28912891u, kH2C1 = 0x3A623A62u, kH2Half = 0x38003800u;
+__device__ __forceinline__ uint32_t gelu_h2(float z0, float z1) {
+  uint32_t z, t, p, y, th, hz, h;
+  asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(z) : "f"(z1), "f"(z0));
+  asm("mul.rn.f16x2 %0, %1, %1;" : "=r"(t) : "r"(z));
+  asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(p) : "r"(t), "r"(kH2C1C2), "r"(kH2C1));
+  asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(y) : "r"(z), "r"(p));
+  asm("tanh.approx.f16x2 %0, %1;" : "=r"(th) : "r"(y));
+  asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(hz) : "r"(z), "r"(kH2Half));
+  asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(h) : "r"(hz), "r"(th), "r"(hz));
+  return h;
+}
+__device__ __forceinline__ void unpack_h2(uint32_t h, float &a, float &b) {
+  asm("{\n\t.reg .f16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\tcvt.f32.f16 %0, lo;\n\tcvt.f32.f16 %1, hi;\n\t}"
+      : "=f"(a), "=f"(b)
+      : "r"(h));
 }
 
 // One group of 128 threads evaluating the network on a tile of 128 points
 // (thread t holds point t): shared-memory operands, its tensor-memory
 // accumulator, the barrier its MMAs complete on.
 struct MlpGroup {
-  const float *W1, *B1, *B2, *B3, *W4, *B4;   // shared memory, FP32
-  uint8_t *Ahi, *Alo;                          // the group's activation tiles
+  const float *W1, *B1, *B2, *B3, *B4;         // shared memory, FP32
+  uint8_t *A;                                  // the group's activation tile (FP16)
   uint64_t *bar;                               // MMA-completion barrier
-  uint32_t aW2, aW3, aHi, aLo;                 // shared addresses of the operand tiles
+  uint32_t aW2, aW3, aW4, aA;                  // shared addresses of the operand tiles
   uint32_t dcol;                               // accumulator: first tensor-memory column
   uint32_t lane;                               // this warp's lane base (bits 16..)
   int bar_id;                                  // named barrier of the group
   uint32_t phase;
 };
 
-// 8 hidden values -> one 16-byte chunk of the hi and lo tiles of row t.
-__device__ __forceinline__ void store_chunk_split(const MlpGroup &G, int t, int c, const float *h) {
-  if constexpr (!kMlpSplit) {
-    *reinterpret_cast<uint4 *>(G.Ahi + sw128_chunk(t, c)) =
-        make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]), pack_bf16(h[6], h[7]));
-  } else {
-  float v[8], l[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    v[i] = bf16_round(h[i]);
-    l[i] = h[i] - v[i];
-  }
-  *reinterpret_cast<uint4 *>(G.Ahi + sw128_chunk(t, c)) =
-      make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
-  *reinterpret_cast<uint4 *>(G.Alo + sw128_chunk(t, c)) =
-      make_uint4(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]), pack_bf16(l[4], l[5]), pack_bf16(l[6], l[7]));
-  }
-}
-
-// The network on this thread's features x -> y (Yx, Yy).  Every thread of
-// the group calls it together; false when an MMA never completed (the
-// group then stops using the tensor cores).
-__device__ __forceinline__ bool mlp_group_eval(MlpGroup &G, int t, const float *x, float *y) {
-  // layer 1, FP32, 8 units at a time
-#pragma unroll 1
-  for (int c = 0; c < 16; ++c) {
-    float h[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int j = 8 * c + i;
-      float z = G.B1[j];
-      z = fmaf(G.W1[3 * j], x[0], z);
-      z = fmaf(G.W1[3 * j + 1], x[1], z);
-      z = fmaf(G.W1[3 * j + 2], x[2], z);
-      h[i] = gelu_f(z);
-    }
-    store_chunk_split(G, t, c, h);
-  }
-  float o0 = G.B4[0], o1 = G.B4[1];
-#pragma unroll 1
-  for (int layer = 0; layer < 2; ++layer) {
-    fence_proxy_async();
-    tc_fence_before();
-    named_barrier(G.bar_id, 128);
-    if (t == 0) {
-      tc_fence_after();
-      issue_layer(G.dcol, G.aHi, G.aLo, layer == 0 ? G.aW2 : G.aW3, false);
-      umma_commit(G.bar);
-    }
-    if (!group_all(mbar_wait(G.bar, G.phase, kMlpWaitLimit), G.bar_id, 128)) {
-      mbar_wait(G.bar, G.phase, kMlpWaitLimit);   // a second bounded wait for the MMAs in flight
-      return false;
-    }
-    G.phase ^= 1u;
+// Issue (one thread) and wait (all) for one product of the group; false
+// when it never completed (a second bounded wait then covers the MMAs in
+// flight).
+template <int KIND>
+__device__ __forceinline__ bool group_mma(MlpGroup &G, int t, uint32_t b) {
+  fence_proxy_async();
+  tc_fence_before();
+  named_barrier(G.bar_id, 128);
+  if (t == 0) {
     tc_fence_after();
-    const float *bias = layer == 0 ? G.B2 : G.B3;
-#pragma unroll 1
-    for (int q = 0; q < 4; ++q) {
-      float v[32];
-      tmem_ld32(G.dcol + G.lane + 32 * q, v);
-      tmem_ld_wait();
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        float h[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) h[i] = gelu_f(v[8 * c + i] + bias[32 * q + 8 * c + i]);
-        if (layer == 0) {
-          store_chunk_split(G, t, 4 * q + c, h);
-        } else {
-#pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            o0 = fmaf(G.W4[32 * q + 8 * c + i], h[i], o0);
-            o1 = fmaf(G.W4[128 + 32 * q + 8 * c + i], h[i], o1);
-          }
-        }
-      }
-    }
+    if (KIND == 0) issue_hidden_f16(G.dcol, G.aA, b);
+    else issue_out_f16(G.dcol, G.aA, b);
+    umma_commit(G.bar);
   }
-  y[0] = o0;
-  y[1] = o1;
+  if (!group_all(mbar_wait(G.bar, G.phase, kMlpWaitLimit), G.bar_id, 128)) {
+    mbar_wait(G.bar, G.phase, kMlpWaitLimit);
+    return false;
+  }
+  G.phase ^= 1u;
+  tc_fence_after();
   return true;
 }
 
-// Device view of a network: FP32 parameters and the BF16 operand tiles.
-struct MlpDev {
-  const float *P;               // master parameters (kMlpNParam)
-  const uint8_t *W2t, *W3t;     // BF16 operand tiles of W2, W3 (rows n, k)
-  const uint8_t *W2tT, *W3tT;   // of W2^T, W3^T (rows k, n)
+// Layer 1 of this thread's point (FP32 pre-activations, FP16 GELU) into
+// row t of the activation tile; z1 / h1 (may be null) receive the values.
+__device__ __forceinline__ void mlp_layer1(const MlpGroup &G, int t, const float *x, float *z1, float *h1) {
+  const float4 *W1v = reinterpret_cast<const float4 *>(G.W1), *B1v = reinterpret_cast<const float4 *>(G.B1);
+#pragma unroll 1
+  for (int c = 0; c < 16; ++c) {
+    float w[24], bb[8], z[8];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      const float4 v = W1v[6 * c + i];
+      w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w;
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const float4 v = B1v[2 * c + i];
+      bb[4 * i] = v.x; bb[4 * i + 1] = v.y; bb[4 * i + 2] = v.z; bb[4 * i + 3] = v.w;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      float zz = bb[i];
+      zz = fmaf(w[3 * i], x[0], zz);
+      zz = fmaf(w[3 * i + 1], x[1], zz);
+      zz = fmaf(w[3 * i + 2], x[2], zz);
+      z[i] = zz;
+    }
+    uint32_t h[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) h[i] = gelu_h2(z[2 * i], z[2 * i + 1]);
+    *reinterpret_cast<uint4 *>(G.A + sw128_chunk(t, c)) = make_uint4(h[0], h[1], h[2], h[3]);
+    if (z1) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) z1[8 * c + i] = z[i];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) unpack_h2(h[i], h1[8 * c + 2 * i], h1[8 * c + 2 * i + 1]);
+    }
+  }
+}
+
+// Epilogue of a hidden layer: accumulator + bias, FP16 GELU, into row t of
+// the activation tile (after every thread of the group has read the
+// accumulator the tile may be overwritten: the product that read it has
+// completed).  zs / hs (may be null) receive the values.
+__device__ __forceinline__ void mlp_hidden_epilogue(const MlpGroup &G, int t, const float *bias_smem, float *zs,
+                                                    float *hs) {
+  const float4 *bias = reinterpret_cast<const float4 *>(bias_smem);
+#pragma unroll 1
+  for (int q = 0; q < 4; ++q) {
+    float v[32];
+    tmem_ld32(G.dcol + G.lane + 32 * q, v);
+    tmem_ld_wait();
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      float z[8];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const float4 bv = bias[8 * q + 2 * c + i];
+        z[4 * i] = v[8 * c + 4 * i] + bv.x;
+        z[4 * i + 1] = v[8 * c + 4 * i + 1] + bv.y;
+        z[4 * i + 2] = v[8 * c + 4 * i + 2] + bv.z;
+        z[4 * i + 3] = v[8 * c + 4 * i + 3] + bv.w;
+      }
+      uint32_t h[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) h[i] = gelu_h2(z[2 * i], z[2 * i + 1]);
+      *reinterpret_cast<uint4 *>(G.A + sw128_chunk(t, 4 * q + c)) = make_uint4(h[0], h[1], h[2], h[3]);
+      if (zs) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) zs[32 * q + 8 * c + i] = z[i];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) unpack_h2(h[i], hs[32 * q + 8 * c + 2 * i], hs[32 * q + 8 * c + 2 * i + 1]);
+      }
+    }
+  }
+  tc_fence_before();
+}
+
+// Rows of one point's saved forward values (training), or all null.
+struct MlpRowSave {
+  float *z1, *z2, *z3, *h1, *h2, *h3;
 };
 
-// Shared-memory footprint of a CTA of kMlpGroups groups that evaluates the
-// network: two weight tiles, the groups' activation tiles, the FP32 layers.
-constexpr size_t kMlpCtaSmem = (2 + (size_t)kMlpGroups * (kMlpSplit ? 2 : 1)) * kTileBytes + 1024 + 8192;
+// The network on this thread's features x -> y (Yx, Yy).  Every thread of
+// the group calls it together; false when an MMA never completed (the
+// group then stops using the tensor cores).  sv: where this point's
+// pre-activations and activations go (training), or null.
+__device__ __forceinline__ bool mlp_group_eval(MlpGroup &G, int t, const float *x, float *y,
+                                               const MlpRowSave *sv = nullptr) {
+  mlp_layer1(G, t, x, sv ? sv->z1 : nullptr, sv ? sv->h1 : nullptr);
+  if (!group_mma<0>(G, t, G.aW2)) return false;
+  mlp_hidden_epilogue(G, t, G.B2, sv ? sv->z2 : nullptr, sv ? sv->h2 : nullptr);
+  if (!group_mma<0>(G, t, G.aW3)) return false;
+  mlp_hidden_epilogue(G, t, G.B3, sv ? sv->z3 : nullptr, sv ? sv->h3 : nullptr);
+  if (!group_mma<1>(G, t, G.aW4)) return false;
+  float o0, o1;
+  tmem_ld2(G.dcol + G.lane, o0, o1);
+  tmem_ld_wait();
+  tc_fence_before();
+  y[0] = o0 + G.B4[0];
+  y[1] = o1 + G.B4[1];
+  return true;
+}
+
+// Device view of a network: FP32 parameters and the operand tiles.
+struct MlpDev {
+  const float *P;               // master parameters (kMlpNParam)
+  const uint8_t *W2t, *W3t;     // FP16 operand tiles of W2, W3 (rows n, k)
+  const uint8_t *W4t;           // FP16 [16][128] tile of W4 (rows 2..15 zero)
+  const uint8_t *W2tT, *W3tT;   // BF16 tiles of W2^T, W3^T (rows k, n), backward
+};
+
+// Shared-memory footprint of a CTA of `groups` groups that evaluates the
+// network: two weight tiles, the W4 tile, the groups' activation tiles,
+// the FP32 layers and barriers.
+__host__ __device__ constexpr size_t mlp_cta_smem(int groups) {
+  return (2 + (size_t)groups) * kTileBytes + kW4TileBytes + 1024 + 4096;
+}
+constexpr size_t kMlpCtaSmem = mlp_cta_smem(kMlpGroups);
 
 __device__ __forceinline__ uint8_t *align1024(uint8_t *p) {
   return reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(p) + 1023) & ~(uintptr_t)1023);
 }
 
-// Load the network into a CTA of kMlpGroups x 128 threads and set up group
+// Load the network into a CTA of `groups` x 128 threads and set up group
 // `g`; returns the tensor-memory base (allocated here: free it with
 // mlp_cta_release).  Every thread of the CTA calls it.
-__device__ __forceinline__ uint32_t mlp_cta_setup(const MlpDev &M, uint8_t *base, MlpGroup &G) {
-  const int nthr = 128 * kMlpGroups, g = threadIdx.x >> 7;
-  float *fp = reinterpret_cast<float *>(base + (2 + kMlpGroups * (kMlpSplit ? 2 : 1)) * kTileBytes);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(fp + 1032);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(fp + 1032 + 2 * kMlpGroups);
+__device__ __forceinline__ uint32_t mlp_cta_setup(const MlpDev &M, uint8_t *base, MlpGroup &G,
+                                                  int groups = kMlpGroups) {
+  const int nthr = 128 * groups, g = threadIdx.x >> 7;
+  uint8_t *w4 = base + (2 + groups) * kTileBytes;
+  float *fp = reinterpret_cast<float *>(w4 + kW4TileBytes);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(fp + 776);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(fp + 776 + 2 * 8);
   {
     const uint4 *s2 = reinterpret_cast<const uint4 *>(M.W2t), *s3 = reinterpret_cast<const uint4 *>(M.W3t);
     uint4 *d2 = reinterpret_cast<uint4 *>(base), *d3 = reinterpret_cast<uint4 *>(base + kTileBytes);
@@ -334,6 +413,8 @@ __device__ __forceinline__ uint32_t mlp_cta_setup(const MlpDev &M, uint8_t *base
       d2[i] = s2[i];
       d3[i] = s3[i];
     }
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(M.W4t);
+    for (int i = threadIdx.x; i < kW4TileBytes / 16; i += nthr) reinterpret_cast<uint4 *>(w4)[i] = s4[i];
   }
   for (int i = threadIdx.x; i < 384; i += nthr) fp[i] = M.P[kMlpW1 + i];
   for (int i = threadIdx.x; i < 128; i += nthr) {
@@ -341,39 +422,37 @@ __device__ __forceinline__ uint32_t mlp_cta_setup(const MlpDev &M, uint8_t *base
     fp[512 + i] = M.P[kMlpB2 + i];
     fp[640 + i] = M.P[kMlpB3 + i];
   }
-  for (int i = threadIdx.x; i < 256; i += nthr) fp[768 + i] = M.P[kMlpW4 + i];
-  if (threadIdx.x < 2) fp[1024 + threadIdx.x] = M.P[kMlpB4 + threadIdx.x];
+  if (threadIdx.x < 2) fp[768 + threadIdx.x] = M.P[kMlpB4 + threadIdx.x];
   if (threadIdx.x == 0) {
-    for (int q = 0; q < kMlpGroups; ++q) mbar_init(&bar[q], 1);
+    for (int q = 0; q < groups; ++q) mbar_init(&bar[q], 1);
     fence_mbar_init();
   }
   if (threadIdx.x < 32) {
-    tmem_alloc(tslot, 128 * kMlpGroups);
+    tmem_alloc(tslot, 128 * groups);
     tmem_relinquish();
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  G.W1 = fp; G.B1 = fp + 384; G.B2 = fp + 512; G.B3 = fp + 640; G.W4 = fp + 768; G.B4 = fp + 1024;
-  G.Ahi = base + (2 + (kMlpSplit ? 2 : 1) * g) * kTileBytes;
-  G.Alo = kMlpSplit ? G.Ahi + kTileBytes : nullptr;
+  G.W1 = fp; G.B1 = fp + 384; G.B2 = fp + 512; G.B3 = fp + 640; G.B4 = fp + 768;
+  G.A = base + (2 + g) * kTileBytes;
   G.bar = &bar[g];
   G.aW2 = smem_u32(base);
   G.aW3 = smem_u32(base + kTileBytes);
-  G.aHi = smem_u32(G.Ahi);
-  G.aLo = kMlpSplit ? smem_u32(G.Alo) : 0u;
+  G.aW4 = smem_u32(w4);
+  G.aA = smem_u32(G.A);
   G.dcol = tmem + 128u * g;
   G.lane = (uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16;
   G.bar_id = 1 + g;
   G.phase = 0;
   return tmem;
 }
-__device__ __forceinline__ void mlp_cta_release(uint32_t tmem) {
+__device__ __forceinline__ void mlp_cta_release(uint32_t tmem, int groups = kMlpGroups) {
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (threadIdx.x < 32) tmem_dealloc(tmem, 128 * kMlpGroups);
+  if (threadIdx.x < 32) tmem_dealloc(tmem, 128 * groups);
 }
 
 // The network's input features and targets.
@@ -436,28 +515,29 @@ namespace mbt {
 // cores failed.
 __device__ __forceinline__ bool mlp_group_field(MlpGroup &G, int t, bool active, double dx, double dy, double sx,
                                                 double sy, double &gx, double &gy, bool &in_domain) {
-  const double sgx = dx < 0.0 ? -1.0 : 1.0, sgy = dy < 0.0 ? -1.0 : 1.0;
-  double ax = fabs(dx), ay = fabs(dy), s1 = sx, s2 = sy;
+  // the network's inputs and the field's assembly in FP32 (its 1e-7 is far
+  // below the network's accuracy)
   const bool swap = sy > sx;
-  if (swap) {
-    const double u = ax; ax = ay; ay = u;
-    const double v = s1; s1 = s2; s2 = v;
-  }
-  const double a = ax / s1, b = ay / s2, r = s2 / s1;
-  in_domain = active && s2 > 0.0 && a < 8.0 && b < 8.0 && r >= 0.05;
+  const float ax = (float)fabs(swap ? dy : dx), ay = (float)fabs(swap ? dx : dy);
+  const float s1 = (float)(swap ? sy : sx), s2 = (float)(swap ? sx : sy);
+  const float inv1 = 1.0f / s1;
+  const float a = ax * inv1, b = ay / s2, r = s2 * inv1;
+  in_domain = active && s2 > 0.0f && a < 8.0f && b < 8.0f && r >= 0.05f;
   float x[3], y[2];
-  mlp_features(in_domain ? (float)a : 0.0f, in_domain ? (float)b : 0.0f, in_domain ? (float)r : 1.0f, x);
+  mlp_features(in_domain ? a : 0.0f, in_domain ? b : 0.0f, in_domain ? r : 1.0f, x);
   if (!mlp_group_eval(G, t, x, y)) return false;
   if (in_domain) {
     float ex, ey;
-    mlp_envelopes((float)a, (float)b, (float)r, ex, ey);
-    double fx = a * (double)ex * (1.0 + (double)y[0] / kMlpResidualScale);
-    double fy = b * (double)ey * (1.0 + (double)y[1] / kMlpResidualScale);
+    mlp_envelopes(a, b, r, ex, ey);
+    float fx = a * ex * fmaf(y[0], 1.0f / kMlpResidualScale, 1.0f);
+    float fy = b * ey * fmaf(y[1], 1.0f / kMlpResidualScale, 1.0f);
     if (swap) {
-      const double u = fx; fx = fy; fy = u;
+      const float u = fx; fx = fy; fy = u;
     }
-    gx = sgx * fx / s1;
-    gy = sgy * fy / s1;
+    gx = (double)(fx * inv1);
+    gy = (double)(fy * inv1);
+    if (dx < 0.0) gx = -gx;
+    if (dy < 0.0) gy = -gy;
   }
   return true;
 }

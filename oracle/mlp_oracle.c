@@ -1,9 +1,10 @@
 /*
  * mlp_oracle.c -- TEST INFRASTRUCTURE ONLY: CPU restatement of the learned
  * field network of libmbt (mbt.h, mbt_mlp_*): forward pass and gradient
- * with the same roundings of the tensor-core operands (BF16 weights, BF16
- * hi + lo activations in the forward pass, BF16 operands of the backward
- * products), sums in double.  Used by tests/ to check the GPU kernels.
+ * with the same roundings of the tensor-core operands (FP16 weights and
+ * activations and FP16 GELU arithmetic in the forward pass, BF16 operands
+ * of the backward products), sums in double.  Used by tests/ to check the
+ * GPU kernels.
  */
 #include <math.h>
 #include <stdint.h>
@@ -33,14 +34,35 @@ static float bf16r(float v)
   return v;
 }
 
-/* GELU in its tanh form; the GPU evaluates tanh with the hardware
- * approximation (relative error below 2^-10.987), this restatement with
- * libm's tanhf. */
+/* round to the nearest FP16 (ties to even), as a float */
+static float h16(double v)
+{
+  const double a = fabs(v);
+  double q;
+  int e;
+  if (!(a < 65520.0)) return a != a ? (float) v : (float) copysign(INFINITY, v);
+  if (a < 6.103515625e-05) {
+    q = 5.9604644775390625e-08;              /* subnormal step 2^-24 */
+  } else {
+    frexp(a, &e);                            /* a in [2^(e-1), 2^e) */
+    q = ldexp(1.0, e - 11);                  /* 11 significant bits */
+  }
+  return (float) (nearbyint(v / q) * q);
+}
+
+/* GELU in FP16 pair arithmetic as the GPU evaluates it (gelu_h2): every
+ * step rounded to FP16, FP16 constants; the GPU's tanh is the hardware
+ * approximation, this restatement libm's tanh rounded to FP16. */
 static float gelu(float x)
 {
-  const float y = x * fmaf(0.035677408136300125f, x * x, 0.7978845608028654f);
-  const float hx = 0.5f * x;
-  return fmaf(hx, tanhf(y), hx);
+  const float c1c2 = 0.035675048828125f, c1 = 0.7978515625f;
+  const float z = h16(x);
+  const float t = h16((double) z * z);
+  const float p = h16((double) c1c2 * t + c1);
+  const float y = h16((double) z * p);
+  const float th = h16(tanh((double) y));
+  const float hz = h16(0.5 * z);
+  return h16((double) hz * th + hz);
 }
 
 static float gelu_grad(float x)
@@ -50,8 +72,6 @@ static float gelu_grad(float x)
   return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * 0.7978845608028654f * (1.0f + 0.134145f * x * x);
 }
 
-/* activations enter the products as BF16 (libm's kMlpSplit = false) */
-#define SPLIT 0
 
 typedef struct fwd_t {
   float x[3], z1[H], h1[H], z2[H], h2[H], z3[H], h3[H], out[2];
@@ -71,29 +91,23 @@ static void forward_one(const float *P, const float *abr, fwd_t *f)
     f->z1[j] = z;
     f->h1[j] = gelu(z);
   }
+  /* the activations are FP16 values already; the weights round to FP16 */
   for (j = 0; j < H; j++) {
     double s = 0.0;
-    for (k = 0; k < H; k++) {
-      const float hi = bf16r(f->h1[k]), lo = SPLIT ? bf16r(f->h1[k] - hi) : 0.0f;
-      s += ((double) hi + (double) lo) * (double) bf16r(P[W2 + H * j + k]);
-    }
+    for (k = 0; k < H; k++) s += (double) f->h1[k] * (double) h16(P[W2 + H * j + k]);
     f->z2[j] = (float) s + P[B2 + j];
     f->h2[j] = gelu(f->z2[j]);
   }
   for (j = 0; j < H; j++) {
     double s = 0.0;
-    for (k = 0; k < H; k++) {
-      const float hi = bf16r(f->h2[k]), lo = SPLIT ? bf16r(f->h2[k] - hi) : 0.0f;
-      s += ((double) hi + (double) lo) * (double) bf16r(P[W3 + H * j + k]);
-    }
+    for (k = 0; k < H; k++) s += (double) f->h2[k] * (double) h16(P[W3 + H * j + k]);
     f->z3[j] = (float) s + P[B3 + j];
     f->h3[j] = gelu(f->z3[j]);
   }
-  f->out[0] = P[B4];
-  f->out[1] = P[B4 + 1];
-  for (j = 0; j < H; j++) {
-    f->out[0] = fmaf(P[W4 + j], f->h3[j], f->out[0]);
-    f->out[1] = fmaf(P[W4 + H + j], f->h3[j], f->out[1]);
+  for (j = 0; j < 2; j++) {
+    double s = 0.0;
+    for (k = 0; k < H; k++) s += (double) f->h3[k] * (double) h16(P[W4 + H * j + k]);
+    f->out[j] = (float) s + P[B4 + j];
   }
 }
 

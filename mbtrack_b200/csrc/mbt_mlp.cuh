@@ -94,6 +94,25 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// 16 consecutive FP32 columns, and a wait that the 16 values depend on (so
+// that no use of them is scheduled before it)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_wait16(float *v) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7]),
+                 "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]), "+f"(v[14]), "+f"(v[15])
+               :
+               : "memory");
+}
 
 // AND of `v` over the `count` threads of named barrier `id` (a barrier too)
 __device__ __forceinline__ bool group_all(bool v, int id, int count) {
@@ -312,40 +331,53 @@ __device__ __forceinline__ void mlp_layer1(const MlpGroup &G, int t, const float
   }
 }
 
+// 16 accumulator columns (k0 .. k0+15) + bias -> FP16 GELU -> two chunks
+// of row t of the activation tile.
+__device__ __forceinline__ void mlp_epi16(const MlpGroup &G, int t, const float4 *bias, int k0, const float *v,
+                                          float *zs, float *hs) {
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    float z[8];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const float4 bv = bias[(k0 + 8 * c) / 4 + i];
+      z[4 * i] = v[8 * c + 4 * i] + bv.x;
+      z[4 * i + 1] = v[8 * c + 4 * i + 1] + bv.y;
+      z[4 * i + 2] = v[8 * c + 4 * i + 2] + bv.z;
+      z[4 * i + 3] = v[8 * c + 4 * i + 3] + bv.w;
+    }
+    uint32_t h[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) h[i] = gelu_h2(z[2 * i], z[2 * i + 1]);
+    *reinterpret_cast<uint4 *>(G.A + sw128_chunk(t, (k0 >> 3) + c)) = make_uint4(h[0], h[1], h[2], h[3]);
+    if (zs) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) zs[k0 + 8 * c + i] = z[i];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) unpack_h2(h[i], hs[k0 + 8 * c + 2 * i], hs[k0 + 8 * c + 2 * i + 1]);
+    }
+  }
+}
+
 // Epilogue of a hidden layer: accumulator + bias, FP16 GELU, into row t of
-// the activation tile (after every thread of the group has read the
-// accumulator the tile may be overwritten: the product that read it has
-// completed).  zs / hs (may be null) receive the values.
+// the activation tile (the product that read the tile has completed), 16
+// columns at a time with the next 16 loading meanwhile.  zs / hs (may be
+// null) receive the values.
 __device__ __forceinline__ void mlp_hidden_epilogue(const MlpGroup &G, int t, const float *bias_smem, float *zs,
                                                     float *hs) {
   const float4 *bias = reinterpret_cast<const float4 *>(bias_smem);
+  const uint32_t col = G.dcol + G.lane;
+  float va[16], vb[16];
+  tmem_ld16(col, va);
+  tmem_wait16(va);
 #pragma unroll 1
-  for (int q = 0; q < 4; ++q) {
-    float v[32];
-    tmem_ld32(G.dcol + G.lane + 32 * q, v);
-    tmem_ld_wait();
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      float z[8];
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const float4 bv = bias[8 * q + 2 * c + i];
-        z[4 * i] = v[8 * c + 4 * i] + bv.x;
-        z[4 * i + 1] = v[8 * c + 4 * i + 1] + bv.y;
-        z[4 * i + 2] = v[8 * c + 4 * i + 2] + bv.z;
-        z[4 * i + 3] = v[8 * c + 4 * i + 3] + bv.w;
-      }
-      uint32_t h[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) h[i] = gelu_h2(z[2 * i], z[2 * i + 1]);
-      *reinterpret_cast<uint4 *>(G.A + sw128_chunk(t, 4 * q + c)) = make_uint4(h[0], h[1], h[2], h[3]);
-      if (zs) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) zs[32 * q + 8 * c + i] = z[i];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) unpack_h2(h[i], hs[32 * q + 8 * c + 2 * i], hs[32 * q + 8 * c + 2 * i + 1]);
-      }
-    }
+  for (int k0 = 0; k0 < 128; k0 += 32) {
+    tmem_ld16(col + k0 + 16, vb);
+    mlp_epi16(G, t, bias, k0, va, zs, hs);
+    tmem_wait16(vb);
+    if (k0 + 32 < 128) tmem_ld16(col + k0 + 32, va);
+    mlp_epi16(G, t, bias, k0 + 16, vb, zs, hs);
+    if (k0 + 32 < 128) tmem_wait16(va);
   }
   tc_fence_before();
 }
@@ -479,26 +511,31 @@ static __constant__ float kGl16Wf[16] = {
     0.09472530522753432f,  0.09130170752246182f,  0.084578259697501323f, 0.074797994408288354f,
     0.062314485627767036f, 0.047579255841246303f, 0.031126761969323728f, 0.013576229705877088f};
 
-// The envelopes Ex, Ey of the field's shape (FP32).
+// The envelopes Ex, Ey of the field's shape (FP32 with the hardware
+// reciprocal, exponential and reciprocal square root: the network learns
+// the residual of exactly this function, its training targets use it too).
 __device__ __forceinline__ void mlp_envelopes(float a, float b, float r, float &ex, float &ey) {
   const float a2 = a * a, br2 = (b * r) * (b * r), q = 1.0f - r * r;
+  const float i1r = __fdividef(1.0f, 1.0f + r);
   float sx = 0.0f;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    const float u = r + (1.0f - r) * kGl8X[i];
-    const float t2 = (1.0f - kGl8X[i]) * (1.0f + u) / (1.0f + r);
-    sx += kGl8W[i] * __expf(-0.5f * t2 * (a2 + br2 / (u * u)));
+    const float u = fmaf(1.0f - r, kGl8X[i], r);
+    const float iu = __fdividef(1.0f, u);
+    const float t2 = (1.0f - kGl8X[i]) * (1.0f + u) * i1r;
+    sx = fmaf(kGl8W[i], __expf(-0.5f * t2 * fmaf(br2, iu * iu, a2)), sx);
   }
-  ex = sx / (3.14159265358979f * (1.0f + r));
-  const float smax = fminf(1.0f, 80.0f / fmaxf(a2 + br2, 1e-30f));
+  ex = sx * i1r * 0.31830988618379067f;
+  const float smax = fminf(1.0f, __fdividef(80.0f, fmaxf(a2 + br2, 1e-30f)));
   float sy = 0.0f;
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
     const float sg = smax * kGl16Xf[i];
-    const float d = 1.0f - q * sg;
-    sy += kGl16Wf[i] * __expf(-0.5f * sg * (a2 + br2 / d)) * rsqrtf(d * d * d);
+    const float d = fmaf(-q, sg, 1.0f);
+    const float id = __fdividef(1.0f, d);
+    sy = fmaf(kGl16Wf[i] * id * rsqrtf(d), __expf(-0.5f * sg * fmaf(br2, id, a2)), sy);
   }
-  ey = r * 0.5f * smax * sy / 3.14159265358979f;
+  ey = r * 0.5f * smax * sy * 0.31830988618379067f;
 }
 
 constexpr float kMlpResidualScale = 8.0f;   // Y = 8 (F / envelope - 1)

@@ -338,6 +338,8 @@ def run_b200(args):
             # network FLOPs: 2 x (3x128 + 2x128x128 + 128x2) per evaluation
             tfl = 66816.0 * bi_info["field_evaluations_per_turn"] / (bi_ms * 1e-3) / 1e12
             bi_info["network_tflops"] = tfl
+        if args.growth_turns > 0 and bi.surrogate:
+            bi_info["growth_check"] = growth_check(cfg, mlp, args.growth_turns)
     peak, peak_kind = measured_peak()
     achieved = BYTES_PER_MP_TURN * npart / (k1_ms * 1e-3) / 1e9
     traffic = profile_traffic(args.workload)
@@ -442,6 +444,43 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+
+def growth_check(cfg, mlp, turns):
+    """Growth rate of the vertical coupled-bunch motion with the Faddeeva
+    and with the learned field, same train, ions and seeds: the beam-ion
+    configuration reduced to 5e3 macroparticles per bunch and 4 interaction
+    points at 10 nTorr, so that the instability grows within a few hundred
+    turns."""
+    import numpy as np
+    import torch
+    from mbtrack_b200 import analysis, api
+    amps, secs = {}, {}
+    for surr in (0, 1):
+        bi = cfg.beam_ion()
+        bi.n_ip, bi.pressure, bi.surrogate = 4, 10e-9, surr
+        t = api.Tracker(cfg.params, cfg.bucket, np.full(cfg.nbunch, 5000), cfg.bunch_currents())
+        t.generate_beam(3)
+        t.enable_beam_ion(bi)
+        if surr:
+            t.use_mlp(mlp)
+        t.prepare()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = t.run(turns)
+        torch.cuda.synchronize()
+        secs[surr] = time.perf_counter() - t0
+        t.close()
+        amps[surr] = analysis.centroid_amplitude(st, "VER")
+    w = analysis.exponential_window(amps[0])
+    out = {"config": "beam-ion train, 5e3 macroparticles per bunch, 4 interaction points, 10 nTorr",
+           "turns": turns, "seconds": {"faddeeva": secs[0], "learned": secs[1]}}
+    if w is None:
+        out["window"] = None
+        return out
+    k0, k1 = analysis.growth_rate(amps[0], w), analysis.growth_rate(amps[1], w)
+    out.update({"window": list(w), "rate_faddeeva": k0, "rate_learned": k1, "rel_diff": abs(k1 - k0) / abs(k0)})
+    return out
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -456,6 +495,9 @@ def main():
     ap.add_argument("--cpu-turns", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--mlp-steps", type=int, default=48000, help="training steps of the learned field")
+    ap.add_argument("--growth-turns", type=int, default=0,
+                    help="beam_ion_mlp: also compare the instability growth rate of the learned and the "
+                         "Faddeeva stage over this many turns on a reduced train (0: skip)")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 20 if args.workload.startswith("beam_ion") else 200

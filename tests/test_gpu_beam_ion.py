@@ -106,3 +106,33 @@ def test_surrogate_stage_tracks_the_faddeeva_stage(tmp_path, cuda_device):
     assert rel < 1e-12      # ion counts do not depend on the field
     for m in (1, 2, 3, 4):
         assert np.abs(c1[..., m] - c0[..., m]).max() <= 1e-2 * np.abs(c0[..., 3:]).max(), m
+
+
+def test_surrogate_growth_rate_within_one_percent(tmp_path, cuda_device):
+    """The vertical beam-ion instability grows at the same rate with the
+    learned field as with the Faddeeva field (within 1 %): the 200-bunch
+    train with 5e3 macroparticles per bunch, 4 interaction points at
+    10 nTorr (growth within a few hundred turns), same beam, ions and
+    seeds; the rate is fitted over the exponential rise of the rms bunch
+    centroid (mbtrack_b200.analysis)."""
+    from mbtrack_b200 import analysis
+    mlp = api.Mlp(seed=31)
+    mlp.train(nsamples=1 << 23, batch=8192, steps=24000, lr=2e-3, seed=32)
+    amp = {}
+    for surr in (0, 1):
+        C = api.Config(small_conf(tmp_path, "beam_ion.conf", Np=5000))
+        bi = C.beam_ion()
+        bi.n_ip, bi.pressure, bi.surrogate = 4, 10e-9, surr
+        t = api.Tracker(C.params, C.bucket, np.full(C.nbunch, 5000), C.bunch_currents())
+        t.generate_beam(3)
+        t.enable_beam_ion(bi)
+        if surr:
+            t.use_mlp(mlp)
+        t.prepare()
+        amp[surr] = analysis.centroid_amplitude(t.run(450), "VER")
+        t.close()
+    w = analysis.exponential_window(amp[0])
+    assert w is not None and w[1] - w[0] >= 50, w
+    k0, k1 = analysis.growth_rate(amp[0], w), analysis.growth_rate(amp[1], w)
+    print("growth rate per turn: Faddeeva %.5e, learned %.5e (turns %d..%d)" % (k0, k1, w[0], w[1]))
+    assert k0 > 0 and abs(k1 - k0) <= 0.01 * k0

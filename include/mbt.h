@@ -514,6 +514,37 @@ int mbt_mlp_targets_dev(long n, const float *abr_dev, float *t_dev, void *stream
 int mbt_mlp_train(mbt_mlp *m, long nsamples, int batch, int steps, float lr,
                   uint64_t seed, float *loss_hist);
 
+/* ---- coherent tune analysis ------------------------------------------ */
+
+/* Normalised tune spectra of nseries centroid histories on the GPU
+ * (replaces the transforms of get_tunepeaks_coherent, tune.c:144-328):
+ * history s at x_dev + s * ld (device, FP64), nturn turns, a power of two.
+ *   plane 0 (LON): |DFT| / nturn of the nturn points, bin 0 halved,
+ *     normalised by the maximum over bins 1 .. nturn/2; nturn/2 + 1 bins
+ *     per history, bin 0 set to 0 (tune.c:177-197); nturn <= 4096.
+ *   plane 1, 2 (HOR, VER): |FFT| of the history zero-padded to 2 nturn,
+ *     bins 0 .. nturn-1 (bin j at j / (2 nturn) per turn) normalised by
+ *     their maximum (tune.c:240-276); nturn <= 2048.  Bin 0 is |Re X_0|:
+ *     the reference reads past its array there.
+ * spec_dev receives the spectra one after the other.  A history that is 0
+ * everywhere gives 0.  stream: a cudaStream_t or NULL. */
+int mbt_tune_spectra_dev(const double *x_dev, long ld, int nseries, int nturn, int plane,
+                         double *spec_dev, void *stream);
+
+/* Peaks of one normalised spectrum (host; identify_tunepeaks,
+ * tune.c:383-480): bins that stand 0.2 above both neighbours (pcase 1) or
+ * plateaus within 0.2 that end 0.2 lower (pcase 2, at their middle),
+ * refined by a parabola through three bins; value = peak bin / nrev, as
+ * the reference reports it.  nrev is the history length: the search runs
+ * over bins 1 .. nrev/2 - 2 (for the padded HOR / VER spectra that is the
+ * lower half, and value is twice the frequency of the bin).  At most
+ * min(10, max_peaks) peaks; value, ampli, pcase (may be NULL) hold
+ * max_peaks entries.  A plateau of exactly equal bins gives NaN (0/0 in
+ * the parabola), as in the reference.  Returns the number of peaks or
+ * MBT_ERR_INVALID. */
+int mbt_tune_peaks(const double *spec, long nrev, double *value, double *ampli, int *pcase,
+                   int max_peaks);
+
 /* ---- output files (C host; the reference's text formats) ------------- */
 
 /* A writer produces, in work_path, the files the reference's manager and

@@ -52,3 +52,29 @@ def growth_rate(amp, window, baseline_turns=50):
     turns = np.arange(first, last + 1)
     coh = np.sqrt(np.maximum(a[first:last + 1] ** 2 - base * base, 1e-300))
     return float(np.polyfit(turns, np.log(coh), 1)[0])
+
+
+def coherent_tunes(stats, plane="VER", nturn=None, max_peaks=10):
+    """Coherent tunes of every bunch from the centroid history of `plane`
+    (get_tunepeaks_coherent and identify_tunepeaks of tune.c, the spectra on
+    the GPU): the last nturn turns (a power of two; the largest one that
+    fits by default).  Returns per bunch a list of (tune, amplitude) with the
+    tune as a fraction of the revolution frequency; for HOR and VER the
+    reference's value (bin / nturn of the spectrum zero-padded to 2 nturn)
+    is halved to give that fraction."""
+    import torch
+    from . import api
+    s = np.asarray(stats)
+    n = nturn or 1 << int(np.floor(np.log2(s.shape[0])))
+    hist = np.ascontiguousarray(s[-n:, :, PLANE_COLUMN[plane]].T)
+    pl = PLANE_COLUMN[plane]
+    nout = n // 2 + 1 if pl == 0 else n
+    x = torch.as_tensor(hist, dtype=torch.float64, device="cuda")
+    spec = torch.zeros((hist.shape[0], nout), dtype=torch.float64, device="cuda")
+    api.tune_spectra_dev(x.data_ptr(), n, hist.shape[0], n, pl, spec.data_ptr(), None)
+    torch.cuda.synchronize()
+    out = []
+    for row in spec.cpu().numpy():
+        v, a, _ = api.tune_peaks(row, n, max_peaks)
+        out.append([(float(t) / (1.0 if pl == 0 else 2.0), float(m)) for t, m in zip(v, a)])
+    return out

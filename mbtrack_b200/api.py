@@ -29,6 +29,8 @@ SIGNATURES = {
     "mbt_config_error": (ctypes.c_char_p, []),
     "mbt_bunch_current": (ctypes.c_double, [_P(MbtParams), ctypes.c_int, ctypes.c_double]),
     "mbt_rw_first_bin": (ctypes.c_int, [ctypes.c_double, _P(ctypes.c_double), _P(ctypes.c_double)]),
+    "mbt_tune_spectra_dev": (ctypes.c_int, [_vp, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "mbt_tune_peaks": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp, _vp, ctypes.c_int]),
     "mbt_create": (ctypes.c_int, [_P(MbtParams), ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp,
                                   ctypes.c_int, ctypes.c_uint64, _P(_vp)]),
     "mbt_destroy": (ctypes.c_int, [_vp]),
@@ -436,6 +438,24 @@ def rw_first_bin(u):
     if lib().mbt_rw_first_bin(float(u), ctypes.byref(a), ctypes.byref(b)) != 0:
         raise MbtError(MBT_ERR_INVALID, "bin of %g s0 is narrower than 19.8 s0" % u)
     return a.value, b.value
+
+
+def tune_spectra_dev(x_ptr, ld, nseries, nturn, plane, spec_ptr, stream=None):
+    """Normalised tune spectra of device centroid histories (mbt_tune_spectra_dev)."""
+    _gchk(lib().mbt_tune_spectra_dev(x_ptr, ld, nseries, nturn, plane, spec_ptr, stream))
+
+
+def tune_peaks(spec, nrev, max_peaks=10):
+    """(values, amplitudes, cases) of the peaks of one normalised spectrum
+    (mbt_tune_peaks)."""
+    s = np.ascontiguousarray(spec, dtype=np.float64)
+    v = np.zeros(max_peaks)
+    a = np.zeros(max_peaks)
+    c = np.zeros(max_peaks, dtype=np.int32)
+    n = lib().mbt_tune_peaks(_ptr(s), nrev, _ptr(v), _ptr(a), _ptr(c), max_peaks)
+    if n < 0:
+        raise MbtError(n, "tune peaks: bad argument")
+    return v[:n], a[:n], c[:n]
 
 
 def wofz_dev(x_ptr, y_ptr, re_ptr, im_ptr, n, flag_ptr=None, stream=None):

@@ -23,7 +23,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr
 # host C: no contraction of multiply-adds, as in the reference's x86-64 build
 CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include")]
 
-CU_SOURCES = ["mbt_runtime.cu", "mbt_step.cu", "mbt_fields.cu", "mbt_mlp.cu"]
+CU_SOURCES = ["mbt_runtime.cu", "mbt_step.cu", "mbt_fields.cu", "mbt_mlp.cu", "mbt_tune.cu"]
 # per-file extra flags: w(z) and the BE field keep every multiply and add
 # separately rounded, as the reference's x86-64 build does
 CU_EXTRA = {"mbt_fields.cu": ["-fmad=false"]}

@@ -847,3 +847,75 @@ int refh_output_info(long *nrev_scan, long *nrev_pot, int *ampinv_out, int *bunc
   for (i = 0; i < track.Nbunch_out && i < cap; i++) bunch_out[i] = track.bunch_out[i];
   return track.Nbunch_out;
 }
+
+/* ------------------------------------------------------------------ */
+/* Coherent tune analysis (tune.c) of the reference on given data      */
+
+#include "tune.h"
+
+/* tune.c:144, not declared in tune.h */
+int get_tunepeaks_coherent(tuneC_t *tune, plane_t pl, FILE *fp);
+
+static int tune_setup(tuneC_t *T, int Nt)
+{
+  const int N = 1 << Nt;
+  memset(T, 0, sizeof(*T));
+  T->Nt = Nt;
+  T->xt_tune_C = (double *) calloc(N, sizeof(double));
+  T->xx_tune_C = (double *) calloc(N, sizeof(double));
+  T->xz_tune_C = (double *) calloc(N, sizeof(double));
+  T->tunes = (double *) calloc(N, sizeof(double));
+  T->pk_numbr = (unsigned *) calloc(N > 3 ? N : 3, sizeof(unsigned));
+  T->pk_value = (double *) calloc((size_t) (N > 3 ? N : 3) * 10, sizeof(double));
+  T->pk_ampli = (double *) calloc((size_t) (N > 3 ? N : 3) * 10, sizeof(double));
+  return T->xt_tune_C && T->xx_tune_C && T->xz_tune_C && T->tunes && T->pk_numbr && T->pk_value && T->pk_ampli
+             ? 0 : -1;
+}
+
+static int tune_collect(tuneC_t *T, int pl, FILE *fp, char *text, double *value, double *ampli, int cap)
+{
+  int n = 0, i;
+  const char *p;
+  fclose(fp);
+  for (p = text; *p; p++)
+    if (p[0] == '\n' && p[1] == ' ') n++;      /* one line " rev Pl i pcase value ampli" per peak */
+  for (i = 0; i < n && i < cap; i++) {
+    value[i] = T->pk_value[pl * 10 + i];
+    ampli[i] = T->pk_ampli[pl * 10 + i];
+  }
+  free(T->xt_tune_C); free(T->xx_tune_C); free(T->xz_tune_C); free(T->tunes);
+  free(T->pk_numbr); free(T->pk_value); free(T->pk_ampli);
+  return n;
+}
+
+/* identify_tunepeaks (tune.c:383-480) on a normalised spectrum cofu of
+ * nrev/2 + 1 bins; the printed lines go to text.  Returns the peak count. */
+int refh_tune_identify(const double *cofu, long nrev, int pl, double *value, double *ampli, int cap, char *text,
+                       int textcap)
+{
+  tuneC_t T;
+  FILE *fp;
+  double *buf;
+  if (tune_setup(&T, 2)) return -1;
+  buf = (double *) malloc((size_t) (nrev / 2 + 2) * sizeof(double));
+  memcpy(buf, cofu, (size_t) (nrev / 2 + 1) * sizeof(double));
+  memset(text, 0, textcap);
+  fp = fmemopen(text, textcap - 1, "w");
+  identify_tunepeaks(&T, buf, (unsigned) pl, (unsigned long) nrev, fp);
+  free(buf);
+  return tune_collect(&T, pl, fp, text, value, ampli, cap);
+}
+
+/* The LON branch of get_tunepeaks_coherent (tune.c:175-233) on a centroid
+ * history of 2^Nt turns. */
+int refh_tune_lon(const double *xt, int Nt, double *value, double *ampli, int cap, char *text, int textcap)
+{
+  tuneC_t T;
+  FILE *fp;
+  if (tune_setup(&T, Nt)) return -1;
+  memcpy(T.xt_tune_C, xt, (size_t) (1 << Nt) * sizeof(double));
+  memset(text, 0, textcap);
+  fp = fmemopen(text, textcap - 1, "w");
+  get_tunepeaks_coherent(&T, LON, fp);
+  return tune_collect(&T, LON, fp, text, value, ampli, cap);
+}

@@ -344,7 +344,30 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
     // ---- moments (statistics.c:91-128): shifted sums of the updated chunk,
     //      one coordinate column per warp (the bulk store only reads it too)
     const int nlive = min(kChunk, tile.count - c * kChunk);
-    if (warp < 6) {
+    if (nlive == kChunk) {
+      // full chunk: two elements per lane and load, no bounds test
+      if (warp < 6) {
+        const double2 *col = reinterpret_cast<const double2 *>(st + (size_t)warp * kChunk);
+#pragma unroll
+        for (int q = 0; q < kChunk / 64; ++q) {
+          const double2 v = col[q * 32 + lane];
+          const double d0 = v.x - col_shift, d1 = v.y - col_shift;
+          col_s += d0;
+          col_q += d0 * d0;
+          col_s += d1;
+          col_q += d1 * d1;
+        }
+      } else {
+        const double2 *ca = reinterpret_cast<const double2 *>(st + (size_t)cx * kChunk);
+        const double2 *cb = reinterpret_cast<const double2 *>(st + (size_t)(cx + 3) * kChunk);
+#pragma unroll
+        for (int q = 0; q < kChunk / 64; ++q) {
+          const double2 va = ca[q * 32 + lane], vb = cb[q * 32 + lane];
+          col_s += (va.x - sh_a) * (vb.x - sh_b);
+          col_s += (va.y - sh_a) * (vb.y - sh_b);
+        }
+      }
+    } else if (warp < 6) {
       const double *col = st + (size_t)warp * kChunk;
 #pragma unroll
       for (int q = 0; q < kChunk / 32; ++q) {

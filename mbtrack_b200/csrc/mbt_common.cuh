@@ -58,6 +58,28 @@ __device__ __forceinline__ void sincos_near(double d, double S, double C, double
   c = C + fma(C, cm1, -(S * sd));
 }
 
+// The same with the d^11 / d^12 series for every |d| <= 0.25, no branch
+// (for offsets that spread over both ranges within a warp, where the two
+// branches would both run).
+__device__ __forceinline__ void sincos_near_full(double d, double S, double C, double &s, double &c) {
+  const double d2 = d * d;
+  double ps = -1.0 / 39916800.0;
+  ps = fma(ps, d2, 1.0 / 362880.0);
+  ps = fma(ps, d2, -1.0 / 5040.0);
+  ps = fma(ps, d2, 1.0 / 120.0);
+  ps = fma(ps, d2, -1.0 / 6.0);
+  double pc = 1.0 / 479001600.0;
+  pc = fma(pc, d2, -1.0 / 3628800.0);
+  pc = fma(pc, d2, 1.0 / 40320.0);
+  pc = fma(pc, d2, -1.0 / 720.0);
+  pc = fma(pc, d2, 1.0 / 24.0);
+  pc = fma(pc, d2, -0.5);
+  const double sd = fma(d * d2, ps, d);
+  const double cm1 = pc * d2;
+  s = S + fma(S, cm1, C * sd);
+  c = C + fma(C, cm1, -(S * sd));
+}
+
 // a / b for b near 1 (|b - 1| < 0.5): single-precision reciprocal refined
 // by two Newton steps (relative error ~1e-28) then one product; within one
 // rounding of the IEEE quotient.

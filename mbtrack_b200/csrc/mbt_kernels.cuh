@@ -611,6 +611,14 @@ __host__ __device__ constexpr size_t rw_window_doubles(int Nmlt, int nharm) {
   return (size_t)2 * (((size_t)(Nmlt + 1) * nharm + kRwSplit - 1) / kRwSplit + nharm);
 }
 
+// Dynamic shared memory of ring_scan (doubles): block 0 keeps 2 doubles and
+// one int per bucket, the resistive-wall blocks their window.
+__host__ __device__ constexpr size_t ring_scan_smem_doubles(int rw_long, int Nmlt, int nharm) {
+  const size_t scan = 2 * (size_t)nharm + ((size_t)nharm + 1) / 2 + 1;
+  const size_t rw = rw_long ? rw_window_doubles(Nmlt, nharm) : 0;
+  return scan > rw ? scan : rw;
+}
+
 __device__ void rw_partial_sums(const Args &a, int blk, double *win) {
   const int ngroup = (a.nbunch + kRwGroup - 1) / kRwGroup;
   const int grp = blk % ngroup, part = blk / ngroup;
@@ -628,12 +636,27 @@ __device__ void rw_partial_sums(const Args &a, int blk, double *win) {
   const int len = max(0, q1 - q0) + span;
   double *w0 = win, *w1 = win + per + h;
   const double *E0 = a.rw_e, *E1 = a.rw_e + n;
-  for (int t = threadIdx.x; t < len; t += kBlock) {
-    int idx = base0 + q0 + t;
-    idx -= (idx >= n) ? n : 0;
-    idx -= (idx >= n) ? n : 0;
-    w0[t] = E0[idx];
-    w1[t] = E1[idx];
+  // the window, 8 loads per thread in flight at a time (the loads, not the
+  // arithmetic, set this kernel's time)
+  for (int t0 = threadIdx.x; t0 < len; t0 += 8 * kBlock) {
+    double va[8], vb[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = min(t0 + u * kBlock, len - 1);   // in range for every u
+      int idx = base0 + q0 + t;
+      idx -= (idx >= n) ? n : 0;
+      idx -= (idx >= n) ? n : 0;
+      va[u] = E0[idx];
+      vb[u] = E1[idx];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * kBlock;
+      if (t < len) {
+        w0[t] = va[u];
+        w1[t] = vb[u];
+      }
+    }
   }
   __syncthreads();
   int dk[kRwGroup];
@@ -704,8 +727,24 @@ __global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init
   __syncthreads();
   const int chunk = (h + 31) / 32;
   const int m0 = min(lane * chunk, h), m1 = min(m0 + chunk, h);
+  // the scan's per-bucket inputs, loaded once by the whole block (the scan
+  // itself walks them serially per lane): bunch of each bucket and the
+  // in-bucket phasor after the bunch's last bin
+  double *su = dyn;                                   // h x 2
+  int *sbi = reinterpret_cast<int *>(dyn + 2 * h);    // h
   for (int r = 0; r < a.nlr; ++r) {
     const LrConst &L = a.lr[r];
+    __syncthreads();
+    for (int i = threadIdx.x; i < h; i += kBlock) {
+      const int bi = a.bucket_bunch[i];
+      sbi[i] = bi;
+      if (bi >= 0) {
+        const double *u = a.lr_u + ((size_t)r * a.nbunch + bi) * a.ncell * 2 + 2 * (a.ncell - 1);
+        su[2 * i] = u[0];
+        su[2 * i + 1] = u[1];
+      }
+    }
+    __syncthreads();
     const bool fb = L.fb && fb_live;
     const double G0 = L.gap[0] * L.gap[1], G1 = L.gap[0] * L.gap[2];
     const double E0 = L.emp[0] * L.emp[1], E1 = L.emp[0] * L.emp[2];
@@ -716,10 +755,11 @@ __global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init
       if (warp == 0) {
         Aff f = aff_id();
         for (int m = m0; m < m1; ++m) {
-          const int bi = a.bucket_bunch[h - m - 1];
+          const int i = h - m - 1;
+          const int bi = sbi[i];
           Aff g;
           if (bi >= 0) {
-            const double *u = a.lr_u + ((size_t)r * a.nbunch + bi) * a.ncell * 2 + 2 * (a.ncell - 1);
+            const double *u = su + 2 * i;
             g = Aff{PG0, PG1, u[0] * G0 - u[1] * G1, u[0] * G1 + u[1] * G0};
           } else {
             g = Aff{E0, E1, 0.0, 0.0};
@@ -732,13 +772,13 @@ __global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init
         double *vs = a.lr_vs + (size_t)r * h * 2;
         for (int m = m0; m < m1; ++m) {
           const int i = h - m - 1;
-          const int bi = a.bucket_bunch[i];
+          const int bi = sbi[i];
           vs[2 * i] = v0;
           vs[2 * i + 1] = v1;
           if (fb) { vbuf[4 * m] = v0; vbuf[4 * m + 1] = v1; }
           double n0, n1;
           if (bi >= 0) {
-            const double *u = a.lr_u + ((size_t)r * a.nbunch + bi) * a.ncell * 2 + 2 * (a.ncell - 1);
+            const double *u = su + 2 * i;
             const double w0 = (v0 * L.pn[0] - v1 * L.pn[1]) + u[0];
             const double w1 = (v0 * L.pn[1] + v1 * L.pn[0]) + u[1];
             n0 = w0 * G0 - w1 * G1;

@@ -236,7 +236,7 @@ int rw_blocks(const mbt_ctx *c) {
   return c->p.rw_long ? (c->nbunch + mbt::kRwGroup - 1) / mbt::kRwGroup * mbt::kRwSplit : 0;
 }
 size_t smem_scan(const mbt_ctx *c) {
-  return c->p.rw_long ? mbt::rw_window_doubles(c->p.Nmlt, c->p.nharm) * sizeof(double) : 0;
+  return mbt::ring_scan_smem_doubles(c->p.rw_long, c->p.Nmlt, c->p.nharm) * sizeof(double);
 }
 
 // The beam-ion stage of a turn: frames, ion clouds, electron kicks.
@@ -906,8 +906,8 @@ int mbt_prepare(mbt_ctx *c, double *init_stats) {
   launch_map_noise<false>(c, MBT_NOISE_NONE);
   mbt::bunch_reduce<<<c->nbunch, mbt::kBlock, smem_reduce(c), c->stream>>>(a, mbt::kReducePrologue, c->stats_init);
   if (c->nlr > 0 && c->p.lr_init_turns > 0)
-    mbt::ring_scan<<<1, mbt::kBlock, 0, c->stream>>>(a, c->p.lr_init_turns, 1, c->vbuf);
-  mbt::ring_scan<<<1, mbt::kBlock, 0, c->stream>>>(a, 1, 0, c->vbuf);
+    mbt::ring_scan<<<1, mbt::kBlock, smem_scan(c), c->stream>>>(a, c->p.lr_init_turns, 1, c->vbuf);
+  mbt::ring_scan<<<1, mbt::kBlock, smem_scan(c), c->stream>>>(a, 1, 0, c->vbuf);
   mbt::bunch_wakes<<<c->nbunch, mbt::kBlock, smem_wakes(c), c->stream>>>(a, 0);
   CK(cudaGetLastError());
   int r = sync_and_check(c);

@@ -99,6 +99,37 @@ def test_short_range_rw(tmp_path, cuda_device, libmbt):
     t.close()
 
 
+def test_ragged_and_tiny_bunches(tmp_path, cuda_device, libmbt):
+    """Ten bunches of 1 .. 20000 macroparticles (sizes that do not fill a
+    warp, a 512-particle stage or a tile; 8193 and 20000 span several
+    tiles), resistive wall and the HOM, one bunch displaced by 7 sigma in
+    time so that part of it falls outside the binning window (the
+    out-of-range counters): 25 turns against the oracle."""
+    from tests.util import small_conf as sc
+    cfg = api.Config(sc(tmp_path, "uniform_fill.conf", filling="SINGLE10", Nmlt=3, EnableQuantum=0,
+                        xxCM_offset=0.05, zzCM_offset=0.02))
+    np_ = np.array([1, 2, 31, 33, 511, 513, 1025, 4097, 8193, 20000], dtype=np.int32)
+    assert cfg.nbunch == len(np_)
+    o = Oracle(cfg.params, cfg.bucket, np_, cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh)
+    o.generate_beam()
+    X = o.get_particles(6).reshape(6, -1).copy()
+    X[0] += 7.0 * cfg.params.sigma_tau
+    o.set_particles(6, X.ravel())
+    t = api.Tracker(cfg.params, cfg.bucket, np_, cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh)
+    for i in range(cfg.nbunch):
+        t.load_particles(i, o.get_particles(i))
+    so0, st0 = o.prepare(), t.prepare()
+    so, st = o.run(25), t.run(25)
+    many = np_ >= 2                                  # one macroparticle has no rms to scale by
+    assert np.max(stats_err(st0[many], so0[many])) < STATS_TOL
+    assert np.max(stats_err(st[:, many], so[:, many])) < STATS_TOL
+    assert np.max(np.abs(st[:, 0, :3] - so[:, 0, :3])) <= 1e-12 * np.max(np.abs(so[:, 0, :3]))
+    worst = max(np.max(coord_err(t.get_particles(i), o.get_particles(i))) for i in range(cfg.nbunch))
+    assert worst < COORD_TOL, worst
+    assert t.state().n_trash_high + t.state().n_trash_low > 0
+    t.close()
+
+
 def test_single_bunch_full_size_2000_turns(tmp_path, cuda_device, libmbt):
     """Single bunch, 1e5 macroparticles, broadband resonator in three planes,
     noise off, 2000 turns: checked after 1, 10 and 2000 turns."""

@@ -67,6 +67,7 @@ struct orc_ctx {
   orc_bunch *b;
   int *filled;           /* [h] */
   double *ibunch;        /* [h] mA */
+  double *np_bucket;     /* [h] macroparticles of the bunch in each bucket (0: empty) */
   double *Gl, *Gv, *Gh;
   double *fnp_ring[3];   /* [h][ncell] */
   double *dipole;        /* [(Nmlt+2) h][2] */
@@ -179,6 +180,7 @@ orc_ctx *orc_create(const mbt_params *p, int nbunch, const int *bucket,
   o->b = (orc_bunch *) calloc(nbunch, sizeof(orc_bunch));
   o->filled = (int *) calloc(h, sizeof(int));
   o->ibunch = (double *) calloc(h, sizeof(double));
+  o->np_bucket = (double *) calloc(h, sizeof(double));
   o->Gl = (double *) calloc(nc, sizeof(double));
   o->Gv = (double *) calloc(nc, sizeof(double));
   o->Gh = (double *) calloc(nc, sizeof(double));
@@ -193,6 +195,7 @@ orc_ctx *orc_create(const mbt_params *p, int nbunch, const int *bucket,
     o->filled[b->kb] = 1;
     /* manager_weakweak.c:78: ring.Ibunch[kb] = bunch_Ib * FKILO */
     o->ibunch[b->kb] = ib[i] * FKILO;
+    o->np_bucket[b->kb] = (double) np[i];
     for (k = 0; k < 6; k++) b->c[k] = (double *) calloc(np[i] > 0 ? np[i] : 1, sizeof(double));
     rng_init(&b->rng);
     b->Vrf0 = p->Vrf0;
@@ -217,7 +220,7 @@ void orc_destroy(orc_ctx *o)
     free(o->b[i].rffb_hist); free(o->b[i].fnp); free(o->b[i].dipV); free(o->b[i].dipH);
   }
   for (k = 0; k < 3; k++) free(o->fnp_ring[k]);
-  free(o->dipole); free(o->b); free(o->filled); free(o->ibunch);
+  free(o->dipole); free(o->b); free(o->filled); free(o->ibunch); free(o->np_bucket);
   free(o->bi_frame); free(o->bi_cloud); free(o->bi_sum);
   free(o->Gl); free(o->Gv); free(o->Gh);
   free(o);
@@ -447,7 +450,7 @@ static void rffb_correct(const mbt_params *p, orc_bunch *b)
 typedef struct phasor_consts {
   double prog[2], p2b[2], pb2b[2];
   double e_gap, c_gap, s_gap, e_emp, c_emp, s_emp;
-  double fac;
+  double amp;
   int fb;
 } phasor_consts;
 
@@ -463,7 +466,7 @@ static void phasor_setup(const orc_ctx *o, const orc_bunch *b, int plane, int l,
   double tbucket = (p->T0 / hd - p->ncell * dTau);
   double C0 = -alpha, C1 = wr;
   double taubeam = 0, taub2beam = 0;
-  q->fac = Amp / b->np * FMILLI;
+  q->amp = Amp;
   q->prog[0] = exp(C0 * dTau) * cos(C1 * dTau);
   q->prog[1] = exp(C0 * dTau) * sin(C1 * dTau);
   q->fb = (b->rffb_on && plane == LON && p->rffb_resonator == l + 1);
@@ -494,11 +497,15 @@ static void phasor_pass(orc_ctx *o, orc_bunch *b, int plane, int l, const phasor
     if (q->fb)
       rffb_sample(p, b, V_new[0] * q->p2b[0] - V_new[1] * q->p2b[1], V_new[0] * q->p2b[1] + V_new[1] * q->p2b[0]);
     if (o->filled[i] == 1) {
+      /* Amp / Np * 1e-3 of the SOURCE bunch: the reference's single Np is
+         every bunch's; with per-bunch counts the charge per macroparticle
+         of the bunch whose histogram drives the phasor is Ib / its Np */
+      const double fac = q->amp / o->np_bucket[i] * FMILLI;
       for (j = 0; j < Nbin; j++) {
-        V_new[0] = (V_old[0] * q->prog[0] - V_old[1] * q->prog[1]) - o->ibunch[i] * fnp[i * Nbin + j] * q->fac;
+        V_new[0] = (V_old[0] * q->prog[0] - V_old[1] * q->prog[1]) - o->ibunch[i] * fnp[i * Nbin + j] * fac;
         V_new[1] = (V_old[0] * q->prog[1] + V_old[1] * q->prog[0]);
         if (lr_wake != NULL && i == b->kb)
-          lr_wake[j] += V_new[0] + 0.5 * o->ibunch[i] * fnp[i * Nbin + j] * q->fac;
+          lr_wake[j] += V_new[0] + 0.5 * o->ibunch[i] * fnp[i * Nbin + j] * fac;
         V_old[0] = V_new[0];
         V_old[1] = V_new[1];
       }

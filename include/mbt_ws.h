@@ -1,0 +1,141 @@
+/*
+ * mbt_ws.h -- C ABI of the slice model (BunchModel = STRONG) with fast
+ * beam-ion interaction (FBII): the weak-strong pair manager_weakstrong /
+ * worker_weakstrong that mbtrack-mpi.c:139-155 dispatches to
+ * (mbtrack-mpi.h:14-37), on one GPU.
+ *
+ * Each filled bunch is 2 Nslc + 1 longitudinal slices of fixed population
+ * (npop) carrying slice centroids (xtau, xeps, xx, xp, zz, zp).  One turn:
+ *
+ *   1. short-range step (transformSbunch_shortrange rw_weakstrong.c:10-66):
+ *      RF kick and drift of the slice xtau/xeps, slice-weighted centroids
+ *      appended to each bunch's centroid history (bunch_CM_history_append
+ *      bunch.c:95-115); the Bassetti-Erskine field of every slice on a
+ *      Ngrid x Ngrid absolute grid, and the macro-ions each slice ionises at
+ *      its local grid, pulled by the later slices of the same bunch
+ *      (fbi_weakstrong_bunch fbi_weakstrong.c:45-297);
+ *   2. one-turn betatron rotation of the slice centroids
+ *      (transformSbunch_optic rw_weakstrong.c:194-253) and, with
+ *      EnableRW_long, the long-range resistive-wall kick from the
+ *      centroid histories of all bunches (transformSbunch_longrange
+ *      rw_weakstrong.c:68-192);
+ *   3. the ion train (fbi_weakstrong_train fbi_weakstrong.c:300-451): the
+ *      ions of every bunch drift to the following bunches and are pulled
+ *      by each of their slices' fields (bilinear interpolation,
+ *      get_linearly_interpolated_Efields :454-580); each slice centroid
+ *      takes the kick of all ions present when it passes.
+ *
+ * Conventions as mbt.h: 0 = ok, negative MBT_ERR_* with the message in
+ * mbt_ws_last_error(); one context per host thread; the context owns its
+ * device memory.  Parameters and the slicing come from the host (C,
+ * libm), the turn runs on the device.
+ */
+#ifndef MBT_WS_H
+#define MBT_WS_H
+
+#include "mbt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mbt_ws_params {
+  /* ring and tracking fields the slice model reads: nharm, E0, T0, wrf,
+     Vrf0, phai0, Urad, ac, QH0, QV0, alpha1/beta1/gamma1, Lc, beffH[0],
+     beffV[0], Iring, track_plane, rw_long, Nmlt, triggerRW, nrev_tot,
+     nrev_mon (see mbt_params) */
+  mbt_params base;
+  int    nslc;          /* [distribution] Nslc: 2 nslc + 1 slices */
+  int    fbii;          /* [tracking] EnableFBII */
+  int    np;            /* [distribution] Np: macroparticles the slicing counts */
+  int    ngrid;         /* field grid points per transverse axis (5, bunch.c:818) */
+  int    ndivs;         /* local grid steps per rms size (3, bunch.c:820) */
+  double sgm_xx, sgm_zz;     /* rms sizes [mm], bunch_macroparticle_model_t units */
+  double sgmatau;       /* rms duration [s] (input.c:1806) */
+  double max_tau, dtau; /* slicing window and slice width in sgmatau: 7.0 and
+                           0.3, fixed by read_input (input.c:179-180) */
+  /* derived by mbt_ws_config_load (or the caller) */
+  double agLOCx, agLOCz;     /* local grid steps [m] (bunch.c:827-831) */
+  double agABSx, agABSz;     /* absolute grid steps = 2 x local (bunch.c:833-835) */
+  double deltT;         /* slice duration [s] = dtau sgmatau (bunch.c:849) */
+  double factBE;        /* sqrt(2 (sgm_xx^2 - sgm_zz^2)) / 1e3 [m] (worker_weakstrong.c:68) */
+  double factF;         /* e / (A m_p) for CO, A = 28 (fbi_weakstrong.c:37-41) */
+  double Ldmsgm;        /* CO ions one electron makes per turn (fbi_weakstrong.c:20-36) */
+  double Gamma;         /* Lorentz factor 1957 E0 (input.c:1562) */
+} mbt_ws_params;
+
+/* Read an mbtrack .conf file with BunchModel = STRONG: read_conf_file,
+ * setup_ring_parameters, macrop_model_setup_parameters, e_beam_setup,
+ * fbii_grid_setup_parameters (bunch.c:811-851) and fbii_model_init
+ * (fbi_weakstrong.c:18-43).  Fills *w and the fill pattern as
+ * mbt_config_load does.  fix_rw_beff != 0 reads beffH3/beffV3 for the
+ * long-range resistive wall even without EnableRW_short (the reference
+ * leaves them 0 and divides by their cube, rw_weakstrong.c:101-128).
+ * Refuses 2 Nslc + 1 > 49 slices (NCELL_MAX - 1, bunch.h:65), sgm_zz >=
+ * sgm_xx (the field formula needs a flat beam) and an untracked
+ * transverse plane. */
+int mbt_ws_config_load(const char *conf_path, int fix_rw_beff, mbt_ws_params *w,
+                       int *nbunch, int *bucket, double *ib_frac);
+
+/* Slices of a bunch of np macroparticles, soa6 = xtau[np], x[np], z[np],
+ * xeps[np], xp[np], zp[np] (SI): strong_generate_eCMs bunch_strong.c:
+ * 59-198.  Particle jp goes to slice (int)((max_tau - xtau/sgmatau) /
+ * dtau), clamped to [0, 2 nslc + 1] (the last one is an overflow cell that
+ * no slice reads); npop[S] counts them; cm4[4][S] are the slice means of
+ * x, xp, z, zp (0 for an empty slice); nofe[S][G][G] counts the particles
+ * of each slice around its centroid on the local grid (offset rounded
+ * half away from zero, clamped to +-(G-1)/2).  S = 2 nslc + 1,
+ * G = ngrid. */
+int mbt_ws_slice_beam(const mbt_ws_params *w, const double *soa6, int np,
+                      int *npop, int *nofe, double *cm4);
+
+typedef struct mbt_ws mbt_ws;
+
+/* A device context for nbunch filled bunches in buckets bucket[] (ascending)
+ * with currents ibunch[] [mA] (ring.Ibunch), all of the slicing npop / nofe
+ * (the reference's manager sends bunch0's populations to every worker,
+ * manager_weakstrong.c:61-66).  Slice state starts at zero. */
+int mbt_ws_create(const mbt_ws_params *w, int nbunch, const int *bucket,
+                  const double *ibunch, const int *npop, const int *nofe,
+                  mbt_ws **out);
+
+/* Slice state, host array [nbunch][6][S]: xtau, xeps, xx, xp, zz, zp. */
+int mbt_ws_load_slices(mbt_ws *ws, const double *slices);
+int mbt_ws_get_slices(mbt_ws *ws, double *slices);
+
+/* Run nturns turns.  Host outputs (any may be NULL), per turn t and filled
+ * bunch i:
+ *   cm[t][i][6]   slice-weighted centroids after the short-range step:
+ *                 xtau, xeps, x, xp, z, zp (the x, xp, z, zp four are the
+ *                 history entry, manager_weakstrong.c:120-127);
+ *   ion[t][i][2]  Nri-weighted centroid (x, y) [m] of the ion list after
+ *                 bunch i's train step (writeoutCMImotions
+ *                 fbi_weakstrong.c:626-646), NaN without ions;
+ *   zcm[t][nharm] mean slice zz per bucket after the turn, 0 for empty
+ *                 buckets (writeoutVCMmotionsPM2 :708-718);
+ *   stats[m][i][18] on the turns with turn % nrev_mon == 0, in order:
+ *                 pos, pos_sigma, slope, slope_sigma, ampinv, ampinv_cm,
+ *                 each (LON, HOR, VER) (bunch_strong_distribution_
+ *                 statistics bunch.c:516-549; 0 for untracked planes). */
+int mbt_ws_run_turns(mbt_ws *ws, long nturns, double *cm, double *ion,
+                     double *zcm, double *stats);
+
+/* Field grid of filled bunch ib from the last turn, exey[S G G][2] (Ex, Ey
+ * [V/m] per slice, x index, z index), and its macro-ions after the
+ * intra-bunch pull, ions5[5][S G G] (Nri, x, vx, y, vy).  Either may be
+ * NULL. */
+int mbt_ws_bunch_fields(mbt_ws *ws, int ib, double *exey, double *ions5);
+
+/* Turns done. */
+long mbt_ws_turn(const mbt_ws *ws);
+
+/* Message of the last failing call on ws (or of the last failing create
+ * when ws is NULL). */
+const char *mbt_ws_last_error(const mbt_ws *ws);
+
+void mbt_ws_destroy(mbt_ws *ws);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MBT_WS_H */

@@ -101,6 +101,21 @@ class MbtBeamIon(ctypes.Structure):
     ]
 
 
+class MbtWsParams(ctypes.Structure):
+    """mbt_ws_params (include/mbt_ws.h)."""
+    _fields_ = [
+        ("base", MbtParams),
+        ("nslc", _i), ("fbii", _i), ("np", _i), ("ngrid", _i), ("ndivs", _i),
+        ("sgm_xx", _d), ("sgm_zz", _d), ("sgmatau", _d), ("max_tau", _d), ("dtau", _d),
+        ("agLOCx", _d), ("agLOCz", _d), ("agABSx", _d), ("agABSz", _d),
+        ("deltT", _d), ("factBE", _d), ("factF", _d), ("Ldmsgm", _d), ("Gamma", _d),
+    ]
+
+    @property
+    def slices(self):
+        return 2 * self.nslc + 1
+
+
 def params_to_dict(p):
     """Flatten an MbtParams into {field: scalar or nested list}."""
     out = {}

@@ -13,7 +13,7 @@ import tempfile
 
 import numpy as np
 
-from mbtrack_b200.abi import MbtParams
+from mbtrack_b200.abi import MbtParams, MbtWsParams
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
@@ -366,6 +366,181 @@ class Reference:
         self.lib.refh_ampinv.argtypes = [ctypes.c_int, _vp]
         self.lib.refh_ampinv(ib, _ptr(out))
         return out
+
+
+class ReferenceSlices:
+    """The reference's slice model (BunchModel = STRONG) with fast beam-ion
+    interaction, run by ref_ws_harness.c.  fix_ibunch sets the bunch
+    currents the reference's slice-model manager leaves at zero."""
+
+    def __init__(self, conf, fix_ibunch=True, workdir="/tmp"):
+        so = build_reference()
+        if so is None:
+            raise RuntimeError("reference harness unavailable")
+        Reference._count += 1
+        priv = os.path.join(tempfile.gettempdir(), "libmbtref_%d_%d.so" % (os.getpid(), Reference._count))
+        shutil.copyfile(so, priv)
+        self.lib = L = ctypes.CDLL(priv, mode=getattr(os, "RTLD_LOCAL", 0))
+        os.unlink(priv)
+        L.refws_init.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
+        L.refws_info.argtypes = [_vp] * 6
+        L.refws_particles.argtypes = [_vp]
+        L.refws_get_slices.argtypes = [_vp]
+        L.refws_set_slices.argtypes = [_vp]
+        L.refws_run.argtypes = [ctypes.c_long, _vp, _vp, _vp, _vp]
+        L.refws_bunch_fields.argtypes = [ctypes.c_int, _vp, _vp]
+        L.refws_interp.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp]
+        self.nb = L.refws_init(conf.encode(), workdir.encode(), int(fix_ibunch))
+        if self.nb <= 0:
+            raise RuntimeError("refws_init failed: %d" % self.nb)
+        oi = np.zeros(9, np.int32)
+        od = np.zeros(11)
+        L.refws_info(_ptr(oi), _ptr(od), None, None, None, None)
+        self.nslc, self.slices, self.ngrid, self.offst, self.np, self.nharm, self.nmultit, self.fbii, self.rw = \
+            [int(v) for v in oi]
+        (self.agLOCx, self.agLOCz, self.agABSx, self.agABSz, self.deltT, self.factBE, self.factF, self.Ldmsgm,
+         self.sgm_xx, self.sgm_zz, self.sgmatau) = [float(v) for v in od]
+        S, G = self.slices, self.ngrid
+        self.bucket = np.zeros(self.nb, np.int32)
+        self.ibunch = np.zeros(self.nb)
+        self.npop = np.zeros(S, np.int32)
+        self.nofe = np.zeros((S, G, G), np.int32)
+        L.refws_info(_ptr(oi), _ptr(od), _ptr(self.bucket), _ptr(self.ibunch), _ptr(self.npop), _ptr(self.nofe))
+        self.nmon_done = 0
+
+    def params(self):
+        """mbt_ws_params from the reference's set-up: base through
+        refh_fill_params (the same globals), the slice-model values from
+        refws_info."""
+        w = MbtWsParams()
+        self.lib.refh_fill_params.argtypes = [_P(MbtParams)]
+        self.lib.refh_fill_params(ctypes.byref(w.base))
+        w.nslc, w.fbii, w.np, w.ngrid, w.ndivs = self.nslc, self.fbii, self.np, self.ngrid, 3
+        w.sgm_xx, w.sgm_zz, w.sgmatau, w.max_tau, w.dtau = self.sgm_xx, self.sgm_zz, self.sgmatau, 7.0, 0.3
+        w.agLOCx, w.agLOCz, w.agABSx, w.agABSz = self.agLOCx, self.agLOCz, self.agABSx, self.agABSz
+        w.deltT, w.factBE, w.factF, w.Ldmsgm = self.deltT, self.factBE, self.factF, self.Ldmsgm
+        w.Gamma = 1957.0 * w.base.E0
+        return w
+
+    def particles(self):
+        a = np.zeros((6, self.np))
+        self.lib.refws_particles(_ptr(a))
+        return a
+
+    def slices_state(self):
+        a = np.zeros((self.nb, 6, self.slices))
+        self.lib.refws_get_slices(_ptr(a))
+        return a
+
+    def set_slices(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self.lib.refws_set_slices(_ptr(a))
+
+    def run(self, nturns, nrev_mon, rev0=0):
+        """Per-turn outputs of refws_run: cm (n, nb, 6), ion (n, nb, 2),
+        zcm (n, nharm), stats (monitor turns, nb, 18)."""
+        nmon = sum(1 for r in range(rev0, rev0 + nturns) if r % nrev_mon == 0)
+        cm = np.zeros((nturns, self.nb, 6))
+        ion = np.zeros((nturns, self.nb, 2))
+        zcm = np.zeros((nturns, self.nharm))
+        st = np.zeros((max(nmon, 1), self.nb, 18))
+        rc = self.lib.refws_run(nturns, _ptr(cm), _ptr(ion), _ptr(zcm), _ptr(st))
+        if rc != 0:
+            raise RuntimeError("refws_run failed: %d" % rc)
+        return cm, ion, zcm, st[:nmon]
+
+    def bunch_fields(self, ib):
+        n = self.slices * self.ngrid * self.ngrid
+        e = np.zeros((n, 2))
+        ions = np.zeros((5, n))
+        self.lib.refws_bunch_fields(ib, _ptr(e), _ptr(ions))
+        return e, ions
+
+    def interp(self, ib, icell, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        out = np.zeros((x.size, 2))
+        self.lib.refws_interp(ib, icell, _ptr(x), _ptr(y), x.size, _ptr(out))
+        return out
+
+
+class OracleSlices:
+    """The C restatement of the slice model (ws_oracle.c)."""
+
+    def __init__(self, w, bucket, ibunch, npop, nofe):
+        self.lib = L = ctypes.CDLL(build_oracle())
+        L.ows_create.restype = _vp
+        L.ows_create.argtypes = [_P(MbtWsParams), ctypes.c_int, _vp, _vp, _vp, _vp]
+        L.ows_destroy.argtypes = [_vp]
+        L.ows_set_slices.argtypes = [_vp, _vp]
+        L.ows_get_slices.argtypes = [_vp, _vp]
+        L.ows_run.argtypes = [_vp, ctypes.c_long, _vp, _vp, _vp, _vp]
+        L.ows_bunch_fields.argtypes = [_vp, ctypes.c_int, _vp, _vp]
+        L.ows_interp_n.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp]
+        self.w = w
+        self.nb = len(bucket)
+        self.S = w.slices
+        self.nion = self.S * w.ngrid * w.ngrid
+        self.nharm = w.base.nharm
+        self.rev = 0
+        self._keep = [np.ascontiguousarray(bucket, dtype=np.int32), np.ascontiguousarray(ibunch, dtype=np.float64),
+                      np.ascontiguousarray(npop, dtype=np.int32), np.ascontiguousarray(nofe, dtype=np.int32)]
+        self.o = L.ows_create(ctypes.byref(w), self.nb, *[_ptr(a) for a in self._keep])
+        if not self.o:
+            raise RuntimeError("ows_create failed")
+
+    def __del__(self):
+        if getattr(self, "o", None):
+            self.lib.ows_destroy(self.o)
+            self.o = None
+
+    def set_slices(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self.lib.ows_set_slices(self.o, _ptr(a))
+
+    def slices_state(self):
+        a = np.zeros((self.nb, 6, self.S))
+        self.lib.ows_get_slices(self.o, _ptr(a))
+        return a
+
+    def run(self, nturns):
+        nmon = sum(1 for r in range(self.rev, self.rev + nturns) if r % self.w.base.nrev_mon == 0)
+        cm = np.zeros((nturns, self.nb, 6))
+        ion = np.zeros((nturns, self.nb, 2))
+        zcm = np.zeros((nturns, self.nharm))
+        st = np.zeros((max(nmon, 1), self.nb, 18))
+        rc = self.lib.ows_run(self.o, nturns, _ptr(cm), _ptr(ion), _ptr(zcm), _ptr(st))
+        if rc != 0:
+            raise RuntimeError("ows_run failed: %d" % rc)
+        self.rev += nturns
+        return cm, ion, zcm, st[:nmon]
+
+    def bunch_fields(self, ib):
+        e = np.zeros((self.nion, 2))
+        ions = np.zeros((5, self.nion))
+        self.lib.ows_bunch_fields(self.o, ib, _ptr(e), _ptr(ions))
+        return e, ions
+
+    def interp(self, ib, icell, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        out = np.zeros((x.size, 2))
+        self.lib.ows_interp_n(self.o, ib, icell, _ptr(x), _ptr(y), x.size, _ptr(out))
+        return out
+
+
+def slice_beam(w, soa6):
+    """ows_slice_beam: (npop[S], nofe[S, G, G], cm4[4, S]) of soa6."""
+    L = ctypes.CDLL(build_oracle())
+    L.ows_slice_beam.argtypes = [_P(MbtWsParams), _vp, ctypes.c_int, _vp, _vp, _vp]
+    soa6 = np.ascontiguousarray(soa6, dtype=np.float64)
+    S, G = w.slices, w.ngrid
+    npop = np.zeros(S, np.int32)
+    nofe = np.zeros((S, G, G), np.int32)
+    cm4 = np.zeros((4, S))
+    if L.ows_slice_beam(ctypes.byref(w), _ptr(soa6), soa6.shape[1], _ptr(npop), _ptr(nofe), _ptr(cm4)) != 0:
+        raise RuntimeError("ows_slice_beam failed")
+    return npop, nofe, cm4
 
 
 def mlp_forward(params, abr):

@@ -17,6 +17,7 @@
 #define MBT_ORACLE_H
 
 #include "mbt.h"
+#include "mbt_ws.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -90,6 +91,20 @@ int orc_enable_beam_ion(orc_ctx *o, const mbt_beam_ion *bi);
 void orc_beam_ion_clouds(const orc_ctx *o, double *clouds);
 /* unit-charge field of an elliptic Gaussian (mbt_gauss_field_dev) */
 void orc_gauss_field(double dx, double dy, double sx, double sy, double *gx, double *gy);
+
+/* ---- slice model (BunchModel = STRONG) with fast beam-ion interaction:
+ * ws_oracle.c, the restatement of manager_/worker_weakstrong.c,
+ * rw_weakstrong.c and fbi_weakstrong.c; outputs as mbt_ws.h. */
+typedef struct ows ows_t;
+int ows_slice_beam(const mbt_ws_params *w, const double *soa6, int np, int *npop, int *nofe, double *cm4);
+ows_t *ows_create(const mbt_ws_params *w, int nb, const int *bucket, const double *ibunch, const int *npop,
+                  const int *nofe);
+void ows_destroy(ows_t *o);
+void ows_set_slices(ows_t *o, const double *s);
+void ows_get_slices(const ows_t *o, double *s);
+int ows_run(ows_t *o, long nturns, double *cm, double *ion, double *zcm, double *stats);
+void ows_bunch_fields(const ows_t *o, int ib, double *exey, double *ions5);
+void ows_interp_n(const ows_t *o, int ib, int icell, const double *x, const double *y, int n, double *exey);
 
 #ifdef __cplusplus
 }

@@ -89,6 +89,9 @@ int mbt_ws_config_load(const char *conf_path, int fix_rw_beff, mbt_ws_params *w,
 int mbt_ws_slice_beam(const mbt_ws_params *w, const double *soa6, int np,
                       int *npop, int *nofe, double *cm4);
 
+/* sizeof(mbt_ws_params) as compiled into the library (binding check). */
+size_t mbt_ws_params_size(void);
+
 typedef struct mbt_ws mbt_ws;
 
 /* A device context for nbunch filled bunches in buckets bucket[] (ascending)

@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 from .abi import (MBT_ERR_INVALID, MBT_NOISE_INJECTED, MBT_NOISE_PHILOX, MBT_WRITER_OWN_AMPINV, MbtBeamIon, MbtOutputCfg,
-                  MbtParams, MbtState)
+                  MbtParams, MbtState, MbtWsParams)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmbt.so")
@@ -93,6 +93,18 @@ SIGNATURES = {
     "mbt_wofz_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mbt_be_field_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, _vp, _vp, _vp]),
+    # include/mbt_ws.h: the slice model with fast beam-ion interaction
+    "mbt_ws_params_size": (ctypes.c_size_t, []),
+    "mbt_ws_config_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _P(MbtWsParams), _vp, _vp, _vp]),
+    "mbt_ws_slice_beam": (ctypes.c_int, [_P(MbtWsParams), _vp, ctypes.c_int, _vp, _vp, _vp]),
+    "mbt_ws_create": (ctypes.c_int, [_P(MbtWsParams), ctypes.c_int, _vp, _vp, _vp, _vp, _P(_vp)]),
+    "mbt_ws_load_slices": (ctypes.c_int, [_vp, _vp]),
+    "mbt_ws_get_slices": (ctypes.c_int, [_vp, _vp]),
+    "mbt_ws_run_turns": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp, _vp, _vp]),
+    "mbt_ws_bunch_fields": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
+    "mbt_ws_turn": (ctypes.c_long, [_vp]),
+    "mbt_ws_last_error": (ctypes.c_char_p, [_vp]),
+    "mbt_ws_destroy": (None, [_vp]),
 }
 
 
@@ -117,6 +129,9 @@ def lib():
         if L.mbt_params_size() != ctypes.sizeof(MbtParams):
             raise ImportError("mbt_params layout mismatch: C %d bytes, ctypes %d bytes"
                               % (L.mbt_params_size(), ctypes.sizeof(MbtParams)))
+        if L.mbt_ws_params_size() != ctypes.sizeof(MbtWsParams):
+            raise ImportError("mbt_ws_params layout mismatch: C %d bytes, ctypes %d bytes"
+                              % (L.mbt_ws_params_size(), ctypes.sizeof(MbtWsParams)))
         _lib = L
     return _lib
 
@@ -545,3 +560,102 @@ class Mlp:
 
 def mlp_targets_dev(n, abr_ptr, tgt_ptr):
     _gchk(lib().mbt_mlp_targets_dev(n, abr_ptr, tgt_ptr, None))
+
+
+class SliceModel:
+    """The slice model (BunchModel = STRONG) with fast beam-ion interaction
+    on one GPU (include/mbt_ws.h): manager_weakstrong / worker_weakstrong
+    of the reference for every filled bunch at once."""
+
+    def __init__(self, w, bucket, ibunch, npop, nofe):
+        L = lib()
+        self.w = w
+        self.nb = len(bucket)
+        self.S = w.slices
+        self.nion = self.S * w.ngrid * w.ngrid
+        self.nharm = w.base.nharm
+        keep = [np.ascontiguousarray(bucket, dtype=np.int32), np.ascontiguousarray(ibunch, dtype=np.float64),
+                np.ascontiguousarray(npop, dtype=np.int32), np.ascontiguousarray(nofe, dtype=np.int32)]
+        h = _vp()
+        rc = L.mbt_ws_create(ctypes.byref(w), self.nb, *[_ptr(a) for a in keep], ctypes.byref(h))
+        if rc != 0:
+            raise MbtError(rc, L.mbt_ws_last_error(None).decode(errors="replace"))
+        self.h = h
+
+    @staticmethod
+    def config(path, fix_rw_beff=True):
+        """(mbt_ws_params, bucket, ib_frac) of a BunchModel = STRONG .conf."""
+        L = lib()
+        w = MbtWsParams()
+        nb = ctypes.c_int()
+        cap = 4096
+        bucket = np.zeros(cap, np.int32)
+        frac = np.zeros(cap)
+        rc = L.mbt_ws_config_load(path.encode(), int(fix_rw_beff), ctypes.byref(w), ctypes.byref(nb), _ptr(bucket),
+                                  _ptr(frac))
+        if rc != 0:
+            raise MbtError(rc, L.mbt_config_error().decode(errors="replace"))
+        return w, bucket[:nb.value].copy(), frac[:nb.value].copy()
+
+    @staticmethod
+    def slice_beam(w, soa6):
+        """mbt_ws_slice_beam: (npop[S], nofe[S, G, G], cm4[4, S])."""
+        soa6 = np.ascontiguousarray(soa6, dtype=np.float64)
+        S, G = w.slices, w.ngrid
+        npop = np.zeros(S, np.int32)
+        nofe = np.zeros((S, G, G), np.int32)
+        cm4 = np.zeros((4, S))
+        rc = lib().mbt_ws_slice_beam(ctypes.byref(w), _ptr(soa6), soa6.shape[1], _ptr(npop), _ptr(nofe), _ptr(cm4))
+        if rc != 0:
+            raise MbtError(rc, "mbt_ws_slice_beam failed")
+        return npop, nofe, cm4
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise MbtError(rc, lib().mbt_ws_last_error(self.h).decode(errors="replace"))
+
+    def load_slices(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.shape == (self.nb, 6, self.S)
+        self._chk(lib().mbt_ws_load_slices(self.h, _ptr(a)))
+
+    def slices(self):
+        a = np.zeros((self.nb, 6, self.S))
+        self._chk(lib().mbt_ws_get_slices(self.h, _ptr(a)))
+        return a
+
+    @property
+    def turn(self):
+        return lib().mbt_ws_turn(self.h)
+
+    def run(self, nturns, outputs=True):
+        """Run nturns turns; returns (cm, ion, zcm, stats) as mbt_ws_run_turns
+        fills them (None each when outputs is False)."""
+        if not outputs:
+            self._chk(lib().mbt_ws_run_turns(self.h, nturns, None, None, None, None))
+            return None, None, None, None
+        t0 = self.turn
+        nmon = sum(1 for r in range(t0, t0 + nturns) if r % self.w.base.nrev_mon == 0)
+        cm = np.zeros((nturns, self.nb, 6))
+        ion = np.zeros((nturns, self.nb, 2))
+        zcm = np.zeros((nturns, self.nharm))
+        st = np.zeros((max(nmon, 1), self.nb, 18))
+        self._chk(lib().mbt_ws_run_turns(self.h, nturns, _ptr(cm), _ptr(ion), _ptr(zcm), _ptr(st)))
+        return cm, ion, zcm, st[:nmon]
+
+    def bunch_fields(self, ib):
+        e = np.zeros((self.nion, 2))
+        ions = np.zeros((5, self.nion))
+        self._chk(lib().mbt_ws_bunch_fields(self.h, ib, _ptr(e), _ptr(ions)))
+        return e, ions
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mbt_ws_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -23,10 +23,10 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr
 # host C: no contraction of multiply-adds, as in the reference's x86-64 build
 CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include")]
 
-CU_SOURCES = ["mbt_runtime.cu", "mbt_step.cu", "mbt_fields.cu", "mbt_mlp.cu", "mbt_tune.cu"]
+CU_SOURCES = ["mbt_runtime.cu", "mbt_step.cu", "mbt_fields.cu", "mbt_mlp.cu", "mbt_tune.cu", "mbt_ws.cu"]
 # per-file extra flags: w(z) and the BE field keep every multiply and add
 # separately rounded, as the reference's x86-64 build does
-CU_EXTRA = {"mbt_fields.cu": ["-fmad=false"]}
+CU_EXTRA = {"mbt_fields.cu": ["-fmad=false"], "mbt_ws.cu": ["-fmad=false"]}
 C_SOURCES = ["mbt_host.c", "mbt_beam.c", "mbt_output.c"]
 # the drop-in executable for mbtrack-mpi's weak-weak runs
 CLI_SOURCE = "mbtrack_gpu.c"
@@ -49,7 +49,7 @@ def _stale(target, deps):
 
 def build(verbose_ptxas=False, force=False):
     os.makedirs(BUILD, exist_ok=True)
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "mbt.h")]
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", h) for h in ("mbt.h", "mbt_ws.h")]
     objs = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)

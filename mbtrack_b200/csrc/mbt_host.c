@@ -34,6 +34,7 @@
 #include <time.h>
 
 #include "mbt.h"
+#include "mbt_ws.h"
 
 #ifndef M_PI
 #define M_PI 3.14159265358979323846
@@ -251,12 +252,14 @@ typedef struct cfg {
   double lr_detune[MBT_MAX_LR];
   int rffb_len_raw;
   int Nslc;
+  int strong;                    /* BunchModel = STRONG (slice model) */
+  int fbii;                      /* EnableFBII */
   double q;                      /* ring->q = U0 / Vrf0 / 1e6 (input.c:1606) */
   mbt_output_cfg out;            /* output settings */
   int *bunch_out;                /* nharm: output buckets (setup_beam) */
 } cfg_t;
 
-static int read_conf(const char *path, int fix_rw_beff, cfg_t *g)
+static int read_conf(const char *path, int fix_rw_beff, int allow_strong, cfg_t *g)
 {
   conf_t C;
   mbt_params *p = &g->p;
@@ -284,7 +287,11 @@ static int read_conf(const char *path, int fix_rw_beff, cfg_t *g)
     if (g->filling < 0) snprintf(g->fill_file, sizeof g->fill_file, "%s", s);
   }
   REQ_S("tracking", "BunchModel", s);
-  if (strcmp(s, "WEAK") != 0) { r = cfg_fail("BunchModel %s: only WEAK is supported", s); goto out; }
+  if (allow_strong && strcmp(s, "STRONG") == 0) g->strong = 1;
+  else if (strcmp(s, "WEAK") != 0) {
+    r = cfg_fail("BunchModel %s: only WEAK is supported here (STRONG through mbt_ws_config_load)", s);
+    goto out;
+  }
   REQ_I("tracking", "TrackPlane_LON", &p->track_plane[0]);
   if (p->track_plane[0] == 0) { r = cfg_fail("LON tracking switched off"); goto out; }
   REQ_I("tracking", "TrackPlane_HOR", &p->track_plane[1]);
@@ -293,7 +300,7 @@ static int read_conf(const char *path, int fix_rw_beff, cfg_t *g)
   REQ_L("tracking", "NrevMon", &p->nrev_mon);
   REQ_I("tracking", "EnableRW_short", &g->enable_rw_short);
   REQ_I("tracking", "EnableRW_long", &p->rw_long);
-  REQ_I("tracking", "EnableFBII", &tmp_i);
+  REQ_I("tracking", "EnableFBII", &g->fbii);
   REQ_I("tracking", "EnableQuantum", &p->quantum);
   REQ_I("tracking", "EnableIdealHC", &p->ideal_hc);
   if (!get_int(&C, "tracking", "EnableRW_short_LON", &g->enable_rw_short_lon))
@@ -777,7 +784,7 @@ int mbt_config_load(const char *conf_path, int fix_rw_beff, mbt_params *p, int *
   if (!conf_path || !p) return MBT_ERR_INVALID;
   g = (cfg_t *) calloc(1, sizeof(cfg_t));
   if (!g) return MBT_ERR_NOMEM;
-  r = read_conf(conf_path, fix_rw_beff, g);
+  r = read_conf(conf_path, fix_rw_beff, 0, g);
   if (!r) r = setup_ring(g);
   if (!r) r = setup_tracking(g);
   if (!r) r = setup_beam(g, &nb, bucket, ib_frac);
@@ -789,6 +796,138 @@ int mbt_config_load(const char *conf_path, int fix_rw_beff, mbt_params *p, int *
   return r;
 }
 
+/* ---- slice model (BunchModel = STRONG) ------------------------------- */
+
+#define WS_E_CHARGE 1.602e-19
+#define WS_E_MASS   9.1e-31
+#define WS_MP_O_EM  1.836e3
+
+/* fbii_grid_setup_parameters bunch.c:811-851, fbii_model_init
+   fbi_weakstrong.c:18-43, worker_weakstrong.c:67-68 */
+static int ws_derive(const cfg_t *g, mbt_ws_params *w)
+{
+  double Pave, Pu20, Pm, dm, sigmam, Lu20;
+  memset(w, 0, sizeof(*w));
+  w->base = g->p;
+  w->nslc = g->Nslc;
+  w->fbii = g->fbii;
+  w->np = g->p.np_model;
+  w->ngrid = 5;
+  w->ndivs = 3;
+  w->sgm_xx = g->sgm[2];
+  w->sgm_zz = g->sgm[4];
+  w->sgmatau = g->sgm[0] / FGIGA;
+  w->max_tau = 7.0;
+  w->dtau = 0.3;
+  if (w->nslc < 0 || 2 * w->nslc + 1 > 49)
+    return cfg_fail("Nslc %d: 2 Nslc + 1 slices must be 1..49", w->nslc);
+  if (w->np < 2) return cfg_fail("Np %d: the slicing needs at least 2 macroparticles", w->np);
+  if (!(w->sgm_zz < w->sgm_xx) || !(w->sgm_zz > 0.0))
+    return cfg_fail("sgm_zz %g, sgm_xx %g: the slice field needs 0 < sgm_zz < sgm_xx", w->sgm_zz, w->sgm_xx);
+  if (!g->p.track_plane[1] || !g->p.track_plane[2])
+    return cfg_fail("the slice model needs both transverse planes tracked");
+  w->agLOCz = w->sgm_zz / ((double) w->ndivs) / FKILO;
+  w->agLOCx = w->sgm_xx / ((double) w->ndivs) / FKILO;
+  w->agABSz = 2.0 * w->agLOCz;
+  w->agABSx = 2.0 * w->agLOCx;
+  w->deltT = w->dtau * w->sgmatau;
+  w->factBE = sqrt(2 * (w->sgm_xx * w->sgm_xx - w->sgm_zz * w->sgm_zz)) / FKILO;
+  Pave = 2.7e-9;
+  Pu20 = 5 * Pave;
+  Pm = 0.15 * Pu20 / 1.3332;
+  dm = 3.22e22 * Pm;
+  sigmam = 1.78;
+  Lu20 = 354.0;
+  w->Ldmsgm = Lu20 * dm * sigmam * 1e-22;
+  w->factF = WS_E_CHARGE / (28.0 * WS_MP_O_EM * WS_E_MASS);
+  w->Gamma = 1957.0 * g->p.E0;
+  return 0;
+}
+
+int mbt_ws_config_load(const char *conf_path, int fix_rw_beff, mbt_ws_params *w, int *nbunch, int *bucket,
+                       double *ib_frac)
+{
+  cfg_t *g;
+  int r, nb = 0;
+  if (!conf_path || !w) return MBT_ERR_INVALID;
+  g = (cfg_t *) calloc(1, sizeof(cfg_t));
+  if (!g) return MBT_ERR_NOMEM;
+  r = read_conf(conf_path, fix_rw_beff, 1, g);
+  if (!r && !g->strong) r = cfg_fail("%s: BunchModel is not STRONG (use mbt_config_load)", conf_path);
+  if (!r) r = setup_ring(g);
+  if (!r) r = setup_tracking(g);
+  if (!r) r = setup_beam(g, &nb, bucket, ib_frac);
+  if (!r) r = ws_derive(g, w);
+  if (!r && nbunch) *nbunch = nb;
+  free(g);
+  return r;
+}
+
+size_t mbt_ws_params_size(void) { return sizeof(mbt_ws_params); }
+
+/* strong_generate_eCMs bunch_strong.c:117-198 */
+int mbt_ws_slice_beam(const mbt_ws_params *w, const double *soa6, int np, int *npop, int *nofe, double *cm4)
+{
+  int S, G, off, jp, c, k;
+  int *cell, *cnt;
+  double *sum;
+  if (!w || !soa6 || np < 1 || !npop || !nofe || !cm4) return MBT_ERR_INVALID;
+  S = 2 * w->nslc + 1;
+  G = w->ngrid;
+  off = (G - 1) / 2;
+  if (S < 1 || G < 1 || !(w->sgmatau > 0.0) || !(w->dtau > 0.0)) return MBT_ERR_INVALID;
+  cell = (int *) malloc((size_t) np * sizeof(int));
+  cnt = (int *) calloc((size_t) S + 1, sizeof(int));
+  sum = (double *) calloc(4 * ((size_t) S + 1), sizeof(double));
+  if (!cell || !cnt || !sum) { free(cell); free(cnt); free(sum); return MBT_ERR_NOMEM; }
+  {
+    const double *t0 = soa6, *x = soa6 + np, *z = soa6 + 2 * (size_t) np;
+    const double *xp = soa6 + 4 * (size_t) np, *zp = soa6 + 5 * (size_t) np;
+    /* slice index of each particle, counts and coordinate sums in
+       particle order (the overflow cell S collects the tail) */
+    for (jp = 0; jp < np; jp++) {
+      const double u = (w->max_tau + (-t0[jp] / w->sgmatau)) / w->dtau;
+      int ic = !(u >= 1.0) ? 0 : (u >= (double) S ? S : (int) u);
+      double *sc = sum + ic;
+      cell[jp] = ic;
+      cnt[ic]++;
+      sc[0] = sc[0] + x[jp];
+      sc[S + 1] = sc[S + 1] + xp[jp];
+      sc[2 * (S + 1)] = sc[2 * (S + 1)] + z[jp];
+      sc[3 * (S + 1)] = sc[3 * (S + 1)] + zp[jp];
+    }
+    for (c = 0; c < S; c++) {
+      npop[c] = cnt[c];
+      for (k = 0; k < 4; k++) {
+        const double v = sum[k * (S + 1) + c];
+        cm4[k * S + c] = cnt[c] ? v / cnt[c] : v;
+      }
+    }
+    /* offsets from the slice centroid in half local steps, rounded half
+       away from zero, clamped to the grid */
+    memset(nofe, 0, (size_t) S * G * G * sizeof(int));
+    for (jp = 0; jp < np; jp++) {
+      const int ic = cell[jp];
+      double ux, uz;
+      int mx, mz;
+      if (ic >= S) continue;
+      ux = 2.0 * (x[jp] - cm4[ic]) / w->agLOCx;
+      uz = 2.0 * (z[jp] - cm4[2 * S + ic]) / w->agLOCz;
+      ux = ux > 1e6 ? 1e6 : (ux < -1e6 ? -1e6 : ux);
+      uz = uz > 1e6 ? 1e6 : (uz < -1e6 ? -1e6 : uz);
+      mx = (int) ux;
+      mz = (int) uz;
+      mx = mx >= 0 ? (mx + 1) / 2 : (mx - 1) / 2;
+      mz = mz >= 0 ? (mz + 1) / 2 : (mz - 1) / 2;
+      mx = mx > off ? off : (mx < -off ? -off : mx);
+      mz = mz > off ? off : (mz < -off ? -off : mz);
+      nofe[(ic * G + mx + off) * G + mz + off]++;
+    }
+  }
+  free(cell); free(cnt); free(sum);
+  return 0;
+}
+
 int mbt_config_output(const char *conf_path, mbt_output_cfg *o, int *bunch_out)
 {
   cfg_t *g;
@@ -796,7 +935,7 @@ int mbt_config_output(const char *conf_path, mbt_output_cfg *o, int *bunch_out)
   if (!conf_path || !o) return MBT_ERR_INVALID;
   g = (cfg_t *) calloc(1, sizeof(cfg_t));
   if (!g) return MBT_ERR_NOMEM;
-  r = read_conf(conf_path, 1, g);
+  r = read_conf(conf_path, 1, 0, g);
   if (!r) r = setup_ring(g);
   if (!r) r = setup_tracking(g);
   if (!r) {
@@ -1081,7 +1220,7 @@ int mbt_config_greens(const char *conf_path, mbt_params *p, double *Gl, double *
   if (!conf_path || !p || !Gl || !Gv || !Gh) return MBT_ERR_INVALID;
   g = (cfg_t *) calloc(1, sizeof(cfg_t));
   if (!g) return MBT_ERR_NOMEM;
-  r = read_conf(conf_path, 0, g);
+  r = read_conf(conf_path, 0, 0, g);
   if (r) { free(g); return r; }
   nc = p->ncell;
   memset(Gl, 0, nc * sizeof(double));

@@ -1,0 +1,757 @@
+// mbt_ws.cu -- the slice model (BunchModel = STRONG) with fast beam-ion
+// interaction on the device: the C ABI of mbt_ws.h.
+//
+// One turn is four launches on the context's stream:
+//
+//   ws_bunch     one block per filled bunch: RF step of the slice xtau/xeps
+//                (transformSbunch_shortrange rw_weakstrong.c:24-37), the
+//                slice-weighted centroids (bunch_strong_updateCM
+//                bunch_strong.c:221-270) into the centroid history, the
+//                monitor statistics (bunch.c:516-549), the Bassetti-Erskine
+//                field grid of every slice and the bunch's own macro-ions
+//                with their pull by the later slices of the bunch
+//                (fbi_weakstrong_bunch fbi_weakstrong.c:98-290);
+//   ws_optic_rw  one block per filled bunch: one-turn rotation of the
+//                slice centroids (transformSbunch_optic rw_weakstrong.c:
+//                194-253) and the long-range resistive-wall kick of every
+//                source bunch (transformSbunch_longrange :68-192), one
+//                thread per source, added in source order;
+//   ws_train     one block per SOURCE bunch, two macro-ions per thread: the
+//                ions of that bunch travel down the train (drift between
+//                buckets, pull by each slice of each later bunch,
+//                fbi_weakstrong_train fbi_weakstrong.c:325-426); per later
+//                bunch and slice the block writes its share of the kick
+//                sum  sum_ions Nri E  to a triangular buffer, in a fixed
+//                reduction order (warp shuffles, then warps in order), so
+//                runs repeat bit for bit;
+//   ws_kick      one block per filled bunch: adds the shares of all
+//                earlier source bunches in source order and kicks each
+//                slice's xp/zp (fbi_weakstrong.c:409-416); ion-list
+//                centroid and mean slice zz for the output files.
+//
+// Ion trajectories depend only on the field grids, which the bunch step
+// fixes before the train, so the ions of different source bunches never
+// wait on one another: the train has no grid-wide synchronisation, and its
+// length is the first bunch's chain of (nbunch - 1) x slices pulls.
+//
+// The file is compiled with -fmad=false: every product and sum rounds as
+// the reference's x86-64 build does (no contraction), so the arithmetic
+// differs from the reference only where the device's sin, exp and w(z)
+// differ from glibc's in the last bits, and in the summation order of the
+// ion kick and ion centroid sums.  Constants the reference computes with
+// libm (the one-turn matrices, the resistive-wall prefactors) come from
+// the host.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "mbt.h"
+#include "mbt_ws.h"
+#include "mbt_wofz.cuh"
+
+namespace {
+
+constexpr double kCLight = 2.997925e+08;
+constexpr double kEps0 = 8.854187817620e-12;
+constexpr double kECharge = 1.602e-19;
+constexpr double kERadius = 2.819e-15;
+constexpr double kFKilo = 1.0e+03;
+constexpr double kFMega = 1.0e+06;
+constexpr double kFTera = 1.0e+12;
+constexpr int kMaxSlices = 49;
+constexpr int kMaxHist = 32;
+constexpr int kBunchThreads = 256;
+constexpr int kRwThreads = 128;
+constexpr int kKickThreads = 64;
+constexpr long kChunk = 256;   // turns per block of host outputs
+
+struct WsConst {
+  int nb, S, G, off, nion, nmt, nharm, fbii, rw_long, trigger_rw, Nmlt;
+  int track[3];
+  long nrev_mon;
+  double vrf_e0, wrf, phai0, Urad, T0, ac;
+  double alpha1[3], beta1[3], gamma1[3];
+  double v11, v12, v21, v22, h11, h12, h21, h22;   // one-turn matrices VER, HOR
+  double a11[2], a12[2];                           // history rotation HOR, VER
+  double prfrw[2], prfrw_trig[2];
+  double Pref0, Dub0, Lc, fNp;
+  double factBE, sgm_xx, sgm_zz, agLOCx, agLOCz, agABSx, agABSz, deltT, factF, Ldmsgm;
+  double fdq_den;   // 2 eps0 sqrt(pi) factBE c deltT
+  double factjp0;   // 1e2 4 pi eps0 r_e / Gamma
+  double T0h;       // T0 / h
+  double cdt;       // c deltT
+};
+
+// get_linearly_interpolated_Efields (fbi_weakstrong.c:454-580): truncated
+// grid index of (xx, yy) on the absolute grid, the neighbour on the side
+// away from the origin, linear in each axis, constant beyond the grid.
+__device__ __forceinline__ void ws_interp(const WsConst &C, const double *__restrict__ Ex,
+                                          const double *__restrict__ Ey, int icell, double xx, double yy, double &ex,
+                                          double &ey) {
+  const int off = C.off, G = C.G;
+  const bool px = xx >= 0.0, pz = yy >= 0.0;
+  int k1x = __double2int_rz(xx / C.agABSx), k1z = __double2int_rz(yy / C.agABSz), k2x, k2z;
+  if (pz) {
+    k2z = k1z < off ? k1z + 1 : k1z;
+    k1z = min(k1z, off);
+    k2z = min(k2z, off);
+  } else {
+    k2z = k1z > -off ? k1z - 1 : k1z;
+    k1z = max(k1z, -off);
+    k2z = max(k2z, -off);
+  }
+  if (px) {
+    k2x = k1x < off ? k1x + 1 : k1x;
+    k1x = min(k1x, off);
+    k2x = min(k2x, off);
+  } else {
+    k2x = k1x > -off ? k1x - 1 : k1x;
+    k1x = max(k1x, -off);
+    k2x = max(k2x, -off);
+  }
+  const int b = icell * G;
+  const int i1 = (b + k1x + off) * G + k1z + off, i2 = (b + k2x + off) * G + k1z + off;
+  const int i3 = (b + k1x + off) * G + k2z + off, i4 = (b + k2x + off) * G + k2z + off;
+  const double fx = (xx - k1x * C.agABSx) / C.agABSx;
+  const double fz = (yy - k1z * C.agABSz) / C.agABSz;
+  const double y1 = Ey[i1], y2 = Ey[i2], y3 = Ey[i3], y4 = Ey[i4];
+  const double x1 = Ex[i1], x2 = Ex[i2], x3 = Ex[i3], x4 = Ex[i4];
+  double ey5, ey6, ex5, ex6;
+  if (px) {
+    ey5 = y1 + fx * (y2 - y1);
+    ey6 = y3 + fx * (y4 - y3);
+    ex5 = x1 + fx * (x2 - x1);
+    ex6 = x3 + fx * (x4 - x3);
+  } else {
+    ey5 = y1 - fx * (y2 - y1);
+    ey6 = y3 - fx * (y4 - y3);
+    ex5 = x1 - fx * (x2 - x1);
+    ex6 = x3 - fx * (x4 - x3);
+  }
+  ey = pz ? ey5 + fz * (ey6 - ey5) : ey5 - fz * (ey6 - ey5);
+  ex = pz ? ex5 + fz * (ex6 - ex5) : ex5 - fz * (ex6 - ex5);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(kBunchThreads) ws_bunch(WsConst C, double *__restrict__ s,
+                                                         double *__restrict__ hist, const int *__restrict__ npop,
+                                                         const int *__restrict__ nofe,
+                                                         const double *__restrict__ nelec, double *__restrict__ fx,
+                                                         double *__restrict__ fy, double *__restrict__ ion,
+                                                         double *__restrict__ own, double *__restrict__ cm_out,
+                                                         double *__restrict__ st_out) {
+  extern __shared__ double sh[];   // Ex[nion], Ey[nion]
+  __shared__ double c6[6];
+  __shared__ double red[3][kBunchThreads / 32];
+  const int ib = blockIdx.x, S = C.S, n = C.nion, tid = threadIdx.x;
+  double *sl = s + (size_t)ib * 6 * S;
+  double *xtau = sl, *xeps = sl + S, *xx = sl + 2 * S, *zz = sl + 4 * S;
+  if (tid < S) {
+    const double t0 = xtau[tid], e0 = xeps[tid];
+    const double gain = C.vrf_e0 * sin(C.wrf * t0 + C.phai0);
+    xeps[tid] = e0 + gain - C.Urad;
+    xtau[tid] = t0 - e0 * C.T0 * C.ac;
+  }
+  __syncthreads();
+  if (tid < 3) {
+    const double *u = sl + 2 * tid * S, *up = u + S;
+    double uu = 0.0, ss = 0.0;
+    int np = 0;
+    for (int c = 0; c < S; ++c) {
+      const double w = (double)npop[c];
+      uu += u[c] * w;
+      ss += up[c] * w;
+      np += npop[c];
+    }
+    c6[2 * tid] = uu / (double)np;
+    c6[2 * tid + 1] = ss / (double)np;
+  }
+  __syncthreads();
+  if (cm_out && tid < 6) cm_out[(size_t)ib * 6 + tid] = c6[tid];
+  if (tid < 4) {
+    double *h = hist + ((size_t)ib * 4 + tid) * C.nmt;
+    for (int j = C.nmt - 2; j >= 0; --j) h[j + 1] = h[j];
+    h[0] = c6[2 + tid];
+  }
+  if (st_out && tid < 3) {
+    double *o = st_out + (size_t)ib * 18;
+    const int pl = tid;
+    if (!C.track[pl]) {
+      for (int k = 0; k < 6; ++k) o[3 * k + pl] = 0.0;
+    } else {
+      const double *u = sl + 2 * pl * S, *up = u + S;
+      const double pos = c6[2 * pl], slope = c6[2 * pl + 1];
+      const double g = C.gamma1[pl], a = C.alpha1[pl], be = C.beta1[pl];
+      double sq = 0.0, sp = 0.0, ai = 0.0;
+      int nw = 0;
+      for (int c = 0; c < S; ++c) {
+        const double w = (double)npop[c];
+        sq += (u[c] - pos) * (u[c] - pos) * w;
+        sp += (up[c] - slope) * (up[c] - slope) * w;
+        ai += w * (g * (u[c] * u[c]) + 2.0 * a * u[c] * up[c] + be * (up[c] * up[c]));
+        nw += npop[c];
+      }
+      o[pl] = pos;
+      o[3 + pl] = sqrt(sq / (double)nw);
+      o[6 + pl] = slope;
+      o[9 + pl] = sqrt(sp / (double)nw);
+      o[12 + pl] = ai / (double)nw;
+      o[15 + pl] = g * (pos * pos) + 2.0 * a * pos * slope + be * (slope * slope);
+    }
+  }
+  if (!C.fbii) return;
+  const int G2 = C.G * C.G;
+  const double ne = nelec[ib];
+  for (int p = tid; p < n; p += blockDim.x) {
+    const int icell = p / G2, r = p - icell * G2;
+    const int msx = r / C.G - C.off, msz = r % C.G - C.off;
+    const double dQ = ne * (double)npop[icell] * kECharge;
+    const double factdQ = dQ / C.fdq_den;
+    const double Dx = msx * C.agABSx - xx[icell];
+    const double xi1 = Dx / C.factBE, xi2 = xi1 * C.sgm_zz / C.sgm_xx;
+    const double Dy = msz * C.agABSz - zz[icell];
+    const double yi1 = Dy / C.factBE, yi2 = yi1 * C.sgm_xx / C.sgm_zz;
+    double w1r, w1i, w2r, w2i;
+    mbt::wofz_dev(xi1, yi1, w1r, w1i);
+    mbt::wofz_dev(xi2, yi2, w2r, w2i);
+    const double e = exp(-(Dx * Dx * kFMega / (2 * C.sgm_xx * C.sgm_xx) + Dy * Dy * kFMega / (2 * C.sgm_zz * C.sgm_zz)));
+    const double ex = -factdQ * (w1i - e * w2i), ey = -factdQ * (w1r - e * w2r);
+    sh[p] = ex;
+    sh[n + p] = ey;
+    fx[(size_t)ib * n + p] = ex;
+    fy[(size_t)ib * n + p] = ey;
+  }
+  __syncthreads();
+  const double convion = ne * C.Ldmsgm;
+  double sN = 0.0, sX = 0.0, sY = 0.0;
+  double *li = ion + (size_t)ib * 5 * n;
+  for (int p = tid; p < n; p += blockDim.x) {
+    const int icell = p / G2, r = p - icell * G2;
+    const int msx = r / C.G - C.off, msz = r % C.G - C.off;
+    const double N = convion * (double)nofe[p];
+    double x = xx[icell] + msx * C.agLOCx, y = zz[icell] + msz * C.agLOCz, xd = 0.0, yd = 0.0;
+    for (int c = icell + 1; c < S; ++c) {
+      double ex, ey;
+      ws_interp(C, sh, sh + n, c, x, y, ex, ey);
+      xd = xd + C.deltT * (C.factF * ex);
+      x = x + C.deltT * xd;
+      yd = yd + C.deltT * (C.factF * ey);
+      y = y + C.deltT * yd;
+    }
+    li[p] = N;
+    li[n + p] = x;
+    li[2 * n + p] = xd;
+    li[3 * n + p] = y;
+    li[4 * n + p] = yd;
+    sN += N;
+    sX += N * x;
+    sY += N * y;
+  }
+  sN = warp_sum(sN);
+  sX = warp_sum(sX);
+  sY = warp_sum(sY);
+  if ((tid & 31) == 0) {
+    red[0][tid >> 5] = sN;
+    red[1][tid >> 5] = sX;
+    red[2][tid >> 5] = sY;
+  }
+  __syncthreads();
+  if (tid < 3) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[tid][w];
+    own[(size_t)ib * 3 + tid] = v;
+  }
+}
+
+__global__ void __launch_bounds__(kRwThreads) ws_optic_rw(WsConst C, double *__restrict__ s,
+                                                         const double *__restrict__ hist,
+                                                         const double *__restrict__ ibunch,
+                                                         const int *__restrict__ bucket, long rev) {
+  extern __shared__ double dup[];   // [nb]
+  const int ib = blockIdx.x, S = C.S, tid = threadIdx.x;
+  double *sl = s + (size_t)ib * 6 * S;
+  double *xx = sl + 2 * S, *xp = sl + 3 * S, *zz = sl + 4 * S, *zp = sl + 5 * S;
+  if (tid < S) {
+    const double z = zz[tid], zq = zp[tid], x = xx[tid], xq = xp[tid];
+    zz[tid] = C.v11 * z + C.v12 * zq;
+    zp[tid] = C.v21 * z + C.v22 * zq;
+    xx[tid] = C.h11 * x + C.h12 * xq;
+    xp[tid] = C.h21 * x + C.h22 * xq;
+  }
+  if (!C.rw_long) return;
+  const int kb = bucket[ib];
+  for (int pl = 1; pl <= 2; ++pl) {
+    if (!C.track[pl]) continue;
+    __syncthreads();
+    const double prf = (C.trigger_rw && rev < 50) ? C.prfrw_trig[pl - 1] : C.prfrw[pl - 1];
+    const double a11 = C.a11[pl - 1], a12 = C.a12[pl - 1];
+    for (int jb = tid; jb < C.nb; jb += blockDim.x) {
+      double Dup = 0.0;
+      if (rev >= C.Nmlt) {
+        const int sb = bucket[jb];
+        const double *uh = hist + ((size_t)jb * 4 + (pl == 1 ? 0 : 2)) * C.nmt, *ph = uh + C.nmt;
+        double D0 = C.Lc;
+        if (sb > kb) D0 = (double)(sb - kb) * C.Dub0;
+        if (sb < kb) D0 = (double)(C.nharm + sb - kb) * C.Dub0;
+        for (int j = 0; j <= C.Nmlt; ++j) {
+          const double Dujk = D0 + (double)j * C.Lc;
+          const double Dtjk = Dujk / kCLight;
+          const double W = prf / sqrt(Dtjk);
+          const int jm = sb > kb ? j : j + 1;
+          const double u = a11 * uh[jm] + a12 * ph[jm];
+          Dup = Dup + (C.fNp * u) * W;
+        }
+        Dup = C.Pref0 * ibunch[jb] * Dup;
+      }
+      dup[jb] = Dup;
+    }
+    __syncthreads();
+    if (tid < S) {
+      double *up = pl == 1 ? xp : zp;
+      double v = up[tid];
+      for (int jb = 0; jb < C.nb; ++jb) v += dup[jb];
+      up[tid] = v;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(1024) ws_train(WsConst C, const int *__restrict__ bucket,
+                                                 const double *__restrict__ fx, const double *__restrict__ fy,
+                                                 const double *__restrict__ ion, double *__restrict__ part,
+                                                 double *__restrict__ ipart) {
+  extern __shared__ double sw[];   // [S][nw][2] kick shares, then [nw][2] centroid shares
+  const int src = blockIdx.x, tid = threadIdx.x, n = C.nion, S = C.S;
+  const int nw = blockDim.x >> 5, lane = tid & 31, wid = tid >> 5;
+  const double *li = ion + (size_t)src * 5 * n;
+  double N[2], X[2], XD[2], Y[2], YD[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int p = tid + q * blockDim.x;
+    const bool ok = p < n;
+    N[q] = ok ? li[p] : 0.0;
+    X[q] = ok ? li[n + p] : 0.0;
+    XD[q] = ok ? li[2 * n + p] : 0.0;
+    Y[q] = ok ? li[3 * n + p] : 0.0;
+    YD[q] = ok ? li[4 * n + p] : 0.0;
+  }
+  double *wsum = sw, *wcm = sw + (size_t)S * nw * 2;
+  int kbprev = bucket[src];
+  for (int k = src + 1; k < C.nb; ++k) {
+    const int kb = bucket[k];
+    const double Dt = fabs((double)(kb - kbprev)) * C.T0h;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      X[q] = X[q] + Dt * XD[q];
+      Y[q] = Y[q] + Dt * YD[q];
+    }
+    const double *Ex = fx + (size_t)k * n, *Ey = fy + (size_t)k * n;
+    for (int c = 0; c < S; ++c) {
+      double ax = 0.0, ay = 0.0;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        double ex, ey;
+        ws_interp(C, Ex, Ey, c, X[q], Y[q], ex, ey);
+        XD[q] = XD[q] + C.deltT * (C.factF * ex);
+        X[q] = X[q] + C.deltT * XD[q];
+        YD[q] = YD[q] + C.deltT * (C.factF * ey);
+        Y[q] = Y[q] + C.deltT * YD[q];
+        ax += N[q] * ex;
+        ay += N[q] * ey;
+      }
+      ax = warp_sum(ax);
+      ay = warp_sum(ay);
+      if (lane == 0) {
+        wsum[((size_t)c * nw + wid) * 2] = ax;
+        wsum[((size_t)c * nw + wid) * 2 + 1] = ay;
+      }
+    }
+    double cx = N[0] * X[0] + N[1] * X[1], cy = N[0] * Y[0] + N[1] * Y[1];
+    cx = warp_sum(cx);
+    cy = warp_sum(cy);
+    if (lane == 0) {
+      wcm[wid * 2] = cx;
+      wcm[wid * 2 + 1] = cy;
+    }
+    __syncthreads();
+    const size_t rowk = (size_t)k * (k - 1) / 2;
+    for (int t = tid; t < 2 * S; t += blockDim.x) {
+      const int c = t >> 1, comp = t & 1;
+      double v = 0.0;
+      for (int w = 0; w < nw; ++w) v += wsum[((size_t)c * nw + w) * 2 + comp];
+      part[((rowk * S) + (size_t)c * k + src) * 2 + comp] = v;
+    }
+    if (tid < 2) {
+      double v = 0.0;
+      for (int w = 0; w < nw; ++w) v += wcm[w * 2 + tid];
+      ipart[(rowk + src) * 2 + tid] = v;
+    }
+    __syncthreads();
+    kbprev = kb;
+  }
+}
+
+__global__ void __launch_bounds__(kKickThreads) ws_kick(WsConst C, const int *__restrict__ bucket,
+                                                       const int *__restrict__ npop,
+                                                       const double *__restrict__ nelec, double *__restrict__ s,
+                                                       const double *__restrict__ part,
+                                                       const double *__restrict__ ipart,
+                                                       const double *__restrict__ own, double *__restrict__ ion_out,
+                                                       double *__restrict__ zcm_out) {
+  const int k = blockIdx.x, S = C.S, tid = threadIdx.x;
+  double *sl = s + (size_t)k * 6 * S;
+  double *xp = sl + 3 * S, *zz = sl + 4 * S, *zp = sl + 5 * S;
+  const size_t rowk = (size_t)k * (k - 1) / 2;
+  if (C.fbii && k > 0 && tid < S) {
+    const int c = tid;
+    double sx = 0.0, sy = 0.0;
+    for (int src = 0; src < k; ++src) {
+      sx += part[((rowk * S) + (size_t)c * k + src) * 2];
+      sy += part[((rowk * S) + (size_t)c * k + src) * 2 + 1];
+    }
+    const double dQ = nelec[k] * (double)npop[c] * kECharge;
+    const double factjp = dQ > 0.0 ? C.factjp0 / dQ : 0.0;
+    sx = factjp * sx;
+    sy = factjp * sy;
+    xp[c] = xp[c] + C.cdt * sx;
+    zp[c] = zp[c] + C.cdt * sy;
+  }
+  if (tid == kKickThreads - 1 && ion_out) {
+    double xs = 0.0, ys = 0.0, nt = 0.0;
+    if (C.fbii) {
+      for (int src = 0; src < k; ++src) {
+        xs += ipart[(rowk + src) * 2];
+        ys += ipart[(rowk + src) * 2 + 1];
+      }
+      xs += own[(size_t)k * 3 + 1];
+      ys += own[(size_t)k * 3 + 2];
+      for (int src = 0; src <= k; ++src) nt += own[(size_t)src * 3];
+    }
+    ion_out[(size_t)k * 2] = nt == 0.0 ? NAN : xs / nt;
+    ion_out[(size_t)k * 2 + 1] = nt == 0.0 ? NAN : ys / nt;
+  }
+  if (tid == kKickThreads - 2 && zcm_out) {
+    double z = 0.0;
+    for (int c = 0; c < S; ++c) z = z + zz[c];
+    zcm_out[bucket[k]] = z / (double)S;
+  }
+}
+
+thread_local char g_ws_err[512] = "";
+
+}  // namespace
+
+struct mbt_ws {
+  mbt_ws_params w;
+  WsConst C;
+  long turn;
+  int tpb;
+  int *d_bucket, *d_npop, *d_nofe;
+  double *d_nelec, *d_ibunch;
+  double *d_s, *d_hist, *d_fx, *d_fy, *d_ion, *d_own, *d_part, *d_ipart;
+  double *d_cm, *d_io, *d_zcm, *d_st;
+  cudaStream_t stream;
+  char err[512];
+};
+
+static int ws_fail(mbt_ws *ws, int code, const char *fmt, ...) {
+  char *dst = ws ? ws->err : g_ws_err;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(dst, 512, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define WS_CUDA(ws, call)                                                                         \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) return ws_fail((ws), MBT_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+static void ws_free(mbt_ws *ws) {
+  void *ptrs[] = {ws->d_bucket, ws->d_npop, ws->d_nofe, ws->d_nelec, ws->d_ibunch, ws->d_s, ws->d_hist,
+                  ws->d_fx, ws->d_fy, ws->d_ion, ws->d_own, ws->d_part, ws->d_ipart, ws->d_cm,
+                  ws->d_io, ws->d_zcm, ws->d_st};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (ws->stream) cudaStreamDestroy(ws->stream);
+}
+
+// Constants the reference computes on its host with libm, in its operand
+// order (rw_weakstrong.c:97-128,210-229, fbi_weakstrong.c:155-156,
+// 338-339,416, bunch.c:849).
+static void ws_constants(const mbt_ws_params *w, int nb, WsConst *C) {
+  const mbt_params *p = &w->base;
+  memset(C, 0, sizeof(*C));
+  C->nb = nb;
+  C->S = 2 * w->nslc + 1;
+  C->G = w->ngrid;
+  C->off = (w->ngrid - 1) / 2;
+  C->nion = C->S * C->G * C->G;
+  C->nmt = p->Nmlt + 2;
+  C->nharm = p->nharm;
+  C->fbii = w->fbii;
+  C->rw_long = p->rw_long;
+  C->trigger_rw = p->triggerRW;
+  C->Nmlt = p->Nmlt;
+  for (int i = 0; i < 3; ++i) {
+    C->track[i] = p->track_plane[i];
+    C->alpha1[i] = p->alpha1[i];
+    C->beta1[i] = p->beta1[i];
+    C->gamma1[i] = p->gamma1[i];
+  }
+  C->nrev_mon = p->nrev_mon;
+  C->vrf_e0 = p->Vrf0 / (p->E0 * kFKilo);
+  C->wrf = p->wrf;
+  C->phai0 = p->phai0;
+  C->Urad = p->Urad;
+  C->T0 = p->T0;
+  C->ac = p->ac;
+  {
+    const double PsiV0 = 2.0 * M_PI * p->QV0 / 1.0, PsiH0 = 2.0 * M_PI * p->QH0 / 1.0;
+    const double cV = cos(PsiV0), sV = sin(PsiV0), cH = cos(PsiH0), sH = sin(PsiH0);
+    C->v11 = cV + p->alpha1[2] * sV;
+    C->v12 = p->beta1[2] * sV;
+    C->v21 = -p->gamma1[2] * sV;
+    C->v22 = cV - p->alpha1[2] * sV;
+    C->h11 = cH + p->alpha1[1] * sH;
+    C->h12 = p->beta1[1] * sH;
+    C->h21 = -p->gamma1[1] * sH;
+    C->h22 = cH - p->alpha1[1] * sH;
+  }
+  {
+    const double kappa = 1.0 / 2.8e-08;
+    const double R = p->Lc / (2.0 * M_PI);
+    for (int pl = 1; pl <= 2; ++pl) {
+      const double Psi0 = 2.0 * M_PI * (pl == 1 ? p->QH0 : p->QV0) / 1.0;
+      const double Psi = 0.0 + Psi0;
+      const double cP = cos(Psi), sP = sin(Psi);
+      const double beff3 = pow(pl == 1 ? p->beffH[0] : p->beffV[0], 3);
+      const double beff3t = pow(2.0e-3, 3);
+      C->a11[pl - 1] = cP + p->alpha1[pl] * sP;
+      C->a12[pl - 1] = +p->beta1[pl] * sP;
+      C->prfrw[pl - 1] = 2.0 * R / (beff3) / sqrt(M_PI * kappa * kEps0) / 1.0;
+      C->prfrw_trig[pl - 1] = 2.0 * R / (beff3t) / sqrt(M_PI * kappa * kEps0) / 1.0;
+    }
+    C->fNp = (double)w->np;
+    C->Pref0 = p->T0 / p->E0 / C->fNp / kFTera;
+    C->Dub0 = p->Lc / (double)p->nharm;
+    C->Lc = p->Lc;
+  }
+  C->factBE = w->factBE;
+  C->sgm_xx = w->sgm_xx;
+  C->sgm_zz = w->sgm_zz;
+  C->agLOCx = w->agLOCx;
+  C->agLOCz = w->agLOCz;
+  C->agABSx = w->agABSx;
+  C->agABSz = w->agABSz;
+  C->deltT = w->deltT;
+  C->factF = w->factF;
+  C->Ldmsgm = w->Ldmsgm;
+  C->fdq_den = 2 * kEps0 * sqrt(M_PI) * w->factBE * kCLight * w->deltT;
+  C->factjp0 = 1e+2 * 4.0 * M_PI * kEps0 * kERadius / w->Gamma;
+  C->T0h = p->T0 / (double)p->nharm;
+  C->cdt = kCLight * w->deltT;
+}
+
+extern "C" int mbt_ws_create(const mbt_ws_params *w, int nbunch, const int *bucket, const double *ibunch,
+                             const int *npop, const int *nofe, mbt_ws **out) {
+  if (!out) return ws_fail(nullptr, MBT_ERR_INVALID, "mbt_ws_create: null output pointer");
+  *out = nullptr;
+  if (!w || !bucket || !ibunch || !npop || !nofe || nbunch < 1)
+    return ws_fail(nullptr, MBT_ERR_INVALID, "mbt_ws_create: null argument or no bunch");
+  const int S = 2 * w->nslc + 1;
+  if (S < 1 || S > kMaxSlices || w->ngrid < 1 || (w->ngrid & 1) == 0)
+    return ws_fail(nullptr, MBT_ERR_INVALID, "mbt_ws_create: %d slices (1..%d), grid %d (odd)", S, kMaxSlices,
+                   w->ngrid);
+  if (w->base.Nmlt < 0 || w->base.Nmlt + 2 > kMaxHist)
+    return ws_fail(nullptr, MBT_ERR_INVALID, "mbt_ws_create: Nmlt %d (0..%d)", w->base.Nmlt, kMaxHist - 2);
+  if (w->np < 1 || w->base.nrev_mon < 1 || w->base.nharm < 1)
+    return ws_fail(nullptr, MBT_ERR_INVALID, "mbt_ws_create: Np, NrevMon and h must be positive");
+  for (int i = 0; i < nbunch; ++i)
+    if (bucket[i] < 0 || bucket[i] >= w->base.nharm || (i > 0 && bucket[i] <= bucket[i - 1]))
+      return ws_fail(nullptr, MBT_ERR_INVALID, "mbt_ws_create: buckets must ascend within 0..%d",
+                     w->base.nharm - 1);
+  const int nion = S * w->ngrid * w->ngrid;
+  if (2 * 1024 < nion) return ws_fail(nullptr, MBT_ERR_INVALID, "mbt_ws_create: %d ions per bunch", nion);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return ws_fail(nullptr, MBT_ERR_NODEVICE, "mbt_ws_create: no CUDA device");
+  mbt_ws *ws = (mbt_ws *)calloc(1, sizeof(mbt_ws));
+  if (!ws) return ws_fail(nullptr, MBT_ERR_NOMEM, "mbt_ws_create: out of host memory");
+  ws->w = *w;
+  ws_constants(w, nbunch, &ws->C);
+  ws->tpb = ((nion + 1) / 2 + 31) / 32 * 32;
+  const WsConst &C = ws->C;
+  const size_t nb = (size_t)nbunch, pairs = nb * (nb - 1) / 2;
+  std::vector<double> nelec(nb);
+  for (size_t i = 0; i < nb; ++i) nelec[i] = (ibunch[i] * w->base.T0 / (w->np * kECharge * kFKilo));
+  int rc = 0;
+#define WS_ALLOC(ptr, count)                                                                   \
+  if (!rc && cudaMalloc(&(ptr), (count) * sizeof(*(ptr))) != cudaSuccess)                     \
+    rc = ws_fail(nullptr, MBT_ERR_NOMEM, "mbt_ws_create: device allocation of %zu bytes failed", \
+                 (size_t)((count) * sizeof(*(ptr))));
+  WS_ALLOC(ws->d_bucket, nb);
+  WS_ALLOC(ws->d_npop, (size_t)S);
+  WS_ALLOC(ws->d_nofe, (size_t)nion);
+  WS_ALLOC(ws->d_nelec, nb);
+  WS_ALLOC(ws->d_ibunch, nb);
+  WS_ALLOC(ws->d_s, nb * 6 * S);
+  WS_ALLOC(ws->d_hist, nb * 4 * C.nmt);
+  WS_ALLOC(ws->d_fx, nb * nion);
+  WS_ALLOC(ws->d_fy, nb * nion);
+  WS_ALLOC(ws->d_ion, nb * 5 * nion);
+  WS_ALLOC(ws->d_own, nb * 3);
+  WS_ALLOC(ws->d_part, (pairs > 0 ? pairs : 1) * S * 2);
+  WS_ALLOC(ws->d_ipart, (pairs > 0 ? pairs : 1) * 2);
+  WS_ALLOC(ws->d_cm, (size_t)kChunk * nb * 6);
+  WS_ALLOC(ws->d_io, (size_t)kChunk * nb * 2);
+  WS_ALLOC(ws->d_zcm, (size_t)kChunk * C.nharm);
+  WS_ALLOC(ws->d_st, (size_t)kChunk * nb * 18);
+#undef WS_ALLOC
+  if (!rc && cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) != cudaSuccess)
+    rc = ws_fail(nullptr, MBT_ERR_CUDA, "mbt_ws_create: stream creation failed");
+  if (!rc) {
+    const cudaStream_t st = ws->stream;
+    bool ok = cudaMemcpyAsync(ws->d_bucket, bucket, nb * sizeof(int), cudaMemcpyHostToDevice, st) == cudaSuccess &&
+              cudaMemcpyAsync(ws->d_npop, npop, S * sizeof(int), cudaMemcpyHostToDevice, st) == cudaSuccess &&
+              cudaMemcpyAsync(ws->d_nofe, nofe, nion * sizeof(int), cudaMemcpyHostToDevice, st) == cudaSuccess &&
+              cudaMemcpyAsync(ws->d_nelec, nelec.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st) ==
+                  cudaSuccess &&
+              cudaMemcpyAsync(ws->d_ibunch, ibunch, nb * sizeof(double), cudaMemcpyHostToDevice, st) == cudaSuccess &&
+              cudaMemsetAsync(ws->d_s, 0, nb * 6 * S * sizeof(double), st) == cudaSuccess &&
+              cudaMemsetAsync(ws->d_hist, 0, nb * 4 * C.nmt * sizeof(double), st) == cudaSuccess &&
+              cudaMemsetAsync(ws->d_fx, 0, nb * nion * sizeof(double), st) == cudaSuccess &&
+              cudaMemsetAsync(ws->d_fy, 0, nb * nion * sizeof(double), st) == cudaSuccess &&
+              cudaMemsetAsync(ws->d_ion, 0, nb * 5 * nion * sizeof(double), st) == cudaSuccess &&
+              cudaMemsetAsync(ws->d_own, 0, nb * 3 * sizeof(double), st) == cudaSuccess &&
+              cudaStreamSynchronize(st) == cudaSuccess;
+    if (!ok) rc = ws_fail(nullptr, MBT_ERR_CUDA, "mbt_ws_create: upload failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  if (!rc) {
+    const size_t train_smem = ((size_t)S * (ws->tpb / 32) * 2 + (ws->tpb / 32) * 2) * sizeof(double);
+    const size_t bunch_smem = 2 * (size_t)nion * sizeof(double);
+    if (train_smem > 48 * 1024 &&
+        cudaFuncSetAttribute(ws_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem) != cudaSuccess)
+      rc = ws_fail(nullptr, MBT_ERR_CUDA, "mbt_ws_create: train shared memory %zu bytes", train_smem);
+    if (!rc && bunch_smem > 48 * 1024 &&
+        cudaFuncSetAttribute(ws_bunch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bunch_smem) != cudaSuccess)
+      rc = ws_fail(nullptr, MBT_ERR_CUDA, "mbt_ws_create: bunch shared memory %zu bytes", bunch_smem);
+    if (!rc && nb * sizeof(double) > 48 * 1024 &&
+        cudaFuncSetAttribute(ws_optic_rw, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(nb * sizeof(double))) != cudaSuccess)
+      rc = ws_fail(nullptr, MBT_ERR_CUDA, "mbt_ws_create: %zu bunches", nb);
+  }
+  if (rc) {
+    ws_free(ws);
+    free(ws);
+    return rc;
+  }
+  *out = ws;
+  return 0;
+}
+
+extern "C" int mbt_ws_load_slices(mbt_ws *ws, const double *slices) {
+  if (!ws || !slices) return ws_fail(ws, MBT_ERR_INVALID, "mbt_ws_load_slices: null argument");
+  WS_CUDA(ws, cudaMemcpyAsync(ws->d_s, slices, (size_t)ws->C.nb * 6 * ws->C.S * sizeof(double),
+                              cudaMemcpyHostToDevice, ws->stream));
+  WS_CUDA(ws, cudaStreamSynchronize(ws->stream));
+  return 0;
+}
+
+extern "C" int mbt_ws_get_slices(mbt_ws *ws, double *slices) {
+  if (!ws || !slices) return ws_fail(ws, MBT_ERR_INVALID, "mbt_ws_get_slices: null argument");
+  WS_CUDA(ws, cudaMemcpyAsync(slices, ws->d_s, (size_t)ws->C.nb * 6 * ws->C.S * sizeof(double),
+                              cudaMemcpyDeviceToHost, ws->stream));
+  WS_CUDA(ws, cudaStreamSynchronize(ws->stream));
+  return 0;
+}
+
+extern "C" int mbt_ws_run_turns(mbt_ws *ws, long nturns, double *cm, double *ion, double *zcm, double *stats) {
+  if (!ws || nturns < 0) return ws_fail(ws, MBT_ERR_INVALID, "mbt_ws_run_turns: null context or negative turns");
+  const WsConst &C = ws->C;
+  const cudaStream_t st = ws->stream;
+  const size_t nb = (size_t)C.nb, S = (size_t)C.S, n = (size_t)C.nion;
+  const size_t bunch_smem = 2 * n * sizeof(double);
+  const size_t train_smem = (S * (ws->tpb / 32) * 2 + (ws->tpb / 32) * 2) * sizeof(double);
+  long imon_total = 0;
+  for (long t0 = 0; t0 < nturns; t0 += kChunk) {
+    const long nt = nturns - t0 < kChunk ? nturns - t0 : kChunk;
+    long imon = 0;
+    if (zcm) WS_CUDA(ws, cudaMemsetAsync(ws->d_zcm, 0, (size_t)nt * C.nharm * sizeof(double), st));
+    for (long t = 0; t < nt; ++t) {
+      const long rev = ws->turn;
+      const bool mon = rev % C.nrev_mon == 0;
+      ws_bunch<<<C.nb, kBunchThreads, bunch_smem, st>>>(C, ws->d_s, ws->d_hist, ws->d_npop, ws->d_nofe, ws->d_nelec,
+                                                        ws->d_fx, ws->d_fy, ws->d_ion, ws->d_own,
+                                                        cm ? ws->d_cm + (size_t)t * nb * 6 : nullptr,
+                                                        (mon && stats) ? ws->d_st + (size_t)imon * nb * 18 : nullptr);
+      ws_optic_rw<<<C.nb, kRwThreads, nb * sizeof(double), st>>>(C, ws->d_s, ws->d_hist, ws->d_ibunch,
+                                                                  ws->d_bucket, rev);
+      if (C.fbii && C.nb > 1)
+        ws_train<<<C.nb, ws->tpb, train_smem, st>>>(C, ws->d_bucket, ws->d_fx, ws->d_fy, ws->d_ion, ws->d_part,
+                                                    ws->d_ipart);
+      ws_kick<<<C.nb, kKickThreads, 0, st>>>(C, ws->d_bucket, ws->d_npop, ws->d_nelec, ws->d_s, ws->d_part,
+                                             ws->d_ipart, ws->d_own, ion ? ws->d_io + (size_t)t * nb * 2 : nullptr,
+                                             zcm ? ws->d_zcm + (size_t)t * C.nharm : nullptr);
+      WS_CUDA(ws, cudaGetLastError());
+      if (mon) ++imon;
+      ++ws->turn;
+    }
+    if (cm)
+      WS_CUDA(ws, cudaMemcpyAsync(cm + (size_t)t0 * nb * 6, ws->d_cm, (size_t)nt * nb * 6 * sizeof(double),
+                                  cudaMemcpyDeviceToHost, st));
+    if (ion)
+      WS_CUDA(ws, cudaMemcpyAsync(ion + (size_t)t0 * nb * 2, ws->d_io, (size_t)nt * nb * 2 * sizeof(double),
+                                  cudaMemcpyDeviceToHost, st));
+    if (zcm)
+      WS_CUDA(ws, cudaMemcpyAsync(zcm + (size_t)t0 * C.nharm, ws->d_zcm, (size_t)nt * C.nharm * sizeof(double),
+                                  cudaMemcpyDeviceToHost, st));
+    if (stats && imon > 0)
+      WS_CUDA(ws, cudaMemcpyAsync(stats + (size_t)imon_total * nb * 18, ws->d_st,
+                                  (size_t)imon * nb * 18 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    WS_CUDA(ws, cudaStreamSynchronize(st));
+    imon_total += imon;
+  }
+  return 0;
+}
+
+extern "C" int mbt_ws_bunch_fields(mbt_ws *ws, int ib, double *exey, double *ions5) {
+  if (!ws || ib < 0 || ib >= ws->C.nb) return ws_fail(ws, MBT_ERR_INVALID, "mbt_ws_bunch_fields: bunch %d", ib);
+  const size_t n = (size_t)ws->C.nion;
+  if (exey) {
+    std::vector<double> ex(n), ey(n);
+    WS_CUDA(ws, cudaMemcpyAsync(ex.data(), ws->d_fx + ib * n, n * sizeof(double), cudaMemcpyDeviceToHost, ws->stream));
+    WS_CUDA(ws, cudaMemcpyAsync(ey.data(), ws->d_fy + ib * n, n * sizeof(double), cudaMemcpyDeviceToHost, ws->stream));
+    WS_CUDA(ws, cudaStreamSynchronize(ws->stream));
+    for (size_t i = 0; i < n; ++i) {
+      exey[2 * i] = ex[i];
+      exey[2 * i + 1] = ey[i];
+    }
+  }
+  if (ions5) {
+    WS_CUDA(ws, cudaMemcpyAsync(ions5, ws->d_ion + ib * 5 * n, 5 * n * sizeof(double), cudaMemcpyDeviceToHost,
+                                ws->stream));
+    WS_CUDA(ws, cudaStreamSynchronize(ws->stream));
+  }
+  return 0;
+}
+
+extern "C" long mbt_ws_turn(const mbt_ws *ws) { return ws ? ws->turn : -1; }
+
+extern "C" const char *mbt_ws_last_error(const mbt_ws *ws) { return ws ? ws->err : g_ws_err; }
+
+extern "C" void mbt_ws_destroy(mbt_ws *ws) {
+  if (!ws) return;
+  if (ws->stream) cudaStreamSynchronize(ws->stream);
+  ws_free(ws);
+  free(ws);
+}

@@ -1,5 +1,6 @@
 """libmbt.so builds, loads without a GPU, and exports every entry point
-include/mbt.h declares; calls that need a device fail with an error code."""
+include/mbt.h and include/mbt_ws.h declare; calls that need a device fail
+with an error code."""
 import ctypes
 import os
 import re
@@ -7,13 +8,13 @@ import re
 import pytest
 
 from mbtrack_b200 import api
-from mbtrack_b200.abi import MbtParams
+from mbtrack_b200.abi import MbtParams, MbtWsParams
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    text = open(os.path.join(ROOT, "include", "mbt.h")).read()
+    text = "".join(open(os.path.join(ROOT, "include", h)).read() for h in ("mbt.h", "mbt_ws.h"))
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(mbt_[a-z_]+)\s*\(", text)))
 
@@ -28,6 +29,7 @@ def test_every_declared_symbol_is_exported(libmbt):
 
 def test_params_layout(libmbt):
     assert libmbt.mbt_params_size() == ctypes.sizeof(MbtParams)
+    assert libmbt.mbt_ws_params_size() == ctypes.sizeof(MbtWsParams)
 
 
 def test_no_device_is_an_error_not_a_fallback(libmbt):

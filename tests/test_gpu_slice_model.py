@@ -1,0 +1,114 @@
+"""Slice model (BunchModel = STRONG) with fast beam-ion interaction on the
+GPU (mbt_ws.h) against the oracle (oracle/ws_oracle.c, itself bit-exact
+with the reference's functions, tests/test_slice_model.py).
+
+The device reproduces the oracle's arithmetic operation by operation
+(libmbt's mbt_ws.cu is built without multiply-add contraction); what
+differs is the last bits of sin, exp and w(z) on the device and the
+summation order of the ion kick and ion centroid sums (a fixed tree on the
+device, sequential in the reference).  Tolerances: 1e-9 of each output's
+largest magnitude after 30 turns; 1e-12 for the field grids and ions of
+one turn."""
+import os
+
+import numpy as np
+import pytest
+
+from mbtrack_b200 import api
+from oracle import binding
+from tests.util import GOLDEN, SLICE_CASES, SLICE_TURNS, slice_conf
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(tmp_path, case, **over):
+    w, bucket, frac = api.SliceModel.config(slice_conf(tmp_path, case, **over))
+    L = api.lib()
+    ib = np.array([L.mbt_bunch_current(w.base, len(bucket), float(f)) * 1e3 for f in frac])
+    g = np.load(os.path.join(GOLDEN, "slice_fbii_%s.npz" % case))
+    npop, nofe, _ = api.SliceModel.slice_beam(w, g["particles"])
+    return w, bucket, ib, npop, nofe, g
+
+
+def _close(got, want, rel, name):
+    scale = np.nanmax(np.abs(want))
+    assert np.array_equal(np.isnan(got), np.isnan(want)), name
+    err = np.nanmax(np.abs(got - want)) if want.size else 0.0
+    assert err <= rel * scale, "%s: %.3e of %.3e" % (name, err, scale)
+    return err / scale if scale else 0.0
+
+
+@pytest.mark.parametrize("case", sorted(SLICE_CASES))
+def test_device_matches_oracle(tmp_path, cuda_device, case):
+    w, bucket, ib, npop, nofe, g = _setup(tmp_path, case)
+    dev = api.SliceModel(w, bucket, ib, npop, nofe)
+    dev.load_slices(g["slices0"])
+    o = binding.OracleSlices(w, bucket, ib, npop, nofe)
+    o.set_slices(g["slices0"])
+    # one turn: field grids and the bunches' own ions
+    a = dev.run(1)
+    b = o.run(1)
+    for ibn in range(len(bucket)):
+        e1, i1 = dev.bunch_fields(ibn)
+        e2, i2 = o.bunch_fields(ibn)
+        _close(e1, e2, 1e-12, "fields %d" % ibn)
+        _close(i1, i2, 1e-12, "ions %d" % ibn)
+    for name, x, y in zip(("cm", "ion", "zcm", "stats"), a, b):
+        _close(x, y, 1e-12, name)
+    # the rest of the 30 turns, against the oracle and the reference's fixture
+    a2 = dev.run(SLICE_TURNS - 1)
+    b2 = o.run(SLICE_TURNS - 1)
+    worst = {}
+    for k, name in enumerate(("cm", "ion", "zcm", "stats")):
+        x = np.concatenate([a[k], a2[k]])
+        y = np.concatenate([b[k], b2[k]])
+        worst[name] = _close(x, y, 1e-9, name)
+        _close(x, g[name], 1e-9, name + " (reference)")
+    _close(dev.slices(), o.slices_state(), 1e-9, "slices")
+    print(case, "relative deviations:", worst)
+
+
+def test_device_runs_repeat_bit_for_bit(tmp_path, cuda_device):
+    """Fixed reduction order: two contexts give identical outputs."""
+    w, bucket, ib, npop, nofe, g = _setup(tmp_path, "train")
+    outs = []
+    for _ in range(2):
+        dev = api.SliceModel(w, bucket, ib, npop, nofe)
+        dev.load_slices(g["slices0"])
+        outs.append(dev.run(12) + (dev.slices(),))
+        dev.close()
+    for x, y in zip(*outs):
+        assert np.array_equal(x, y, equal_nan=True)
+
+
+@pytest.mark.parametrize("over", [{"EnableFBII": 0}, {"EnableRW_long": 0}, {"NrevMon": 1}],
+                         ids=["no_fbii", "no_rw", "mon_every_turn"])
+def test_device_variants(tmp_path, cuda_device, over):
+    """Beam-ion off (no ions: NaN ion centroid, resistive wall only),
+    resistive wall off, statistics every turn."""
+    w, bucket, ib, npop, nofe, g = _setup(tmp_path, "train", **over)
+    dev = api.SliceModel(w, bucket, ib, npop, nofe)
+    dev.load_slices(g["slices0"])
+    o = binding.OracleSlices(w, bucket, ib, npop, nofe)
+    o.set_slices(g["slices0"])
+    a = dev.run(15)
+    b = o.run(15)
+    for name, x, y in zip(("cm", "ion", "zcm", "stats"), a, b):
+        _close(x, y, 1e-9, name)
+    if not w.fbii:
+        assert np.isnan(a[1]).all()
+
+
+def test_chunked_outputs(tmp_path, cuda_device):
+    """A run longer than one block of host outputs (256 turns) equals the
+    same turns run in pieces."""
+    w, bucket, ib, npop, nofe, g = _setup(tmp_path, "gaps", NrevTot=600)
+    d1 = api.SliceModel(w, bucket, ib, npop, nofe)
+    d1.load_slices(g["slices0"])
+    a = d1.run(300)
+    d2 = api.SliceModel(w, bucket, ib, npop, nofe)
+    d2.load_slices(g["slices0"])
+    parts = [d2.run(n) for n in (100, 7, 193)]
+    for k in range(4):
+        assert np.array_equal(a[k], np.concatenate([p[k] for p in parts]), equal_nan=True)
+    assert d2.turn == 300

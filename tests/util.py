@@ -123,3 +123,26 @@ def stats_err(a, b):
             err[..., mean_col] = np.abs(a[..., mean_col] - b[..., mean_col]) / scale
             err[..., rms_col] = np.abs(a[..., rms_col] - b[..., rms_col]) / scale
     return err
+
+
+# Slice model (BunchModel = STRONG) cases: ten consecutive bunches of
+# 0.5 nC with the long-range resistive wall; and six bunches followed by a
+# 5 nC bunch 195 buckets later (ions drift across the gap), 41 slices, the
+# resistive-wall trigger on.
+SLICE_CASES = {
+    "train": {"Np": 2000, "NrevTot": 40},
+    "gaps": {"Np": 2000, "NrevTot": 40, "Nslc": 20, "filling": os.path.join(CONFS, "short_fill.txt"),
+             "Iring": 3.38},
+}
+SLICE_TURNS = 30
+
+
+def slice_conf(tmp_path, case, **over):
+    """A copy of tests/confs/slice_fbii.conf for SLICE_CASES[case]."""
+    keys = dict(SLICE_CASES[case])
+    keys.update(over)
+    trigger = keys.pop("triggerRW", 1 if case == "gaps" else None)
+    path = conf_with(conf("slice_fbii.conf"), os.path.join(str(tmp_path), "slice_%s.conf" % case), **keys)
+    if trigger is not None:
+        add_tracking_keys(path, triggerRW=trigger)
+    return path

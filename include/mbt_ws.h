@@ -62,6 +62,10 @@ typedef struct mbt_ws_params {
   double factF;         /* e / (A m_p) for CO, A = 28 (fbi_weakstrong.c:37-41) */
   double Ldmsgm;        /* CO ions one electron makes per turn (fbi_weakstrong.c:20-36) */
   double Gamma;         /* Lorentz factor 1957 E0 (input.c:1562) */
+  /* [distribution] as read (input units, the set-up's values for the
+     negative sigmas): sgm_xtau [ns], sgm_xeps, sgm_xx [mm], sgm_xp [mrad],
+     sgm_zz [mm], sgm_zp [mrad]; the CM offsets in the same units */
+  double sgm_in[6], cm_in[6];
 } mbt_ws_params;
 
 /* Read an mbtrack .conf file with BunchModel = STRONG: read_conf_file,
@@ -88,6 +92,17 @@ int mbt_ws_config_load(const char *conf_path, int fix_rw_beff, mbt_ws_params *w,
  * G = ngrid. */
 int mbt_ws_slice_beam(const mbt_ws_params *w, const double *soa6, int np,
                       int *npop, int *nofe, double *cm4);
+
+/* The reference's generated bunch and bunch offsets: the np = w->np
+ * particles strong_generate_eCMs draws (generate_initial_sbunch_
+ * distribution2 bunch.c:226-330 for LON, HOR, VER: Irwin-Hall normals of
+ * c_fnorm, glibc's rand() seeded as a fresh reference process seeds it)
+ * into soa6 (layout of mbt_ws_slice_beam), then the per-bunch centroid
+ * offsets of generate_initial_general_distribution2 (bunch_strong.c:13-56,
+ * seed 571030, drawn on in the same generator) into off4[nbunch][4]
+ * (x, xp, z, zp [m, rad]) -- what the manager adds to every slice of
+ * bunch i.  off4 may be NULL. */
+int mbt_ws_reference_beam(const mbt_ws_params *w, int nbunch, double *soa6, double *off4);
 
 /* sizeof(mbt_ws_params) as compiled into the library (binding check). */
 size_t mbt_ws_params_size(void);

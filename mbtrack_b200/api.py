@@ -97,6 +97,7 @@ SIGNATURES = {
     "mbt_ws_params_size": (ctypes.c_size_t, []),
     "mbt_ws_config_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _P(MbtWsParams), _vp, _vp, _vp]),
     "mbt_ws_slice_beam": (ctypes.c_int, [_P(MbtWsParams), _vp, ctypes.c_int, _vp, _vp, _vp]),
+    "mbt_ws_reference_beam": (ctypes.c_int, [_P(MbtWsParams), ctypes.c_int, _vp, _vp]),
     "mbt_ws_create": (ctypes.c_int, [_P(MbtWsParams), ctypes.c_int, _vp, _vp, _vp, _vp, _P(_vp)]),
     "mbt_ws_load_slices": (ctypes.c_int, [_vp, _vp]),
     "mbt_ws_get_slices": (ctypes.c_int, [_vp, _vp]),
@@ -609,6 +610,26 @@ class SliceModel:
         if rc != 0:
             raise MbtError(rc, "mbt_ws_slice_beam failed")
         return npop, nofe, cm4
+
+    @staticmethod
+    def reference_beam(w, nbunch):
+        """mbt_ws_reference_beam: (soa6[6, np], off4[nbunch, 4])."""
+        soa6 = np.zeros((6, w.np))
+        off4 = np.zeros((nbunch, 4))
+        rc = lib().mbt_ws_reference_beam(ctypes.byref(w), nbunch, _ptr(soa6), _ptr(off4))
+        if rc != 0:
+            raise MbtError(rc, "mbt_ws_reference_beam failed")
+        return soa6, off4
+
+    @staticmethod
+    def initial_slices(w, cm4, off4):
+        """The manager's starting slices (generate_initial_general_
+        distribution2): cm4 plus each bunch's offsets, xtau/xeps zero."""
+        nb = off4.shape[0]
+        s = np.zeros((nb, 6, w.slices))
+        for k in range(4):
+            s[:, 2 + k, :] = cm4[k][None, :] + off4[:, k][:, None]
+        return s
 
     def _chk(self, rc):
         if rc != 0:

@@ -24,6 +24,7 @@
 #include <string.h>
 
 #include "mbt.h"
+#include "mbt_ws.h"
 
 typedef struct beam_rng {
   struct random_data rd;
@@ -81,5 +82,45 @@ int mbt_reference_beam(const mbt_params *p, int bucket, int np, double *soa6)
       slope[j] = p->slope_offset[plane] + p->slope_sgm[plane] * irwin_hall12(&r, seed) + p->correlate[plane] * dpos;
     }
   }
+  return 0;
+}
+
+/* generate_initial_sbunch_distribution2 (bunch.c:226-330) for LON, HOR and
+   VER in that order, as strong_generate_eCMs calls it (bunch_strong.c:
+   80-91), then generate_initial_general_distribution2's offsets
+   (bunch_strong.c:30-44) on the same generator: one fresh process. */
+int mbt_ws_reference_beam(const mbt_ws_params *w, int nbunch, double *soa6, double *off4)
+{
+  beam_rng r;
+  const int np = w ? w->np : 0;
+  const double FN = 1.0e-09, FM = 1.0e-03;
+  int j, plane, i;
+  if (!w || !soa6 || np < 1 || nbunch < 0) return MBT_ERR_INVALID;
+  rng_open(&r);
+  for (plane = 0; plane < 3; plane++) {
+    double *pos = soa6 + (size_t) plane * np, *slope = soa6 + (size_t) (3 + plane) * np;
+    const int seed = w->base.iseed[plane];
+    const double sp = w->sgm_in[2 * plane], ss = w->sgm_in[2 * plane + 1];
+    const double cp = w->cm_in[2 * plane], cs = w->cm_in[2 * plane + 1];
+    if (np == 1) {
+      pos[0] = plane == 0 ? cp * FN : cp * FM;
+      slope[0] = plane == 0 ? cs : cs * FM;
+      continue;
+    }
+    for (j = 0; j < np; j++) {
+      if (plane == 0) {
+        pos[j] = (cp + sp * irwin_hall12(&r, seed)) * FN;
+        slope[j] = cs + ss * irwin_hall12(&r, seed);
+      } else {
+        const double u = sp * irwin_hall12(&r, seed);
+        const double v = ss * irwin_hall12(&r, seed);
+        pos[j] = u * FM;
+        slope[j] = v * FM;
+      }
+    }
+  }
+  if (off4)
+    for (i = 0; i < nbunch; i++)
+      for (j = 0; j < 4; j++) off4[4 * i + j] = w->cm_in[2 + j] * FM * irwin_hall12(&r, 571030);
   return 0;
 }

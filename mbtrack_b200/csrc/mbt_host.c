@@ -253,6 +253,7 @@ typedef struct cfg {
   int rffb_len_raw;
   int Nslc;
   int strong;                    /* BunchModel = STRONG (slice model) */
+  int ngen[3];                   /* nGen_LON/HOR/VER */
   int fbii;                      /* EnableFBII */
   double q;                      /* ring->q = U0 / Vrf0 / 1e6 (input.c:1606) */
   mbt_output_cfg out;            /* output settings */
@@ -385,6 +386,7 @@ static int read_conf(const char *path, int fix_rw_beff, int allow_strong, cfg_t 
     REQ_I("distribution", "nGen_LON", &ng[0]);
     REQ_I("distribution", "nGen_HOR", &ng[1]);
     REQ_I("distribution", "nGen_VER", &ng[2]);
+    memcpy(g->ngen, ng, sizeof ng);
     for (i = 0; i < 3; i++)
       if (!ng[i] && p->track_plane[i]) { r = cfg_fail("distribution files (nGen = 0) are not supported"); goto out; }
   }
@@ -826,6 +828,10 @@ static int ws_derive(const cfg_t *g, mbt_ws_params *w)
     return cfg_fail("sgm_zz %g, sgm_xx %g: the slice field needs 0 < sgm_zz < sgm_xx", w->sgm_zz, w->sgm_xx);
   if (!g->p.track_plane[1] || !g->p.track_plane[2])
     return cfg_fail("the slice model needs both transverse planes tracked");
+  if (!g->ngen[0] || !g->ngen[1] || !g->ngen[2])
+    return cfg_fail("the slice model generates all three planes: nGen_LON/HOR/VER must be nonzero");
+  memcpy(w->sgm_in, g->sgm, sizeof w->sgm_in);
+  memcpy(w->cm_in, g->cm, sizeof w->cm_in);
   w->agLOCz = w->sgm_zz / ((double) w->ndivs) / FKILO;
   w->agLOCx = w->sgm_xx / ((double) w->ndivs) / FKILO;
   w->agABSz = 2.0 * w->agLOCz;

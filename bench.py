@@ -1,7 +1,7 @@
 """Benchmark of the per-turn weak-weak tracking loop on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload uniform|single|uneven|beam_ion|beam_ion_mlp]
+                    [--workload uniform|single|uneven|beam_ion|beam_ion_mlp|slice_fbii]
 
 Default workload (the uniform multi-bunch configuration): all 416 buckets
 filled at 0.5 nC, 2e4 macroparticles per bunch (8.32e6, 400 MB of FP64
@@ -20,6 +20,11 @@ scaling); the time is the max over ranks.
 reference arm: the reference's own CPU code (oracle/_ref, the reference's
 sources compiled unmodified; the C restatement in oracle/ when that library
 is absent) on the host cores, bunches split across one process per core.
+
+slice_fbii: the reference's slice model (BunchModel = STRONG) with fast
+beam-ion interaction (include/mbt_ws.h) on the 200-bunch train, 47 slices per
+bunch; metric turns/s of the whole ring, the reference arm its own
+functions on one core (its ion train passes bunch to bunch in sequence).
 """
 import argparse
 import json
@@ -48,7 +53,11 @@ WORKLOADS = {
     "beam_ion_mlp": ("beam_ion.conf", {}, "beam-ion weak-strong: 200-bunch train x 5e4 macroparticles, CO at "
                                           "1 nTorr, 20 interaction points, 1000 macro-ions per passage per "
                                           "point, learned field (tensor-core MLP, 1% audit)"),
+    "slice_fbii": ("slice_fbii.conf", {"Nslc": 23, "Np": 5000, "Iring": 84.6, "NrevTot": 1000, "NrevMon": 100},
+                   "slice model (BunchModel = STRONG) with fast beam-ion interaction: 200-bunch train, 47 "
+                   "slices x 25 grid points per bunch (1175 macro-ions), long-range RW over 10 turns"),
 }
+SLICE_FLOP_PER_PULL = 40   # FP64 operations of one ion-slice pull in the reference's expressions
 BEAM_ION_CPU_SCALE = 100   # the CPU sample keeps 1/100 of the electrons and of the ions
 BYTES_PER_MP_TURN = 96   # 6 FP64 coordinates read and written per macroparticle per turn
 METRIC = "macroparticle-turns/s"
@@ -61,7 +70,7 @@ def conf_path(workload, tmpdir):
     over = dict(over)
     if "uneven" in name:
         over["filling"] = os.path.join(CONFS, "uneven_fill.txt")
-    if "beam_ion" in name:
+    if "beam_ion" in name or workload == "slice_fbii":
         over["filling"] = os.path.join(CONFS, "beam_ion_fill.txt")
     if not over:
         return src
@@ -445,6 +454,156 @@ def run_reference(args):
 
 
 
+
+def slice_setup(conf):
+    """Slice model of a BunchModel = STRONG file: the reference's generated
+    bunch, its slicing and bunch offsets (all in libmbt's host code)."""
+    from mbtrack_b200 import api
+    w, bucket, frac = api.SliceModel.config(conf)
+    L = api.lib()
+    ib = [L.mbt_bunch_current(w.base, len(bucket), float(f)) * 1e3 for f in frac]
+    soa, off = api.SliceModel.reference_beam(w, len(bucket))
+    npop, nofe, cm4 = api.SliceModel.slice_beam(w, soa)
+    return w, bucket, ib, npop, nofe, api.SliceModel.initial_slices(w, cm4, off)
+
+
+def slice_cpu(conf, turns):
+    """Seconds per turn of the reference's slice model on one core
+    (oracle/_ref; the C restatement when that library is absent)."""
+    from oracle import binding
+    import numpy as np
+    if binding.reference_available() or os.path.exists(binding.REF_SO):
+        r = binding.ReferenceSlices(conf)
+        kind = "reference"
+        t0 = time.perf_counter()
+        r.run(turns, 100)
+    else:
+        w, bucket, ib, npop, nofe, s0 = slice_setup(conf)
+        r = binding.OracleSlices(w, bucket, ib, npop, nofe)
+        r.set_slices(s0)
+        kind = "port"
+        t0 = time.perf_counter()
+        r.run(turns)
+    return (time.perf_counter() - t0) / turns, kind, r.nb
+
+
+def run_slice_b200(args):
+    import numpy as np
+    import torch
+    from mbtrack_b200 import api
+    import tempfile
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    tmp = tempfile.mkdtemp()
+    conf = conf_path(args.workload, tmp)
+    w, bucket, ib, npop, nofe, s0 = slice_setup(conf)
+    nb = len(bucket)
+    nion = w.slices * w.ngrid * w.ngrid
+    pulls = nb * (nb - 1) // 2 * nion * w.slices
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sec, kind, _ = slice_cpu(conf, 1)
+        cpu = {"value": 1.0 / sec, "unit": "turns/s", "cores": 1, "kind": kind,
+               "sample": "1 turn of the whole %d-bunch ring on one core (%.1f s)" % (nb, sec)}
+    dev = api.SliceModel(w, bucket, ib, npop, nofe)
+    dev.load_slices(s0)
+    dev.run(args.warmup, outputs=False)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        dev.run(args.steps, outputs=False)
+    torch.cuda.synchronize()
+    t_local = dev.last_ms() / 1e3
+    if dist:
+        tt = torch.tensor([t_local], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    else:
+        t_max = t_local
+    value = world * args.steps / t_max
+    prof = dev.profile(args.profile_turns)
+    # end to end through the public API: slices up from host memory, the
+    # per-turn outputs and the slices back down, every step
+    e2e_turns = 10
+    e2e_t = []
+    for _ in range(args.e2e_steps + 1):
+        t0 = time.perf_counter()
+        dev.load_slices(s0)
+        out = dev.run(e2e_turns)
+        back = dev.slices()
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_sec = float(np.mean(e2e_t[1:]))
+    if dist:
+        tt = torch.tensor([e2e_sec], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_sec = float(tt.item())
+        dist.barrier()
+        dist.destroy_process_group()
+    ok = bool(np.isfinite(back).all() and np.isfinite(out[0]).all())
+    dev.close()
+    if rank != 0:
+        return
+    peak = 37.0
+    achieved = SLICE_FLOP_PER_PULL * pulls / (prof[2] * 1e-3) / 1e12
+    line = {
+        "metric": "turns/s", "value": value, "unit": "turns/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS[args.workload][2], "bunches": nb, "slices": w.slices,
+                   "macro_ions_per_bunch": nion, "ion_slice_pulls_per_turn": pulls, "turns_per_step": 1,
+                   "l2": "state of %.1f MB fits L2; the turn is FP64-bound, not memory-bound"
+                         % (nb * nion * 7 * 8 / 1e6),
+                   "parallelism": "replicas x%d" % world},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None, "kernel": "ws_train (ion train)",
+                     "peak_source": "nominal B200 FP64 (no measured FP64 peak); FMA counted as 2",
+                     "flop_per_pull": SLICE_FLOP_PER_PULL, "launch_ms": float(prof[2])},
+        "kernels_ms_per_turn": {"ws_bunch": float(prof[0]), "ws_optic_rw": float(prof[1]),
+                                "ws_train": float(prof[2]), "ws_kick": float(prof[3])},
+        "e2e": {"value": world * e2e_turns / e2e_sec, "unit": "turns/s",
+                "h2d_bytes_per_step": nb * 6 * w.slices * 8,
+                "d2h_bytes_per_step": (e2e_turns * (nb * 8 + w.base.nharm) + nb * 6 * w.slices) * 8,
+                "turns_per_step": e2e_turns, "steps": args.e2e_steps,
+                "call": "SliceModel.load_slices + run(%d turns, outputs to host) + slices()" % e2e_turns},
+        "gpu_launches": 4 * args.steps,
+        "clocks": clk.summary(),
+        "finite": ok,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line))
+
+
+def run_slice_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    import tempfile
+    tmp = tempfile.mkdtemp()
+    conf = conf_path(args.workload, tmp)
+    turns = min(args.steps, 2)
+    sec, kind, nb = slice_cpu(conf, turns)
+    value = 1.0 / sec
+    line = {
+        "impl": "reference", "metric": "turns/s", "value": value, "unit": "turns/s", "n_gpus": world,
+        "steps": turns, "warmup": 0, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS[args.workload][2], "bunches": nb, "turns_per_step": 1,
+                   "parallelism": "1 host process"},
+        "cpu_baseline": {"value": value, "unit": "turns/s", "cores": 1, "kind": kind,
+                         "sample": "%d turns of the whole ring on one core (the ion train runs bunch after "
+                                   "bunch in the reference, manager_weakstrong.c:184-233)" % turns},
+        "e2e": {"value": value, "unit": "turns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
 def growth_check(cfg, mlp, turns):
     """Growth rate of the vertical coupled-bunch motion with the Faddeeva
     and with the learned field, same train, ions and seeds: the beam-ion
@@ -500,12 +659,14 @@ def main():
                          "Faddeeva stage over this many turns on a reduced train (0: skip)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = 20 if args.workload.startswith("beam_ion") else 200
+        args.steps = 20 if args.workload.startswith("beam_ion") or args.workload == "slice_fbii" else 200
     if args.workload.startswith("beam_ion"):
         args.cpu_turns = min(args.cpu_turns, 2)
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
-    if args.impl == "reference":
+    if args.workload == "slice_fbii":
+        (run_slice_reference if args.impl == "reference" else run_slice_b200)(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)

@@ -144,6 +144,21 @@ int mbt_ws_run_turns(mbt_ws *ws, long nturns, double *cm, double *ion,
  * NULL. */
 int mbt_ws_bunch_fields(mbt_ws *ws, int ib, double *exey, double *ions5);
 
+/* Device time [ms] of the last mbt_ws_run_turns call: CUDA events on the
+ * context's stream around its kernels (host copies of the outputs between
+ * blocks of 256 turns excluded). */
+double mbt_ws_last_ms(const mbt_ws *ws);
+
+/* Run nturns turns (no outputs) with CUDA events between the four kernels
+ * of a turn; ms4 = mean device time per turn of the bunch step, the optic
+ * and resistive-wall step, the ion train and the kick step. */
+int mbt_ws_profile(mbt_ws *ws, long nturns, double *ms4);
+
+/* The device's field-grid interpolation (get_linearly_interpolated_
+ * Efields fbi_weakstrong.c:454-580) on filled bunch ib's field grid of the
+ * last turn, slice icell, at n points (x[i], y[i]) [m]: exey[n][2]. */
+int mbt_ws_interp(mbt_ws *ws, int ib, int icell, const double *x, const double *y, int n, double *exey);
+
 /* Turns done. */
 long mbt_ws_turn(const mbt_ws *ws);
 

@@ -104,6 +104,9 @@ SIGNATURES = {
     "mbt_ws_run_turns": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp, _vp, _vp]),
     "mbt_ws_bunch_fields": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "mbt_ws_turn": (ctypes.c_long, [_vp]),
+    "mbt_ws_last_ms": (ctypes.c_double, [_vp]),
+    "mbt_ws_profile": (ctypes.c_int, [_vp, ctypes.c_long, _vp]),
+    "mbt_ws_interp": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp]),
     "mbt_ws_last_error": (ctypes.c_char_p, [_vp]),
     "mbt_ws_destroy": (None, [_vp]),
 }
@@ -663,6 +666,24 @@ class SliceModel:
         st = np.zeros((max(nmon, 1), self.nb, 18))
         self._chk(lib().mbt_ws_run_turns(self.h, nturns, _ptr(cm), _ptr(ion), _ptr(zcm), _ptr(st)))
         return cm, ion, zcm, st[:nmon]
+
+    def last_ms(self):
+        """Device time [ms] of the last run."""
+        return lib().mbt_ws_last_ms(self.h)
+
+    def profile(self, nturns):
+        """Mean device ms per turn of (bunch step, optic + RW, ion train, kicks)."""
+        ms = np.zeros(4)
+        self._chk(lib().mbt_ws_profile(self.h, nturns, _ptr(ms)))
+        return ms
+
+    def interp(self, ib, icell, x, y):
+        """The device's grid interpolation on bunch ib's last field grid."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        out = np.zeros((x.size, 2))
+        self._chk(lib().mbt_ws_interp(self.h, ib, icell, _ptr(x), _ptr(y), x.size, _ptr(out)))
+        return out
 
     def bunch_fields(self, ib):
         e = np.zeros((self.nion, 2))

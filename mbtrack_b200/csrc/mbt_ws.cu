@@ -16,7 +16,7 @@
 //                194-253) and the long-range resistive-wall kick of every
 //                source bunch (transformSbunch_longrange :68-192), one
 //                thread per source, added in source order;
-//   ws_train     one block per SOURCE bunch, two macro-ions per thread: the
+//   ws_train     one block per SOURCE bunch, MBT_WS_IPT macro-ions per thread: the
 //                ions of that bunch travel down the train (drift between
 //                buckets, pull by each slice of each later bunch,
 //                fbi_weakstrong_train fbi_weakstrong.c:325-426); per later
@@ -69,6 +69,12 @@ constexpr int kBunchThreads = 256;
 constexpr int kRwThreads = 128;
 constexpr int kKickThreads = 64;
 constexpr long kChunk = 256;   // turns per block of host outputs
+#ifndef MBT_WS_IPT
+#define MBT_WS_IPT 2             // macro-ions per thread in the ion train
+#endif
+constexpr int kIpt = MBT_WS_IPT;
+// largest train block: 49 slices x 25 grid points, kIpt ions a thread
+constexpr int kTrainMaxThreads = ((kMaxSlices * 25 + kIpt - 1) / kIpt + 31) / 32 * 32;
 
 struct WsConst {
   int nb, S, G, off, nion, nmt, nharm, fbii, rw_long, trigger_rw, Nmlt;
@@ -81,11 +87,29 @@ struct WsConst {
   double prfrw[2], prfrw_trig[2];
   double Pref0, Dub0, Lc, fNp;
   double factBE, sgm_xx, sgm_zz, agLOCx, agLOCz, agABSx, agABSz, deltT, factF, Ldmsgm;
+  double rABSx, rABSz;   // 1 / agABSx, 1 / agABSz, correctly rounded
   double fdq_den;   // 2 eps0 sqrt(pi) factBE c deltT
   double factjp0;   // 1e2 4 pi eps0 r_e / Gamma
   double T0h;       // T0 / h
   double cdt;       // c deltT
 };
+
+// a / b, correctly rounded, for a divisor b whose correctly rounded
+// reciprocal rb is known: q0 = a rb is within about one ulp of a / b; one
+// residual correction q1 = q0 + (a - b q0) rb (the residual exact by FMA)
+// makes it faithful, a second gives the correctly rounded quotient
+// (P. Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Dev. 34(1), 1990: with rb the
+// correctly rounded 1/b and q faithful, q + (a - b q) rb rounds to a / b).
+// A zero residual means q is exact and is kept, sign of zero included.
+// Five FP64 operations in place of a full division.
+__device__ __forceinline__ double div_known(double a, double b, double rb) {
+  const double q0 = __dmul_rn(a, rb);
+  const double r0 = __fma_rn(-q0, b, a);
+  const double q1 = r0 == 0.0 ? q0 : __fma_rn(r0, rb, q0);
+  const double r1 = __fma_rn(-q1, b, a);
+  return r1 == 0.0 ? q1 : __fma_rn(r1, rb, q1);
+}
 
 // get_linearly_interpolated_Efields (fbi_weakstrong.c:454-580): truncated
 // grid index of (xx, yy) on the absolute grid, the neighbour on the side
@@ -95,7 +119,8 @@ __device__ __forceinline__ void ws_interp(const WsConst &C, const double *__rest
                                           double &ey) {
   const int off = C.off, G = C.G;
   const bool px = xx >= 0.0, pz = yy >= 0.0;
-  int k1x = __double2int_rz(xx / C.agABSx), k1z = __double2int_rz(yy / C.agABSz), k2x, k2z;
+  int k1x = __double2int_rz(div_known(xx, C.agABSx, C.rABSx));
+  int k1z = __double2int_rz(div_known(yy, C.agABSz, C.rABSz)), k2x, k2z;
   if (pz) {
     k2z = k1z < off ? k1z + 1 : k1z;
     k1z = min(k1z, off);
@@ -117,8 +142,8 @@ __device__ __forceinline__ void ws_interp(const WsConst &C, const double *__rest
   const int b = icell * G;
   const int i1 = (b + k1x + off) * G + k1z + off, i2 = (b + k2x + off) * G + k1z + off;
   const int i3 = (b + k1x + off) * G + k2z + off, i4 = (b + k2x + off) * G + k2z + off;
-  const double fx = (xx - k1x * C.agABSx) / C.agABSx;
-  const double fz = (yy - k1z * C.agABSz) / C.agABSz;
+  const double fx = div_known(xx - k1x * C.agABSx, C.agABSx, C.rABSx);
+  const double fz = div_known(yy - k1z * C.agABSz, C.agABSz, C.rABSz);
   const double y1 = Ey[i1], y2 = Ey[i2], y3 = Ey[i3], y4 = Ey[i4];
   const double x1 = Ex[i1], x2 = Ex[i2], x3 = Ex[i3], x4 = Ex[i4];
   double ey5, ey6, ex5, ex6;
@@ -324,7 +349,7 @@ __global__ void __launch_bounds__(kRwThreads) ws_optic_rw(WsConst C, double *__r
   }
 }
 
-__global__ void __launch_bounds__(1024) ws_train(WsConst C, const int *__restrict__ bucket,
+__global__ void __launch_bounds__(kTrainMaxThreads) ws_train(WsConst C, const int *__restrict__ bucket,
                                                  const double *__restrict__ fx, const double *__restrict__ fy,
                                                  const double *__restrict__ ion, double *__restrict__ part,
                                                  double *__restrict__ ipart) {
@@ -332,9 +357,9 @@ __global__ void __launch_bounds__(1024) ws_train(WsConst C, const int *__restric
   const int src = blockIdx.x, tid = threadIdx.x, n = C.nion, S = C.S;
   const int nw = blockDim.x >> 5, lane = tid & 31, wid = tid >> 5;
   const double *li = ion + (size_t)src * 5 * n;
-  double N[2], X[2], XD[2], Y[2], YD[2];
+  double N[kIpt], X[kIpt], XD[kIpt], Y[kIpt], YD[kIpt];
 #pragma unroll
-  for (int q = 0; q < 2; ++q) {
+  for (int q = 0; q < kIpt; ++q) {
     const int p = tid + q * blockDim.x;
     const bool ok = p < n;
     N[q] = ok ? li[p] : 0.0;
@@ -349,7 +374,7 @@ __global__ void __launch_bounds__(1024) ws_train(WsConst C, const int *__restric
     const int kb = bucket[k];
     const double Dt = fabs((double)(kb - kbprev)) * C.T0h;
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < kIpt; ++q) {
       X[q] = X[q] + Dt * XD[q];
       Y[q] = Y[q] + Dt * YD[q];
     }
@@ -357,7 +382,7 @@ __global__ void __launch_bounds__(1024) ws_train(WsConst C, const int *__restric
     for (int c = 0; c < S; ++c) {
       double ax = 0.0, ay = 0.0;
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
+      for (int q = 0; q < kIpt; ++q) {
         double ex, ey;
         ws_interp(C, Ex, Ey, c, X[q], Y[q], ex, ey);
         XD[q] = XD[q] + C.deltT * (C.factF * ex);
@@ -374,7 +399,12 @@ __global__ void __launch_bounds__(1024) ws_train(WsConst C, const int *__restric
         wsum[((size_t)c * nw + wid) * 2 + 1] = ay;
       }
     }
-    double cx = N[0] * X[0] + N[1] * X[1], cy = N[0] * Y[0] + N[1] * Y[1];
+    double cx = 0.0, cy = 0.0;
+#pragma unroll
+    for (int q = 0; q < kIpt; ++q) {
+      cx += N[q] * X[q];
+      cy += N[q] * Y[q];
+    }
     cx = warp_sum(cx);
     cy = warp_sum(cy);
     if (lane == 0) {
@@ -445,6 +475,17 @@ __global__ void __launch_bounds__(kKickThreads) ws_kick(WsConst C, const int *__
   }
 }
 
+__global__ void ws_interp_points(WsConst C, const double *__restrict__ fx, const double *__restrict__ fy, int ib,
+                                 int icell, const double *__restrict__ x, const double *__restrict__ y, int n,
+                                 double *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double ex, ey;
+  ws_interp(C, fx + (size_t)ib * C.nion, fy + (size_t)ib * C.nion, icell, x[i], y[i], ex, ey);
+  out[2 * i] = ex;
+  out[2 * i + 1] = ey;
+}
+
 thread_local char g_ws_err[512] = "";
 
 }  // namespace
@@ -459,6 +500,8 @@ struct mbt_ws {
   double *d_s, *d_hist, *d_fx, *d_fy, *d_ion, *d_own, *d_part, *d_ipart;
   double *d_cm, *d_io, *d_zcm, *d_st;
   cudaStream_t stream;
+  cudaEvent_t ev[5];
+  double last_ms;   // device time of the last mbt_ws_run_turns
   char err[512];
 };
 
@@ -483,6 +526,8 @@ static void ws_free(mbt_ws *ws) {
                   ws->d_io, ws->d_zcm, ws->d_st};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  for (cudaEvent_t e : ws->ev)
+    if (e) cudaEventDestroy(e);
   if (ws->stream) cudaStreamDestroy(ws->stream);
 }
 
@@ -554,6 +599,8 @@ static void ws_constants(const mbt_ws_params *w, int nb, WsConst *C) {
   C->agLOCz = w->agLOCz;
   C->agABSx = w->agABSx;
   C->agABSz = w->agABSz;
+  C->rABSx = 1.0 / w->agABSx;
+  C->rABSz = 1.0 / w->agABSz;
   C->deltT = w->deltT;
   C->factF = w->factF;
   C->Ldmsgm = w->Ldmsgm;
@@ -582,14 +629,14 @@ extern "C" int mbt_ws_create(const mbt_ws_params *w, int nbunch, const int *buck
       return ws_fail(nullptr, MBT_ERR_INVALID, "mbt_ws_create: buckets must ascend within 0..%d",
                      w->base.nharm - 1);
   const int nion = S * w->ngrid * w->ngrid;
-  if (2 * 1024 < nion) return ws_fail(nullptr, MBT_ERR_INVALID, "mbt_ws_create: %d ions per bunch", nion);
+  if (((nion + kIpt - 1) / kIpt + 31) / 32 * 32 > kTrainMaxThreads) return ws_fail(nullptr, MBT_ERR_INVALID, "mbt_ws_create: %d ions per bunch", nion);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return ws_fail(nullptr, MBT_ERR_NODEVICE, "mbt_ws_create: no CUDA device");
   mbt_ws *ws = (mbt_ws *)calloc(1, sizeof(mbt_ws));
   if (!ws) return ws_fail(nullptr, MBT_ERR_NOMEM, "mbt_ws_create: out of host memory");
   ws->w = *w;
   ws_constants(w, nbunch, &ws->C);
-  ws->tpb = ((nion + 1) / 2 + 31) / 32 * 32;
+  ws->tpb = ((nion + kIpt - 1) / kIpt + 31) / 32 * 32;
   const WsConst &C = ws->C;
   const size_t nb = (size_t)nbunch, pairs = nb * (nb - 1) / 2;
   std::vector<double> nelec(nb);
@@ -619,6 +666,8 @@ extern "C" int mbt_ws_create(const mbt_ws_params *w, int nbunch, const int *buck
 #undef WS_ALLOC
   if (!rc && cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) != cudaSuccess)
     rc = ws_fail(nullptr, MBT_ERR_CUDA, "mbt_ws_create: stream creation failed");
+  for (int i = 0; i < 5 && !rc; ++i)
+    if (cudaEventCreate(&ws->ev[i]) != cudaSuccess) rc = ws_fail(nullptr, MBT_ERR_CUDA, "mbt_ws_create: events");
   if (!rc) {
     const cudaStream_t st = ws->stream;
     bool ok = cudaMemcpyAsync(ws->d_bucket, bucket, nb * sizeof(int), cudaMemcpyHostToDevice, st) == cudaSuccess &&
@@ -683,10 +732,12 @@ extern "C" int mbt_ws_run_turns(mbt_ws *ws, long nturns, double *cm, double *ion
   const size_t bunch_smem = 2 * n * sizeof(double);
   const size_t train_smem = (S * (ws->tpb / 32) * 2 + (ws->tpb / 32) * 2) * sizeof(double);
   long imon_total = 0;
+  ws->last_ms = 0.0;
   for (long t0 = 0; t0 < nturns; t0 += kChunk) {
     const long nt = nturns - t0 < kChunk ? nturns - t0 : kChunk;
     long imon = 0;
     if (zcm) WS_CUDA(ws, cudaMemsetAsync(ws->d_zcm, 0, (size_t)nt * C.nharm * sizeof(double), st));
+    WS_CUDA(ws, cudaEventRecord(ws->ev[0], st));
     for (long t = 0; t < nt; ++t) {
       const long rev = ws->turn;
       const bool mon = rev % C.nrev_mon == 0;
@@ -706,6 +757,7 @@ extern "C" int mbt_ws_run_turns(mbt_ws *ws, long nturns, double *cm, double *ion
       if (mon) ++imon;
       ++ws->turn;
     }
+    WS_CUDA(ws, cudaEventRecord(ws->ev[1], st));
     if (cm)
       WS_CUDA(ws, cudaMemcpyAsync(cm + (size_t)t0 * nb * 6, ws->d_cm, (size_t)nt * nb * 6 * sizeof(double),
                                   cudaMemcpyDeviceToHost, st));
@@ -719,8 +771,71 @@ extern "C" int mbt_ws_run_turns(mbt_ws *ws, long nturns, double *cm, double *ion
       WS_CUDA(ws, cudaMemcpyAsync(stats + (size_t)imon_total * nb * 18, ws->d_st,
                                   (size_t)imon * nb * 18 * sizeof(double), cudaMemcpyDeviceToHost, st));
     WS_CUDA(ws, cudaStreamSynchronize(st));
+    float ms = 0.0f;
+    WS_CUDA(ws, cudaEventElapsedTime(&ms, ws->ev[0], ws->ev[1]));
+    ws->last_ms += ms;
     imon_total += imon;
   }
+  return 0;
+}
+
+extern "C" double mbt_ws_last_ms(const mbt_ws *ws) { return ws ? ws->last_ms : -1.0; }
+
+extern "C" int mbt_ws_profile(mbt_ws *ws, long nturns, double *ms4) {
+  if (!ws || nturns < 1 || !ms4) return ws_fail(ws, MBT_ERR_INVALID, "mbt_ws_profile: bad argument");
+  const WsConst &C = ws->C;
+  const cudaStream_t st = ws->stream;
+  const size_t nb = (size_t)C.nb, S = (size_t)C.S, n = (size_t)C.nion;
+  const size_t bunch_smem = 2 * n * sizeof(double);
+  const size_t train_smem = (S * (ws->tpb / 32) * 2 + (ws->tpb / 32) * 2) * sizeof(double);
+  double acc[4] = {0, 0, 0, 0};
+  for (long t = 0; t < nturns; ++t) {
+    const long rev = ws->turn;
+    WS_CUDA(ws, cudaEventRecord(ws->ev[0], st));
+    ws_bunch<<<C.nb, kBunchThreads, bunch_smem, st>>>(C, ws->d_s, ws->d_hist, ws->d_npop, ws->d_nofe, ws->d_nelec,
+                                                      ws->d_fx, ws->d_fy, ws->d_ion, ws->d_own, nullptr, nullptr);
+    WS_CUDA(ws, cudaEventRecord(ws->ev[1], st));
+    ws_optic_rw<<<C.nb, kRwThreads, nb * sizeof(double), st>>>(C, ws->d_s, ws->d_hist, ws->d_ibunch, ws->d_bucket,
+                                                                rev);
+    WS_CUDA(ws, cudaEventRecord(ws->ev[2], st));
+    if (C.fbii && C.nb > 1)
+      ws_train<<<C.nb, ws->tpb, train_smem, st>>>(C, ws->d_bucket, ws->d_fx, ws->d_fy, ws->d_ion, ws->d_part,
+                                                  ws->d_ipart);
+    WS_CUDA(ws, cudaEventRecord(ws->ev[3], st));
+    ws_kick<<<C.nb, kKickThreads, 0, st>>>(C, ws->d_bucket, ws->d_npop, ws->d_nelec, ws->d_s, ws->d_part,
+                                           ws->d_ipart, ws->d_own, nullptr, nullptr);
+    WS_CUDA(ws, cudaEventRecord(ws->ev[4], st));
+    WS_CUDA(ws, cudaGetLastError());
+    WS_CUDA(ws, cudaEventSynchronize(ws->ev[4]));
+    for (int k = 0; k < 4; ++k) {
+      float ms = 0.0f;
+      WS_CUDA(ws, cudaEventElapsedTime(&ms, ws->ev[k], ws->ev[k + 1]));
+      acc[k] += ms;
+    }
+    ++ws->turn;
+  }
+  for (int k = 0; k < 4; ++k) ms4[k] = acc[k] / (double)nturns;
+  return 0;
+}
+
+extern "C" int mbt_ws_interp(mbt_ws *ws, int ib, int icell, const double *x, const double *y, int n, double *exey) {
+  if (!ws || ib < 0 || ib >= ws->C.nb || icell < 0 || icell >= ws->C.S || n < 0 || (n > 0 && (!x || !y || !exey)))
+    return ws_fail(ws, MBT_ERR_INVALID, "mbt_ws_interp: bunch %d slice %d, %d points", ib, icell, n);
+  if (n == 0) return 0;
+  double *d = nullptr;
+  WS_CUDA(ws, cudaMalloc(&d, (size_t)n * 4 * sizeof(double)));
+  cudaError_t e = cudaMemcpyAsync(d, x, n * sizeof(double), cudaMemcpyHostToDevice, ws->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d + n, y, n * sizeof(double), cudaMemcpyHostToDevice, ws->stream);
+  if (e == cudaSuccess) {
+    ws_interp_points<<<(n + 255) / 256, 256, 0, ws->stream>>>(ws->C, ws->d_fx, ws->d_fy, ib, icell, d, d + n, n,
+                                                              d + 2 * n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(exey, d + 2 * n, 2 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, ws->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ws->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return ws_fail(ws, MBT_ERR_CUDA, "mbt_ws_interp: %s", cudaGetErrorString(e));
   return 0;
 }
 

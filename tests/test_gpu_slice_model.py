@@ -114,3 +114,70 @@ def test_chunked_outputs(tmp_path, cuda_device):
     for k in range(4):
         assert np.array_equal(a[k], np.concatenate([p[k] for p in parts]), equal_nan=True)
     assert d2.turn == 300
+
+
+def _np_interp(Ex, Ey, icell, G, ax, az, xs, ys):
+    """get_linearly_interpolated_Efields (fbi_weakstrong.c:454-580) in
+    Python floats: IEEE division, the reference's operand order."""
+    off = (G - 1) // 2
+    out = np.zeros((len(xs), 2))
+    for i, (xx, yy) in enumerate(zip(xs, ys)):
+        k1x, k1z = int(xx / ax), int(yy / az)
+        if yy >= 0:
+            k2z = k1z + 1 if k1z < off else k1z
+            k1z, k2z = min(k1z, off), min(k2z, off)
+        else:
+            k2z = k1z - 1 if k1z > -off else k1z
+            k1z, k2z = max(k1z, -off), max(k2z, -off)
+        if xx >= 0:
+            k2x = k1x + 1 if k1x < off else k1x
+            k1x, k2x = min(k1x, off), min(k2x, off)
+        else:
+            k2x = k1x - 1 if k1x > -off else k1x
+            k1x, k2x = max(k1x, -off), max(k2x, -off)
+        b = icell * G
+        i1 = (b + k1x + off) * G + k1z + off
+        i2 = (b + k2x + off) * G + k1z + off
+        i3 = (b + k1x + off) * G + k2z + off
+        i4 = (b + k2x + off) * G + k2z + off
+        fx = (xx - k1x * ax) / ax
+        fz = (yy - k1z * az) / az
+        r = []
+        for E in (Ex, Ey):
+            if xx >= 0:
+                e5 = E[i1] + fx * (E[i2] - E[i1])
+                e6 = E[i3] + fx * (E[i4] - E[i3])
+            else:
+                e5 = E[i1] - fx * (E[i2] - E[i1])
+                e6 = E[i3] - fx * (E[i4] - E[i3])
+            r.append(e5 + fz * (e6 - e5) if yy >= 0 else e5 - fz * (e6 - e5))
+        out[i] = r
+    return out
+
+
+def test_device_interpolation_bit_exact(tmp_path, cuda_device):
+    """The device's interpolation, with its division by the grid step done
+    as a multiplication by the reciprocal plus two residual corrections,
+    equals the reference's expression with IEEE division bit for bit: at
+    random points, on and one ulp either side of every grid line, far
+    outside the grid and at zero of both signs."""
+    w, bucket, ib, npop, nofe, g = _setup(tmp_path, "train")
+    dev = api.SliceModel(w, bucket, ib, npop, nofe)
+    dev.load_slices(g["slices0"])
+    dev.run(2, outputs=False)
+    ax, az = w.agABSx, w.agABSz
+    rng = np.random.default_rng(11)
+    lines = np.arange(-4, 5)
+    xs = [rng.uniform(-4, 4, 1500) * ax, rng.uniform(-300, 300, 200) * ax,
+          np.nextafter(lines * ax, np.inf), np.nextafter(lines * ax, -np.inf), lines * ax,
+          np.array([0.0, -0.0, 0.0, -0.0])]
+    ys = [rng.uniform(-4, 4, 1500) * az, rng.uniform(-300, 300, 200) * az,
+          np.nextafter(lines * az, -np.inf), np.nextafter(lines * az, np.inf), lines * az,
+          np.array([0.0, -0.0, -0.0, 0.0])]
+    x = np.concatenate(xs)
+    y = np.concatenate(ys)
+    for ibn, icell in ((0, 23), (3, 10), (9, 30)):
+        exey, _ = dev.bunch_fields(ibn)
+        got = dev.interp(ibn, icell, x, y)
+        want = _np_interp(exey[:, 0], exey[:, 1], icell, w.ngrid, ax, az, x, y)
+        assert np.array_equal(got, want), np.abs(got - want).max()

@@ -168,6 +168,43 @@ const char *mbt_ws_last_error(const mbt_ws *ws);
 
 void mbt_ws_destroy(mbt_ws *ws);
 
+/* ---- output files of the slice-model manager ----------------------- */
+
+typedef struct mbt_ws_writer mbt_ws_writer;
+
+/* Create, in work_path, CMmotionsV.out (writeoutVCMmotionsPM2
+ * fbi_weakstrong.c:672-737) and with w->fbii CMImotionsH.out /
+ * CMImotionsV.out (writeoutCMImotions :583-669).  flags:
+ * MBT_WRITER_OWN_AMPINV prints each bunch's own amplitude invariants in
+ * the per-monitor ampinv files; by default the writer keeps the
+ * reference's monitor x Nbunch + bucket history and prints entry monitor +
+ * bucket as bunch_strong_writeout_ampinv does (bunch.c:645-702), 0 where
+ * the reference reads past its array. */
+int mbt_ws_writer_open(const char *work_path, const mbt_ws_params *w, int nbunch,
+                       const int *bucket, int flags, mbt_ws_writer **out);
+
+/* The next nturns turns, outputs of mbt_ws_run_turns: ion (needed with
+ * EnableFBII), zcm, and stats for the monitor turns among them (may be
+ * NULL without one): motion lines and ampinv_<P>_<turn>.dat files. */
+int mbt_ws_writer_turns(mbt_ws_writer *wr, long nturns, const double *ion,
+                        const double *zcm, const double *stats);
+
+/* The generated bunch (soa6 of np particles, mbt_ws_reference_beam) into
+ * the three gendst_datafile paths (LON, HOR, VER) as the manager's
+ * strong_generate_eCMs writes them (bunch.c:314-331). */
+int mbt_ws_writer_distribution(const mbt_ws_writer *wr, const char *const *paths,
+                               const double *soa6, int np);
+
+/* ampinv_<P>_mean.dat and cmpos_<P>_mean.dat for HOR and VER
+ * (bunch_writeout_mean_ampinv_pos bunch.c:704-770), then close. */
+int mbt_ws_writer_close(mbt_ws_writer *wr);
+
+/* Message of the last failing mbt_ws_writer_* call. */
+const char *mbt_ws_writer_error(void);
+
+/* BunchModel of a .conf file: 0 WEAK, 1 STRONG, or MBT_ERR_CONFIG. */
+int mbt_config_bunch_model(const char *conf_path);
+
 #ifdef __cplusplus
 }
 #endif

@@ -109,6 +109,13 @@ SIGNATURES = {
     "mbt_ws_interp": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp]),
     "mbt_ws_last_error": (ctypes.c_char_p, [_vp]),
     "mbt_ws_destroy": (None, [_vp]),
+    "mbt_ws_writer_open": (ctypes.c_int, [ctypes.c_char_p, _P(MbtWsParams), ctypes.c_int, _vp, ctypes.c_int,
+                                          _P(_vp)]),
+    "mbt_ws_writer_turns": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp, _vp]),
+    "mbt_ws_writer_distribution": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
+    "mbt_ws_writer_close": (ctypes.c_int, [_vp]),
+    "mbt_ws_writer_error": (ctypes.c_char_p, []),
+    "mbt_config_bunch_model": (ctypes.c_int, [ctypes.c_char_p]),
 }
 
 
@@ -701,3 +708,38 @@ class SliceModel:
             self.close()
         except Exception:
             pass
+
+
+class SliceWriter:
+    """The slice-model manager's output files (mbt_ws_writer_*)."""
+
+    def __init__(self, work_path, w, bucket, own_ampinv=False):
+        L = lib()
+        self.w = w
+        self._bucket = np.ascontiguousarray(bucket, dtype=np.int32)
+        h = _vp()
+        rc = L.mbt_ws_writer_open(work_path.encode(), ctypes.byref(w), len(bucket), _ptr(self._bucket),
+                                  MBT_WRITER_OWN_AMPINV if own_ampinv else 0, ctypes.byref(h))
+        if rc != 0:
+            raise MbtError(rc, L.mbt_ws_writer_error().decode(errors="replace"))
+        self.h = h
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise MbtError(rc, lib().mbt_ws_writer_error().decode(errors="replace"))
+
+    def turns(self, ion, zcm, stats):
+        ion = np.ascontiguousarray(ion, dtype=np.float64)
+        zcm = np.ascontiguousarray(zcm, dtype=np.float64)
+        stats = None if stats is None or len(stats) == 0 else np.ascontiguousarray(stats, dtype=np.float64)
+        self._chk(lib().mbt_ws_writer_turns(self.h, zcm.shape[0], _ptr(ion), _ptr(zcm), _ptr(stats)))
+
+    def distribution(self, paths, soa6):
+        arr = (ctypes.c_char_p * 3)(*[p.encode() for p in paths])
+        soa6 = np.ascontiguousarray(soa6, dtype=np.float64)
+        self._chk(lib().mbt_ws_writer_distribution(self.h, ctypes.cast(arr, _vp), _ptr(soa6), soa6.shape[1]))
+
+    def close(self):
+        if getattr(self, "h", None):
+            h, self.h = self.h, None
+            self._chk(lib().mbt_ws_writer_close(h))

@@ -27,7 +27,7 @@ CU_SOURCES = ["mbt_runtime.cu", "mbt_step.cu", "mbt_fields.cu", "mbt_mlp.cu", "m
 # per-file extra flags: w(z) and the BE field keep every multiply and add
 # separately rounded, as the reference's x86-64 build does
 CU_EXTRA = {"mbt_fields.cu": ["-fmad=false"], "mbt_ws.cu": ["-fmad=false"]}
-C_SOURCES = ["mbt_host.c", "mbt_beam.c", "mbt_output.c"]
+C_SOURCES = ["mbt_host.c", "mbt_beam.c", "mbt_output.c", "mbt_ws_output.c"]
 # the drop-in executable for mbtrack-mpi's weak-weak runs
 CLI_SOURCE = "mbtrack_gpu.c"
 CLI = os.path.join(HERE, "mbtrack-gpu")

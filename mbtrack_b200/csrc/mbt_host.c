@@ -871,6 +871,21 @@ int mbt_ws_config_load(const char *conf_path, int fix_rw_beff, mbt_ws_params *w,
 
 size_t mbt_ws_params_size(void) { return sizeof(mbt_ws_params); }
 
+int mbt_config_bunch_model(const char *conf_path)
+{
+  conf_t C;
+  char s[64];
+  int r;
+  if (!conf_path) return MBT_ERR_INVALID;
+  if (conf_read(conf_path, &C) != 0) return cfg_fail("cannot open %s", conf_path);
+  if (!get_str(&C, "tracking", "BunchModel", s, sizeof s)) r = cfg_fail("missing [tracking] BunchModel");
+  else if (strcmp(s, "WEAK") == 0) r = 0;
+  else if (strcmp(s, "STRONG") == 0) r = 1;
+  else r = cfg_fail("BunchModel %s: WEAK or STRONG", s);
+  conf_free(&C);
+  return r;
+}
+
 /* strong_generate_eCMs bunch_strong.c:117-198 */
 int mbt_ws_slice_beam(const mbt_ws_params *w, const double *soa6, int np, int *npop, int *nofe, double *cm4)
 {
@@ -941,7 +956,7 @@ int mbt_config_output(const char *conf_path, mbt_output_cfg *o, int *bunch_out)
   if (!conf_path || !o) return MBT_ERR_INVALID;
   g = (cfg_t *) calloc(1, sizeof(cfg_t));
   if (!g) return MBT_ERR_NOMEM;
-  r = read_conf(conf_path, 1, 0, g);
+  r = read_conf(conf_path, 1, 1, g);
   if (!r) r = setup_ring(g);
   if (!r) r = setup_tracking(g);
   if (!r) {

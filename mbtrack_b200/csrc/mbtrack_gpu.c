@@ -1,8 +1,12 @@
 /*
- * mbtrack_gpu.c -- `mbtrack-gpu input.conf [/path/to/work]`: the weak-weak
- * run of mbtrack-mpi (mbtrack-mpi.c:22-160 with manager_weakweak and
- * worker_weakweak) on one GPU, without MPI and without the rank-count check
- * of mbtrack-mpi.c:85-90.
+ * mbtrack_gpu.c -- `mbtrack-gpu input.conf [/path/to/work]`: the run of
+ * mbtrack-mpi (mbtrack-mpi.c:22-160) on one GPU, without MPI and without the
+ * rank-count check of mbtrack-mpi.c:85-90: manager_weakweak /
+ * worker_weakweak for BunchModel = WEAK, manager_weakstrong /
+ * worker_weakstrong (the slice model with fast beam-ion interaction,
+ * mbt_ws.h) for BunchModel = STRONG.  The slice model runs with the bunch
+ * currents of the fill (the reference's slice-model manager never sets
+ * ring.Ibunch, so its charges, ions and wall kicks are all zero).
  *
  * The arguments, the terminal messages and the files in the work directory
  * are the reference's.  Options (anywhere on the command line):
@@ -26,6 +30,7 @@
 #include <unistd.h>
 
 #include "mbt.h"
+#include "mbt_ws.h"
 
 typedef struct beam_job {
   const mbt_params *p;
@@ -82,6 +87,105 @@ static void ctx_error(mbt_ctx *ctx, const char *what)
   fprintf(stderr, "ERROR: %s: %s\n", what, msg);
 }
 
+/* manager_weakstrong.c:7-263 with worker_weakstrong.c:13-247 */
+static int run_strong(const char *conf, const char *work, int own_ampinv)
+{
+  mbt_ws_params w;
+  mbt_output_cfg o;
+  mbt_ws *ws = NULL;
+  mbt_ws_writer *wr = NULL;
+  int nb = 0, i, k, c, S, G;
+  int *bucket, *npop, *nofe;
+  double *frac, *ib, *soa6, *off4, *cm4, *sl, *ion, *zcm, *stats;
+  long rev, chunk = 256;
+  const char *gendst[3];
+
+  if (mbt_ws_config_load(conf, 1, &w, &nb, NULL, NULL) != 0) {
+    fprintf(stderr, "ERROR: read_input failed: %s\n", mbt_config_error());
+    return -1;
+  }
+  bucket = (int *) calloc(w.base.nharm, sizeof(int));
+  frac = (double *) calloc(w.base.nharm, sizeof(double));
+  if (!bucket || !frac || mbt_ws_config_load(conf, 1, &w, &nb, bucket, frac) != 0 ||
+      mbt_config_output(conf, &o, NULL) != 0) {
+    fprintf(stderr, "ERROR: read_input failed: %s\n", mbt_config_error());
+    return -1;
+  }
+  if (nb <= 0) { fprintf(stderr, "ERROR: e_beam_setup: no filled bucket\n"); return -1; }
+  S = 2 * w.nslc + 1;
+  G = w.ngrid;
+  printf("Starting job \"%s\"\n\n", o.jobtitle);
+  printf("Generating initial distribution...\n");
+  ib = (double *) malloc(nb * sizeof(double));
+  soa6 = (double *) malloc((size_t) 6 * w.np * sizeof(double));
+  off4 = (double *) malloc((size_t) 4 * nb * sizeof(double));
+  npop = (int *) malloc(S * sizeof(int));
+  nofe = (int *) malloc((size_t) S * G * G * sizeof(int));
+  cm4 = (double *) malloc((size_t) 4 * S * sizeof(double));
+  sl = (double *) calloc((size_t) nb * 6 * S, sizeof(double));
+  ion = (double *) malloc((size_t) chunk * nb * 2 * sizeof(double));
+  zcm = (double *) malloc((size_t) chunk * w.base.nharm * sizeof(double));
+  stats = (double *) malloc((size_t) chunk * nb * 18 * sizeof(double));
+  if (!ib || !soa6 || !off4 || !npop || !nofe || !cm4 || !sl || !ion || !zcm || !stats) {
+    fprintf(stderr, "ERROR: out of host memory\n");
+    return -1;
+  }
+  for (i = 0; i < nb; i++) ib[i] = 1.0e+03 * mbt_bunch_current(&w.base, nb, frac[i]);
+  /* strong_generate_eCMs (with its distribution files) and
+     generate_initial_general_distribution2 */
+  if (mbt_ws_reference_beam(&w, nb, soa6, off4) != 0 || mbt_ws_slice_beam(&w, soa6, w.np, npop, nofe, cm4) != 0) {
+    fprintf(stderr, "ERROR: generate_eCMs failed\n");
+    return -1;
+  }
+  for (i = 0; i < nb; i++)
+    for (k = 0; k < 4; k++)
+      for (c = 0; c < S; c++) sl[((size_t) i * 6 + 2 + k) * S + c] = cm4[k * S + c] + off4[4 * i + k];
+  if (mbt_ws_create(&w, nb, bucket, ib, npop, nofe, &ws) != 0) {
+    fprintf(stderr, "ERROR: mbt_ws_create: %s\n", mbt_ws_last_error(NULL));
+    return -1;
+  }
+  if (mbt_ws_load_slices(ws, sl) != 0) { fprintf(stderr, "ERROR: %s\n", mbt_ws_last_error(ws)); return -1; }
+  if (mbt_ws_writer_open(work, &w, nb, bucket, own_ampinv ? MBT_WRITER_OWN_AMPINV : 0, &wr) != 0) {
+    fprintf(stderr, "ERROR: %s\n", mbt_ws_writer_error());
+    return -1;
+  }
+  for (k = 0; k < 3; k++) gendst[k] = o.gendst_file[k];
+  if (mbt_ws_writer_distribution(wr, gendst, soa6, w.np) != 0) {
+    fprintf(stderr, "%s\nERROR: generate_eCMs failed\n", mbt_ws_writer_error());
+    return -1;
+  }
+  printf("Starting multi bunch tracking...\n");
+  for (rev = 0; rev < w.base.nrev_tot;) {
+    const long n = w.base.nrev_tot - rev < chunk ? w.base.nrev_tot - rev : chunk;
+    long t;
+    if (mbt_ws_run_turns(ws, n, NULL, ion, zcm, stats) != 0) {
+      fprintf(stderr, "ERROR: %s\n", mbt_ws_last_error(ws));
+      return -1;
+    }
+    if (mbt_ws_writer_turns(wr, n, ion, zcm, stats) != 0) {
+      fprintf(stderr, "ERROR: %s\n", mbt_ws_writer_error());
+      return -1;
+    }
+    /* terminal output of manager_weakstrong.c:84-92, 236-240 */
+    for (t = rev; t < rev + n; t++) {
+      if (t % 100 == 0) {
+        if (t + 99 >= w.base.nrev_tot) printf("Transformation for turn %3ld to %3ld", t, w.base.nrev_tot - 1);
+        else printf("Transformation for turn %3ld to %3ld", t, t + 99);
+        fflush(stdout);
+      }
+      if (t % 10 == 9) printf(".");
+      fflush(stdout);
+      if (t % 100 == 99 || t == w.base.nrev_tot - 1) printf(" done\n");
+    }
+    rev += n;
+  }
+  if (mbt_ws_writer_close(wr) != 0) fprintf(stderr, "ERROR: %s\n", mbt_ws_writer_error());
+  mbt_ws_destroy(ws);
+  free(bucket); free(frac); free(ib); free(soa6); free(off4); free(npop); free(nofe); free(cm4); free(sl);
+  free(ion); free(zcm); free(stats);
+  return 0;
+}
+
 int main(int argc, char **argv)
 {
   const char *conf = NULL, *work = "work/";
@@ -118,6 +222,12 @@ int main(int argc, char **argv)
   }
 
   /* read_input + setup_* (mbtrack-mpi.c:61-97), checked */
+  r = mbt_config_bunch_model(conf);
+  if (r < 0) {
+    fprintf(stderr, "ERROR: read_input failed: %s\n", mbt_config_error());
+    return -1;
+  }
+  if (r == 1) return run_strong(conf, work, own_ampinv);
   if (mbt_config_load(conf, 1, &p, &nb, NULL, NULL) != 0) {
     fprintf(stderr, "ERROR: read_input failed: %s\n", mbt_config_error());
     return -1;

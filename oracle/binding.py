@@ -427,6 +427,17 @@ class ReferenceSlices:
         self.lib.refws_particles(_ptr(a))
         return a
 
+    def files(self, on=True):
+        """The manager's writers into the work directory (refws_files)."""
+        self.lib.refws_files(int(on))
+
+    def finish(self):
+        self.lib.refws_finish()
+
+    def write_distribution(self):
+        if self.lib.refws_write_distribution() != 0:
+            raise RuntimeError("refws_write_distribution failed")
+
     def slices_state(self):
         a = np.zeros((self.nb, 6, self.slices))
         self.lib.refws_get_slices(_ptr(a))

@@ -55,6 +55,11 @@ extern ring_t ring;
 extern tracking_t track;
 extern grid_t fbii_grid;
 
+/* defined in bunch.c:703-770 without a header prototype */
+int bunch_writeout_mean_ampinv_pos(const long int NrevTot, const long int NrevMon,
+                                   const bunch_CM_history_strong_t * CMhist,
+                                   const e_beam_t ebeam, const plane_t plane);
+
 typedef struct wsw {
   int kb;
   bunch_strong_t bunch0;        /* worker_weakstrong.c:15 */
@@ -75,6 +80,7 @@ static ion_beam_t *ws_ions = NULL;
 static long ws_rev = 0;
 static int ws_slices = 0;
 static double *ws_soa = NULL;                 /* the Np generated particles */
+static int ws_files = 0;                      /* call the manager's writers */
 
 static void free_all(void)
 {
@@ -310,6 +316,20 @@ int refws_run(long nturns, double *cm, double *ion, double *zcm, double *stats)
       }
       if (rev % track.NrevMon == 0) {
         bunch_strong_distribution_statistics(&w->bunch, S);
+        if (ws_files) {
+          /* manager_weakstrong.c:131-138; an index past the array (the
+             reference writes there) is skipped */
+          const long k = (rev / track.NrevMon) * ws_ebeam.Nbunch + kb;
+          const long nslot = (long) (track.NrevTot / track.NrevMon * ws_ebeam.Nbunch) + 2;
+          if (k < nslot) {
+            ws_hist_m->cm[k] = w->bunch.stats.pos;
+            ws_hist_m->rms[k] = w->bunch.stats.pos_sigma;
+            ws_hist_m->cm_slope[k] = w->bunch.stats.slope;
+            ws_hist_m->rms_slope[k] = w->bunch.stats.slope_sigma;
+            ws_hist_m->ampinv[k] = w->bunch.stats.ampinv;
+            ws_hist_m->ampinv_cm[k] = w->bunch.stats.ampinv_cm;
+          }
+        }
         if (stats) {
           double *o = stats + ((size_t) imon * ws_nb + ib) * 18;
           put_vec(o, &w->bunch.stats.pos); put_vec(o + 3, &w->bunch.stats.pos_sigma);
@@ -318,7 +338,10 @@ int refws_run(long nturns, double *cm, double *ion, double *zcm, double *stats)
         }
       }
     }
-    if (rev % track.NrevMon == 0) imon++;
+    if (rev % track.NrevMon == 0) {
+      if (ws_files) bunch_strong_writeout_ampinv(rev, rev / track.NrevMon, ws_hist_m, ws_ebeam);
+      imon++;
+    }
 
     /* phase 2: manager_weakstrong.c:143-178, worker_weakstrong.c:138-183 */
     sortCMdata((int) rev, ws_hist_m);
@@ -348,6 +371,8 @@ int refws_run(long nturns, double *cm, double *ion, double *zcm, double *stats)
           && fbi_weakstrong_train(ws_model, ws_fbii, ws_ebeam, w->ion, ws_ions, &w->bunch, ib, w->kb) < 0)
         return -2;
       copy_arrays(&ws_bunches[w->kb], &w->bunch);
+      if (ws_files && track.EnableFBII)
+        writeoutCMImotions(track.work_path, (int) rev, ib, ws_ions, &ws_ebeam, ws_model);
       if (ion) {
         /* writeoutCMImotions fbi_weakstrong.c:626-646 */
         double xs = 0.0, ys = 0.0, nt = 0.0;
@@ -361,6 +386,7 @@ int refws_run(long nturns, double *cm, double *ion, double *zcm, double *stats)
         ion[((size_t) t * ws_nb + ib) * 2 + 1] = nt == 0.0 ? NAN : ys / nt;
       }
     }
+    if (ws_files) writeoutVCMmotionsPM2(track.work_path, (int) rev, ws_bunches, &ws_ebeam);
     if (zcm) {
       /* writeoutVCMmotionsPM2 fbi_weakstrong.c:708-718 */
       unsigned kb;
@@ -406,4 +432,26 @@ void refws_interp(int ib, int icell, const double *x, const double *y, int n, do
     exey[2 * i] = e[0];
     exey[2 * i + 1] = e[1];
   }
+}
+
+/* Switch the manager's writers on (files in the work directory given to
+   refws_init): motion files every turn, ampinv files every NrevMon. */
+void refws_files(int on) { ws_files = on; }
+
+/* The end-of-run files of manager_weakstrong.c:244-247. */
+void refws_finish(void)
+{
+  if (track.TrackPlane[HOR]) bunch_writeout_mean_ampinv_pos(track.NrevTot, track.NrevMon, ws_hist_m, ws_ebeam, HOR);
+  if (track.TrackPlane[VER]) bunch_writeout_mean_ampinv_pos(track.NrevTot, track.NrevMon, ws_hist_m, ws_ebeam, VER);
+}
+
+/* The manager's generated-bunch files (strong_generate_eCMs with writeout,
+   bunch_strong.c:80-91): the three gendst_datafile paths of the input. */
+int refws_write_distribution(void)
+{
+  static double a[30000], b[30000];
+  if (generate_initial_sbunch_distribution2(ws_model.nGen[LON], 1, LON, a, b, ring, ws_model) < 0) return -1;
+  if (generate_initial_sbunch_distribution2(ws_model.nGen[HOR], 1, HOR, a, b, ring, ws_model) < 0) return -1;
+  if (generate_initial_sbunch_distribution2(ws_model.nGen[VER], 1, VER, a, b, ring, ws_model) < 0) return -1;
+  return 0;
 }

@@ -181,3 +181,39 @@ def test_device_interpolation_bit_exact(tmp_path, cuda_device):
         got = dev.interp(ibn, icell, x, y)
         want = _np_interp(exey[:, 0], exey[:, 1], icell, w.ngrid, ax, az, x, y)
         assert np.array_equal(got, want), np.abs(got - want).max()
+
+
+def test_cli_slice_model_writes_reference_files(tmp_path, cuda_device):
+    """mbtrack-gpu on a BunchModel = STRONG file: the reference's generated
+    bunch and slicing, the device turn, and the files of the reference's
+    slice-model manager (its own writers, tests/golden/slice_fbii_cli.npz):
+    motion files every turn, ampinv files every NrevMon, the means and the
+    generated distribution.  Numbers may sit one unit apart in the last
+    printed digit (tests/test_gpu_cli.py's rule); nothing else may differ."""
+    import subprocess
+    from mbtrack_b200 import build
+    from tests.test_gpu_cli import compare_text
+    from tests.util import SLICE_CLI_OVER
+    build.build()
+    over = dict(SLICE_CLI_OVER)
+    for pl in ("LON", "HOR", "VER"):
+        over["gendst_datafile_" + pl] = str(tmp_path / ("gendst_" + pl))
+    conf = slice_conf(tmp_path, "train", **over)
+    work = tmp_path / "work"
+    work.mkdir()
+    r = subprocess.run([build.CLI, conf, str(work)], cwd=str(work), capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr + r.stdout
+    assert "Starting multi bunch tracking..." in r.stdout and " done" in r.stdout
+    z = np.load(os.path.join(GOLDEN, "slice_fbii_cli.npz"))
+    ref = {k: str(z[k]) for k in z.files}
+    ours = sorted(os.listdir(work))
+    assert ours == sorted(k for k in ref if not k.startswith("gendst_"))
+    flips, total, bad = 0, 0, []
+    for f in ours + ["gendst_LON", "gendst_HOR", "gendst_VER"]:
+        p = work / f if not f.startswith("gendst_") else tmp_path / f
+        n, b = compare_text(f, p.read_text(), ref[f])
+        bad += b
+        flips += n
+        total += len(ref[f].split())
+    assert not bad, "\n".join(bad[:30])
+    assert flips <= max(3, total // 10000), "%d numbers one digit apart of %d tokens" % (flips, total)

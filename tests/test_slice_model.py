@@ -178,3 +178,43 @@ def test_slice_model_needs_a_device(tmp_path, libmbt):
     with pytest.raises(api.MbtError) as e:
         api.SliceModel(w, bucket, ib, np.ones(S, np.int32), np.zeros((S, 5, 5), np.int32))
     assert e.value.code == -7
+
+
+@pytest.mark.reference
+@pytest.mark.parametrize("case", ["train", "nofbii"])
+def test_writer_matches_reference_files(tmp_path, libmbt, case):
+    """mbt_ws_writer_* writes the slice-model manager's files byte for byte
+    as the reference's own writers do on the same numbers: CMmotionsV.out,
+    CMImotionsH/V.out, ampinv_<P>_<turn>.dat every NrevMon (with the
+    reference's history indexing), ampinv/cmpos means, gendst files."""
+    if not binding.reference_available() and not os.path.exists(binding.REF_SO):
+        pytest.skip("reference harness unavailable")
+    over = {"NrevTot": 30, "NrevMon": 10}
+    if case == "nofbii":
+        over["EnableFBII"] = 0
+    for pl in ("LON", "HOR", "VER"):
+        over["gendst_datafile_" + pl] = str(tmp_path / ("ref_gendst_" + pl))
+    path = slice_conf(tmp_path, "train", **over)
+    ref_dir, mine_dir = tmp_path / "ref", tmp_path / "mine"
+    ref_dir.mkdir()
+    mine_dir.mkdir()
+    r = binding.ReferenceSlices(path, workdir=str(ref_dir))
+    r.files(True)
+    r.write_distribution()
+    cm, ion, zcm, st = r.run(30, 10)
+    r.finish()
+    w, bucket, _ = _product(tmp_path, "train", **over)
+    wr = api.SliceWriter(str(mine_dir), w, bucket)
+    wr.turns(ion[:13], zcm[:13], st[:2])
+    wr.turns(ion[13:], zcm[13:], st[2:])
+    soa, _ = api.SliceModel.reference_beam(w, len(bucket))
+    mine_g = [str(tmp_path / ("mine_gendst_" + pl)) for pl in ("LON", "HOR", "VER")]
+    wr.distribution(mine_g, soa)
+    wr.close()
+    names = sorted(os.listdir(ref_dir))
+    assert names == sorted(os.listdir(mine_dir))
+    assert ("CMImotionsH.out" in names) == (case == "train") and "ampinv_VER_21.dat" in names
+    for n in names:
+        assert (ref_dir / n).read_bytes() == (mine_dir / n).read_bytes(), n
+    for pl, m in zip(("LON", "HOR", "VER"), mine_g):
+        assert (tmp_path / ("ref_gendst_" + pl)).read_bytes() == open(m, "rb").read(), pl

@@ -135,6 +135,8 @@ SLICE_CASES = {
              "Iring": 3.38},
 }
 SLICE_TURNS = 30
+# the drop-in executable's slice-model run: 60 turns, monitors every 20
+SLICE_CLI_OVER = {"Np": 2000, "NrevTot": 60, "NrevMon": 20}
 
 
 def slice_conf(tmp_path, case, **over):

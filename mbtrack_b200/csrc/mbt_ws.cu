@@ -16,7 +16,8 @@
 //                194-253) and the long-range resistive-wall kick of every
 //                source bunch (transformSbunch_longrange :68-192), one
 //                thread per source, added in source order;
-//   ws_train     one block per SOURCE bunch, MBT_WS_IPT macro-ions per thread: the
+//   ws_train     MBT_WS_SPLIT blocks per SOURCE bunch (one for up to 512
+//                ions), MBT_WS_IPT macro-ions per thread: the
 //                ions of that bunch travel down the train (drift between
 //                buckets, pull by each slice of each later bunch,
 //                fbi_weakstrong_train fbi_weakstrong.c:325-426); per later
@@ -72,12 +73,16 @@ constexpr long kChunk = 256;   // turns per block of host outputs
 #ifndef MBT_WS_IPT
 #define MBT_WS_IPT 2             // macro-ions per thread in the ion train
 #endif
+#ifndef MBT_WS_SPLIT
+#define MBT_WS_SPLIT 2           // train blocks per source bunch (above 512 ions)
+#endif
 constexpr int kIpt = MBT_WS_IPT;
 // largest train block: 49 slices x 25 grid points, kIpt ions a thread
 constexpr int kTrainMaxThreads = ((kMaxSlices * 25 + kIpt - 1) / kIpt + 31) / 32 * 32;
 
 struct WsConst {
   int nb, S, G, off, nion, nmt, nharm, fbii, rw_long, trigger_rw, Nmlt;
+  int nsplit;   // train blocks per source bunch
   int track[3];
   long nrev_mon;
   double vrf_e0, wrf, phai0, Urad, T0, ac;
@@ -349,18 +354,49 @@ __global__ void __launch_bounds__(kRwThreads) ws_optic_rw(WsConst C, double *__r
   }
 }
 
+__device__ __forceinline__ void warp_sum4(double &a, double &b, double &c, double &d) {
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+    d += __shfl_xor_sync(0xffffffffu, d, o);
+  }
+}
+
+// One slice's pull on this thread's ions: the kick-sum shares (ax, ay).
+__device__ __forceinline__ void train_pull(const WsConst &C, const double *__restrict__ Ex,
+                                           const double *__restrict__ Ey, int c, const double (&N)[kIpt],
+                                           double (&X)[kIpt], double (&XD)[kIpt], double (&Y)[kIpt],
+                                           double (&YD)[kIpt], double &ax, double &ay) {
+  ax = 0.0;
+  ay = 0.0;
+#pragma unroll
+  for (int q = 0; q < kIpt; ++q) {
+    double ex, ey;
+    ws_interp(C, Ex, Ey, c, X[q], Y[q], ex, ey);
+    XD[q] = XD[q] + C.deltT * (C.factF * ex);
+    X[q] = X[q] + C.deltT * XD[q];
+    YD[q] = YD[q] + C.deltT * (C.factF * ey);
+    Y[q] = Y[q] + C.deltT * YD[q];
+    ax += N[q] * ex;
+    ay += N[q] * ey;
+  }
+}
+
 __global__ void __launch_bounds__(kTrainMaxThreads) ws_train(WsConst C, const int *__restrict__ bucket,
-                                                 const double *__restrict__ fx, const double *__restrict__ fy,
-                                                 const double *__restrict__ ion, double *__restrict__ part,
-                                                 double *__restrict__ ipart) {
+                                                             const double *__restrict__ fx,
+                                                             const double *__restrict__ fy,
+                                                             const double *__restrict__ ion,
+                                                             double *__restrict__ part, double *__restrict__ ipart) {
   extern __shared__ double sw[];   // [S][nw][2] kick shares, then [nw][2] centroid shares
-  const int src = blockIdx.x, tid = threadIdx.x, n = C.nion, S = C.S;
+  const int src = blockIdx.x / C.nsplit, piece = blockIdx.x - src * C.nsplit;
+  const int tid = threadIdx.x, n = C.nion, S = C.S;
   const int nw = blockDim.x >> 5, lane = tid & 31, wid = tid >> 5;
   const double *li = ion + (size_t)src * 5 * n;
   double N[kIpt], X[kIpt], XD[kIpt], Y[kIpt], YD[kIpt];
 #pragma unroll
   for (int q = 0; q < kIpt; ++q) {
-    const int p = tid + q * blockDim.x;
+    const int p = (piece * kIpt + q) * blockDim.x + tid;
     const bool ok = p < n;
     N[q] = ok ? li[p] : 0.0;
     X[q] = ok ? li[n + p] : 0.0;
@@ -379,50 +415,61 @@ __global__ void __launch_bounds__(kTrainMaxThreads) ws_train(WsConst C, const in
       Y[q] = Y[q] + Dt * YD[q];
     }
     const double *Ex = fx + (size_t)k * n, *Ey = fy + (size_t)k * n;
-    for (int c = 0; c < S; ++c) {
-      double ax = 0.0, ay = 0.0;
+    // slices two at a time: the two slices' shuffle reductions interleave
+    int c = 0;
+    for (; c + 1 < S; c += 2) {
+      double ax0, ay0, ax1, ay1;
+      train_pull(C, Ex, Ey, c, N, X, XD, Y, YD, ax0, ay0);
+      train_pull(C, Ex, Ey, c + 1, N, X, XD, Y, YD, ax1, ay1);
+      warp_sum4(ax0, ay0, ax1, ay1);
+      if (lane == 0) {
+        wsum[((size_t)c * nw + wid) * 2] = ax0;
+        wsum[((size_t)c * nw + wid) * 2 + 1] = ay0;
+        wsum[((size_t)(c + 1) * nw + wid) * 2] = ax1;
+        wsum[((size_t)(c + 1) * nw + wid) * 2 + 1] = ay1;
+      }
+    }
+    double cx = 0.0, cy = 0.0;
+    if (c < S) {
+      double ax, ay;
+      train_pull(C, Ex, Ey, c, N, X, XD, Y, YD, ax, ay);
 #pragma unroll
       for (int q = 0; q < kIpt; ++q) {
-        double ex, ey;
-        ws_interp(C, Ex, Ey, c, X[q], Y[q], ex, ey);
-        XD[q] = XD[q] + C.deltT * (C.factF * ex);
-        X[q] = X[q] + C.deltT * XD[q];
-        YD[q] = YD[q] + C.deltT * (C.factF * ey);
-        Y[q] = Y[q] + C.deltT * YD[q];
-        ax += N[q] * ex;
-        ay += N[q] * ey;
+        cx += N[q] * X[q];
+        cy += N[q] * Y[q];
       }
-      ax = warp_sum(ax);
-      ay = warp_sum(ay);
+      warp_sum4(ax, ay, cx, cy);
       if (lane == 0) {
         wsum[((size_t)c * nw + wid) * 2] = ax;
         wsum[((size_t)c * nw + wid) * 2 + 1] = ay;
       }
-    }
-    double cx = 0.0, cy = 0.0;
+    } else {
 #pragma unroll
-    for (int q = 0; q < kIpt; ++q) {
-      cx += N[q] * X[q];
-      cy += N[q] * Y[q];
+      for (int q = 0; q < kIpt; ++q) {
+        cx += N[q] * X[q];
+        cy += N[q] * Y[q];
+      }
+      cx = warp_sum(cx);
+      cy = warp_sum(cy);
     }
-    cx = warp_sum(cx);
-    cy = warp_sum(cy);
     if (lane == 0) {
       wcm[wid * 2] = cx;
       wcm[wid * 2 + 1] = cy;
     }
     __syncthreads();
-    const size_t rowk = (size_t)k * (k - 1) / 2;
+    // shares of destination k: row of k x nsplit source pieces
+    const size_t row = (size_t)k * C.nsplit, rowk = (size_t)k * (k - 1) / 2 * C.nsplit;
+    const size_t col = (size_t)src * C.nsplit + piece;
     for (int t = tid; t < 2 * S; t += blockDim.x) {
-      const int c = t >> 1, comp = t & 1;
+      const int cc = t >> 1, comp = t & 1;
       double v = 0.0;
-      for (int w = 0; w < nw; ++w) v += wsum[((size_t)c * nw + w) * 2 + comp];
-      part[((rowk * S) + (size_t)c * k + src) * 2 + comp] = v;
+      for (int w = 0; w < nw; ++w) v += wsum[((size_t)cc * nw + w) * 2 + comp];
+      part[((rowk * S) + (size_t)cc * row + col) * 2 + comp] = v;
     }
     if (tid < 2) {
       double v = 0.0;
       for (int w = 0; w < nw; ++w) v += wcm[w * 2 + tid];
-      ipart[(rowk + src) * 2 + tid] = v;
+      ipart[(rowk + col) * 2 + tid] = v;
     }
     __syncthreads();
     kbprev = kb;
@@ -439,13 +486,13 @@ __global__ void __launch_bounds__(kKickThreads) ws_kick(WsConst C, const int *__
   const int k = blockIdx.x, S = C.S, tid = threadIdx.x;
   double *sl = s + (size_t)k * 6 * S;
   double *xp = sl + 3 * S, *zz = sl + 4 * S, *zp = sl + 5 * S;
-  const size_t rowk = (size_t)k * (k - 1) / 2;
+  const size_t row = (size_t)k * C.nsplit, rowk = (size_t)k * (k - 1) / 2 * C.nsplit;
   if (C.fbii && k > 0 && tid < S) {
     const int c = tid;
     double sx = 0.0, sy = 0.0;
-    for (int src = 0; src < k; ++src) {
-      sx += part[((rowk * S) + (size_t)c * k + src) * 2];
-      sy += part[((rowk * S) + (size_t)c * k + src) * 2 + 1];
+    for (size_t j = 0; j < row; ++j) {
+      sx += part[((rowk * S) + (size_t)c * row + j) * 2];
+      sy += part[((rowk * S) + (size_t)c * row + j) * 2 + 1];
     }
     const double dQ = nelec[k] * (double)npop[c] * kECharge;
     const double factjp = dQ > 0.0 ? C.factjp0 / dQ : 0.0;
@@ -457,9 +504,9 @@ __global__ void __launch_bounds__(kKickThreads) ws_kick(WsConst C, const int *__
   if (tid == kKickThreads - 1 && ion_out) {
     double xs = 0.0, ys = 0.0, nt = 0.0;
     if (C.fbii) {
-      for (int src = 0; src < k; ++src) {
-        xs += ipart[(rowk + src) * 2];
-        ys += ipart[(rowk + src) * 2 + 1];
+      for (size_t j = 0; j < row; ++j) {
+        xs += ipart[(rowk + j) * 2];
+        ys += ipart[(rowk + j) * 2 + 1];
       }
       xs += own[(size_t)k * 3 + 1];
       ys += own[(size_t)k * 3 + 2];
@@ -636,7 +683,8 @@ extern "C" int mbt_ws_create(const mbt_ws_params *w, int nbunch, const int *buck
   if (!ws) return ws_fail(nullptr, MBT_ERR_NOMEM, "mbt_ws_create: out of host memory");
   ws->w = *w;
   ws_constants(w, nbunch, &ws->C);
-  ws->tpb = ((nion + kIpt - 1) / kIpt + 31) / 32 * 32;
+  ws->C.nsplit = nion > 512 ? MBT_WS_SPLIT : 1;
+  ws->tpb = ((nion + kIpt * ws->C.nsplit - 1) / (kIpt * ws->C.nsplit) + 31) / 32 * 32;
   const WsConst &C = ws->C;
   const size_t nb = (size_t)nbunch, pairs = nb * (nb - 1) / 2;
   std::vector<double> nelec(nb);
@@ -657,8 +705,8 @@ extern "C" int mbt_ws_create(const mbt_ws_params *w, int nbunch, const int *buck
   WS_ALLOC(ws->d_fy, nb * nion);
   WS_ALLOC(ws->d_ion, nb * 5 * nion);
   WS_ALLOC(ws->d_own, nb * 3);
-  WS_ALLOC(ws->d_part, (pairs > 0 ? pairs : 1) * S * 2);
-  WS_ALLOC(ws->d_ipart, (pairs > 0 ? pairs : 1) * 2);
+  WS_ALLOC(ws->d_part, (pairs > 0 ? pairs : 1) * C.nsplit * S * 2);
+  WS_ALLOC(ws->d_ipart, (pairs > 0 ? pairs : 1) * C.nsplit * 2);
   WS_ALLOC(ws->d_cm, (size_t)kChunk * nb * 6);
   WS_ALLOC(ws->d_io, (size_t)kChunk * nb * 2);
   WS_ALLOC(ws->d_zcm, (size_t)kChunk * C.nharm);
@@ -748,8 +796,8 @@ extern "C" int mbt_ws_run_turns(mbt_ws *ws, long nturns, double *cm, double *ion
       ws_optic_rw<<<C.nb, kRwThreads, nb * sizeof(double), st>>>(C, ws->d_s, ws->d_hist, ws->d_ibunch,
                                                                   ws->d_bucket, rev);
       if (C.fbii && C.nb > 1)
-        ws_train<<<C.nb, ws->tpb, train_smem, st>>>(C, ws->d_bucket, ws->d_fx, ws->d_fy, ws->d_ion, ws->d_part,
-                                                    ws->d_ipart);
+        ws_train<<<C.nb * C.nsplit, ws->tpb, train_smem, st>>>(C, ws->d_bucket, ws->d_fx, ws->d_fy, ws->d_ion,
+                                                               ws->d_part, ws->d_ipart);
       ws_kick<<<C.nb, kKickThreads, 0, st>>>(C, ws->d_bucket, ws->d_npop, ws->d_nelec, ws->d_s, ws->d_part,
                                              ws->d_ipart, ws->d_own, ion ? ws->d_io + (size_t)t * nb * 2 : nullptr,
                                              zcm ? ws->d_zcm + (size_t)t * C.nharm : nullptr);
@@ -799,8 +847,8 @@ extern "C" int mbt_ws_profile(mbt_ws *ws, long nturns, double *ms4) {
                                                                 rev);
     WS_CUDA(ws, cudaEventRecord(ws->ev[2], st));
     if (C.fbii && C.nb > 1)
-      ws_train<<<C.nb, ws->tpb, train_smem, st>>>(C, ws->d_bucket, ws->d_fx, ws->d_fy, ws->d_ion, ws->d_part,
-                                                  ws->d_ipart);
+      ws_train<<<C.nb * C.nsplit, ws->tpb, train_smem, st>>>(C, ws->d_bucket, ws->d_fx, ws->d_fy, ws->d_ion,
+                                                             ws->d_part, ws->d_ipart);
     WS_CUDA(ws, cudaEventRecord(ws->ev[3], st));
     ws_kick<<<C.nb, kKickThreads, 0, st>>>(C, ws->d_bucket, ws->d_npop, ws->d_nelec, ws->d_s, ws->d_part,
                                            ws->d_ipart, ws->d_own, nullptr, nullptr);

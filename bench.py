@@ -487,6 +487,61 @@ def slice_cpu(conf, turns):
     return (time.perf_counter() - t0) / turns, kind, r.nb
 
 
+
+def slice_growth_compare(turns):
+    """Growth rate of the vertical coupled-bunch motion in the slice model
+    and in the per-particle beam-ion stage on one configuration: the
+    200-bunch train of tests/confs/beam_ion.conf (same ring, fill and
+    charge), CO at the slice model's pressure (2.7e-9 mbar x 5 x 0.15 / 1.3332
+    = 1.519 nTorr, fbi_weakstrong.c:20-36) ionised over the whole
+    circumference (one interaction point), no wall, no chromaticity (the
+    slice model has none), no radiation noise or damping.  The slice model
+    runs with the reference's ion kick factor 1e2 and with the thin-lens
+    value 1; the per-particle stage with 5e3 macroparticles per bunch."""
+    import numpy as np
+    import torch
+    import tempfile
+    from mbtrack_b200 import analysis, api
+    from oracle.binding import conf_with
+    tmp = tempfile.mkdtemp()
+    fill = os.path.join(CONFS, "beam_ion_fill.txt")
+    out = {"config": "200-bunch train x 0.5 nC, CO at 1.519 nTorr over the ring, 1 interaction point, no wall, "
+                     "no chromaticity, no radiation noise", "turns": turns}
+
+    def rate(a):
+        wdw = analysis.exponential_window(a)
+        return {"window": list(wdw) if wdw else None, "rate_per_turn": analysis.growth_rate(a, wdw) if wdw else None,
+                "start": float(np.median(a[:50])), "max": float(a.max())}
+
+    sconf = conf_with(os.path.join(CONFS, "slice_fbii.conf"), os.path.join(tmp, "s.conf"), Nslc=23, Np=5000,
+                      Iring=84.6875, NrevTot=turns, NrevMon=100, EnableRW_long=0, filling=fill)
+    for kf in (1e2, 1.0):
+        w, bucket, ib, npop, nofe, s0 = slice_setup(sconf)
+        w.kick_factor = kf
+        dev = api.SliceModel(w, bucket, ib, npop, nofe)
+        dev.load_slices(s0)
+        t0 = time.perf_counter()
+        cm = dev.run(turns)[0]
+        dev.close()
+        r = rate(np.sqrt((cm[:, :, 4] ** 2).mean(axis=1)))
+        r["seconds"] = time.perf_counter() - t0
+        out["slice_kick_factor_%g" % kf] = r
+    pconf = conf_with(os.path.join(CONFS, "beam_ion.conf"), os.path.join(tmp, "p.conf"), NrevTot=turns, Cx=0.0,
+                      Cz=0.0, EnableQuantum=0, n_ip=1, pressure_nTorr=0.15 * 5 * 2.7 / 1.3332, filling=fill)
+    cfg = api.Config(pconf)
+    t = api.Tracker(cfg.params, cfg.bucket, np.full(cfg.nbunch, 5000), cfg.bunch_currents())
+    t.generate_beam(3)
+    t.enable_beam_ion(cfg.beam_ion())
+    t.prepare()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    st = t.run(turns)
+    t.close()
+    r = rate(analysis.centroid_amplitude(st, "VER"))
+    r["seconds"] = time.perf_counter() - t0
+    out["per_particle"] = r
+    return out
+
 def run_slice_b200(args):
     import numpy as np
     import torch
@@ -577,6 +632,8 @@ def run_slice_b200(args):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if args.growth_turns > 0:
+        line["growth_compare"] = slice_growth_compare(args.growth_turns)
     print(json.dumps(line))
 
 
@@ -656,7 +713,8 @@ def main():
     ap.add_argument("--mlp-steps", type=int, default=48000, help="training steps of the learned field")
     ap.add_argument("--growth-turns", type=int, default=0,
                     help="beam_ion_mlp: also compare the instability growth rate of the learned and the "
-                         "Faddeeva stage over this many turns on a reduced train (0: skip)")
+                         "Faddeeva stage over this many turns on a reduced train; slice_fbii: compare the "
+                         "slice model's growth rate with the per-particle stage's (0: skip)")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 20 if args.workload.startswith("beam_ion") or args.workload == "slice_fbii" else 200

@@ -66,6 +66,11 @@ typedef struct mbt_ws_params {
      negative sigmas): sgm_xtau [ns], sgm_xeps, sgm_xx [mm], sgm_xp [mrad],
      sgm_zz [mm], sgm_zp [mrad]; the CM offsets in the same units */
   double sgm_in[6], cm_in[6];
+  /* factRN of fbi_weakstrong.c:334, the factor on the ions' kick on the
+     electron slices: 1e2 in the reference (its comment marks it as an
+     assumption); 1 is the thin-lens kick of the ions' charge, since
+     e^2 / m_e = 4 pi eps0 r_e c^2 */
+  double kick_factor;
 } mbt_ws_params;
 
 /* Read an mbtrack .conf file with BunchModel = STRONG: read_conf_file,

@@ -109,7 +109,7 @@ class MbtWsParams(ctypes.Structure):
         ("sgm_xx", _d), ("sgm_zz", _d), ("sgmatau", _d), ("max_tau", _d), ("dtau", _d),
         ("agLOCx", _d), ("agLOCz", _d), ("agABSx", _d), ("agABSz", _d),
         ("deltT", _d), ("factBE", _d), ("factF", _d), ("Ldmsgm", _d), ("Gamma", _d),
-        ("sgm_in", _d * 6), ("cm_in", _d * 6),
+        ("sgm_in", _d * 6), ("cm_in", _d * 6), ("kick_factor", _d),
     ]
 
     @property

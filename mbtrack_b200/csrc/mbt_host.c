@@ -847,6 +847,7 @@ static int ws_derive(const cfg_t *g, mbt_ws_params *w)
   w->Ldmsgm = Lu20 * dm * sigmam * 1e-22;
   w->factF = WS_E_CHARGE / (28.0 * WS_MP_O_EM * WS_E_MASS);
   w->Gamma = 1957.0 * g->p.E0;
+  w->kick_factor = 1e+2;
   return 0;
 }
 

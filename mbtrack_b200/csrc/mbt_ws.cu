@@ -16,7 +16,7 @@
 //                194-253) and the long-range resistive-wall kick of every
 //                source bunch (transformSbunch_longrange :68-192), one
 //                thread per source, added in source order;
-//   ws_train     MBT_WS_SPLIT blocks per SOURCE bunch (one for up to 512
+//   ws_train     one block per SOURCE bunch (MBT_WS_SPLIT blocks above 512
 //                ions), MBT_WS_IPT macro-ions per thread: the
 //                ions of that bunch travel down the train (drift between
 //                buckets, pull by each slice of each later bunch,
@@ -74,7 +74,10 @@ constexpr long kChunk = 256;   // turns per block of host outputs
 #define MBT_WS_IPT 2             // macro-ions per thread in the ion train
 #endif
 #ifndef MBT_WS_SPLIT
-#define MBT_WS_SPLIT 2           // train blocks per source bunch (above 512 ions)
+#define MBT_WS_SPLIT 1           // train blocks per source bunch (above 512 ions)
+#endif
+#ifndef MBT_WS_PAIR
+#define MBT_WS_PAIR 0            // reduce the kick sums of two slices together
 #endif
 constexpr int kIpt = MBT_WS_IPT;
 // largest train block: 49 slices x 25 grid points, kIpt ions a thread
@@ -94,7 +97,7 @@ struct WsConst {
   double factBE, sgm_xx, sgm_zz, agLOCx, agLOCz, agABSx, agABSz, deltT, factF, Ldmsgm;
   double rABSx, rABSz;   // 1 / agABSx, 1 / agABSz, correctly rounded
   double fdq_den;   // 2 eps0 sqrt(pi) factBE c deltT
-  double factjp0;   // 1e2 4 pi eps0 r_e / Gamma
+  double factjp0;   // factRN 4 pi eps0 r_e / Gamma
   double T0h;       // T0 / h
   double cdt;       // c deltT
 };
@@ -417,6 +420,18 @@ __global__ void __launch_bounds__(kTrainMaxThreads) ws_train(WsConst C, const in
     const double *Ex = fx + (size_t)k * n, *Ey = fy + (size_t)k * n;
     // slices two at a time: the two slices' shuffle reductions interleave
     int c = 0;
+#if !MBT_WS_PAIR
+    for (; c + 1 < S; ++c) {
+      double ax, ay;
+      train_pull(C, Ex, Ey, c, N, X, XD, Y, YD, ax, ay);
+      ax = warp_sum(ax);
+      ay = warp_sum(ay);
+      if (lane == 0) {
+        wsum[((size_t)c * nw + wid) * 2] = ax;
+        wsum[((size_t)c * nw + wid) * 2 + 1] = ay;
+      }
+    }
+#endif
     for (; c + 1 < S; c += 2) {
       double ax0, ay0, ax1, ay1;
       train_pull(C, Ex, Ey, c, N, X, XD, Y, YD, ax0, ay0);
@@ -652,7 +667,7 @@ static void ws_constants(const mbt_ws_params *w, int nb, WsConst *C) {
   C->factF = w->factF;
   C->Ldmsgm = w->Ldmsgm;
   C->fdq_den = 2 * kEps0 * sqrt(M_PI) * w->factBE * kCLight * w->deltT;
-  C->factjp0 = 1e+2 * 4.0 * M_PI * kEps0 * kERadius / w->Gamma;
+  C->factjp0 = w->kick_factor * 4.0 * M_PI * kEps0 * kERadius / w->Gamma;
   C->T0h = p->T0 / (double)p->nharm;
   C->cdt = kCLight * w->deltT;
 }

@@ -420,6 +420,7 @@ class ReferenceSlices:
         w.agLOCx, w.agLOCz, w.agABSx, w.agABSz = self.agLOCx, self.agLOCz, self.agABSx, self.agABSz
         w.deltT, w.factBE, w.factF, w.Ldmsgm = self.deltT, self.factBE, self.factF, self.Ldmsgm
         w.Gamma = 1957.0 * w.base.E0
+        w.kick_factor = 1e2
         return w
 
     def particles(self):

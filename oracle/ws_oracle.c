@@ -421,7 +421,7 @@ int ows_run(ows_t *o, long nturns, double *cm, double *ion, double *zcm, double 
         const double *li = o->li + (size_t) ib * 5 * n;
         long q;
         if (w->fbii && ib > 0) {
-          const double factjp0 = 1e+2 * 4.0 * M_PI * ORC_EPSILON0 * ORC_E_RADIUS / w->Gamma;
+          const double factjp0 = w->kick_factor * 4.0 * M_PI * ORC_EPSILON0 * ORC_E_RADIUS / w->Gamma;
           const double Nelec = (o->ib[ib] * p->T0 / (w->np * ORC_E_CHARGE * ORC_FKILO));
           const double Dtime = fabs((double) (kb - kbF)) * (p->T0 / (double) p->nharm);
           const double *Ex = o->ex + (size_t) ib * n, *Ey = o->ey + (size_t) ib * n;

@@ -14,7 +14,7 @@ from oracle import binding
 from tests.util import GOLDEN, SLICE_CASES, SLICE_TURNS, slice_conf
 
 DERIVED = ("nslc", "fbii", "np", "ngrid", "ndivs", "sgm_xx", "sgm_zz", "sgmatau", "max_tau", "dtau", "agLOCx",
-           "agLOCz", "agABSx", "agABSz", "deltT", "factBE", "factF", "Ldmsgm", "Gamma")
+           "agLOCz", "agABSx", "agABSz", "deltT", "factBE", "factF", "Ldmsgm", "Gamma", "kick_factor")
 BASE = ("nharm", "E0", "T0", "wrf", "Vrf0", "phai0", "Urad", "ac", "QH0", "QV0", "Lc", "Iring", "Nmlt",
         "triggerRW", "rw_long", "nrev_tot", "nrev_mon")
 

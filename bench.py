@@ -511,10 +511,14 @@ def slice_growth_compare(turns):
     def rate(a):
         wdw = analysis.exponential_window(a)
         return {"window": list(wdw) if wdw else None, "rate_per_turn": analysis.growth_rate(a, wdw) if wdw else None,
-                "start": float(np.median(a[:50])), "max": float(a.max())}
+                "start": float(np.median(a[:50])), "max": float(a.max()),
+                "amplitude_every_100_turns": [float(x) for x in a[::100]]}
 
+    # bunch offsets of 0.1 um rms (slice model): a start below the
+    # per-particle stage's sampling noise (0.26 um), as in a linear regime
     sconf = conf_with(os.path.join(CONFS, "slice_fbii.conf"), os.path.join(tmp, "s.conf"), Nslc=23, Np=5000,
-                      Iring=84.6875, NrevTot=turns, NrevMon=100, EnableRW_long=0, filling=fill)
+                      Iring=84.6875, NrevTot=turns, NrevMon=100, EnableRW_long=0, filling=fill, xxCM_offset=0.0001,
+                      xpCM_offset=0.00001, zzCM_offset=0.0001, zpCM_offset=0.00001)
     for kf in (1e2, 1.0):
         w, bucket, ib, npop, nofe, s0 = slice_setup(sconf)
         w.kick_factor = kf

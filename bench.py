@@ -508,6 +508,14 @@ def slice_growth_compare(turns):
     out = {"config": "200-bunch train x 0.5 nC, CO at 1.519 nTorr over the ring, 1 interaction point, no wall, "
                      "no chromaticity, no radiation noise", "turns": turns}
 
+    def envelope(z, zp, par):
+        """rms over bunches of the betatron amplitude sqrt(beta J) of the
+        vertical centroid (J the Courant-Snyder invariant): free of the
+        turn-to-turn betatron phase."""
+        g, a, b = par.gamma1[2], par.alpha1[2], par.beta1[2]
+        inv = g * z * z + 2.0 * a * z * zp + b * zp * zp
+        return np.sqrt((b * inv).mean(axis=1))
+
     def rate(a):
         wdw = analysis.exponential_window(a)
         return {"window": list(wdw) if wdw else None, "rate_per_turn": analysis.growth_rate(a, wdw) if wdw else None,
@@ -527,7 +535,7 @@ def slice_growth_compare(turns):
         t0 = time.perf_counter()
         cm = dev.run(turns)[0]
         dev.close()
-        r = rate(np.sqrt((cm[:, :, 4] ** 2).mean(axis=1)))
+        r = rate(envelope(cm[:, :, 4], cm[:, :, 5], w.base))
         r["seconds"] = time.perf_counter() - t0
         out["slice_kick_factor_%g" % kf] = r
     pconf = conf_with(os.path.join(CONFS, "beam_ion.conf"), os.path.join(tmp, "p.conf"), NrevTot=turns, Cx=0.0,
@@ -541,7 +549,7 @@ def slice_growth_compare(turns):
     t0 = time.perf_counter()
     st = t.run(turns)
     t.close()
-    r = rate(analysis.centroid_amplitude(st, "VER"))
+    r = rate(envelope(st[:, :, 2], st[:, :, 8], cfg.params))
     r["seconds"] = time.perf_counter() - t0
     out["per_particle"] = r
     return out

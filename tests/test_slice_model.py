@@ -218,3 +218,28 @@ def test_writer_matches_reference_files(tmp_path, libmbt, case):
         assert (ref_dir / n).read_bytes() == (mine_dir / n).read_bytes(), n
     for pl, m in zip(("LON", "HOR", "VER"), mine_g):
         assert (tmp_path / ("ref_gendst_" + pl)).read_bytes() == open(m, "rb").read(), pl
+
+
+@pytest.mark.parametrize("case", sorted(SLICE_CASES))
+def test_reference_beam_matches_reference(tmp_path, libmbt, case):
+    """mbt_ws_reference_beam draws the reference's particles (the three
+    planes of generate_initial_sbunch_distribution2 on glibc's generator,
+    as a fresh reference process seeds it) and the bunch offsets of
+    generate_initial_general_distribution2; with the slicing they give the
+    reference manager's starting slices bit for bit."""
+    g = _golden(case)
+    w, bucket, _ = _product(tmp_path, case)
+    soa, off = api.SliceModel.reference_beam(w, len(bucket))
+    assert np.array_equal(soa, g["particles"])
+    _, _, cm4 = api.SliceModel.slice_beam(w, soa)
+    assert np.array_equal(api.SliceModel.initial_slices(w, cm4, off), g["slices0"])
+
+
+def test_bunch_model_probe(tmp_path, libmbt):
+    """mbt_config_bunch_model tells the drop-in executable which model a
+    file asks for."""
+    L = api.lib()
+    assert L.mbt_config_bunch_model(slice_conf(tmp_path, "train").encode()) == 1
+    assert L.mbt_config_bunch_model(os.path.join(os.path.dirname(os.path.abspath(__file__)), "confs",
+                                                 "uniform_fill.conf").encode()) == 0
+    assert L.mbt_config_bunch_model(str(tmp_path / "missing.conf").encode()) < 0

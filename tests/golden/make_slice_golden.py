@@ -6,7 +6,8 @@ oracle/ref_ws_harness.c on the configurations of SLICE_CASES (tests/util.py).
 Each file holds the particles the reference slices, its slicing (npop,
 nofe), the fill (bucket, ibunch [mA]), the initial slice state and the
 per-turn outputs of TURNS turns (cm, ion, zcm, stats) with the final slice
-state.  slice_fbii_cli.npz holds the files the reference's manager writes
+state (slice_fbii_uneven.npz: the 321-bunch fill of SLICE_UNEVEN, two turns,
+without the particles).  slice_fbii_cli.npz holds the files the reference's manager writes
 for SLICE_CLI_OVER (its writers called by the harness): name -> text.
 
     python tests/golden/make_slice_golden.py
@@ -21,10 +22,19 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle import binding  # noqa: E402
-from tests.util import SLICE_CASES, SLICE_CLI_OVER, SLICE_TURNS, slice_conf  # noqa: E402
+from tests.util import SLICE_CASES, SLICE_CLI_OVER, SLICE_TURNS, SLICE_UNEVEN, SLICE_UNEVEN_TURNS, slice_conf  # noqa: E402
 
 
 def main():
+    with tempfile.TemporaryDirectory() as tmp:
+        path = slice_conf(tmp, "train", **SLICE_UNEVEN)
+        r = binding.ReferenceSlices(path)
+        s0 = r.slices_state()
+        cm, ion, zcm, st = r.run(SLICE_UNEVEN_TURNS, r.params().base.nrev_mon)
+        out = os.path.join(HERE, "slice_fbii_uneven.npz")
+        np.savez_compressed(out, npop=r.npop, nofe=r.nofe, bucket=r.bucket, ibunch=r.ibunch, slices0=s0, cm=cm,
+                            ion=ion, zcm=zcm, stats=st, slices=r.slices_state())
+        print(out, r.nb, "bunches", r.slices, "slices")
     for case in SLICE_CASES:
         with tempfile.TemporaryDirectory() as tmp:
             path = slice_conf(tmp, case)

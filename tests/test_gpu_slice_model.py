@@ -16,7 +16,7 @@ import pytest
 
 from mbtrack_b200 import api
 from oracle import binding
-from tests.util import GOLDEN, SLICE_CASES, SLICE_TURNS, slice_conf
+from tests.util import GOLDEN, SLICE_CASES, SLICE_TURNS, SLICE_UNEVEN, SLICE_UNEVEN_TURNS, slice_conf
 
 pytestmark = pytest.mark.gpu
 
@@ -217,3 +217,18 @@ def test_cli_slice_model_writes_reference_files(tmp_path, cuda_device):
         total += len(ref[f].split())
     assert not bad, "\n".join(bad[:30])
     assert flips <= max(3, total // 10000), "%d numbers one digit apart of %d tokens" % (flips, total)
+
+
+def test_device_matches_reference_uneven_fill(tmp_path, cuda_device):
+    """The 321-bunch uneven fill: two device turns against the reference's
+    own (tests/golden/slice_fbii_uneven.npz)."""
+    g = np.load(os.path.join(GOLDEN, "slice_fbii_uneven.npz"))
+    w, bucket, frac = api.SliceModel.config(slice_conf(tmp_path, "train", **SLICE_UNEVEN))
+    L = api.lib()
+    ib = np.array([L.mbt_bunch_current(w.base, len(bucket), float(f)) * 1e3 for f in frac])
+    dev = api.SliceModel(w, bucket, ib, g["npop"], g["nofe"])
+    dev.load_slices(g["slices0"])
+    out = dev.run(SLICE_UNEVEN_TURNS)
+    for name, x in zip(("cm", "ion", "zcm", "stats"), out):
+        _close(x, g[name], 1e-11, name)
+    _close(dev.slices(), g["slices"], 1e-11, "slices")

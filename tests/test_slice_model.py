@@ -11,7 +11,7 @@ import pytest
 
 from mbtrack_b200 import api
 from oracle import binding
-from tests.util import GOLDEN, SLICE_CASES, SLICE_TURNS, slice_conf
+from tests.util import GOLDEN, SLICE_CASES, SLICE_TURNS, SLICE_UNEVEN, SLICE_UNEVEN_TURNS, slice_conf
 
 DERIVED = ("nslc", "fbii", "np", "ngrid", "ndivs", "sgm_xx", "sgm_zz", "sgmatau", "max_tau", "dtau", "agLOCx",
            "agLOCz", "agABSx", "agABSz", "deltT", "factBE", "factF", "Ldmsgm", "Gamma", "kick_factor")
@@ -243,3 +243,17 @@ def test_bunch_model_probe(tmp_path, libmbt):
     assert L.mbt_config_bunch_model(os.path.join(os.path.dirname(os.path.abspath(__file__)), "confs",
                                                  "uniform_fill.conf").encode()) == 0
     assert L.mbt_config_bunch_model(str(tmp_path / "missing.conf").encode()) < 0
+
+
+def test_oracle_matches_golden_uneven_fill(tmp_path, libmbt):
+    """The 321-bunch uneven fill (gaps, a 5 nC camshaft bunch, lognormal
+    charges): two turns of the oracle equal the reference's bit for bit."""
+    g = _golden("uneven")
+    w, bucket, ib = _product(tmp_path, "train", **SLICE_UNEVEN)
+    assert np.array_equal(bucket, g["bucket"]) and _same(ib, g["ibunch"])
+    o = binding.OracleSlices(w, bucket, ib, g["npop"], g["nofe"])
+    o.set_slices(g["slices0"])
+    out = o.run(SLICE_UNEVEN_TURNS)
+    for name, got in zip(("cm", "ion", "zcm", "stats"), out):
+        assert _same(got, g[name]), name
+    assert _same(o.slices_state(), g["slices"])

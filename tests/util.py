@@ -135,6 +135,11 @@ SLICE_CASES = {
              "Iring": 3.38},
 }
 SLICE_TURNS = 30
+# the 321-bunch uneven fill (three trains, camshaft bunch, lognormal charges)
+# with 21 slices, two turns
+SLICE_UNEVEN = {"Np": 2000, "NrevTot": 10, "Nslc": 10, "filling": os.path.join(CONFS, "uneven_fill.txt"),
+                "Iring": 150.0}
+SLICE_UNEVEN_TURNS = 2
 # the drop-in executable's slice-model run: 60 turns, monitors every 20
 SLICE_CLI_OVER = {"Np": 2000, "NrevTot": 60, "NrevMon": 20}
 

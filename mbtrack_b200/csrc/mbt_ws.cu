@@ -76,6 +76,9 @@ constexpr long kChunk = 256;   // turns per block of host outputs
 #ifndef MBT_WS_SPLIT
 #define MBT_WS_SPLIT 1           // train blocks per source bunch (above 512 ions)
 #endif
+#ifndef MBT_WS_EXCLUSIVE
+#define MBT_WS_EXCLUSIVE 0       // pad the train's shared memory to one block per SM
+#endif
 #ifndef MBT_WS_PAIR
 #define MBT_WS_PAIR 0            // reduce the kick sums of two slices together
 #endif
@@ -582,6 +585,13 @@ static int ws_fail(mbt_ws *ws, int code, const char *fmt, ...) {
     if (e_ != cudaSuccess) return ws_fail((ws), MBT_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
   } while (0)
 
+// dynamic shared memory of the train: the warps' kick and centroid shares,
+// padded past half an SM's 228 KB when one block per SM is wanted
+static size_t train_smem_bytes(int S, int tpb) {
+  const size_t need = ((size_t)S * (tpb / 32) * 2 + (tpb / 32) * 2) * sizeof(double);
+  return MBT_WS_EXCLUSIVE && need < 116 * 1024 ? 116 * 1024 : need;
+}
+
 static void ws_free(mbt_ws *ws) {
   void *ptrs[] = {ws->d_bucket, ws->d_npop, ws->d_nofe, ws->d_nelec, ws->d_ibunch, ws->d_s, ws->d_hist,
                   ws->d_fx, ws->d_fy, ws->d_ion, ws->d_own, ws->d_part, ws->d_ipart, ws->d_cm,
@@ -749,7 +759,7 @@ extern "C" int mbt_ws_create(const mbt_ws_params *w, int nbunch, const int *buck
     if (!ok) rc = ws_fail(nullptr, MBT_ERR_CUDA, "mbt_ws_create: upload failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   if (!rc) {
-    const size_t train_smem = ((size_t)S * (ws->tpb / 32) * 2 + (ws->tpb / 32) * 2) * sizeof(double);
+    const size_t train_smem = train_smem_bytes(S, ws->tpb);
     const size_t bunch_smem = 2 * (size_t)nion * sizeof(double);
     if (train_smem > 48 * 1024 &&
         cudaFuncSetAttribute(ws_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem) != cudaSuccess)
@@ -793,7 +803,7 @@ extern "C" int mbt_ws_run_turns(mbt_ws *ws, long nturns, double *cm, double *ion
   const cudaStream_t st = ws->stream;
   const size_t nb = (size_t)C.nb, S = (size_t)C.S, n = (size_t)C.nion;
   const size_t bunch_smem = 2 * n * sizeof(double);
-  const size_t train_smem = (S * (ws->tpb / 32) * 2 + (ws->tpb / 32) * 2) * sizeof(double);
+  const size_t train_smem = train_smem_bytes((int)S, ws->tpb);
   long imon_total = 0;
   ws->last_ms = 0.0;
   for (long t0 = 0; t0 < nturns; t0 += kChunk) {
@@ -850,7 +860,7 @@ extern "C" int mbt_ws_profile(mbt_ws *ws, long nturns, double *ms4) {
   const cudaStream_t st = ws->stream;
   const size_t nb = (size_t)C.nb, S = (size_t)C.S, n = (size_t)C.nion;
   const size_t bunch_smem = 2 * n * sizeof(double);
-  const size_t train_smem = (S * (ws->tpb / 32) * 2 + (ws->tpb / 32) * 2) * sizeof(double);
+  const size_t train_smem = train_smem_bytes((int)S, ws->tpb);
   double acc[4] = {0, 0, 0, 0};
   for (long t = 0; t < nturns; ++t) {
     const long rev = ws->turn;

@@ -394,7 +394,9 @@ __global__ void __launch_bounds__(kTrainMaxThreads) ws_train(WsConst C, const in
                                                              const double *__restrict__ fy,
                                                              const double *__restrict__ ion,
                                                              double *__restrict__ part, double *__restrict__ ipart) {
-  extern __shared__ double sw[];   // [S][nw][2] kick shares, then [nw][2] centroid shares
+  // [2][nion] the destination bunch's field grid, [S][nw][2] kick shares,
+  // [nw][2] centroid shares
+  extern __shared__ double sw[];
   const int src = blockIdx.x / C.nsplit, piece = blockIdx.x - src * C.nsplit;
   const int tid = threadIdx.x, n = C.nion, S = C.S;
   const int nw = blockDim.x >> 5, lane = tid & 31, wid = tid >> 5;
@@ -410,17 +412,25 @@ __global__ void __launch_bounds__(kTrainMaxThreads) ws_train(WsConst C, const in
     Y[q] = ok ? li[3 * n + p] : 0.0;
     YD[q] = ok ? li[4 * n + p] : 0.0;
   }
-  double *wsum = sw, *wcm = sw + (size_t)S * nw * 2;
+  double *gx = sw, *gy = sw + n;
+  double *wsum = sw + 2 * (size_t)n, *wcm = wsum + (size_t)S * nw * 2;
   int kbprev = bucket[src];
   for (int k = src + 1; k < C.nb; ++k) {
     const int kb = bucket[k];
     const double Dt = fabs((double)(kb - kbprev)) * C.T0h;
+    // the destination bunch's grid into shared memory: one coalesced pass
+    // instead of dependent L2 reads inside every pull
+    for (int i = tid; i < n; i += blockDim.x) {
+      gx[i] = fx[(size_t)k * n + i];
+      gy[i] = fy[(size_t)k * n + i];
+    }
 #pragma unroll
     for (int q = 0; q < kIpt; ++q) {
       X[q] = X[q] + Dt * XD[q];
       Y[q] = Y[q] + Dt * YD[q];
     }
-    const double *Ex = fx + (size_t)k * n, *Ey = fy + (size_t)k * n;
+    __syncthreads();
+    const double *Ex = gx, *Ey = gy;
     // slices two at a time: the two slices' shuffle reductions interleave
     int c = 0;
 #if !MBT_WS_PAIR
@@ -585,10 +595,11 @@ static int ws_fail(mbt_ws *ws, int code, const char *fmt, ...) {
     if (e_ != cudaSuccess) return ws_fail((ws), MBT_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
   } while (0)
 
-// dynamic shared memory of the train: the warps' kick and centroid shares,
-// padded past half an SM's 228 KB when one block per SM is wanted
-static size_t train_smem_bytes(int S, int tpb) {
-  const size_t need = ((size_t)S * (tpb / 32) * 2 + (tpb / 32) * 2) * sizeof(double);
+// dynamic shared memory of the train: one field grid, the warps' kick and
+// centroid shares; padded past half an SM's 228 KB when one block per SM is
+// wanted
+static size_t train_smem_bytes(int S, int nion, int tpb) {
+  const size_t need = (2 * (size_t)nion + (size_t)S * (tpb / 32) * 2 + (tpb / 32) * 2) * sizeof(double);
   return MBT_WS_EXCLUSIVE && need < 116 * 1024 ? 116 * 1024 : need;
 }
 
@@ -759,7 +770,7 @@ extern "C" int mbt_ws_create(const mbt_ws_params *w, int nbunch, const int *buck
     if (!ok) rc = ws_fail(nullptr, MBT_ERR_CUDA, "mbt_ws_create: upload failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   if (!rc) {
-    const size_t train_smem = train_smem_bytes(S, ws->tpb);
+    const size_t train_smem = train_smem_bytes(S, nion, ws->tpb);
     const size_t bunch_smem = 2 * (size_t)nion * sizeof(double);
     if (train_smem > 48 * 1024 &&
         cudaFuncSetAttribute(ws_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem) != cudaSuccess)
@@ -803,7 +814,7 @@ extern "C" int mbt_ws_run_turns(mbt_ws *ws, long nturns, double *cm, double *ion
   const cudaStream_t st = ws->stream;
   const size_t nb = (size_t)C.nb, S = (size_t)C.S, n = (size_t)C.nion;
   const size_t bunch_smem = 2 * n * sizeof(double);
-  const size_t train_smem = train_smem_bytes((int)S, ws->tpb);
+  const size_t train_smem = train_smem_bytes((int)S, (int)n, ws->tpb);
   long imon_total = 0;
   ws->last_ms = 0.0;
   for (long t0 = 0; t0 < nturns; t0 += kChunk) {
@@ -860,7 +871,7 @@ extern "C" int mbt_ws_profile(mbt_ws *ws, long nturns, double *ms4) {
   const cudaStream_t st = ws->stream;
   const size_t nb = (size_t)C.nb, S = (size_t)C.S, n = (size_t)C.nion;
   const size_t bunch_smem = 2 * n * sizeof(double);
-  const size_t train_smem = train_smem_bytes((int)S, ws->tpb);
+  const size_t train_smem = train_smem_bytes((int)S, (int)n, ws->tpb);
   double acc[4] = {0, 0, 0, 0};
   for (long t = 0; t < nturns; ++t) {
     const long rev = ws->turn;

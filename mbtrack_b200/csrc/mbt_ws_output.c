@@ -130,9 +130,9 @@ static int write_ampinv(mbt_ws_writer *wr, long rev, long mon, const double *sta
 int mbt_ws_writer_turns(mbt_ws_writer *wr, long nturns, const double *ion, const double *zcm, const double *stats)
 {
   long t, imon = 0;
-  int i;
-  const int nh = wr->w.base.nharm;
+  int i, nh;
   if (!wr || nturns < 0 || !zcm || (wr->w.fbii && !ion)) return wsfail(wr, MBT_ERR_INVALID, "bad arguments");
+  nh = wr->w.base.nharm;
   for (t = 0; t < nturns; t++, wr->rev++) {
     const long rev = wr->rev;
     if (rev % wr->w.base.nrev_mon == 0 && stats) {

@@ -83,11 +83,13 @@ def test_device_runs_repeat_bit_for_bit(tmp_path, cuda_device):
         assert np.array_equal(x, y, equal_nan=True)
 
 
-@pytest.mark.parametrize("over", [{"EnableFBII": 0}, {"EnableRW_long": 0}, {"NrevMon": 1}],
-                         ids=["no_fbii", "no_rw", "mon_every_turn"])
+@pytest.mark.parametrize("over", [{"EnableFBII": 0}, {"EnableRW_long": 0}, {"NrevMon": 1}, {"Nslc": 3}],
+                         ids=["no_fbii", "no_rw", "mon_every_turn", "nslc3_all_in_overflow"])
 def test_device_variants(tmp_path, cuda_device, over):
     """Beam-ion off (no ions: NaN ion centroid, resistive wall only),
-    resistive wall off, statistics every turn."""
+    resistive wall off, statistics every turn, and the reference's default
+    Nslc = 3, where every particle falls in the overflow cell (empty slices:
+    NaN centroids, as in the reference)."""
     w, bucket, ib, npop, nofe, g = _setup(tmp_path, "train", **over)
     dev = api.SliceModel(w, bucket, ib, npop, nofe)
     dev.load_slices(g["slices0"])

@@ -91,10 +91,12 @@ def test_device_variants(tmp_path, cuda_device, over):
     Nslc = 3, where every particle falls in the overflow cell (empty slices:
     NaN centroids, as in the reference)."""
     w, bucket, ib, npop, nofe, g = _setup(tmp_path, "train", **over)
+    soa, off = api.SliceModel.reference_beam(w, len(bucket))
+    s0 = api.SliceModel.initial_slices(w, api.SliceModel.slice_beam(w, soa)[2], off)
     dev = api.SliceModel(w, bucket, ib, npop, nofe)
-    dev.load_slices(g["slices0"])
+    dev.load_slices(s0)
     o = binding.OracleSlices(w, bucket, ib, npop, nofe)
-    o.set_slices(g["slices0"])
+    o.set_slices(s0)
     a = dev.run(15)
     b = o.run(15)
     for name, x, y in zip(("cm", "ion", "zcm", "stats"), a, b):

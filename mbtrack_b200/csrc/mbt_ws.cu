@@ -16,11 +16,13 @@
 //                194-253) and the long-range resistive-wall kick of every
 //                source bunch (transformSbunch_longrange :68-192), one
 //                thread per source, added in source order;
-//   ws_train     one block per SOURCE bunch (MBT_WS_SPLIT blocks above 512
-//                ions), MBT_WS_IPT macro-ions per thread: the
-//                ions of that bunch travel down the train (drift between
-//                buckets, pull by each slice of each later bunch,
-//                fbi_weakstrong_train fbi_weakstrong.c:325-426); per later
+//   ws_train     one block per SOURCE bunch (MBT_WS_SPLIT > 1 cuts a
+//                bunch of more than 512 ions over several blocks),
+//                MBT_WS_IPT macro-ions per thread: the ions of that bunch
+//                travel down the train (drift between buckets, pull by each
+//                slice of each later bunch, whose field grid the block
+//                stages in shared memory first; fbi_weakstrong_train
+//                fbi_weakstrong.c:325-426); per later
 //                bunch and slice the block writes its share of the kick
 //                sum  sum_ions Nri E  to a triangular buffer, in a fixed
 //                reduction order (warp shuffles, then warps in order), so
@@ -36,7 +38,8 @@
 // length is the first bunch's chain of (nbunch - 1) x slices pulls.
 //
 // The file is compiled with -fmad=false: every product and sum rounds as
-// the reference's x86-64 build does (no contraction), so the arithmetic
+// the reference's x86-64 build does (no contraction; the divisions by the
+// grid step go through div_known, exact by construction), so the arithmetic
 // differs from the reference only where the device's sin, exp and w(z)
 // differ from glibc's in the last bits, and in the summation order of the
 // ion kick and ion centroid sums.  Constants the reference computes with

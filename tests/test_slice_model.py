@@ -257,3 +257,25 @@ def test_oracle_matches_golden_uneven_fill(tmp_path, libmbt):
     for name, got in zip(("cm", "ion", "zcm", "stats"), out):
         assert _same(got, g[name]), name
     assert _same(o.slices_state(), g["slices"])
+
+
+def test_writer_own_ampinv(tmp_path, libmbt):
+    """With MBT_WRITER_OWN_AMPINV every per-monitor ampinv file lists each
+    bunch's own invariants (the reference's history indexing otherwise
+    shows other bunches' entries after the first monitor)."""
+    g = _golden("train")
+    w, bucket, ib = _product(tmp_path, "train", NrevTot=30, NrevMon=10)
+    o = binding.OracleSlices(w, bucket, ib, g["npop"], g["nofe"])
+    o.set_slices(g["slices0"])
+    cm, ion, zcm, st = o.run(30)
+    out = tmp_path / "own"
+    out.mkdir()
+    wr = api.SliceWriter(str(out), w, bucket, own_ampinv=True)
+    wr.turns(ion, zcm, st)
+    wr.close()
+    for m, turn in enumerate((1, 11, 21)):
+        rows = [l.split() for l in (out / ("ampinv_VER_%d.dat" % turn)).read_text().splitlines()[2:]]
+        assert [int(r[0]) for r in rows] == list(bucket)
+        got = np.array([[float(r[1]), float(r[2])] for r in rows])
+        want = np.stack([st[m, :, 17], st[m, :, 14]], axis=1)
+        assert np.allclose(got, want, rtol=1e-7, atol=0)

@@ -545,6 +545,30 @@ int mbt_tune_spectra_dev(const double *x_dev, long ld, int nseries, int nturn, i
 int mbt_tune_peaks(const double *spec, long nrev, double *value, double *ampli, int *pcase,
                    int max_peaks);
 
+/* ---- checkpoint / resume ------------------------------------------- */
+
+/* Write the device state that carries one turn into the next to path:
+ * coordinates, the histograms and kick tables of the next pass, the pending
+ * resistive-wall kick, long-range phasors, the resistive-wall dipole
+ * history, the RF-feedback history, the bunch currents of a scan and the
+ * ring state with the turn count (the Philox noise is keyed by the turn,
+ * so a resumed run draws the same deviates).  Between mbt_run_* calls.  A
+ * 64-bit FNV-1a checksum closes the file; it is written beside path and
+ * renamed, so a reader never sees half a file. */
+int mbt_checkpoint_save(mbt_ctx *ctx, const char *path);
+
+/* Restore a checkpoint into a prepared context created with the same fill,
+ * parameters, noise mode and seed, the same watched bunches and beam-ion
+ * stage: the next turn continues the saved run exactly.  The file is
+ * checked whole first (checksum, record sizes, configuration key); a bad
+ * or foreign file returns MBT_ERR_IO / MBT_ERR_STATE and leaves the context
+ * untouched. */
+int mbt_checkpoint_load(mbt_ctx *ctx, const char *path);
+
+/* Check a checkpoint file on the host, without a device: structure and
+ * checksum; *turn and *nbunch (either may be NULL) of the saved run. */
+int mbt_checkpoint_check(const char *path, long *turn, int *nbunch);
+
 /* ---- output files (C host; the reference's text formats) ------------- */
 
 /* A writer produces, in work_path, the files the reference's manager and

@@ -93,6 +93,9 @@ SIGNATURES = {
     "mbt_wofz_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mbt_be_field_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, _vp, _vp, _vp]),
+    "mbt_checkpoint_save": (ctypes.c_int, [_vp, ctypes.c_char_p]),
+    "mbt_checkpoint_load": (ctypes.c_int, [_vp, ctypes.c_char_p]),
+    "mbt_checkpoint_check": (ctypes.c_int, [ctypes.c_char_p, _P(ctypes.c_long), _P(ctypes.c_int)]),
     # include/mbt_ws.h: the slice model with fast beam-ion interaction
     "mbt_ws_params_size": (ctypes.c_size_t, []),
     "mbt_ws_config_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _P(MbtWsParams), _vp, _vp, _vp]),
@@ -311,6 +314,14 @@ class Tracker:
         n = np.full(cfg.nbunch, cfg.params.np_model if np_per_bunch is None else np_per_bunch)
         return cls(cfg.params, cfg.bucket, n, cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh,
                    noise=noise, seed=seed)
+
+    def checkpoint_save(self, path):
+        """mbt_checkpoint_save: the state that carries into the next turn."""
+        _check(lib().mbt_checkpoint_save(self.h, path.encode()), self.h)
+
+    def checkpoint_load(self, path):
+        """mbt_checkpoint_load into this prepared context."""
+        _check(lib().mbt_checkpoint_load(self.h, path.encode()), self.h)
 
     def close(self):
         if getattr(self, "h", None):
@@ -743,3 +754,14 @@ class SliceWriter:
         if getattr(self, "h", None):
             h, self.h = self.h, None
             self._chk(lib().mbt_ws_writer_close(h))
+
+
+def checkpoint_check(path):
+    """mbt_checkpoint_check: (turn, nbunch) of a checkpoint file, checked on
+    the host (structure and checksum); raises MbtError for a bad file."""
+    t = ctypes.c_long()
+    n = ctypes.c_int()
+    rc = lib().mbt_checkpoint_check(path.encode(), ctypes.byref(t), ctypes.byref(n))
+    if rc != 0:
+        _check(rc, None)
+    return t.value, n.value

@@ -66,6 +66,7 @@ struct mbt_ctx {
   cudaGraphExec_t graph = nullptr;
   int graph_turns = 0;
   std::vector<void *> allocs;
+  std::vector<size_t> alloc_bytes;  // size of each entry of allocs
   float *dev = nullptr;
   size_t dev_cap = 0;
   double *vbuf = nullptr;
@@ -115,6 +116,7 @@ int dalloc(mbt_ctx *c, T **ptr, size_t n) {
   if (e != cudaSuccess) return fail(c, MBT_ERR_NOMEM, "cudaMalloc(%zu): %s", n * sizeof(T), cudaGetErrorString(e));
   cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(T));
   c->allocs.push_back(p);
+  c->alloc_bytes.push_back(std::max<size_t>(n, 1) * sizeof(T));
   *ptr = static_cast<T *>(p);
   return 0;
 }
@@ -1177,5 +1179,243 @@ int mbt_geometry(mbt_ctx *c, int *npad, int *tile, int *ntile) {
 }
 
 // ---- per-step device entry points
+
+}  // extern "C"
+
+// ---- checkpoint / resume
+
+namespace {
+
+constexpr char kCkptMagic[8] = {'M', 'B', 'T', 'C', 'K', 'P', 'T', '1'};
+constexpr uint32_t kCkptVersion = 1;
+
+uint64_t fnv1a(uint64_t h, const void *p, size_t n) {
+  const unsigned char *b = static_cast<const unsigned char *>(p);
+  for (size_t i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+// What must match between the context that wrote a checkpoint and the one
+// that reads it: geometry, fill, noise key and which optional stages exist.
+struct CkptKey {
+  int32_t nbunch, npad, ntile, ncell, nlr, nharm, Nmlt, rw_long, rffb_len, noise, stats_cap, nwatch, bi_on;
+  int32_t pad0;
+  uint64_t seed;
+  uint64_t fill_hash;   // buckets, macroparticle counts, tiles
+};
+
+CkptKey ckpt_key(const mbt_ctx *c) {
+  CkptKey k{};
+  k.nbunch = c->nbunch; k.npad = c->npad; k.ntile = c->ntile; k.ncell = c->nc; k.nlr = c->nlr;
+  k.nharm = c->p.nharm; k.Nmlt = c->p.Nmlt; k.rw_long = c->p.rw_long; k.rffb_len = c->a.rffb_len;
+  k.noise = c->noise; k.stats_cap = c->a.stats_cap; k.nwatch = (int)c->watch.size(); k.bi_on = c->bi_on;
+  k.seed = c->seed;
+  uint64_t h = 1469598103934665603ull;
+  h = fnv1a(h, c->bucket.data(), c->bucket.size() * sizeof(int));
+  h = fnv1a(h, c->np.data(), c->np.size() * sizeof(int));
+  for (const Tile &t : c->tiles) {
+    const int32_t v[3] = {t.bunch, t.start, t.count};
+    h = fnv1a(h, v, sizeof v);
+  }
+  k.fill_hash = h;
+  return k;
+}
+
+// The device buffers that carry state from one turn to the next (ids are
+// part of the file format), with their allocated sizes.
+struct CkptBuf {
+  uint32_t id;
+  void *ptr;
+  size_t bytes;
+};
+
+std::vector<CkptBuf> ckpt_buffers(const mbt_ctx *c) {
+  const Args &a = c->a;
+  const void *list[] = {a.coord, a.bunch_ib, a.bunch_factg, a.ibunch, a.rw_ib, a.part, a.shift, a.hist, a.cellrange,
+                        a.kick, a.rw_part, a.lr_u, a.lr_b, a.lr_vs, a.dipole, a.rw_e, a.rffb_hist, a.rs, a.pot,
+                        a.bi_mom, a.stats, a.ampinv, c->stats_init};
+  std::vector<CkptBuf> out;
+  for (uint32_t id = 0; id < sizeof list / sizeof list[0]; ++id) {
+    const void *p = list[id];
+    if (!p) continue;
+    bool dup = false;
+    for (const CkptBuf &b : out) dup = dup || b.ptr == p;
+    if (dup) continue;   // rw_ib is ibunch unless a current scan runs with the wall
+    for (size_t i = 0; i < c->allocs.size(); ++i)
+      if (c->allocs[i] == p) out.push_back({id, const_cast<void *>(p), c->alloc_bytes[i]});
+  }
+  return out;
+}
+
+struct CkptHeader {
+  char magic[8];
+  uint32_t version, nbuf;
+  CkptKey key;
+};
+
+// Reads and checks a whole checkpoint file: magic, version, sizes, checksum.
+int ckpt_read(const char *path, std::vector<char> &data, CkptHeader &h, char *err) {
+  FILE *f = fopen(path, "rb");
+  if (!f) { snprintf(err, 512, "checkpoint %s: cannot open", path); return MBT_ERR_IO; }
+  fseek(f, 0, SEEK_END);
+  const long n = ftell(f);
+  fseek(f, 0, SEEK_SET);
+  if (n < (long)(sizeof(CkptHeader) + sizeof(uint64_t))) {
+    fclose(f);
+    snprintf(err, 512, "checkpoint %s: truncated (%ld bytes)", path, n);
+    return MBT_ERR_IO;
+  }
+  data.resize((size_t)n);
+  const size_t got = fread(data.data(), 1, (size_t)n, f);
+  fclose(f);
+  if (got != (size_t)n) { snprintf(err, 512, "checkpoint %s: read error", path); return MBT_ERR_IO; }
+  memcpy(&h, data.data(), sizeof h);
+  if (memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != kCkptVersion) {
+    snprintf(err, 512, "checkpoint %s: not an mbt checkpoint of version %u", path, kCkptVersion);
+    return MBT_ERR_IO;
+  }
+  uint64_t sum;
+  memcpy(&sum, data.data() + n - sizeof sum, sizeof sum);
+  if (fnv1a(1469598103934665603ull, data.data(), (size_t)n - sizeof sum) != sum) {
+    snprintf(err, 512, "checkpoint %s: checksum mismatch (truncated or corrupted)", path);
+    return MBT_ERR_IO;
+  }
+  // walk the records: each one must lie inside the file
+  size_t off = sizeof h;
+  for (uint32_t i = 0; i < h.nbuf; ++i) {
+    uint32_t id;
+    uint64_t bytes;
+    if (off + sizeof id + sizeof bytes > (size_t)n - sizeof sum) {
+      snprintf(err, 512, "checkpoint %s: record %u runs past the end", path, i);
+      return MBT_ERR_IO;
+    }
+    memcpy(&id, data.data() + off, sizeof id);
+    memcpy(&bytes, data.data() + off + sizeof id, sizeof bytes);
+    off += sizeof id + sizeof bytes;
+    if (bytes > (size_t)n - sizeof sum - off) {
+      snprintf(err, 512, "checkpoint %s: record %u runs past the end", path, i);
+      return MBT_ERR_IO;
+    }
+    off += bytes;
+  }
+  if (off != (size_t)n - sizeof sum) {
+    snprintf(err, 512, "checkpoint %s: trailing bytes", path);
+    return MBT_ERR_IO;
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mbt_checkpoint_save(mbt_ctx *c, const char *path) {
+  if (!c || !path) return MBT_ERR_INVALID;
+  if (!c->prepared) return fail(c, MBT_ERR_STATE, "mbt_checkpoint_save: mbt_prepare must come first");
+  CK(cudaStreamSynchronize(c->stream));
+  const std::vector<CkptBuf> bufs = ckpt_buffers(c);
+  CkptHeader h{};
+  memcpy(h.magic, kCkptMagic, 8);
+  h.version = kCkptVersion;
+  h.nbuf = (uint32_t)bufs.size();
+  h.key = ckpt_key(c);
+  size_t total = sizeof h;
+  for (const CkptBuf &b : bufs) total += sizeof(uint32_t) + sizeof(uint64_t) + b.bytes;
+  std::vector<char> data(total + sizeof(uint64_t));
+  memcpy(data.data(), &h, sizeof h);
+  size_t off = sizeof h;
+  for (const CkptBuf &b : bufs) {
+    const uint64_t bytes = b.bytes;
+    memcpy(data.data() + off, &b.id, sizeof b.id);
+    memcpy(data.data() + off + sizeof b.id, &bytes, sizeof bytes);
+    off += sizeof b.id + sizeof bytes;
+    CK(cudaMemcpy(data.data() + off, b.ptr, b.bytes, cudaMemcpyDeviceToHost));
+    off += b.bytes;
+  }
+  const uint64_t sum = fnv1a(1469598103934665603ull, data.data(), total);
+  memcpy(data.data() + total, &sum, sizeof sum);
+  // write beside the target, then rename: a reader never sees half a file
+  std::string tmp = std::string(path) + ".tmp";
+  FILE *f = fopen(tmp.c_str(), "wb");
+  if (!f) return fail(c, MBT_ERR_IO, "mbt_checkpoint_save: cannot create %s", tmp.c_str());
+  const bool ok = fwrite(data.data(), 1, data.size(), f) == data.size();
+  if (fclose(f) != 0 || !ok) {
+    remove(tmp.c_str());
+    return fail(c, MBT_ERR_IO, "mbt_checkpoint_save: write error on %s", tmp.c_str());
+  }
+  if (rename(tmp.c_str(), path) != 0) {
+    remove(tmp.c_str());
+    return fail(c, MBT_ERR_IO, "mbt_checkpoint_save: cannot rename %s", tmp.c_str());
+  }
+  return 0;
+}
+
+int mbt_checkpoint_load(mbt_ctx *c, const char *path) {
+  if (!c || !path) return MBT_ERR_INVALID;
+  if (!c->prepared) return fail(c, MBT_ERR_STATE, "mbt_checkpoint_load: mbt_prepare must come first");
+  std::vector<char> data;
+  CkptHeader h{};
+  int r = ckpt_read(path, data, h, c->err);
+  if (r) return r;
+  const CkptKey k = ckpt_key(c);
+  if (memcmp(&k, &h.key, sizeof k) != 0)
+    return fail(c, MBT_ERR_STATE, "mbt_checkpoint_load: %s was written by a context of another configuration "
+                "(fill, geometry, noise key, watched bunches or beam-ion stage differ)", path);
+  const std::vector<CkptBuf> bufs = ckpt_buffers(c);
+  if (bufs.size() != h.nbuf) return fail(c, MBT_ERR_STATE, "mbt_checkpoint_load: %s holds %u buffers, this context %zu",
+                                         path, h.nbuf, bufs.size());
+  // check every record against this context before the first device write
+  size_t off = sizeof h;
+  std::vector<size_t> at(bufs.size());
+  for (size_t i = 0; i < bufs.size(); ++i) {
+    uint32_t id;
+    uint64_t bytes;
+    memcpy(&id, data.data() + off, sizeof id);
+    memcpy(&bytes, data.data() + off + sizeof id, sizeof bytes);
+    off += sizeof id + sizeof bytes;
+    if (id != bufs[i].id || bytes != bufs[i].bytes)
+      return fail(c, MBT_ERR_STATE, "mbt_checkpoint_load: %s record %zu (buffer %u, %llu bytes) does not match "
+                  "this context (buffer %u, %zu bytes)", path, i, id, (unsigned long long)bytes, bufs[i].id,
+                  bufs[i].bytes);
+    at[i] = off;
+    off += bytes;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  for (size_t i = 0; i < bufs.size(); ++i)
+    CK(cudaMemcpy(bufs[i].ptr, data.data() + at[i], bufs[i].bytes, cudaMemcpyHostToDevice));
+  if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; c->graph_turns = 0; }
+  return 0;
+}
+
+int mbt_checkpoint_check(const char *path, long *turn, int *nbunch) {
+  std::vector<char> data;
+  CkptHeader h{};
+  char err[512];
+  if (!path) return MBT_ERR_INVALID;
+  int r = ckpt_read(path, data, h, err);
+  if (r) {
+    snprintf(g_create_error, sizeof g_create_error, "%s", err);
+    return r;
+  }
+  if (nbunch) *nbunch = h.key.nbunch;
+  if (turn) {
+    // the ring state record (id 17) holds the turn count first
+    size_t off = sizeof h;
+    *turn = -1;
+    for (uint32_t i = 0; i < h.nbuf; ++i) {
+      uint32_t id;
+      uint64_t bytes;
+      memcpy(&id, data.data() + off, sizeof id);
+      memcpy(&bytes, data.data() + off + sizeof id, sizeof bytes);
+      off += sizeof id + sizeof bytes;
+      if (id == 17 && bytes >= sizeof(long)) memcpy(turn, data.data() + off, sizeof(long));
+      off += bytes;
+    }
+  }
+  return 0;
+}
 
 }  // extern "C"

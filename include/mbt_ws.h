@@ -164,6 +164,13 @@ int mbt_ws_profile(mbt_ws *ws, long nturns, double *ms4);
  * last turn, slice icell, at n points (x[i], y[i]) [m]: exey[n][2]. */
 int mbt_ws_interp(mbt_ws *ws, int ib, int icell, const double *x, const double *y, int n, double *exey);
 
+/* Checkpoint of the slice state, the centroid histories and the turn
+ * count (all that carries into the next turn), with a 64-bit FNV-1a
+ * checksum; written beside path and renamed.  Loading checks the whole
+ * file against this context before the first device write. */
+int mbt_ws_checkpoint_save(mbt_ws *ws, const char *path);
+int mbt_ws_checkpoint_load(mbt_ws *ws, const char *path);
+
 /* Turns done. */
 long mbt_ws_turn(const mbt_ws *ws);
 

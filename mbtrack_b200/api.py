@@ -107,6 +107,8 @@ SIGNATURES = {
     "mbt_ws_run_turns": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp, _vp, _vp]),
     "mbt_ws_bunch_fields": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "mbt_ws_turn": (ctypes.c_long, [_vp]),
+    "mbt_ws_checkpoint_save": (ctypes.c_int, [_vp, ctypes.c_char_p]),
+    "mbt_ws_checkpoint_load": (ctypes.c_int, [_vp, ctypes.c_char_p]),
     "mbt_ws_last_ms": (ctypes.c_double, [_vp]),
     "mbt_ws_profile": (ctypes.c_int, [_vp, ctypes.c_long, _vp]),
     "mbt_ws_interp": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp]),
@@ -684,6 +686,12 @@ class SliceModel:
         st = np.zeros((max(nmon, 1), self.nb, 18))
         self._chk(lib().mbt_ws_run_turns(self.h, nturns, _ptr(cm), _ptr(ion), _ptr(zcm), _ptr(st)))
         return cm, ion, zcm, st[:nmon]
+
+    def checkpoint_save(self, path):
+        self._chk(lib().mbt_ws_checkpoint_save(self.h, path.encode()))
+
+    def checkpoint_load(self, path):
+        self._chk(lib().mbt_ws_checkpoint_load(self.h, path.encode()))
 
     def last_ms(self):
         """Device time [ms] of the last run."""

@@ -52,6 +52,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "mbt.h"
@@ -956,4 +957,72 @@ extern "C" void mbt_ws_destroy(mbt_ws *ws) {
   if (ws->stream) cudaStreamSynchronize(ws->stream);
   ws_free(ws);
   free(ws);
+}
+
+// ---- checkpoint / resume: the slices, the centroid histories and the
+// turn count carry one turn into the next (field grids, ions and kick
+// shares are rebuilt every turn).  Layout: "MBTWSCK1", turn, bunches,
+// slices, history length, the two arrays, 64-bit FNV-1a of all before it.
+
+static uint64_t ws_fnv1a(uint64_t h, const void *p, size_t n) {
+  const unsigned char *b = static_cast<const unsigned char *>(p);
+  for (size_t i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+extern "C" int mbt_ws_checkpoint_save(mbt_ws *ws, const char *path) {
+  if (!ws || !path) return ws_fail(ws, MBT_ERR_INVALID, "mbt_ws_checkpoint_save: null argument");
+  const WsConst &C = ws->C;
+  const size_t ns = (size_t)C.nb * 6 * C.S, nh = (size_t)C.nb * 4 * C.nmt;
+  const int64_t head[5] = {(int64_t)ws->turn, C.nb, C.S, C.nmt, C.nion};
+  std::vector<char> data(8 + sizeof head + (ns + nh) * sizeof(double) + sizeof(uint64_t));
+  memcpy(data.data(), "MBTWSCK1", 8);
+  memcpy(data.data() + 8, head, sizeof head);
+  double *arr = reinterpret_cast<double *>(data.data() + 8 + sizeof head);
+  WS_CUDA(ws, cudaStreamSynchronize(ws->stream));
+  WS_CUDA(ws, cudaMemcpy(arr, ws->d_s, ns * sizeof(double), cudaMemcpyDeviceToHost));
+  WS_CUDA(ws, cudaMemcpy(arr + ns, ws->d_hist, nh * sizeof(double), cudaMemcpyDeviceToHost));
+  const size_t body = data.size() - sizeof(uint64_t);
+  const uint64_t sum = ws_fnv1a(1469598103934665603ull, data.data(), body);
+  memcpy(data.data() + body, &sum, sizeof sum);
+  const std::string tmp = std::string(path) + ".tmp";
+  FILE *f = fopen(tmp.c_str(), "wb");
+  if (!f) return ws_fail(ws, MBT_ERR_IO, "mbt_ws_checkpoint_save: cannot create %s", tmp.c_str());
+  const bool ok = fwrite(data.data(), 1, data.size(), f) == data.size();
+  if (fclose(f) != 0 || !ok || rename(tmp.c_str(), path) != 0) {
+    remove(tmp.c_str());
+    return ws_fail(ws, MBT_ERR_IO, "mbt_ws_checkpoint_save: cannot write %s", path);
+  }
+  return 0;
+}
+
+extern "C" int mbt_ws_checkpoint_load(mbt_ws *ws, const char *path) {
+  if (!ws || !path) return ws_fail(ws, MBT_ERR_INVALID, "mbt_ws_checkpoint_load: null argument");
+  const WsConst &C = ws->C;
+  const size_t ns = (size_t)C.nb * 6 * C.S, nh = (size_t)C.nb * 4 * C.nmt;
+  int64_t head[5];
+  const size_t want = 8 + sizeof head + (ns + nh) * sizeof(double) + sizeof(uint64_t);
+  FILE *f = fopen(path, "rb");
+  if (!f) return ws_fail(ws, MBT_ERR_IO, "mbt_ws_checkpoint_load: cannot open %s", path);
+  std::vector<char> data(want + 1);
+  const size_t got = fread(data.data(), 1, data.size(), f);
+  fclose(f);
+  if (got != want || memcmp(data.data(), "MBTWSCK1", 8) != 0)
+    return ws_fail(ws, MBT_ERR_IO, "mbt_ws_checkpoint_load: %s is not a slice-model checkpoint of this size", path);
+  uint64_t sum;
+  memcpy(&sum, data.data() + want - sizeof sum, sizeof sum);
+  if (ws_fnv1a(1469598103934665603ull, data.data(), want - sizeof sum) != sum)
+    return ws_fail(ws, MBT_ERR_IO, "mbt_ws_checkpoint_load: %s: checksum mismatch", path);
+  memcpy(head, data.data() + 8, sizeof head);
+  if (head[1] != C.nb || head[2] != C.S || head[3] != C.nmt || head[4] != C.nion || head[0] < 0)
+    return ws_fail(ws, MBT_ERR_STATE, "mbt_ws_checkpoint_load: %s was written by another configuration", path);
+  const double *arr = reinterpret_cast<const double *>(data.data() + 8 + sizeof head);
+  WS_CUDA(ws, cudaStreamSynchronize(ws->stream));
+  WS_CUDA(ws, cudaMemcpy(ws->d_s, arr, ns * sizeof(double), cudaMemcpyHostToDevice));
+  WS_CUDA(ws, cudaMemcpy(ws->d_hist, arr + ns, nh * sizeof(double), cudaMemcpyHostToDevice));
+  ws->turn = (long)head[0];
+  return 0;
 }

@@ -236,3 +236,27 @@ def test_device_matches_reference_uneven_fill(tmp_path, cuda_device):
     for name, x in zip(("cm", "ion", "zcm", "stats"), out):
         _close(x, g[name], 1e-11, name)
     _close(dev.slices(), g["slices"], 1e-11, "slices")
+
+
+def test_checkpoint_resume(tmp_path, cuda_device):
+    """A slice-model run saved after 12 turns and resumed in a fresh
+    context continues bit for bit; a truncated file is refused."""
+    w, bucket, ib, npop, nofe, g = _setup(tmp_path, "train")
+    ck = str(tmp_path / "ws.ckpt")
+    a = api.SliceModel(w, bucket, ib, npop, nofe)
+    a.load_slices(g["slices0"])
+    a.run(12)
+    a.checkpoint_save(ck)
+    ra = a.run(8)
+    b = api.SliceModel(w, bucket, ib, npop, nofe)
+    b.checkpoint_load(ck)
+    assert b.turn == 12
+    rb = b.run(8)
+    for x, y in zip(ra, rb):
+        assert np.array_equal(x, y, equal_nan=True)
+    data = open(ck, "rb").read()
+    bad = str(tmp_path / "bad.ckpt")
+    open(bad, "wb").write(data[:-9])
+    with pytest.raises(api.MbtError):
+        b.checkpoint_load(bad)
+    assert b.turn == 20

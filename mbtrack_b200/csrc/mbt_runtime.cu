@@ -301,7 +301,10 @@ int sync_and_check(mbt_ctx *c) {
   CK(cudaGetLastError());
   RingState rs;
   CK(cudaMemcpy(&rs, c->a.rs, sizeof(rs), cudaMemcpyDeviceToHost));
-  if (rs.error) return fail(c, MBT_ERR_STATE, "device error word %d (deviates exhausted?)", rs.error);
+  if (rs.error & 2)
+    return fail(c, MBT_ERR_TIMEOUT, "device error word %d: a bounded pipeline wait of the particle pass gave up",
+                rs.error);
+  if (rs.error) return fail(c, MBT_ERR_STATE, "device error word %d: injected deviates exhausted", rs.error);
   return 0;
 }
 

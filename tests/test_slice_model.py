@@ -303,3 +303,21 @@ def test_slicing_edge_particles(tmp_path, libmbt):
     # the NaN and the far-ahead particle sit in slice 0, the far-behind one
     # in the overflow cell that npop does not count
     assert a[0][0] >= 2 and a[0].sum() < n
+
+
+@pytest.mark.reference
+def test_oracle_matches_reference_long_run(tmp_path, libmbt):
+    """200 turns of the 10-bunch train with the wall and the ions on, the
+    oracle beside the reference's own functions: bit for bit throughout."""
+    if not binding.reference_available() and not os.path.exists(binding.REF_SO):
+        pytest.skip("reference harness unavailable")
+    path = slice_conf(tmp_path, "train", NrevTot=300, NrevMon=50)
+    r = binding.ReferenceSlices(path)
+    w, bucket, ib = _product(tmp_path, "train", NrevTot=300, NrevMon=50)
+    o = binding.OracleSlices(w, bucket, ib, r.npop, r.nofe)
+    o.set_slices(r.slices_state())
+    a = r.run(200, w.base.nrev_mon)
+    b = o.run(200)
+    for name, x, y in zip(("cm", "ion", "zcm", "stats"), a, b):
+        assert _same(x, y), name
+    assert _same(r.slices_state(), o.slices_state())

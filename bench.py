@@ -155,34 +155,30 @@ class ClockSampler:
 
 def _cpu_worker(args):
     """One host process: bunches [lo, hi) of the ring for `turns` turns;
-    returns the wall time of each turn."""
+    returns the wall time of each turn.  Loads the reference's library
+    (oracle/_ref) or the C restatement (oracle/), never libmbt."""
     kind, conf, lo, hi, turns = args
     sys.path.insert(0, ROOT)
+    import numpy as np
+    from oracle.binding import Oracle, Reference, beam_ion_section
     if kind == "beam_ion":
-        import numpy as np
-        from mbtrack_b200 import api as _api   # configuration parser only (C host)
-        from oracle.binding import Oracle
-        cfg = _api.Config(conf)
-        bi = cfg.beam_ion()
+        # no reference code exists for this stage: the C restatement, its
+        # ring and bunches as the reference's own parser reads the file
+        p, bucket, npb, ib, Gl, Gv, Gh = Reference(conf, private=False).oracle_inputs()
+        bi = beam_ion_section(conf)
         bi.ions_per_passage = max(1, bi.ions_per_passage // BEAM_ION_CPU_SCALE)
-        npb = max(2, cfg.params.np_model // BEAM_ION_CPU_SCALE)
-        O = Oracle(cfg.params, cfg.bucket, np.full(cfg.nbunch, npb), cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh)
+        O = Oracle(p, bucket, np.maximum(2, npb // BEAM_ION_CPU_SCALE), ib, Gl, Gv, Gh)
         O.generate_beam()
         O.prepare()
         O.enable_beam_ion(bi)
         step = lambda: O.lib.orc_run(O.h, 1, None, None, None, 0)   # noqa: E731
     elif kind == "reference":
-        from oracle.binding import Reference
-        R = Reference(conf, bunch_range=(lo, hi))
+        R = Reference(conf, bunch_range=(lo, hi), private=False)
         R.prepare()
         step = lambda: R.lib.refh_run(1, None, None, 0)   # noqa: E731
     else:
-        import numpy as np
-        from mbtrack_b200 import api as _api   # configuration parser only (C host)
-        from oracle.binding import Oracle
-        cfg = _api.Config(conf)
-        O = Oracle(cfg.params, cfg.bucket, np.full(cfg.nbunch, cfg.params.np_model),
-                   cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh)
+        p, bucket, npb, ib, Gl, Gv, Gh = Reference(conf, private=False).oracle_inputs()
+        O = Oracle(p, bucket, npb, ib, Gl, Gv, Gh)
         O.set_range(lo, hi)
         O.generate_beam()
         O.prepare()
@@ -195,6 +191,15 @@ def _cpu_worker(args):
     return times
 
 
+def _ring_probe(conf):
+    """(bunches, macroparticles per bunch) as the reference's own parser
+    reads the file (a spawned process; libmbt is not loaded)."""
+    sys.path.insert(0, ROOT)
+    from oracle.binding import Reference
+    R = Reference(conf, private=False)
+    return int(R.nb), [int(x) for x in R.np]
+
+
 def cpu_kind():
     from oracle import binding
     if binding.build_reference() is not None:
@@ -205,33 +210,33 @@ def cpu_kind():
 
 def cpu_run(workload, turns, tmpdir, cores=None):
     """Time `turns` turns of the whole ring on the host cores (bunches split
-    over one process per core).  Returns (per-turn seconds list, info)."""
-    from mbtrack_b200 import api
+    over one process per core).  Returns (per-turn seconds list, info).
+    Every process is spawned and loads only the reference's library or the
+    C restatement."""
     conf = conf_path(workload, tmpdir)
-    cfg = api.Config(conf)
-    nb = cfg.nbunch
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        nb, npb = pool.apply(_ring_probe, (conf,))
+    particles = int(sum(npb))
     if workload.startswith("beam_ion"):
         # no reference code for this stage: the C restatement (oracle) on one
         # core, 1/BEAM_ION_CPU_SCALE of the electrons and ions, the time per
         # turn scaled back up (the work is linear in both counts)
-        ctx = mp.get_context("spawn")
         with ctx.Pool(1) as pool:
             res = pool.map(_cpu_worker, [("beam_ion", conf, 0, nb, turns)])
         per_turn = [x * BEAM_ION_CPU_SCALE for x in res[0]]
-        return per_turn, {"kind": "port", "cores": 1, "bunches": nb, "particles": int(nb * cfg.params.np_model),
-                          "scaled": BEAM_ION_CPU_SCALE}
+        return per_turn, {"kind": "port", "cores": 1, "bunches": nb, "particles": particles,
+                          "np_per_bunch": npb[0], "scaled": BEAM_ION_CPU_SCALE}
     if cores is None:
         cores = len(os.sched_getaffinity(0))
     procs = max(1, min(cores, nb))
     edges = [round(i * nb / procs) for i in range(procs + 1)]
     kind = cpu_kind()
     jobs = [(kind, conf, edges[i], edges[i + 1], turns) for i in range(procs)]
-    ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
         res = pool.map(_cpu_worker, jobs)
     per_turn = [max(r[t] for r in res) for t in range(turns)]
-    info = {"kind": kind, "cores": procs, "bunches": nb,
-            "particles": int(nb * cfg.params.np_model)}
+    info = {"kind": kind, "cores": procs, "bunches": nb, "particles": particles, "np_per_bunch": npb[0]}
     return per_turn, info
 
 
@@ -257,7 +262,8 @@ def run_b200(args):
     tmp = tempfile.mkdtemp()
     conf = conf_path(args.workload, tmp)
     cfg = api.Config(conf)
-    npart = int(cfg.nbunch * cfg.params.np_model)
+    np_model = args.np_per_bunch or cfg.params.np_model
+    npart = int(cfg.nbunch * np_model)
 
     # CPU baseline first (spawned processes; rank 0 at N=1 only)
     cpu = None
@@ -267,7 +273,7 @@ def run_b200(args):
         cpu = {"value": npart / t, "unit": METRIC, "cores": info["cores"], "kind": info["kind"],
                "sample": "%d turns of the whole ring (%d bunches x %d macroparticles) split over %d "
                          "processes, one per core; first turn dropped; time = slowest process"
-                         % (args.cpu_turns, info["bunches"], cfg.params.np_model, info["cores"])}
+                         % (args.cpu_turns, info["bunches"], info["np_per_bunch"], info["cores"])}
         if info.get("scaled"):
             cpu["sample"] = ("%d turns of the C restatement (no reference code exists for this stage) on one "
                              "core with 1/%d of the electrons and of the macro-ions, time scaled by %d; first "
@@ -288,16 +294,20 @@ def run_b200(args):
                           seed=1000 + rank)
         npart = int(npb.sum())
     else:
-        trk = api.Tracker.from_config(cfg, seed=1000 + rank)
+        trk = api.Tracker.from_config(cfg, np_per_bunch=np_model, seed=1000 + rank)
     trk.generate_beam(77 + rank)
     bi_info = None
     if args.workload.startswith("beam_ion"):
         bi = cfg.beam_ion()
         bi.surrogate = 1 if args.workload == "beam_ion_mlp" else 0
+        if args.n_ip:
+            bi.n_ip = args.n_ip
+        if args.ions_per_passage:
+            bi.ions_per_passage = args.ions_per_passage
         trk.enable_beam_ion(bi)
         bi_info = {"n_ip": bi.n_ip, "ions_per_passage": bi.ions_per_passage,
                    "field_evaluations_per_turn": bi.n_ip * (bi.ions_per_passage * cfg.nbunch * (cfg.nbunch - 1) // 2
-                                                            + cfg.params.np_model * (cfg.nbunch - 1))}
+                                                            + np_model * (cfg.nbunch - 1))}
         if bi.surrogate:
             mlp = api.Mlp(seed=31 + rank)
             torch.cuda.synchronize()
@@ -383,7 +393,7 @@ def run_b200(args):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": desc, "bunches": int(cfg.nbunch), "np_per_bunch": int(cfg.params.np_model),
+        "config": {"workload": desc, "bunches": int(cfg.nbunch), "np_per_bunch": int(np_model),
                    "macroparticles": npart, "turns_per_step": 1, "noise": "Philox4x32-10 counter RNG",
                    "l2": "beam of %.0f MB > 126 MB L2, no flush" % (npart * 48 / 1e6),
                    "parallelism": "replicas x%d" % world},
@@ -723,6 +733,11 @@ def main():
     ap.add_argument("--cpu-turns", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--mlp-steps", type=int, default=48000, help="training steps of the learned field")
+    ap.add_argument("--np-per-bunch", type=int, default=0,
+                    help="macroparticles per bunch in place of the workload's (small cases for profiling)")
+    ap.add_argument("--n-ip", type=int, default=0, help="beam-ion workloads: interaction points (small cases)")
+    ap.add_argument("--ions-per-passage", type=int, default=0,
+                    help="beam-ion workloads: macro-ions per bunch passage per point (small cases)")
     ap.add_argument("--growth-turns", type=int, default=0,
                     help="beam_ion_mlp: also compare the instability growth rate of the learned and the "
                          "Faddeeva stage over this many turns on a reduced train; slice_fbii: compare the "

@@ -18,7 +18,9 @@ from mbtrack_b200.abi import MbtParams, MbtWsParams
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmbtref.so")
-REFERENCE_DIR = "/root/reference"
+# the reference tree this library is built from (present in the build
+# container only); MBT_REFERENCE_DIR overrides the default location
+REFERENCE_DIR = os.environ.get("MBT_REFERENCE_DIR", "/root/reference")
 
 _vp = ctypes.c_void_p
 _P = ctypes.POINTER
@@ -62,6 +64,35 @@ def conf_with(src, dst, **overrides):
     with open(dst, "w") as f:
         f.write(text)
     return dst
+
+
+def beam_ion_section(conf):
+    """The [beam_ion] section of a .conf file (an MbtBeamIon), read here
+    for the C restatement with the defaults and units that libmbt's
+    mbt_config_beam_ion documents (pressure in nTorr, cross-section in Mb);
+    None when the file has no such section."""
+    from mbtrack_b200.abi import MbtBeamIon
+    section, vals, seen = None, {}, False
+    for line in open(conf):
+        t = line.split("#", 1)[0].strip()
+        if t.startswith("[") and t.endswith("]"):
+            section = t[1:-1].strip()
+            seen = seen or section == "beam_ion"
+        elif section == "beam_ion" and "=" in t:
+            k, v = t.split("=", 1)
+            vals[k.strip()] = v.strip()
+    if not seen:
+        return None
+    bi = MbtBeamIon()
+    bi.n_ip = int(vals.get("n_ip", 1))
+    bi.ions_per_passage = int(vals.get("ions_per_passage", 1000))
+    bi.gas_A = float(vals.get("gas_A", 28.0))
+    bi.pressure = float(vals.get("pressure_nTorr", 1.0)) * 1e-9
+    bi.sigma_ion = float(vals.get("sigma_ion_Mb", 1.78)) * 1e-22
+    bi.seed = int(vals.get("seed", 1)) & 0xFFFFFFFF
+    bi.surrogate = int(vals.get("surrogate", 0))
+    bi.audit_fraction = float(vals.get("audit_fraction", 0.01))
+    return bi
 
 
 class Oracle:
@@ -248,18 +279,23 @@ class Reference:
 
     _count = 0
 
-    def __init__(self, conf, fix_rw_beff=True, workdir="/tmp", bunch_range=None):
+    def __init__(self, conf, fix_rw_beff=True, workdir="/tmp", bunch_range=None, private=True):
         so = build_reference()
         if so is None:
             raise RuntimeError("reference harness unavailable")
-        # The reference keeps its state in globals and statics (bunch.c's
-        # RNG cache among them): load a private copy of the library per
-        # instance so instances never share them.
-        Reference._count += 1
-        priv = os.path.join(tempfile.gettempdir(), "libmbtref_%d_%d.so" % (os.getpid(), Reference._count))
-        shutil.copyfile(so, priv)
-        self.lib = L = ctypes.CDLL(priv, mode=getattr(os, "RTLD_LOCAL", 0))
-        os.unlink(priv)
+        if private:
+            # The reference keeps its state in globals and statics (bunch.c's
+            # RNG cache among them): load a private copy of the library per
+            # instance so instances never share them.
+            Reference._count += 1
+            priv = os.path.join(tempfile.gettempdir(), "libmbtref_%d_%d.so" % (os.getpid(), Reference._count))
+            shutil.copyfile(so, priv)
+            self.lib = L = ctypes.CDLL(priv, mode=getattr(os, "RTLD_LOCAL", 0))
+            os.unlink(priv)
+        else:
+            # one instance in this process (a worker of the timed CPU
+            # baseline): the built library itself
+            self.lib = L = ctypes.CDLL(so, mode=getattr(os, "RTLD_LOCAL", 0))
         L.refh_init.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
         L.refh_run.restype = ctypes.c_int
         L.refh_run.argtypes = [ctypes.c_long, _vp, _vp, ctypes.c_long]
@@ -306,6 +342,12 @@ class Reference:
         p = MbtParams()
         self.lib.refh_fill_params(ctypes.byref(p))
         return p
+
+    def oracle_inputs(self):
+        """(params, bucket, np, ib, Gl, Gv, Gh) of this file as the reference's
+        own parser and set-up read it: what the C restatement needs."""
+        Gl, Gv, Gh, _ = self.greens(0)
+        return self.params(), self.bucket.copy(), self.np.copy(), self.ib.copy(), Gl, Gv, Gh
 
     def greens(self, ib=0):
         p = self.params()

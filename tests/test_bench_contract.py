@@ -50,3 +50,19 @@ def test_reference_arm_two_ranks():
     assert len(lines) == 1
     _check(lines[0])
     assert lines[0]["n_gpus"] == 2
+
+
+def test_reference_arm_loads_no_product_code():
+    """The reference arm's processes load the reference's own library
+    (oracle/_ref) or the C restatement, never libmbt.so."""
+    code = (
+        "import os, sys, tempfile; sys.path.insert(0, %r)\n"
+        "import bench\n"
+        "conf = bench.conf_path('single', tempfile.mkdtemp())\n"
+        "nb, npb = bench._ring_probe(conf)\n"
+        "t = bench._cpu_worker((bench.cpu_kind(), conf, 0, nb, 1))\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('libmbt.so' in maps, 'libmbtref.so' in maps or 'liboracle.so' in maps, nb, len(t))\n" % ROOT)
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.split()[-4:] == ["False", "True", "1", "1"], r.stdout

@@ -242,6 +242,26 @@ int mbt_destroy(mbt_ctx *ctx);
  * mbt_create when ctx is NULL). */
 int mbt_last_error(const mbt_ctx *ctx, char *buf, size_t len);
 
+/* Failure reporting.  Every kernel that waits (the particle pass's copy
+ * pipeline, the learned field's tensor-core products) bounds its waits; a
+ * wait that gives up sets a bit of the context's sticky device error word
+ * and the kernel returns.  The next mbt_run_turns / mbt_track reads the
+ * word and fails: bits 2 (particle-pass pipeline) and 4 (learned-field
+ * tensor cores) give MBT_ERR_TIMEOUT, bit 1 (injected deviates exhausted)
+ * MBT_ERR_STATE.  No counterpart in the reference (its MPI ranks have no
+ * failure detection).
+ *
+ * mbt_inject_device_error ORs `bits` into that word from the host, for
+ * tests of the reporting path without a device fault. */
+int mbt_inject_device_error(mbt_ctx *ctx, int bits);
+
+/* One bounded wait that nothing ends: a kernel waits `polls` times on an
+ * mbarrier no thread arrives at, with the helper every waiting kernel uses,
+ * and reports giving up.  Returns MBT_ERR_TIMEOUT when the wait gave up as
+ * it must, 0 if it did not (a broken bound).  For tests of the bounded
+ * waits on the GPU; no counterpart in the reference. */
+int mbt_selftest_bounded_wait(long polls, void *stream);
+
 /* Copy one bunch's coordinates in (host soa6, np doubles per coordinate).
  * Allowed before mbt_prepare and between runs. */
 int mbt_load_particles(mbt_ctx *ctx, int ibunch, const double *soa6, int np);
@@ -384,15 +404,20 @@ int mbt_bunch_moments_dev(int np, const double *coord_dev, double sigma_tau,
                           const int track_plane[3], double *stats,
                           double *hist_dev, void *stream);
 
-/* Same result as mbt_bunch_moments_dev, for callers that must not allocate
- * device memory during the call (their memory is owned by a pool or a
- * framework allocator, or they cannot afford a possibly synchronising
- * cudaMalloc per call).  It has no counterpart in the reference.
+/* mbt_bunch_moments_dev for callers that must not allocate device memory
+ * during the call (their memory is owned by a pool or a framework
+ * allocator, or they cannot afford a possibly synchronising cudaMalloc per
+ * call).  It has no counterpart in the reference.  Histogram counts are
+ * identical to mbt_bunch_moments_dev's; sums and statistics agree to
+ * rounding (with large ncell and np the partial sums are split over fewer
+ * blocks).  The call waits for its stream and returns the statistics in
+ * host memory, as mbt_bunch_moments_dev does.
  * Its scratch is a fixed 2 MiB device array inside libmbt, present on every
- * GPU that loads the library until the process exits; the first call on a
- * device looks up that array's address, so make it before any stream
- * capture.  Calls share the array: calls that overlap on the GPU race.
- * ncell is limited to MBT_NOALLOC_MAX_NCELL (larger values return
+ * GPU that loads the library until the process exits; each call looks up
+ * that array's address on the current device, and the first call on a
+ * device also loads libmbt's device code there, so make it before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU
+ * race.  ncell is limited to MBT_NOALLOC_MAX_NCELL (larger values return
  * MBT_ERR_INVALID); np is not limited.  It calls no allocator. */
 #define MBT_NOALLOC_MAX_NCELL 1024
 int mbt_bunch_moments_dev_noalloc(int np, const double *coord_dev,
@@ -479,13 +504,16 @@ int mbt_gauss_field_dev(long n, const double *dx_dev, const double *dy_dev,
 /* A 3 -> 128 -> 128 -> 128 -> 2 GELU network trained on the GPU to stand
  * in for mbt_gauss_field_dev inside a = |dx|/sx < 8, b = |dy|/sy < 8,
  * r = sy/sx in [0.05, 1] (sy > sx by swapping the axes).  The dimensionless
- * field F = sx (gx, gy) is Fx = a Ex (1 + Yx/8), Fy = b Ey (1 + Yy/8):
- * Ex, Ey are 8- and 16-node Gauss-Legendre quadratures of the field
- * integral (within about 10 % of the field), the network maps (a, b, r)
- * to the residuals (Yx, Yy).  The hidden 128 x 128 layers run on the
- * tensor cores (BF16 operands, FP32 accumulation), the first and last
- * layers in FP32.  Parameters: MBT_MLP_NPARAM floats, W1[128][3], b1[128],
- * W2[128][128], b2, W3[128][128], b3, W4[2][128], b4[2]. */
+ * field F = sx (gx, gy) is Fx = a Ex (1 + Yx/S), Fy = b Ey (1 + Yy/S),
+ * S = 4096: (a Ex, b Ey) is a two-panel 8 + 8 node Gauss-Legendre rule of
+ * the field integral in FP32 (within 2e-4 of the field everywhere in the
+ * domain), the network maps (a, b, r) to the scaled residuals (Yx, Yy).
+ * Every layer runs on the tensor cores with BF16 weights and activations
+ * and FP32 accumulation: the inputs and the biases enter as BF16 pairs
+ * (high and low part) through extra columns of the operands, the
+ * activations are GELU (tanh form) in BF16 pair arithmetic.  Parameters
+ * (FP32 masters): MBT_MLP_NPARAM floats, W1[128][3], b1[128], W2[128][128],
+ * b2, W3[128][128], b3, W4[2][128], b4[2]. */
 #define MBT_MLP_NPARAM 33794
 
 /* Network with seeded Glorot-uniform weights, zero biases. */
@@ -502,6 +530,16 @@ int mbt_mlp_forward_dev(mbt_mlp *m, long n, const float *abr_dev,
  * (device arrays), into grad (host, MBT_MLP_NPARAM floats); *loss set. */
 int mbt_mlp_gradient(mbt_mlp *m, int n, const float *abr_dev,
                      const float *target_dev, float *grad, double *loss);
+
+/* The learned field at n points, in place of mbt_gauss_field_dev (same
+ * arguments and units, device arrays): the network inside its domain, the
+ * Faddeeva-based field outside it.  *fallbacks (host, may be NULL)
+ * receives the number of points outside the domain.  No counterpart in the
+ * reference: the field it replaces is fbi_weakstrong.c:154-197 with
+ * physic.c:75-301. */
+int mbt_mlp_field_dev(mbt_mlp *m, long n, const double *dx_dev, const double *dy_dev,
+                      const double *sx_dev, const double *sy_dev, double *gx_dev,
+                      double *gy_dev, long *fallbacks, void *stream);
 
 /* Residual targets (Yx, Yy) of n inputs from the Faddeeva-based field. */
 int mbt_mlp_targets_dev(long n, const float *abr_dev, float *t_dev, void *stream);

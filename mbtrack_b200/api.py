@@ -47,6 +47,8 @@ SIGNATURES = {
     "mbt_track": (ctypes.c_int, [_vp, _vp, ctypes.c_long, _vp]),
     "mbt_profile_turns": (ctypes.c_int, [_vp, ctypes.c_long, _vp]),
     "mbt_get_state": (ctypes.c_int, [_vp, _P(MbtState)]),
+    "mbt_inject_device_error": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "mbt_selftest_bounded_wait": (ctypes.c_int, [ctypes.c_long, _vp]),
     "mbt_get_histograms": (ctypes.c_int, [_vp, ctypes.c_int] + [_vp] * 6),
     "mbt_last_timing": (ctypes.c_int, [_vp, _vp, _vp]),
     "mbt_geometry": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
@@ -88,6 +90,7 @@ SIGNATURES = {
     "mbt_mlp_forward_dev": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp, _vp]),
     "mbt_mlp_gradient": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _P(ctypes.c_double)]),
     "mbt_mlp_targets_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp]),
+    "mbt_mlp_field_dev": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp, _P(ctypes.c_long), _vp]),
     "mbt_mlp_train": (ctypes.c_int, [_vp, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                      ctypes.c_uint64, _vp]),
     "mbt_wofz_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -438,6 +441,10 @@ class Tracker:
         _check(lib().mbt_profile_turns(self.h, nturns, _ptr(out)), self.h)
         return out
 
+    def inject_device_error(self, bits):
+        """mbt_inject_device_error: set bits of the sticky device error word."""
+        _check(lib().mbt_inject_device_error(self.h, bits), self.h)
+
     def state(self):
         st = MbtState()
         _check(lib().mbt_get_state(self.h, ctypes.byref(st)), self.h)
@@ -564,6 +571,14 @@ class Mlp:
         loss = ctypes.c_double()
         _gchk(lib().mbt_mlp_gradient(self.h, n, abr_ptr, tgt_ptr, _ptr(g), ctypes.byref(loss)))
         return g, loss.value
+
+    def field_dev(self, n, dx_ptr, dy_ptr, sx_ptr, sy_ptr, gx_ptr, gy_ptr):
+        """mbt_mlp_field_dev: the learned field at n points; returns the
+        number of points outside the network's domain."""
+        fb = ctypes.c_long()
+        _gchk(lib().mbt_mlp_field_dev(self.h, n, dx_ptr, dy_ptr, sx_ptr, sy_ptr, gx_ptr, gy_ptr, ctypes.byref(fb),
+                                      None))
+        return fb.value
 
     def train(self, nsamples, batch, steps, lr, seed):
         hist = np.zeros(steps, dtype=np.float32)

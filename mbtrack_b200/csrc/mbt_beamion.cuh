@@ -53,6 +53,7 @@ struct BiArgs {
   const int *bunch_kb;             // nbunch buckets
   const double *ib;                // nbunch currents [A]
   const long *turn;                // device turn counter
+  int *error;                      // the ring's sticky error word: bit 4 = a tensor-core wait gave up
   // learned field (surrogate runs)
   uint32_t audit_threshold;        // audit an evaluation when its hash is below this (2^32 x fraction)
   unsigned long long *audit;       // [0] audited evaluations, [1] max relative error (bits), [2] fallbacks,
@@ -250,11 +251,11 @@ __device__ __forceinline__ bool bi_field_mlp(const BiArgs &bi, MlpGroup &G, int 
     gauss_field_ool(dx, dy, sx, sy, &gx, &gy);
     ++fallbacks;
   } else if (active && h < bi.audit_threshold) {
+    // relative error of the field vector: |F_net - F| / |F|
     double ex, ey;
     gauss_field_ool(dx, dy, sx, sy, &ex, &ey);
-    const double e0 = ex != 0.0 ? fabs(gx - ex) / fabs(ex) : 0.0;
-    const double e1 = ey != 0.0 ? fabs(gy - ey) / fabs(ey) : 0.0;
-    const double e = fmax(e0, e1);
+    const double f = hypot(ex, ey);
+    const double e = f > 0.0 ? hypot(gx - ex, gy - ey) / f : 0.0;
     aud_max = fmax(aud_max, e);
     aud_sq += e * e;
     ++aud_n;
@@ -332,7 +333,10 @@ __global__ void __launch_bounds__(128 * kMlpGroups, 1) bi_ions_mlp(BiArgs bi, Ml
       }
     }
   }
-  if (!ok && t == 0) atomicAdd(&bi.audit[3], 1ull);
+  if (!ok && t == 0) {
+    atomicAdd(&bi.audit[3], 1ull);
+    atomicOr(bi.error, 4);
+  }
   bi_audit_flush(bi, aud_max, aud_sq, aud_n, fallbacks);
   mlp_cta_release(tmem);
 }
@@ -343,11 +347,6 @@ __global__ void __launch_bounds__(128 * kMlpGroups, 1) bi_kick_mlp(Args a, BiArg
   MlpGroup G;
   const uint32_t tmem = mlp_cta_setup(M, align1024(smem_raw), G);
   const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
-  __shared__ double cl[kMlpGroups][kBiMaxIp][5];
-  __shared__ double tr[kBiMaxIp][4];
-  for (int i = threadIdx.x; i < bi.n_ip; i += blockDim.x)
-    for (int m = 0; m < 4; ++m) tr[i][m] = bi.trig[4 * i + m];
-  __syncthreads();
   const long turn = *bi.turn;
   const size_t n6 = (size_t)a.npad;
   double *C = a.coord;
@@ -360,13 +359,6 @@ __global__ void __launch_bounds__(128 * kMlpGroups, 1) bi_kick_mlp(Args a, BiArg
     const int sub = (int)(item % 64);
     if (sub * 128 >= tile.count) continue;   // the same for the whole group
     const int b = tile.bunch;
-    named_barrier(G.bar_id, 128);            // the group's previous cloud table is no longer read
-    for (int i = t; i < bi.n_ip; i += 128) {
-      const double *Cl = bi.cloud + ((size_t)i * bi.nb + b) * 5;
-      cl[g][i][0] = bi.ke * Cl[0];
-      for (int m = 1; m < 5; ++m) cl[g][i][m] = Cl[m];
-    }
-    named_barrier(G.bar_id, 128);
     const int p = tile.start + sub * 128 + t;
     const bool live = sub * 128 + t < tile.count;
     double x = 0.0, z = 0.0, xp = 0.0, zp = 0.0;
@@ -378,18 +370,25 @@ __global__ void __launch_bounds__(128 * kMlpGroups, 1) bi_kick_mlp(Args a, BiArg
     }
     double ddx = 0.0, ddxp = 0.0, ddz = 0.0, ddzp = 0.0;
     for (int k = 0; k < bi.n_ip; ++k) {
-      if (cl[g][k][0] == 0.0) continue;        // the same for the whole group
-      const double mx = tr[k][0] + bi.alphaH * tr[k][1], sxb = bi.betaH * tr[k][1];
-      const double my = tr[k][2] + bi.alphaV * tr[k][3], syb = bi.betaV * tr[k][3];
+      // the cloud this bunch meets at point k and the point's phase
+      // advance: the same addresses in every thread (cached broadcasts)
+      const double *Cl = bi.cloud + ((size_t)k * bi.nb + b) * 5;
+      const double nion = __ldg(Cl);
+      if (nion == 0.0) continue;               // the same for the whole group
+      const double *tr = bi.trig + 4 * k;
+      const double c0 = __ldg(tr), s0 = __ldg(tr + 1), c1 = __ldg(tr + 2), s1 = __ldg(tr + 3);
+      const double mx = c0 + bi.alphaH * s0, sxb = bi.betaH * s0;
+      const double my = c1 + bi.alphaV * s1, syb = bi.betaV * s1;
       const double xk = mx * x + sxb * xp, zk = my * z + syb * zp;
       double gx = 0.0, gy = 0.0;
-      if (!bi_field_mlp(bi, G, t, live, xk - cl[g][k][1], zk - cl[g][k][2], cl[g][k][3], cl[g][k][4],
+      if (!bi_field_mlp(bi, G, t, live, xk - __ldg(Cl + 1), zk - __ldg(Cl + 2), __ldg(Cl + 3), __ldg(Cl + 4),
                         bi_hash((uint32_t)turn + 0x51ED27u, (uint32_t)k, (uint32_t)(p >> 5)), gx, gy, aud_max, aud_sq,
                         aud_n, fallbacks)) {
         ok = false;
         break;
       }
-      const double thx = cl[g][k][0] * gx, thy = cl[g][k][0] * gy;
+      const double kn = bi.ke * nion;
+      const double thx = kn * gx, thy = kn * gy;
       ddx = ddx - sxb * thx;
       ddxp = ddxp + mx * thx;
       ddz = ddz - syb * thy;
@@ -402,7 +401,10 @@ __global__ void __launch_bounds__(128 * kMlpGroups, 1) bi_kick_mlp(Args a, BiArg
       C[5 * n6 + p] = zp + ddzp;
     }
   }
-  if (!ok && t == 0) atomicAdd(&bi.audit[3], 1ull);
+  if (!ok && t == 0) {
+    atomicAdd(&bi.audit[3], 1ull);
+    atomicOr(bi.error, 4);
+  }
   bi_audit_flush(bi, aud_max, aud_sq, aud_n, fallbacks);
   mlp_cta_release(tmem);
 }

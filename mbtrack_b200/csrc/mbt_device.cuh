@@ -78,7 +78,8 @@ struct RingState {
   int rffb_on;
   int rffb_count;
   int rw_m;            // resistive-wall trigger counter (worker_weakweak.c:254)
-  int error;           // sticky device error word (0 = ok)
+  int error;           // sticky device error word (0 = ok): 1 injected deviates exhausted, 2 a
+                       // particle-pass pipeline wait gave up, 4 a learned-field tensor-core wait gave up
   int trash_low, trash_high;
   double phasor[3][kMaxLr][2];
   // values of the last completed turn (what the reference holds after it)

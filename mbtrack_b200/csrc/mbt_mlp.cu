@@ -2,14 +2,14 @@
 // field (mbt_mlp.cuh) with the project's own kernels.
 //
 //   mlp_prepare   FP32 master weights -> operand tiles in the swizzled
-//                 K-major layout: FP16 W2, W3, W4 (forward), BF16 W2^T,
-//                 W3^T (backward)
+//                 K-major layout: BF16 W2/2, W3/2, the layer-1 and bias
+//                 columns, W4/2 with its bias (forward), BF16 W2^T, W3^T
+//                 (backward)
 //   mlp_forward   128-point tiles, two tile groups per CTA (256 threads),
-//                 the inference path of mbt_mlp.cuh (layer 1 on the FP32
-//                 pipes, layers 2, 3 and 4 as tcgen05.mma with FP16
-//                 operands and FP32 accumulation in tensor memory, GELU in
-//                 FP16 pairs), keeping z and h of every point for the
-//                 backward pass
+//                 the inference path of mbt_mlp.cuh (every layer a
+//                 tcgen05.mma with BF16 operands and FP32 accumulation in
+//                 tensor memory, activations in BF16 pairs), keeping z and
+//                 gelu(z) of every point for the backward pass
 //   mlp_backward  per 128-point tile: dz3 -> dh2 = dz3 W3 and
 //                 dW3 += dz3^T h2 on the tensor cores, dz2 -> dh1 = dz2 W2
 //                 and dW2 += dz2^T h1; dW2, dW3 accumulate in tensor memory
@@ -18,6 +18,8 @@
 //                 layer-4 and bias gradients, the deterministic sum of the
 //                 partials, Adam
 //   mlp_targets   labels from the Faddeeva-based field (gauss_field)
+// The forward pass rounds its operands to BF16; the gradient is taken for
+// the FP32 master weights through those roundings (straight through).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -53,18 +55,68 @@ struct MlpSave {
   float *z1, *z2, *z3, *h1, *h2, *h3;
 };
 
-__global__ void mlp_prepare(const float *P, uint8_t *W2t, uint8_t *W3t, uint8_t *W2tT, uint8_t *W3tT, uint8_t *W4t) {
+// the BF16 pair (hi, lo) of v: element `which` of it
+__device__ __forceinline__ float bf16_pair(float v, int which) {
+  const float hi = bf16_round(v);
+  return which == 0 ? hi : v - hi;
+}
+
+__global__ void mlp_prepare(const float *P, uint8_t *W) {
+  uint8_t *W2f = W + kOffW2, *W3f = W + kOffW3, *Ext = W + kOffExt, *W4f = W + kOffW4, *W2T = W + kOffW2T,
+          *W3T = W + kOffW3T;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 128 * 128; i += gridDim.x * blockDim.x) {
     const int n = i / 128, k = i % 128;
-    *reinterpret_cast<__half *>(W2t + sw128_elem(n, k)) = __float2half_rn(P[kMlpW2 + i]);
-    *reinterpret_cast<__half *>(W3t + sw128_elem(n, k)) = __float2half_rn(P[kMlpW3 + i]);
-    *reinterpret_cast<__nv_bfloat16 *>(W2tT + sw128_elem(k, n)) = __float2bfloat16_rn(P[kMlpW2 + i]);
-    *reinterpret_cast<__nv_bfloat16 *>(W3tT + sw128_elem(k, n)) = __float2bfloat16_rn(P[kMlpW3 + i]);
-    if (i < 16 * 128) {
-      const float w4 = n < 2 ? P[kMlpW4 + i] : 0.0f;
-      *reinterpret_cast<__half *>(W4t + sw128_chunk_rows(n, k >> 3, 16) + (k & 7) * 2) = __float2half_rn(w4);
+    *reinterpret_cast<__nv_bfloat16 *>(W2f + sw128_elem(n, k)) = __float2bfloat16_rn(0.5f * P[kMlpW2 + i]);
+    *reinterpret_cast<__nv_bfloat16 *>(W3f + sw128_elem(n, k)) = __float2bfloat16_rn(0.5f * P[kMlpW3 + i]);
+    *reinterpret_cast<__nv_bfloat16 *>(W2T + sw128_elem(k, n)) = __float2bfloat16_rn(P[kMlpW2 + i]);
+    *reinterpret_cast<__nv_bfloat16 *>(W3T + sw128_elem(k, n)) = __float2bfloat16_rn(P[kMlpW3 + i]);
+    if (i < 128 * 64) {
+      // [128][64]: row r = output r; k 0..2 W1 (for the inputs), 3..5 W1
+      // again (for their low parts), 6, 7 the pair of b1; 16, 17 the pair
+      // of b2; 32, 33 the pair of b3; 48, 49 ones (k-step 3 is the A
+      // operand of every bias step); zeros elsewhere
+      const int r = i / 64, c = i % 64;
+      float v = 0.0f;
+      if (c < 6) v = P[kMlpW1 + 3 * r + (c % 3)];
+      else if (c == 6 || c == 7) v = bf16_pair(P[kMlpB1 + r], c - 6);
+      else if (c == 16 || c == 17) v = bf16_pair(P[kMlpB2 + r], c - 16);
+      else if (c == 32 || c == 33) v = bf16_pair(P[kMlpB3 + r], c - 32);
+      else if (c == 48 || c == 49) v = 1.0f;
+      *reinterpret_cast<__nv_bfloat16 *>(Ext + sw128_elem(r, c)) = __float2bfloat16_rn(v);
+    }
+    if (i < 16 * 192) {
+      // [16][192]: rows 0, 1 hold W4 / 2 (k < 128) and the pair of b4
+      // (k = 128, 129); zeros elsewhere
+      const int r = i / 192, c = i % 192;
+      float v = 0.0f;
+      if (r < 2 && c < 128) v = 0.5f * P[kMlpW4 + 128 * r + c];
+      else if (r < 2 && (c == 128 || c == 129)) v = bf16_pair(P[kMlpB4 + r], c - 128);
+      *reinterpret_cast<__nv_bfloat16 *>(W4f + sw128_chunk_rows(r, c >> 3, 16) + (c & 7) * 2) =
+          __float2bfloat16_rn(v);
     }
   }
+}
+
+// Row `row` of a BF16 tile (backward operands).
+__device__ __forceinline__ void store_row_bf16(uint8_t *t, int row, const float *h) {
+#pragma unroll
+  for (int c = 0; c < 16; ++c) {
+    const uint4 p = make_uint4(pack_bf16(h[8 * c], h[8 * c + 1]), pack_bf16(h[8 * c + 2], h[8 * c + 3]),
+                               pack_bf16(h[8 * c + 4], h[8 * c + 5]), pack_bf16(h[8 * c + 6], h[8 * c + 7]));
+    *reinterpret_cast<uint4 *>(t + sw128_chunk(row, c)) = p;
+  }
+}
+// Column `col` of a BF16 tile (the transpose of a row).
+__device__ __forceinline__ void store_col_bf16(uint8_t *t, int col, const float *h) {
+#pragma unroll 8
+  for (int k = 0; k < 128; ++k)
+    *reinterpret_cast<__nv_bfloat16 *>(t + sw128_elem(k, col)) = __float2bfloat16_rn(h[k]);
+}
+// Issue one 128 x 128 x 128 BF16 product D (+)= A.B^T (backward).
+__device__ __forceinline__ void issue_layer(uint32_t d_tmem, uint32_t a, uint32_t b, bool acc0) {
+#pragma unroll
+  for (int s = 0; s < 8; ++s)
+    umma_f16(d_tmem, tile_desc(a, s), tile_desc(b, s), kIdescBf16, (s > 0 || acc0) ? 1u : 0u);
 }
 
 __device__ __forceinline__ void copy_tile(uint8_t *dst, const uint8_t *src, int tid, int nthr) {
@@ -152,6 +204,42 @@ mlp_infer(MlpDev M, long n, const float *__restrict__ abr, float *__restrict__ o
   mlp_cta_release(tmem);
 }
 
+// The learned field at n points (dx, dy, sx, sy) -> (gx, gy), with the
+// Faddeeva field outside the network's domain (counted in *fallbacks).
+__global__ void __launch_bounds__(kInfThreads, 1)
+mlp_field(MlpDev M, long n, const double *__restrict__ dx, const double *__restrict__ dy,
+          const double *__restrict__ sx, const double *__restrict__ sy, double *__restrict__ gx,
+          double *__restrict__ gy, unsigned long long *fallbacks, int *err) {
+  extern __shared__ uint8_t smem_raw[];
+  MlpGroup G;
+  const uint32_t tmem = mlp_cta_setup(M, align1024(smem_raw), G);
+  const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
+  const long ntiles = (n + 127) / 128;
+  int fb = 0;
+  for (long tile = (long)blockIdx.x * kMlpGroups + g; tile < ntiles; tile += (long)gridDim.x * kMlpGroups) {
+    const long m = tile * 128 + t;
+    const bool live = m < n;
+    double u = 0.0, v = 0.0;
+    bool in_domain;
+    if (!mlp_group_field(G, t, live, live ? dx[m] : 0.0, live ? dy[m] : 0.0, live ? sx[m] : 1.0,
+                         live ? sy[m] : 1.0, u, v, in_domain)) {
+      if (t == 0) atomicOr(err, 4);
+      break;
+    }
+    if (live && !in_domain) {
+      gauss_field(dx[m], dy[m], sx[m], sy[m], u, v);
+      ++fb;
+    }
+    if (live) {
+      gx[m] = u;
+      gy[m] = v;
+    }
+  }
+  const int f = warp_sum(fb);
+  if ((threadIdx.x & 31) == 0 && f) atomicAdd(fallbacks, (unsigned long long)f);
+  mlp_cta_release(tmem);
+}
+
 // Backward pass of a batch of n points (forward values in sv, outputs in
 // `out`, targets in `tgt`); loss = sum over points and outputs of the
 // squared error / n.  Writes dz1, dz2, dz3 ([point][128]) and dT
@@ -167,8 +255,8 @@ mlp_backward(MlpDev M, int n, const float *__restrict__ out, const float *__rest
   uint64_t *bar = reinterpret_cast<uint64_t *>(sW4 + 256);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(sW4 + 260);
   const int t = threadIdx.x;
-  copy_tile(sW3T, M.W3tT, t, kBwdThreads);
-  copy_tile(sW2T, M.W2tT, t, kBwdThreads);
+  copy_tile(sW3T, M.W3T, t, kBwdThreads);
+  copy_tile(sW2T, M.W2T, t, kBwdThreads);
   for (int i = t; i < 256; i += kBwdThreads) sW4[i] = M.P[kMlpW4 + i];
   if (t == 0) {
     mbar_init(bar, 1);
@@ -336,7 +424,7 @@ __global__ void mlp_adam(float *P, const float *g, float *mo, float *ve, float l
   P[i] -= lr * (mo[i] * c1) / (sqrtf(ve[i] * c2) + eps);
 }
 
-// Residual targets Y = 8 (F / (coordinate x envelope) - 1) of one input,
+// Residual targets Y = S (F / (coordinate x envelope) - 1) of one input,
 // F from the Faddeeva-based field (FP64).
 __device__ __forceinline__ void mlp_target(float a, float b, float q, float *y) {
   double gx, gy;
@@ -380,8 +468,9 @@ __global__ void mlp_targets_kernel(long n, const float *abr, float *tgt) {
 
 struct mbt_mlp {
   float *P = nullptr, *G = nullptr, *Mo = nullptr, *Ve = nullptr;
-  uint8_t *W = nullptr;   // operand tiles: FP16 W2, W3; BF16 W2^T, W3^T; FP16 W4 (16 rows)
+  uint8_t *W = nullptr;   // operand tiles (kOff* offsets of mbt_mlp.cuh)
   int *err = nullptr;
+  unsigned long long *counter = nullptr;   // fallbacks of mlp_field
   long adam_t = 0;
   int nsm = 148;
   // training scratch
@@ -396,11 +485,12 @@ namespace {
 MlpDev dev_view(const mbt_mlp *m) {
   MlpDev d;
   d.P = m->P;
-  d.W2t = m->W;
-  d.W3t = m->W + kTileBytes;
-  d.W2tT = m->W + 2 * kTileBytes;
-  d.W3tT = m->W + 3 * kTileBytes;
-  d.W4t = m->W + 4 * kTileBytes;
+  d.W2f = m->W + kOffW2;
+  d.W3f = m->W + kOffW3;
+  d.Ext = m->W + kOffExt;
+  d.W4f = m->W + kOffW4;
+  d.W2T = m->W + kOffW2T;
+  d.W3T = m->W + kOffW3T;
   return d;
 }
 
@@ -410,8 +500,7 @@ int ck(cudaError_t e, const char *what) {
 }
 
 int prepare(mbt_mlp *m, cudaStream_t st) {
-  mlp_prepare<<<64, 256, 0, st>>>(m->P, m->W, m->W + kTileBytes, m->W + 2 * kTileBytes, m->W + 3 * kTileBytes,
-                                  m->W + 4 * kTileBytes);
+  mlp_prepare<<<64, 256, 0, st>>>(m->P, m->W);
   return ck(cudaGetLastError(), "mlp_prepare");
 }
 
@@ -481,6 +570,7 @@ int set_attrs() {
   int r = ck(cudaFuncSetAttribute(mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem), "attr");
   if (!r) r = ck(cudaFuncSetAttribute(mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInfSmem), "attr");
   if (!r) r = ck(cudaFuncSetAttribute(mlp_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmem), "attr");
+  if (!r) r = ck(cudaFuncSetAttribute(mlp_field, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInfSmem), "attr");
   if (!r) attrs_set = true;
   return r;
 }
@@ -506,7 +596,8 @@ int mbt_mlp_create(uint64_t seed, mbt_mlp **out) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, dev);
   if (cudaMalloc(&m->P, kMlpNParam * 4) || cudaMalloc(&m->G, kMlpNParam * 4) || cudaMalloc(&m->Mo, kMlpNParam * 4) ||
-      cudaMalloc(&m->Ve, kMlpNParam * 4) || cudaMalloc(&m->W, 4 * kTileBytes + kW4TileBytes) || cudaMalloc(&m->err, sizeof(int))) {
+      cudaMalloc(&m->Ve, kMlpNParam * 4) || cudaMalloc(&m->W, kMlpTileBytes) || cudaMalloc(&m->err, sizeof(int)) ||
+      cudaMalloc(&m->counter, sizeof(unsigned long long))) {
     mbt_mlp_destroy(m);
     return mbt::fail_global(MBT_ERR_NOMEM, "MLP parameters");
   }
@@ -540,6 +631,7 @@ int mbt_mlp_create(uint64_t seed, mbt_mlp **out) {
 int mbt_mlp_destroy(mbt_mlp *m) {
   if (!m) return 0;
   cudaFree(m->P); cudaFree(m->G); cudaFree(m->Mo); cudaFree(m->Ve); cudaFree(m->W); cudaFree(m->err);
+  cudaFree(m->counter);
   cudaFree(m->abr); cudaFree(m->tgt); cudaFree(m->outb); cudaFree(m->save); cudaFree(m->dz); cudaFree(m->dT);
   cudaFree(m->part); cudaFree(m->lpart);
   delete m;
@@ -573,6 +665,27 @@ int mbt_mlp_forward_dev(mbt_mlp *m, long n, const float *abr, float *t_out, void
   r = ck(cudaGetLastError(), "mlp_infer");
   if (!r) r = ck(cudaStreamSynchronize((cudaStream_t)stream), "mlp_forward");
   if (!r) r = check_err(m);
+  return r;
+}
+
+int mbt_mlp_field_dev(mbt_mlp *m, long n, const double *dx, const double *dy, const double *sx, const double *sy,
+                      double *gx, double *gy, long *fallbacks, void *stream) {
+  if (!m || n < 0 || (n > 0 && (!dx || !dy || !sx || !sy || !gx || !gy))) return MBT_ERR_INVALID;
+  if (fallbacks) *fallbacks = 0;
+  if (n == 0) return 0;
+  int r = set_attrs();
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  r = ck(cudaMemsetAsync(m->counter, 0, sizeof(unsigned long long), st), "counter");
+  if (r) return r;
+  const int grid = (int)std::max<long>(1, std::min<long>(m->nsm, ((n + 127) / 128 + kMlpGroups - 1) / kMlpGroups));
+  mlp_field<<<grid, kInfThreads, kInfSmem, st>>>(dev_view(m), n, dx, dy, sx, sy, gx, gy, m->counter, m->err);
+  r = ck(cudaGetLastError(), "mlp_field");
+  unsigned long long fb = 0;
+  if (!r) r = ck(cudaMemcpyAsync(&fb, m->counter, sizeof fb, cudaMemcpyDeviceToHost, st), "fallbacks");
+  if (!r) r = ck(cudaStreamSynchronize(st), "mlp_field");
+  if (!r) r = check_err(m);
+  if (!r && fallbacks) *fallbacks = (long)fb;
   return r;
 }
 

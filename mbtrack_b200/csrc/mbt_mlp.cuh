@@ -1,40 +1,45 @@
 // mbt_mlp.cuh -- the learned Bassetti-Erskine field: a 3 -> 128 -> 128 ->
-// 128 -> 2 GELU network whose two hidden 128 x 128 layers run on the
-// fifth-generation tensor cores (tcgen05.mma, BF16 operands from shared
-// memory, FP32 accumulators in tensor memory), with the 3 -> 128 and
-// 128 -> 2 layers on the FP32 pipes.
+// 128 -> 2 GELU network with every layer on the fifth-generation tensor
+// cores (tcgen05.mma kind::f16, BF16 operands from shared memory, FP32
+// accumulators in tensor memory) and its activations in BF16 pair
+// arithmetic.
 //
 // What it learns.  For the unit-charge field of mbt_gauss_field_dev with
 // a = |dx|/sx, b = |dy|/sy in [0, 8), r = sy/sx in [0.05, 1] (axes swapped
 // when sy > sx, signs restored from dx, dy), the dimensionless field
 // F = sx (gx, gy) is written as
-//   Fx = a Ex (1 + Yx / 8),   Fy = b Ey (1 + Yy / 8),
-// where Ex, Ey are coarse Gauss-Legendre quadratures (8 and 16 nodes, FP32)
-// of the field integral in substitutions that follow its two scales,
-//   Ex = 1/(pi (1+r)) sum_i w_i exp(-t_i^2 (a^2 + b^2 r^2 / u_i^2) / 2),
-//        u_i = r + (1-r) x_i,  t_i^2 = (1 - x_i)(1 + u_i)/(1 + r),
-//   Ey = r S/(2 pi) sum_i w_i exp(-s_i (a^2 + b^2 r^2 / d_i) / 2) d_i^(-3/2),
-//        s_i = S x_i,  d_i = 1 - (1 - r^2) s_i,  S = min(1, 80/(a^2 + b^2 r^2)),
-// which carry the field to within about 10 % everywhere, and the network
-// predicts the residuals Y (of order one).  Its error therefore enters the
-// field divided by 8 and by the envelope's share.
-
-// Numerics of a forward pass (the oracle restates them):
-//   x = (a/4 - 1, b/4 - 1, 1 + 2 ln r / ln 20);  z1 = W1 x + b1  (FP32)
-//   h1 = gelu(z1) in FP16 pair arithmetic (gelu_h2), an FP16 value
-//   z2 = W2h h1 + b2: W2h = W2 rounded to FP16, FP32 sums on the tensor
-//   cores, FP32 bias;  h2 = gelu(z2);  z3 = W3h h2 + b3;  h3 = gelu(z3)
-//   Y = W4h h3 + b4  (tensor cores, N = 16 with W4 padded; FP32 bias)
-// gelu(x) = x (1 + tanh(x (c1 + c1 c2 x^2))) / 2, c1 = sqrt(2/pi),
-// c2 = 0.044715 (FP16 constants), with the hardware tanh.  ln r spreads the
-// flat aspect ratios, where the field changes fastest and the beam-ion
-// stage evaluates most, over the feature range.
+//   Fx = a Ex (1 + Yx / S),   Fy = b Ey (1 + Yy / S),   S = 4096,
+// where (a Ex, b Ey) is the field integral
+//   F = (a, b r) / (2 pi) Int_0^1 e^-Phi(s) (D^-1/2, D^-3/2) ds,
+//   D = 1 - (1 - r^2) s,   Phi = s (a^2 + b^2 r^2 / D) / 2
+// evaluated by a two-panel 8 + 8 node Gauss-Legendre rule in FP32 (the
+// envelope, mlp_envelopes): panel 1 in s over [0, s_top], s_top =
+// min(1/2, 40 / (a^2 + b^2 r^2)); panel 2 over [1/2, 1] in v = D^-1/2 on a
+// geometric map for r <= 1/2 (where D^-3/2 peaks near s = 1), in s above.
+// The envelope carries the field to within 2e-4 everywhere in the domain
+// (median 1e-7); the network predicts the scaled residuals Y (below 1), so
+// its BF16 rounding noise (a few 1e-3 of its output scale) enters the field
+// divided by S.
 //
-// Tile shape: 128 points per MMA tile (M = 128, N = 128 or 16, K = 16 per
-// instruction, 8 k-steps); operands in the canonical K-major 128-byte-
-// swizzled layout: a [128][128] BF16 tile is two 16 KB column blocks of 64
-// elements, each 16 groups of 8 rows x 128 B, the 16-byte chunk index of a
-// row XORed with the row index inside its group.
+// Numerics of a forward pass (the oracle restates them):
+//   x = (a/4 - 1, b/4 - 1, 1 + 2 ln r / ln 20) in FP32, split into BF16
+//   pairs x = xh + xl;
+//   layer 1:  z1 = W1h xh + W1h xl + (b1h + b1l)   (one K = 16 product: the
+//             inputs, their low parts and two bias columns of ones)
+//   hidden:   h' = z (1 + tanh(z (c1 + c1c2 z^2))) = 2 gelu(z) in BF16 pair
+//             arithmetic, c1 = sqrt(2/pi), c2 = 0.044715 (BF16 constants,
+//             hardware tanh); the 1/2 of GELU is folded into the next
+//             layer's weights (exact in BF16):
+//   layers 2, 3:  z = (W/2)h h' + (bh + bl)   (8 k-steps of the activation
+//             tile and one of a column pair of ones against the bias columns)
+//   output:   Y = (W4/2)h h3' + (b4h + b4l)   (N = 16, rows 2.. zero)
+// with Wh = W rounded to BF16, bh + bl the BF16 pair of a bias, FP32 sums.
+//
+// Tiles: 128 points per MMA tile (M = 128, N = 128 or 16, K = 16 per
+// instruction) in the canonical K-major 128-byte-swizzled layout: a
+// [rows][128] BF16 tile is two column blocks of 64 elements, each rows/8
+// groups of 8 rows x 128 B, the 16-byte chunk index of a row XORed with the
+// row index inside its group.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -48,7 +53,14 @@ constexpr int kMlpH = 128;
 constexpr int kMlpW1 = 0, kMlpB1 = 384, kMlpW2 = 512, kMlpB2 = kMlpW2 + 16384, kMlpW3 = kMlpB2 + 128,
               kMlpB3 = kMlpW3 + 16384, kMlpW4 = kMlpB3 + 128, kMlpB4 = kMlpW4 + 256, kMlpNParam = kMlpB4 + 2;
 constexpr int kTileBytes = 128 * 128 * 2;   // one [128][128] BF16 operand tile
-constexpr long kMlpWaitLimit = 1L << 24;     // polls of an MMA-completion barrier before giving up
+constexpr int kExtBytes = 128 * 64 * 2;     // [128][64]: layer 1 (k-step 0), bias columns (k-steps 1, 2), ones (3)
+constexpr int kW4Bytes = 16 * 192 * 2;      // [16][192]: W4 / 2 (k < 128) and its bias columns (k-step 8)
+constexpr long kMlpWaitLimit = 1L << 24;    // polls of an MMA-completion barrier before giving up
+constexpr float kMlpResidualScale = 4096.0f;   // Y = S (F / envelope - 1)
+
+// Operand tiles in global memory (mlp_prepare writes them), byte offsets.
+constexpr int kOffW2 = 0, kOffW3 = kTileBytes, kOffExt = 2 * kTileBytes, kOffW4 = kOffExt + kExtBytes,
+              kOffW2T = kOffW4 + kW4Bytes, kOffW3T = kOffW2T + kTileBytes, kMlpTileBytes = kOffW3T + kTileBytes;
 
 // ---- tcgen05 / tensor-memory primitives
 __device__ __forceinline__ void tmem_alloc(uint32_t *dst, uint32_t ncols) {
@@ -64,9 +76,10 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// D[tmem] (+)= A[smem] . B[smem]^T, M = N = 128, K = 16, BF16 -> FP32
-__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                          uint32_t accumulate) {
+// D[tmem] (+)= A[smem] . B[smem]^T, kind::f16 (A and B of the same 16-bit
+// type), FP32 accumulator
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
@@ -113,6 +126,13 @@ __device__ __forceinline__ void tmem_wait16(float *v) {
                :
                : "memory");
 }
+// Two FP32 columns of this thread's tensor-memory lane.
+__device__ __forceinline__ void tmem_ld2(uint32_t taddr, float &a, float &b) {
+  uint32_t r0, r1;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(r0), "=r"(r1) : "r"(taddr));
+  a = __uint_as_float(r0);
+  b = __uint_as_float(r1);
+}
 
 // AND of `v` over the `count` threads of named barrier `id` (a barrier too)
 __device__ __forceinline__ bool group_all(bool v, int id, int count) {
@@ -135,23 +155,32 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
          ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
-// descriptor of k-step s (16 elements) of a [128][128] tile at `base`
-__device__ __forceinline__ uint64_t tile_desc(uint32_t base, int s) {
-  return sw128_desc(base + (uint32_t)(s >> 2) * 16384u + (uint32_t)(s & 3) * 32u);
+// descriptor of k-step s (16 elements) of a tile of `rows` rows at `base`
+__device__ __forceinline__ uint64_t tile_desc_rows(uint32_t base, int s, int rows) {
+  return sw128_desc(base + (uint32_t)(s >> 2) * (uint32_t)(rows * 128) + (uint32_t)(s & 3) * 32u);
 }
+__device__ __forceinline__ uint64_t tile_desc(uint32_t base, int s) { return tile_desc_rows(base, s, 128); }
+
 // instruction descriptor: FP32 accumulator, BF16 A and B, both K-major,
-// N = 128, M = 128
-constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
-
-// byte offset of the 16-byte chunk c (elements 8c .. 8c+7) of row `row`
-__device__ __forceinline__ uint32_t sw128_chunk(int row, int c) {
-  return (uint32_t)((c >> 3) * 16384 + (row >> 3) * 1024 + (row & 7) * 128 + (((c & 7) ^ (row & 7)) << 4));
+// M = 128, N = n
+__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
 }
-// byte offset of element (row, k)
-__device__ __forceinline__ uint32_t sw128_elem(int row, int k) { return sw128_chunk(row, k >> 3) + (k & 7) * 2; }
+constexpr uint32_t kIdescBf16 = idesc_bf16(128), kIdescBf16N16 = idesc_bf16(16);
 
-__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
-  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+// byte offset of the 16-byte chunk c (elements 8c .. 8c+7) of row `row` in
+// a tile of `rows` rows
+__host__ __device__ __forceinline__ uint32_t sw128_chunk_rows(int row, int c, int rows) {
+  return (uint32_t)((c >> 3) * rows * 128 + (row >> 3) * 1024 + (row & 7) * 128 + (((c & 7) ^ (row & 7)) << 4));
+}
+__host__ __device__ __forceinline__ uint32_t sw128_chunk(int row, int c) { return sw128_chunk_rows(row, c, 128); }
+// byte offset of element (row, k)
+__host__ __device__ __forceinline__ uint32_t sw128_elem(int row, int k) {
+  return sw128_chunk(row, k >> 3) + (k & 7) * 2;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<const uint32_t *>(&h);
 }
 __device__ __forceinline__ float bf16_round(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
@@ -163,125 +192,79 @@ __device__ __forceinline__ float tanh_hw(float x) {
   return y;
 }
 constexpr float kGeluC1 = 0.7978845608028654f, kGeluC1C2 = 0.035677408136300125f;
+// derivative of gelu(x) = x (1 + tanh(x (c1 + c1c2 x^2))) / 2 (FP32)
 __device__ __forceinline__ float gelu_grad(float x) {
   const float y = x * fmaf(kGeluC1C2, x * x, kGeluC1);
   const float th = tanh_hw(y);
   return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * 0.7978845608028654f * (1.0f + 0.134145f * x * x);
 }
 
-// Forward operands are FP16 (the weights W2, W3, W4 and the activations;
-// FP16 keeps 11 significant bits where BF16 keeps 8), backward operands
-// BF16 (gradients need BF16's exponent range).  In one MMA both operands
-// have the same type.
-constexpr int kMlpGroups = 4;                       // 128-thread groups per inference CTA
-constexpr int kW4TileBytes = 16 * 128 * 2;          // W4 as a [16][128] FP16 tile (rows 2..15 zero)
-
-// FP32 accumulator, FP16 A and B, both K-major, M = 128, N = n
-__host__ __device__ constexpr uint32_t idesc_f16(uint32_t n) {
-  return (1u << 4) | ((n >> 3) << 17) | ((128u >> 4) << 24);
-}
-constexpr uint32_t kIdescF16 = idesc_f16(128), kIdescF16N16 = idesc_f16(16);
-
-// byte offset of the 16-byte chunk c of row `row` in a tile of `rows` rows
-__device__ __forceinline__ uint32_t sw128_chunk_rows(int row, int c, int rows) {
-  return (uint32_t)((c >> 3) * rows * 128 + (row >> 3) * 1024 + (row & 7) * 128 + (((c & 7) ^ (row & 7)) << 4));
-}
-// descriptor of k-step s of a tile of `rows` rows at `base`
-__device__ __forceinline__ uint64_t tile_desc_rows(uint32_t base, int s, int rows) {
-  return sw128_desc(base + (uint32_t)(s >> 2) * (uint32_t)(rows * 128) + (uint32_t)(s & 3) * 32u);
-}
-
-// Row `row` of a tile, BF16 only (backward operands).
-__device__ __forceinline__ void store_row_bf16(uint8_t *t, int row, const float *h) {
-#pragma unroll
-  for (int c = 0; c < 16; ++c) {
-    const uint4 p = make_uint4(pack_bf16(h[8 * c], h[8 * c + 1]), pack_bf16(h[8 * c + 2], h[8 * c + 3]),
-                               pack_bf16(h[8 * c + 4], h[8 * c + 5]), pack_bf16(h[8 * c + 6], h[8 * c + 7]));
-    *reinterpret_cast<uint4 *>(t + sw128_chunk(row, c)) = p;
-  }
-}
-// Column `col` of a tile (the transpose of a row), BF16.
-__device__ __forceinline__ void store_col_bf16(uint8_t *t, int col, const float *h) {
-#pragma unroll 8
-  for (int k = 0; k < 128; ++k)
-    *reinterpret_cast<__nv_bfloat16 *>(t + sw128_elem(k, col)) = __float2bfloat16_rn(h[k]);
-}
-
-// Issue one 128 x 128 x 128 BF16 product D (+)= A.B^T (backward).
-__device__ __forceinline__ void issue_layer(uint32_t d_tmem, uint32_t a, uint32_t b, bool acc0) {
-#pragma unroll
-  for (int s = 0; s < 8; ++s)
-    umma_bf16(d_tmem, tile_desc(a, s), tile_desc(b, s), kIdescBf16, (s > 0 || acc0) ? 1u : 0u);
-}
-// The forward products: a hidden layer (N = 128) and the output layer
-// (N = 16, W4 padded), FP16 operands.
-__device__ __forceinline__ void issue_hidden_f16(uint32_t d_tmem, uint32_t a, uint32_t b) {
-#pragma unroll
-  for (int s = 0; s < 8; ++s) umma_bf16(d_tmem, tile_desc(a, s), tile_desc(b, s), kIdescF16, s > 0 ? 1u : 0u);
-}
-__device__ __forceinline__ void issue_out_f16(uint32_t d_tmem, uint32_t a, uint32_t b16) {
-#pragma unroll
-  for (int s = 0; s < 8; ++s)
-    umma_bf16(d_tmem, tile_desc(a, s), tile_desc_rows(b16, s, 16), kIdescF16N16, s > 0 ? 1u : 0u);
-}
-
-// Two FP32 columns of this thread's tensor-memory lane.
-__device__ __forceinline__ void tmem_ld2(uint32_t taddr, float &a, float &b) {
-  uint32_t r0, r1;
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(r0), "=r"(r1) : "r"(taddr));
-  a = __uint_as_float(r0);
-  b = __uint_as_float(r1);
-}
-
-// GELU of a pair of pre-activations in FP16 pair arithmetic, one
+// The activation of a pair of pre-activations in BF16 pair arithmetic, one
 // instruction per step for both values and one hardware tanh per pair:
-//   z = fp16(z),  y = z (c1 + c1c2 z^2),  h = z/2 + (z/2) tanh(y),
-// with the FP16 constants c1c2 = 0x2891, c1 = 0x3A62, 1/2 = 0x3800 and every
-// step rounded to FP16.  Returns the FP16 pair (low half from z0).
-constexpr uint32_t kH2C1C2 = 0x28912891u, kH2C1 = 0x3A623A62u, kH2Half = 0x38003800u;
-__device__ __forceinline__ uint32_t gelu_h2(float z0, float z1) {
-  uint32_t z, t, p, y, th, hz, h;
-  asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(z) : "f"(z1), "f"(z0));
-  asm("mul.rn.f16x2 %0, %1, %1;" : "=r"(t) : "r"(z));
-  asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(p) : "r"(t), "r"(kH2C1C2), "r"(kH2C1));
-  asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(y) : "r"(z), "r"(p));
-  asm("tanh.approx.f16x2 %0, %1;" : "=r"(th) : "r"(y));
-  asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(hz) : "r"(z), "r"(kH2Half));
-  asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(h) : "r"(hz), "r"(th), "r"(hz));
+//   z = bf16(z),  y = z (c1 + c1c2 z^2),  h' = z + z tanh(y) = 2 gelu(z),
+// with the BF16 constants c1 = 0x3F4C, c1c2 = 0x3D12 and every step rounded
+// to BF16.  Returns the BF16 pair (low half from z0).
+constexpr uint32_t kB2C1 = 0x3F4C3F4Cu, kB2C1C2 = 0x3D123D12u;
+__device__ __forceinline__ uint32_t act_bf16x2(float z0, float z1) {
+  uint32_t z, t, p, y, th, h;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(z) : "f"(z1), "f"(z0));
+  asm("mul.rn.bf16x2 %0, %1, %1;" : "=r"(t) : "r"(z));
+  asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(p) : "r"(t), "r"(kB2C1C2), "r"(kB2C1));
+  asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(y) : "r"(z), "r"(p));
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(th) : "r"(y));
+  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(h) : "r"(z), "r"(th));
   return h;
 }
-__device__ __forceinline__ void unpack_h2(uint32_t h, float &a, float &b) {
-  asm("{\n\t.reg .f16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\tcvt.f32.f16 %0, lo;\n\tcvt.f32.f16 %1, hi;\n\t}"
-      : "=f"(a), "=f"(b)
-      : "r"(h));
+__device__ __forceinline__ void unpack_bf16x2(uint32_t h, float &lo, float &hi) {
+  lo = __uint_as_float(h << 16);
+  hi = __uint_as_float(h & 0xFFFF0000u);
 }
 
 // One group of 128 threads evaluating the network on a tile of 128 points
 // (thread t holds point t): shared-memory operands, its tensor-memory
 // accumulator, the barrier its MMAs complete on.
 struct MlpGroup {
-  const float *W1, *B1, *B2, *B3, *B4;         // shared memory, FP32
-  uint8_t *A;                                  // the group's activation tile (FP16)
+  uint8_t *A;                                  // the group's activation tile
   uint64_t *bar;                               // MMA-completion barrier
-  uint32_t aW2, aW3, aW4, aA;                  // shared addresses of the operand tiles
+  uint32_t aW2, aW3, aExt, aW4, aA;            // shared addresses of the operand tiles
   uint32_t dcol;                               // accumulator: first tensor-memory column
   uint32_t lane;                               // this warp's lane base (bits 16..)
+  uint32_t row;                                // byte offset of this thread's row in a column block
+  int swz;                                     // this thread's row inside its 8-row group
   int bar_id;                                  // named barrier of the group
   uint32_t phase;
 };
 
-// Issue (one thread) and wait (all) for one product of the group; false
-// when it never completed (a second bounded wait then covers the MMAs in
+// The products of one layer; one thread issues them.
+enum { kLayer1 = 0, kLayer2 = 1, kLayer3 = 2, kLayerOut = 3 };
+template <int L>
+__device__ __forceinline__ void issue_layer_fwd(const MlpGroup &G) {
+  if (L == kLayer1) {
+    umma_f16(G.dcol, tile_desc(G.aA, 0), tile_desc(G.aExt, 0), kIdescBf16, 0u);
+  } else if (L == kLayerOut) {
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
+      umma_f16(G.dcol, tile_desc(G.aA, s), tile_desc_rows(G.aW4, s, 16), kIdescBf16N16, s > 0 ? 1u : 0u);
+    umma_f16(G.dcol, tile_desc(G.aExt, 3), tile_desc_rows(G.aW4, 8, 16), kIdescBf16N16, 1u);
+  } else {
+    const uint32_t w = L == kLayer2 ? G.aW2 : G.aW3;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) umma_f16(G.dcol, tile_desc(G.aA, s), tile_desc(w, s), kIdescBf16, s > 0 ? 1u : 0u);
+    umma_f16(G.dcol, tile_desc(G.aExt, 3), tile_desc(G.aExt, L), kIdescBf16, 1u);
+  }
+}
+
+// Issue (one thread) and wait (all) for one layer of the group; false when
+// it never completed (a second bounded wait then covers the MMAs in
 // flight).
-template <int KIND>
-__device__ __forceinline__ bool group_mma(MlpGroup &G, int t, uint32_t b) {
+template <int L>
+__device__ __forceinline__ bool group_mma(MlpGroup &G, int t) {
   fence_proxy_async();
   tc_fence_before();
   named_barrier(G.bar_id, 128);
   if (t == 0) {
     tc_fence_after();
-    if (KIND == 0) issue_hidden_f16(G.dcol, G.aA, b);
-    else issue_out_f16(G.dcol, G.aA, b);
+    issue_layer_fwd<L>(G);
     umma_commit(G.bar);
   }
   if (!group_all(mbar_wait(G.bar, G.phase, kMlpWaitLimit), G.bar_id, 128)) {
@@ -293,79 +276,46 @@ __device__ __forceinline__ bool group_mma(MlpGroup &G, int t, uint32_t b) {
   return true;
 }
 
-// Layer 1 of this thread's point (FP32 pre-activations, FP16 GELU) into
-// row t of the activation tile; z1 / h1 (may be null) receive the values.
-__device__ __forceinline__ void mlp_layer1(const MlpGroup &G, int t, const float *x, float *z1, float *h1) {
-  const float4 *W1v = reinterpret_cast<const float4 *>(G.W1), *B1v = reinterpret_cast<const float4 *>(G.B1);
-#pragma unroll 1
-  for (int c = 0; c < 16; ++c) {
-    float w[24], bb[8], z[8];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      const float4 v = W1v[6 * c + i];
-      w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w;
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const float4 v = B1v[2 * c + i];
-      bb[4 * i] = v.x; bb[4 * i + 1] = v.y; bb[4 * i + 2] = v.z; bb[4 * i + 3] = v.w;
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      float zz = bb[i];
-      zz = fmaf(w[3 * i], x[0], zz);
-      zz = fmaf(w[3 * i + 1], x[1], zz);
-      zz = fmaf(w[3 * i + 2], x[2], zz);
-      z[i] = zz;
-    }
-    uint32_t h[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) h[i] = gelu_h2(z[2 * i], z[2 * i + 1]);
-    *reinterpret_cast<uint4 *>(G.A + sw128_chunk(t, c)) = make_uint4(h[0], h[1], h[2], h[3]);
-    if (z1) {
-#pragma unroll
-      for (int i = 0; i < 8; ++i) z1[8 * c + i] = z[i];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) unpack_h2(h[i], h1[8 * c + 2 * i], h1[8 * c + 2 * i + 1]);
-    }
-  }
+// Row t of the layer-1 operand (k-step 0 of the activation tile): the BF16
+// pairs of the three features, their low parts, two ones; zeros.
+__device__ __forceinline__ void mlp_input_row(const MlpGroup &G, const float *x) {
+  const float h0 = bf16_round(x[0]), h1 = bf16_round(x[1]), h2 = bf16_round(x[2]);
+  const uint4 c0 = make_uint4(pack_bf16(h0, h1), pack_bf16(h2, x[0] - h0), pack_bf16(x[1] - h1, x[2] - h2),
+                              0x3F803F80u);
+  *reinterpret_cast<uint4 *>(G.A + G.row + ((0 ^ G.swz) << 4)) = c0;
+  *reinterpret_cast<uint4 *>(G.A + G.row + ((1 ^ G.swz) << 4)) = make_uint4(0u, 0u, 0u, 0u);
 }
 
-// 16 accumulator columns (k0 .. k0+15) + bias -> FP16 GELU -> two chunks
-// of row t of the activation tile.
-__device__ __forceinline__ void mlp_epi16(const MlpGroup &G, int t, const float4 *bias, int k0, const float *v,
-                                          float *zs, float *hs) {
+// 16 accumulator columns (k0 .. k0+15) -> activation -> two chunks of row t
+// of the activation tile; zs / hs (may be null) receive the pre-activations
+// and the activations gelu(z) = h'/2.
+__device__ __forceinline__ void mlp_act16(const MlpGroup &G, int k0, const float *v, float *zs, float *hs) {
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
-    float z[8];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const float4 bv = bias[(k0 + 8 * c) / 4 + i];
-      z[4 * i] = v[8 * c + 4 * i] + bv.x;
-      z[4 * i + 1] = v[8 * c + 4 * i + 1] + bv.y;
-      z[4 * i + 2] = v[8 * c + 4 * i + 2] + bv.z;
-      z[4 * i + 3] = v[8 * c + 4 * i + 3] + bv.w;
-    }
     uint32_t h[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) h[i] = gelu_h2(z[2 * i], z[2 * i + 1]);
-    *reinterpret_cast<uint4 *>(G.A + sw128_chunk(t, (k0 >> 3) + c)) = make_uint4(h[0], h[1], h[2], h[3]);
+    for (int i = 0; i < 4; ++i) h[i] = act_bf16x2(v[8 * c + 2 * i], v[8 * c + 2 * i + 1]);
+    const int ch = (k0 >> 3) + c;
+    *reinterpret_cast<uint4 *>(G.A + (ch >> 3) * 16384 + G.row + (((ch & 7) ^ G.swz) << 4)) =
+        make_uint4(h[0], h[1], h[2], h[3]);
     if (zs) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) zs[k0 + 8 * c + i] = z[i];
+      for (int i = 0; i < 8; ++i) zs[k0 + 8 * c + i] = v[8 * c + i];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) unpack_h2(h[i], hs[k0 + 8 * c + 2 * i], hs[k0 + 8 * c + 2 * i + 1]);
+      for (int i = 0; i < 4; ++i) {
+        float lo, hi;
+        unpack_bf16x2(h[i], lo, hi);
+        hs[k0 + 8 * c + 2 * i] = 0.5f * lo;
+        hs[k0 + 8 * c + 2 * i + 1] = 0.5f * hi;
+      }
     }
   }
 }
 
-// Epilogue of a hidden layer: accumulator + bias, FP16 GELU, into row t of
-// the activation tile (the product that read the tile has completed), 16
-// columns at a time with the next 16 loading meanwhile.  zs / hs (may be
-// null) receive the values.
-__device__ __forceinline__ void mlp_hidden_epilogue(const MlpGroup &G, int t, const float *bias_smem, float *zs,
-                                                    float *hs) {
-  const float4 *bias = reinterpret_cast<const float4 *>(bias_smem);
+// Epilogue of a layer: accumulator (bias included) -> activation -> row t
+// of the activation tile (the product that read the tile has completed), 16
+// columns at a time with the next 16 loading meanwhile.
+__device__ __forceinline__ void mlp_epilogue(const MlpGroup &G, float *zs, float *hs) {
   const uint32_t col = G.dcol + G.lane;
   float va[16], vb[16];
   tmem_ld16(col, va);
@@ -373,10 +323,10 @@ __device__ __forceinline__ void mlp_hidden_epilogue(const MlpGroup &G, int t, co
 #pragma unroll 1
   for (int k0 = 0; k0 < 128; k0 += 32) {
     tmem_ld16(col + k0 + 16, vb);
-    mlp_epi16(G, t, bias, k0, va, zs, hs);
+    mlp_act16(G, k0, va, zs, hs);
     tmem_wait16(vb);
     if (k0 + 32 < 128) tmem_ld16(col + k0 + 32, va);
-    mlp_epi16(G, t, bias, k0 + 16, vb, zs, hs);
+    mlp_act16(G, k0 + 16, vb, zs, hs);
     if (k0 + 32 < 128) tmem_wait16(va);
   }
   tc_fence_before();
@@ -393,36 +343,41 @@ struct MlpRowSave {
 // pre-activations and activations go (training), or null.
 __device__ __forceinline__ bool mlp_group_eval(MlpGroup &G, int t, const float *x, float *y,
                                                const MlpRowSave *sv = nullptr) {
-  mlp_layer1(G, t, x, sv ? sv->z1 : nullptr, sv ? sv->h1 : nullptr);
-  if (!group_mma<0>(G, t, G.aW2)) return false;
-  mlp_hidden_epilogue(G, t, G.B2, sv ? sv->z2 : nullptr, sv ? sv->h2 : nullptr);
-  if (!group_mma<0>(G, t, G.aW3)) return false;
-  mlp_hidden_epilogue(G, t, G.B3, sv ? sv->z3 : nullptr, sv ? sv->h3 : nullptr);
-  if (!group_mma<1>(G, t, G.aW4)) return false;
-  float o0, o1;
-  tmem_ld2(G.dcol + G.lane, o0, o1);
+  mlp_input_row(G, x);
+  if (!group_mma<kLayer1>(G, t)) return false;
+  mlp_epilogue(G, sv ? sv->z1 : nullptr, sv ? sv->h1 : nullptr);
+  if (!group_mma<kLayer2>(G, t)) return false;
+  mlp_epilogue(G, sv ? sv->z2 : nullptr, sv ? sv->h2 : nullptr);
+  if (!group_mma<kLayer3>(G, t)) return false;
+  mlp_epilogue(G, sv ? sv->z3 : nullptr, sv ? sv->h3 : nullptr);
+  if (!group_mma<kLayerOut>(G, t)) return false;
+  tmem_ld2(G.dcol + G.lane, y[0], y[1]);
   tmem_ld_wait();
   tc_fence_before();
-  y[0] = o0 + G.B4[0];
-  y[1] = o1 + G.B4[1];
   return true;
 }
 
 // Device view of a network: FP32 parameters and the operand tiles.
 struct MlpDev {
   const float *P;               // master parameters (kMlpNParam)
-  const uint8_t *W2t, *W3t;     // FP16 operand tiles of W2, W3 (rows n, k)
-  const uint8_t *W4t;           // FP16 [16][128] tile of W4 (rows 2..15 zero)
-  const uint8_t *W2tT, *W3tT;   // BF16 tiles of W2^T, W3^T (rows k, n), backward
+  const uint8_t *W2f, *W3f;     // BF16 tiles of W2 / 2, W3 / 2 (rows n, k)
+  const uint8_t *Ext;           // BF16 [128][64]: layer 1 (k-step 0), biases of layers 2, 3 (k-steps 1, 2),
+                                //   ones in columns 48, 49 (k-step 3, the A operand of every bias step)
+  const uint8_t *W4f;           // BF16 [16][192]: W4 / 2 (rows 0, 1) and its bias (k-step 8)
+  const uint8_t *W2T, *W3T;     // BF16 tiles of W2^T, W3^T (rows k, n), backward
 };
 
 // Shared-memory footprint of a CTA of `groups` groups that evaluates the
-// network: two weight tiles, the W4 tile, the groups' activation tiles,
-// the FP32 layers and barriers.
+// network: W2, W3, the layer-1/bias/ones tile, the W4 tile, the groups'
+// activation tiles, barriers (plus 1 KB of alignment slack).
+constexpr size_t kSmemW2 = 0, kSmemW3 = kTileBytes, kSmemExt = 2 * kTileBytes, kSmemW4 = kSmemExt + kExtBytes,
+                 kSmemA = kSmemW4 + kW4Bytes;
 __host__ __device__ constexpr size_t mlp_cta_smem(int groups) {
-  return (2 + (size_t)groups) * kTileBytes + kW4TileBytes + 1024 + 4096;
+  return kSmemA + (size_t)groups * kTileBytes + 128 + 1024;
 }
+constexpr int kMlpGroups = 4;   // 128-thread groups per inference CTA
 constexpr size_t kMlpCtaSmem = mlp_cta_smem(kMlpGroups);
+static_assert(kMlpCtaSmem <= 232448, "inference CTA exceeds the 227 KB of shared memory");
 
 __device__ __forceinline__ uint8_t *align1024(uint8_t *p) {
   return reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(p) + 1023) & ~(uintptr_t)1023);
@@ -433,28 +388,21 @@ __device__ __forceinline__ uint8_t *align1024(uint8_t *p) {
 // mlp_cta_release).  Every thread of the CTA calls it.
 __device__ __forceinline__ uint32_t mlp_cta_setup(const MlpDev &M, uint8_t *base, MlpGroup &G,
                                                   int groups = kMlpGroups) {
-  const int nthr = 128 * groups, g = threadIdx.x >> 7;
-  uint8_t *w4 = base + (2 + groups) * kTileBytes;
-  float *fp = reinterpret_cast<float *>(w4 + kW4TileBytes);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(fp + 776);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(fp + 776 + 2 * 8);
+  const int nthr = 128 * groups, g = threadIdx.x >> 7, t = threadIdx.x & 127;
   {
-    const uint4 *s2 = reinterpret_cast<const uint4 *>(M.W2t), *s3 = reinterpret_cast<const uint4 *>(M.W3t);
-    uint4 *d2 = reinterpret_cast<uint4 *>(base), *d3 = reinterpret_cast<uint4 *>(base + kTileBytes);
+    const uint4 *s2 = reinterpret_cast<const uint4 *>(M.W2f), *s3 = reinterpret_cast<const uint4 *>(M.W3f);
+    uint4 *d2 = reinterpret_cast<uint4 *>(base + kSmemW2), *d3 = reinterpret_cast<uint4 *>(base + kSmemW3);
     for (int i = threadIdx.x; i < kTileBytes / 16; i += nthr) {
       d2[i] = s2[i];
       d3[i] = s3[i];
     }
-    const uint4 *s4 = reinterpret_cast<const uint4 *>(M.W4t);
-    for (int i = threadIdx.x; i < kW4TileBytes / 16; i += nthr) reinterpret_cast<uint4 *>(w4)[i] = s4[i];
+    const uint4 *se = reinterpret_cast<const uint4 *>(M.Ext);
+    for (int i = threadIdx.x; i < kExtBytes / 16; i += nthr) reinterpret_cast<uint4 *>(base + kSmemExt)[i] = se[i];
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(M.W4f);
+    for (int i = threadIdx.x; i < kW4Bytes / 16; i += nthr) reinterpret_cast<uint4 *>(base + kSmemW4)[i] = s4[i];
   }
-  for (int i = threadIdx.x; i < 384; i += nthr) fp[i] = M.P[kMlpW1 + i];
-  for (int i = threadIdx.x; i < 128; i += nthr) {
-    fp[384 + i] = M.P[kMlpB1 + i];
-    fp[512 + i] = M.P[kMlpB2 + i];
-    fp[640 + i] = M.P[kMlpB3 + i];
-  }
-  if (threadIdx.x < 2) fp[768 + threadIdx.x] = M.P[kMlpB4 + threadIdx.x];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(base + kSmemA + (size_t)groups * kTileBytes);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 8);
   if (threadIdx.x == 0) {
     for (int q = 0; q < groups; ++q) mbar_init(&bar[q], 1);
     fence_mbar_init();
@@ -467,15 +415,17 @@ __device__ __forceinline__ uint32_t mlp_cta_setup(const MlpDev &M, uint8_t *base
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  G.W1 = fp; G.B1 = fp + 384; G.B2 = fp + 512; G.B3 = fp + 640; G.B4 = fp + 768;
-  G.A = base + (2 + g) * kTileBytes;
+  G.A = base + kSmemA + (size_t)g * kTileBytes;
   G.bar = &bar[g];
-  G.aW2 = smem_u32(base);
-  G.aW3 = smem_u32(base + kTileBytes);
-  G.aW4 = smem_u32(w4);
+  G.aW2 = smem_u32(base + kSmemW2);
+  G.aW3 = smem_u32(base + kSmemW3);
+  G.aExt = smem_u32(base + kSmemExt);
+  G.aW4 = smem_u32(base + kSmemW4);
   G.aA = smem_u32(G.A);
   G.dcol = tmem + 128u * g;
   G.lane = (uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16;
+  G.row = (uint32_t)((t >> 3) * 1024 + (t & 7) * 128);
+  G.swz = t & 7;
   G.bar_id = 1 + g;
   G.phase = 0;
   return tmem;
@@ -487,58 +437,110 @@ __device__ __forceinline__ void mlp_cta_release(uint32_t tmem, int groups = kMlp
   if (threadIdx.x < 32) tmem_dealloc(tmem, 128 * groups);
 }
 
-// The network's input features and targets.
+// The network's input features.
 constexpr float kMlpLogR = 0.66761703f;   // 2 / ln 20: r = 0.05 -> -1, r = 1 -> 1
 __device__ __forceinline__ void mlp_features(float a, float b, float r, float *x) {
   x[0] = 0.25f * a - 1.0f;
   x[1] = 0.25f * b - 1.0f;
   x[2] = fmaf(kMlpLogR, logf(r), 1.0f);
 }
+
+// 8-point Gauss-Legendre rule on [0, 1]
 static __constant__ float kGl8X[8] = {0.019855071751231912f, 0.10166676129318664f, 0.2372337950418355f,
                                        0.40828267875217511f, 0.59171732124782483f, 0.7627662049581645f,
                                        0.89833323870681336f, 0.98014492824876809f};
 static __constant__ float kGl8W[8] = {0.050614268145188532f, 0.11119051722668721f, 0.15685332293894344f,
                                        0.18134189168918083f, 0.18134189168918083f, 0.15685332293894344f,
                                        0.11119051722668721f, 0.050614268145188532f};
-static __constant__ float kGl16Xf[16] = {
-    0.0052995325041750307f, 0.0277124884633837f, 0.067184398806084122f, 0.1222977958224985f,
-    0.19106187779867811f,   0.27099161117138632f, 0.35919822461037054f, 0.45249374508118129f,
-    0.54750625491881877f,   0.64080177538962946f, 0.72900838882861363f, 0.80893812220132189f,
-    0.87770220417750155f,   0.93281560119391593f, 0.9722875115366163f,  0.99470046749582497f};
-static __constant__ float kGl16Wf[16] = {
-    0.013576229705877088f, 0.031126761969323728f, 0.047579255841246303f, 0.062314485627767036f,
-    0.074797994408288354f, 0.084578259697501323f, 0.09130170752246182f,  0.09472530522753432f,
-    0.09472530522753432f,  0.09130170752246182f,  0.084578259697501323f, 0.074797994408288354f,
-    0.062314485627767036f, 0.047579255841246303f, 0.031126761969323728f, 0.013576229705877088f};
 
-// The envelopes Ex, Ey of the field's shape (FP32 with the hardware
-// reciprocal, exponential and reciprocal square root: the network learns
-// the residual of exactly this function, its training targets use it too).
-__device__ __forceinline__ void mlp_envelopes(float a, float b, float r, float &ex, float &ey) {
-  const float a2 = a * a, br2 = (b * r) * (b * r), q = 1.0f - r * r;
-  const float i1r = __fdividef(1.0f, 1.0f + r);
-  float sx = 0.0f;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const float u = fmaf(1.0f - r, kGl8X[i], r);
-    const float iu = __fdividef(1.0f, u);
-    const float t2 = (1.0f - kGl8X[i]) * (1.0f + u) * i1r;
-    sx = fmaf(kGl8W[i], __expf(-0.5f * t2 * fmaf(br2, iu * iu, a2)), sx);
-  }
-  ex = sx * i1r * 0.31830988618379067f;
-  const float smax = fminf(1.0f, __fdividef(80.0f, fmaxf(a2 + br2, 1e-30f)));
-  float sy = 0.0f;
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    const float sg = smax * kGl16Xf[i];
-    const float d = fmaf(-q, sg, 1.0f);
-    const float id = __fdividef(1.0f, d);
-    sy = fmaf(kGl16Wf[i] * id * rsqrtf(d), __expf(-0.5f * sg * fmaf(br2, id, a2)), sy);
-  }
-  ey = r * 0.5f * smax * sy * 0.31830988618379067f;
+__device__ __forceinline__ float ex2_hw(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rsqrt_hw(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_hw(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float lg2_hw(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
 }
 
-constexpr float kMlpResidualScale = 8.0f;   // Y = 8 (F / envelope - 1)
+constexpr float kEnvS1 = 0.5f;          // panel boundary in s
+constexpr float kEnvPhiC = 20.0f;       // panel 1 stops where Phi > 20 at D = 1
+constexpr float kEnvRswitch = 0.5f;     // panel 2 in v = D^-1/2 at and below this aspect ratio
+constexpr float kHalfLog2e = 0.72134752044448170f;   // log2(e) / 2
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kInv2Pi = 0.15915494309189535f;
+
+// One panel of the field integral in s on [s0, s0 + w]: sums of
+// e^-Phi D^-1/2 and e^-Phi D^-3/2 times the panel width.
+__device__ __forceinline__ void env_panel_s(float s0, float w, float q, float a2, float br2, float &ix, float &iy) {
+  float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const float s = fmaf(w, kGl8X[i], s0);
+    const float D = fmaf(-q, s, 1.0f);
+    const float rs = rsqrt_hw(D);
+    const float iD = rs * rs;
+    const float e = ex2_hw(-kHalfLog2e * s * fmaf(br2, iD, a2));
+    const float er = kGl8W[i] * e * rs;
+    sx += er;
+    sy = fmaf(er, iD, sy);
+  }
+  ix = w * sx;
+  iy = w * sy;
+}
+
+// The envelopes Ex = Fx / a, Ey = Fy / b of the field (FP32, hardware
+// reciprocal, square root, exponential and logarithm: the network learns
+// the residual of exactly this function, its training targets use it too).
+__device__ __forceinline__ void mlp_envelopes(float a, float b, float r, float &ex, float &ey) {
+  const float q = fmaf(-r, r, 1.0f);
+  const float a2 = a * a, br = b * r, br2 = br * br;
+  const float st = fminf(kEnvS1, 2.0f * kEnvPhiC * rcp_hw(fmaxf(a2 + br2, 1e-30f)));
+  float ix, iy;
+  env_panel_s(0.0f, st, q, a2, br2, ix, iy);
+  if (st >= kEnvS1) {   // the rest of [0, 1] is not negligible
+    float jx, jy;
+    if (r <= kEnvRswitch) {
+      // v = D^-1/2 from v1 (s = 1/2) to 1/r on a geometric map v = v1 (1/(r v1))^x:
+      // ds = 2 L v^-2 / q dx, D^-1/2 = v, D^-3/2 = v^3, L = ln(1 / (r v1))
+      const float v1 = rsqrt_hw(fmaf(-q, kEnvS1, 1.0f));
+      const float L2 = -lg2_hw(r * v1);   // log2(1 / (r v1))
+      const float iq = rcp_hw(q);
+      float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const float v = v1 * ex2_hw(L2 * kGl8X[i]);
+        const float v2 = v * v;
+        const float iv2 = rcp_hw(v2);
+        const float sv = (1.0f - iv2) * iq;
+        const float e = ex2_hw(-kHalfLog2e * sv * fmaf(br2, v2, a2));
+        const float ev = kGl8W[i] * e * v;
+        sx = fmaf(ev, iv2, sx);
+        sy += ev;
+      }
+      const float c = 2.0f * (L2 / kLog2e) * iq;
+      jx = c * sx;
+      jy = c * sy;
+    } else {
+      env_panel_s(kEnvS1, 1.0f - kEnvS1, q, a2, br2, jx, jy);
+    }
+    ix += jx;
+    iy += jy;
+  }
+  ex = ix * kInv2Pi;
+  ey = r * iy * kInv2Pi;
+}
 
 }  // namespace mbt
 
@@ -557,8 +559,8 @@ __device__ __forceinline__ bool mlp_group_field(MlpGroup &G, int t, bool active,
   const bool swap = sy > sx;
   const float ax = (float)fabs(swap ? dy : dx), ay = (float)fabs(swap ? dx : dy);
   const float s1 = (float)(swap ? sy : sx), s2 = (float)(swap ? sx : sy);
-  const float inv1 = 1.0f / s1;
-  const float a = ax * inv1, b = ay / s2, r = s2 * inv1;
+  const float inv1 = rcp_hw(s1);
+  const float a = ax * inv1, b = ay * rcp_hw(s2), r = s2 * inv1;
   in_domain = active && s2 > 0.0f && a < 8.0f && b < 8.0f && r >= 0.05f;
   float x[3], y[2];
   mlp_features(in_domain ? a : 0.0f, in_domain ? b : 0.0f, in_domain ? r : 1.0f, x);

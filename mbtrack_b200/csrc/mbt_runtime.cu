@@ -304,6 +304,9 @@ int sync_and_check(mbt_ctx *c) {
   if (rs.error & 2)
     return fail(c, MBT_ERR_TIMEOUT, "device error word %d: a bounded pipeline wait of the particle pass gave up",
                 rs.error);
+  if (rs.error & 4)
+    return fail(c, MBT_ERR_TIMEOUT,
+                "device error word %d: a bounded wait on the tensor cores of the learned field gave up", rs.error);
   if (rs.error) return fail(c, MBT_ERR_STATE, "device error word %d: injected deviates exhausted", rs.error);
   return 0;
 }
@@ -840,6 +843,7 @@ int mbt_enable_beam_ion(mbt_ctx *c, const mbt_beam_ion *cfg) {
   bi.trig = tr; bi.mom = mom; bi.frame = frame; bi.part = part; bi.cloud = cloud; bi.ib = ibd;
   bi.bunch_kb = c->a.bunch_kb;
   bi.turn = &c->a.rs->turn;
+  bi.error = &c->a.rs->error;
   c->a.bi_mom = mom;
   if (!c->bi_ev) CK(cudaEventCreate(&c->bi_ev));
   c->bicfg = *cfg;
@@ -1067,6 +1071,16 @@ int mbt_profile_turns(mbt_ctx *c, long nturns, double out[4]) {
   if (r) return r;
   for (int k = 0; k < 4; ++k) out[k] = acc[k] / nturns;
   c->bi_ms = acc_bi / nturns;
+  return 0;
+}
+
+int mbt_inject_device_error(mbt_ctx *c, int bits) {
+  if (!c || bits <= 0) return MBT_ERR_INVALID;
+  RingState rs;
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(&rs, c->a.rs, sizeof rs, cudaMemcpyDeviceToHost));
+  rs.error |= bits;
+  CK(cudaMemcpy(&c->a.rs->error, &rs.error, sizeof rs.error, cudaMemcpyHostToDevice));
   return 0;
 }
 

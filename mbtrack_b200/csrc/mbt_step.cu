@@ -190,36 +190,39 @@ extern "C" int mbt_bunch_moments_dev(int np, const double *coord_dev, double sig
 // one file-scope device array of fixed size instead of per-call memory.
 //
 // That array exists once on every GPU that loads this library and stays
-// allocated until the process exits.  Its device address is looked up once
-// per device (cudaGetSymbolAddress) by the first call made with that device
-// current; make that first call before any stream capture.  Every call uses
-// the same array and leaves its contents behind; each call writes every
-// element it later reads (partial records, then the result area), so nothing
-// has to be cleared.  Two calls whose work overlaps on the GPU (different
-// streams, or different host threads on one device) race on the array.
+// allocated until the process exits.  Every call looks up its device address
+// (cudaGetSymbolAddress, with the caller's device current: the address is
+// only valid there) and passes it to the kernels; a lookup allocates
+// nothing, and looking up on every call keeps the address right after a
+// cudaDeviceReset has reloaded the module.  The first call on a device also
+// loads the module's device code and data there, so make it before any
+// stream capture.  Every call uses the same array and leaves its contents
+// behind; each call writes every element it later reads (partial records,
+// then the result area), so nothing has to be cleared.  Two calls whose
+// work overlaps on the GPU (different streams, or different host threads on
+// one device) race on the array.
 
 namespace {
 
 constexpr size_t kNoAllocDoubles = 262144;      // 2 MiB
-constexpr int kNoAllocMaxDevices = 64;
 __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
-double *g_noalloc_addr[kNoAllocMaxDevices] = {};
+// the largest histogram (MBT_MAX_NCELL bins) fits: the result area and at
+// least one block record
+static_assert(MBT_NOALLOC_MAX_NCELL <= MBT_MAX_NCELL, "limit above the library's");
+static_assert(12 + 3 * (size_t)MBT_NOALLOC_MAX_NCELL + 12 + 3 * (size_t)MBT_NOALLOC_MAX_NCELL + kExtra <=
+                  kNoAllocDoubles,
+              "the scratch array cannot hold the largest histogram");
 
 int noalloc_scratch(double **out) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0)
     return mbt::fail_global(MBT_ERR_NODEVICE, "no CUDA device: libmbt has no CPU path");
-  if (dev >= kNoAllocMaxDevices)
-    return mbt::fail_global(MBT_ERR_INVALID, "device %d: the allocation-free path serves devices 0..%d", dev,
-                            kNoAllocMaxDevices - 1);
-  if (g_noalloc_addr[dev] == nullptr) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || p == nullptr)
-      return mbt::fail_global(MBT_ERR_CUDA, "cudaGetSymbolAddress of the scratch array: %s", cudaGetErrorString(e));
-    g_noalloc_addr[dev] = static_cast<double *>(p);
-  }
-  *out = g_noalloc_addr[dev];
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || p == nullptr)
+    return mbt::fail_global(MBT_ERR_CUDA, "cudaGetSymbolAddress of the scratch array on device %d: %s", dev,
+                            cudaGetErrorString(e));
+  *out = static_cast<double *>(p);
   return 0;
 }
 
@@ -228,20 +231,53 @@ int noalloc_scratch(double **out) {
 extern "C" int mbt_bunch_moments_dev_noalloc(int np, const double *coord_dev, double sigma_tau, double nsigma,
                                              double dT, int ncell, const int track_plane[3], double *stats,
                                              double *hist_dev, void *stream) {
+  // check_args rejects ncell above MBT_MAX_NCELL = MBT_NOALLOC_MAX_NCELL
   int r = check_args(np, coord_dev, sigma_tau, dT, ncell, track_plane, stats, hist_dev);
   if (r) return r;
-  if (ncell > MBT_NOALLOC_MAX_NCELL)
-    return mbt::fail_global(MBT_ERR_INVALID, "allocation-free bunch moments: ncell %d exceeds %d", ncell,
-                            MBT_NOALLOC_MAX_NCELL);
   double *scratch = nullptr;
   r = noalloc_scratch(&scratch);
   if (r) return r;
   const int prec = 3 * ncell + kExtra;
   const size_t result = 12 + 3 * (size_t)ncell + 12;
   const int fit = (int)((kNoAllocDoubles - result) / (size_t)prec);
-  const int nblk = std::min(blocks_for(np), fit);
-  if (nblk < 1)
-    return mbt::fail_global(MBT_ERR_INVALID, "allocation-free bunch moments: ncell %d does not fit the scratch", ncell);
+  const int nblk = std::min(blocks_for(np), fit);   // fit >= 1 (static_assert above)
   return run_moments(np, coord_dev, (size_t)np, sigma_tau, nsigma, dT, ncell, track_plane, stats, hist_dev,
                      (cudaStream_t)stream, scratch, nblk);
+}
+
+// ---------------------------------------------------------------------------
+// Self-test of the bounded waits: one thread waits on an mbarrier that no
+// thread arrives at, with the same helper (mbt::mbar_wait) and the same
+// give-up path as the kernels; the wait must end after `polls` polls.
+
+namespace {
+__global__ void bounded_wait_probe(long polls, int *gave_up) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbt::mbar_init(&bar, 1);
+    mbt::fence_mbar_init();
+    *gave_up = mbt::mbar_wait(&bar, 0u, polls) ? 0 : 1;
+  }
+}
+}  // namespace
+
+extern "C" int mbt_selftest_bounded_wait(long polls, void *stream) {
+  if (polls < 1 || polls > (1L << 24))
+    return mbt::fail_global(MBT_ERR_INVALID, "bounded wait self-test: polls %ld outside 1..2^24", polls);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return mbt::fail_global(MBT_ERR_NODEVICE, "no CUDA device: libmbt has no CPU path");
+  cudaStream_t st = (cudaStream_t)stream;
+  int *flag = nullptr;
+  if (cudaMalloc(&flag, sizeof(int)) != cudaSuccess)
+    return mbt::fail_global(MBT_ERR_NOMEM, "bounded wait self-test: flag");
+  int gave_up = -1;
+  bounded_wait_probe<<<1, 32, 0, st>>>(polls, flag);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&gave_up, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(flag);
+  if (e != cudaSuccess) return mbt::fail_global(MBT_ERR_CUDA, "bounded wait self-test: %s", cudaGetErrorString(e));
+  if (gave_up == 1) return mbt::fail_global(MBT_ERR_TIMEOUT, "bounded wait gave up after %ld polls", polls);
+  return 0;
 }

@@ -1,10 +1,11 @@
 /*
  * mlp_oracle.c -- TEST INFRASTRUCTURE ONLY: CPU restatement of the learned
  * field network of libmbt (mbt.h, mbt_mlp_*): forward pass and gradient
- * with the same roundings of the tensor-core operands (FP16 weights and
- * activations and FP16 GELU arithmetic in the forward pass, BF16 operands
- * of the backward products), sums in double.  Used by tests/ to check the
- * GPU kernels.
+ * with the same roundings of the tensor-core operands (BF16 pairs of the
+ * inputs and biases, BF16 weights, W/2 after a hidden layer, activations
+ * h' = 2 gelu(z) in BF16 pair arithmetic in the forward pass; BF16
+ * operands of the backward products), sums in double.  Used by tests/ to
+ * check the GPU kernels.
  */
 #include <math.h>
 #include <stdint.h>
@@ -34,35 +35,31 @@ static float bf16r(float v)
   return v;
 }
 
-/* round to the nearest FP16 (ties to even), as a float */
-static float h16(double v)
+/* round a double to the nearest BF16 value (ties to even), as a float */
+static float rbf(double v)
 {
   const double a = fabs(v);
   double q;
   int e;
-  if (!(a < 65520.0)) return a != a ? (float) v : (float) copysign(INFINITY, v);
-  if (a < 6.103515625e-05) {
-    q = 5.9604644775390625e-08;              /* subnormal step 2^-24 */
-  } else {
-    frexp(a, &e);                            /* a in [2^(e-1), 2^e) */
-    q = ldexp(1.0, e - 11);                  /* 11 significant bits */
-  }
+  if (a == 0.0 || a != a || a > 3.3e38) return (float) v;
+  frexp(a, &e);                              /* a in [2^(e-1), 2^e) */
+  q = ldexp(1.0, (e - 1 < -126 ? -126 : e - 1) - 7);   /* 8 significant bits */
   return (float) (nearbyint(v / q) * q);
 }
 
-/* GELU in FP16 pair arithmetic as the GPU evaluates it (gelu_h2): every
- * step rounded to FP16, FP16 constants; the GPU's tanh is the hardware
- * approximation, this restatement libm's tanh rounded to FP16. */
-static float gelu(float x)
+/* The activation of the forward pass (act_bf16x2): every step rounded to
+ * BF16, BF16 constants c1 = 0x3F4C, c1c2 = 0x3D12; the GPU's tanh is the
+ * hardware approximation, this restatement libm's tanh rounded to BF16.
+ * Returns h' = 2 gelu(z). */
+static float act(float x)
 {
-  const float c1c2 = 0.035675048828125f, c1 = 0.7978515625f;
-  const float z = h16(x);
-  const float t = h16((double) z * z);
-  const float p = h16((double) c1c2 * t + c1);
-  const float y = h16((double) z * p);
-  const float th = h16(tanh((double) y));
-  const float hz = h16(0.5 * z);
-  return h16((double) hz * th + hz);
+  const double c1 = 0.796875, c1c2 = 0.03564453125;
+  const double z = rbf(x);
+  const double t = rbf(z * z);
+  const double p = rbf(t * c1c2 + c1);
+  const double y = rbf(z * p);
+  const double th = rbf(tanh(y));
+  return rbf(z * th + z);
 }
 
 static float gelu_grad(float x)
@@ -77,37 +74,54 @@ typedef struct fwd_t {
   float x[3], z1[H], h1[H], z2[H], h2[H], z3[H], h3[H], out[2];
 } fwd_t;
 
+/* the BF16 pair (hi, lo) of a bias, summed */
+static double bias_pair(float b)
+{
+  const float hi = bf16r(b);
+  return (double) hi + (double) bf16r(b - hi);
+}
+
+/* One point: the saved activations are gelu(z) = h' / 2. */
 static void forward_one(const float *P, const float *abr, fwd_t *f)
 {
-  int j, k;
+  int i, j, k;
+  float xh[3], xl[3], h[H], hn[H];
   f->x[0] = 0.25f * abr[0] - 1.0f;
   f->x[1] = 0.25f * abr[1] - 1.0f;
   f->x[2] = fmaf(0.66761703f, logf(abr[2]), 1.0f);   /* 1 + 2 ln r / ln 20 */
-  for (j = 0; j < H; j++) {
-    float z = P[B1 + j];
-    z = fmaf(P[W1 + 3 * j], f->x[0], z);
-    z = fmaf(P[W1 + 3 * j + 1], f->x[1], z);
-    z = fmaf(P[W1 + 3 * j + 2], f->x[2], z);
-    f->z1[j] = z;
-    f->h1[j] = gelu(z);
-  }
-  /* the activations are FP16 values already; the weights round to FP16 */
-  for (j = 0; j < H; j++) {
-    double s = 0.0;
-    for (k = 0; k < H; k++) s += (double) f->h1[k] * (double) h16(P[W2 + H * j + k]);
-    f->z2[j] = (float) s + P[B2 + j];
-    f->h2[j] = gelu(f->z2[j]);
+  for (i = 0; i < 3; i++) {
+    xh[i] = bf16r(f->x[i]);
+    xl[i] = bf16r(f->x[i] - xh[i]);
   }
   for (j = 0; j < H; j++) {
-    double s = 0.0;
-    for (k = 0; k < H; k++) s += (double) f->h2[k] * (double) h16(P[W3 + H * j + k]);
-    f->z3[j] = (float) s + P[B3 + j];
-    f->h3[j] = gelu(f->z3[j]);
+    double s = bias_pair(P[B1 + j]);
+    for (i = 0; i < 3; i++) s += (double) bf16r(P[W1 + 3 * j + i]) * ((double) xh[i] + (double) xl[i]);
+    f->z1[j] = (float) s;
+    h[j] = act(f->z1[j]);
+    f->h1[j] = 0.5f * h[j];
+  }
+  for (j = 0; j < H; j++) {
+    double s = bias_pair(P[B2 + j]);
+    for (k = 0; k < H; k++) s += (double) h[k] * (double) bf16r(0.5f * P[W2 + H * j + k]);
+    f->z2[j] = (float) s;
+  }
+  for (j = 0; j < H; j++) {
+    hn[j] = act(f->z2[j]);
+    f->h2[j] = 0.5f * hn[j];
+  }
+  for (j = 0; j < H; j++) {
+    double s = bias_pair(P[B3 + j]);
+    for (k = 0; k < H; k++) s += (double) hn[k] * (double) bf16r(0.5f * P[W3 + H * j + k]);
+    f->z3[j] = (float) s;
+  }
+  for (j = 0; j < H; j++) {
+    h[j] = act(f->z3[j]);
+    f->h3[j] = 0.5f * h[j];
   }
   for (j = 0; j < 2; j++) {
-    double s = 0.0;
-    for (k = 0; k < H; k++) s += (double) f->h3[k] * (double) h16(P[W4 + H * j + k]);
-    f->out[j] = (float) s + P[B4 + j];
+    double s = bias_pair(P[B4 + j]);
+    for (k = 0; k < H; k++) s += (double) h[k] * (double) bf16r(0.5f * P[W4 + H * j + k]);
+    f->out[j] = (float) s;
   }
 }
 

@@ -53,6 +53,11 @@ WORKLOADS = {
     "beam_ion_mlp": ("beam_ion.conf", {}, "beam-ion weak-strong: 200-bunch train x 5e4 macroparticles, CO at "
                                           "1 nTorr, 20 interaction points, 1000 macro-ions per passage per "
                                           "point, learned field (tensor-core MLP, 1% audit)"),
+    "combined": ("combined.conf", {}, "combined: uneven fill (321 bunches incl. 5 nC camshaft, macroparticles "
+                                      "proportional to charge, 2e3..1e5, 8e6 in all), RW + HOM + RF feedback with a "
+                                      "generator loop (gain 10, one-turn delay), beam-ion (CO 1 nTorr, 20 points, 1000 "
+                                      "macro-ions per passage per point) with the learned field and a 1% audit, "
+                                      "quantum excitation on"),
     "slice_fbii": ("slice_fbii.conf", {"Nslc": 23, "Np": 5000, "Iring": 84.6, "NrevTot": 1000, "NrevMon": 100},
                    "slice model (BunchModel = STRONG) with fast beam-ion interaction: 200-bunch train, 47 "
                    "slices x 25 grid points per bunch (1175 macro-ions), long-range RW over 10 turns"),
@@ -68,7 +73,7 @@ def conf_path(workload, tmpdir):
     name, over, _ = WORKLOADS[workload]
     src = os.path.join(CONFS, name)
     over = dict(over)
-    if "uneven" in name:
+    if "uneven" in name or workload == "combined":
         over["filling"] = os.path.join(CONFS, "uneven_fill.txt")
     if "beam_ion" in name or workload == "slice_fbii":
         over["filling"] = os.path.join(CONFS, "beam_ion_fill.txt")
@@ -280,7 +285,7 @@ def run_b200(args):
                              "turn dropped" % (args.cpu_turns, info["scaled"], info["scaled"]))
 
     tiles = None
-    if args.workload == "uneven":
+    if args.workload in ("uneven", "combined"):
         # macroparticles proportional to the bunch charge, clamped to
         # 2e3 .. 1e5, about 8e6 in total
         frac = np.asarray(cfg.ib_frac, dtype=np.float64)
@@ -297,9 +302,9 @@ def run_b200(args):
         trk = api.Tracker.from_config(cfg, np_per_bunch=np_model, seed=1000 + rank)
     trk.generate_beam(77 + rank)
     bi_info = None
-    if args.workload.startswith("beam_ion"):
+    if args.workload.startswith("beam_ion") or args.workload == "combined":
         bi = cfg.beam_ion()
-        bi.surrogate = 1 if args.workload == "beam_ion_mlp" else 0
+        bi.surrogate = 1 if args.workload in ("beam_ion_mlp", "combined") else 0
         if args.n_ip:
             bi.n_ip = args.n_ip
         if args.ions_per_passage:
@@ -307,19 +312,19 @@ def run_b200(args):
         trk.enable_beam_ion(bi)
         bi_info = {"n_ip": bi.n_ip, "ions_per_passage": bi.ions_per_passage,
                    "field_evaluations_per_turn": bi.n_ip * (bi.ions_per_passage * cfg.nbunch * (cfg.nbunch - 1) // 2
-                                                            + np_model * (cfg.nbunch - 1))}
+                                                            + (npart - int(trk.np[0])))}
         if bi.surrogate:
             mlp = api.Mlp(seed=31 + rank)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            hist = mlp.train(nsamples=1 << 23, batch=8192, steps=args.mlp_steps, lr=2e-3, seed=32 + rank)
+            tr = dict(api.MLP_TRAIN, steps=args.mlp_steps or api.MLP_TRAIN["steps"])
+            hist = mlp.train(seed=32 + rank, **tr)
             torch.cuda.synchronize()
-            bi_info["training"] = {"seconds": time.perf_counter() - t0, "steps": args.mlp_steps, "batch": 8192,
-                                   "samples": 1 << 23, "final_loss": float(hist[-1])}
+            bi_info["training"] = dict(tr, seconds=time.perf_counter() - t0, final_loss=float(hist[-1]))
             trk.use_mlp(mlp)
-    trk.prepare()
-    if args.workload == "uneven":
-        tiles = [int(x) for x in trk.autotune(trial_turns=10)]   # its trial turns are warm-up turns
+    init_stats = trk.prepare()
+    if args.workload in ("uneven", "combined"):
+        tiles = [int(x) for x in trk.autotune(trial_turns=10 if args.workload == "uneven" else 2)]
     trk.run(args.warmup, stats=False)
     if bi_info is not None and bi_info.get("training"):
         trk.beam_ion_audit()   # reset the audit counters before the timed region
@@ -357,7 +362,9 @@ def run_b200(args):
             # network FLOPs: 2 x (3x128 + 2x128x128 + 128x2) per evaluation
             tfl = 66816.0 * bi_info["field_evaluations_per_turn"] / (bi_ms * 1e-3) / 1e12
             bi_info["network_tflops"] = tfl
-        if args.growth_turns > 0 and bi.surrogate:
+        if args.workload == "combined":
+            bi_info.update(combined_extras(args, cfg, trk, mlp, init_stats, tiles, tmp))
+        elif args.growth_turns > 0 and bi.surrogate:
             bi_info["growth_check"] = growth_check(cfg, mlp, args.growth_turns)
     peak, peak_kind = measured_peak()
     achieved = BYTES_PER_MP_TURN * npart / (k1_ms * 1e-3) / 1e9
@@ -420,6 +427,11 @@ def run_b200(args):
         line["config"]["tiles_chosen_by"] = "mbt_autotune (coordinate descent, 10 device-timed turns per candidate)"
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if args.workload == "uniform" and world == 1 and args.beam_ion_record:
+        # the north star's ratio: learned vs Faddeeva field on the beam-ion
+        # configuration, measured in the same run as the headline
+        line["beam_ion"] = beam_ion_record(args, tmp)
+        line["gpu_launches_beam_ion"] = 8 * (args.bi_steps + args.bi_warmup)
     print(json.dumps(line))
 
 
@@ -683,6 +695,126 @@ def run_slice_reference(args):
     print(json.dumps(line))
 
 
+def beam_ion_record(args, tmp):
+    """The beam-ion configuration at full size (200-bunch train x 5e4
+    macroparticles, CO at 1 nTorr, 20 interaction points, 1000 macro-ions per
+    passage per point), one run with the Faddeeva field and one with the
+    learned field (trained here): whole-turn device times and the ratio of
+    the two macroparticle-turns/s, the beam-ion stage's share, training
+    time, the audited field error, the growth-rate comparison."""
+    import numpy as np
+    import torch
+    from mbtrack_b200 import api
+    conf = conf_path("beam_ion", tmp)
+    cfg = api.Config(conf)
+    nb, npb = cfg.nbunch, cfg.params.np_model
+    bi0 = cfg.beam_ion()
+    evals = bi0.n_ip * (bi0.ions_per_passage * nb * (nb - 1) // 2 + npb * (nb - 1))
+    rec = {"workload": WORKLOADS["beam_ion"][2], "bunches": nb, "np_per_bunch": npb, "macroparticles": nb * npb,
+           "field_evaluations_per_turn": evals, "turns_timed": args.bi_steps, "turns_warmup": args.bi_warmup}
+    mlp = api.Mlp(seed=31)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = mlp.train(seed=32, **api.MLP_TRAIN)
+    torch.cuda.synchronize()
+    rec["training"] = dict(api.MLP_TRAIN, seconds=time.perf_counter() - t0, final_loss=float(hist[-1]),
+                           samples_from="the project's Faddeeva field (gauss_field, TOMS 680 w(z))")
+    runs = {}
+    for name, surr in (("faddeeva", 0), ("learned", 1)):
+        bi = cfg.beam_ion()
+        bi.surrogate = surr
+        trk = api.Tracker.from_config(cfg, seed=1000)
+        trk.generate_beam(77)
+        trk.enable_beam_ion(bi)
+        if surr:
+            trk.use_mlp(mlp)
+        trk.prepare()
+        trk.run(args.bi_warmup, stats=False)
+        if surr:
+            trk.beam_ion_audit()            # counters from the timed turns only
+        torch.cuda.synchronize()
+        with ClockSampler(0) as clk:
+            st = trk.run(args.bi_steps, stats=True)
+        torch.cuda.synchronize()
+        turn_ms = float(trk.timing()[0][3]) / args.bi_steps
+        r = {"ms_per_turn": turn_ms, "macroparticle_turns_per_s": nb * npb / (turn_ms * 1e-3),
+             "clocks": clk.summary(), "finite": bool(np.all(np.isfinite(st)))}
+        if surr:
+            a = trk.beam_ion_audit()
+            r["audit"] = {"audited": int(a[0]), "max_rel_error": float(a[1]), "rms_rel_error": float(a[2]),
+                          "faddeeva_fallbacks": int(a[3]), "tensor_failures": int(a[4]),
+                          "error": "|F_learned - F_Faddeeva| / |F_Faddeeva| of the field vector, a hashed 1% "
+                                   "of the warps each turn"}
+        trk.profile(2)
+        r["stage_ms_per_turn"] = trk.beam_ion_timing()
+        r["field_evaluations_per_s"] = evals / (r["stage_ms_per_turn"] * 1e-3)
+        trk.close()
+        runs[name] = r
+    rec.update(runs)
+    rec["surrogate_vs_plain"] = runs["faddeeva"]["ms_per_turn"] / runs["learned"]["ms_per_turn"]
+    rec["surrogate_vs_plain_meaning"] = ("whole-turn macroparticle-turns/s with the learned field over the same with "
+                                         "the Faddeeva field (device time, same beam, ions and seeds)")
+    # network arithmetic: 2 x (3x128 + 2x128x128 + 128x2) = 66816 FLOP per evaluation
+    rec["learned"]["network_tflops"] = 66816.0 * runs["learned"]["field_evaluations_per_s"] / 1e12
+    rec["faddeeva"]["fp64_pipe_active"] = {"value": 0.355, "from": "profiles/beam_ion_faddeeva.md (ncu, small case)"}
+    if args.growth_turns_bi > 0:
+        rec["growth_check"] = growth_check(cfg, mlp, args.growth_turns_bi)
+    mlp.close()
+    return rec
+
+
+def combined_extras(args, cfg, trk, mlp, init_stats, tiles, tmp):
+    """The combined workload's comparisons: the same fill, beam and seeds
+    with the Faddeeva field (whole-turn time ratio), and, with
+    --growth-turns N, N more turns of the learned-field run written through
+    the reference's writers (bunch-by-bunch centroid history among them)
+    with the transverse growth rates of the coherent motion."""
+    import numpy as np
+    import torch
+    from mbtrack_b200 import analysis, api
+    out = {}
+    npb = trk.np.copy()
+    bi = cfg.beam_ion()
+    bi.surrogate = 0
+    ref = api.Tracker(cfg.params, cfg.bucket, npb, cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh, seed=1000)
+    ref.generate_beam(77)
+    ref.enable_beam_ion(bi)
+    ref.prepare()
+    ref.set_tiles(tiles)
+    ref.run(2, stats=False)
+    torch.cuda.synchronize()
+    ref.run(args.plain_turns, stats=False)
+    plain_ms = float(ref.timing()[0][3]) / args.plain_turns
+    ref.close()
+    learned_ms = float(trk.timing()[0][3]) / args.steps
+    out["faddeeva_ms_per_turn"] = plain_ms
+    out["learned_ms_per_turn"] = learned_ms
+    out["surrogate_vs_plain"] = plain_ms / learned_ms
+    if args.growth_turns > 0:
+        work = os.path.join(tmp, "combined_work")
+        os.makedirs(work, exist_ok=True)
+        ocfg, bunch_out = cfg.output()
+        w = api.Writer(work, cfg.params, ocfg, bunch_out, cfg.bucket, cfg.bunch_currents())
+        w.wakes(cfg.Gl, cfg.Gv, cfg.Gh)
+        w.begin(init_stats)
+        trk.beam_ion_audit()
+        st, ai = trk.run_ampinv(args.growth_turns)
+        a = trk.beam_ion_audit()
+        w.turns(st, ai)
+        w.end(trk.get_stats())
+        w.close()
+        g = {"turns": args.growth_turns, "audit_max_rel_error": float(a[1]), "audit_rms_rel_error": float(a[2]),
+             "files": {f: os.path.getsize(os.path.join(work, f)) for f in sorted(os.listdir(work))}}
+        for plane in ("HOR", "VER"):
+            amp = analysis.centroid_amplitude(st, plane)
+            wdw = analysis.exponential_window(amp)
+            g[plane] = {"window": list(wdw) if wdw else None,
+                        "rate_per_turn": analysis.growth_rate(amp, wdw) if wdw else None,
+                        "amplitude_start": float(np.median(amp[:50])), "amplitude_end": float(amp[-1])}
+        out["growth"] = g
+    return out
+
+
 def growth_check(cfg, mlp, turns):
     """Growth rate of the vertical coupled-bunch motion with the Faddeeva
     and with the learned field, same train, ions and seeds: the beam-ion
@@ -732,7 +864,16 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-turns", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--mlp-steps", type=int, default=48000, help="training steps of the learned field")
+    ap.add_argument("--mlp-steps", type=int, default=0,
+                    help="training steps of the learned field (0: the library's standard settings)")
+    ap.add_argument("--beam-ion-record", type=int, default=1,
+                    help="uniform workload at 1 GPU: add the beam-ion record (learned vs Faddeeva field; 0: skip)")
+    ap.add_argument("--bi-steps", type=int, default=5, help="timed turns of each beam-ion run of the record")
+    ap.add_argument("--bi-warmup", type=int, default=3, help="warm-up turns of each beam-ion run of the record")
+    ap.add_argument("--growth-turns-bi", type=int, default=450,
+                    help="turns of the growth-rate comparison in the beam-ion record (0: skip)")
+    ap.add_argument("--plain-turns", type=int, default=3,
+                    help="combined workload: timed turns of the Faddeeva-field comparison run")
     ap.add_argument("--np-per-bunch", type=int, default=0,
                     help="macroparticles per bunch in place of the workload's (small cases for profiling)")
     ap.add_argument("--n-ip", type=int, default=0, help="beam-ion workloads: interaction points (small cases)")
@@ -744,7 +885,7 @@ def main():
                          "slice model's growth rate with the per-particle stage's (0: skip)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = 20 if args.workload.startswith("beam_ion") or args.workload == "slice_fbii" else 200
+        args.steps = 20 if args.workload.startswith("beam_ion") or args.workload in ("slice_fbii", "combined") else 200
     if args.workload.startswith("beam_ion"):
         args.cpu_turns = min(args.cpu_turns, 2)
     if args.warmup < 3:

@@ -143,6 +143,16 @@ typedef struct mbt_params {
   int    rffb_len;       /* averaging length (absolute value) */
   int    rffb_off_after_init; /* negative averaging_length: correct once, then off */
   double rffb_vrf_design, rffb_phi0_design;
+  /* Generator loop (extension, no counterpart in the reference; [rf_feedback]
+   * keys generator_gain, loop_delay): with gain G > 0 the generator phasor
+   * V_g = Vrf0 e^{i phai0} follows the reference's full correction V_f (the
+   * phasor its feedback sets every turn) through a loop of gain G and a delay
+   * of loop_delay turns (0 or 1):
+   *   V_g(n) = V_g(n-1) + G/(1+G) (V_f(n - delay) - V_g(n-1)),
+   * after the reference's full correction at set-up.  G = 0 (the default)
+   * is the reference's feedback. */
+  double rffb_gain;
+  int    rffb_delay;
 } mbt_params;
 
 typedef struct mbt_ctx mbt_ctx;
@@ -481,9 +491,9 @@ int mbt_beam_ion_use_mlp(mbt_ctx *ctx, mbt_mlp *m);
 
 /* Audit of the learned field since the last call (counters reset):
  * out[0] audited evaluations, out[1] largest and out[2] rms relative error
- * of a field component against the Faddeeva field, out[3] evaluations
- * outside the network's domain (Faddeeva fallback), out[4] tensor-core
- * failures. */
+ * of the field vector, |F_net - F| / |F| against the Faddeeva field F,
+ * out[3] evaluations outside the network's domain (Faddeeva fallback),
+ * out[4] tensor-core failures. */
 int mbt_beam_ion_audit(mbt_ctx *ctx, double out[5]);
 
 /* Average device time [ms] of the beam-ion stage per turn in the last

@@ -63,7 +63,7 @@ class MbtParams(ctypes.Structure):
         ("lr_init_turns", _i),
         ("rffb", _i), ("rffb_resonator", _i), ("rffb_len", _i),
         ("rffb_off_after_init", _i),
-        ("rffb_vrf_design", _d), ("rffb_phi0_design", _d),
+        ("rffb_vrf_design", _d), ("rffb_phi0_design", _d), ("rffb_gain", _d), ("rffb_delay", _i),
     ]
 
     def copy(self):

@@ -544,6 +544,13 @@ def _gchk(rc):
         raise MbtError(rc, buf.value.decode(errors="replace"))
 
 
+# Training settings of the learned field for the beam-ion runs (bench.py and
+# the tests of the field-error and growth-rate tolerances): 1e7 seeded
+# samples labelled by the Faddeeva field, minibatches of 8192, Adam at 2e-3
+# with cosine decay.
+MLP_TRAIN = {"nsamples": 10_000_000, "batch": 8192, "steps": 20000, "lr": 2e-3}
+
+
 class Mlp:
     """The learned field network (mbt_mlp_*).  Device arrays are passed as
     integer addresses (e.g. torch tensors' data_ptr())."""

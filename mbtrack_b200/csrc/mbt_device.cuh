@@ -78,6 +78,7 @@ struct RingState {
   int rffb_on;
   int rffb_count;
   int rw_m;            // resistive-wall trigger counter (worker_weakweak.c:254)
+  double rffb_full_prev[2];   // generator loop: last turn's full-correction phasor (cos, sin parts)
   int error;           // sticky device error word (0 = ok): 1 injected deviates exhausted, 2 a
                        // particle-pass pipeline wait gave up, 4 a learned-field tensor-core wait gave up
   int trash_low, trash_high;
@@ -158,6 +159,8 @@ struct Args {
   int rffb_off_after_init;
   double *rffb_hist;          // len x 2
   double rffb_vrf_design, rffb_phi0_design;
+  double rffb_kappa;          // generator loop: G / (1 + G) (0: the reference's full correction)
+  int rffb_delay;             // generator loop delay [turns], 0 or 1
   double E0;
   // noise
   int noise;                  // MBT_NOISE_PHILOX / _INJECTED / NONE

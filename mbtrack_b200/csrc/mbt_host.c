@@ -472,6 +472,14 @@ static int read_conf(const char *path, int fix_rw_beff, int allow_strong, cfg_t 
     p->rffb = 1;
     REQ_I("rf_feedback", "resonator", &p->rffb_resonator);
     REQ_I("rf_feedback", "averaging_length", &g->rffb_len_raw);
+    /* extension: the generator loop (mbt_params.rffb_gain / rffb_delay) */
+    p->rffb_delay = 1;
+    get_double(&C, "rf_feedback", "generator_gain", &p->rffb_gain);
+    get_int(&C, "rf_feedback", "loop_delay", &p->rffb_delay);
+    if (!(p->rffb_gain >= 0.0) || p->rffb_delay < 0 || p->rffb_delay > 1) {
+      r = cfg_fail("[rf_feedback]: generator_gain must be >= 0 and loop_delay 0 or 1");
+      goto out;
+    }
   }
   /* [active_HC_N] */
   for (i = 1; ; i++) {

@@ -838,9 +838,25 @@ __global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init
       const double phibar = ps / a.rffb_len;
       vmbar = vmbar * a.E0 * 1.0e3;
       const double tmp = a.rffb_vrf_design * sin(a.rffb_phi0_design) - vmbar * sin(phibar);
-      const double ph = atan2(tmp, a.rffb_vrf_design * cos(a.rffb_phi0_design) - vmbar * cos(phibar));
+      const double den = a.rffb_vrf_design * cos(a.rffb_phi0_design) - vmbar * cos(phibar);
+      double ph, vrf;
+      if (a.rffb_kappa > 0.0 && !init) {
+        // generator loop: follow the full correction (den, tmp), of this
+        // turn or the last, by the fraction kappa of the difference
+        const double fc = a.rffb_delay ? rs->rffb_full_prev[0] : den;
+        const double fs = a.rffb_delay ? rs->rffb_full_prev[1] : tmp;
+        const double gc = rs->Vrf0 * rs->cos_phai0, gs = rs->Vrf0 * rs->sin_phai0;
+        const double nc = gc + a.rffb_kappa * (fc - gc), ns = gs + a.rffb_kappa * (fs - gs);
+        ph = atan2(ns, nc);
+        vrf = ns / sin(ph);
+      } else {
+        ph = atan2(tmp, den);
+        vrf = tmp / sin(ph);
+      }
+      rs->rffb_full_prev[0] = den;
+      rs->rffb_full_prev[1] = tmp;
       rs->phai0 = ph;
-      rs->Vrf0 = tmp / sin(ph);
+      rs->Vrf0 = vrf;
       rs->sin_phai0 = sin(ph);
       rs->cos_phai0 = cos(ph);
       if (init && a.rffb_off_after_init) rs->rffb_on = 0;

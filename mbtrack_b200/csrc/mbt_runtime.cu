@@ -600,6 +600,8 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   a.rffb_off_after_init = p->rffb_off_after_init;
   a.rffb_vrf_design = p->rffb_vrf_design;
   a.rffb_phi0_design = p->rffb_phi0_design;
+  a.rffb_kappa = p->rffb_gain > 0.0 ? p->rffb_gain / (1.0 + p->rffb_gain) : 0.0;
+  a.rffb_delay = p->rffb_delay;
   rc = rc ? rc : dalloc(c, &a.rffb_hist, (size_t)2 * std::max(a.rffb_len, 1));
   rc = rc ? rc : dalloc(c, &a.rs, 1);
   rc = rc ? rc : dalloc(c, &c->xfer, (size_t)6 * c->npad);

@@ -15,6 +15,13 @@
  *   --seed N        key of the counter-based quantum-excitation noise
  *                   (default: iseed_LON)
  *   --device N      CUDA device (default 0)
+ *   --np-by-charge MIN:MAX:TOTAL   macroparticles of each bunch proportional
+ *                   to its charge, clamped to [MIN, MAX], about TOTAL in all
+ *                   (the reference has one Np for every bunch)
+ *   --train-steps N training steps of the learned field (default 20000)
+ * A [beam_ion] section (mbt_config_beam_ion) adds the per-macroparticle
+ * beam-ion stage; with surrogate = 1 the learned field is trained first
+ * (1e7 samples of the Faddeeva field) and its audit is printed at the end.
  * The initial distribution is the reference's (same generator, same seeds).
  * The quantum-excitation noise is a Philox stream instead of glibc rand():
  * with EnableQuantum = 0 the run reproduces the reference's numbers, with
@@ -22,6 +29,7 @@
  */
 #define _DEFAULT_SOURCE
 #include <pthread.h>
+#include <math.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -186,10 +194,39 @@ static int run_strong(const char *conf, const char *work, int own_ampinv)
   return 0;
 }
 
+/* macroparticles proportional to the bunch charge, clamped to [lo, hi],
+ * summing to about `total` (bisection on the proportionality factor) */
+static int set_np_by_charge(int nb, const double *frac, long lo, long hi, long total, int *np)
+{
+  double k0 = 1e-6, k1 = 1e15, k, fsum = 0.0;
+  int i, it;
+  for (i = 0; i < nb; i++) fsum += frac[i];
+  if (!(fsum > 0.0)) return -1;
+  for (it = 0; it < 200; it++) {
+    double sum = 0.0;
+    k = sqrt(k0 * k1);
+    for (i = 0; i < nb; i++) {
+      double n = floor(k * frac[i] + 0.5);
+      sum += n < lo ? lo : n > hi ? hi : n;
+    }
+    if (sum < (double) total) k0 = k; else k1 = k;
+  }
+  k = sqrt(k0 * k1);
+  for (i = 0; i < nb; i++) {
+    double n = floor(k * frac[i] + 0.5);
+    np[i] = (int) (n < lo ? lo : n > hi ? hi : n);
+  }
+  return 0;
+}
+
 int main(int argc, char **argv)
 {
   const char *conf = NULL, *work = "work/";
-  int own_ampinv = 0, device = 0, have_seed = 0, npos = 0, i, r, nb = 0;
+  int own_ampinv = 0, device = 0, have_seed = 0, npos = 0, i, r, nb = 0, train_steps = 20000;
+  long np_min = 0, np_max = 0, np_total = 0;
+  mbt_beam_ion bi;
+  mbt_mlp *mlp = NULL;
+  int bi_on = 0;
   unsigned long long seed = 0;
   mbt_params p;
   mbt_output_cfg o;
@@ -208,12 +245,21 @@ int main(int argc, char **argv)
     if (strcmp(argv[i], "--own-ampinv") == 0) own_ampinv = 1;
     else if (strcmp(argv[i], "--seed") == 0 && i + 1 < argc) { seed = strtoull(argv[++i], NULL, 0); have_seed = 1; }
     else if (strcmp(argv[i], "--device") == 0 && i + 1 < argc) device = atoi(argv[++i]);
+    else if (strcmp(argv[i], "--train-steps") == 0 && i + 1 < argc) train_steps = atoi(argv[++i]);
+    else if (strcmp(argv[i], "--np-by-charge") == 0 && i + 1 < argc) {
+      if (sscanf(argv[++i], "%ld:%ld:%ld", &np_min, &np_max, &np_total) != 3 || np_min < 1 || np_max < np_min ||
+          np_total < 1) {
+        fprintf(stderr, "ERROR: --np-by-charge MIN:MAX:TOTAL\n");
+        return -1;
+      }
+    }
     else if (npos == 0) { conf = argv[i]; npos++; }
     else if (npos == 1) { work = argv[i]; npos++; }
     else npos = 3;
   }
   if (npos < 1 || npos > 2) {
-    fprintf(stderr, "ERROR ! \n\nUsage:\nmbtrack-gpu inputfile.conf [/path/to/work] [--own-ampinv] [--seed N] [--device N]\n");
+    fprintf(stderr, "ERROR ! \n\nUsage:\nmbtrack-gpu inputfile.conf [/path/to/work] [--own-ampinv] [--seed N] [--device N]"
+                    " [--np-by-charge MIN:MAX:TOTAL] [--train-steps N]\n");
     return -1;
   }
   if (mbt_use_device(device) != 0) {
@@ -258,8 +304,12 @@ int main(int argc, char **argv)
   for (i = 0; i < nb; i++) {
     np[i] = p.np_model;                              /* manager_weakweak.c:61 */
     ib[i] = mbt_bunch_current(&p, nb, frac[i]);     /* manager_weakweak.c:74-75 */
-    nbeam += (size_t) 6 * np[i];
   }
+  if (np_total > 0 && set_np_by_charge(nb, frac, np_min, np_max, np_total, np) != 0) {
+    fprintf(stderr, "ERROR: --np-by-charge: no bunch charge\n");
+    return -1;
+  }
+  for (i = 0; i < nb; i++) nbeam += (size_t) 6 * np[i];
   beam = (double *) malloc(nbeam * sizeof(double));
   if (!beam) { fprintf(stderr, "ERROR: out of host memory for %zu coordinates\n", nbeam); return -1; }
   if ((r = reference_beam_all(&p, nb, bucket, np, beam)) != 0) {
@@ -273,6 +323,24 @@ int main(int argc, char **argv)
     return -1;
   }
   if (mbt_load_all(ctx, beam) != 0) { ctx_error(ctx, "loading the beam"); return -1; }
+
+  /* the beam-ion stage (an extension of the weak-weak model) */
+  r = mbt_config_beam_ion(conf, &bi);
+  if (r < 0) { fprintf(stderr, "ERROR: [beam_ion]: %s\n", mbt_config_error()); return -1; }
+  if (r == 0) {
+    bi_on = 1;
+    if (mbt_enable_beam_ion(ctx, &bi) != 0) { ctx_error(ctx, "mbt_enable_beam_ion"); return -1; }
+    if (bi.surrogate) {
+      printf("Training the learned beam-ion field (%d steps)...\n", train_steps);
+      fflush(stdout);
+      if (mbt_mlp_create(seed ^ 0x6D6C70ull, &mlp) != 0 ||
+          mbt_mlp_train(mlp, 10000000L, 8192, train_steps, 2e-3f, seed + 1, NULL) != 0 ||
+          mbt_beam_ion_use_mlp(ctx, mlp) != 0) {
+        ctx_error(ctx, "learned field");
+        return -1;
+      }
+    }
+  }
 
   /* the output bunches */
   watch = (int *) calloc(nb, sizeof(int));
@@ -348,8 +416,15 @@ int main(int argc, char **argv)
              st.n_trash_low, st.n_trash_high);
     if (p.rffb && nwatch > 0) printf("\nFinal RF voltage and phase: %.7f MV, %.5f\n", st.Vrf0, st.phai0);
   }
+  if (bi_on && bi.surrogate) {
+    double a[5];
+    if (mbt_beam_ion_audit(ctx, a) == 0)
+      printf("\nLearned field audit: %.0f evaluations, max relative field error %.3e, rms %.3e, %.0f outside "
+             "the domain, %.0f tensor-core failures\n", a[0], a[1], a[2], a[3], a[4]);
+  }
   mbt_writer_close(w);
   mbt_destroy(ctx);
+  if (mlp) mbt_mlp_destroy(mlp);
   free(bucket); free(frac); free(bunch_out); free(np); free(ib); free(Gl); free(Gv); free(Gh);
   free(beam); free(init_stats); free(stats); free(ampinv); free(pot); free(watch);
   return 0;

@@ -53,6 +53,7 @@ typedef struct orc_bunch {
   int rffb_on;
   double *rffb_hist;     /* [len][2] */
   int rffb_count;
+  double rffb_full_prev[2];   /* generator loop: last full-correction phasor */
   double phasor[3][MBT_MAX_LR][2];
   int m;                 /* RW trigger counter */
   int trash_low, trash_high;
@@ -428,8 +429,12 @@ static void rffb_sample(const mbt_params *p, orc_bunch *b, double vreal, double 
 }
 
 /* rffb_calc_mean_voltage_phase feedback_rf.c:22-34 followed by the
- * correction of worker_weakweak.c:268-278 (and :149-162 at set-up). */
-static void rffb_correct(const mbt_params *p, orc_bunch *b)
+ * correction of worker_weakweak.c:268-278 (and :149-162 at set-up, init).
+ * With p->rffb_gain > 0 (an extension, no reference counterpart) the
+ * generator phasor Vrf0 e^{i phai0} moves towards the full correction of
+ * this turn (rffb_delay 0) or the last (1) by G / (1 + G) of the
+ * difference; the set-up correction is the full one. */
+static void rffb_correct(const mbt_params *p, orc_bunch *b, int init)
 {
   double vrf_sum = 0, phi_sum = 0, vmbar, phibar;
   int m;
@@ -441,7 +446,22 @@ static void rffb_correct(const mbt_params *p, orc_bunch *b)
   phibar = phi_sum / p->rffb_len;
   vmbar = vmbar * p->E0 * FKILO;
   double tmp_numrtor = p->rffb_vrf_design * sin(p->rffb_phi0_design) - vmbar * sin(phibar);
-  b->phai0 = atan2(tmp_numrtor, p->rffb_vrf_design * cos(p->rffb_phi0_design) - vmbar * cos(phibar));
+  double den = p->rffb_vrf_design * cos(p->rffb_phi0_design) - vmbar * cos(phibar);
+  if (p->rffb_gain > 0.0 && !init) {
+    const double kappa = p->rffb_gain / (1.0 + p->rffb_gain);
+    const double fc = p->rffb_delay ? b->rffb_full_prev[0] : den;
+    const double fs = p->rffb_delay ? b->rffb_full_prev[1] : tmp_numrtor;
+    const double gc = b->Vrf0 * cos(b->phai0), gs = b->Vrf0 * sin(b->phai0);
+    const double nc = gc + kappa * (fc - gc), ns = gs + kappa * (fs - gs);
+    b->rffb_full_prev[0] = den;
+    b->rffb_full_prev[1] = tmp_numrtor;
+    b->phai0 = atan2(ns, nc);
+    b->Vrf0 = ns / sin(b->phai0);
+    return;
+  }
+  b->rffb_full_prev[0] = den;
+  b->rffb_full_prev[1] = tmp_numrtor;
+  b->phai0 = atan2(tmp_numrtor, den);
   b->Vrf0 = tmp_numrtor / sin(b->phai0);
 }
 
@@ -727,7 +747,7 @@ int orc_prepare(orc_ctx *o, double *init_stats)
       if (!IN_RANGE(o, ib)) continue;
       wake_phasor_init(o, b, LON);
       if (b->rffb_on) {
-        rffb_correct(p, b);
+        rffb_correct(p, b, 1);
         if (p->rffb_off_after_init) b->rffb_on = 0;
       }
     }
@@ -1012,7 +1032,7 @@ long orc_run(orc_ctx *o, long nturns, double *stats, const float *dev_in,
     if (p->ncell > 0 && p->planeL + p->planeV + p->planeH + lr_tot > 0)
       for (ib = o->lo; ib < o->hi && ib < o->nb; ib++) selffield(o, &o->b[ib]);
     for (ib = o->lo; ib < o->hi && ib < o->nb; ib++)
-      if (o->b[ib].rffb_on) rffb_correct(p, &o->b[ib]);
+      if (o->b[ib].rffb_on) rffb_correct(p, &o->b[ib], 0);
     for (ib = 0; ib < o->nb; ib++) {
       orc_bunch *b = &o->b[ib];
       if (!IN_RANGE(o, ib)) continue;

@@ -27,3 +27,15 @@ def cuda_device():
     if not torch.cuda.is_available():
         pytest.fail("GPU test selected but no CUDA device is visible")
     return torch.device("cuda:0")
+
+
+@pytest.fixture(scope="session")
+def trained_mlp(cuda_device):
+    """The learned field trained once per session with the library's
+    standard settings (api.MLP_TRAIN: 1e7 samples of the Faddeeva field),
+    as bench.py trains it; returns (network, loss history)."""
+    from mbtrack_b200 import api
+    m = api.Mlp(seed=31)
+    hist = m.train(seed=32, **api.MLP_TRAIN)
+    yield m, hist
+    m.close()

@@ -74,16 +74,16 @@ def test_beam_ion_turns_match_oracle(tmp_path, cuda_device, n_ip, ions, pressure
     assert np.abs(co[..., 0]).max() > 0
 
 
-def test_surrogate_stage_tracks_the_faddeeva_stage(tmp_path, cuda_device):
-    """The beam-ion stage with the learned field (trained here on the
-    project's own Faddeeva field) follows the Faddeeva stage: same clouds
-    and centroids to the network's accuracy, audited errors reported, the
-    out-of-domain evaluations handed to the Faddeeva field."""
+def test_surrogate_stage_tracks_the_faddeeva_stage(tmp_path, cuda_device, trained_mlp):
+    """The beam-ion stage with the learned field (trained with the standard
+    settings on the project's own Faddeeva field) follows the Faddeeva
+    stage: the audited relative field error |F_net - F| / |F| stays within
+    the north star's 1e-4 at its maximum, the clouds and centroids agree to
+    that level, the out-of-domain evaluations go to the Faddeeva field and
+    no tensor-core wait fails."""
+    mlp, _ = trained_mlp
     conf = small_conf(tmp_path, "beam_ion.conf", Np=2000, filling="SINGLE10", xxCM_offset=0.3, zzCM_offset=0.5)
     C = api.Config(conf)
-    mlp = api.Mlp(seed=21)
-    hist = mlp.train(nsamples=1 << 21, batch=8192, steps=3000, lr=2e-3, seed=22)
-    assert hist[-1] < 1e-3
     runs = {}
     for surr in (0, 1):
         bi = C.beam_ion()
@@ -98,17 +98,18 @@ def test_surrogate_stage_tracks_the_faddeeva_stage(tmp_path, cuda_device):
         runs[surr] = (t.run(8), t.beam_ion_clouds(), t.beam_ion_audit() if surr else None)
     (s0, c0, _), (s1, c1, audit) = runs[0], runs[1]
     n_audit, max_err, rms_err, fallbacks, failures = audit
+    print("audit: %d evaluations, max %.2e, rms %.2e, %d fallbacks" % (n_audit, max_err, rms_err, fallbacks))
     assert failures == 0
-    assert n_audit > 1000 and max_err < 0.05 and rms_err < 5e-3, audit
+    assert n_audit > 1000 and max_err <= 1e-4 and rms_err <= 1e-5, audit
     # centroids (relative to the rms size) and clouds agree to the field error
-    assert stats_err(s1, s0).max() < 5e-3
+    assert stats_err(s1, s0).max() < 1e-5
     rel = np.abs(c1[..., 0] - c0[..., 0]).max() / np.abs(c0[..., 0]).max()
     assert rel < 1e-12      # ion counts do not depend on the field
     for m in (1, 2, 3, 4):
-        assert np.abs(c1[..., m] - c0[..., m]).max() <= 1e-2 * np.abs(c0[..., 3:]).max(), m
+        assert np.abs(c1[..., m] - c0[..., m]).max() <= 1e-5 * np.abs(c0[..., 3:]).max(), m
 
 
-def test_surrogate_growth_rate_within_one_percent(tmp_path, cuda_device):
+def test_surrogate_growth_rate_within_one_percent(tmp_path, cuda_device, trained_mlp):
     """The vertical beam-ion instability grows at the same rate with the
     learned field as with the Faddeeva field (within 1 %): the 200-bunch
     train with 5e3 macroparticles per bunch, 4 interaction points at
@@ -116,8 +117,7 @@ def test_surrogate_growth_rate_within_one_percent(tmp_path, cuda_device):
     seeds; the rate is fitted over the exponential rise of the rms bunch
     centroid (mbtrack_b200.analysis)."""
     from mbtrack_b200 import analysis
-    mlp = api.Mlp(seed=31)
-    mlp.train(nsamples=1 << 23, batch=8192, steps=24000, lr=2e-3, seed=32)
+    mlp, _ = trained_mlp
     amp = {}
     for surr in (0, 1):
         C = api.Config(small_conf(tmp_path, "beam_ion.conf", Np=5000))
@@ -130,6 +130,9 @@ def test_surrogate_growth_rate_within_one_percent(tmp_path, cuda_device):
             t.use_mlp(mlp)
         t.prepare()
         amp[surr] = analysis.centroid_amplitude(t.run(450), "VER")
+        if surr:
+            a = t.beam_ion_audit()
+            assert a[4] == 0 and a[1] <= 1e-4, a
         t.close()
     w = analysis.exponential_window(amp[0])
     assert w is not None and w[1] - w[0] >= 50, w

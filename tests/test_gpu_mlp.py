@@ -1,6 +1,7 @@
 """The learned field network on a B200: tensor-core forward pass and
 gradient against the CPU restatement (oracle/mlp_oracle.c, same operand
-roundings), and training on the project's own Faddeeva-based field."""
+roundings), and the trained network against the Faddeeva field with the
+north star's tolerance (1e-4 relative field error)."""
 import numpy as np
 import pytest
 import torch
@@ -39,12 +40,13 @@ def test_forward_matches_oracle(cuda_device):
     m.forward_dev(len(x), xd.data_ptr(), out.data_ptr())
     ref = binding.mlp_forward(p, x)
     got = out.cpu().numpy()
-    # the GPU's GELU uses the hardware tanh (relative error < 2^-10.987),
-    # the oracle libm's tanhf; the BF16 rounding of an activation may then
-    # land on the other side of a tie: differences of a few 1e-3 of scale
+    # BF16 activations keep 8 significant bits; the GPU's hardware tanh and
+    # the oracle's libm tanh can round to neighbouring BF16 values, and such
+    # a difference of 2^-8 in one activation propagates: a few 1e-3 of the
+    # output scale at most
     scale = np.abs(ref).max()
-    assert np.max(np.abs(got - ref)) <= 5e-3 * scale, np.max(np.abs(got - ref)) / scale
-    assert np.median(np.abs(got - ref)) <= 5e-4 * scale
+    assert np.max(np.abs(got - ref)) <= 1e-2 * scale, np.max(np.abs(got - ref)) / scale
+    assert np.median(np.abs(got - ref)) <= 2e-3 * scale
 
 
 def test_gradient_matches_oracle(cuda_device):
@@ -62,25 +64,49 @@ def test_gradient_matches_oracle(cuda_device):
         assert np.linalg.norm(g[lo:hi] - gr[lo:hi]) <= 2e-2 * norm, (name, np.linalg.norm(g[lo:hi] - gr[lo:hi]) / norm)
 
 
-def test_training_reduces_the_loss(cuda_device):
-    """Training on the GPU; what the trained network gains over the method
-    without it: the envelopes alone (network output 0) miss the field by up
-    to ~14 %, the trained network by well under 1 %."""
-    m = api.Mlp(seed=10)
-    hist = m.train(nsamples=1 << 21, batch=8192, steps=2000, lr=2e-3, seed=11)
-    assert np.all(np.isfinite(hist))
-    assert hist[-50:].mean() < 0.1 * hist[:5].mean(), (hist[:5], hist[-50:])
-    # held-out points: targets from the Faddeeva-based field
-    x = inputs(20000, 12)
-    xd = torch.as_tensor(x, device="cuda")
-    tgt = torch.zeros((len(x), 2), dtype=torch.float32, device="cuda")
-    api.mlp_targets_dev(len(x), xd.data_ptr(), tgt.data_ptr())
-    out = torch.zeros_like(tgt)
-    m.forward_dev(len(x), xd.data_ptr(), out.data_ptr())
-    # relative field error = |Y - target| / (8 + target)
-    rel = ((out - tgt).abs() / (8.0 + tgt)).cpu().numpy()
-    rel0 = (tgt.abs() / (8.0 + tgt)).cpu().numpy()      # the envelopes alone
-    print("held-out relative field error: median %.2e p99 %.2e max %.2e; envelopes alone max %.2e"
-          % (np.median(rel), np.percentile(rel, 99), rel.max(), rel0.max()))
-    assert np.median(rel) < 2e-4 and np.percentile(rel, 99) < 5e-3
-    assert rel0.max() > 0.05 and rel.max() < 0.5 * rel0.max()
+def field_points(n, seed, kind):
+    """Offsets and rms sizes of elliptic Gaussians [m]: offsets uniform in
+    the network's box (|a|, |b| < 8) or Gaussian with twice the rms size,
+    aspect ratios uniform or log-uniform (flat beams), a third of them with
+    sy > sx."""
+    rng = np.random.default_rng(seed)
+    sx = rng.uniform(2e-5, 3e-4, n)
+    r = 0.05 * 20 ** rng.random(n) if kind == "flat" else rng.uniform(0.05, 1.0, n)
+    sy = sx * r
+    if kind == "box":
+        dx, dy = rng.uniform(-7.99, 7.99, n) * sx, rng.uniform(-7.99, 7.99, n) * sy
+    else:
+        dx, dy = rng.normal(0, 2, n) * sx, rng.normal(0, 2, n) * sy
+    sw = rng.random(n) < 0.3
+    return (np.where(sw, dy, dx), np.where(sw, dx, dy), np.where(sw, sy, sx), np.where(sw, sx, sy))
+
+
+@pytest.mark.parametrize("kind", ["box", "core", "flat"])
+def test_trained_field_within_the_tolerance(cuda_device, trained_mlp, kind):
+    """The network trained with the standard settings against the Faddeeva
+    field (mbt_gauss_field_dev, FP64) on 2e6 held-out points: relative error
+    of the field vector |F_net - F| / |F| at most 1e-4 (the north star's
+    bar) everywhere.  What the network gains over the method without it:
+    the quadrature envelope alone (network output 0) misses the bar, the
+    trained network is at least 10 times closer at its worst point."""
+    m, hist = trained_mlp
+    assert np.all(np.isfinite(hist)) and hist[-100:].mean() < 0.01 * hist[:5].mean()
+    n = 2_000_000
+    arrs = [torch.as_tensor(a, device="cuda") for a in field_points(n, 17, kind)]
+    ptr = [a.data_ptr() for a in arrs]
+    f, g, e = [[torch.empty(n, dtype=torch.float64, device="cuda") for _ in range(2)] for _ in range(3)]
+    assert api.lib().mbt_gauss_field_dev(n, *ptr, f[0].data_ptr(), f[1].data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    fallbacks = m.field_dev(n, *ptr, g[0].data_ptr(), g[1].data_ptr())
+    zero = api.Mlp(seed=1)
+    zero.set_params(np.zeros(api.MLP_NPARAM, dtype=np.float32))
+    zero.field_dev(n, *ptr, e[0].data_ptr(), e[1].data_ptr())
+    zero.close()
+    F = torch.hypot(f[0], f[1])
+    err = (torch.hypot(g[0] - f[0], g[1] - f[1]) / F).cpu().numpy()
+    err0 = (torch.hypot(e[0] - f[0], e[1] - f[1]) / F).cpu().numpy()
+    print("%s: learned field max %.2e p99.9 %.2e median %.2e; envelope alone max %.2e; %d outside the domain"
+          % (kind, err.max(), np.percentile(err, 99.9), np.median(err), err0.max(), fallbacks))
+    assert np.all(np.isfinite(err))
+    assert err.max() <= 1e-4
+    assert err0.max() > 1e-4 and err.max() <= 0.1 * err0.max()

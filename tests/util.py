@@ -125,6 +125,25 @@ def stats_err(a, b):
     return err
 
 
+def centroid_err(a, b):
+    """Centroid histories relative to their own size: for every bunch and
+    plane (position and slope means, columns 0-2 and 6-8), the largest
+    difference over the turns divided by max(largest |centroid| of b over
+    the turns, 1e-6 x that plane's rms).  Statistics arrays are
+    [turns, bunches, 12] (or [bunches, 12] for one turn)."""
+    a = np.asarray(a, dtype=float)
+    b = np.asarray(b, dtype=float)
+    if a.ndim == 2:
+        a, b = a[None], b[None]
+    out = np.zeros(b.shape[1:-1] + (6,))
+    for j, (mean_col, rms_col) in enumerate(((0, 3), (1, 4), (2, 5), (6, 9), (7, 10), (8, 11))):
+        amp = np.max(np.abs(b[..., mean_col]), axis=0)
+        floor = 1e-6 * np.max(np.abs(b[..., rms_col]), axis=0)
+        scale = np.maximum(np.maximum(amp, floor), 1e-300)
+        out[..., j] = np.max(np.abs(a[..., mean_col] - b[..., mean_col]), axis=0) / scale
+    return out
+
+
 # Slice model (BunchModel = STRONG) cases: ten consecutive bunches of
 # 0.5 nC with the long-range resistive wall; and six bunches followed by a
 # 5 nC bunch 195 buckets later (ions drift across the gap), 41 slices, the

@@ -710,7 +710,10 @@ def beam_ion_record(args, tmp):
     nb, npb = cfg.nbunch, cfg.params.np_model
     bi0 = cfg.beam_ion()
     evals = bi0.n_ip * (bi0.ions_per_passage * nb * (nb - 1) // 2 + npb * (nb - 1))
-    rec = {"workload": WORKLOADS["beam_ion"][2], "bunches": nb, "np_per_bunch": npb, "macroparticles": nb * npb,
+    rec = {"workload": "beam-ion weak-strong: 200-bunch train x 5e4 macroparticles, CO at 1 nTorr, 20 interaction "
+                       "points, 1000 macro-ions per passage per point; the same turns with the Faddeeva field and with "
+                       "the learned field",
+           "bunches": nb, "np_per_bunch": npb, "macroparticles": nb * npb,
            "field_evaluations_per_turn": evals, "turns_timed": args.bi_steps, "turns_warmup": args.bi_warmup}
     mlp = api.Mlp(seed=31)
     torch.cuda.synchronize()
@@ -794,7 +797,9 @@ def combined_extras(args, cfg, trk, mlp, init_stats, tiles, tmp):
         work = os.path.join(tmp, "combined_work")
         os.makedirs(work, exist_ok=True)
         ocfg, bunch_out = cfg.output()
-        w = api.Writer(work, cfg.params, ocfg, bunch_out, cfg.bucket, cfg.bunch_currents())
+        wp = cfg.params.copy()
+        wp.nrev_tot = args.growth_turns             # the files cover the turns run here
+        w = api.Writer(work, wp, ocfg, bunch_out, cfg.bucket, cfg.bunch_currents())
         w.wakes(cfg.Gl, cfg.Gv, cfg.Gh)
         w.begin(init_stats)
         trk.beam_ion_audit()

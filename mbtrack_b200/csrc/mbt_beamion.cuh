@@ -236,9 +236,12 @@ __device__ __forceinline__ uint32_t bi_hash(uint32_t a, uint32_t b, uint32_t c) 
 }
 
 // The Faddeeva field out of line, for the rare fallbacks and audits of the
-// learned-field kernels (keeps their register budget for the network).
-__device__ __noinline__ void gauss_field_ool(double dx, double dy, double sx, double sy, double *gx, double *gy) {
-  gauss_field(dx, dy, sx, sy, *gx, *gy);
+// learned-field kernels (keeps their register budget for the network);
+// returned by value, so that no caller variable has its address taken.
+__device__ __noinline__ double2 gauss_field_ool(double dx, double dy, double sx, double sy) {
+  double2 g;
+  gauss_field(dx, dy, sx, sy, g.x, g.y);
+  return g;
 }
 
 // The learned field with its fallback and audit, for one group.
@@ -248,12 +251,14 @@ __device__ __forceinline__ bool bi_field_mlp(const BiArgs &bi, MlpGroup &G, int 
   bool in_domain;
   if (!mlp_group_field(G, t, active, dx, dy, sx, sy, gx, gy, in_domain)) return false;
   if (active && !in_domain) {
-    gauss_field_ool(dx, dy, sx, sy, &gx, &gy);
+    const double2 f = gauss_field_ool(dx, dy, sx, sy);
+    gx = f.x;
+    gy = f.y;
     ++fallbacks;
   } else if (active && h < bi.audit_threshold) {
     // relative error of the field vector: |F_net - F| / |F|
-    double ex, ey;
-    gauss_field_ool(dx, dy, sx, sy, &ex, &ey);
+    const double2 fe = gauss_field_ool(dx, dy, sx, sy);
+    const double ex = fe.x, ey = fe.y;
     const double f = hypot(ex, ey);
     const double e = f > 0.0 ? hypot(gx - ex, gy - ey) / f : 0.0;
     aud_max = fmax(aud_max, e);

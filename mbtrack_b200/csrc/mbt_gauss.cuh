@@ -45,10 +45,13 @@ __device__ __forceinline__ void gauss_field(double dx, double dy, double sx, dou
   if (r <= kBiRoundRatio) {
     const double fbe = sqrt(2.0 * (sx * sx - sy * sy));
     const double x1 = ax / fbe, y1 = ay / fbe;
-    double w1r, w1i, w2r, w2i;
+    double w1r, w1i, w2r = 0.0, w2i = 0.0;
     wofz_dev(x1, y1, w1r, w1i);
-    wofz_dev(x1 * r, y1 / r, w2r, w2i);
-    const double e = exp(-(ax * ax / (2.0 * sx * sx) + ay * ay / (2.0 * sy * sy)));
+    // beyond exp(-50) the second term lies below the last bit of the first
+    // (|w| <= 1 in the upper half plane): w(z2) is not evaluated there
+    const double arg = ax * ax / (2.0 * sx * sx) + ay * ay / (2.0 * sy * sy);
+    const double e = arg > 50.0 ? 0.0 : exp(-arg);
+    if (e != 0.0) wofz_dev(x1 * r, y1 / r, w2r, w2i);
     const double c = 1.0 / (1.7724538509055160273 * fbe);
     fx = c * (w1i - e * w2i);
     fy = c * (w1r - e * w2r);

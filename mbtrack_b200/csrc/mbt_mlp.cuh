@@ -254,11 +254,11 @@ __device__ __forceinline__ void issue_layer_fwd(const MlpGroup &G) {
   }
 }
 
-// Issue (one thread) and wait (all) for one layer of the group; false when
-// it never completed (a second bounded wait then covers the MMAs in
-// flight).
+// Issue one layer of the group: the operand tile written by every thread
+// is made visible to the tensor cores, then one thread issues the products
+// and a commit to the group's barrier.
 template <int L>
-__device__ __forceinline__ bool group_mma(MlpGroup &G, int t) {
+__device__ __forceinline__ void group_issue(const MlpGroup &G, int t) {
   fence_proxy_async();
   tc_fence_before();
   named_barrier(G.bar_id, 128);
@@ -267,6 +267,10 @@ __device__ __forceinline__ bool group_mma(MlpGroup &G, int t) {
     issue_layer_fwd<L>(G);
     umma_commit(G.bar);
   }
+}
+// Wait (all threads) for the group's products; false when they never
+// completed (a second bounded wait then covers the MMAs in flight).
+__device__ __forceinline__ bool group_wait(MlpGroup &G) {
   if (!group_all(mbar_wait(G.bar, G.phase, kMlpWaitLimit), G.bar_id, 128)) {
     mbar_wait(G.bar, G.phase, kMlpWaitLimit);
     return false;
@@ -274,6 +278,11 @@ __device__ __forceinline__ bool group_mma(MlpGroup &G, int t) {
   G.phase ^= 1u;
   tc_fence_after();
   return true;
+}
+template <int L>
+__device__ __forceinline__ bool group_mma(MlpGroup &G, int t) {
+  group_issue<L>(G, t);
+  return group_wait(G);
 }
 
 // Row t of the layer-1 operand (k-step 0 of the activation tile): the BF16
@@ -337,18 +346,31 @@ struct MlpRowSave {
   float *z1, *z2, *z3, *h1, *h2, *h3;
 };
 
+// Work the caller interleaves with the network: `a()` runs while the
+// layer-2 products execute, `b()` after the barrier that issues layer 3
+// (every thread's writes of a() are visible to the group then).
+struct NoSideWork {
+  __device__ __forceinline__ void a() const {}
+  __device__ __forceinline__ void b() const {}
+};
+
 // The network on this thread's features x -> y (Yx, Yy).  Every thread of
 // the group calls it together; false when an MMA never completed (the
 // group then stops using the tensor cores).  sv: where this point's
 // pre-activations and activations go (training), or null.
+template <typename Side = NoSideWork>
 __device__ __forceinline__ bool mlp_group_eval(MlpGroup &G, int t, const float *x, float *y,
-                                               const MlpRowSave *sv = nullptr) {
+                                               const MlpRowSave *sv = nullptr, const Side &side = Side()) {
   mlp_input_row(G, x);
   if (!group_mma<kLayer1>(G, t)) return false;
   mlp_epilogue(G, sv ? sv->z1 : nullptr, sv ? sv->h1 : nullptr);
-  if (!group_mma<kLayer2>(G, t)) return false;
+  group_issue<kLayer2>(G, t);
+  side.a();
+  if (!group_wait(G)) return false;
   mlp_epilogue(G, sv ? sv->z2 : nullptr, sv ? sv->h2 : nullptr);
-  if (!group_mma<kLayer3>(G, t)) return false;
+  group_issue<kLayer3>(G, t);
+  side.b();
+  if (!group_wait(G)) return false;
   mlp_epilogue(G, sv ? sv->z3 : nullptr, sv ? sv->h3 : nullptr);
   if (!group_mma<kLayerOut>(G, t)) return false;
   tmem_ld2(G.dcol + G.lane, y[0], y[1]);
@@ -554,8 +576,10 @@ namespace mbt {
 // whose point lies outside a, b < 8, r >= 0.05 (`in_domain` false), gets
 // no value and uses the Faddeeva field instead.  false when the tensor
 // cores failed.
+template <typename Side = NoSideWork>
 __device__ __forceinline__ bool mlp_group_field(MlpGroup &G, int t, bool active, double dx, double dy, double sx,
-                                                double sy, double &gx, double &gy, bool &in_domain) {
+                                                double sy, double &gx, double &gy, bool &in_domain,
+                                                const Side &side = Side()) {
   // the network's inputs and the field's assembly in FP32 (its 1e-7 is far
   // below the network's accuracy)
   const bool swap = sy > sx;
@@ -566,7 +590,7 @@ __device__ __forceinline__ bool mlp_group_field(MlpGroup &G, int t, bool active,
   in_domain = active && s2 > 0.0f && a < 8.0f && b < 8.0f && r >= 0.05f;
   float x[3], y[2];
   mlp_features(in_domain ? a : 0.0f, in_domain ? b : 0.0f, in_domain ? r : 1.0f, x);
-  if (!mlp_group_eval(G, t, x, y)) return false;
+  if (!mlp_group_eval(G, t, x, y, nullptr, side)) return false;
   if (in_domain) {
     float ex, ey;
     mlp_envelopes(a, b, r, ex, ey);

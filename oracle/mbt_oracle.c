@@ -844,10 +844,13 @@ void orc_gauss_field(double dx, double dy, double sx, double sy, double *gx, dou
   if (r <= 0.995) {
     const double fbe = sqrt(2.0 * (sx * sx - sy * sy));
     const double x1 = ax / fbe, y1 = ay / fbe;
-    double w1r, w1i, w2r, w2i, e, c;
+    double w1r, w1i, w2r = 0.0, w2i = 0.0, e, c, arg;
     orc_wofz(x1, y1, &w1r, &w1i);
-    orc_wofz(x1 * r, y1 / r, &w2r, &w2i);
-    e = exp(-(ax * ax / (2.0 * sx * sx) + ay * ay / (2.0 * sy * sy)));
+    /* beyond exp(-50) the second term lies below the last bit of the first
+     * (|w| <= 1 in the upper half plane): w(z2) is not evaluated there */
+    arg = ax * ax / (2.0 * sx * sx) + ay * ay / (2.0 * sy * sy);
+    e = arg > 50.0 ? 0.0 : exp(-arg);
+    if (e != 0.0) orc_wofz(x1 * r, y1 / r, &w2r, &w2i);
     c = 1.0 / (1.7724538509055160273 * fbe);
     fx = c * (w1i - e * w2i);
     fy = c * (w1r - e * w2r);

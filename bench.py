@@ -354,6 +354,8 @@ def run_b200(args):
     if bi_info is not None:
         bi_ms = trk.beam_ion_timing()
         bi_info["stage_ms_per_turn"] = bi_ms
+        bi_info["kernels_ms_per_turn"] = dict(zip(("frames", "ions", "clouds", "kick"),
+                                                  [float(v) for v in trk.beam_ion_kernel_times()]))
         bi_info["field_evaluations_per_s"] = bi_info["field_evaluations_per_turn"] / (bi_ms * 1e-3)
         if audit is not None:
             bi_info["audit"] = {"audited": int(audit[0]), "max_rel_error": float(audit[1]),
@@ -750,6 +752,8 @@ def beam_ion_record(args, tmp):
                                    "of the warps each turn"}
         trk.profile(2)
         r["stage_ms_per_turn"] = trk.beam_ion_timing()
+        r["kernels_ms_per_turn"] = dict(zip(("frames", "ions", "clouds", "kick"),
+                                            [float(v) for v in trk.beam_ion_kernel_times()]))
         r["field_evaluations_per_s"] = evals / (r["stage_ms_per_turn"] * 1e-3)
         trk.close()
         runs[name] = r

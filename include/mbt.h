@@ -500,6 +500,10 @@ int mbt_beam_ion_audit(mbt_ctx *ctx, double out[5]);
  * mbt_profile_turns call (0 when the stage is off). */
 int mbt_beam_ion_timing(mbt_ctx *ctx, double *ms_per_turn);
 
+/* The same split by kernel: frames, ions, clouds, electron kicks [ms per
+ * turn] in the last mbt_profile_turns call (zeros when the stage is off). */
+int mbt_beam_ion_kernel_times(mbt_ctx *ctx, double ms_per_turn[4]);
+
 /* Unit-charge field of an elliptic Gaussian at n points (device arrays):
  * E = lambda / (2 eps0) (gx, gy) for line density lambda.  Bassetti-
  * Erskine with w(z) for aspect ratios up to 0.995, a Gauss-Legendre

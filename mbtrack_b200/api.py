@@ -80,6 +80,7 @@ SIGNATURES = {
     "mbt_enable_beam_ion": (ctypes.c_int, [_vp, _P(MbtBeamIon)]),
     "mbt_beam_ion_clouds": (ctypes.c_int, [_vp, _vp]),
     "mbt_beam_ion_timing": (ctypes.c_int, [_vp, _vp]),
+    "mbt_beam_ion_kernel_times": (ctypes.c_int, [_vp, _vp]),
     "mbt_gauss_field_dev": (ctypes.c_int, [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mbt_beam_ion_use_mlp": (ctypes.c_int, [_vp, _vp]),
     "mbt_beam_ion_audit": (ctypes.c_int, [_vp, _vp]),
@@ -392,6 +393,12 @@ class Tracker:
         v = ctypes.c_double()
         _check(lib().mbt_beam_ion_timing(self.h, ctypes.byref(v)), self.h)
         return v.value
+
+    def beam_ion_kernel_times(self):
+        """ms per turn of (frames, ions, clouds, electron kicks), last profile."""
+        v = np.zeros(4)
+        _check(lib().mbt_beam_ion_kernel_times(self.h, _ptr(v)), self.h)
+        return v
 
     def watch_potentials(self, bunches):
         b = np.ascontiguousarray(bunches, dtype=np.int32)

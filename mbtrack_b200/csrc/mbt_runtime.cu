@@ -77,6 +77,8 @@ struct mbt_ctx {
   mbt_beam_ion bicfg{};
   mbt::BiArgs bi{};
   cudaEvent_t bi_ev = nullptr;   // end of the beam-ion stage (profiling)
+  cudaEvent_t bi_kev[3] = {nullptr, nullptr, nullptr};   // after frames, ions, clouds (profiling)
+  double bi_kms[4] = {0, 0, 0, 0};                        // frames, ions, clouds, kick: last profile
   mbt::MlpDev mlp{};             // learned field (surrogate runs)
   bool mlp_set = false;
   double bi_ms = 0.0;            // its average device time in the last mbt_profile_turns
@@ -241,23 +243,29 @@ size_t smem_scan(const mbt_ctx *c) {
   return mbt::ring_scan_smem_doubles(c->p.rw_long, c->p.Nmlt, c->p.nharm) * sizeof(double);
 }
 
-// The beam-ion stage of a turn: frames, ion clouds, electron kicks.
-void enqueue_beam_ion(mbt_ctx *c) {
+// The beam-ion stage of a turn: frames, ion clouds, electron kicks; with
+// `prof`, events between its kernels.
+void enqueue_beam_ion(mbt_ctx *c, bool prof = false) {
   const mbt::BiArgs &bi = c->bi;
   const int n = bi.n_ip * bi.nb;
   mbt::bi_frames<<<(n + 127) / 128, 128, 0, c->stream>>>(bi);
+  if (prof) cudaEventRecord(c->bi_kev[0], c->stream);
   if (c->bicfg.surrogate) {
     const int grid = c->nsm;
     if (bi.nb > 1)
       mbt::bi_ions_mlp<<<grid, 128 * mbt::kMlpGroups, mbt::kMlpCtaSmem, c->stream>>>(bi, c->mlp);
+    if (prof) cudaEventRecord(c->bi_kev[1], c->stream);
     mbt::bi_clouds<<<dim3(bi.nb, bi.n_ip), mbt::kBiThreads, 0, c->stream>>>(bi);
+    if (prof) cudaEventRecord(c->bi_kev[2], c->stream);
     mbt::bi_kick_mlp<<<grid, 128 * mbt::kMlpGroups, mbt::kMlpCtaSmem, c->stream>>>(c->a, bi, c->mlp);
     return;
   }
   if (bi.nb > 1) {
     mbt::bi_ions<<<dim3(bi.bpp, bi.nb - 1, bi.n_ip), mbt::kBiThreads, 0, c->stream>>>(bi);
   }
+  if (prof) cudaEventRecord(c->bi_kev[1], c->stream);
   mbt::bi_clouds<<<dim3(bi.nb, bi.n_ip), mbt::kBiThreads, 0, c->stream>>>(bi);
+  if (prof) cudaEventRecord(c->bi_kev[2], c->stream);
   mbt::bi_kick<<<c->ntile, mbt::kBiThreads, 0, c->stream>>>(c->a, bi);
 }
 
@@ -286,7 +294,7 @@ void enqueue_turn(mbt_ctx *c, cudaEvent_t *ev, bool boundary = false) {
   mbt::bunch_wakes<<<c->nbunch, mbt::kBlock, smem_wakes(c), c->stream>>>(c->a, 1);
   if (ev) cudaEventRecord(ev[4], c->stream);
   if (c->bi_on) {
-    enqueue_beam_ion(c);
+    enqueue_beam_ion(c, ev != nullptr);
     if (ev) cudaEventRecord(c->bi_ev, c->stream);
   }
   if (boundary) {
@@ -632,6 +640,8 @@ int mbt_destroy(mbt_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->graph) cudaGraphExecDestroy(c->graph);
   if (c->bi_ev) cudaEventDestroy(c->bi_ev);
+  for (cudaEvent_t e : c->bi_kev)
+    if (e) cudaEventDestroy(e);
   for (void *p : c->allocs) cudaFree(p);
   if (c->dev) cudaFree(c->dev);
   for (auto &e : c->ev) if (e) cudaEventDestroy(e);
@@ -848,6 +858,8 @@ int mbt_enable_beam_ion(mbt_ctx *c, const mbt_beam_ion *cfg) {
   bi.error = &c->a.rs->error;
   c->a.bi_mom = mom;
   if (!c->bi_ev) CK(cudaEventCreate(&c->bi_ev));
+  for (cudaEvent_t &e : c->bi_kev)
+    if (!e) CK(cudaEventCreate(&e));
   c->bicfg = *cfg;
   c->bi_on = 1;
   if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; c->graph_turns = 0; }
@@ -1052,7 +1064,7 @@ int mbt_profile_turns(mbt_ctx *c, long nturns, double out[4]) {
   if (!c->prepared) return fail(c, MBT_ERR_STATE, "mbt_prepare must come first");
   if (c->bi_on && c->bicfg.surrogate && !c->mlp_set)
     return fail(c, MBT_ERR_STATE, "surrogate beam-ion fields need mbt_beam_ion_use_mlp");
-  double acc[4] = {0, 0, 0, 0}, acc_bi = 0.0;
+  double acc[4] = {0, 0, 0, 0}, acc_bi = 0.0, acc_k[4] = {0, 0, 0, 0};
   RingState rs;
   CK(cudaMemcpy(&rs, c->a.rs, sizeof rs, cudaMemcpyDeviceToHost));
   for (long t = 0; t < nturns; ++t) {
@@ -1067,12 +1079,24 @@ int mbt_profile_turns(mbt_ctx *c, long nturns, double out[4]) {
       float ms = 0;
       cudaEventElapsedTime(&ms, c->ev[4], c->bi_ev);
       acc_bi += ms;
+      const cudaEvent_t seq[5] = {c->ev[4], c->bi_kev[0], c->bi_kev[1], c->bi_kev[2], c->bi_ev};
+      for (int k = 0; k < 4; ++k) {
+        cudaEventElapsedTime(&ms, seq[k], seq[k + 1]);
+        acc_k[k] += ms;
+      }
     }
   }
   int r = sync_and_check(c);
   if (r) return r;
   for (int k = 0; k < 4; ++k) out[k] = acc[k] / nturns;
   c->bi_ms = acc_bi / nturns;
+  for (int k = 0; k < 4; ++k) c->bi_kms[k] = acc_k[k] / nturns;
+  return 0;
+}
+
+int mbt_beam_ion_kernel_times(mbt_ctx *c, double ms_per_turn[4]) {
+  if (!c || !ms_per_turn) return MBT_ERR_INVALID;
+  for (int k = 0; k < 4; ++k) ms_per_turn[k] = c->bi_on ? c->bi_kms[k] : 0.0;
   return 0;
 }
 

@@ -244,20 +244,6 @@ __device__ __noinline__ double2 gauss_field_ool(double dx, double dy, double sx,
   return g;
 }
 
-// OR of `v` over the `count` threads of named barrier `id` (a barrier too)
-__device__ __forceinline__ bool group_any(bool v, int id, int count) {
-  uint32_t out;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.u32 p, %1, 0;\n\t"
-      "bar.red.or.pred q, %2, %3, p;\n\t"
-      "selp.u32 %0, 1, 0, q;\n\t}"
-      : "=r"(out)
-      : "r"((uint32_t)v), "r"(id), "r"(count)
-      : "memory");
-  return out != 0;
-}
-
 // The Faddeeva fallbacks of a group, evaluated with the group's lanes
 // packed: every thread whose point lies outside the network's domain
 // appends (dx, dy, sx, sy) to a list in the group's activation tile (free
@@ -266,7 +252,6 @@ __device__ __forceinline__ bool group_any(bool v, int id, int count) {
 // would otherwise make every warp run the Faddeeva branch.
 __device__ __forceinline__ void bi_group_fallbacks(MlpGroup &G, int t, bool need, double dx, double dy, double sx,
                                                    double sy, double &gx, double &gy, int &fallbacks) {
-  if (!group_any(need, G.bar_id, 128)) return;
   const int warp = t >> 5, lane = t & 31;
   const unsigned ball = __ballot_sync(0xffffffffu, need);
   int *cnt = reinterpret_cast<int *>(G.A);
@@ -308,9 +293,9 @@ __device__ __forceinline__ bool bi_field_mlp(const BiArgs &bi, MlpGroup &G, int 
                                              double sx, double sy, uint32_t h, double &gx, double &gy,
                                              double &aud_max, double &aud_sq, int &aud_n, int &fallbacks,
                                              const Side &side = Side()) {
-  bool in_domain;
-  if (!mlp_group_field(G, t, active, dx, dy, sx, sy, gx, gy, in_domain, side)) return false;
-  bi_group_fallbacks(G, t, active && !in_domain, dx, dy, sx, sy, gx, gy, fallbacks);
+  bool in_domain, any_out;
+  if (!mlp_group_field(G, t, active, dx, dy, sx, sy, gx, gy, in_domain, any_out, side)) return false;
+  if (any_out) bi_group_fallbacks(G, t, active && !in_domain, dx, dy, sx, sy, gx, gy, fallbacks);
   if (active && in_domain && h < bi.audit_threshold) {
     // relative error of the field vector: |F_net - F| / |F|
     const double2 fe = gauss_field_ool(dx, dy, sx, sy);
@@ -337,28 +322,6 @@ __device__ __forceinline__ void bi_audit_flush(const BiArgs &bi, double aud_max,
     if (f) atomicAdd(&bi.audit[2], (unsigned long long)f);
   }
 }
-
-// The cloud moments of one group's ions at one passage, as side work of
-// the network (mlp_group_eval): a() sums w, w dx, w dy, w dx^2, w dy^2 over
-// each warp into the group's shared slots, b() adds the four warps' sums in
-// a fixed order and writes the passage's partial record.
-struct BiMoments {
-  double w, dx, dy;
-  int lane, warp, t;
-  double *red;      // [4 warps][5]
-  double *out;      // 5 doubles of the partial record
-  __device__ __forceinline__ void a() const {
-    double s[5] = {w, w * dx, w * dy, w * (dx * dx), w * (dy * dy)};
-#pragma unroll
-    for (int m = 0; m < 5; ++m) s[m] = warp_sum(s[m]);
-    if (lane == 0)
-#pragma unroll
-      for (int m = 0; m < 5; ++m) red[warp * 5 + m] = s[m];
-  }
-  __device__ __forceinline__ void b() const {
-    if (t < 5) out[t] = ((red[t] + red[5 + t]) + red[10 + t]) + red[15 + t];
-  }
-};
 
 // Ions with the learned field: work item = (creating passage b0, point k,
 // 128-ion block), longest first; every group takes items round-robin.
@@ -394,14 +357,18 @@ __global__ void __launch_bounds__(128 * kMlpGroups, 1) bi_ions_mlp(BiArgs bi, Ml
       y = y + dt * vy;
       const double *F = bi.frame + ((size_t)k * bi.nb + b) * 4;
       const double dx = x - F[0], dy = y - F[1];
-      // the cloud moments of this passage, summed while the network's
-      // layer-2 products run (side work a) and written after the next
-      // barrier (b)
-      const BiMoments mom{w, dx, dy, lane, warp, t, &red[g][0][0],
-                          bi.part + (((size_t)k * bi.T + bi_tri(b) + b0) * bi.bpp + blk) * 5};
+      double s[5] = {w, w * dx, w * dy, w * (dx * dx), w * (dy * dy)};
+#pragma unroll
+      for (int m = 0; m < 5; ++m) s[m] = warp_sum(s[m]);
+      if (lane == 0)
+        for (int m = 0; m < 5; ++m) red[g][warp][m] = s[m];
+      named_barrier(G.bar_id, 128);
+      if (t < 5)
+        bi.part[(((size_t)k * bi.T + bi_tri(b) + b0) * bi.bpp + blk) * 5 + t] =
+            ((red[g][0][t] + red[g][1][t]) + red[g][2][t]) + red[g][3][t];
       double gx = 0.0, gy = 0.0;
       if (!bi_field_mlp(bi, G, t, live, dx, dy, F[2], F[3], bi_hash((uint32_t)turn, (uint32_t)(k * 65536 + b), (uint32_t)(b0 * 1048576 + (j >> 5))),
-                        gx, gy, aud_max, aud_sq, aud_n, fallbacks, mom)) {
+                        gx, gy, aud_max, aud_sq, aud_n, fallbacks)) {
         ok = false;
         break;
       }
@@ -412,12 +379,11 @@ __global__ void __launch_bounds__(128 * kMlpGroups, 1) bi_ions_mlp(BiArgs bi, Ml
       }
     }
   }
-  if (!ok && t == 0) {
+  bi_audit_flush(bi, aud_max, aud_sq, aud_n, fallbacks);
+  if ((mlp_cta_release(tmem, G) || !ok) && t == 0) {
     atomicAdd(&bi.audit[3], 1ull);
     atomicOr(bi.error, 4);
   }
-  bi_audit_flush(bi, aud_max, aud_sq, aud_n, fallbacks);
-  mlp_cta_release(tmem);
 }
 
 // Electrons with the learned field: work item = 128 particles of a tile.
@@ -480,12 +446,11 @@ __global__ void __launch_bounds__(128 * kMlpGroups, 1) bi_kick_mlp(Args a, BiArg
       C[5 * n6 + p] = zp + ddzp;
     }
   }
-  if (!ok && t == 0) {
+  bi_audit_flush(bi, aud_max, aud_sq, aud_n, fallbacks);
+  if ((mlp_cta_release(tmem, G) || !ok) && t == 0) {
     atomicAdd(&bi.audit[3], 1ull);
     atomicOr(bi.error, 4);
   }
-  bi_audit_flush(bi, aud_max, aud_sq, aud_n, fallbacks);
-  mlp_cta_release(tmem);
 }
 
 }  // namespace mbt

@@ -175,7 +175,7 @@ mlp_forward(MlpDev M, long n, const float *__restrict__ abr, float *__restrict__
     for (int w = 0; w < kFwdThreads / 32; ++w) s += lred[w];
     loss_part[blockIdx.x] = s;
   }
-  mlp_cta_release(tmem, kFwdGroups);
+  if (mlp_cta_release(tmem, G, kFwdGroups) && t == 0) atomicOr(err, 1);
 }
 
 // Inference over n points (a, b, r) -> (Yx, Yy): two groups of 128 threads
@@ -201,7 +201,7 @@ mlp_infer(MlpDev M, long n, const float *__restrict__ abr, float *__restrict__ o
       out[2 * m + 1] = y[1];
     }
   }
-  mlp_cta_release(tmem);
+  if (mlp_cta_release(tmem, G) && t == 0) atomicOr(err, 4);
 }
 
 // The learned field at n points (dx, dy, sx, sy) -> (gx, gy), with the
@@ -220,9 +220,9 @@ mlp_field(MlpDev M, long n, const double *__restrict__ dx, const double *__restr
     const long m = tile * 128 + t;
     const bool live = m < n;
     double u = 0.0, v = 0.0;
-    bool in_domain;
+    bool in_domain, any_out;
     if (!mlp_group_field(G, t, live, live ? dx[m] : 0.0, live ? dy[m] : 0.0, live ? sx[m] : 1.0,
-                         live ? sy[m] : 1.0, u, v, in_domain)) {
+                         live ? sy[m] : 1.0, u, v, in_domain, any_out)) {
       if (t == 0) atomicOr(err, 4);
       break;
     }
@@ -237,7 +237,7 @@ mlp_field(MlpDev M, long n, const double *__restrict__ dx, const double *__restr
   }
   const int f = warp_sum(fb);
   if ((threadIdx.x & 31) == 0 && f) atomicAdd(fallbacks, (unsigned long long)f);
-  mlp_cta_release(tmem);
+  if (mlp_cta_release(tmem, G) && t == 0) atomicOr(err, 4);
 }
 
 // Backward pass of a batch of n points (forward values in sv, outputs in

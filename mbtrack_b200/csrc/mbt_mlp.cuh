@@ -233,6 +233,7 @@ struct MlpGroup {
   int swz;                                     // this thread's row inside its 8-row group
   int bar_id;                                  // named barrier of the group
   uint32_t phase;
+  volatile int *fail;                          // set when a wait of the group gave up
 };
 
 // The products of one layer; one thread issues them.
@@ -254,35 +255,51 @@ __device__ __forceinline__ void issue_layer_fwd(const MlpGroup &G) {
   }
 }
 
+// OR of `v` over the `count` threads of named barrier `id` (a barrier too)
+__device__ __forceinline__ bool group_any(bool v, int id, int count) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(out)
+      : "r"((uint32_t)v), "r"(id), "r"(count)
+      : "memory");
+  return out != 0;
+}
+
 // Issue one layer of the group: the operand tile written by every thread
 // is made visible to the tensor cores, then one thread issues the products
-// and a commit to the group's barrier.
+// and a commit to the group's barrier.  The layer-1 barrier also returns
+// the OR of `flag` over the group.  `failed`: a wait of the group gave up
+// before this barrier (every thread reads the same flag after it); nothing
+// is issued then.
 template <int L>
-__device__ __forceinline__ void group_issue(const MlpGroup &G, int t) {
+__device__ __forceinline__ bool group_issue(const MlpGroup &G, int t, bool &failed, bool flag = false) {
   fence_proxy_async();
   tc_fence_before();
-  named_barrier(G.bar_id, 128);
-  if (t == 0) {
+  bool any = false;
+  if (L == kLayer1) any = group_any(flag, G.bar_id, 128);
+  else named_barrier(G.bar_id, 128);
+  failed = *G.fail != 0;
+  if (t == 0 && !failed) {
     tc_fence_after();
     issue_layer_fwd<L>(G);
     umma_commit(G.bar);
   }
+  return any;
 }
-// Wait (all threads) for the group's products; false when they never
-// completed (a second bounded wait then covers the MMAs in flight).
-__device__ __forceinline__ bool group_wait(MlpGroup &G) {
-  if (!group_all(mbar_wait(G.bar, G.phase, kMlpWaitLimit), G.bar_id, 128)) {
+// Wait (each thread) for the group's products.  A wait that gives up sets
+// the group's flag, which every thread sees after the group's next barrier,
+// and waits once more (bounded) for the products still in flight.
+__device__ __forceinline__ void group_wait(MlpGroup &G) {
+  if (!mbar_wait(G.bar, G.phase, kMlpWaitLimit)) {
+    *G.fail = 1;
     mbar_wait(G.bar, G.phase, kMlpWaitLimit);
-    return false;
   }
   G.phase ^= 1u;
   tc_fence_after();
-  return true;
-}
-template <int L>
-__device__ __forceinline__ bool group_mma(MlpGroup &G, int t) {
-  group_issue<L>(G, t);
-  return group_wait(G);
 }
 
 // Row t of the layer-1 operand (k-step 0 of the activation tile): the BF16
@@ -358,21 +375,34 @@ struct NoSideWork {
 // the group calls it together; false when an MMA never completed (the
 // group then stops using the tensor cores).  sv: where this point's
 // pre-activations and activations go (training), or null.
+// `flag` / `any`: a per-thread predicate and its OR over the group (taken
+// from the layer-1 barrier, at no extra synchronisation).
+// A wait that gives up in the output layer is seen at the group's next
+// barrier (the next call, or mlp_cta_release).
 template <typename Side = NoSideWork>
 __device__ __forceinline__ bool mlp_group_eval(MlpGroup &G, int t, const float *x, float *y,
-                                               const MlpRowSave *sv = nullptr, const Side &side = Side()) {
+                                               const MlpRowSave *sv = nullptr, const Side &side = Side(),
+                                               bool flag = false, bool *any = nullptr) {
+  bool failed;
   mlp_input_row(G, x);
-  if (!group_mma<kLayer1>(G, t)) return false;
+  const bool a1 = group_issue<kLayer1>(G, t, failed, flag);
+  if (any) *any = a1;
+  if (failed) return false;
+  group_wait(G);
   mlp_epilogue(G, sv ? sv->z1 : nullptr, sv ? sv->h1 : nullptr);
-  group_issue<kLayer2>(G, t);
+  group_issue<kLayer2>(G, t, failed);
+  if (failed) return false;
   side.a();
-  if (!group_wait(G)) return false;
+  group_wait(G);
   mlp_epilogue(G, sv ? sv->z2 : nullptr, sv ? sv->h2 : nullptr);
-  group_issue<kLayer3>(G, t);
+  group_issue<kLayer3>(G, t, failed);
+  if (failed) return false;
   side.b();
-  if (!group_wait(G)) return false;
+  group_wait(G);
   mlp_epilogue(G, sv ? sv->z3 : nullptr, sv ? sv->h3 : nullptr);
-  if (!group_mma<kLayerOut>(G, t)) return false;
+  group_issue<kLayerOut>(G, t, failed);
+  if (failed) return false;
+  group_wait(G);
   tmem_ld2(G.dcol + G.lane, y[0], y[1]);
   tmem_ld_wait();
   tc_fence_before();
@@ -425,10 +455,12 @@ __device__ __forceinline__ uint32_t mlp_cta_setup(const MlpDev &M, uint8_t *base
   }
   uint64_t *bar = reinterpret_cast<uint64_t *>(base + kSmemA + (size_t)groups * kTileBytes);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 8);
+  int *fail = reinterpret_cast<int *>(tslot + 1);
   if (threadIdx.x == 0) {
     for (int q = 0; q < groups; ++q) mbar_init(&bar[q], 1);
     fence_mbar_init();
   }
+  if (threadIdx.x < groups) fail[threadIdx.x] = 0;
   if (threadIdx.x < 32) {
     tmem_alloc(tslot, 128 * groups);
     tmem_relinquish();
@@ -450,13 +482,18 @@ __device__ __forceinline__ uint32_t mlp_cta_setup(const MlpDev &M, uint8_t *base
   G.swz = t & 7;
   G.bar_id = 1 + g;
   G.phase = 0;
+  G.fail = fail + g;
   return tmem;
 }
-__device__ __forceinline__ void mlp_cta_release(uint32_t tmem, int groups = kMlpGroups) {
+// Free the CTA's tensor memory; true when a wait of this thread's group
+// gave up at any time (every thread of the group sees the same value).
+__device__ __forceinline__ bool mlp_cta_release(uint32_t tmem, const MlpGroup &G, int groups = kMlpGroups) {
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
+  const bool failed = *G.fail != 0;
   if (threadIdx.x < 32) tmem_dealloc(tmem, 128 * groups);
+  return failed;
 }
 
 // The network's input features.
@@ -576,9 +613,26 @@ namespace mbt {
 // whose point lies outside a, b < 8, r >= 0.05 (`in_domain` false), gets
 // no value and uses the Faddeeva field instead.  false when the tensor
 // cores failed.
+// any_out: whether some thread of the group has an active point outside
+// the domain.
+// The envelope as side work of the network (it needs only a, b, r):
+// evaluated while the layer-2 products run.
+template <typename Side>
+struct EnvelopeSide {
+  const Side &inner;
+  float av, bv, rv;
+  bool on;
+  mutable float ex, ey;
+  __device__ __forceinline__ void a() const {
+    if (on) mlp_envelopes(av, bv, rv, ex, ey);
+    inner.a();
+  }
+  __device__ __forceinline__ void b() const { inner.b(); }
+};
+
 template <typename Side = NoSideWork>
 __device__ __forceinline__ bool mlp_group_field(MlpGroup &G, int t, bool active, double dx, double dy, double sx,
-                                                double sy, double &gx, double &gy, bool &in_domain,
+                                                double sy, double &gx, double &gy, bool &in_domain, bool &any_out,
                                                 const Side &side = Side()) {
   // the network's inputs and the field's assembly in FP32 (its 1e-7 is far
   // below the network's accuracy)
@@ -590,10 +644,10 @@ __device__ __forceinline__ bool mlp_group_field(MlpGroup &G, int t, bool active,
   in_domain = active && s2 > 0.0f && a < 8.0f && b < 8.0f && r >= 0.05f;
   float x[3], y[2];
   mlp_features(in_domain ? a : 0.0f, in_domain ? b : 0.0f, in_domain ? r : 1.0f, x);
-  if (!mlp_group_eval(G, t, x, y, nullptr, side)) return false;
+  const EnvelopeSide<Side> env{side, a, b, r, in_domain, 0.0f, 0.0f};
+  if (!mlp_group_eval(G, t, x, y, nullptr, env, active && !in_domain, &any_out)) return false;
   if (in_domain) {
-    float ex, ey;
-    mlp_envelopes(a, b, r, ex, ey);
+    const float ex = env.ex, ey = env.ey;
     float fx = a * ex * fmaf(y[0], 1.0f / kMlpResidualScale, 1.0f);
     float fy = b * ey * fmaf(y[1], 1.0f / kMlpResidualScale, 1.0f);
     if (swap) {

@@ -14,10 +14,14 @@
 //              creating passage, block), no atomics;
 //   bi_clouds  one block per (point, bunch): the slots summed in a fixed
 //              order -> ions, centroid and rms of the cloud that bunch meets;
-//   bi_kick    one block per tile: every electron kicked by the clouds of its
-//              bunch at every point, kicks mapped back to the kick point.
+//   bi_kick_grouped  one block per tile: every electron kicked by the
+//              clouds of its bunch at every point, kicks mapped back to the
+//              kick point.
+// bi_ions and bi_kick_grouped sort their field evaluations by the branch of
+// w(z) they take before evaluating them (gauss_field_key), so that a warp
+// runs one branch at a time.
 // With the learned field, bi_ions_mlp and bi_kick_mlp replace bi_ions and
-// bi_kick: persistent CTAs of four 128-thread groups that share the
+// bi_kick_grouped: persistent CTAs of four 128-thread groups that share the
 // network's weights; a group evaluates the field for its 128 ions (or
 // electrons) at once on the tensor cores, falls back to the Faddeeva field
 // outside the network's domain, and re-evaluates a hashed sample with it
@@ -90,6 +94,39 @@ __device__ __forceinline__ void bi_normals(const U4 &r, double &g1, double &g2) 
   g2 = sqrt(-2.0 * log(u3)) * cos(2.0 * 3.14159265358979323846 * u4);
 }
 
+// ---- region-grouped evaluation of the Faddeeva field
+
+// TOMS 680 branch of w(z) at x, y >= 0 (wofz_dev): 0 power series, 1
+// Taylor series with continued-fraction derivatives, 2 Laplace continued
+// fraction.
+__device__ __forceinline__ int wofz_branch(double x, double y) {
+  const double xs = x / 6.3, ys = y / 4.4;
+  const double q = xs * xs + ys * ys;
+  return q < 0.085264 ? 0 : (q > 1.0 ? 2 : 1);
+}
+constexpr int kFieldKeys = 13;
+// Key of gauss_field(dx, dy, sx, sy) by the branches its evaluation takes:
+// 4 x (branch of w(z1)) + (branch of w(z2), or 3 when the second term is
+// skipped); 12 for the near-round quadrature.
+__device__ __forceinline__ int gauss_field_key(double dx, double dy, double sx, double sy) {
+  double ax = fabs(dx), ay = fabs(dy);
+  if (sy > sx) {
+    const double t = ax; ax = ay; ay = t;
+    const double u = sx; sx = sy; sy = u;
+  }
+  sy = fmax(sy, 1e-6 * sx);
+  const double r = sy / sx;
+  if (r > kBiRoundRatio) return 12;
+  const double fbe = sqrt(2.0 * (sx * sx - sy * sy));
+  const double x1 = ax / fbe, y1 = ay / fbe;
+  const double arg = ax * ax / (2.0 * sx * sx) + ay * ay / (2.0 * sy * sy);
+  return 4 * wofz_branch(x1, y1) + (arg > 50.0 ? 3 : wofz_branch(x1 * r, y1 / r));
+}
+
+// One thread per macro-ion; at every later passage the block's field
+// evaluations are sorted by the TOMS 680 branches they take (a counting sort
+// in shared memory, as bi_kick_grouped) so that the warps evaluate runs of
+// one branch, and each ion reads its field back.
 __global__ void __launch_bounds__(kBiThreads) bi_ions(BiArgs bi) {
   const int blk = blockIdx.x, b0 = blockIdx.y, k = blockIdx.z;
   const int j = blk * kBiThreads + threadIdx.x;
@@ -106,6 +143,9 @@ __global__ void __launch_bounds__(kBiThreads) bi_ions(BiArgs bi) {
     w = bi.w_per_amp * bi.ib[b0];
   }
   __shared__ double red[kBiThreads / 32][5];
+  __shared__ int cnt[kFieldKeys], base[kFieldKeys], total;
+  __shared__ double fin[2 * kBiThreads], fout[2 * kBiThreads];
+  __shared__ int ev_of[kBiThreads];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int b = b0 + 1; b < bi.nb; ++b) {
     const double dt = (double)(bi.bunch_kb[b] - bi.bunch_kb[b - 1]) * bi.dt_bucket;
@@ -118,19 +158,47 @@ __global__ void __launch_bounds__(kBiThreads) bi_ions(BiArgs bi) {
     for (int m = 0; m < 5; ++m) s[m] = warp_sum(s[m]);
     if (lane == 0)
       for (int m = 0; m < 5; ++m) red[warp][m] = s[m];
+    if (threadIdx.x < kFieldKeys) cnt[threadIdx.x] = 0;
     __syncthreads();
     if (threadIdx.x < 5) {
       double t = 0.0;
       for (int q = 0; q < kBiThreads / 32; ++q) t += red[q][threadIdx.x];
       bi.part[(((size_t)k * bi.T + bi_tri(b) + b0) * bi.bpp + blk) * 5 + threadIdx.x] = t;
     }
+    int v = -1;
+    if (live) {
+      const int key = gauss_field_key(dx, dy, F[2], F[3]);
+      v = (key << 16) | atomicAdd(&cnt[key], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int sum = 0;
+      for (int q = 0; q < kFieldKeys; ++q) {
+        base[q] = sum;
+        sum += cnt[q];
+      }
+      total = sum;
+    }
+    __syncthreads();
+    if (v >= 0) {
+      const int sl = base[v >> 16] + (v & 0xFFFF);
+      fin[2 * sl] = dx;
+      fin[2 * sl + 1] = dy;
+      ev_of[sl] = threadIdx.x;
+    }
+    __syncthreads();
+    if (threadIdx.x < total) {
+      const int e = ev_of[threadIdx.x];
+      double gx, gy;
+      gauss_field(fin[2 * threadIdx.x], fin[2 * threadIdx.x + 1], F[2], F[3], gx, gy);
+      fout[2 * e] = gx;
+      fout[2 * e + 1] = gy;
+    }
     __syncthreads();
     if (live) {
-      double gx, gy;
-      gauss_field(dx, dy, F[2], F[3], gx, gy);
       const double kk = bi.kion_per_amp * bi.ib[b];
-      vx = vx + kk * gx;
-      vy = vy + kk * gy;
+      vx = vx + kk * fout[2 * threadIdx.x];
+      vy = vy + kk * fout[2 * threadIdx.x + 1];
     }
   }
 }
@@ -169,43 +237,115 @@ __global__ void __launch_bounds__(kBiThreads) bi_clouds(BiArgs bi) {
   }
 }
 
+constexpr int kKickChunk = 64;   // electrons per pass of bi_kick_grouped
+// shared memory of bi_kick_grouped for n_ip points
+__host__ __device__ constexpr size_t bi_kick_grouped_smem(int n_ip) {
+  return (size_t)kKickChunk * n_ip * (4 * sizeof(double) + 2 * sizeof(int));
+}
+
 // Every electron of a tile: the deflection by each cloud its bunch meets,
 // at that point's coordinates, mapped back to the kick point
-// (x += -beta s theta, x' += (c + alpha s) theta).
-__global__ void __launch_bounds__(kBiThreads) bi_kick(Args a, BiArgs bi) {
+// (x += -beta s theta, x' += (c + alpha s) theta).  The field evaluations
+// of 64 electrons at all points are gathered first and sorted by the
+// TOMS 680 branches they take (a counting sort in shared memory), so that
+// the warps evaluate runs of one branch; the kicks are then summed per
+// electron over the points in order.
+__global__ void __launch_bounds__(kBiThreads) bi_kick_grouped(Args a, BiArgs bi) {
   const Tile tile = a.tiles[blockIdx.x];
   const int b = tile.bunch;
   __shared__ double cl[kBiMaxIp][5];
-  __shared__ double tr[kBiMaxIp][4];
-  for (int i = threadIdx.x; i < bi.n_ip; i += kBiThreads) {
-    const double *C = bi.cloud + ((size_t)i * bi.nb + b) * 5;
-    cl[i][0] = bi.ke * C[0];
-    for (int m = 1; m < 5; ++m) cl[i][m] = C[m];
-    for (int m = 0; m < 4; ++m) tr[i][m] = bi.trig[4 * i + m];
+  __shared__ double tr[kBiMaxIp][4];   // mx, sxb, my, syb of the point
+  __shared__ int cnt[kFieldKeys], base[kFieldKeys];
+  extern __shared__ double dsm[];
+  const int nk = bi.n_ip, ne = kKickChunk * nk;
+  double *buf = dsm;                                      // ne x 2 by evaluation: offsets, then fields
+  double *in = dsm + 2 * ne;                              // ne x 2 by slot: offsets
+  int *key_rank = reinterpret_cast<int *>(dsm + 4 * ne);  // ne by evaluation: key << 16 | rank, -1 none
+  int *ev_of = key_rank + ne;                             // ne by slot: its evaluation
+  for (int i = threadIdx.x; i < nk; i += kBiThreads) {
+    const double *Cl = bi.cloud + ((size_t)i * bi.nb + b) * 5;
+    cl[i][0] = bi.ke * Cl[0];
+    for (int m = 1; m < 5; ++m) cl[i][m] = Cl[m];
+    const double *T = bi.trig + 4 * i;
+    tr[i][0] = T[0] + bi.alphaH * T[1];
+    tr[i][1] = bi.betaH * T[1];
+    tr[i][2] = T[2] + bi.alphaV * T[3];
+    tr[i][3] = bi.betaV * T[3];
   }
-  __syncthreads();
   const size_t n6 = (size_t)a.npad;
   double *C = a.coord;
-  for (int p = tile.start + threadIdx.x; p < tile.start + tile.count; p += kBiThreads) {
-    const double x = C[1 * n6 + p], z = C[2 * n6 + p], xp = C[4 * n6 + p], zp = C[5 * n6 + p];
-    double ddx = 0.0, ddxp = 0.0, ddz = 0.0, ddzp = 0.0;
-    for (int k = 0; k < bi.n_ip; ++k) {
-      if (cl[k][0] == 0.0) continue;
-      const double mx = tr[k][0] + bi.alphaH * tr[k][1], sxb = bi.betaH * tr[k][1];
-      const double my = tr[k][2] + bi.alphaV * tr[k][3], syb = bi.betaV * tr[k][3];
-      const double xk = mx * x + sxb * xp, zk = my * z + syb * zp;
-      double gx, gy;
-      gauss_field(xk - cl[k][1], zk - cl[k][2], cl[k][3], cl[k][4], gx, gy);
-      const double thx = cl[k][0] * gx, thy = cl[k][0] * gy;
-      ddx = ddx - sxb * thx;
-      ddxp = ddxp + mx * thx;
-      ddz = ddz - syb * thy;
-      ddzp = ddzp + my * thy;
+  for (int c0 = 0; c0 < tile.count; c0 += kKickChunk) {
+    const int nchunk = min(kKickChunk, tile.count - c0);
+    if (threadIdx.x < kFieldKeys) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    // offsets and key of every evaluation e = k kKickChunk + i (point k,
+    // electron i of the chunk); the rank within a key comes from shared
+    // atomics (slot order varies between runs, the results do not)
+    for (int e = threadIdx.x; e < ne; e += kBiThreads) {
+      const int k = e / kKickChunk, i = e % kKickChunk;
+      int v = -1;
+      if (i < nchunk && cl[k][0] != 0.0) {
+        const int p = tile.start + c0 + i;
+        const double x = C[1 * n6 + p], z = C[2 * n6 + p], xp = C[4 * n6 + p], zp = C[5 * n6 + p];
+        const double xk = tr[k][0] * x + tr[k][1] * xp, zk = tr[k][2] * z + tr[k][3] * zp;
+        const double dx = xk - cl[k][1], dy = zk - cl[k][2];
+        buf[2 * e] = dx;
+        buf[2 * e + 1] = dy;
+        const int key = gauss_field_key(dx, dy, cl[k][3], cl[k][4]);
+        v = (key << 16) | atomicAdd(&cnt[key], 1);
+      }
+      key_rank[e] = v;
     }
-    C[1 * n6 + p] = x + ddx;
-    C[4 * n6 + p] = xp + ddxp;
-    C[2 * n6 + p] = z + ddz;
-    C[5 * n6 + p] = zp + ddzp;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int sum = 0;
+      for (int q = 0; q < kFieldKeys; ++q) {
+        base[q] = sum;
+        sum += cnt[q];
+      }
+      cnt[0] = sum;
+    }
+    __syncthreads();
+    const int total = cnt[0];
+    for (int e = threadIdx.x; e < ne; e += kBiThreads) {
+      const int v = key_rank[e];
+      if (v >= 0) {
+        const int sl = base[v >> 16] + (v & 0xFFFF);
+        in[2 * sl] = buf[2 * e];
+        in[2 * sl + 1] = buf[2 * e + 1];
+        ev_of[sl] = e;
+      }
+    }
+    __syncthreads();
+    // the evaluations in slot order: consecutive slots share a key
+    for (int sl = threadIdx.x; sl < total; sl += kBiThreads) {
+      const int e = ev_of[sl], k = e / kKickChunk;
+      double gx, gy;
+      gauss_field(in[2 * sl], in[2 * sl + 1], cl[k][3], cl[k][4], gx, gy);
+      buf[2 * e] = gx;
+      buf[2 * e + 1] = gy;
+    }
+    __syncthreads();
+    // the kicks of each electron, summed over the points in order
+    if (threadIdx.x < nchunk) {
+      const int i = threadIdx.x, p = tile.start + c0 + i;
+      const double x = C[1 * n6 + p], z = C[2 * n6 + p], xp = C[4 * n6 + p], zp = C[5 * n6 + p];
+      double ddx = 0.0, ddxp = 0.0, ddz = 0.0, ddzp = 0.0;
+      for (int k = 0; k < nk; ++k) {
+        if (cl[k][0] == 0.0) continue;
+        const int e = k * kKickChunk + i;
+        const double thx = cl[k][0] * buf[2 * e], thy = cl[k][0] * buf[2 * e + 1];
+        ddx = ddx - tr[k][1] * thx;
+        ddxp = ddxp + tr[k][0] * thx;
+        ddz = ddz - tr[k][3] * thy;
+        ddzp = ddzp + tr[k][2] * thy;
+      }
+      C[1 * n6 + p] = x + ddx;
+      C[4 * n6 + p] = xp + ddxp;
+      C[2 * n6 + p] = z + ddz;
+      C[5 * n6 + p] = zp + ddzp;
+    }
+    __syncthreads();
   }
 }
 

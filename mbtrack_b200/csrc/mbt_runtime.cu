@@ -266,7 +266,7 @@ void enqueue_beam_ion(mbt_ctx *c, bool prof = false) {
   if (prof) cudaEventRecord(c->bi_kev[1], c->stream);
   mbt::bi_clouds<<<dim3(bi.nb, bi.n_ip), mbt::kBiThreads, 0, c->stream>>>(bi);
   if (prof) cudaEventRecord(c->bi_kev[2], c->stream);
-  mbt::bi_kick<<<c->ntile, mbt::kBiThreads, 0, c->stream>>>(c->a, bi);
+  mbt::bi_kick_grouped<<<c->ntile, mbt::kBiThreads, mbt::bi_kick_grouped_smem(bi.n_ip), c->stream>>>(c->a, bi);
 }
 
 // Whether turn `turn` (0-based) ends a scan interval: (rev+1) % NrevScan
@@ -852,6 +852,8 @@ int mbt_enable_beam_ion(mbt_ctx *c, const mbt_beam_ion *cfg) {
     CK(cudaFuncSetAttribute(mbt::bi_ions_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mbt::kMlpCtaSmem));
     CK(cudaFuncSetAttribute(mbt::bi_kick_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mbt::kMlpCtaSmem));
   }
+  CK(cudaFuncSetAttribute(mbt::bi_kick_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)mbt::bi_kick_grouped_smem(cfg->n_ip)));
   bi.trig = tr; bi.mom = mom; bi.frame = frame; bi.part = part; bi.cloud = cloud; bi.ib = ibd;
   bi.bunch_kb = c->a.bunch_kb;
   bi.turn = &c->a.rs->turn;

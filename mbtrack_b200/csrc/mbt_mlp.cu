@@ -3,8 +3,8 @@
 //
 //   mlp_prepare   FP32 master weights -> operand tiles in the swizzled
 //                 K-major layout: BF16 W2/2, W3/2, the layer-1 and bias
-//                 columns, W4/2 with its bias (forward), BF16 W2^T, W3^T
-//                 (backward)
+//                 columns (scaled by c = k/2 of the sigmoid-form GELU),
+//                 W4/k with its bias (forward), BF16 W2^T, W3^T (backward)
 //   mlp_forward   128-point tiles, two tile groups per CTA (256 threads),
 //                 the inference path of mbt_mlp.cuh (every layer a
 //                 tcgen05.mma with BF16 operands and FP32 accumulation in
@@ -71,25 +71,25 @@ __global__ void mlp_prepare(const float *P, uint8_t *W) {
     *reinterpret_cast<__nv_bfloat16 *>(W2T + sw128_elem(k, n)) = __float2bfloat16_rn(P[kMlpW2 + i]);
     *reinterpret_cast<__nv_bfloat16 *>(W3T + sw128_elem(k, n)) = __float2bfloat16_rn(P[kMlpW3 + i]);
     if (i < 128 * 64) {
-      // [128][64]: row r = output r; k 0..2 W1 (for the inputs), 3..5 W1
-      // again (for their low parts), 6, 7 the pair of b1; 16, 17 the pair
-      // of b2; 32, 33 the pair of b3; 48, 49 ones (k-step 3 is the A
-      // operand of every bias step); zeros elsewhere
+      // [128][64]: row r = output r; k 0..2 c W1 (for the inputs), 3..5
+      // c W1 again (for their low parts), 6, 7 the pair of c b1; 16, 17 the
+      // pair of c b2; 32, 33 the pair of c b3; 48, 49 ones (k-step 3 is the
+      // A operand of every bias step); zeros elsewhere
       const int r = i / 64, c = i % 64;
       float v = 0.0f;
-      if (c < 6) v = P[kMlpW1 + 3 * r + (c % 3)];
-      else if (c == 6 || c == 7) v = bf16_pair(P[kMlpB1 + r], c - 6);
-      else if (c == 16 || c == 17) v = bf16_pair(P[kMlpB2 + r], c - 16);
-      else if (c == 32 || c == 33) v = bf16_pair(P[kMlpB3 + r], c - 32);
+      if (c < 6) v = kGeluC * P[kMlpW1 + 3 * r + (c % 3)];
+      else if (c == 6 || c == 7) v = bf16_pair(kGeluC * P[kMlpB1 + r], c - 6);
+      else if (c == 16 || c == 17) v = bf16_pair(kGeluC * P[kMlpB2 + r], c - 16);
+      else if (c == 32 || c == 33) v = bf16_pair(kGeluC * P[kMlpB3 + r], c - 32);
       else if (c == 48 || c == 49) v = 1.0f;
       *reinterpret_cast<__nv_bfloat16 *>(Ext + sw128_elem(r, c)) = __float2bfloat16_rn(v);
     }
     if (i < 16 * 192) {
-      // [16][192]: rows 0, 1 hold W4 / 2 (k < 128) and the pair of b4
+      // [16][192]: rows 0, 1 hold W4 / k (k < 128) and the pair of b4
       // (k = 128, 129); zeros elsewhere
       const int r = i / 192, c = i % 192;
       float v = 0.0f;
-      if (r < 2 && c < 128) v = 0.5f * P[kMlpW4 + 128 * r + c];
+      if (r < 2 && c < 128) v = kGeluInvK * P[kMlpW4 + 128 * r + c];
       else if (r < 2 && (c == 128 || c == 129)) v = bf16_pair(P[kMlpB4 + r], c - 128);
       *reinterpret_cast<__nv_bfloat16 *>(W4f + sw128_chunk_rows(r, c >> 3, 16) + (c & 7) * 2) =
           __float2bfloat16_rn(v);

@@ -24,16 +24,22 @@
 // Numerics of a forward pass (the oracle restates them):
 //   x = (a/4 - 1, b/4 - 1, 1 + 2 ln r / ln 20) in FP32, split into BF16
 //   pairs x = xh + xl;
-//   layer 1:  z1 = W1h xh + W1h xl + (b1h + b1l)   (one K = 16 product: the
-//             inputs, their low parts and two bias columns of ones)
-//   hidden:   h' = z (1 + tanh(z (c1 + c1c2 z^2))) = 2 gelu(z) in BF16 pair
-//             arithmetic, c1 = sqrt(2/pi), c2 = 0.044715 (BF16 constants,
-//             hardware tanh); the 1/2 of GELU is folded into the next
-//             layer's weights (exact in BF16):
-//   layers 2, 3:  z = (W/2)h h' + (bh + bl)   (8 k-steps of the activation
+//   GELU in its sigmoid form, gelu(z) = z sigma(k z), k = 1.702 (the
+//   second approximation of Hendrycks and Gimpel's GELU paper), with
+//   c = k/2 folded into each hidden layer's product, which then gives
+//   w = c z, and the activation
+//     h' = w (1 + tanh w) = k gelu(z)
+//   in BF16 pair arithmetic (one conversion, one hardware tanh, one FMA
+//   per pair of values); the 1/k is folded into the next layer, whose
+//   product c z' = c (W gelu(z) + b') is then (W/2) h' + c b':
+//   layer 1:  w1 = (c W1)h xh + (c W1)h xl + pair(c b1)   (one K = 16
+//             product: the inputs, their low parts and two bias columns of
+//             ones)
+//   layers 2, 3:  w = (W/2)h h' + pair(c b)   (8 k-steps of the activation
 //             tile and one of a column pair of ones against the bias columns)
-//   output:   Y = (W4/2)h h3' + (b4h + b4l)   (N = 16, rows 2.. zero)
-// with Wh = W rounded to BF16, bh + bl the BF16 pair of a bias, FP32 sums.
+//   output:   Y = (W4/k)h h3' + pair(b4)   (N = 16, rows 2.. zero)
+// with Wh = W rounded to BF16, pair(b) = bh + bl the BF16 pair of a bias,
+// FP32 sums.
 //
 // Tiles: 128 points per MMA tile (M = 128, N = 128 or 16, K = 16 per
 // instruction) in the canonical K-major 128-byte-swizzled layout: a
@@ -191,28 +197,23 @@ __device__ __forceinline__ float tanh_hw(float x) {
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
-constexpr float kGeluC1 = 0.7978845608028654f, kGeluC1C2 = 0.035677408136300125f;
-// derivative of gelu(x) = x (1 + tanh(x (c1 + c1c2 x^2))) / 2 (FP32)
+// GELU in its sigmoid form: gelu(z) = z sigma(k z) = z (1 + tanh(c z)) / 2.
+// kGeluInvK and kGeluInvC are 1/k and 1/c rounded to FP32.
+constexpr float kGeluK = 1.702f, kGeluC = 0.851f, kGeluInvK = 0.58754406f, kGeluInvC = 1.1750881f;
+// derivative of gelu(x) (FP32): s + k x s (1 - s), s = sigma(k x)
 __device__ __forceinline__ float gelu_grad(float x) {
-  const float y = x * fmaf(kGeluC1C2, x * x, kGeluC1);
-  const float th = tanh_hw(y);
-  return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * 0.7978845608028654f * (1.0f + 0.134145f * x * x);
+  const float s = 0.5f + 0.5f * tanh_hw(kGeluC * x);
+  return s + kGeluK * x * s * (1.0f - s);
 }
 
-// The activation of a pair of pre-activations in BF16 pair arithmetic, one
-// instruction per step for both values and one hardware tanh per pair:
-//   z = bf16(z),  y = z (c1 + c1c2 z^2),  h' = z + z tanh(y) = 2 gelu(z),
-// with the BF16 constants c1 = 0x3F4C, c1c2 = 0x3D12 and every step rounded
-// to BF16.  Returns the BF16 pair (low half from z0).
-constexpr uint32_t kB2C1 = 0x3F4C3F4Cu, kB2C1C2 = 0x3D123D12u;
-__device__ __forceinline__ uint32_t act_bf16x2(float z0, float z1) {
-  uint32_t z, t, p, y, th, h;
-  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(z) : "f"(z1), "f"(z0));
-  asm("mul.rn.bf16x2 %0, %1, %1;" : "=r"(t) : "r"(z));
-  asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(p) : "r"(t), "r"(kB2C1C2), "r"(kB2C1));
-  asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(y) : "r"(z), "r"(p));
-  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(th) : "r"(y));
-  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(h) : "r"(z), "r"(th));
+// The activation of a pair of scaled pre-activations w = c z in BF16 pair
+// arithmetic: w = bf16(w), h' = w + w tanh(w) = k gelu(z), each step
+// rounded to BF16, hardware tanh.  Returns the BF16 pair (low half from w0).
+__device__ __forceinline__ uint32_t act_bf16x2(float w0, float w1) {
+  uint32_t w, th, h;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(w) : "f"(w1), "f"(w0));
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(th) : "r"(w));
+  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(h) : "r"(w), "r"(th));
   return h;
 }
 __device__ __forceinline__ void unpack_bf16x2(uint32_t h, float &lo, float &hi) {
@@ -314,7 +315,7 @@ __device__ __forceinline__ void mlp_input_row(const MlpGroup &G, const float *x)
 
 // 16 accumulator columns (k0 .. k0+15) -> activation -> two chunks of row t
 // of the activation tile; zs / hs (may be null) receive the pre-activations
-// and the activations gelu(z) = h'/2.
+// z = w/c and the activations gelu(z) = h'/k.
 __device__ __forceinline__ void mlp_act16(const MlpGroup &G, int k0, const float *v, float *zs, float *hs) {
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
@@ -326,13 +327,13 @@ __device__ __forceinline__ void mlp_act16(const MlpGroup &G, int k0, const float
         make_uint4(h[0], h[1], h[2], h[3]);
     if (zs) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) zs[k0 + 8 * c + i] = v[8 * c + i];
+      for (int i = 0; i < 8; ++i) zs[k0 + 8 * c + i] = kGeluInvC * v[8 * c + i];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         float lo, hi;
         unpack_bf16x2(h[i], lo, hi);
-        hs[k0 + 8 * c + 2 * i] = 0.5f * lo;
-        hs[k0 + 8 * c + 2 * i + 1] = 0.5f * hi;
+        hs[k0 + 8 * c + 2 * i] = kGeluInvK * lo;
+        hs[k0 + 8 * c + 2 * i + 1] = kGeluInvK * hi;
       }
     }
   }

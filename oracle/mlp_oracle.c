@@ -2,10 +2,14 @@
  * mlp_oracle.c -- TEST INFRASTRUCTURE ONLY: CPU restatement of the learned
  * field network of libmbt (mbt.h, mbt_mlp_*): forward pass and gradient
  * with the same roundings of the tensor-core operands (BF16 pairs of the
- * inputs and biases, BF16 weights, W/2 after a hidden layer, activations
- * h' = 2 gelu(z) in BF16 pair arithmetic in the forward pass; BF16
- * operands of the backward products), sums in double.  Used by tests/ to
- * check the GPU kernels.
+ * inputs and biases, BF16 weights, activations h' = k gelu(z) in BF16 pair
+ * arithmetic in the forward pass; BF16 operands of the backward products),
+ * sums in double.  Used by tests/ to check the GPU kernels.
+ *
+ * GELU in its sigmoid form gelu(z) = z sigma(k z) = z (1 + tanh(c z)) / 2,
+ * k = 1.702, c = k/2.  The kernels fold c into each hidden layer's weights
+ * and bias (the product is w = c z), compute h' = w (1 + tanh w) = k gelu(z)
+ * and fold 1/k into the next layer: W2/2, W3/2 (c/k = 1/2) and W4/k.
  */
 #include <math.h>
 #include <stdint.h>
@@ -47,26 +51,27 @@ static float rbf(double v)
   return (float) (nearbyint(v / q) * q);
 }
 
-/* The activation of the forward pass (act_bf16x2): every step rounded to
- * BF16, BF16 constants c1 = 0x3F4C, c1c2 = 0x3D12; the GPU's tanh is the
+#define GELU_K 1.702f
+#define GELU_C 0.851f
+#define GELU_INV_K 0.58754406f
+#define GELU_INV_C 1.1750881f
+
+/* The activation of the forward pass (act_bf16x2) of a scaled
+ * pre-activation x = c z: every step rounded to BF16; the GPU's tanh is the
  * hardware approximation, this restatement libm's tanh rounded to BF16.
- * Returns h' = 2 gelu(z). */
+ * Returns h' = k gelu(z). */
 static float act(float x)
 {
-  const double c1 = 0.796875, c1c2 = 0.03564453125;
-  const double z = rbf(x);
-  const double t = rbf(z * z);
-  const double p = rbf(t * c1c2 + c1);
-  const double y = rbf(z * p);
-  const double th = rbf(tanh(y));
-  return rbf(z * th + z);
+  const double w = rbf(x);
+  const double th = rbf(tanh(w));
+  return rbf(w * th + w);
 }
 
+/* derivative of gelu(x) = x sigma(k x): s + k x s (1 - s) */
 static float gelu_grad(float x)
 {
-  const float y = x * fmaf(0.035677408136300125f, x * x, 0.7978845608028654f);
-  const float th = tanhf(y);
-  return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * 0.7978845608028654f * (1.0f + 0.134145f * x * x);
+  const float s = 0.5f + 0.5f * tanhf(GELU_C * x);
+  return s + GELU_K * x * s * (1.0f - s);
 }
 
 
@@ -81,7 +86,8 @@ static double bias_pair(float b)
   return (double) hi + (double) bf16r(b - hi);
 }
 
-/* One point: the saved activations are gelu(z) = h' / 2. */
+/* One point: the saved pre-activations are z = w / c, the saved
+ * activations gelu(z) = h' / k. */
 static void forward_one(const float *P, const float *abr, fwd_t *f)
 {
   int i, j, k;
@@ -94,33 +100,29 @@ static void forward_one(const float *P, const float *abr, fwd_t *f)
     xl[i] = bf16r(f->x[i] - xh[i]);
   }
   for (j = 0; j < H; j++) {
-    double s = bias_pair(P[B1 + j]);
-    for (i = 0; i < 3; i++) s += (double) bf16r(P[W1 + 3 * j + i]) * ((double) xh[i] + (double) xl[i]);
-    f->z1[j] = (float) s;
-    h[j] = act(f->z1[j]);
-    f->h1[j] = 0.5f * h[j];
+    double s = bias_pair(GELU_C * P[B1 + j]);
+    for (i = 0; i < 3; i++) s += (double) bf16r(GELU_C * P[W1 + 3 * j + i]) * ((double) xh[i] + (double) xl[i]);
+    h[j] = act((float) s);
+    f->z1[j] = GELU_INV_C * (float) s;
+    f->h1[j] = GELU_INV_K * h[j];
   }
   for (j = 0; j < H; j++) {
-    double s = bias_pair(P[B2 + j]);
+    double s = bias_pair(GELU_C * P[B2 + j]);
     for (k = 0; k < H; k++) s += (double) h[k] * (double) bf16r(0.5f * P[W2 + H * j + k]);
-    f->z2[j] = (float) s;
+    hn[j] = act((float) s);
+    f->z2[j] = GELU_INV_C * (float) s;
+    f->h2[j] = GELU_INV_K * hn[j];
   }
   for (j = 0; j < H; j++) {
-    hn[j] = act(f->z2[j]);
-    f->h2[j] = 0.5f * hn[j];
-  }
-  for (j = 0; j < H; j++) {
-    double s = bias_pair(P[B3 + j]);
+    double s = bias_pair(GELU_C * P[B3 + j]);
     for (k = 0; k < H; k++) s += (double) hn[k] * (double) bf16r(0.5f * P[W3 + H * j + k]);
-    f->z3[j] = (float) s;
-  }
-  for (j = 0; j < H; j++) {
-    h[j] = act(f->z3[j]);
-    f->h3[j] = 0.5f * h[j];
+    h[j] = act((float) s);
+    f->z3[j] = GELU_INV_C * (float) s;
+    f->h3[j] = GELU_INV_K * h[j];
   }
   for (j = 0; j < 2; j++) {
     double s = bias_pair(P[B4 + j]);
-    for (k = 0; k < H; k++) s += (double) h[k] * (double) bf16r(0.5f * P[W4 + H * j + k]);
+    for (k = 0; k < H; k++) s += (double) h[k] * (double) bf16r(GELU_INV_K * P[W4 + H * j + k]);
     f->out[j] = (float) s;
   }
 }

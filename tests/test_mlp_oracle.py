@@ -26,8 +26,8 @@ def _params(seed):
 
 
 def _fp64_network(p, x):
-    def gelu(z):
-        return 0.5 * z * (1 + np.tanh(0.7978845608028654 * (z + 0.044715 * z ** 3)))
+    def gelu(z):     # sigmoid form z sigma(1.702 z)
+        return z / (1 + np.exp(-1.702 * z))
     f = np.stack([x[:, 0] / 4 - 1, x[:, 1] / 4 - 1, 1 + 2 * np.log(x[:, 2]) / np.log(20)], 1).astype(float)
     W1, b1 = p[0:384].reshape(128, 3), p[384:512]
     W2, b2 = p[512:16896].reshape(128, 128), p[16896:17024]

@@ -360,7 +360,9 @@ def run_b200(args):
         if audit is not None:
             bi_info["audit"] = {"audited": int(audit[0]), "max_rel_error": float(audit[1]),
                                 "rms_rel_error": float(audit[2]), "faddeeva_fallbacks": int(audit[3]),
-                                "tensor_failures": int(audit[4])}
+                                "tensor_failures": int(audit[4]),
+                                "fallback_fraction": int(audit[3]) / float(bi_info["field_evaluations_per_turn"]
+                                                                           * args.steps)}
             # network FLOPs: 2 x (3x128 + 2x128x128 + 128x2) per evaluation
             tfl = 66816.0 * bi_info["field_evaluations_per_turn"] / (bi_ms * 1e-3) / 1e12
             bi_info["network_tflops"] = tfl
@@ -408,6 +410,9 @@ def run_b200(args):
                    "parallelism": "replicas x%d" % world},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
+                     "traffic_source": (None if traffic is None else
+                                        "dram__bytes_read.sum + dram__bytes_write.sum of one launch from the "
+                                        "committed ncu summary in profiles/ (not measured by this run)"),
                      "kernel": "turn_map (particle pass)", "peak_source": peak_kind,
                      "bytes_per_launch": BYTES_PER_MP_TURN * npart, "launch_ms": k1_ms},
         "kernels_ms_per_turn": {"turn_map": k1_ms, "bunch_reduce": float(prof[1]),
@@ -748,6 +753,7 @@ def beam_ion_record(args, tmp):
             a = trk.beam_ion_audit()
             r["audit"] = {"audited": int(a[0]), "max_rel_error": float(a[1]), "rms_rel_error": float(a[2]),
                           "faddeeva_fallbacks": int(a[3]), "tensor_failures": int(a[4]),
+                          "fallback_fraction": int(a[3]) / float(evals * args.bi_steps),
                           "error": "|F_learned - F_Faddeeva| / |F_Faddeeva| of the field vector, a hashed 1% "
                                    "of the warps each turn"}
         trk.profile(2)
@@ -763,7 +769,11 @@ def beam_ion_record(args, tmp):
                                          "the Faddeeva field (device time, same beam, ions and seeds)")
     # network arithmetic: 2 x (3x128 + 2x128x128 + 128x2) = 66816 FLOP per evaluation
     rec["learned"]["network_tflops"] = 66816.0 * runs["learned"]["field_evaluations_per_s"] / 1e12
-    rec["faddeeva"]["fp64_pipe_active"] = {"value": 0.355, "from": "profiles/beam_ion_faddeeva.md (ncu, small case)"}
+    rec["faddeeva"]["fp64_pipe_active"] = {"value": 0.30, "from": "profiles/beam_ion_faddeeva.md (ncu, small case: "
+                                                         "bi_ions 0.313, bi_kick_grouped 0.275, weighted by "
+                                                         "their full-size times)"}
+    rec["learned"]["xu_pipe_active"] = {"value": 0.69, "from": "profiles/beam_ion_learned_field.md (ncu, small case: "
+                                                      "bi_ions_mlp 0.69, bi_kick_mlp 0.59)"}
     if args.growth_turns_bi > 0:
         rec["growth_check"] = growth_check(cfg, mlp, args.growth_turns_bi)
     mlp.close()

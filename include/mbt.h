@@ -425,9 +425,8 @@ int mbt_bunch_moments_dev(int np, const double *coord_dev, double sigma_tau,
  * Its scratch is a fixed 2 MiB device array inside libmbt, present on every
  * GPU that loads the library until the process exits; each call looks up
  * that array's address on the current device, and the first call on a
- * device also loads libmbt's device code there, so make it before any
- * stream capture.  Calls share the array: calls that overlap on the GPU
- * race.  ncell is limited to MBT_NOALLOC_MAX_NCELL (larger values return
+ * device also loads libmbt's device code there.  Calls share the array:
+ * calls that overlap on the GPU race.  ncell is limited to MBT_NOALLOC_MAX_NCELL (larger values return
  * MBT_ERR_INVALID); np is not limited.  It calls no allocator. */
 #define MBT_NOALLOC_MAX_NCELL 1024
 int mbt_bunch_moments_dev_noalloc(int np, const double *coord_dev,

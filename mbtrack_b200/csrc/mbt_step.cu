@@ -195,8 +195,8 @@ extern "C" int mbt_bunch_moments_dev(int np, const double *coord_dev, double sig
 // only valid there) and passes it to the kernels; a lookup allocates
 // nothing, and looking up on every call keeps the address right after a
 // cudaDeviceReset has reloaded the module.  The first call on a device also
-// loads the module's device code and data there, so make it before any
-// stream capture.  Every call uses the same array and leaves its contents
+// loads the module's device code and data there.  Every call uses the same
+// array and leaves its contents
 // behind; each call writes every element it later reads (partial records,
 // then the result area), so nothing has to be cleared.  Two calls whose
 // work overlaps on the GPU (different streams, or different host threads on

@@ -196,9 +196,9 @@ extern "C" int mbt_bunch_moments_dev(int np, const double *coord_dev, double sig
 // nothing, and looking up on every call keeps the address right after a
 // cudaDeviceReset has reloaded the module.  The first call on a device also
 // loads the module's device code and data there.  Every call uses the same
-// array and leaves its contents
-// behind; each call writes every element it later reads (partial records,
-// then the result area), so nothing has to be cleared.  Two calls whose
+// array and leaves its contents behind; each call writes every element it
+// later reads (partial records, then the result area), so nothing has to be
+// cleared.  Two calls whose
 // work overlaps on the GPU (different streams, or different host threads on
 // one device) race on the array.
 

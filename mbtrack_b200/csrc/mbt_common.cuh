@@ -26,6 +26,30 @@ __device__ __forceinline__ int bin_fast(double xtau, double sgm, double nsig, do
   return bin_of(xtau, sgm, nsig, dT);
 }
 
+// Order-independent sums of coordinates.  x enters as floor(x 2^70) =
+// hi 2^32 + lo with hi = floor(x 2^38) and lo in [0, 2^32), each summed by a
+// 64-bit integer atomic: integer sums do not depend on the order of the
+// additions, so the sums repeat bit for bit.  Each particle is truncated to
+// 2^-70 m (below the FP64 rounding of a sum of coordinates near 1e-4 m).
+// The hi sum is exact while the sum of |x| stays below 2^25 m; the lo sum
+// stays below 2^63 for fewer than 2^31 particles.  A coordinate with
+// |x| >= 2^10 m, or NaN, sets bit 63 of lo instead (an OR, which commutes
+// with the additions since they never carry into that bit): the sum is
+// then NaN.
+__device__ __forceinline__ void fx70_add(unsigned long long *hi, unsigned long long *lo, double x) {
+  if (fabs(x) < 0x1p10) {
+    const double s = x * 0x1p38, f = floor(s);   // both exact; s - f in [0, 1) exact
+    atomicAdd(hi, (unsigned long long)__double2ll_rz(f));
+    atomicAdd(lo, (unsigned long long)__double2uint_rz((s - f) * 0x1p32));
+  } else {
+    atomicOr(lo, 1ull << 63);
+  }
+}
+__device__ __forceinline__ double fx70_value(unsigned long long hi, unsigned long long lo) {
+  if (lo >> 63) return __longlong_as_double(0x7FF8000000000000LL);
+  return (double)(long long)hi * 0x1p-38 + (double)lo * 0x1p-70;
+}
+
 // sin and cos of (a + d) from S = sin a, C = cos a and a small offset
 // |d| <= 0.25: angle addition, with sin d and cos d - 1 from their Taylor
 // series, to d^11 and d^12 in general and to d^7 and d^8 for |d| <= 0.04

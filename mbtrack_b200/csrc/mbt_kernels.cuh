@@ -180,9 +180,10 @@ constexpr int kStages = MBT_MAP_STAGES;
 constexpr int kMapThreads = kBlock + 32;   // 8 compute warps + 1 producer warp
 constexpr long kWaitLimit = 1L << 24;      // polls before a wait is declared failed
 
-// stages, kick tables and histograms
-__host__ __device__ constexpr size_t turn_map_smem(int nc) {
-  return (size_t)kStages * 6 * kChunk * sizeof(double) + (size_t)nc * 5 * sizeof(double) +
+// stages, kick tables and histograms (with the dipole histograms: two
+// fixed-point words for each of x and z per bin)
+__host__ __device__ constexpr size_t turn_map_smem(int nc, bool histxz = false) {
+  return (size_t)kStages * 6 * kChunk * sizeof(double) + (size_t)nc * (histxz ? 7 : 5) * sizeof(double) +
          (size_t)nc * sizeof(int);
 }
 
@@ -202,13 +203,15 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
   double *kL = smem + kStages * 6 * kChunk;
   double *kV = kL + nc;
   double *kH = kL + 2 * nc;
-  double *hx = kL + 3 * nc;
-  double *hz = kL + 4 * nc;
-  int *hc = reinterpret_cast<int *>(kL + 5 * nc);
+  // dipole histograms: fixed-point sums of x (hi, lo words) and z per bin
+  unsigned long long *fxh = reinterpret_cast<unsigned long long *>(kL + 3 * nc);
+  unsigned long long *fxl = fxh + nc, *fzh = fxh + 2 * nc, *fzl = fxh + 3 * nc;
+  int *hc = reinterpret_cast<int *>(kL + (HISTXZ ? 7 : 5) * nc);
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ __align__(8) uint64_t empty[kStages];
   __shared__ double red[14];
-  __shared__ double trash[6];
+  __shared__ double trash_n[2];                 // out-of-range particles below / above the bins
+  __shared__ unsigned long long trash_fx[8];    // their x and z, fixed-point (hi, lo) pairs
   __shared__ double shift[6];
 
   const bool sf = MOVE && a.selffield;
@@ -219,12 +222,11 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
       kH[i] = a.kick[(size_t)(b * 3 + 2) * nc + i];
     }
     hc[i] = 0;
-    if (HISTXZ) { hx[i] = 0.0; hz[i] = 0.0; }
+    if (HISTXZ) fxh[i] = fxl[i] = fzh[i] = fzl[i] = 0ull;
   }
-  if (threadIdx.x < 6) {
-    trash[threadIdx.x] = 0.0;
-    shift[threadIdx.x] = a.shift[b * 6 + threadIdx.x];
-  }
+  if (threadIdx.x < 8) trash_fx[threadIdx.x] = 0ull;
+  if (threadIdx.x < 2) trash_n[threadIdx.x] = 0.0;
+  if (threadIdx.x < 6) shift[threadIdx.x] = a.shift[b * 6 + threadIdx.x];
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
@@ -336,14 +338,14 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
           atomicAdd(&hc[ic], 1);
 #endif
           if (HISTXZ) {
-            atomicAdd(&hx[ic], x);
-            atomicAdd(&hz[ic], z);
+            fx70_add(&fxh[ic], &fxl[ic], x);
+            fx70_add(&fzh[ic], &fzl[ic], z);
           }
         } else if (live) {
-          double *t = trash + (ic < 0 ? 0 : 3);
-          atomicAdd(&t[0], 1.0);
-          atomicAdd(&t[1], x);
-          atomicAdd(&t[2], z);
+          unsigned long long *t = trash_fx + (ic < 0 ? 0 : 4);
+          atomicAdd(&trash_n[ic < 0 ? 0 : 1], 1.0);   // integer counts: exact in any order
+          fx70_add(&t[0], &t[1], x);
+          fx70_add(&t[2], &t[3], z);
         }
       }
     }
@@ -410,14 +412,19 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
   named_barrier(1, kBlock);
   double *rec = a.part + (size_t)blockIdx.x * a.prec;
   if (threadIdx.x < kPartialExtra) {
-    const double sum = threadIdx.x < 6 ? trash[threadIdx.x] : red[threadIdx.x - 6];
+    // out-of-range extras: count, x sum, z sum below the bins, then above
+    const int q = threadIdx.x % 3, side = threadIdx.x / 3;
+    double sum;
+    if (threadIdx.x >= 6) sum = red[threadIdx.x - 6];
+    else if (q == 0) sum = trash_n[side];
+    else sum = fx70_value(trash_fx[4 * side + 2 * (q - 1)], trash_fx[4 * side + 2 * (q - 1) + 1]);
     rec[a.hoff + threadIdx.x] = sum;
   }
   for (int i = threadIdx.x; i < nc; i += kBlock) {
     rec[i] = (double)hc[i];
     if (HISTXZ) {
-      rec[nc + i] = hx[i];
-      rec[2 * nc + i] = hz[i];
+      rec[nc + i] = fx70_value(fxh[i], fxl[i]);
+      rec[2 * nc + i] = fx70_value(fzh[i], fzl[i]);
     }
   }
 }

@@ -209,11 +209,11 @@ int validate(mbt_ctx *c, const mbt_params *p, int nbunch, const int *bucket, con
 
 template <bool MOVE, int NOISE, bool HISTXZ>
 void launch_map(mbt_ctx *c) {
-  const size_t sm = mbt::turn_map_smem(c->nc);
+  const size_t sm = mbt::turn_map_smem(c->nc, HISTXZ);
   static bool attr_set = false;   // per instantiation, per process
   if (!attr_set) {
     cudaFuncSetAttribute(mbt::turn_map<MOVE, NOISE, HISTXZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)mbt::turn_map_smem(MBT_MAX_NCELL));
+                         (int)mbt::turn_map_smem(MBT_MAX_NCELL, HISTXZ));
     attr_set = true;
   }
   mbt::turn_map<MOVE, NOISE, HISTXZ><<<c->ntile, mbt::kMapThreads, sm, c->stream>>>(c->a);

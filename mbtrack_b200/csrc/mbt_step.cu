@@ -27,10 +27,15 @@ __global__ void __launch_bounds__(kThreads)
 moments_partial(int np, const double *__restrict__ c, size_t ld, double sgm, double nsig, double dT, int nc,
                 double *__restrict__ part, int prec) {
   extern __shared__ double sh[];
-  double *hx = sh, *hz = sh + nc;
-  int *hc = reinterpret_cast<int *>(sh + 2 * nc);
+  // x and z sums per bin as fixed-point (hi, lo) integer pairs
+  unsigned long long *fxh = reinterpret_cast<unsigned long long *>(sh);
+  unsigned long long *fxl = fxh + nc, *fzh = fxh + 2 * nc, *fzl = fxh + 3 * nc;
+  int *hc = reinterpret_cast<int *>(sh + 4 * nc);
   __shared__ double red[kThreads / 32][kExtra];
-  for (int i = threadIdx.x; i < nc; i += kThreads) { hx[i] = 0.0; hz[i] = 0.0; hc[i] = 0; }
+  for (int i = threadIdx.x; i < nc; i += kThreads) {
+    fxh[i] = fxl[i] = fzh[i] = fzl[i] = 0ull;
+    hc[i] = 0;
+  }
   __syncthreads();
   const size_t n6 = ld;
   double s[6];
@@ -50,8 +55,8 @@ moments_partial(int np, const double *__restrict__ c, size_t ld, double sgm, dou
       const int ic = mbt::bin_of(v[0], sgm, nsig, dT);
       if (ic >= 0 && ic < nc) {
         atomicAdd(&hc[ic], 1);
-        atomicAdd(&hx[ic], v[1]);
-        atomicAdd(&hz[ic], v[2]);
+        mbt::fx70_add(&fxh[ic], &fxl[ic], v[1]);
+        mbt::fx70_add(&fzh[ic], &fzl[ic], v[2]);
       }
     }
   }
@@ -70,8 +75,8 @@ moments_partial(int np, const double *__restrict__ c, size_t ld, double sgm, dou
   }
   for (int i = threadIdx.x; i < nc; i += kThreads) {
     rec[i] = (double)hc[i];
-    rec[nc + i] = hx[i];
-    rec[2 * nc + i] = hz[i];
+    rec[nc + i] = mbt::fx70_value(fxh[i], fxl[i]);
+    rec[2 * nc + i] = mbt::fx70_value(fzh[i], fzl[i]);
   }
 }
 
@@ -133,7 +138,7 @@ int check_args(int np, const double *coord, double sgm, double dT, int ncell, co
 int run_moments(int np, const double *coord, size_t ld, double sgm, double nsig, double dT, int ncell,
                 const int *tp, double *stats, double *hist, cudaStream_t st, double *scratch, int nblk) {
   const int prec = 3 * ncell + kExtra;
-  const size_t smem = (size_t)ncell * (2 * sizeof(double) + sizeof(int));
+  const size_t smem = (size_t)ncell * (4 * sizeof(unsigned long long) + sizeof(int));
   double *part = scratch, *out = scratch + (size_t)nblk * prec;
   moments_partial<<<nblk, kThreads, smem, st>>>(np, coord, ld, sgm, nsig, dT, ncell, part, prec);
   moments_final<<<1, kThreads, 0, st>>>(np, coord, ld, ncell, nblk, part, prec, tp[1] != 0, tp[2] != 0, out);

@@ -325,7 +325,12 @@ int mbt_prepare(mbt_ctx *ctx, double *init_stats);
 int mbt_set_deviates(mbt_ctx *ctx, const float *dev, long nturns);
 
 /* Run nturns turns of the weak-weak loop (worker_weakweak.c:259-394) for
- * all bunches.  stats (may be NULL): nturns x nbunch x 12 doubles. */
+ * all bunches.  stats (may be NULL): nturns x nbunch x 12 doubles.  The
+ * statistics are copied to stats every 8 turns on a second stream while the
+ * next turns run.  A pageable stats buffer is pinned (cudaHostRegister) for
+ * the duration of the call and unpinned before it returns; where pinning is
+ * refused the copies go to pageable memory, which is slower.  The same holds
+ * for the ampinv buffer of mbt_run_turns_ampinv. */
 int mbt_run_turns(mbt_ctx *ctx, long nturns, double *stats);
 
 /* As mbt_run_turns, also returning the amplitude invariants of every turn

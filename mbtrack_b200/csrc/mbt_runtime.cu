@@ -86,6 +86,8 @@ struct mbt_ctx {
   int scan_steps = 0;            // a scan boundary launches scan_currents / scan_rw
   double scan_d_ma = 0.0, scan_d_a = 0.0;   // current steps [mA] per bucket, [A] per bunch
   cudaEvent_t ev[6] = {};
+  cudaStream_t copy_stream = nullptr;   // statistics to the host, beside the turns
+  cudaEvent_t cev[3] = {};              // two units of turns in flight, the copies' tail
   double timing[4] = {0, 0, 0, 0};
   int device = 0;
   int nsm = 148;
@@ -383,9 +385,11 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   cudaGetDeviceProperties(&prop, c->device);
   c->nsm = prop.multiProcessorCount;
   auto bail = [&](int code) { int rc = code; mbt_destroy(c); return rc; };
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(nullptr, MBT_ERR_CUDA, "stream create"));
   for (auto &e : c->ev) cudaEventCreate(&e);
+  for (auto &e : c->cev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
 
   // geometry: bunches padded to 32 particles, tiles inside bunches
   const int t0 = choose_tile(c->np, prop.multiProcessorCount);
@@ -645,6 +649,9 @@ int mbt_destroy(mbt_ctx *c) {
   for (void *p : c->allocs) cudaFree(p);
   if (c->dev) cudaFree(c->dev);
   for (auto &e : c->ev) if (e) cudaEventDestroy(e);
+  for (auto &e : c->cev) if (e) cudaEventDestroy(e);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -998,6 +1005,85 @@ static int run_core(mbt_ctx *c, long nturns, double *stats, double *ampinv, bool
   long turn = rs.turn;
   const long cap = c->a.stats_cap;
   long done = 0;
+  // The statistics (and amplitude invariants) leave the device one unit of
+  // turns at a time (a graph of 8 turns, or a single turn) on the copy
+  // stream, each copy behind the turns that write it and beside the turns
+  // that follow.  A unit's copy is issued only after the next unit has been
+  // enqueued: a copy into pageable host memory returns when it is complete,
+  // and the GPU keeps busy with that next unit meanwhile.  Before a pass
+  // over the statistics ring starts again at slot 0, every copy is issued
+  // and the turns wait for them, so that no slot is overwritten before it
+  // has been copied.
+  const size_t row = (size_t)c->nbunch;
+  struct Unit { long done, slot, n; int ev; };
+  Unit pend[2] = {};
+  int npend = 0;
+  auto issue = [&](const Unit &u) -> int {
+    CK(cudaStreamWaitEvent(c->copy_stream, c->cev[u.ev], 0));
+    if (stats)
+      CK(cudaMemcpyAsync(stats + (size_t)u.done * row * 12, c->a.stats + (size_t)u.slot * row * 12,
+                         (size_t)u.n * row * 12 * sizeof(double), cudaMemcpyDeviceToHost, c->copy_stream));
+    if (ampinv)
+      CK(cudaMemcpyAsync(ampinv + (size_t)u.done * row * 6, c->a.ampinv + (size_t)u.slot * row * 6,
+                         (size_t)u.n * row * 6 * sizeof(double), cudaMemcpyDeviceToHost, c->copy_stream));
+    return 0;
+  };
+  auto unit_enqueued = [&](long at_done, long slot, long n) -> int {
+    if (!stats && !ampinv) return 0;
+    const int ev = npend == 0 ? 0 : 1 - pend[npend - 1].ev;
+    CK(cudaEventRecord(c->cev[ev], c->stream));
+    if (npend == 2) {
+      int r = issue(pend[0]);
+      if (r) return r;
+      pend[0] = pend[1];
+      npend = 1;
+    }
+    pend[npend++] = Unit{at_done, slot, n, ev};
+    return 0;
+  };
+  auto flush = [&]() -> int {
+    for (int i = 0; i < npend; ++i) {
+      int r = issue(pend[i]);
+      if (r) return r;
+    }
+    npend = 0;
+    if (stats || ampinv) {
+      CK(cudaEventRecord(c->cev[2], c->copy_stream));
+      CK(cudaStreamWaitEvent(c->stream, c->cev[2], 0));
+    }
+    return 0;
+  };
+  // The caller's buffers are pinned for the call when they are pageable
+  // (and pinning is allowed), so that the copies run as asynchronous DMA;
+  // otherwise each copy returns when complete, as described above.
+  auto pin = [&](double *p, size_t bytes) -> bool {
+    if (!p || bytes == 0) return false;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if (at.type != cudaMemoryTypeUnregistered) return false;   // already pinned or device memory
+    if (cudaHostRegister(p, bytes, cudaHostRegisterDefault) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    return true;
+  };
+  const bool pinned_s = pin(stats, (size_t)nturns * row * 12 * sizeof(double));
+  const bool pinned_a = pin(ampinv, (size_t)nturns * row * 6 * sizeof(double));
+  struct Unpin {   // on every return: no copy into the buffers left in flight, then unpin
+    mbt_ctx *c;
+    double *s, *a;
+    ~Unpin() {
+      if (!s && !a) return;
+      cudaStreamSynchronize(c->stream);
+      cudaStreamSynchronize(c->copy_stream);
+      if (s) cudaHostUnregister(s);
+      if (a) cudaHostUnregister(a);
+      cudaGetLastError();
+    }
+  } unpin{c, pinned_s ? stats : nullptr, pinned_a ? ampinv : nullptr};
   CK(cudaEventRecord(c->ev[5], c->stream));
   while (done < nturns) {
     // a chunk never crosses a wrap of the statistics buffer, and ends at
@@ -1009,25 +1095,38 @@ static int run_core(mbt_ctx *c, long nturns, double *stats, double *ampinv, bool
       const long left = c->p.nrev_scan - turn % c->p.nrev_scan;   // turns up to the boundary, inclusive
       if (left <= chunk) { chunk = left; boundary = true; }
     }
+    if (slot == 0 && done > 0) {
+      int r = flush();
+      if (r) return r;
+    }
     const long plain = boundary ? chunk - 1 : chunk;
     long t = 0;
+    int r = 0;
     if (use_graph && plain >= 8) {
       const int G = 8;
-      int r = build_graph(c, G);
+      r = build_graph(c, G);
       if (r) return r;
-      for (; t + G <= plain; t += G) CK(cudaGraphLaunch(c->graph, c->stream));
+      for (; t + G <= plain && !r; t += G) {
+        CK(cudaGraphLaunch(c->graph, c->stream));
+        r = unit_enqueued(done + t, slot + t, G);
+      }
     }
-    for (; t < plain; ++t) enqueue_turn(c, nullptr);
-    if (boundary) enqueue_turn(c, nullptr, true);
+    for (; t < plain && !r; ++t) {
+      enqueue_turn(c, nullptr);
+      r = unit_enqueued(done + t, slot + t, 1);
+    }
+    if (boundary && !r) {
+      enqueue_turn(c, nullptr, true);
+      r = unit_enqueued(done + t, slot + t, 1);
+    }
+    if (r) return r;
     CK(cudaGetLastError());
-    if (stats)
-      CK(cudaMemcpyAsync(stats + (size_t)done * c->nbunch * 12, c->a.stats + (size_t)slot * c->nbunch * 12,
-                         (size_t)chunk * c->nbunch * 12 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    if (ampinv)
-      CK(cudaMemcpyAsync(ampinv + (size_t)done * c->nbunch * 6, c->a.ampinv + (size_t)slot * c->nbunch * 6,
-                         (size_t)chunk * c->nbunch * 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     done += chunk;
     turn += chunk;
+  }
+  {
+    int r = flush();
+    if (r) return r;
   }
   CK(cudaEventRecord(c->ev[4], c->stream));
   int r = sync_and_check(c);

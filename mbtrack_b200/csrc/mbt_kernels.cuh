@@ -995,6 +995,42 @@ __global__ void add_pending_rw(Args a, double *out) {
   }
 }
 
+// Whole-beam host layout (bunch b's 6 x np coordinates from pack[b], one
+// coordinate after the other) to the device layout, and back; the export
+// folds in the pending resistive-wall kick as add_pending_rw does.
+__global__ void beam_import(Args a, const long *pack, const double *src) {
+  const size_t n6 = (size_t)a.npad;
+  const int b = blockIdx.y;
+  const int off = a.bunch_off[b], np = a.bunch_np[b];
+  const double *s = src + pack[b];
+  for (int k = 0; k < 6; ++k)
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += gridDim.x * blockDim.x)
+      a.coord[k * n6 + off + j] = s[(size_t)k * np + j];
+}
+
+__global__ void beam_export(Args a, const long *pack, double *dst) {
+  const size_t n6 = (size_t)a.npad;
+  const int b = blockIdx.y;
+  const int off = a.bunch_off[b], np = a.bunch_np[b];
+  const bool pend = a.rw_long && a.rs->turn > 0;
+  double rh = 0.0, rv = 0.0;
+  if (pend) {
+    for (int q = 0; q < kRwSplit; ++q) {
+      rh += a.rw_part[((size_t)b * kRwSplit + q) * 2 + 0];
+      rv += a.rw_part[((size_t)b * kRwSplit + q) * 2 + 1];
+    }
+  }
+  double *d = dst + pack[b];
+  for (int k = 0; k < 6; ++k) {
+    const bool kick = pend && ((k == 4 && a.oc.track_h) || (k == 5 && a.oc.track_v));
+    const double add = k == 4 ? rh : rv;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += gridDim.x * blockDim.x) {
+      const double v = a.coord[k * n6 + off + j];
+      d[(size_t)k * np + j] = kick ? v + add : v;
+    }
+  }
+}
+
 // Current-scan step, first half (tracking_scan_step_worker tracking.c:43-57,
 // called at the end of turn rev when (rev+1) % NrevScan == 0): the bucket
 // currents of the long-range source terms and the bunch currents behind

@@ -72,6 +72,7 @@ struct mbt_ctx {
   double *vbuf = nullptr;
   double *stats_init = nullptr;
   double *xfer = nullptr;        // device staging for exports
+  long *pack = nullptr;          // per bunch: start of its 6 x np coordinates in a whole-beam host buffer
   double *stat_scratch = nullptr; // block partials of mbt_get_stats
   int bi_on = 0;                 // beam-ion stage
   mbt_beam_ion bicfg{};
@@ -570,6 +571,12 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   rc = rc ? rc : dupload(c, &ip, np_v.data(), nbunch); a.bunch_np = ip;
   rc = rc ? rc : dupload(c, &ip, kb_v.data(), nbunch); a.bunch_kb = ip;
   rc = rc ? rc : dupload(c, &ip, c->off.data(), nbunch); a.bunch_off = ip;
+  {
+    std::vector<long> pack(nbunch);
+    long pos = 0;
+    for (int b = 0; b < nbunch; ++b) { pack[b] = pos; pos += 6L * np_v[b]; }
+    rc = rc ? rc : dupload(c, &c->pack, pack.data(), nbunch);
+  }
   rc = rc ? rc : dupload(c, &ip, c->bucket_bunch.data(), p->nharm); a.bucket_bunch = ip;
   double *dp;
   rc = rc ? rc : dupload(c, &dp, c->ib.data(), nbunch); a.bunch_ib = dp;
@@ -668,15 +675,16 @@ int mbt_load_particles(mbt_ctx *c, int ibunch, const double *soa6, int np) {
   return 0;
 }
 
+// The whole beam crosses PCIe as one copy into the staging buffer (host
+// layout: bunch after bunch, 6 x np each), and a kernel moves it to the
+// device layout (coordinate arrays of npad, bunches at their offsets).
 int mbt_load_all(mbt_ctx *c, const double *soa6_all) {
   if (!c || !soa6_all) return MBT_ERR_INVALID;
-  size_t pos = 0;
-  for (int b = 0; b < c->nbunch; ++b) {
-    for (int k = 0; k < 6; ++k)
-      CK(cudaMemcpyAsync(c->a.coord + (size_t)k * c->npad + c->off[b], soa6_all + pos + (size_t)k * c->np[b],
-                         c->np[b] * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    pos += (size_t)6 * c->np[b];
-  }
+  long total = 0;
+  for (int n : c->np) total += n;
+  CK(cudaMemcpyAsync(c->xfer, soa6_all, (size_t)6 * total * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  mbt::beam_import<<<dim3(16, c->nbunch), 256, 0, c->stream>>>(c->a, c->pack, c->xfer);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
@@ -722,17 +730,16 @@ int mbt_get_particles(mbt_ctx *c, int ibunch, double *soa6, int np) {
   return 0;
 }
 
+// The reverse of mbt_load_all: a kernel writes the beam (with the pending
+// resistive-wall kick, as export_all) into the staging buffer in host
+// layout, then one copy.
 int mbt_get_all(mbt_ctx *c, double *soa6_all) {
   if (!c || !soa6_all) return MBT_ERR_INVALID;
-  int r = export_all(c);
-  if (r) return r;
-  size_t pos = 0;
-  for (int b = 0; b < c->nbunch; ++b) {
-    for (int k = 0; k < 6; ++k)
-      CK(cudaMemcpyAsync(soa6_all + pos + (size_t)k * c->np[b], c->xfer + (size_t)k * c->npad + c->off[b],
-                         c->np[b] * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    pos += (size_t)6 * c->np[b];
-  }
+  long total = 0;
+  for (int n : c->np) total += n;
+  mbt::beam_export<<<dim3(16, c->nbunch), 256, 0, c->stream>>>(c->a, c->pack, c->xfer);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(soa6_all, c->xfer, (size_t)6 * total * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }

@@ -133,6 +133,28 @@ def test_ragged_and_tiny_bunches(tmp_path, cuda_device, libmbt):
     t.close()
 
 
+def test_whole_beam_transfers_on_ragged_bunches(tmp_path, cuda_device, libmbt):
+    """mbt_load_all / mbt_get_all (one copy each way and a layout kernel) on
+    bunches of 1 .. 20000 macroparticles: the beam comes back bit for bit,
+    and after some turns with the resistive wall (a pending kick in the
+    slopes) it equals the per-bunch exports."""
+    from tests.util import small_conf as sc
+    cfg = api.Config(sc(tmp_path, "uniform_fill.conf", filling="SINGLE10", Nmlt=3, EnableQuantum=0))
+    np_ = np.array([1, 2, 31, 33, 511, 513, 1025, 4097, 8193, 20000], dtype=np.int32)
+    t = api.Tracker(cfg.params, cfg.bucket, np_, cfg.bunch_currents(), cfg.Gl, cfg.Gv, cfg.Gh)
+    buf = np.random.default_rng(4).normal(0, 1e-3, 6 * int(np_.sum()))
+    t.load_all(buf)
+    assert np.array_equal(t.get_all(), buf)
+    per = [t.get_particles(i) for i in range(cfg.nbunch)]
+    assert np.array_equal(np.concatenate([x.ravel() for x in per]), buf)
+    t.prepare()
+    t.run(4, stats=False)
+    got = t.get_all()
+    per = np.concatenate([t.get_particles(i).ravel() for i in range(cfg.nbunch)])
+    assert np.array_equal(got, per)
+    t.close()
+
+
 def test_single_bunch_full_size_2000_turns(tmp_path, cuda_device, libmbt):
     """Single bunch, 1e5 macroparticles, broadband resonator in three planes,
     noise off, 2000 turns: checked after 1, 10 and 2000 turns."""

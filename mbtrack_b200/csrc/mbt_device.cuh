@@ -23,8 +23,6 @@ constexpr int kMaxLr = 8;          // MBT_MAX_LR
 constexpr int kMaxAhc = 8;         // MBT_MAX_AHC
 constexpr int kPartialExtra = 20;  // 6 out-of-range values + 12 moment sums + 2 cross sums
 constexpr int kBlock = 256;        // threads per block of every kernel
-constexpr int kRwGroup = 4;        // bunches per resistive-wall sum block
-constexpr int kRwSplit = 4;        // parts of the resistive-wall history per bunch
 
 // Offsets inside a partial record (after the 3 x ncell histograms).
 constexpr int kTrLowN = 0, kTrLowX = 1, kTrLowZ = 2;
@@ -125,7 +123,9 @@ struct Args {
   double *bi_mom;             // nbunch x 10: transverse moments for the beam-ion stage, or null
   double *pot;                // watched bunches x 7 x ncell: potential terms of the next turn, or null
   const int *pot_slot;        // nbunch: watch slot or -1
-  double *rw_part;            // nbunch x kRwSplit x 2: partial RW kicks (HOR, VER)
+  double *rw_part;            // nbunch x 2: the pending RW kick (HOR, VER)
+  double *rw_acc;             // rw_nblk x nbunch x 2: its parts, one per block of history steps
+  int rw_nblk;                // blocks of the resistive-wall sums in ring_scan
   double *stats;              // stats_cap x nbunch x 12
   double *ampinv;             // stats_cap x nbunch x 6: ampinv[3], ampinv_cm[3]
   int stats_cap;

@@ -286,10 +286,8 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
   double rwH = 0.0, rwV = 0.0;
   const bool rw = MOVE && a.rw_long && turn > 0;
   if (rw) {
-    for (int q = 0; q < kRwSplit; ++q) {
-      rwH += a.rw_part[((size_t)b * kRwSplit + q) * 2 + 0];
-      rwV += a.rw_part[((size_t)b * kRwSplit + q) * 2 + 1];
-    }
+    rwH = a.rw_part[(size_t)b * 2 + 0];
+    rwV = a.rw_part[(size_t)b * 2 + 1];
   }
   const bool kick_l = sf && a.lr_kick[0];
   const bool kick_h = sf && a.lr_kick[1];
@@ -606,99 +604,65 @@ __device__ __forceinline__ void rffb_store(Args &a, int slot, double vr, double 
 }
 
 // Long-range resistive wall (transform_weak.c:779-833) of the turn just
-// completed, applied at the start of the next particle pass.  Bunch b sums
-// w_m E[base_b + m - 1], m = 1 .. (Nmlt+1) h, over consecutive slots of the
-// dipole history (E = dipole x bucket current, empty buckets 0), with
-// base_b = base_b0 + (kb_b - kb_b0).  A block serves kRwGroup consecutive
-// bunches and one of kRwSplit parts of the m range: it stages that part of
-// the history once in shared memory.  The kRwSplit partial kicks of a bunch
-// are summed, in order, by the particle pass.
-
-__host__ __device__ constexpr size_t rw_window_doubles(int Nmlt, int nharm) {
-  return (size_t)2 * (((size_t)(Nmlt + 1) * nharm + kRwSplit - 1) / kRwSplit + nharm);
+// completed, applied at the start of the next particle pass.  The kick of
+// bunch b sums E(step j of b) rsq[j + 1] over the (Nmlt + 1) h history
+// steps j (E = dipole x bucket current, empty buckets 0), where step j of
+// bunch b is the cyclic history slot -turn h + kb_b + 1 + j.
+// The bunches' windows are one window shifted by their bucket offsets, so
+// each block of the sums takes a range of steps for every bunch: it stages
+// that range of the history (plus the bunches' bucket span) and the
+// weights once, and each thread sums whole bunches.  rw_steps_per_block:
+// the length of a block's range for nblk blocks.
+__host__ __device__ constexpr int rw_steps_per_block(int Nmlt, int nharm, int nblk) {
+  return ((Nmlt + 1) * nharm + nblk - 1) / nblk;
+}
+__host__ __device__ constexpr size_t rw_window_doubles(int per, int nharm) {
+  return (size_t)2 * (per + nharm) + per;
 }
 
 // Dynamic shared memory of ring_scan (doubles): block 0 keeps 2 doubles and
-// one int per bucket, the resistive-wall blocks their window.
-__host__ __device__ constexpr size_t ring_scan_smem_doubles(int rw_long, int Nmlt, int nharm) {
+// one int per bucket, the resistive-wall blocks their window and weights.
+__host__ __device__ constexpr size_t ring_scan_smem_doubles(int rw_long, int Nmlt, int nharm, int rw_nblk) {
   const size_t scan = 2 * (size_t)nharm + ((size_t)nharm + 1) / 2 + 1;
-  const size_t rw = rw_long ? rw_window_doubles(Nmlt, nharm) : 0;
+  const size_t rw = rw_long && rw_nblk > 0 ? rw_window_doubles(rw_steps_per_block(Nmlt, nharm, rw_nblk), nharm) : 0;
   return scan > rw ? scan : rw;
 }
 
+// Block blk of a.rw_nblk: steps [q0, q1) of every bunch, times the kick
+// constant of the plane, into rw_acc[blk][bunch][plane].
 __device__ void rw_partial_sums(const Args &a, int blk, double *win) {
-  const int ngroup = (a.nbunch + kRwGroup - 1) / kRwGroup;
-  const int grp = blk % ngroup, part = blk / ngroup;
-  const int b0 = grp * kRwGroup, b1 = min(b0 + kRwGroup, a.nbunch);
   const long turn = a.rs->turn;              // the turn just completed (advanced by bunch_wakes)
   const int h = a.nharm;
   const int n = (a.Nmlt + 2) * h;
   const int M = (a.Nmlt + 1) * h;
-  const int per = (M + kRwSplit - 1) / kRwSplit;
-  const int q0 = part * per, q1 = min(M, q0 + per);
-  const int kb0 = a.bunch_kb[b0];
-  const int span = a.bunch_kb[b1 - 1] - kb0;
-  const int base0 = (int)cyc_slot(-turn * h + kb0 + 1, n);
-  const bool th = a.oc.track_h, tv = a.oc.track_v;
-  const int len = max(0, q1 - q0) + span;
-  double *w0 = win, *w1 = win + per + h;
-  const double *E0 = a.rw_e, *E1 = a.rw_e + n;
-  // the window, 8 loads per thread in flight at a time (the loads, not the
-  // arithmetic, set this kernel's time)
-  for (int t0 = threadIdx.x; t0 < len; t0 += 8 * kBlock) {
-    double va[8], vb[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int t = min(t0 + u * kBlock, len - 1);   // in range for every u
-      int idx = base0 + q0 + t;
-      idx -= (idx >= n) ? n : 0;
-      idx -= (idx >= n) ? n : 0;
-      va[u] = E0[idx];
-      vb[u] = E1[idx];
-    }
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int t = t0 + u * kBlock;
-      if (t < len) {
-        w0[t] = va[u];
-        w1[t] = vb[u];
-      }
-    }
+  const int per = rw_steps_per_block(a.Nmlt, h, a.rw_nblk);
+  const int q0 = min(M, blk * per), q1 = min(M, q0 + per), L = q1 - q0;
+  const int kb0 = a.bunch_kb[0];
+  const int len = L + (a.bunch_kb[a.nbunch - 1] - kb0);
+  const int base = (int)cyc_slot(-turn * h + kb0 + 1 + q0, n);
+  double *w0 = win, *w1 = win + len, *wt = win + 2 * len;
+  for (int t = threadIdx.x; t < len; t += kBlock) {
+    int idx = base + t;                      // base < n and t < n: one wrap at most
+    idx -= (idx >= n) ? n : 0;
+    w0[t] = a.rw_e[idx];
+    w1[t] = a.rw_e[n + idx];
   }
+  for (int t = threadIdx.x; t < L; t += kBlock) wt[t] = a.rw_rsq[q0 + t + 1];
   __syncthreads();
-  int dk[kRwGroup];
-#pragma unroll
-  for (int g = 0; g < kRwGroup; ++g) dk[g] = (b0 + g < b1) ? a.bunch_kb[b0 + g] - kb0 : -1;
-  double s[2 * kRwGroup];
-#pragma unroll
-  for (int g = 0; g < 2 * kRwGroup; ++g) s[g] = 0.0;
-  for (int j = threadIdx.x; j < q1 - q0; j += kBlock) {
-    const double w = a.rw_rsq[q0 + j + 1];
-#pragma unroll
-    for (int g = 0; g < kRwGroup; ++g) {
-      if (dk[g] >= 0) {
-        s[2 * g] += w0[j + dk[g]] * w;
-        s[2 * g + 1] += w1[j + dk[g]] * w;
-      }
+  const int mtrig = a.rs->rw_m;              // RW kicks done before this one
+  const int trig = (a.triggerRW && mtrig < 50) ? 1 : 0;
+  const double cH = a.oc.track_h ? a.rw_const[trig][0] : 0.0, cV = a.oc.track_v ? a.rw_const[trig][1] : 0.0;
+  for (int b = threadIdx.x; b < a.nbunch; b += kBlock) {
+    const double *e0 = w0 + (a.bunch_kb[b] - kb0), *e1 = w1 + (a.bunch_kb[b] - kb0);
+    double s0 = 0.0, s1 = 0.0;
+    for (int j = 0; j < L; ++j) {
+      const double w = wt[j];
+      s0 += e0[j] * w;
+      s1 += e1[j] * w;
     }
-  }
-  __shared__ double red[kBlock / 32][2 * kRwGroup];
-#pragma unroll
-  for (int g = 0; g < 2 * kRwGroup; ++g) {
-    const double v = warp_sum(s[g]);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][g] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x < 2 * kRwGroup) {
-    const int g = threadIdx.x >> 1, pl = threadIdx.x & 1;
-    if (b0 + g < b1) {
-      double v = 0.0;
-      for (int w = 0; w < kBlock / 32; ++w) v += red[w][threadIdx.x];
-      const int mtrig = a.rs->rw_m;          // RW kicks done before this one
-      const int trig = (a.triggerRW && mtrig < 50) ? 1 : 0;
-      const bool on = pl == 0 ? th : tv;
-      a.rw_part[((size_t)(b0 + g) * kRwSplit + part) * 2 + pl] = on ? v * a.rw_const[trig][pl] : 0.0;
-    }
+    double *out = a.rw_acc + ((size_t)blk * a.nbunch + b) * 2;
+    out[0] = s0 * cH;
+    out[1] = s1 * cV;
   }
 }
 
@@ -896,6 +860,15 @@ __global__ void __launch_bounds__(kBlock) bunch_wakes(Args a, int advance) {
   const double *H = a.hist + (size_t)b * 6 * nc;
   const int kb = a.bunch_kb[b];
   __shared__ int cmin, cmax;
+  // the pending resistive-wall kick of this bunch: the ring scan's parts
+  // summed in a fixed order
+  if (a.rw_long && threadIdx.x < 64) {
+    const int pl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double v = 0.0;
+    for (int k = lane; k < a.rw_nblk; k += 32) v += a.rw_acc[((size_t)k * a.nbunch + b) * 2 + pl];
+    v = warp_sum(v);
+    if (lane == 0) a.rw_part[(size_t)b * 2 + pl] = v;
+  }
   if (!a.selffield) return;
   for (int j = threadIdx.x - PADC; j < nc + PADC; j += kBlock) {
     const bool in = j >= 0 && j < nc;
@@ -984,11 +957,7 @@ __global__ void add_pending_rw(Args a, double *out) {
   const size_t n6 = (size_t)a.npad;
   const int b = blockIdx.y;
   const int off = a.bunch_off[b], np = a.bunch_np[b];
-  double rh = 0.0, rv = 0.0;
-  for (int q = 0; q < kRwSplit; ++q) {
-    rh += a.rw_part[((size_t)b * kRwSplit + q) * 2 + 0];
-    rv += a.rw_part[((size_t)b * kRwSplit + q) * 2 + 1];
-  }
+  const double rh = a.rw_part[(size_t)b * 2 + 0], rv = a.rw_part[(size_t)b * 2 + 1];
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += gridDim.x * blockDim.x) {
     if (a.oc.track_h) out[4 * n6 + off + j] = a.coord[4 * n6 + off + j] + rh;
     if (a.oc.track_v) out[5 * n6 + off + j] = a.coord[5 * n6 + off + j] + rv;
@@ -1015,10 +984,8 @@ __global__ void beam_export(Args a, const long *pack, double *dst) {
   const bool pend = a.rw_long && a.rs->turn > 0;
   double rh = 0.0, rv = 0.0;
   if (pend) {
-    for (int q = 0; q < kRwSplit; ++q) {
-      rh += a.rw_part[((size_t)b * kRwSplit + q) * 2 + 0];
-      rv += a.rw_part[((size_t)b * kRwSplit + q) * 2 + 1];
-    }
+    rh = a.rw_part[(size_t)b * 2 + 0];
+    rv = a.rw_part[(size_t)b * 2 + 1];
   }
   double *d = dst + pack[b];
   for (int k = 0; k < 6; ++k) {

@@ -239,11 +239,16 @@ int effective_noise(const mbt_ctx *c) { return c->p.quantum ? c->noise : MBT_NOI
 
 size_t smem_reduce(const mbt_ctx *c) { return (size_t)c->prec * sizeof(double); }
 size_t smem_wakes(const mbt_ctx *c) { return mbt::bunch_wakes_smem(c->nc); }
-int rw_blocks(const mbt_ctx *c) {
-  return c->p.rw_long ? (c->nbunch + mbt::kRwGroup - 1) / mbt::kRwGroup * mbt::kRwSplit : 0;
+// Blocks of the resistive-wall sums: one per SM at most, at least 32
+// history steps each.
+int rw_blocks_for(const mbt_params *p, int nsm) {
+  if (!p->rw_long) return 0;
+  const long M = (long)(p->Nmlt + 1) * p->nharm;
+  return (int)std::max<long>(1, std::min<long>(nsm, (M + 31) / 32));
 }
+int rw_blocks(const mbt_ctx *c) { return c->a.rw_nblk; }
 size_t smem_scan(const mbt_ctx *c) {
-  return mbt::ring_scan_smem_doubles(c->p.rw_long, c->p.Nmlt, c->p.nharm) * sizeof(double);
+  return mbt::ring_scan_smem_doubles(c->p.rw_long, c->p.Nmlt, c->p.nharm, c->a.rw_nblk) * sizeof(double);
 }
 
 // The beam-ion stage of a turn: frames, ion clouds, electron kicks; with
@@ -598,7 +603,9 @@ int mbt_create(const mbt_params *p, int nbunch, const int *bucket, const int *np
   rc = rc ? rc : dalloc(c, &a.hist, (size_t)nbunch * 6 * c->nc);
   rc = rc ? rc : dalloc(c, &a.cellrange, (size_t)nbunch * 2);
   rc = rc ? rc : dalloc(c, &a.kick, (size_t)nbunch * 3 * c->nc);
-  rc = rc ? rc : dalloc(c, &a.rw_part, (size_t)nbunch * mbt::kRwSplit * 2);
+  a.rw_nblk = rw_blocks_for(p, c->nsm);
+  rc = rc ? rc : dalloc(c, &a.rw_part, (size_t)nbunch * 2);
+  rc = rc ? rc : dalloc(c, &a.rw_acc, (size_t)std::max(a.rw_nblk, 1) * nbunch * 2);
   a.stats_cap = 256;
   rc = rc ? rc : dalloc(c, &a.stats, (size_t)a.stats_cap * nbunch * 12);
   rc = rc ? rc : dalloc(c, &c->stats_init, (size_t)nbunch * 12);
@@ -1338,7 +1345,7 @@ int mbt_geometry(mbt_ctx *c, int *npad, int *tile, int *ntile) {
 namespace {
 
 constexpr char kCkptMagic[8] = {'M', 'B', 'T', 'C', 'K', 'P', 'T', '1'};
-constexpr uint32_t kCkptVersion = 1;
+constexpr uint32_t kCkptVersion = 2;   // 2: the pending resistive-wall kick as one record per bunch
 
 uint64_t fnv1a(uint64_t h, const void *p, size_t n) {
   const unsigned char *b = static_cast<const unsigned char *>(p);

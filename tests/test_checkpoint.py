@@ -21,7 +21,7 @@ def fnv1a(data):
     return h
 
 
-def build(turn=1234, nbunch=3, records=None, magic=b"MBTCKPT1", version=1):
+def build(turn=1234, nbunch=3, records=None, magic=b"MBTCKPT1", version=2):
     """A checkpoint in the writer's layout: the ring-state record (id 17)
     starts with the turn count."""
     if records is None:
@@ -52,7 +52,7 @@ def test_damaged_files_are_refused(tmp_path, libmbt, damage):
     elif damage == "magic":
         data = build(magic=b"MBTCKPT0")
     elif damage == "version":
-        data = build(version=2)
+        data = build(version=1)     # the previous format
     elif damage == "overlong_record":
         # a record claiming more bytes than the file holds (checksum valid)
         body = good[:-8]

@@ -365,10 +365,10 @@ int mbt_get_histograms(mbt_ctx *ctx, int ibunch, double *fnp, double *dipV,
  * (out[0..2] are 0), and the number of kernel launches per turn. */
 int mbt_last_timing(mbt_ctx *ctx, double out[4], int *launches_per_turn);
 
-/* Run nturns turns with the four kernels of a turn launched one by one and
- * CUDA events between them; out[0..3] receive the average device time per
- * turn [ms] of the particle pass, the bunch reduction, the ring-wide
- * phasor scan and the bunch wakes. */
+/* Run nturns turns back to back with the four kernels of a turn launched
+ * one by one and CUDA events between them; out[0..3] receive the average
+ * device time per turn [ms] of the particle pass, the bunch reduction, the
+ * ring-wide phasor scan and the bunch wakes. */
 int mbt_profile_turns(mbt_ctx *ctx, long nturns, double out[4]);
 
 /* Device layout: padded particle count, largest tile size, number of tiles. */

@@ -683,17 +683,13 @@ __global__ void __launch_bounds__(kBlock) ring_scan(Args a, int passes, int init
   const int h = a.nharm;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __shared__ int fb_live;
-  if (threadIdx.x == 0) {
-    fb_live = rs->rffb_on;
-    if (!init) {
-      rs->Vrf0_last = rs->Vrf0;
-      rs->phai0_last = rs->phai0;
-      for (int pl = 0; pl < 3; ++pl)
-        for (int l = 0; l < kMaxLr; ++l) {
-          rs->phasor_last[pl][l][0] = rs->phasor[pl][l][0];
-          rs->phasor_last[pl][l][1] = rs->phasor[pl][l][1];
-        }
-    }
+  if (threadIdx.x == 0) fb_live = rs->rffb_on;
+  if (!init) {
+    // the snapshot of the last turn's state, one value per thread
+    constexpr int nv = 3 * kMaxLr * 2;
+    if (threadIdx.x < nv) (&rs->phasor_last[0][0][0])[threadIdx.x] = (&rs->phasor[0][0][0])[threadIdx.x];
+    if (threadIdx.x == nv) rs->Vrf0_last = rs->Vrf0;
+    if (threadIdx.x == nv + 1) rs->phai0_last = rs->phai0;
   }
   __syncthreads();
   const int chunk = (h + 31) / 32;

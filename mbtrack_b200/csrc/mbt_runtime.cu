@@ -1182,27 +1182,48 @@ int mbt_profile_turns(mbt_ctx *c, long nturns, double out[4]) {
   double acc[4] = {0, 0, 0, 0}, acc_bi = 0.0, acc_k[4] = {0, 0, 0, 0};
   RingState rs;
   CK(cudaMemcpy(&rs, c->a.rs, sizeof rs, cudaMemcpyDeviceToHost));
+  // the turns run back to back, as in mbt_run_turns, with their own events
+  // between the kernels (5 per turn, 4 more for the beam-ion stage)
+  const int per = 5 + (c->bi_on ? 4 : 0);
+  struct Events {
+    std::vector<cudaEvent_t> e;
+    ~Events() {
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } E;
+  E.e.assign((size_t)nturns * per, nullptr);
+  for (auto &x : E.e) CK(cudaEventCreate(&x));
+  const cudaEvent_t keep_kev[3] = {c->bi_kev[0], c->bi_kev[1], c->bi_kev[2]}, keep_bi = c->bi_ev;
   for (long t = 0; t < nturns; ++t) {
-    enqueue_turn(c, c->ev, scan_boundary(c, rs.turn + t));
-    CK(cudaEventSynchronize(c->bi_on ? c->bi_ev : c->ev[4]));
+    cudaEvent_t *ev = &E.e[(size_t)t * per];
+    if (c->bi_on) {
+      for (int k = 0; k < 3; ++k) c->bi_kev[k] = ev[5 + k];
+      c->bi_ev = ev[8];
+    }
+    enqueue_turn(c, ev, scan_boundary(c, rs.turn + t));
+  }
+  for (int k = 0; k < 3; ++k) c->bi_kev[k] = keep_kev[k];
+  c->bi_ev = keep_bi;
+  int r = sync_and_check(c);
+  if (r) return r;
+  for (long t = 0; t < nturns; ++t) {
+    const cudaEvent_t *ev = &E.e[(size_t)t * per];
+    float ms = 0;
     for (int k = 0; k < 4; ++k) {
-      float ms = 0;
-      cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]);
+      cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
       acc[k] += ms;
     }
     if (c->bi_on) {
-      float ms = 0;
-      cudaEventElapsedTime(&ms, c->ev[4], c->bi_ev);
+      cudaEventElapsedTime(&ms, ev[4], ev[8]);
       acc_bi += ms;
-      const cudaEvent_t seq[5] = {c->ev[4], c->bi_kev[0], c->bi_kev[1], c->bi_kev[2], c->bi_ev};
+      const cudaEvent_t seq[5] = {ev[4], ev[5], ev[6], ev[7], ev[8]};
       for (int k = 0; k < 4; ++k) {
         cudaEventElapsedTime(&ms, seq[k], seq[k + 1]);
         acc_k[k] += ms;
       }
     }
   }
-  int r = sync_and_check(c);
-  if (r) return r;
   for (int k = 0; k < 4; ++k) out[k] = acc[k] / nturns;
   c->bi_ms = acc_bi / nturns;
   for (int k = 0; k < 4; ++k) c->bi_kms[k] = acc_k[k] / nturns;

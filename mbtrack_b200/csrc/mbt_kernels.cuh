@@ -570,19 +570,21 @@ __global__ void __launch_bounds__(kBlock) bunch_reduce(Args a, int mode, double 
     const double ib = a.ibunch[kb];
     for (int r = warp; r < a.nlr; r += kBlock / 32) {
       const LrConst &L = a.lr[r];
-      const double *src = H + (size_t)(3 + L.plane) * nc;   // dropped histogram of the plane
+      // dropped histogram of the plane (H rows 3..5), read from the summed
+      // records in shared memory; a plane without dipole sums has zeros
+      const double *src = L.plane == 0 ? tot : (a.hist_xz ? tot + (size_t)L.plane * nc : nullptr);
       const double fac = a.bunch_fac[(size_t)r * a.nbunch + b];
       double *u = a.lr_u + ((size_t)r * a.nbunch + b) * nc * 2;
       double *bb = a.lr_b + ((size_t)r * a.nbunch + b) * nc;
       Aff f = aff_id();
       for (int j = j0; j < j1; ++j) {
-        const Aff g{L.prog[0], L.prog[1], -(ib * src[j] * fac), 0.0};
+        const Aff g{L.prog[0], L.prog[1], -(ib * (src ? src[j] : 0.0) * fac), 0.0};
         f = compose(f, g);
       }
       const Aff ex = warp_exclusive_scan(f, lane);
       double v0 = ex.a0, v1 = ex.a1;
       for (int j = j0; j < j1; ++j) {
-        const double s = ib * src[j] * fac;
+        const double s = ib * (src ? src[j] : 0.0) * fac;
         const double n0 = (v0 * L.prog[0] - v1 * L.prog[1]) - s;
         const double n1 = (v0 * L.prog[1] + v1 * L.prog[0]);
         v0 = n0;
@@ -654,15 +656,25 @@ __device__ void rw_partial_sums(const Args &a, int blk, double *win) {
   const double cH = a.oc.track_h ? a.rw_const[trig][0] : 0.0, cV = a.oc.track_v ? a.rw_const[trig][1] : 0.0;
   for (int b = threadIdx.x; b < a.nbunch; b += kBlock) {
     const double *e0 = w0 + (a.bunch_kb[b] - kb0), *e1 = w1 + (a.bunch_kb[b] - kb0);
-    double s0 = 0.0, s1 = 0.0;
-    for (int j = 0; j < L; ++j) {
-      const double w = wt[j];
-      s0 += e0[j] * w;
-      s1 += e1[j] * w;
+    // four partial sums per plane (steps j mod 4), so that the products
+    // do not wait on one another
+    double s0[4] = {0.0, 0.0, 0.0, 0.0}, s1[4] = {0.0, 0.0, 0.0, 0.0};
+    int j = 0;
+    for (; j + 4 <= L; j += 4) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double w = wt[j + u];
+        s0[u] += e0[j + u] * w;
+        s1[u] += e1[j + u] * w;
+      }
+    }
+    for (; j < L; ++j) {
+      s0[0] += e0[j] * wt[j];
+      s1[0] += e1[j] * wt[j];
     }
     double *out = a.rw_acc + ((size_t)blk * a.nbunch + b) * 2;
-    out[0] = s0 * cH;
-    out[1] = s1 * cV;
+    out[0] = ((s0[0] + s0[1]) + (s0[2] + s0[3])) * cH;
+    out[1] = ((s1[0] + s1[1]) + (s1[2] + s1[3])) * cV;
   }
 }
 
@@ -855,7 +867,7 @@ __global__ void __launch_bounds__(kBlock) bunch_wakes(Args a, int advance) {
   double *lr = sm + 3 * (nc + 2 * PADC);      // 3 x nc
   const double *H = a.hist + (size_t)b * 6 * nc;
   const int kb = a.bunch_kb[b];
-  __shared__ int cmin, cmax;
+  __shared__ int wmin[kBlock / 32], wmax[kBlock / 32];
   // the pending resistive-wall kick of this bunch: the ring scan's parts
   // summed in a fixed order
   if (a.rw_long && threadIdx.x < 64) {
@@ -866,22 +878,34 @@ __global__ void __launch_bounds__(kBlock) bunch_wakes(Args a, int advance) {
     if (lane == 0) a.rw_part[(size_t)b * 2 + pl] = v;
   }
   if (!a.selffield) return;
+  // first and last filled bin (transform_weak.c:633-651: the first bin
+  // with particles, else nc - 1; the last one above bin 0, else 0), as a
+  // minimum and a maximum over the block
+  int mn = nc - 1, mx = 0;
   for (int j = threadIdx.x - PADC; j < nc + PADC; j += kBlock) {
     const bool in = j >= 0 && j < nc;
-    fnp[j] = in ? H[j] : 0.0;
+    const double f = in ? H[j] : 0.0;
+    fnp[j] = f;
     dipV[j] = in ? H[nc + j] : 0.0;
     dipH[j] = in ? H[2 * nc + j] : 0.0;
+    if (f > 0) {
+      mn = min(mn, j);
+      if (j >= 1) mx = max(mx, j);
+    }
+  }
+  mn = __reduce_min_sync(0xffffffffu, mn);
+  mx = __reduce_max_sync(0xffffffffu, mx);
+  if ((threadIdx.x & 31) == 0) {
+    wmin[threadIdx.x >> 5] = mn;
+    wmax[threadIdx.x >> 5] = mx;
   }
   for (int j = threadIdx.x; j < 3 * nc; j += kBlock) lr[j] = 0.0;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    // transform_weak.c:633-651
-    int mn = nc - 1, mx = 0;
-    for (int i = 0; i < mn; ++i) if (fnp[i] > 0) { mn = i; break; }
-    for (int i = nc - 1; i > mx; --i) if (fnp[i] > 0) { mx = i; break; }
-    cmin = mn; cmax = mx;
+  int cmin = wmin[0], cmax = wmax[0];
+  for (int w = 1; w < kBlock / 32; ++w) {
+    cmin = min(cmin, wmin[w]);
+    cmax = max(cmax, wmax[w]);
   }
-  __syncthreads();
   // long-range wake per bin: V_j = Vs prog^(j+1) + U_j; the reference adds
   // V_j + Ib fnp_j fac / 2 for every resonator of the plane
   // (transform_weak.c:1020-1023)

@@ -239,12 +239,12 @@ int effective_noise(const mbt_ctx *c) { return c->p.quantum ? c->noise : MBT_NOI
 
 size_t smem_reduce(const mbt_ctx *c) { return (size_t)c->prec * sizeof(double); }
 size_t smem_wakes(const mbt_ctx *c) { return mbt::bunch_wakes_smem(c->nc); }
-// Blocks of the resistive-wall sums: one per SM at most, at least 32
+// Blocks of the resistive-wall sums: two per SM at most, at least 32
 // history steps each.
 int rw_blocks_for(const mbt_params *p, int nsm) {
   if (!p->rw_long) return 0;
   const long M = (long)(p->Nmlt + 1) * p->nharm;
-  return (int)std::max<long>(1, std::min<long>(nsm, (M + 31) / 32));
+  return (int)std::max<long>(1, std::min<long>(2L * nsm, (M + 31) / 32));
 }
 int rw_blocks(const mbt_ctx *c) { return c->a.rw_nblk; }
 size_t smem_scan(const mbt_ctx *c) {

@@ -265,11 +265,13 @@ int mbt_last_error(const mbt_ctx *ctx, char *buf, size_t len);
  * tests of the reporting path without a device fault. */
 int mbt_inject_device_error(mbt_ctx *ctx, int bits);
 
-/* One bounded wait that nothing ends: a kernel waits `polls` times on an
- * mbarrier no thread arrives at, with the helper every waiting kernel uses,
- * and reports giving up.  Returns MBT_ERR_TIMEOUT when the wait gave up as
- * it must, 0 if it did not (a broken bound).  For tests of the bounded
- * waits on the GPU; no counterpart in the reference. */
+/* Bounded waits that nothing ends: a kernel waits on an mbarrier no thread
+ * arrives at, with the two helpers the waiting kernels use (a polling wait
+ * of `polls` polls, a sleeping wait of `polls` x 1000 clock cycles), and
+ * reports giving up.  Returns MBT_ERR_TIMEOUT when both gave up as they
+ * must, 0 if neither did and MBT_ERR_STATE if only one did (a broken
+ * bound).  For tests of the bounded waits on the GPU; no counterpart in the
+ * reference. */
 int mbt_selftest_bounded_wait(long polls, void *stream);
 
 /* Copy one bunch's coordinates in (host soa6, np doubles per coordinate).
@@ -529,10 +531,14 @@ int mbt_gauss_field_dev(long n, const double *dx_dev, const double *dy_dev,
  * Every layer runs on the tensor cores with BF16 weights and activations
  * and FP32 accumulation: the inputs and the biases enter as BF16 pairs
  * (high and low part) through extra columns of the operands, the
- * activations are GELU (tanh form) in BF16 pair arithmetic.  Parameters
- * (FP32 masters): MBT_MLP_NPARAM floats, W1[128][3], b1[128], W2[128][128],
- * b2, W3[128][128], b3, W4[2][128], b4[2]. */
+ * activations are GELU in its sigmoid form, z sigma(1.702 z), evaluated in
+ * FP32 and rounded to BF16: with the hardware tanh, or, for the first
+ * MBT_MLP_POLY_UNITS units of each hidden layer, with an odd polynomial of
+ * tanh over a clamped argument (within 3.5e-3 of tanh) on the FMA pipes.
+ * Parameters (FP32 masters): MBT_MLP_NPARAM floats, W1[128][3], b1[128],
+ * W2[128][128], b2, W3[128][128], b3, W4[2][128], b4[2]. */
 #define MBT_MLP_NPARAM 33794
+#define MBT_MLP_POLY_UNITS 0
 
 /* Network with seeded Glorot-uniform weights, zero biases. */
 int mbt_mlp_create(uint64_t seed, mbt_mlp **out);

@@ -261,4 +261,33 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long l
   return false;
 }
 
+// Suspend-time hint of the sleeping wait [ns]: a thread whose phase is not
+// complete sleeps in the barrier unit until the phase completes or this
+// time passes, instead of polling (polls take issue slots from the warps
+// that do the work).
+constexpr uint32_t kSleepHintNs = 1000000u;
+constexpr long long kSleepLimitCycles = 1LL << 32;   // about 2 s at the B200's clocks
+
+// Bounded wait for phase `parity` of `bar` that sleeps between checks:
+// returns false after `max_cycles` SM clock cycles (or 2^24 checks) without
+// completion.
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t *bar, uint32_t parity,
+                                                long long max_cycles = kSleepLimitCycles) {
+  const uint32_t a = smem_u32(bar);
+  const long long t0 = clock64();
+  for (long k = 0; k < (1L << 24); ++k) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity), "r"(kSleepHintNs)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > max_cycles) return false;
+  }
+  return false;
+}
+
 }  // namespace mbt

@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
   int *hc = reinterpret_cast<int *>(kL + (HISTXZ ? 7 : 5) * nc);
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ __align__(8) uint64_t empty[kStages];
-  __shared__ double red[14];
+  __shared__ double red[8][3];                  // per compute warp: sum, square sum, cross sum
   __shared__ double trash_n[2];                 // out-of-range particles below / above the bins
   __shared__ unsigned long long trash_fx[8];    // their x and z, fixed-point (hi, lo) pairs
   __shared__ double shift[6];
@@ -293,12 +293,17 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
   const bool kick_h = sf && a.lr_kick[1];
   const bool kick_v = sf && a.lr_kick[2];
   const int jb0 = tile.start - a.bunch_off[b];   // index of the tile's first particle in its bunch
-  // moments: warp w < 6 owns coordinate column w of every staged chunk;
-  // warps 6 and 7 sum the cross products x x' and z z' (columns 1*4, 2*5)
-  const double col_shift = warp < 6 ? shift[warp] : 0.0;
-  const int cx = warp == 6 ? 1 : 2;
-  const double sh_a = warp >= 6 ? shift[cx] : 0.0, sh_b = warp >= 6 ? shift[cx + 3] : 0.0;
-  double col_s = 0.0, col_q = 0.0;
+  // moments: warp w < 4 owns coordinate column w (xtau, x, z, eps) of every
+  // staged chunk; warps 4 and 6 share column 4 (x') and the cross product
+  // x x', warps 5 and 7 column 5 (z') and z z', each on half of the chunk.
+  // Every warp then does about the same work per chunk (the per-chunk
+  // barrier waits for the slowest).
+  const int mcol = warp < 4 ? warp : 4 + (warp & 1);          // summed and squared column
+  const int mpair = mcol - 3;                                  // x or z, for the cross product
+  const int mhalf = warp >= 6 ? 1 : 0;                         // warps 6, 7: second half of the chunk
+  const double col_shift = shift[mcol];
+  const double pair_shift = warp >= 4 ? shift[mpair] : 0.0;
+  double col_s = 0.0, col_q = 0.0, col_c = 0.0;
 
   for (int c = 0; c < nchunk; ++c) {
     const int s = c % kStages;
@@ -354,8 +359,8 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
     const int nlive = min(kChunk, tile.count - c * kChunk);
     if (nlive == kChunk) {
       // full chunk: two elements per lane and load, no bounds test
-      if (warp < 6) {
-        const double2 *col = reinterpret_cast<const double2 *>(st + (size_t)warp * kChunk);
+      const double2 *col = reinterpret_cast<const double2 *>(st + (size_t)mcol * kChunk);
+      if (warp < 4) {
 #pragma unroll
         for (int q = 0; q < kChunk / 64; ++q) {
           const double2 v = col[q * 32 + lane];
@@ -366,30 +371,43 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
           col_q += d1 * d1;
         }
       } else {
-        const double2 *ca = reinterpret_cast<const double2 *>(st + (size_t)cx * kChunk);
-        const double2 *cb = reinterpret_cast<const double2 *>(st + (size_t)(cx + 3) * kChunk);
+        const double2 *pr = reinterpret_cast<const double2 *>(st + (size_t)mpair * kChunk);
+        const int q0 = mhalf * (kChunk / 128);
 #pragma unroll
-        for (int q = 0; q < kChunk / 64; ++q) {
-          const double2 va = ca[q * 32 + lane], vb = cb[q * 32 + lane];
-          col_s += (va.x - sh_a) * (vb.x - sh_b);
-          col_s += (va.y - sh_a) * (vb.y - sh_b);
+        for (int q = q0; q < q0 + kChunk / 128; ++q) {
+          const double2 v = col[q * 32 + lane], u = pr[q * 32 + lane];
+          const double d0 = v.x - col_shift, d1 = v.y - col_shift;
+          col_s += d0;
+          col_q += d0 * d0;
+          col_c += (u.x - pair_shift) * d0;
+          col_s += d1;
+          col_q += d1 * d1;
+          col_c += (u.y - pair_shift) * d1;
         }
       }
-    } else if (warp < 6) {
-      const double *col = st + (size_t)warp * kChunk;
-#pragma unroll
-      for (int q = 0; q < kChunk / 32; ++q) {
-        const int e = q * 32 + lane;
-        const double d = e < nlive ? col[e] - col_shift : 0.0;
-        col_s += d;
-        col_q += d * d;
-      }
     } else {
-      const double *ca = st + (size_t)cx * kChunk, *cb = st + (size_t)(cx + 3) * kChunk;
+      const double *col = st + (size_t)mcol * kChunk;
+      if (warp < 4) {
 #pragma unroll
-      for (int q = 0; q < kChunk / 32; ++q) {
-        const int e = q * 32 + lane;
-        col_s += e < nlive ? (ca[e] - sh_a) * (cb[e] - sh_b) : 0.0;
+        for (int q = 0; q < kChunk / 32; ++q) {
+          const int e = q * 32 + lane;
+          const double d = e < nlive ? col[e] - col_shift : 0.0;
+          col_s += d;
+          col_q += d * d;
+        }
+      } else {
+        const double *pr = st + (size_t)mpair * kChunk;
+        const int q0 = mhalf * (kChunk / 64);
+#pragma unroll
+        for (int q = q0; q < q0 + kChunk / 64; ++q) {
+          const int e = q * 32 + lane;
+          if (e < nlive) {
+            const double d = col[e] - col_shift;
+            col_s += d;
+            col_q += d * d;
+            col_c += (pr[e] - pair_shift) * d;
+          }
+        }
       }
     }
     __syncwarp();
@@ -397,14 +415,11 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
   }
   // column sums -> block sums, in a fixed order
   {
-    const double vs = warp_sum(col_s), vq = warp_sum(col_q);
+    const double vs = warp_sum(col_s), vq = warp_sum(col_q), vc = warp < 4 ? 0.0 : warp_sum(col_c);
     if (lane == 0) {
-      if (warp < 6) {
-        red[warp] = vs;
-        red[6 + warp] = vq;
-      } else {
-        red[12 + (warp - 6)] = vs;
-      }
+      red[warp][0] = vs;
+      red[warp][1] = vq;
+      red[warp][2] = vc;
     }
   }
   named_barrier(1, kBlock);
@@ -413,7 +428,12 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
     // out-of-range extras: count, x sum, z sum below the bins, then above
     const int q = threadIdx.x % 3, side = threadIdx.x / 3;
     double sum;
-    if (threadIdx.x >= 6) sum = red[threadIdx.x - 6];
+    if (threadIdx.x >= 6) {
+      // moment m: sums of columns 0..5, their squares, then x x' and z z';
+      // columns 4 and 5 and the cross sums are the two halves' sums, first half first
+      const int m = threadIdx.x - 6, col = m < 12 ? m % 6 : m - 8, kind = m < 6 ? 0 : (m < 12 ? 1 : 2);
+      sum = col < 4 ? red[col][kind] : red[col][kind] + red[col + 2][kind];
+    }
     else if (q == 0) sum = trash_n[side];
     else sum = fx70_value(trash_fx[4 * side + 2 * (q - 1)], trash_fx[4 * side + 2 * (q - 1) + 1]);
     rec[a.hoff + threadIdx.x] = sum;

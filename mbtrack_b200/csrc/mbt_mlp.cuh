@@ -51,6 +51,7 @@
 #include <cuda_fp16.h>
 #include <cstdint>
 
+#include "mbt.h"
 #include "mbt_common.cuh"
 
 namespace mbt {
@@ -206,16 +207,60 @@ __device__ __forceinline__ float gelu_grad(float x) {
   return s + kGeluK * x * s * (1.0f - s);
 }
 
-// The activation of a pair of scaled pre-activations w = c z in BF16 pair
-// arithmetic: w = bf16(w), h' = w + w tanh(w) = k gelu(z), each step
-// rounded to BF16, hardware tanh.  Returns the BF16 pair (low half from w0).
+// The activation of a pair of scaled pre-activations w = c z: h' = w + w
+// tanh(w) = k gelu(z) in FP32 (hardware tanh, one FP32-pair FMA), rounded
+// once to a BF16 pair.  Returns the BF16 pair (low half from w0).
 __device__ __forceinline__ uint32_t act_bf16x2(float w0, float w1) {
-  uint32_t w, th, h;
-  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(w) : "f"(w1), "f"(w0));
-  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(th) : "r"(w));
-  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(h) : "r"(w), "r"(th));
+  const float t0 = tanh_hw(w0), t1 = tanh_hw(w1);
+  uint32_t h;
+  asm("{\n\t.reg .b64 w, t, r;\n\t.reg .f32 r0, r1;\n\t"
+      "mov.b64 w, {%1, %2};\n\t"
+      "mov.b64 t, {%3, %4};\n\t"
+      "fma.rn.f32x2 r, w, t, w;\n\t"
+      "mov.b64 {r0, r1}, r;\n\t"
+      "cvt.rn.bf16x2.f32 %0, r1, r0;\n\t}"
+      : "=r"(h)
+      : "f"(w0), "f"(w1), "f"(t0), "f"(t1));
   return h;
 }
+// The same activation on the FMA pipes, for the first kMlpPolyUnits units of
+// every hidden layer: the hardware tanh of the other units runs on the
+// multi-function unit, which issues 16 results per clock per SM, and with
+// every unit there it bounds the network; these units move a share of the
+// activations to the FP32-pair FMA pipe.  tanh(u) for u clamped to
+// [-kPolyA, kPolyA] is the odd polynomial t = v Q(v^2), v = u / (2 kPolyA),
+// Q of degree 5 (coefficients kPolyC, a minimax fit of tanh over all u with
+// t(kPolyA) = 1: |t - tanh(u)| <= 3.5e-3, so t reaches the limits 0 and 2w of
+// h' beyond the clamp exactly as tanh does).  In FP32: s = sat(w / (2 kPolyA)
+// + 1/2), v = s - 1/2, Horner in v^2, h' = w + (w v) Q, rounded once to BF16
+// (the oracle repeats these FP32 steps exactly).
+constexpr int kMlpPolyUnits = MBT_MLP_POLY_UNITS;    // units 0 .. kMlpPolyUnits - 1 of each hidden layer
+constexpr int kMlpPolyChunks = kMlpPolyUnits / 8;    // in 8-unit chunks
+static_assert(kMlpPolyUnits % 8 == 0 && kMlpPolyUnits <= 128, "whole chunks of a hidden layer");
+constexpr float kPolyA = 3.25f, kPolyAlpha = 0.15384616f;   // alpha = 1 / (2 kPolyA) in FP32
+constexpr float kPolyC0 = 6.39387608f, kPolyC1 = -74.8484726f, kPolyC2 = 714.953674f, kPolyC3 = -4046.01587f,
+                kPolyC4 = 11861.9072f, kPolyC5 = -13806.5342f;
+__device__ __forceinline__ float fma_sat(float a, float b, float c) {
+  float r;
+  asm("fma.rn.sat.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ uint32_t act_poly_bf16x2(float w0, float w1) {
+  const float2 w = make_float2(w0, w1);
+  const float2 s = make_float2(fma_sat(w0, kPolyAlpha, 0.5f), fma_sat(w1, kPolyAlpha, 0.5f));
+  const float2 v = __fadd2_rn(s, make_float2(-0.5f, -0.5f));
+  const float2 v2 = __fmul2_rn(v, v);
+  float2 q = __ffma2_rn(make_float2(kPolyC5, kPolyC5), v2, make_float2(kPolyC4, kPolyC4));
+  q = __ffma2_rn(q, v2, make_float2(kPolyC3, kPolyC3));
+  q = __ffma2_rn(q, v2, make_float2(kPolyC2, kPolyC2));
+  q = __ffma2_rn(q, v2, make_float2(kPolyC1, kPolyC1));
+  q = __ffma2_rn(q, v2, make_float2(kPolyC0, kPolyC0));
+  const float2 h = __ffma2_rn(__fmul2_rn(w, v), q, w);
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(h.y), "f"(h.x));
+  return r;
+}
+
 __device__ __forceinline__ void unpack_bf16x2(uint32_t h, float &lo, float &hi) {
   lo = __uint_as_float(h << 16);
   hi = __uint_as_float(h & 0xFFFF0000u);
@@ -232,6 +277,9 @@ struct MlpGroup {
   uint32_t lane;                               // this warp's lane base (bits 16..)
   uint32_t row;                                // byte offset of this thread's row in a column block
   int swz;                                     // this thread's row inside its 8-row group
+  uint32_t sA;                                 // shared address of this thread's row of the activation
+                                               //   tile with its swizzle: chunk c of column block cb
+                                               //   is at (sA ^ (c << 4)) + cb * 16384
   int bar_id;                                  // named barrier of the group
   uint32_t phase;
   volatile int *fail;                          // set when a wait of the group gave up
@@ -295,9 +343,9 @@ __device__ __forceinline__ bool group_issue(const MlpGroup &G, int t, bool &fail
 // the group's flag, which every thread sees after the group's next barrier,
 // and waits once more (bounded) for the products still in flight.
 __device__ __forceinline__ void group_wait(MlpGroup &G) {
-  if (!mbar_wait(G.bar, G.phase, kMlpWaitLimit)) {
+  if (!mbar_wait_sleep(G.bar, G.phase)) {
     *G.fail = 1;
-    mbar_wait(G.bar, G.phase, kMlpWaitLimit);
+    mbar_wait_sleep(G.bar, G.phase);
   }
   G.phase ^= 1u;
   tc_fence_after();
@@ -313,27 +361,34 @@ __device__ __forceinline__ void mlp_input_row(const MlpGroup &G, const float *x)
   *reinterpret_cast<uint4 *>(G.A + G.row + ((1 ^ G.swz) << 4)) = make_uint4(0u, 0u, 0u, 0u);
 }
 
-// 16 accumulator columns (k0 .. k0+15) -> activation -> two chunks of row t
-// of the activation tile; zs / hs (may be null) receive the pre-activations
-// z = w/c and the activations gelu(z) = h'/k.
-__device__ __forceinline__ void mlp_act16(const MlpGroup &G, int k0, const float *v, float *zs, float *hs) {
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
+}
+
+// 16 accumulator columns 8 ch .. 8 ch + 15 -> activation -> chunks ch, ch + 1
+// of row t of the activation tile (ch even; a compile-time constant where
+// the caller's loop is unrolled); zs / hs (may be null) receive the
+// pre-activations z = w/c and the activations gelu(z) = h'/k.
+__device__ __forceinline__ void mlp_act16(const MlpGroup &G, int ch, const float *v, float *zs, float *hs) {
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
     uint32_t h[4];
+    const int cc = ch + c;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) h[i] = act_bf16x2(v[8 * c + 2 * i], v[8 * c + 2 * i + 1]);
-    const int ch = (k0 >> 3) + c;
-    *reinterpret_cast<uint4 *>(G.A + (ch >> 3) * 16384 + G.row + (((ch & 7) ^ G.swz) << 4)) =
-        make_uint4(h[0], h[1], h[2], h[3]);
+    for (int i = 0; i < 4; ++i)
+      h[i] = cc < kMlpPolyChunks ? act_poly_bf16x2(v[8 * c + 2 * i], v[8 * c + 2 * i + 1])
+                                 : act_bf16x2(v[8 * c + 2 * i], v[8 * c + 2 * i + 1]);
+    st_shared_v4((G.sA ^ (uint32_t)((cc & 7) << 4)) + (uint32_t)(cc >> 3) * 16384u, h[0], h[1], h[2], h[3]);
     if (zs) {
+      const int k0 = 8 * cc;
 #pragma unroll
-      for (int i = 0; i < 8; ++i) zs[k0 + 8 * c + i] = kGeluInvC * v[8 * c + i];
+      for (int i = 0; i < 8; ++i) zs[k0 + i] = kGeluInvC * v[8 * c + i];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         float lo, hi;
         unpack_bf16x2(h[i], lo, hi);
-        hs[k0 + 8 * c + 2 * i] = kGeluInvK * lo;
-        hs[k0 + 8 * c + 2 * i + 1] = kGeluInvK * hi;
+        hs[k0 + 2 * i] = kGeluInvK * lo;
+        hs[k0 + 2 * i + 1] = kGeluInvK * hi;
       }
     }
   }
@@ -341,20 +396,21 @@ __device__ __forceinline__ void mlp_act16(const MlpGroup &G, int k0, const float
 
 // Epilogue of a layer: accumulator (bias included) -> activation -> row t
 // of the activation tile (the product that read the tile has completed), 16
-// columns at a time with the next 16 loading meanwhile.
+// columns at a time with the next 16 loading meanwhile; unrolled, so that
+// every store address is one XOR from the row's base.
 __device__ __forceinline__ void mlp_epilogue(const MlpGroup &G, float *zs, float *hs) {
   const uint32_t col = G.dcol + G.lane;
   float va[16], vb[16];
   tmem_ld16(col, va);
   tmem_wait16(va);
-#pragma unroll 1
-  for (int k0 = 0; k0 < 128; k0 += 32) {
-    tmem_ld16(col + k0 + 16, vb);
-    mlp_act16(G, k0, va, zs, hs);
+#pragma unroll
+  for (int q = 0; q < 8; q += 2) {
+    tmem_ld16(col + 16 * (q + 1), vb);
+    mlp_act16(G, 2 * q, va, zs, hs);
     tmem_wait16(vb);
-    if (k0 + 32 < 128) tmem_ld16(col + k0 + 32, va);
-    mlp_act16(G, k0 + 16, vb, zs, hs);
-    if (k0 + 32 < 128) tmem_wait16(va);
+    if (q + 2 < 8) tmem_ld16(col + 16 * (q + 2), va);
+    mlp_act16(G, 2 * q + 2, vb, zs, hs);
+    if (q + 2 < 8) tmem_wait16(va);
   }
   tc_fence_before();
 }
@@ -481,6 +537,7 @@ __device__ __forceinline__ uint32_t mlp_cta_setup(const MlpDev &M, uint8_t *base
   G.lane = (uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16;
   G.row = (uint32_t)((t >> 3) * 1024 + (t & 7) * 128);
   G.swz = t & 7;
+  G.sA = G.aA + G.row + ((uint32_t)G.swz << 4);
   G.bar_id = 1 + g;
   G.phase = 0;
   G.fail = fail + g;

@@ -252,8 +252,10 @@ extern "C" int mbt_bunch_moments_dev_noalloc(int np, const double *coord_dev, do
 
 // ---------------------------------------------------------------------------
 // Self-test of the bounded waits: one thread waits on an mbarrier that no
-// thread arrives at, with the same helper (mbt::mbar_wait) and the same
-// give-up path as the kernels; the wait must end after `polls` polls.
+// thread arrives at, with the same helpers (mbt::mbar_wait, and the
+// sleeping mbt::mbar_wait_sleep of the learned-field kernels) and the same
+// give-up path as the kernels; the polling wait must end after `polls`
+// polls, the sleeping one after `polls` x 1000 clock cycles.
 
 namespace {
 __global__ void bounded_wait_probe(long polls, int *gave_up) {
@@ -261,7 +263,9 @@ __global__ void bounded_wait_probe(long polls, int *gave_up) {
   if (threadIdx.x == 0) {
     mbt::mbar_init(&bar, 1);
     mbt::fence_mbar_init();
-    *gave_up = mbt::mbar_wait(&bar, 0u, polls) ? 0 : 1;
+    const bool a = mbt::mbar_wait(&bar, 0u, polls);
+    const bool b = mbt::mbar_wait_sleep(&bar, 0u, (long long)polls * 1000);
+    *gave_up = (a ? 0 : 1) + (b ? 0 : 2);
   }
 }
 }  // namespace
@@ -283,6 +287,9 @@ extern "C" int mbt_selftest_bounded_wait(long polls, void *stream) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   cudaFree(flag);
   if (e != cudaSuccess) return mbt::fail_global(MBT_ERR_CUDA, "bounded wait self-test: %s", cudaGetErrorString(e));
-  if (gave_up == 1) return mbt::fail_global(MBT_ERR_TIMEOUT, "bounded wait gave up after %ld polls", polls);
+  if (gave_up == 3)
+    return mbt::fail_global(MBT_ERR_TIMEOUT, "bounded waits gave up after %ld polls / %ld cycles", polls,
+                            polls * 1000);
+  if (gave_up != 0) return mbt::fail_global(MBT_ERR_STATE, "bounded wait self-test: only one wait gave up (%d)", gave_up);
   return 0;
 }

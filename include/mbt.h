@@ -56,7 +56,7 @@ extern "C" {
 
 /* Noise source of the quantum-excitation term (transform_weak.c:71-75,
  * 134-138, 182-186). */
-#define MBT_NOISE_PHILOX   0  /* counter-based Philox4x32-10 normals */
+#define MBT_NOISE_PHILOX   0  /* counter-based Philox4x32-7 normals (mbt_philox.cuh) */
 #define MBT_NOISE_INJECTED 1  /* deviates supplied by mbt_set_deviates() */
 
 /*

@@ -424,6 +424,7 @@ __device__ __forceinline__ void bi_group_fallbacks(MlpGroup &G, int t, bool need
     gy = out[2 * idx + 1];
     ++fallbacks;
   }
+  named_barrier(G.bar_id, 128);   // every result read before the tile is written again
 }
 
 // The learned field with its fallback and audit, for one group; `side`

@@ -1,12 +1,21 @@
 // mbt_philox.cuh -- counter-based normal deviates for quantum excitation.
 //
-// Philox4x32-10 (J. K. Salmon, M. A. Moraes, R. O. Dror, D. E. Shaw,
+// Philox4x32 (J. K. Salmon, M. A. Moraes, R. O. Dror, D. E. Shaw,
 // "Parallel random numbers: as easy as 1, 2, 3", SC'11), keyed by the
 // run seed, with the counter (particle index in its bunch, bucket, turn,
 // block).  Normals come from the Box-Muller transform in single precision,
 // matching the single-precision deviates of the reference's generator
 // (bunch.c:407-436).  Every (seed, bucket, particle, turn) gets the same
 // deviates whatever the tiling or launch shape.
+//
+// Rounds: the five deviates a macroparticle draws every turn
+// (turn_normals1) use kTurnPhiloxRounds = 7, the fewest rounds with which
+// Philox4x32 passes all of TestU01's SmallCrush, Crush and BigCrush
+// batteries in its authors' tests (their recommended default, 10, adds a
+// safety margin of three rounds).  The particle pass is bound by
+// instruction issue, and the three rounds are about 2 % of its
+// instructions.  Everything else (the beam generator, the ions of the
+// beam-ion stage, the training samples of the learned field) uses 10.
 #pragma once
 #include <cstdint>
 
@@ -66,11 +75,15 @@ __host__ __device__ inline PhiloxKeys philox_keys(uint64_t seed) {
   return K;
 }
 
-__device__ __forceinline__ U4 philox4x32_10k(U4 c, const PhiloxKeys &K) {
+template <int R>
+__device__ __forceinline__ U4 philox4x32_rk(U4 c, const PhiloxKeys &K) {
+  static_assert(R >= 7 && R <= 10, "7 to 10 rounds");
 #pragma unroll
-  for (int i = 0; i < 10; ++i) c = philox_round(c, K.k0[i], K.k1[i]);
+  for (int i = 0; i < R; ++i) c = philox_round(c, K.k0[i], K.k1[i]);
   return c;
 }
+__device__ __forceinline__ U4 philox4x32_10k(U4 c, const PhiloxKeys &K) { return philox4x32_rk<10>(c, K); }
+constexpr int kTurnPhiloxRounds = 7;
 
 // Uniform (0, 1] from the top 23 bits of a word, built in the mantissa of
 // a float in [1, 2) (exact, no integer conversion).
@@ -114,12 +127,12 @@ __device__ __forceinline__ void box_muller_u(float u1, uint32_t angle_word, floa
 }
 
 // The five deviates one particle draws per turn, in the reference's roles
-// g[0] energy, g[1] z, g[2] z', g[3] x, g[4] x', from ONE Philox call: its
-// 128 bits give three (23-bit radius, 18-bit angle) pairs.
+// g[0] energy, g[1] z, g[2] z', g[3] x, g[4] x', from ONE Philox4x32-7
+// call: its 128 bits give three (23-bit radius, 18-bit angle) pairs.
 __device__ __forceinline__ void turn_normals1(const PhiloxKeys &K, uint32_t particle, uint32_t bucket,
                                               uint64_t turn, float g[5]) {
   const U4 c0 = {particle, bucket, (uint32_t)turn, ((uint32_t)(turn >> 32) << 1) | 0u};
-  const U4 r = philox4x32_10k(c0, K);
+  const U4 r = philox4x32_rk<kTurnPhiloxRounds>(c0, K);
   box_muller_u(u01_open0(r.x), r.y, g[0], g[1]);
   box_muller_u(u01_open0(r.z), r.w, g[2], g[3]);
   // fifth deviate from the low bits: radius 9 + 14 = 23 bits, angle 18 bits

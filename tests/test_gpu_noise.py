@@ -1,4 +1,4 @@
-"""The counter-based noise of the device path (Philox4x32-10 + Box-Muller)
+"""The counter-based noise of the device path (Philox4x32-7 + Box-Muller)
 against the reference's generator, statistically: the equilibrium beam
 sizes it produces, and reproducibility for a fixed seed."""
 import numpy as np

@@ -772,8 +772,8 @@ def beam_ion_record(args, tmp):
     rec["faddeeva"]["fp64_pipe_active"] = {"value": 0.30, "from": "profiles/beam_ion_faddeeva.md (ncu, small case: "
                                                          "bi_ions 0.313, bi_kick_grouped 0.275, weighted by "
                                                          "their full-size times)"}
-    rec["learned"]["xu_pipe_active"] = {"value": 0.69, "from": "profiles/beam_ion_learned_field.md (ncu, small case: "
-                                                      "bi_ions_mlp 0.69, bi_kick_mlp 0.59)"}
+    rec["learned"]["xu_pipe_active"] = {"value": 0.72, "from": "profiles/beam_ion_learned_field.md (ncu, small case: "
+                                                      "bi_ions_mlp 0.72)"}
     if args.growth_turns_bi > 0:
         rec["growth_check"] = growth_check(cfg, mlp, args.growth_turns_bi)
     mlp.close()

@@ -46,7 +46,7 @@ __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst
                                                  bool kick_h, const double *kL, const double *kV,
                                                  const double *kH, int nc, double eps_const, double phai0,
                                                  double sin_ph, double cos_ph, int kb, uint32_t jb,
-                                                 long turn, size_t p) {
+                                                 long turn, size_t p, bool disp) {
   if (rw) {
     if (oc.track_h) xp = xp + rwH;
     if (oc.track_v) zp = zp + rwV;
@@ -133,12 +133,18 @@ __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst
     else sincos(psi, &sn, &cs);
     const double a11 = cs + oc.alphaH * sn;
     const double a12 = oc.betaH * sn;
-    const double a13 = (1.0 - a11) * oc.dispH - a12 * oc.disppH;
     const double a21 = -oc.gammaH * sn;
     const double a22 = cs - oc.alphaH * sn;
-    const double a23 = -a21 * oc.dispH + (1.0 - a22) * oc.disppH;
-    x = a11 * x0 + a12 * xp0 + a13 * eps;
-    xp = a21 * x0 + a22 * xp0 + a23 * eps;
+    if (disp) {
+      const double a13 = (1.0 - a11) * oc.dispH - a12 * oc.disppH;
+      const double a23 = -a21 * oc.dispH + (1.0 - a22) * oc.disppH;
+      x = a11 * x0 + a12 * xp0 + a13 * eps;
+      xp = a21 * x0 + a22 * xp0 + a23 * eps;
+    } else {
+      // no dispersion at the kick point: the energy terms vanish
+      x = a11 * x0 + a12 * xp0;
+      xp = a21 * x0 + a22 * xp0;
+    }
     if (NOISE != MBT_NOISE_NONE) {
       x = x + oc.qh_pos * (double)dv[3];
       xp = rff * xp + oc.qh_slope * (double)dv[4];
@@ -293,6 +299,7 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
   const bool kick_h = sf && a.lr_kick[1];
   const bool kick_v = sf && a.lr_kick[2];
   const int jb0 = tile.start - a.bunch_off[b];   // index of the tile's first particle in its bunch
+  const bool disp = oc.dispH != 0.0 || oc.disppH != 0.0;
   // moments: warp w < 4 owns coordinate column w (xtau, x, z, eps) of every
   // staged chunk; warps 4 and 6 share column 4 (x') and the cross product
   // x x', warps 5 and 7 column 5 (z') and z z', each on half of the chunk.
@@ -321,7 +328,7 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
       if (MOVE && live) {
         advance_particle<NOISE>(a, oc, v[0], v[1], v[2], v[3], v[4], v[5], rw, rwH, rwV, sf, kick_l, kick_v, kick_h,
                                 kL, kV, kH, nc, eps_const, phai0, sin_ph, cos_ph, kb, (uint32_t)(jb0 + i), turn,
-                                (size_t)tile.start + i);
+                                (size_t)tile.start + i, disp);
 #pragma unroll
         for (int k = 0; k < 6; ++k) st[k * kChunk + e] = v[k];
       }

@@ -39,17 +39,24 @@ namespace mbt {
 
 // One macroparticle through the pending RW kick, the wake kick and the
 // one-turn map (transform_weak.c:21-192); coordinates updated in place.
-template <int NOISE>
+// PLAIN: the common ring of a launch, known at compile time: all three
+// planes tracked, RF without harmonic cavities, no amplitude detuning, no
+// dispersion at the kick point (the general form tests each of these per
+// particle, or computes the unused terms under a predicate).
+template <int NOISE, bool PLAIN>
 __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst &oc, double &xtau, double &x,
                                                  double &z, double &eps, double &xp, double &zp, bool rw,
                                                  double rwH, double rwV, bool sf, bool kick_l, bool kick_v,
                                                  bool kick_h, const double *kL, const double *kV,
                                                  const double *kH, int nc, double eps_const, double phai0,
                                                  double sin_ph, double cos_ph, int kb, uint32_t jb,
-                                                 long turn, size_t p, bool disp) {
+                                                 long turn, size_t p, bool disp_) {
+  const bool track_h = PLAIN || oc.track_h, track_v = PLAIN || oc.track_v;
+  const bool ideal_hc = !PLAIN && oc.ideal_hc, amp_dep = !PLAIN && oc.amp_dep, disp = !PLAIN && disp_;
+  const int n_ahc = PLAIN ? 0 : oc.n_ahc;
   if (rw) {
-    if (oc.track_h) xp = xp + rwH;
-    if (oc.track_v) zp = zp + rwV;
+    if (track_h) xp = xp + rwH;
+    if (track_v) zp = zp + rwV;
   }
   if (sf) {
     int ic = bin_fast(xtau, oc.sigma_tau, oc.nsigma, oc.dT, oc.inv_sigma_tau, oc.inv_dT);
@@ -61,7 +68,7 @@ __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst
   // ---- longitudinal (transform_weak.c:49-97)
   const double xtau0 = xtau, eps0 = eps, x0 = x, xp0 = xp, z0 = z, zp0 = zp;
   double g;
-  if (!oc.ideal_hc) {
+  if (!ideal_hc) {
     // sin(wrf xtau + phai0) with the reference's rounding of the argument
     const double arg = __dadd_rn(__dmul_rn(oc.wrf, xtau0), phai0);
     const double d = arg - phai0;
@@ -70,7 +77,7 @@ __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst
     if (fabs(d) <= 0.25) sincos_near_full(d, sin_ph, cos_ph, sr, cr);
     else sr = sin(arg);
     g = eps_const * sr;
-    for (int j = 0; j < oc.n_ahc; ++j) {
+    for (int j = 0; j < n_ahc; ++j) {
       const double ph = oc.ahc_nhc[j] * (double)kb * 2 * MBT_PI;
       g += oc.ahc_amp[j] * sin(oc.ahc_w[j] * xtau0 + oc.ahc_phi[j] + ph);
     }
@@ -102,13 +109,13 @@ __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst
   xtau = xtau0 - eps * oc.T0 * oc.ac;
   // ---- amplitude terms (transform_weak.c:115-123, 159-167)
   double EV = 0.0, EH = 0.0;
-  if (oc.amp_dep) {
+  if (amp_dep) {
     EV = oc.gammaV * z0 * z0 + 2 * oc.alphaV * z0 * zp0 + oc.betaV * zp0 * zp0;
     EH = oc.gammaV * x0 * x0 + 2 * oc.alphaV * x0 * xp0 + oc.betaV * xp0 * xp0;
   }
   // ---- vertical (transform_weak.c:101-141)
-  if (oc.track_v) {
-    const double dQ = oc.amp_dep ? (oc.CVH * EH + oc.CVV * EV) : 0.0;
+  if (track_v) {
+    const double dQ = amp_dep ? (oc.CVH * EH + oc.CVV * EV) : 0.0;
     const double psi = __dmul_rn(oc.psiV0, __dadd_rn(__dadd_rn(1.0, __dmul_rn(oc.Gziz, eps0)), dQ));
     double sn, cs;
     const double d = psi - oc.psiV0;
@@ -124,8 +131,8 @@ __device__ __forceinline__ void advance_particle(const Args &a, const OpticConst
     }
   }
   // ---- horizontal (transform_weak.c:144-190)
-  if (oc.track_h) {
-    const double dQ = oc.amp_dep ? (oc.CHH * EH + oc.CHV * EV) : 0.0;
+  if (track_h) {
+    const double dQ = amp_dep ? (oc.CHH * EH + oc.CHV * EV) : 0.0;
     const double psi = __dmul_rn(oc.psiH0, __dadd_rn(__dadd_rn(1.0, __dmul_rn(oc.Gzix, eps0)), dQ));
     double sn, cs;
     const double d = psi - oc.psiH0;
@@ -300,6 +307,7 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
   const bool kick_v = sf && a.lr_kick[2];
   const int jb0 = tile.start - a.bunch_off[b];   // index of the tile's first particle in its bunch
   const bool disp = oc.dispH != 0.0 || oc.disppH != 0.0;
+  const bool plain = oc.track_h && oc.track_v && !oc.ideal_hc && oc.n_ahc == 0 && !oc.amp_dep && !disp;
   // moments: warp w < 4 owns coordinate column w (xtau, x, z, eps) of every
   // staged chunk; warps 4 and 6 share column 4 (x') and the cross product
   // x x', warps 5 and 7 column 5 (z') and z z', each on half of the chunk.
@@ -326,9 +334,14 @@ __global__ void __launch_bounds__(kMapThreads, MBT_MAP_MIN_BLOCKS) turn_map(Args
 #pragma unroll
       for (int k = 0; k < 6; ++k) v[k] = live ? st[k * kChunk + e] : 0.0;
       if (MOVE && live) {
-        advance_particle<NOISE>(a, oc, v[0], v[1], v[2], v[3], v[4], v[5], rw, rwH, rwV, sf, kick_l, kick_v, kick_h,
-                                kL, kV, kH, nc, eps_const, phai0, sin_ph, cos_ph, kb, (uint32_t)(jb0 + i), turn,
-                                (size_t)tile.start + i, disp);
+        if (plain)
+          advance_particle<NOISE, true>(a, oc, v[0], v[1], v[2], v[3], v[4], v[5], rw, rwH, rwV, sf, kick_l, kick_v,
+                                        kick_h, kL, kV, kH, nc, eps_const, phai0, sin_ph, cos_ph, kb,
+                                        (uint32_t)(jb0 + i), turn, (size_t)tile.start + i, disp);
+        else
+          advance_particle<NOISE, false>(a, oc, v[0], v[1], v[2], v[3], v[4], v[5], rw, rwH, rwV, sf, kick_l, kick_v,
+                                         kick_h, kL, kV, kH, nc, eps_const, phai0, sin_ph, cos_ph, kb,
+                                         (uint32_t)(jb0 + i), turn, (size_t)tile.start + i, disp);
 #pragma unroll
         for (int k = 0; k < 6; ++k) st[k * kChunk + e] = v[k];
       }

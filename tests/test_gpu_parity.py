@@ -319,3 +319,32 @@ def test_tile_sizes_do_not_change_the_physics(tmp_path, cuda_device):
     from tests.util import stats_err
     assert stats_err(out[1][0], out[0][0]).max() < 1e-11
     assert np.array_equal(out[1][1], out[0][1])
+
+
+def test_plain_and_general_particle_maps_agree(tmp_path, cuda_device, libmbt):
+    """The particle pass compiles the map twice: for the common ring (all
+    planes tracked, no harmonic cavity, no amplitude detuning, no dispersion
+    at the kick point), chosen per launch, and in its general form.  The same
+    ring with one active harmonic cavity of zero voltage runs the general
+    form; with the same beam and the same Philox noise both give the same
+    turns to the parity tolerances (the two forms round alike but the
+    compiler may contract their multiply-adds differently)."""
+    runs = []
+    for i, extra in enumerate(("", "\n[active_HC_1]\n  Vpeak = 0.0\n  nHC = 3.0\n  phi_aHC = 0.0\n")):
+        d = tmp_path / ("run%d" % i)
+        d.mkdir()
+        path = small_conf(d, "single_bunch.conf", Np=4096, EnableQuantum=1, xxCM_offset=0.05, zzCM_offset=0.02)
+        with open(path, "a") as f:
+            f.write(extra)
+        cfg = api.Config(path)
+        assert cfg.params.n_active_hc == i
+        t = api.Tracker.from_config(cfg, seed=4321)
+        t.generate_beam(11)
+        t.prepare()
+        st = t.run(40)
+        runs.append((st, t.get_particles(0)))
+        t.close()
+    (sa, pa), (sb, pb) = runs
+    assert np.max(stats_err(sb, sa)) < STATS_TOL
+    assert np.max(centroid_err(sb, sa)) < STATS_TOL
+    assert np.max(coord_err(pb, pa)) < COORD_TOL

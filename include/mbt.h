@@ -532,13 +532,10 @@ int mbt_gauss_field_dev(long n, const double *dx_dev, const double *dy_dev,
  * and FP32 accumulation: the inputs and the biases enter as BF16 pairs
  * (high and low part) through extra columns of the operands, the
  * activations are GELU in its sigmoid form, z sigma(1.702 z), evaluated in
- * FP32 and rounded to BF16: with the hardware tanh, or, for the first
- * MBT_MLP_POLY_UNITS units of each hidden layer, with an odd polynomial of
- * tanh over a clamped argument (within 3.5e-3 of tanh) on the FMA pipes.
+ * FP32 with the hardware tanh and rounded to BF16.
  * Parameters (FP32 masters): MBT_MLP_NPARAM floats, W1[128][3], b1[128],
  * W2[128][128], b2, W3[128][128], b3, W4[2][128], b4[2]. */
 #define MBT_MLP_NPARAM 33794
-#define MBT_MLP_POLY_UNITS 0
 
 /* Network with seeded Glorot-uniform weights, zero biases. */
 int mbt_mlp_create(uint64_t seed, mbt_mlp **out);

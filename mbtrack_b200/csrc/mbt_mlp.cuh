@@ -51,7 +51,6 @@
 #include <cuda_fp16.h>
 #include <cstdint>
 
-#include "mbt.h"
 #include "mbt_common.cuh"
 
 namespace mbt {
@@ -223,44 +222,6 @@ __device__ __forceinline__ uint32_t act_bf16x2(float w0, float w1) {
       : "f"(w0), "f"(w1), "f"(t0), "f"(t1));
   return h;
 }
-// The same activation on the FMA pipes, for the first kMlpPolyUnits units of
-// every hidden layer: the hardware tanh of the other units runs on the
-// multi-function unit, which issues 16 results per clock per SM, and with
-// every unit there it bounds the network; these units move a share of the
-// activations to the FP32-pair FMA pipe.  tanh(u) for u clamped to
-// [-kPolyA, kPolyA] is the odd polynomial t = v Q(v^2), v = u / (2 kPolyA),
-// Q of degree 5 (coefficients kPolyC, a minimax fit of tanh over all u with
-// t(kPolyA) = 1: |t - tanh(u)| <= 3.5e-3, so t reaches the limits 0 and 2w of
-// h' beyond the clamp exactly as tanh does).  In FP32: s = sat(w / (2 kPolyA)
-// + 1/2), v = s - 1/2, Horner in v^2, h' = w + (w v) Q, rounded once to BF16
-// (the oracle repeats these FP32 steps exactly).
-constexpr int kMlpPolyUnits = MBT_MLP_POLY_UNITS;    // units 0 .. kMlpPolyUnits - 1 of each hidden layer
-constexpr int kMlpPolyChunks = kMlpPolyUnits / 8;    // in 8-unit chunks
-static_assert(kMlpPolyUnits % 8 == 0 && kMlpPolyUnits <= 128, "whole chunks of a hidden layer");
-constexpr float kPolyA = 3.25f, kPolyAlpha = 0.15384616f;   // alpha = 1 / (2 kPolyA) in FP32
-constexpr float kPolyC0 = 6.39387608f, kPolyC1 = -74.8484726f, kPolyC2 = 714.953674f, kPolyC3 = -4046.01587f,
-                kPolyC4 = 11861.9072f, kPolyC5 = -13806.5342f;
-__device__ __forceinline__ float fma_sat(float a, float b, float c) {
-  float r;
-  asm("fma.rn.sat.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-  return r;
-}
-__device__ __forceinline__ uint32_t act_poly_bf16x2(float w0, float w1) {
-  const float2 w = make_float2(w0, w1);
-  const float2 s = make_float2(fma_sat(w0, kPolyAlpha, 0.5f), fma_sat(w1, kPolyAlpha, 0.5f));
-  const float2 v = __fadd2_rn(s, make_float2(-0.5f, -0.5f));
-  const float2 v2 = __fmul2_rn(v, v);
-  float2 q = __ffma2_rn(make_float2(kPolyC5, kPolyC5), v2, make_float2(kPolyC4, kPolyC4));
-  q = __ffma2_rn(q, v2, make_float2(kPolyC3, kPolyC3));
-  q = __ffma2_rn(q, v2, make_float2(kPolyC2, kPolyC2));
-  q = __ffma2_rn(q, v2, make_float2(kPolyC1, kPolyC1));
-  q = __ffma2_rn(q, v2, make_float2(kPolyC0, kPolyC0));
-  const float2 h = __ffma2_rn(__fmul2_rn(w, v), q, w);
-  uint32_t r;
-  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(h.y), "f"(h.x));
-  return r;
-}
-
 __device__ __forceinline__ void unpack_bf16x2(uint32_t h, float &lo, float &hi) {
   lo = __uint_as_float(h << 16);
   hi = __uint_as_float(h & 0xFFFF0000u);
@@ -376,8 +337,7 @@ __device__ __forceinline__ void mlp_act16(const MlpGroup &G, int ch, const float
     const int cc = ch + c;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
-      h[i] = cc < kMlpPolyChunks ? act_poly_bf16x2(v[8 * c + 2 * i], v[8 * c + 2 * i + 1])
-                                 : act_bf16x2(v[8 * c + 2 * i], v[8 * c + 2 * i + 1]);
+      h[i] = act_bf16x2(v[8 * c + 2 * i], v[8 * c + 2 * i + 1]);
     st_shared_v4((G.sA ^ (uint32_t)((cc & 7) << 4)) + (uint32_t)(cc >> 3) * 16384u, h[0], h[1], h[2], h[3]);
     if (zs) {
       const int k0 = 8 * cc;

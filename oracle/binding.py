@@ -608,17 +608,6 @@ def mlp_forward(params, abr):
     return out
 
 
-def mlp_act(poly, x):
-    """orc_mlp_act: a hidden unit's activation h' = k gelu(z) of the scaled
-    pre-activations x = c z, polynomial (poly) or tanh form."""
-    L = ctypes.CDLL(build_oracle())
-    xx = np.ascontiguousarray(x, dtype=np.float32)
-    out = np.zeros_like(xx)
-    L.orc_mlp_act.argtypes = [ctypes.c_int, ctypes.c_long, _vp, _vp]
-    L.orc_mlp_act(int(bool(poly)), xx.size, _ptr(xx), _ptr(out))
-    return out
-
-
 def mlp_gradient(params, abr, tgt):
     """orc_mlp_gradient: (gradient, loss) of one batch."""
     L = ctypes.CDLL(build_oracle())

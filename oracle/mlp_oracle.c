@@ -16,8 +16,6 @@
 #include <stdlib.h>
 #include <string.h>
 
-#include "mbt.h"
-
 #define H 128
 #define W1 0
 #define B1 384
@@ -56,26 +54,6 @@ static float act(float x)
   return bf16r(fmaf(x, th, x));
 }
 
-/* The polynomial activation of the first POLY_UNITS units of every hidden
- * layer (act_poly_bf16x2): tanh(u), u = x clamped to [-3.25, 3.25], by the
- * odd polynomial v Q(v^2), v = u / 6.5, in the kernel's FP32 steps:
- * s = sat(x alpha + 1/2), v = s - 1/2, Horner in v^2, h' = x + (x v) Q,
- * rounded once to BF16. */
-#define POLY_UNITS MBT_MLP_POLY_UNITS
-static float act_poly(float x)
-{
-  float s = fmaf(x, 0.15384616f, 0.5f), v, v2, q;
-  s = s > 0.0f ? (s < 1.0f ? s : 1.0f) : 0.0f;   /* .sat: [0, 1], NaN -> 0 */
-  v = s - 0.5f;
-  v2 = v * v;
-  q = fmaf(-13806.5342f, v2, 11861.9072f);
-  q = fmaf(q, v2, -4046.01587f);
-  q = fmaf(q, v2, 714.953674f);
-  q = fmaf(q, v2, -74.8484726f);
-  q = fmaf(q, v2, 6.39387608f);
-  return bf16r(fmaf(x * v, q, x));
-}
-
 /* derivative of gelu(x) = x sigma(k x): s + k x s (1 - s) */
 static float gelu_grad(float x)
 {
@@ -111,21 +89,21 @@ static void forward_one(const float *P, const float *abr, fwd_t *f)
   for (j = 0; j < H; j++) {
     double s = bias_pair(GELU_C * P[B1 + j]);
     for (i = 0; i < 3; i++) s += (double) bf16r(GELU_C * P[W1 + 3 * j + i]) * ((double) xh[i] + (double) xl[i]);
-    h[j] = j < POLY_UNITS ? act_poly((float) s) : act((float) s);
+    h[j] = act((float) s);
     f->z1[j] = GELU_INV_C * (float) s;
     f->h1[j] = GELU_INV_K * h[j];
   }
   for (j = 0; j < H; j++) {
     double s = bias_pair(GELU_C * P[B2 + j]);
     for (k = 0; k < H; k++) s += (double) h[k] * (double) bf16r(0.5f * P[W2 + H * j + k]);
-    hn[j] = j < POLY_UNITS ? act_poly((float) s) : act((float) s);
+    hn[j] = act((float) s);
     f->z2[j] = GELU_INV_C * (float) s;
     f->h2[j] = GELU_INV_K * hn[j];
   }
   for (j = 0; j < H; j++) {
     double s = bias_pair(GELU_C * P[B3 + j]);
     for (k = 0; k < H; k++) s += (double) hn[k] * (double) bf16r(0.5f * P[W3 + H * j + k]);
-    h[j] = j < POLY_UNITS ? act_poly((float) s) : act((float) s);
+    h[j] = act((float) s);
     f->z3[j] = GELU_INV_C * (float) s;
     f->h3[j] = GELU_INV_K * h[j];
   }
@@ -134,15 +112,6 @@ static void forward_one(const float *P, const float *abr, fwd_t *f)
     for (k = 0; k < H; k++) s += (double) h[k] * (double) bf16r(GELU_INV_K * P[W4 + H * j + k]);
     f->out[j] = (float) s;
   }
-}
-
-/* The two activations of a hidden unit on n scaled pre-activations x = c z:
- * poly != 0 the polynomial (units below POLY_UNITS), else the tanh form;
- * out = h' = k gelu(z) as each computes it (BF16 values). */
-void orc_mlp_act(int poly, long n, const float *x, float *out)
-{
-  long i;
-  for (i = 0; i < n; i++) out[i] = poly ? act_poly(x[i]) : act(x[i]);
 }
 
 void orc_mlp_forward(const float *P, long n, const float *abr, float *out)

@@ -260,3 +260,23 @@ def test_checkpoint_resume(tmp_path, cuda_device):
     with pytest.raises(api.MbtError):
         b.checkpoint_load(bad)
     assert b.turn == 20
+
+
+def test_growth_rate_against_the_per_particle_stage(cuda_device):
+    """The slice model (BunchModel = STRONG, the reference's fast beam-ion
+    interaction) and the per-particle weak-strong beam-ion stage are two
+    models of the same instability; on one shared configuration (the
+    200-bunch train, CO at the slice model's pressure over the whole ring,
+    no wall, no chromaticity, no radiation noise) their vertical growth
+    rates agree within a factor of 3 with the physical (thin-lens) ion kick
+    of the slice model, which grows the slower of the two (its ions sit on
+    a coarse grid around the slice centroids and kick rigid slices); the
+    reference's ion kick factor 1e2 makes the slice model grow far faster."""
+    import bench
+    r = bench.slice_growth_compare(3000)
+    thin, ref, per = r["slice_kick_factor_1"], r["slice_kick_factor_100"], r["per_particle"]
+    for x in (thin, per):
+        assert x["window"] is not None and x["rate_per_turn"] > 0, x
+    assert 1.0 <= per["rate_per_turn"] / thin["rate_per_turn"] <= 3.0, (per["rate_per_turn"], thin["rate_per_turn"])
+    # after 100 turns the reference's kick factor has grown the motion far beyond the thin-lens run
+    assert ref["amplitude_every_100_turns"][1] > 10 * thin["amplitude_every_100_turns"][1], (ref, thin)
